@@ -1,0 +1,138 @@
+"""The CPU oracle against the reference's own outputs (fixtures made by tests/golden/make_golden.py).
+
+Tolerances: the SHT and the modal state agree with the reference to round-off (1e-13 relative);
+solver steps to 1e-9 m in topography and radial displacement with identical iteration counts and
+identical ocean / grounded-ice masks, the bar the reference sets for its own implementations
+(tests/test_fortran_python.sh:37-47 of the reference).
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, FixtureLove, load_golden
+from oracle.memory import ModalState
+from oracle.sht import OracleSHT, gauss_nodes
+from oracle.solver import OracleSolver
+
+TOL_M = 1e-9
+
+
+@pytest.mark.parametrize("n,L", [(16, 15), (32, 31), (32, 20), (64, 63)])
+def test_sht_against_reference(n, L):
+    fx = load_golden("sht.npz")
+    tag = f"n{n}_l{L}"
+    z, w = gauss_nodes(n)
+    assert np.array_equal(z, fx[f"{tag}_nodes"])
+    assert np.array_equal(w, fx[f"{tag}_weights"])
+    s = OracleSHT(n, 2 * n, L)
+    a = s.analysis(fx[f"{tag}_grid"])
+    ref = fx[f"{tag}_ana"]
+    assert np.abs(a - ref).max() <= 1e-13 * np.abs(ref).max()
+    g = s.synthesis(fx[f"{tag}_coef"])
+    ref = fx[f"{tag}_syn"]
+    assert np.abs(g - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_modal_state_against_reference():
+    fx = load_golden("memory.npz")
+    love = FixtureLove(fx)
+    love.he = love.ke = love.hTE = love.kTE = np.zeros(int(fx["lmax"]) + 1)
+    st = ModalState(love, int(fx["lmax"]), 1.0)
+    worst = 0.0
+    for n, dt in enumerate(fx["dts"]):
+        st.set_dt(dt)
+        out = st.advance_and_read()
+        for got, key in zip(out, ("visc", "rad", "sum_il", "sum_m", "sum_tsl", "sum_trr")):
+            ref = fx[key][n]
+            sc = max(np.abs(ref).max(), 1e-300)
+            worst = max(worst, np.abs(got - ref).max() / sc)
+        st.commit(fx["load"][n], fx["dil"][n], fx["dm"][n], fx["dlam"][n])
+    assert worst <= 1e-13, worst
+
+
+def _love_and_topo(fx):
+    love = FixtureLove(fx)
+    topo = fx["topo_mm"] / 1000.0 if "topo_mm" in fx else fx["topo"]
+    return love, topo
+
+
+def _check_run(slv, fx, prefix, ice_fn, nsteps, saved):
+    numiter = []
+    for k in range(1, nsteps + 1):
+        r = slv.step(ice_fn(k))
+        numiter.append(r["numiter"])
+        if f"{prefix}tgrid_{k}" in fx:
+            assert np.abs(r["tgrid"] - fx[f"{prefix}tgrid_{k}"]).max() <= TOL_M, k
+            assert np.abs(r["R"] - fx[f"{prefix}R_{k}"]).max() <= TOL_M, k
+            oc = np.unpackbits(fx[f"{prefix}ocean_{k}"])[: r["ocean"].size].reshape(r["ocean"].shape)
+            be = np.unpackbits(fx[f"{prefix}beta_{k}"])[: r["beta"].size].reshape(r["beta"].shape)
+            assert np.array_equal(r["ocean"] != 0, oc != 0), k
+            assert np.array_equal(r["beta"] != 0, be != 0), k
+        for key in ("gmslc_ocn", "gmslc_ocnBeta", "ocean_area", "oceanBeta_area", "ice_volume"):
+            ref = fx[f"{prefix}{key}"][k - 1]
+            assert abs(r[key] - ref) <= 1e-9 * max(1.0, abs(ref)), (k, key)
+    assert numiter == list(fx[f"{prefix}numiter"])
+
+
+def test_step_c0_plain_against_reference():
+    from slevolve_b200.synthetic import case_c0
+    fx = load_golden("step_c0.npz")
+    love, topo = _love_and_topo(fx)
+    sht = OracleSHT(64, 128, 63)
+    case = case_c0(sht)
+    assert np.array_equal(case.topo, topo), "c0 topography generator drifted from the fixture"
+    slv = OracleSolver(sht, love, topo, case.ice(0), norder=63, dt=1.0)
+    _check_run(slv, fx, "plain_", case.ice, 100, None)
+
+
+def test_step_c0_extrap_against_reference():
+    from slevolve_b200.synthetic import case_c0
+    fx = load_golden("step_c0.npz")
+    love, topo = _love_and_topo(fx)
+    sht = OracleSHT(64, 128, 63)
+    case = case_c0(sht)
+    slv = OracleSolver(sht, love, topo, case.ice(0), norder=63, dt=1.0, opt={"dsl"}, inner="extrap")
+    numiter = []
+    for k in range(1, 101):
+        r = slv.step(case.ice(k))
+        numiter.append(r["numiter"])
+        if f"extrap_tgrid_{k}" in fx:
+            assert np.abs(r["tgrid"] - fx[f"extrap_tgrid_{k}"]).max() <= TOL_M
+    assert numiter == list(fx["extrap_numiter"])
+
+
+def test_step_marine_against_reference():
+    from tests_helpers import marine_ice
+    fx = load_golden("step_marine.npz")
+    love, topo = _love_and_topo(fx)
+    sht = OracleSHT(64, 128, 63)
+    ice = marine_ice(sht.gaulats, 128, fx["ice_heights"])
+    slv = OracleSolver(sht, love, topo, ice[0], norder=63, dt=1000.0)
+    _check_run(slv, fx, "plain_", lambda k: ice[k], 8, None)
+    assert slv.gr_counts["reguess"] > 0
+
+
+def test_step_c1_small_against_reference():
+    from slevolve_b200.synthetic import case_c1
+    fx = load_golden("step_c1s.npz")
+    love, topo = _love_and_topo(fx)
+    sht = OracleSHT(64, 128, 63)
+    case = case_c1(sht, nsteps=60)
+    assert np.array_equal(case.topo, topo)
+    probe = np.array([float(np.abs(case.ice(k)).sum()) for k in range(61)])
+    assert np.array_equal(probe, fx["ice_probe"])
+    slv = OracleSolver(sht, love, topo, case.ice(0), norder=63, dt=1.0)
+    _check_run(slv, fx, "plain_", case.ice, 60, None)
+    assert slv.gr_counts["ice_analyses"] > 0   # the grounded re-guess changed the mask
+
+
+def test_synthetic512_oracle_record():
+    """The oracle reproduced the reference's shipped L=511 golden grid when the fixtures were made."""
+    with open(os.path.join(GOLDEN, "golden_meta.json")) as fh:
+        meta = json.load(fh)
+    rec = meta["synthetic512_oracle"]
+    assert rec["max_abs_vs_tgrid8_m"] <= TOL_M
+    assert rec["numiter"] == [5, 5, 6, 6, 5, 5, 5, 5]
