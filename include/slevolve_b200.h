@@ -1,0 +1,153 @@
+/*
+ * slevolve_b200.h -- C ABI of the B200 (sm_100a) implementation of the SLEvolve
+ * per-time-step sea-level path.
+ *
+ * Every entry point returns an int status (SLE_OK = 0).  On failure,
+ * sle_last_error() returns a message for the calling thread.  Nothing here
+ * aborts, traps or exits.  No torch or CUDA types appear in the signatures:
+ * streams are passed as void* (a cudaStream_t, NULL = the handle's own stream),
+ * device buffers as plain pointers.
+ *
+ * Layouts (identical to the reference Python package):
+ *   grid    float64 [nlat][nlon], Gauss-Legendre rows north -> south.
+ *   dense   complex128 [lmax+1][lmax+1] as [l][m] (interleaved re, im),
+ *           zero for m > l.
+ *   packed  complex128, order-major triangle: order m holds degrees
+ *           l = m..lmax contiguously, offset(m) = m*(lmax+1) - m*(m-1)/2.
+ *
+ * Reference interfaces replaced (SLEvolve, python/slevolve/):
+ *   sle_sht_*     sht.py:148-343 (SHT.__init__/analysis/synthesis, the
+ *                 transform the reference documents as the GPU plug-in point,
+ *                 sht.py:43-46) and sht_ducc.py:206-217 (make_sht).
+ *   sle_solver_*  solver.py:521-644 (SeaLevelSolver.__init__, step 0),
+ *                 solver.py:814-1144 (SeaLevelSolver.step) and the
+ *                 fixed-point-preserving options of solver_opt.py:267-979
+ *                 (dsl, diag, inner="extrap", reuse="warm").
+ */
+#ifndef SLEVOLVE_B200_H
+#define SLEVOLVE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SLE_ABI_VERSION 1
+
+enum sle_status {
+  SLE_OK = 0,
+  SLE_ERR_BAD_SHAPE = 1,     /* ValueError in the reference (sht.py:152-155) */
+  SLE_ERR_BAD_ARG = 2,       /* ValueError (solver_opt.py:282-301) */
+  SLE_ERR_OOM = 3,           /* device allocation failed */
+  SLE_ERR_CUDA = 4,          /* a CUDA runtime call failed */
+  SLE_ERR_NONCONVERGED = 5,  /* RuntimeError at 9999 inner iterations (solver.py:1049-1050) */
+  SLE_ERR_NONFINITE = 6,     /* NaN / Inf met in the inner loop or in the inputs */
+  SLE_ERR_UNSUPPORTED = 7,   /* an option of the reference this build does not provide */
+  SLE_ERR_STATE = 8          /* call out of order (e.g. step before init) */
+};
+
+enum sle_layout { SLE_LAYOUT_DENSE = 0, SLE_LAYOUT_PACKED = 1 };
+
+/* ------------------------------------------------------------------ misc */
+int sle_abi_version(void);
+const char* sle_last_error(void);
+
+/* ------------------------------------------------------------ transforms */
+typedef struct sle_sht sle_sht;
+
+/* sht.py:151-255: nlat even, lmax <= nlon/2; nlon must be a power of two >= 8. */
+int sle_sht_create(int nlat, int nlon, int lmax, sle_sht** out);
+int sle_sht_destroy(sle_sht* plan);
+/* sizes: ncoef = packed length (lmax+1)(lmax+2)/2 */
+int sle_sht_info(const sle_sht* plan, int* nlat, int* nlon, int* lmax, long long* ncoef);
+/* fraction of the (l, m, latitude) Legendre work that is not skipped as negligible (|P~| < 1e-35) */
+int sle_sht_work_fraction(const sle_sht* plan, double* frac);
+/* Gauss-Legendre nodes mu_j (north -> south) and weights, computed on the device (sht.py:65-101). */
+int sle_sht_gauss(const sle_sht* plan, double* mu_host, double* w_host);
+/* sht.py:274-302.  nfields grids -> nfields coefficient arrays (device pointers;
+ * the pointer arrays themselves are host arrays of length nfields, 1 <= nfields <= 4). */
+int sle_sht_analysis(sle_sht* plan, int nfields, const double* const* grids_dev,
+                     void* const* coeffs_dev, int layout, void* stream);
+/* sht.py:305-343.  Im of the m = 0 coefficients is ignored (irfft semantics). */
+int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* coeffs_dev, int layout,
+                      double* const* grids_dev, void* stream);
+/* dense <-> packed conversion of one complex128 spectrum (device buffers) */
+int sle_sht_pack(sle_sht* plan, const void* dense_dev, void* packed_dev, void* stream);
+int sle_sht_unpack(sle_sht* plan, const void* packed_dev, void* dense_dev, void* stream);
+
+/* -------------------------------------------------------------- solver */
+typedef struct sle_solver sle_solver;
+
+typedef struct {
+  int nlat, nlon, lmax;
+  double dt_years;          /* step length (yr), solver.py:529 */
+  double epsilon1;          /* inner tolerance, solver.py:534 */
+  int tpw;                  /* rotational feedback */
+  int checkmarine;          /* flotation test on the ice load */
+  int calcRG;               /* radial displacement / geoid */
+  int opt_dsl;              /* deltasl = dsl + conserv*K00 (solver_opt.py:320-325) */
+  int opt_diag;             /* degree-0 diagnostics by row sums (solver_opt.py:893-916) */
+  int inner_extrap;         /* inner="extrap" first guess (solver_opt.py:148-165) */
+  /* Planet (solver.py:98-110) */
+  double radius, mass, rhoi, rhow, gacc, omega, moiA, moiC, kf;
+} sle_config;
+
+typedef struct {
+  int nmodes;               /* K = max modes per degree */
+  const int* nmod;          /* [lmax+1] modes of each degree */
+  const double* s;          /* [K][lmax+1] inverse relaxation times (1/kyr) */
+  const double* a_sl;       /* [K][lmax+1] (r' - r)/s  (solver.py:261-282) */
+  const double* a_rr;       /* [K][lmax+1] r/s */
+  const double* ttl;        /* [lmax+1] 4 pi a^3 / (M (2l+1)), 0 at l = 0 (solver.py:596-603) */
+  const double* ttlekhl;    /* [lmax+1] ttl (1 + k_l - h_l) */
+  const double* ttlhe;      /* [lmax+1] ttl h_l */
+  const double* a_il;       /* [K] degree-2 rotational weights */
+  const double* a_m;
+  const double* a_tsl;
+  const double* a_trr;
+  double kTE2, hTE2, kE2;   /* tidal k, h and load k at degree 2 */
+} sle_earth;
+
+typedef struct {
+  int iter;                 /* step counter (1-based) */
+  int numiter;              /* inner iterations of the step */
+  int status;               /* sle_status of the step */
+  int gr_reguess;           /* grounded re-guesses this step */
+  int gr_ice_analyses;      /* ice re-analyses this step */
+  double xi;                /* last convergence ratio */
+  double ocean_area, oceanBeta_area, gmslc_ocn, gmslc_ocnBeta, ice_volume;
+  double il[9];             /* [3][3] */
+  double mm[3];
+  double lam[18];           /* [3][3] complex (re, im) */
+} sle_step_info;
+
+enum sle_field {
+  SLE_F_TGRID = 0,          /* topography after the step (grid) */
+  SLE_F_OCEAN = 1,          /* ocean function (grid of 0/1) */
+  SLE_F_BETA = 2,           /* grounded-ice complement mask (grid of 0/1) */
+  SLE_F_R = 3,              /* radial displacement (grid) */
+  SLE_F_G = 4,              /* deltasl + R (grid) */
+  SLE_F_DELTASL = 5,        /* sea-level change (grid) */
+  SLE_F_DS_CONVERGED = 6,   /* converged ocean-load spectrum (dense complex) */
+  SLE_F_LOAD_INC = 7,       /* converged load increment spectrum (dense complex) */
+  SLE_F_ICESTAR = 8,        /* grounded ice (grid) */
+  SLE_F_OCEAN0 = 9,         /* step-0 ocean function cxy0 (grid) */
+  SLE_F_BETA0 = 10          /* step-0 grounded-ice complement beta0 (grid) */
+};
+
+int sle_solver_create(const sle_config* cfg, const sle_earth* earth, sle_solver** out);
+int sle_solver_destroy(sle_solver* s);
+/* step 0 (solver.py:550-581).  topo0, ice0: grids; *_on_device selects host or device pointers. */
+int sle_solver_init(sle_solver* s, const double* topo0, const double* ice0, int on_device,
+                    double* ocean_area0, double* oceanBeta_area0, double* ice_volume0);
+/* one time step (solver.py:814-1144).  dt_years <= 0 keeps the current step length. */
+int sle_solver_step(sle_solver* s, const double* ice, int on_device, double dt_years,
+                    sle_step_info* info);
+/* copy one output of the last step; dst is host or device memory. */
+int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device);
+/* the solver's own CUDA stream (as void*) */
+int sle_solver_stream(sle_solver* s, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SLEVOLVE_B200_H */

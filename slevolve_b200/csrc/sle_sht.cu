@@ -1,0 +1,926 @@
+// Gauss-Legendre spherical-harmonic transform for sm_100a, FP64.
+//
+// Same transform as the reference (SLEvolve python/slevolve/sht.py:148-343, Fortran spharmt):
+//   analysis   U[l,m] = (sum_j P~_lm(mu_j) (S or D by the parity of l-m)_m(j)) / 1.41421356,
+//              S/D = (F_north(m) w_j +/- F_south(m) w_j) / nlon, F = rFFT of the grid rows;
+//   synthesis  G_north/south(m, j) = 1.41421356 * sum_l U[l,m] P~_lm(mu_j) over even +/- odd l-m,
+//              grid rows = unnormalised inverse real FFT of G (Im of m = 0 ignored).
+//
+// Design (B200):
+//   * One kernel per latitude pair does the row FFTs (radix-2 Stockham in shared memory on
+//     nlon/2-point complex sequences, real/complex split) and the north/south fold.
+//   * The Legendre functions are regenerated on the fly in FP64 with a two-term recurrence
+//     Q_l = mu Q_{l-1} + be_l Q_{l-2} (P~_l = cf_l Q_l) that restarts every SEG degrees from
+//     seeds computed once per plan with the reference's own normalised recursion
+//     (sht.py:105-144).  Segments are the work units: analysis = one warp per (m, segment),
+//     latitudes spread over the lanes (8 per lane at nlat = 512), the latitude sum done by a
+//     transposing warp reduction over 8 degrees at a time; synthesis = one block per pair of
+//     orders (m, L-m) with one warp per 32-latitude group, coefficients staged in shared memory.
+//   * (segment, latitude-group) blocks whose |P~| never exceeds 1e-35 (near the poles at high
+//     m) are skipped.
+#include "sle_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+namespace sle {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+
+// --------------------------------------------------------------------------- helpers
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// Sum a per-lane vector v[0..V) over the 32 lanes of a warp.  After the call lane `l` holds
+// in v[0] the warp total of value index (l >> (5 - log2 V)).  log2(V) exchange stages each
+// halve the live values (send the half the partner keeps), then plain butterflies.
+template <int V>
+__device__ __forceinline__ void warp_transpose_reduce(double (&v)[V], int lane) {
+  static_assert(V >= 1 && V <= 32 && (V & (V - 1)) == 0, "V must be a power of two <= 32");
+#pragma unroll
+  for (int C = V, o = 16; C > 1; C >>= 1, o >>= 1) {
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int c = 0; c < C / 2; ++c) {
+      const double send = up ? v[c] : v[c + C / 2];
+      const double keep = up ? v[c + C / 2] : v[c];
+      v[c] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  constexpr int LOGV = (V >= 32) ? 5 : (V >= 16) ? 4 : (V >= 8) ? 3 : (V >= 4) ? 2 : (V >= 2) ? 1 : 0;
+#pragma unroll
+  for (int o = 16 >> LOGV; o > 0; o >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+}
+
+// ------------------------------------------------------------------- plan set-up kernels
+// Gauss-Legendre nodes and weights: the Newton iteration of the reference gaulw
+// (sht.py:65-101), per node, in the same operation order (no contraction into FMA).
+__global__ void k_gauss_nodes(int n, double tol, double* mu, double* w, int* fail) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double pi = 3.141592653589793;  // 4*atan(1) in binary64
+  double z = cos(__ddiv_rn(__dmul_rn(pi, __dsub_rn((double)(i + 1), 0.25)), __dadd_rn((double)n, 0.5)));
+  double zfin = 0.0, ppfin = 1.0;
+  bool done = false;
+  for (int sweep = 0; sweep < 10 && !done; ++sweep) {
+    double p1 = 1.0, p2 = 0.0;
+    for (int k = 1; k <= n; ++k) {
+      const double p3 = p2;
+      p2 = p1;
+      const double a = __dmul_rn(__dmul_rn(__dsub_rn(2.0 * k, 1.0), z), p2);
+      const double b = __dmul_rn(__dsub_rn((double)k, 1.0), p3);
+      p1 = __ddiv_rn(__dsub_rn(a, b), (double)k);
+    }
+    const double pp = __ddiv_rn(__dmul_rn((double)n, __dsub_rn(__dmul_rn(z, p1), p2)),
+                                __dsub_rn(__dmul_rn(z, z), 1.0));
+    const double z1 = z;
+    z = __dsub_rn(z1, __ddiv_rn(p1, pp));
+    if (fabs(__dsub_rn(z, z1)) < tol) {
+      zfin = z;
+      ppfin = pp;
+      done = true;
+    }
+  }
+  if (!done) atomicExch(fail, 1);
+  mu[i] = zfin;
+  w[i] = __ddiv_rn(2.0, __dmul_rn(__dmul_rn(__dsub_rn(1.0, __dmul_rn(zfin, zfin)), ppfin), ppfin));
+}
+
+// Seeds (Q_l0, Q_l0+1) of every (segment, latitude) and the per-(segment, group) maximum of
+// |P~|.  P~ follows the reference LEGEND recursion (sht.py:105-144) operation by operation.
+__global__ void k_legendre_tables(sle::ShtDev P, double2* seeds, double* segmax) {
+  const int m = blockIdx.x, g = blockIdx.y, lane = threadIdx.x;
+  const int j = g * 32 + lane;
+  const bool ok = j < P.nh;
+  const double x = ok ? P.mu[j] : 0.0;
+  const double sinsq = __dsub_rn(1.0, __dmul_rn(x, x));
+  double A = 1.0, B = 0.0, prod = 1.0;
+  for (int i = 1; i <= m; ++i) {
+    A = __dadd_rn(A, 2.0);
+    B = __dadd_rn(B, 2.0);
+    prod = __ddiv_rn(__dmul_rn(__dmul_rn(prod, sinsq), A), B);
+  }
+  const int L = P.lmax;
+  const double pmm = __dsqrt_rn(__dmul_rn(0.5, prod));
+  const double pm1 = __dmul_rn(__dmul_rn(__dsqrt_rn((double)(2 * m + 3)), x), pmm);
+  const int np1 = m + 1;
+  const double eps_m1 = __dsqrt_rn(__ddiv_rn((double)(np1 * np1 - m * m), (double)(4 * np1 * np1 - 1)));
+  double t = __dsub_rn(__dmul_rn(x, pm1), __dmul_rn(eps_m1, pmm));  // x P_{n-1} - eps_{n-1} P_{n-2}
+  double prev1 = 0.0;
+  double smax = 0.0;
+  double2 seed = make_double2(0.0, 0.0);
+  int seg = P.segoff[m];
+  for (int l = m; l <= L; ++l) {
+    double pl, eps_l;
+    if (l == m) {
+      pl = pmm;
+      eps_l = 0.0;
+    } else if (l == m + 1) {
+      pl = pm1;
+      eps_l = eps_m1;
+    } else {
+      eps_l = __dsqrt_rn(__ddiv_rn((double)(l * l - m * m), (double)(4 * l * l - 1)));
+      pl = __ddiv_rn(t, eps_l);
+      t = __dsub_rn(__dmul_rn(x, pl), __dmul_rn(eps_l, prev1));
+    }
+    const int r = (l - m) % SEG;
+    if (r == 0) seed.x = pl;
+    if (r == 1) seed.y = __dmul_rn(pl, eps_l);
+    smax = fmax(smax, ok ? fabs(pl) : 0.0);
+    if (r == SEG - 1 || l == L) {
+      double v = smax;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if (ok) seeds[(size_t)seg * P.nh + j] = seed;
+      if (lane == 0) segmax[(size_t)seg * P.ngrp + g] = v;
+      seed = make_double2(0.0, 0.0);
+      smax = 0.0;
+      ++seg;
+    }
+    prev1 = pl;
+  }
+}
+
+// Recurrence coefficients in segment scale: cf (P~ = cf Q) and be = -eps_{l-1}^2.
+__global__ void k_legendre_coef(sle::ShtDev P, double* be, double* cf) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.nseg) return;
+  const int m = P.seg_m[s], l0 = P.seg_l0[s];
+  const int l1 = min(l0 + SEG, P.lmax + 1);
+  const long long base = P.moff[m] + (l0 - m);
+  double c = 1.0;
+  cf[base] = 1.0;
+  be[base] = 0.0;
+  for (int l = l0 + 1; l < l1; ++l) {
+    const double eps = __dsqrt_rn(__ddiv_rn((double)(l * l - m * m), (double)(4 * l * l - 1)));
+    c = __ddiv_rn(c, eps);
+    cf[base + (l - l0)] = c;
+    const int k = l - 1;
+    be[base + (l - l0)] = -__ddiv_rn((double)(k * k - m * m), (double)(4 * k * k - 1));
+  }
+}
+
+__global__ void k_istart(sle::ShtDev P, const double* segmax, unsigned char* istart) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= P.nseg) return;
+  int g = 0;
+  while (g < P.ngrp && segmax[(size_t)s * P.ngrp + g] < SIG_THRESHOLD) ++g;
+  istart[s] = (unsigned char)g;
+}
+
+__global__ void k_lidx(sle::ShtDev P, int* lidx) {
+  const int m = blockIdx.x;
+  const long long base = P.moff[m];
+  for (int l = m + threadIdx.x; l <= P.lmax; l += blockDim.x) lidx[base + (l - m)] = l;
+}
+
+// ----------------------------------------------------------------------------- FFTs
+// Radix-2 Stockham FFT of `rows` length-n2 sequences laid out back to back in A (B is
+// scratch).  tw[t] = exp(-2 pi i t / (2 n2)); the stage twiddle exp(-+2 pi i k / (2 Ns)) is
+// tw[k n2 / Ns].  Returns the buffer holding the result.
+__device__ double2* stockham(double2* A, double2* B, int n2, int log2n2, int rows,
+                             const double2* tw, bool inverse) {
+  const int half = n2 >> 1;
+  const int tot = rows * half;
+  for (int st = 0; st < log2n2; ++st) {
+    const int Ns = 1 << st;
+    const int tws = n2 >> st;
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+      const int r = idx >> (log2n2 - 1);
+      const int jj = idx & (half - 1);
+      const int k = jj & (Ns - 1);
+      const double2 a = A[r * n2 + jj];
+      const double2 b = A[r * n2 + jj + half];
+      double2 w = tw[k * tws];
+      if (inverse) w.y = -w.y;
+      const double2 bw = cmul(b, w);
+      const int d = ((jj - k) << 1) + k;
+      B[r * n2 + d] = cadd(a, bw);
+      B[r * n2 + d + Ns] = csub(a, bw);
+    }
+    __syncthreads();
+    double2* tmp = A;
+    A = B;
+    B = tmp;
+  }
+  return A;
+}
+
+struct GridPtrs {
+  const double* p[MAXF];
+};
+struct OutGridPtrs {
+  double* p[MAXF];
+};
+struct SpecPtrs {
+  double2* p[MAXF];
+};
+struct CSpecPtrs {
+  const double2* p[MAXF];
+};
+
+// Row rFFT of the north row j and south row nlat-1-j of every field, then the fold
+// S = F_N w_j/nlon + F_S w_j/nlon, D = F_N w_j/nlon - F_S w_j/nlon for m <= lmax
+// (sht.py:277-287).  X layout [f][0=S,1=D][m][j].
+__global__ void __launch_bounds__(256) k_fft_fold(sle::ShtDev P, int nf, GridPtrs g) {
+  extern __shared__ double2 sm[];
+  const int n2 = P.n2;
+  double2* tw = sm;
+  double2* A = sm + n2;
+  double2* B = A + 2 * n2;
+  for (int t = threadIdx.x; t < n2; t += blockDim.x) tw[t] = P.tw[t];
+  const int j = blockIdx.x;
+  const int js = P.nlat - 1 - j;
+  const double wn = P.wn[j], ws = P.ws[j];
+  for (int f = 0; f < nf; ++f) {
+    const double2* rn = reinterpret_cast<const double2*>(g.p[f] + (size_t)j * P.nlon);
+    const double2* rs = reinterpret_cast<const double2*>(g.p[f] + (size_t)js * P.nlon);
+    for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+      A[t] = rn[t];
+      A[n2 + t] = rs[t];
+    }
+    __syncthreads();
+    const double2* Z = stockham(A, B, n2, P.log2n2, 2, tw, false);
+    double2* XS = P.X + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
+    double2* XD = P.X + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
+    for (int m = threadIdx.x; m < P.nm; m += blockDim.x) {
+      double2 xr[2];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const double2* z = Z + r * n2;
+        if (m == 0) {
+          xr[r] = make_double2(z[0].x + z[0].y, 0.0);
+        } else if (m == n2) {
+          xr[r] = make_double2(z[0].x - z[0].y, 0.0);
+        } else {
+          const double2 zm = z[m];
+          const double2 zc = make_double2(z[n2 - m].x, -z[n2 - m].y);
+          const double2 e = cscale(cadd(zm, zc), 0.5);
+          const double2 dz = csub(zm, zc);
+          const double2 o = make_double2(0.5 * dz.y, -0.5 * dz.x);  // (zm - zc) / (2i)
+          xr[r] = cadd(e, cmul(tw[m], o));
+        }
+      }
+      const double2 a = cscale(xr[0], wn);
+      const double2 b = cscale(xr[1], ws);
+      XS[(size_t)m * P.nh + j] = cadd(a, b);
+      XD[(size_t)m * P.nh + j] = csub(a, b);
+    }
+    __syncthreads();
+  }
+}
+
+// Inverse: north spectrum E + O, south E - O (m <= lmax, 0 above), unnormalised inverse
+// real FFT of both rows (sht.py:330-339 with the nlon scaling folded out).
+__global__ void __launch_bounds__(256) k_ifft_unfold(sle::ShtDev P, int nf, OutGridPtrs g,
+                                                     SynEpilogue epi) {
+  extern __shared__ double2 sm[];
+  __shared__ double2 nyq[2];
+  const int n2 = P.n2;
+  double2* tw = sm;
+  double2* A = sm + n2;
+  double2* B = A + 2 * n2;
+  for (int t = threadIdx.x; t < n2; t += blockDim.x) tw[t] = P.tw[t];
+  const int j = blockIdx.x;
+  const int js = P.nlat - 1 - j;
+  for (int f = 0; f < nf; ++f) {
+    const double2* E = P.EO + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
+    const double2* O = P.EO + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
+    // stage G into B (rows north, south); G[n2] (Nyquist, only when lmax == n2) in nyq
+    for (int m = threadIdx.x; m <= n2; m += blockDim.x) {
+      double2 gn = make_double2(0.0, 0.0), gs = gn;
+      if (m < P.nm) {
+        const double2 e = E[(size_t)m * P.nh + j];
+        const double2 o = O[(size_t)m * P.nh + j];
+        gn = cadd(e, o);
+        gs = csub(e, o);
+      }
+      if (m < n2) {
+        B[m] = gn;
+        B[n2 + m] = gs;
+      } else {
+        nyq[0] = gn;
+        nyq[1] = gs;
+      }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 2 * n2; idx += blockDim.x) {
+      const int r = idx / n2;
+      const int m = idx - r * n2;
+      double2 a, b;
+      if (m == 0) {
+        a = make_double2(B[r * n2].x, 0.0);
+        b = make_double2(nyq[r].x, 0.0);
+      } else {
+        a = B[r * n2 + m];
+        const double2 c = B[r * n2 + n2 - m];
+        b = make_double2(c.x, -c.y);
+      }
+      const double2 e = cadd(a, b);
+      const double2 wc = make_double2(tw[m].x, -tw[m].y);  // exp(+2 pi i m / nlon)
+      const double2 o = cmul(csub(a, b), wc);
+      A[r * n2 + m] = make_double2(e.x - o.y, e.y + o.x);  // e + i o
+    }
+    __syncthreads();
+    const double2* Z = stockham(A, B, n2, P.log2n2, 2, tw, true);
+    double2* rn = reinterpret_cast<double2*>(g.p[f] + (size_t)j * P.nlon);
+    double2* rs = reinterpret_cast<double2*>(g.p[f] + (size_t)js * P.nlon);
+    for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+      const double2 vn = Z[t], vs = Z[n2 + t];
+      rn[t] = vn;
+      rs[t] = vs;
+      if (f == 0 && epi.out2) {
+        const double2 mn = reinterpret_cast<const double2*>(epi.mul2 + (size_t)j * P.nlon)[t];
+        const double2 ms = reinterpret_cast<const double2*>(epi.mul2 + (size_t)js * P.nlon)[t];
+        reinterpret_cast<double2*>(epi.out2 + (size_t)j * P.nlon)[t] = make_double2(vn.x * mn.x, vn.y * mn.y);
+        reinterpret_cast<double2*>(epi.out2 + (size_t)js * P.nlon)[t] = make_double2(vs.x * ms.x, vs.y * ms.y);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ Legendre analysis
+constexpr int ANA_TL = 8;      // degrees per warp reduction
+constexpr int ANA_NAMAX = 8;   // latitude groups per lane in one pass
+
+template <int NA>
+__device__ __forceinline__ void ana_segment(const sle::ShtDev& P, int s, int g0, const double2* __restrict__ Xf,
+                                            double2* __restrict__ Uf, int lane, bool accumulate) {
+  constexpr int TL = ANA_TL;
+  constexpr int V = 2 * TL;
+  constexpr int SHIFT = 5 - 4;  // log2(V) = 4
+  const int m = P.seg_m[s], l0 = P.seg_l0[s];
+  const int l1 = min(l0 + SEG, P.lmax + 1);
+  const int nh = P.nh;
+  const double2* XS = Xf + (size_t)m * nh;
+  const double2* XD = Xf + (size_t)(P.nm + m) * nh;
+  double mu[NA], qa[NA], qb[NA];
+  double2 xs[NA], xd[NA];
+#pragma unroll
+  for (int i = 0; i < NA; ++i) {
+    const int j = (g0 + i) * 32 + lane;
+    const bool ok = j < nh;
+    mu[i] = ok ? P.mu[j] : 0.0;
+    const double2 sd = ok ? P.seeds[(size_t)s * nh + j] : make_double2(0.0, 0.0);
+    qa[i] = sd.x;
+    qb[i] = sd.y;
+    xs[i] = ok ? XS[j] : make_double2(0.0, 0.0);
+    xd[i] = ok ? XD[j] : make_double2(0.0, 0.0);
+  }
+  const long long base = P.moff[m] + (l0 - m);
+  for (int lb = l0; lb < l1; lb += TL) {
+    double v[V];
+#pragma unroll
+    for (int t = 0; t < TL; ++t) {
+      const int l = lb + t;
+      double re = 0.0, im = 0.0;
+      if (l < l1) {
+        if (t < 2 && lb == l0) {
+#pragma unroll
+          for (int i = 0; i < NA; ++i) {
+            const double q = (t == 0) ? qa[i] : qb[i];
+            const double2 x = (t & 1) ? xd[i] : xs[i];
+            re = fma(q, x.x, re);
+            im = fma(q, x.y, im);
+          }
+        } else {
+          const double b = __ldg(P.be + base + (l - l0));
+#pragma unroll
+          for (int i = 0; i < NA; ++i) {
+            const double q = fma(mu[i], qb[i], b * qa[i]);
+            qa[i] = qb[i];
+            qb[i] = q;
+            const double2 x = (t & 1) ? xd[i] : xs[i];
+            re = fma(q, x.x, re);
+            im = fma(q, x.y, im);
+          }
+        }
+      }
+      v[2 * t] = re;
+      v[2 * t + 1] = im;
+    }
+    warp_transpose_reduce<V>(v, lane);
+    const int idx = lane >> SHIFT;
+    const int t = idx >> 1, c = idx & 1;
+    const int l = lb + t;
+    if ((lane & ((1 << SHIFT) - 1)) == 0 && l < l1) {
+      const long long pi = base + (l - l0);
+      const double val = __ddiv_rn(v[0] * __ldg(P.cf + pi), SQRT2_LEGACY);
+      double* dst = reinterpret_cast<double*>(Uf + pi) + c;
+      *dst = accumulate ? (*dst + val) : val;
+    }
+  }
+}
+
+__device__ void ana_zero_segment(const sle::ShtDev& P, int s, double2* Uf, int lane) {
+  const int m = P.seg_m[s], l0 = P.seg_l0[s];
+  const int l1 = min(l0 + SEG, P.lmax + 1);
+  const long long base = P.moff[m] + (l0 - m);
+  for (int l = l0 + lane; l < l1; l += 32) Uf[base + (l - l0)] = make_double2(0.0, 0.0);
+}
+
+__global__ void __launch_bounds__(128) k_leg_ana(sle::ShtDev P, SpecPtrs out) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= P.nseg) return;
+  const int f = blockIdx.y;
+  const double2* Xf = P.X + (size_t)f * 2 * P.nm * P.nh;
+  double2* Uf = out.p[f];
+  const int s = P.ana_order[warp];
+  int g0 = P.istart[s];
+  int na = P.ngrp - g0;
+  if (na <= 0) {
+    ana_zero_segment(P, s, Uf, lane);
+    return;
+  }
+  bool acc = false;
+  while (na > 0) {
+    const int nn = na > ANA_NAMAX ? ANA_NAMAX : na;
+    switch (nn) {
+      case 1: ana_segment<1>(P, s, g0, Xf, Uf, lane, acc); break;
+      case 2: ana_segment<2>(P, s, g0, Xf, Uf, lane, acc); break;
+      case 3: ana_segment<3>(P, s, g0, Xf, Uf, lane, acc); break;
+      case 4: ana_segment<4>(P, s, g0, Xf, Uf, lane, acc); break;
+      case 5: ana_segment<5>(P, s, g0, Xf, Uf, lane, acc); break;
+      case 6: ana_segment<6>(P, s, g0, Xf, Uf, lane, acc); break;
+      case 7: ana_segment<7>(P, s, g0, Xf, Uf, lane, acc); break;
+      default: ana_segment<8>(P, s, g0, Xf, Uf, lane, acc); break;
+    }
+    __syncwarp();
+    acc = true;
+    g0 += nn;
+    na -= nn;
+  }
+}
+
+// ----------------------------------------------------------------- Legendre synthesis
+// Block per pair of orders (p, lmax-p); warp per 32-latitude group; E (even l-m) and O
+// (odd l-m) sums of cf_l * 1.41421356 * U_l * Q_l over the significant segments.
+__global__ void __launch_bounds__(1024) k_leg_syn(sle::ShtDev P, CSpecPtrs in) {
+  extern __shared__ double smd[];
+  const int f = blockIdx.y;
+  const int p = blockIdx.x;
+  const int L = P.lmax;
+  double2* Uc = reinterpret_cast<double2*>(smd);          // [nm]
+  double* bes = smd + 2 * P.nm;                            // [nm]
+  const double2* U = in.p[f];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = w * 32 + lane;
+  const bool ok = j < P.nh;
+  const double x = ok ? P.mu[j] : 0.0;
+  double2* Ef = P.EO + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
+  double2* Of = P.EO + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int m = (pass == 0) ? p : L - p;
+    if (pass == 1 && m == p) break;
+    const long long base = P.moff[m];
+    const int nl = L - m + 1;
+    __syncthreads();
+    for (int t = threadIdx.x; t < nl; t += blockDim.x) {
+      const double c = P.cf[base + t] * SQRT2_LEGACY;
+      const double2 u = U[base + t];
+      Uc[t] = make_double2(u.x * c, u.y * c);
+      bes[t] = P.be[base + t];
+    }
+    __syncthreads();
+    double2 E = make_double2(0.0, 0.0), O = make_double2(0.0, 0.0);
+    for (int s = P.segoff[m]; s < P.segoff[m + 1]; ++s) {
+      if (w < (int)P.istart[s]) continue;
+      const int l0 = P.seg_l0[s];
+      const int l1 = min(l0 + SEG, L + 1);
+      const double2 sd = ok ? P.seeds[(size_t)s * P.nh + j] : make_double2(0.0, 0.0);
+      double qa = sd.x, qb = sd.y;
+      int r = l0 - m;
+      {
+        const double2 u = Uc[r];
+        E.x = fma(u.x, qa, E.x);
+        E.y = fma(u.y, qa, E.y);
+      }
+      if (l0 + 1 < l1) {
+        const double2 u = Uc[r + 1];
+        O.x = fma(u.x, qb, O.x);
+        O.y = fma(u.y, qb, O.y);
+      }
+      for (int l = l0 + 2; l < l1; l += 2) {
+        r = l - m;
+        double q = fma(x, qb, bes[r] * qa);
+        qa = qb;
+        qb = q;
+        double2 u = Uc[r];
+        E.x = fma(u.x, q, E.x);
+        E.y = fma(u.y, q, E.y);
+        if (l + 1 < l1) {
+          q = fma(x, qb, bes[r + 1] * qa);
+          qa = qb;
+          qb = q;
+          u = Uc[r + 1];
+          O.x = fma(u.x, q, O.x);
+          O.y = fma(u.y, q, O.y);
+        }
+      }
+    }
+    if (ok) {
+      Ef[(size_t)m * P.nh + j] = E;
+      Of[(size_t)m * P.nh + j] = O;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- dense <-> packed
+__global__ void k_pack(sle::ShtDev P, const double2* dense, double2* packed) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)P.nm * P.nm;
+  if (i >= n) return;
+  const int l = (int)(i / P.nm), m = (int)(i - (long long)l * P.nm);
+  if (m <= l) packed[P.moff[m] + (l - m)] = dense[i];
+}
+
+__global__ void k_unpack(sle::ShtDev P, const double2* packed, double2* dense) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)P.nm * P.nm;
+  if (i >= n) return;
+  const int l = (int)(i / P.nm), m = (int)(i - (long long)l * P.nm);
+  dense[i] = (m <= l) ? packed[P.moff[m] + (l - m)] : make_double2(0.0, 0.0);
+}
+
+// ------------------------------------------------------------------------ launchers
+static size_t fft_smem(const ShtDev& d) { return (size_t)5 * d.n2 * sizeof(double2); }
+static size_t syn_smem(const ShtDev& d) { return (size_t)3 * d.nm * sizeof(double); }
+
+int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, double2* const* out,
+                        cudaStream_t st) {
+  const ShtDev& d = plan->d;
+  if (nf < 1 || nf > MAXF) {
+    set_error("analysis: nfields must be 1..%d", MAXF);
+    return SLE_ERR_BAD_ARG;
+  }
+  GridPtrs g{};
+  SpecPtrs o{};
+  for (int f = 0; f < nf; ++f) {
+    g.p[f] = grids[f];
+    o.p[f] = out[f];
+  }
+  k_fft_fold<<<d.nh, 256, fft_smem(d), st>>>(d, nf, g);
+  const int warps_per_block = 4;
+  dim3 grid((d.nseg + warps_per_block - 1) / warps_per_block, nf);
+  k_leg_ana<<<grid, 32 * warps_per_block, 0, st>>>(d, o);
+  SLE_CUDA(cudaGetLastError());
+  return SLE_OK;
+}
+
+int sht_synthesis_packed(sle_sht* plan, int nf, const double2* const* coeffs, double* const* grids,
+                         const SynEpilogue* epi, cudaStream_t st) {
+  const ShtDev& d = plan->d;
+  if (nf < 1 || nf > MAXF) {
+    set_error("synthesis: nfields must be 1..%d", MAXF);
+    return SLE_ERR_BAD_ARG;
+  }
+  CSpecPtrs c{};
+  OutGridPtrs g{};
+  for (int f = 0; f < nf; ++f) {
+    c.p[f] = coeffs[f];
+    g.p[f] = grids[f];
+  }
+  const int npairs = (d.nm + 1) / 2;
+  k_leg_syn<<<dim3(npairs, nf), 32 * d.ngrp, syn_smem(d), st>>>(d, c);
+  SynEpilogue e = epi ? *epi : SynEpilogue{nullptr, nullptr};
+  k_ifft_unfold<<<d.nh, 256, fft_smem(d), st>>>(d, nf, g, e);
+  SLE_CUDA(cudaGetLastError());
+  return SLE_OK;
+}
+
+int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t st) {
+  const long long n = (long long)plan->d.nm * plan->d.nm;
+  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(plan->d, dense, packed);
+  SLE_CUDA(cudaGetLastError());
+  return SLE_OK;
+}
+
+int sht_unpack(sle_sht* plan, const double2* packed, double2* dense, cudaStream_t st) {
+  const long long n = (long long)plan->d.nm * plan->d.nm;
+  k_unpack<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(plan->d, packed, dense);
+  SLE_CUDA(cudaGetLastError());
+  return SLE_OK;
+}
+
+// ---------------------------------------------------------------------- plan create
+template <typename T>
+static int dalloc(T** p, size_t n) {
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T) + 16);
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(%zu bytes) failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    *p = nullptr;
+    return SLE_ERR_OOM;
+  }
+  return SLE_OK;
+}
+
+static void plan_free(sle_sht* p) {
+  if (!p) return;
+  void* ptrs[] = {p->mu, p->w, p->wn, p->ws, p->be, p->cf, p->moff, p->lidx, p->segoff,
+                  p->seg_m, p->seg_l0, p->ana_order, p->seeds, p->tw, p->X, p->EO, p->istart,
+                  p->packbuf};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete p;
+}
+
+static int plan_build(sle_sht* p, int nlat, int nlon, int lmax) {
+  ShtDev& d = p->d;
+  d.nlat = nlat;
+  d.nlon = nlon;
+  d.lmax = lmax;
+  d.nh = nlat / 2;
+  d.nm = lmax + 1;
+  d.n2 = nlon / 2;
+  d.log2n2 = 0;
+  while ((1 << d.log2n2) < d.n2) ++d.log2n2;
+  d.ngrp = (d.nh + 31) / 32;
+  d.ncoef = (long long)d.nm * (d.nm + 1) / 2;
+  // host tables: packed offsets, segments
+  std::vector<long long> moff(d.nm + 1);
+  std::vector<int> segoff(d.nm + 1), seg_m, seg_l0;
+  for (int m = 0; m <= d.nm; ++m) moff[m] = (long long)m * (lmax + 1) - (long long)m * (m - 1) / 2;
+  for (int m = 0; m < d.nm; ++m) {
+    segoff[m] = (int)seg_m.size();
+    for (int l0 = m; l0 <= lmax; l0 += SEG) {
+      seg_m.push_back(m);
+      seg_l0.push_back(l0);
+    }
+  }
+  segoff[d.nm] = (int)seg_m.size();
+  d.nseg = (int)seg_m.size();
+
+  SLE_TRY(dalloc(&p->mu, nlat));
+  SLE_TRY(dalloc(&p->w, nlat));
+  SLE_TRY(dalloc(&p->wn, d.nh));
+  SLE_TRY(dalloc(&p->ws, d.nh));
+  SLE_TRY(dalloc(&p->moff, d.nm + 1));
+  SLE_TRY(dalloc(&p->lidx, d.ncoef));
+  SLE_TRY(dalloc(&p->segoff, d.nm + 1));
+  SLE_TRY(dalloc(&p->seg_m, d.nseg));
+  SLE_TRY(dalloc(&p->seg_l0, d.nseg));
+  SLE_TRY(dalloc(&p->ana_order, d.nseg));
+  SLE_TRY(dalloc(&p->seeds, (size_t)d.nseg * d.nh));
+  SLE_TRY(dalloc(&p->be, d.ncoef));
+  SLE_TRY(dalloc(&p->cf, d.ncoef));
+  SLE_TRY(dalloc(&p->istart, d.nseg));
+  SLE_TRY(dalloc(&p->tw, d.n2));
+  SLE_TRY(dalloc(&p->X, (size_t)MAXF * 2 * d.nm * d.nh));
+  SLE_TRY(dalloc(&p->EO, (size_t)MAXF * 2 * d.nm * d.nh));
+  SLE_TRY(dalloc(&p->packbuf, (size_t)MAXF * d.ncoef));
+  double* segmax = nullptr;
+  int* fail = nullptr;
+  SLE_TRY(dalloc(&segmax, (size_t)d.nseg * d.ngrp));
+  SLE_TRY(dalloc(&fail, 1));
+  SLE_CUDA(cudaMemset(fail, 0, sizeof(int)));
+  SLE_CUDA(cudaMemcpy(p->moff, moff.data(), moff.size() * sizeof(long long), cudaMemcpyHostToDevice));
+  SLE_CUDA(cudaMemcpy(p->segoff, segoff.data(), segoff.size() * sizeof(int), cudaMemcpyHostToDevice));
+  SLE_CUDA(cudaMemcpy(p->seg_m, seg_m.data(), seg_m.size() * sizeof(int), cudaMemcpyHostToDevice));
+  SLE_CUDA(cudaMemcpy(p->seg_l0, seg_l0.data(), seg_l0.size() * sizeof(int), cudaMemcpyHostToDevice));
+  // twiddles exp(-2 pi i t / nlon), from long-double sin/cos rounded once
+  std::vector<double2> tw(d.n2);
+  for (int t = 0; t < d.n2; ++t) {
+    const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)nlon;
+    tw[t] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  SLE_CUDA(cudaMemcpy(p->tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+
+  d.mu = p->mu;
+  d.w = p->w;
+  d.wn = p->wn;
+  d.ws = p->ws;
+  d.moff = p->moff;
+  d.lidx = p->lidx;
+  d.segoff = p->segoff;
+  d.seg_m = p->seg_m;
+  d.seg_l0 = p->seg_l0;
+  d.seeds = p->seeds;
+  d.be = p->be;
+  d.cf = p->cf;
+  d.istart = p->istart;
+  d.ana_order = p->ana_order;
+  d.tw = p->tw;
+  d.X = p->X;
+  d.EO = p->EO;
+
+  const double tol = std::pow(0.1, 15);  // 0.1**15 as in the reference
+  k_gauss_nodes<<<(nlat + 127) / 128, 128>>>(nlat, tol, p->mu, p->w, fail);
+  SLE_CUDA(cudaGetLastError());
+  // folded weights w/nlon (north rows 0..nh-1, south rows nlat-1 .. nh)
+  std::vector<double> mu(nlat), w(nlat), wn(d.nh), ws(d.nh);
+  SLE_CUDA(cudaMemcpy(mu.data(), p->mu, nlat * sizeof(double), cudaMemcpyDeviceToHost));
+  SLE_CUDA(cudaMemcpy(w.data(), p->w, nlat * sizeof(double), cudaMemcpyDeviceToHost));
+  int hfail = 0;
+  SLE_CUDA(cudaMemcpy(&hfail, fail, sizeof(int), cudaMemcpyDeviceToHost));
+  if (hfail) {
+    set_error("gauss nodes: Newton iteration did not converge");
+    cudaFree(segmax);
+    cudaFree(fail);
+    return SLE_ERR_BAD_SHAPE;
+  }
+  for (int j = 0; j < d.nh; ++j) {
+    wn[j] = w[j] / (double)nlon;
+    ws[j] = w[nlat - 1 - j] / (double)nlon;
+  }
+  SLE_CUDA(cudaMemcpy(p->wn, wn.data(), d.nh * sizeof(double), cudaMemcpyHostToDevice));
+  SLE_CUDA(cudaMemcpy(p->ws, ws.data(), d.nh * sizeof(double), cudaMemcpyHostToDevice));
+
+  k_lidx<<<d.nm, 128>>>(d, p->lidx);
+  k_legendre_tables<<<dim3(d.nm, d.ngrp), 32>>>(d, p->seeds, segmax);
+  k_legendre_coef<<<(d.nseg + 127) / 128, 128>>>(d, p->be, p->cf);
+  k_istart<<<(d.nseg + 127) / 128, 128>>>(d, segmax, p->istart);
+  SLE_CUDA(cudaGetLastError());
+  std::vector<unsigned char> ist(d.nseg);
+  SLE_CUDA(cudaMemcpy(ist.data(), p->istart, d.nseg, cudaMemcpyDeviceToHost));
+  cudaFree(segmax);
+  cudaFree(fail);
+  // analysis order: most work first (segment length x active latitude groups)
+  std::vector<int> order(d.nseg);
+  std::iota(order.begin(), order.end(), 0);
+  std::vector<long long> work(d.nseg);
+  long long done = 0, total = 0;
+  for (int s = 0; s < d.nseg; ++s) {
+    const int len = std::min(SEG, lmax + 1 - seg_l0[s]);
+    work[s] = (long long)len * (d.ngrp - ist[s]);
+    done += work[s];
+    total += (long long)len * d.ngrp;
+  }
+  p->work_frac = total ? (double)done / (double)total : 1.0;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+  SLE_CUDA(cudaMemcpy(p->ana_order, order.data(), d.nseg * sizeof(int), cudaMemcpyHostToDevice));
+
+  SLE_CUDA(cudaFuncSetAttribute(k_fft_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(d)));
+  SLE_CUDA(cudaFuncSetAttribute(k_ifft_unfold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(d)));
+  SLE_CUDA(cudaFuncSetAttribute(k_leg_syn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)syn_smem(d)));
+  SLE_CUDA(cudaDeviceSynchronize());
+  return SLE_OK;
+}
+
+}  // namespace sle
+
+// ============================================================================ C ABI
+using namespace sle;
+
+extern "C" int sle_abi_version(void) { return SLE_ABI_VERSION; }
+extern "C" const char* sle_last_error(void) { return g_err; }
+
+extern "C" int sle_sht_create(int nlat, int nlon, int lmax, sle_sht** out) {
+  if (!out) {
+    set_error("sle_sht_create: out is NULL");
+    return SLE_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  if (nlat < 2 || nlat % 2 != 0) {
+    set_error("nlat must be even");
+    return SLE_ERR_BAD_SHAPE;
+  }
+  if (lmax < 0 || lmax > nlon / 2) {
+    set_error("lmax must be <= nlon/2");
+    return SLE_ERR_BAD_SHAPE;
+  }
+  if (nlon < 8 || (nlon & (nlon - 1)) != 0) {
+    set_error("nlon must be a power of two >= 8 (got %d)", nlon);
+    return SLE_ERR_BAD_SHAPE;
+  }
+  if (nlat > 2048 || nlon > 4096) {
+    set_error("grid %d x %d exceeds the supported maximum 2048 x 4096", nlat, nlon);
+    return SLE_ERR_BAD_SHAPE;
+  }
+  sle_sht* p = new sle_sht();
+  std::memset(p, 0, sizeof(sle_sht));
+  int rc = plan_build(p, nlat, nlon, lmax);
+  if (rc != SLE_OK) {
+    plan_free(p);
+    return rc;
+  }
+  *out = p;
+  return SLE_OK;
+}
+
+extern "C" int sle_sht_destroy(sle_sht* plan) {
+  plan_free(plan);
+  return SLE_OK;
+}
+
+extern "C" int sle_sht_info(const sle_sht* plan, int* nlat, int* nlon, int* lmax, long long* ncoef) {
+  if (!plan) {
+    set_error("sle_sht_info: NULL plan");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (nlat) *nlat = plan->d.nlat;
+  if (nlon) *nlon = plan->d.nlon;
+  if (lmax) *lmax = plan->d.lmax;
+  if (ncoef) *ncoef = plan->d.ncoef;
+  return SLE_OK;
+}
+
+extern "C" int sle_sht_work_fraction(const sle_sht* plan, double* frac) {
+  if (!plan || !frac) {
+    set_error("sle_sht_work_fraction: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  *frac = plan->work_frac;
+  return SLE_OK;
+}
+
+extern "C" int sle_sht_gauss(const sle_sht* plan, double* mu_host, double* w_host) {
+  if (!plan) {
+    set_error("sle_sht_gauss: NULL plan");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (mu_host) SLE_CUDA(cudaMemcpy(mu_host, plan->mu, plan->d.nlat * sizeof(double), cudaMemcpyDeviceToHost));
+  if (w_host) SLE_CUDA(cudaMemcpy(w_host, plan->w, plan->d.nlat * sizeof(double), cudaMemcpyDeviceToHost));
+  return SLE_OK;
+}
+
+static bool aligned16(const void* p) { return p && (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+extern "C" int sle_sht_analysis(sle_sht* plan, int nfields, const double* const* grids_dev,
+                                void* const* coeffs_dev, int layout, void* stream) {
+  if (!plan || !grids_dev || !coeffs_dev) {
+    set_error("sle_sht_analysis: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  for (int f = 0; f < nfields && f < MAXF; ++f)
+    if (!aligned16(grids_dev[f]) || !aligned16(coeffs_dev[f])) {
+      set_error("sle_sht_analysis: device buffers must be non-NULL and 16-byte aligned");
+      return SLE_ERR_BAD_ARG;
+    }
+  if (nfields < 1 || nfields > MAXF) {
+    set_error("sle_sht_analysis: nfields must be 1..%d", MAXF);
+    return SLE_ERR_BAD_ARG;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  double2* outp[MAXF];
+  for (int f = 0; f < nfields; ++f)
+    outp[f] = (layout == SLE_LAYOUT_PACKED) ? reinterpret_cast<double2*>(coeffs_dev[f])
+                                            : plan->packbuf + (size_t)f * plan->d.ncoef;
+  SLE_TRY(sht_analysis_packed(plan, nfields, grids_dev, outp, st));
+  if (layout != SLE_LAYOUT_PACKED)
+    for (int f = 0; f < nfields; ++f)
+      SLE_TRY(sht_unpack(plan, outp[f], reinterpret_cast<double2*>(coeffs_dev[f]), st));
+  return SLE_OK;
+}
+
+extern "C" int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* coeffs_dev, int layout,
+                                 double* const* grids_dev, void* stream) {
+  if (!plan || !grids_dev || !coeffs_dev) {
+    set_error("sle_sht_synthesis: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  for (int f = 0; f < nfields && f < MAXF; ++f)
+    if (!aligned16(grids_dev[f]) || !aligned16(coeffs_dev[f])) {
+      set_error("sle_sht_synthesis: device buffers must be non-NULL and 16-byte aligned");
+      return SLE_ERR_BAD_ARG;
+    }
+  if (nfields < 1 || nfields > MAXF) {
+    set_error("sle_sht_synthesis: nfields must be 1..%d", MAXF);
+    return SLE_ERR_BAD_ARG;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const double2* inp[MAXF];
+  for (int f = 0; f < nfields; ++f) {
+    if (layout == SLE_LAYOUT_PACKED) {
+      inp[f] = reinterpret_cast<const double2*>(coeffs_dev[f]);
+    } else {
+      double2* pb = plan->packbuf + (size_t)f * plan->d.ncoef;
+      SLE_TRY(sht_pack(plan, reinterpret_cast<const double2*>(coeffs_dev[f]), pb, st));
+      inp[f] = pb;
+    }
+  }
+  return sht_synthesis_packed(plan, nfields, inp, grids_dev, nullptr, st);
+}
+
+extern "C" int sle_sht_pack(sle_sht* plan, const void* dense_dev, void* packed_dev, void* stream) {
+  if (!plan || !dense_dev || !packed_dev) {
+    set_error("sle_sht_pack: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  return sht_pack(plan, reinterpret_cast<const double2*>(dense_dev), reinterpret_cast<double2*>(packed_dev),
+                  reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int sle_sht_unpack(sle_sht* plan, const void* packed_dev, void* dense_dev, void* stream) {
+  if (!plan || !dense_dev || !packed_dev) {
+    set_error("sle_sht_unpack: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  return sht_unpack(plan, reinterpret_cast<const double2*>(packed_dev), reinterpret_cast<double2*>(dense_dev),
+                    reinterpret_cast<cudaStream_t>(stream));
+}

@@ -1,0 +1,1249 @@
+// The SLEvolve time step on the device, FP64 (SLEvolve python/slevolve/solver.py:521-1144).
+//
+// All solver state lives in HBM for the life of the handle: grids [nlat][nlon] float64,
+// spectra in the packed order-major triangle (complex128), the modal state R[k][packed].
+// Elementwise kernels reproduce the reference's NumPy statement order with explicitly
+// rounded operations (no FMA contraction), reductions are deterministic (fixed partition,
+// last-block finalisation in index order).  The inner fixed-point loop runs its kernels
+// back to back and reads one small status record per iteration to decide whether to go on.
+#include "sle_internal.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace sle {
+
+constexpr double EPS0 = 2.220446049250313e-16;   // numpy finfo(float64).eps (solver.py:33)
+constexpr double PI_LEGACY = 3.1415926535898;    // truncated literal (solver.py:31)
+constexpr int GR_MAXACC = 3;                      // solver.py:38
+constexpr int MAX_INNER = 9999;                   // solver.py:1049
+constexpr int RED_BLOCKS = 296;                   // 2 x 148 SMs: reduction grid (fixed partition)
+
+// Constants of the rotation block (solver.py:910-975), computed on the host with the
+// reference's expressions.
+struct RotConst {
+  double c_il22, c_il02, c_il12;   // -8 PI a^4/(3 sqrt5), -8 PI a^4/sqrt30, 8 PI a^4/sqrt30
+  double alpha;                    // 1 / (1 - kTE2/kf)
+  double inv_CmA, inv_kf, inv_C;   // 1/(C-A), 1/kf, 1.0/C
+  double onepk;                    // 1 + kE2
+  double r2w2_3, r2w2_6s5, r2w2_s30, r2w2_s120;
+  double ekhTE, hTE2, gacc;
+  double rhoi, rhow;
+};
+
+// Small per-step record, mirrored to pinned host memory once per inner iteration.
+struct Scal {
+  double conserv, sa, so, xi;
+  double K00;
+  int numiter, converged, status, gr_nacc, gr_changed, gr_reguess, gr_ice_an, pad0;
+  unsigned int nd;
+  unsigned int pad1;
+  double diag[5];        // slc_ocn00, c00, slc_b00, cst00 (real parts), ice00
+  // rotation
+  double il[9], mm[3], lam[18];
+  double oldil[9], oldm[3], dlam_prev2[6];
+  double sum_il[9], sum_m[3], sum_tsl[6], sum_trr[6];
+  double dsl_rot[6], rr_rot[6];
+  double dil[9], dm[3], dlam_cur2[6];
+  double p_il[9], p_m[3], p_lambda[6];
+};
+
+struct Dev {
+  int nlat, nlon, nl;
+  long long ng, ncoef;
+  int K;
+  const int* lidx;
+  const int* nmod;
+  const double *decay, *omd, *a_sl, *a_rr, *ttl, *ttlekhl, *ttlhe;
+  const double *a_il, *a_m, *a_tsl, *a_trr;
+  int nmod2;
+  double rhoi, rhow, epsilon1;
+  int checkmarine, tpw, calcRG, opt_dsl;
+  long long i20, i21, i22;   // packed indices of (l=2, m=0..2)
+};
+
+// ------------------------------------------------------------------ reduction helpers
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block sum (fixed order).  Every thread of the block must call it.
+__device__ double block_sum(double v, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (w == 0) {
+    t = (lane < nw) ? sh[lane] : 0.0;
+    t = warp_sum(t);
+  }
+  return t;  // valid in warp 0
+}
+
+// After each block stored its partial, the last block to arrive sums the partials in index
+// order and returns true (in all its threads) with *total set; others return false.
+__device__ bool last_block_total(double part, double* partials, unsigned int* counter, double* total,
+                                 double* sh) {
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = part;
+    __threadfence();
+    const unsigned int t = atomicAdd(counter, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  double v = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) v += ((volatile double*)partials)[i];
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) {
+    *total = v;
+    *counter = 0u;
+  }
+  __syncthreads();
+  return true;
+}
+
+__device__ __forceinline__ double cabs_(double2 z) { return hypot(z.x, z.y); }
+
+// numpy complex division a / b (Smith's method with a reciprocal scale, loops.c.src)
+__device__ __forceinline__ double2 np_cdiv(double2 a, double2 b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    const double rat = __ddiv_rn(b.y, b.x);
+    const double scl = __ddiv_rn(1.0, __dadd_rn(b.x, __dmul_rn(b.y, rat)));
+    return make_double2(__dmul_rn(__dadd_rn(a.x, __dmul_rn(a.y, rat)), scl),
+                        __dmul_rn(__dsub_rn(a.y, __dmul_rn(a.x, rat)), scl));
+  }
+  const double rat = __ddiv_rn(b.x, b.y);
+  const double scl = __ddiv_rn(1.0, __dadd_rn(b.y, __dmul_rn(b.x, rat)));
+  return make_double2(__dmul_rn(__dadd_rn(__dmul_rn(a.x, rat), a.y), scl),
+                      __dmul_rn(__dsub_rn(__dmul_rn(a.y, rat), a.x), scl));
+}
+
+__device__ __forceinline__ double2 np_cmul(double2 a, double2 b) {
+  return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                      __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+
+// ------------------------------------------------------------------------- kernels
+__global__ void k_set_decay(int K, int nl, const double* s, const int* nmod, double dt, double* decay,
+                            double* omd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= K * nl) return;
+  const int k = i / nl, l = i - k * nl;
+  double d = 0.0;
+  if (l >= 1 && k < nmod[l]) d = exp(__ddiv_rn(__dmul_rn(-s[i], dt), 1000.0));
+  decay[i] = d;
+  omd[i] = __dsub_rn(1.0, d);
+}
+
+// R_k <- d R_k + (1-d) P ; visc = sum_k a_sl R_k ; rad = sum_k a_rr R_k   (solver.py:386-407)
+__global__ void k_advance(Dev D, double2* __restrict__ R, const double2* __restrict__ P,
+                          double2* __restrict__ visc, double2* __restrict__ rad) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ncoef) return;
+  const int l = D.lidx[i];
+  const double2 p = P[i];
+  double2 v = make_double2(0.0, 0.0), r = v;
+  const int nk = D.nmod[l];
+  for (int k = 0; k < nk; ++k) {
+    const int kl = k * D.nl + l;
+    const double d = D.decay[kl], o = D.omd[kl], as = D.a_sl[kl], ar = D.a_rr[kl];
+    double2 x = R[(size_t)k * D.ncoef + i];
+    x.x = __dadd_rn(__dmul_rn(x.x, d), __dmul_rn(p.x, o));
+    x.y = __dadd_rn(__dmul_rn(x.y, d), __dmul_rn(p.y, o));
+    R[(size_t)k * D.ncoef + i] = x;
+    v.x = __dadd_rn(v.x, __dmul_rn(x.x, as));
+    v.y = __dadd_rn(v.y, __dmul_rn(x.y, as));
+    r.x = __dadd_rn(r.x, __dmul_rn(x.x, ar));
+    r.y = __dadd_rn(r.y, __dmul_rn(x.y, ar));
+  }
+  visc[i] = v;
+  rad[i] = r;
+}
+
+// degree-2 rotational states and their sums (solver.py:409-421); also snapshot the
+// committed rotational loads (oldil, oldm, dlambda_prev2; solver.py:837-839)
+__global__ void k_rot_advance(Dev D, Scal* sc, double* r_il, double* r_m, double* r_lam) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int q = 0; q < 9; ++q) sc->sum_il[q] = 0.0;
+  for (int q = 0; q < 3; ++q) sc->sum_m[q] = 0.0;
+  for (int q = 0; q < 6; ++q) sc->sum_tsl[q] = sc->sum_trr[q] = 0.0;
+  if (D.nl > 2) {
+    for (int k = 0; k < D.nmod2; ++k) {
+      const double d = D.decay[k * D.nl + 2];
+      const double o = __dsub_rn(1.0, d);
+      for (int q = 0; q < 9; ++q) {
+        const double x = __dadd_rn(__dmul_rn(d, r_il[k * 9 + q]), __dmul_rn(o, sc->p_il[q]));
+        r_il[k * 9 + q] = x;
+      }
+      for (int q = 0; q < 3; ++q) {
+        const double x = __dadd_rn(__dmul_rn(d, r_m[k * 3 + q]), __dmul_rn(o, sc->p_m[q]));
+        r_m[k * 3 + q] = x;
+      }
+      for (int q = 0; q < 6; ++q) {
+        const double x = __dadd_rn(__dmul_rn(d, r_lam[k * 6 + q]), __dmul_rn(o, sc->p_lambda[q]));
+        r_lam[k * 6 + q] = x;
+      }
+      for (int q = 0; q < 9; ++q) sc->sum_il[q] = __dadd_rn(sc->sum_il[q], __dmul_rn(D.a_il[k], r_il[k * 9 + q]));
+      for (int q = 0; q < 3; ++q) sc->sum_m[q] = __dadd_rn(sc->sum_m[q], __dmul_rn(D.a_m[k], r_m[k * 3 + q]));
+      for (int q = 0; q < 6; ++q) {
+        sc->sum_tsl[q] = __dadd_rn(sc->sum_tsl[q], __dmul_rn(D.a_tsl[k], r_lam[k * 6 + q]));
+        sc->sum_trr[q] = __dadd_rn(sc->sum_trr[q], __dmul_rn(D.a_trr[k], r_lam[k * 6 + q]));
+      }
+    }
+  }
+  sc->numiter = 0;
+  sc->converged = 0;
+  sc->status = 0;
+  sc->gr_nacc = 0;
+  sc->gr_changed = 0;
+  sc->gr_reguess = 0;
+  sc->gr_ice_an = 0;
+  for (int q = 0; q < 9; ++q) sc->oldil[q] = sc->p_il[q];
+  for (int q = 0; q < 3; ++q) sc->oldm[q] = sc->p_m[q];
+  for (int q = 0; q < 6; ++q) sc->dlam_prev2[q] = sc->p_lambda[q];
+  for (int q = 0; q < 6; ++q) sc->dsl_rot[q] = sc->rr_rot[q] = sc->dlam_cur2[q] = 0.0;
+  for (int q = 0; q < 9; ++q) sc->dil[q] = 0.0;
+  for (int q = 0; q < 3; ++q) sc->dm[q] = 0.0;
+}
+
+// grounded ice on topography `topo` (flotation test, solver.py:655-659)
+__device__ __forceinline__ double icestar_on(double ice, double topo, double rhow, double rhoi) {
+  const bool keep = (topo > 0.0) || (ice > __ddiv_rn(__dmul_rn(fabs(topo), rhow), rhoi));
+  return keep ? ice : __dmul_rn(ice, 0.0);
+}
+
+// Step prologue on the grid (solver.py:853-887): I* on the previous topography, beta,
+// C* = C beta, tO = T0 (C* - C*0); at step 1 also I* of the previous ice on T0.
+__global__ void k_ice_grid(Dev D, const double* __restrict__ ice, const double* __restrict__ topo_prev,
+                           const double* __restrict__ cxy, const double* __restrict__ tinit,
+                           const double* __restrict__ cstar0, double* __restrict__ icestar,
+                           double* __restrict__ beta, double* __restrict__ cstar, double* __restrict__ tO,
+                           const double* __restrict__ ice_prev, double* __restrict__ oldsrc, Scal* sc) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ng) return;
+  const double v = ice[i];
+  if (!isfinite(v)) sc->status = SLE_ERR_NONFINITE;
+  const double is = D.checkmarine ? icestar_on(v, topo_prev[i], D.rhow, D.rhoi) : v;
+  icestar[i] = is;
+  const double b = (is < EPS0) ? 1.0 : 0.0;
+  beta[i] = b;
+  const double c = __dmul_rn(cxy[i], b);
+  cstar[i] = c;
+  tO[i] = __dmul_rn(tinit[i], __dsub_rn(c, cstar0[i]));
+  if (oldsrc) {
+    const double vp = ice_prev[i];
+    oldsrc[i] = D.checkmarine ? icestar_on(vp, tinit[i], D.rhow, D.rhoi) : vp;
+  }
+}
+
+// dice = I*_lm - old ; dI = p_ice + dice ; first guess of the load increment ; dS_cur ;
+// so = sum|load_inc|  (solver.py:868-905; extrap solver_opt.py:504-513)
+// mode: 0 eustatic, 1 extrap uniform (2 h1 - h2), 2 extrap variable (c1 h1 - c2 h2)
+__global__ void k_pre_spec(Dev D, const double2* __restrict__ icelm, const double2* __restrict__ oldice,
+                           const double2* __restrict__ p_ice, const double2* __restrict__ cstarlm,
+                           const double2* __restrict__ dSprev, const double2* __restrict__ h1,
+                           const double2* __restrict__ h2, int mode, double c1, double c2,
+                           double2* __restrict__ dice, double2* __restrict__ dI, double2* __restrict__ load,
+                           double2* __restrict__ dScur, Scal* sc, double* partials, unsigned int* counter) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  const double2 dice00 = make_double2(__dsub_rn(icelm[0].x, oldice[0].x), __dsub_rn(icelm[0].y, oldice[0].y));
+  const double2 c00 = cstarlm[0];
+  const double fr = -D.rhoi / D.rhow;
+  const double2 s00 = make_double2(__dmul_rn(fr, dice00.x), __dmul_rn(fr, dice00.y));
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < D.ncoef;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 a = icelm[i], o = oldice[i];
+    const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
+    dice[i] = d;
+    const double2 pi = p_ice[i];
+    dI[i] = make_double2(__dadd_rn(pi.x, d.x), __dadd_rn(pi.y, d.y));
+    double2 g;
+    if (mode == 0) {
+      g = np_cmul(np_cdiv(cstarlm[i], c00), s00);
+    } else if (mode == 1) {
+      const double2 u = h1[i], v = h2[i];
+      g = make_double2(__dsub_rn(__dmul_rn(u.x, 2.0), v.x), __dsub_rn(__dmul_rn(u.y, 2.0), v.y));
+    } else {
+      const double2 u = h1[i], v = h2[i];
+      g = make_double2(__dsub_rn(__dmul_rn(u.x, c1), __dmul_rn(c2, v.x)),
+                       __dsub_rn(__dmul_rn(u.y, c1), __dmul_rn(c2, v.y)));
+    }
+    load[i] = g;
+    if (mode == 0) {
+      dScur[i] = make_double2(0.0, 0.0);
+    } else {
+      const double2 p = dSprev[i];
+      dScur[i] = make_double2(__dadd_rn(p.x, g.x), __dadd_rn(p.y, g.y));
+    }
+    acc += cabs_(g);
+  }
+  const double part = block_sum(acc, sh);
+  double tot;
+  if (last_block_total(part, partials, counter, &tot, sh)) {
+    if (threadIdx.x == 0) sc->so = tot;
+  }
+}
+
+// The rotation block (solver.py:910-975), one thread.
+__device__ void rotation_block(const Dev& D, const RotConst& C, const double2* dScur, const double2* dI,
+                               Scal* sc, double2 rot_out[3], double2 rr_out[3], bool write_state) {
+  const double2 s20 = dScur[D.i20], s21 = dScur[D.i21];
+  const double2 i20 = dI[D.i20], i21 = dI[D.i21];
+  const double z20r = __dadd_rn(__dmul_rn(C.rhow, s20.x), __dmul_rn(C.rhoi, i20.x));
+  const double z21r = __dadd_rn(__dmul_rn(C.rhow, s21.x), __dmul_rn(C.rhoi, i21.x));
+  const double z21i = __dadd_rn(__dmul_rn(C.rhow, s21.y), __dmul_rn(C.rhoi, i21.y));
+  // only il[0:3, 2] and lam[0,0], lam[2, 0:3] are ever non-zero (solver.py:916-919, 950-956)
+  double il[9];
+  for (int q = 0; q < 9; ++q) il[q] = 0.0;
+  il[8] = __dmul_rn(C.c_il22, z20r);
+  il[2] = __dmul_rn(C.c_il02, z21r);
+  il[5] = __dmul_rn(C.c_il12, z21i);
+  double mm[3];
+  for (int i = 0; i < 2; ++i) {
+    const double a = __dadd_rn(__dmul_rn(C.onepk, il[i * 3 + 2]), sc->sum_il[i * 3 + 2]);
+    mm[i] = __dmul_rn(C.alpha, __dadd_rn(__dmul_rn(C.inv_CmA, a), __dmul_rn(C.inv_kf, sc->sum_m[i])));
+  }
+  mm[2] = __dmul_rn(-C.inv_C, __dadd_rn(__dmul_rn(C.onepk, il[8]), sc->sum_il[8]));
+  const double m1 = mm[0], m2 = mm[1], m3 = mm[2];
+  const double m1s = __dmul_rn(m1, m1), m2s = __dmul_rn(m2, m2), m3s = __dmul_rn(m3, m3);
+  double lam[18];
+  for (int q = 0; q < 18; ++q) lam[q] = 0.0;
+  // lam[0,0]
+  lam[0] = __dmul_rn(C.r2w2_3, __dadd_rn(__dadd_rn(__dadd_rn(m1s, m2s), m3s), __dmul_rn(2.0, m3)));
+  lam[1] = 0.0;
+  // lam[2,0] at flat (2*3+0)*2
+  lam[12] = __dmul_rn(C.r2w2_6s5, __dsub_rn(__dsub_rn(__dadd_rn(m1s, m2s), __dmul_rn(2.0, m3s)), __dmul_rn(4.0, m3)));
+  lam[13] = 0.0;
+  // lam[2,1] = -(r2w2/sqrt30) * ((m1 - i m2) * (1 + m3))
+  const double op = __dadd_rn(1.0, m3);
+  lam[14] = __dmul_rn(-C.r2w2_s30, __dmul_rn(m1, op));
+  lam[15] = __dmul_rn(-C.r2w2_s30, __dmul_rn(-m2, op));
+  // lam[2,2] = (r2w2/sqrt120) * ((m2^2 - m1^2) + 2 i m1 m2)
+  lam[16] = __dmul_rn(C.r2w2_s120, __dsub_rn(m2s, m1s));
+  lam[17] = __dmul_rn(C.r2w2_s120, __dmul_rn(__dmul_rn(2.0, m1), m2));
+  for (int q = 0; q < 3; ++q) {
+    const double dr = __dsub_rn(lam[12 + 2 * q], sc->dlam_prev2[2 * q]);
+    const double di = __dsub_rn(lam[13 + 2 * q], sc->dlam_prev2[2 * q + 1]);
+    const double tr = __dadd_rn(sc->dlam_prev2[2 * q], dr);
+    const double ti = __dadd_rn(sc->dlam_prev2[2 * q + 1], di);
+    rot_out[q] = make_double2(__ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, tr), sc->sum_tsl[2 * q]), C.gacc),
+                              __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, ti), sc->sum_tsl[2 * q + 1]), C.gacc));
+    rr_out[q] = make_double2(__ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, tr), sc->sum_trr[2 * q]), C.gacc),
+                             __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, ti), sc->sum_trr[2 * q + 1]), C.gacc));
+    if (write_state) {
+      sc->dlam_cur2[2 * q] = dr;
+      sc->dlam_cur2[2 * q + 1] = di;
+    }
+  }
+  if (write_state) {
+    for (int q = 0; q < 9; ++q) {
+      sc->il[q] = il[q];
+      sc->dil[q] = __dsub_rn(il[q], sc->oldil[q]);
+    }
+    for (int q = 0; q < 3; ++q) {
+      sc->mm[q] = mm[q];
+      sc->dm[q] = __dsub_rn(mm[q], sc->oldm[q]);
+    }
+    for (int q = 0; q < 18; ++q) sc->lam[q] = lam[q];
+    for (int q = 0; q < 3; ++q) {
+      sc->dsl_rot[2 * q] = rot_out[q].x;
+      sc->dsl_rot[2 * q + 1] = rot_out[q].y;
+      sc->rr_rot[2 * q] = rr_out[q].x;
+      sc->rr_rot[2 * q + 1] = rr_out[q].y;
+    }
+  }
+}
+
+// Eq. B18 (solver.py:977-991) with the rotation block fused: the three threads owning
+// (l=2, m=0..2) evaluate it, the (2,0) thread records the rotational state.
+__global__ void k_b18(Dev D, RotConst C, const double2* __restrict__ dI, const double2* __restrict__ dSprev,
+                      const double2* __restrict__ load, const double2* __restrict__ visc,
+                      const double2* __restrict__ dScur, double2* __restrict__ sl, Scal* sc) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ncoef) return;
+  const int l = D.lidx[i];
+  const double2 a = dI[i], b = dSprev[i], c = load[i], v = visc[i];
+  const double te = D.ttlekhl[l], t = D.ttl[l];
+  double re = __dadd_rn(__dadd_rn(__dmul_rn(a.x, D.rhoi), __dmul_rn(b.x, D.rhow)), __dmul_rn(c.x, D.rhow));
+  double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(b.y, D.rhow)), __dmul_rn(c.y, D.rhow));
+  re = __dadd_rn(__dmul_rn(re, te), __dmul_rn(v.x, t));
+  im = __dadd_rn(__dmul_rn(im, te), __dmul_rn(v.y, t));
+  if (D.tpw && (i == D.i20 || i == D.i21 || i == D.i22)) {
+    double2 rot[3], rr[3];
+    rotation_block(D, C, dScur, dI, sc, rot, rr, i == D.i20);
+    const int q = (i == D.i20) ? 0 : (i == D.i21) ? 1 : 2;
+    re = __dadd_rn(re, rot[q].x);
+    im = __dadd_rn(im, rot[q].y);
+  }
+  sl[i] = make_double2(re, im);
+}
+
+// conserv, the load update and xi (solver.py:1002-1030):
+//   new = ((-dSprev + rO) + C*_lm conserv) - tO ;  dS_cur = dSprev + new ;  sa = sum|new|
+__global__ void k_update(Dev D, const double2* __restrict__ dSprev, const double2* __restrict__ rOlm,
+                         const double2* __restrict__ cstarlm, const double2* __restrict__ tOlm,
+                         const double2* __restrict__ dI, double2* __restrict__ load,
+                         double2* __restrict__ dScur, Scal* sc, double* partials, unsigned int* counter) {
+  __shared__ double sh[32];
+  // conserv = ((1 / C*_00) * (-(rhoi/rhow) dI_00 - rO_00 + tO_00)).real
+  const double2 c00 = cstarlm[0];
+  const double2 rinv = np_cdiv(make_double2(1.0, 0.0), c00);
+  const double fr = __dmul_rn(-1.0, __ddiv_rn(D.rhoi, D.rhow));
+  const double2 d00 = dI[0], r00 = rOlm[0], t00 = tOlm[0];
+  const double2 x = make_double2(__dadd_rn(__dsub_rn(__dmul_rn(fr, d00.x), r00.x), t00.x),
+                                 __dadd_rn(__dsub_rn(__dmul_rn(fr, d00.y), r00.y), t00.y));
+  const double conserv = __dsub_rn(__dmul_rn(rinv.x, x.x), __dmul_rn(rinv.y, x.y));
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < D.ncoef;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double2 p = dSprev[i], r = rOlm[i], c = cstarlm[i], t = tOlm[i];
+    double nr = __dadd_rn(-p.x, r.x), ni = __dadd_rn(-p.y, r.y);
+    nr = __dadd_rn(nr, __dmul_rn(c.x, conserv));
+    ni = __dadd_rn(ni, __dmul_rn(c.y, conserv));
+    nr = __dsub_rn(nr, t.x);
+    ni = __dsub_rn(ni, t.y);
+    load[i] = make_double2(nr, ni);
+    dScur[i] = make_double2(__dadd_rn(p.x, nr), __dadd_rn(p.y, ni));
+    acc += hypot(nr, ni);
+  }
+  const double part = block_sum(acc, sh);
+  double sa;
+  if (last_block_total(part, partials, counter, &sa, sh)) {
+    if (threadIdx.x == 0) {
+      const double so = sc->so;
+      double xi;
+      if (fabs(sa - so) < EPS0 && fabs(so) < EPS0) xi = 0.0;
+      else if (fabs(so) < EPS0) xi = fabs((sa - so) / (EPS0 * 10.0));
+      else xi = fabs((sa - so) / so);
+      sc->conserv = conserv;
+      sc->sa = sa;
+      sc->xi = xi;
+      sc->so = sa;
+      sc->numiter += 1;
+      if (sc->status != 0 || !(xi == xi) || !isfinite(sa)) {
+        sc->status = SLE_ERR_NONFINITE;
+        sc->converged = 1;
+      } else if (xi <= D.epsilon1) {
+        sc->converged = 1;
+      } else if (sc->numiter >= MAX_INNER) {
+        sc->status = SLE_ERR_NONCONVERGED;
+        sc->converged = 1;
+      }
+    }
+  }
+}
+
+// sl_tot = sl_inc with conserv added to (0,0) (plain path, solver.py:1017-1021)
+__global__ void k_sltot(Dev D, const double2* __restrict__ sl, double2* __restrict__ sltot, const Scal* sc) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ncoef) return;
+  double2 v = sl[i];
+  if (i == 0) v.x = __dadd_rn(v.x, sc->conserv);
+  sltot[i] = v;
+}
+
+// deltasl (dsl identity) and, when not converged, topography / ocean function refresh and
+// the grounded-ice test on the new topography (solver.py:1032-1037, 661-684).
+__global__ void k_refresh1(Dev D, const double* __restrict__ dsl, double* __restrict__ deltasl,
+                           const double* __restrict__ tinit, double* __restrict__ topo,
+                           double* __restrict__ cxy, const double* __restrict__ ice,
+                           const double* __restrict__ beta, double* __restrict__ grnew, Scal* sc,
+                           double* partials, unsigned int* counter) {
+  __shared__ double sh[32];
+  const bool conv = sc->converged != 0;
+  const bool test = !conv && D.checkmarine && sc->gr_nacc < GR_MAXACC;
+  const double cadd = D.opt_dsl ? __dmul_rn(sc->conserv, sc->K00) : 0.0;
+  double cnt = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < D.ng;
+       i += (long long)gridDim.x * blockDim.x) {
+    double ds;
+    if (D.opt_dsl) {
+      ds = __dadd_rn(dsl[i], cadd);
+      deltasl[i] = ds;
+    } else {
+      ds = deltasl[i];
+    }
+    if (!conv) {
+      const double t = __dsub_rn(tinit[i], ds);
+      topo[i] = t;
+      cxy[i] = (t < 0.0) ? 1.0 : 0.0;
+      if (test) {
+        const double g = icestar_on(ice[i], t, D.rhow, D.rhoi);
+        grnew[i] = g;
+        const bool bnew = g < EPS0;
+        if (bnew != (beta[i] != 0.0)) cnt += 1.0;
+      }
+    }
+  }
+  if (!test) return;
+  const double part = block_sum(cnt, sh);
+  double tot;
+  if (last_block_total(part, partials, counter, &tot, sh)) {
+    if (threadIdx.x == 0) {
+      sc->gr_reguess += 1;
+      sc->nd = (unsigned int)tot;
+      if (tot > 0.0) {
+        sc->gr_changed = 1;
+        sc->gr_nacc += 1;
+        sc->gr_ice_an += 1;
+      } else {
+        sc->gr_changed = 0;
+      }
+    }
+  }
+}
+
+// C* and tO on the refreshed ocean function; accepted grounded-ice mask (solver.py:664-684)
+__global__ void k_refresh2(Dev D, const double* __restrict__ cxy, const double* __restrict__ tinit,
+                           const double* __restrict__ cstar0, const double* __restrict__ grnew,
+                           double* __restrict__ icestar, double* __restrict__ beta,
+                           double* __restrict__ cstar, double* __restrict__ tO, int changed) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ng) return;
+  double b;
+  if (changed) {
+    const double g = grnew[i];
+    icestar[i] = g;
+    b = (g < EPS0) ? 1.0 : 0.0;
+    beta[i] = b;
+  } else {
+    b = beta[i];
+  }
+  const double c = __dmul_rn(cxy[i], b);
+  cstar[i] = c;
+  tO[i] = __dmul_rn(tinit[i], __dsub_rn(c, cstar0[i]));
+}
+
+__global__ void k_dice(Dev D, const double2* __restrict__ icelm, const double2* __restrict__ oldice,
+                       const double2* __restrict__ p_ice, double2* __restrict__ dice, double2* __restrict__ dI) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ncoef) return;
+  const double2 a = icelm[i], o = oldice[i], p = p_ice[i];
+  const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
+  dice[i] = d;
+  dI[i] = make_double2(__dadd_rn(p.x, d.x), __dadd_rn(p.y, d.y));
+}
+
+// Radial displacement spectrum (solver.py:1054-1069)
+__global__ void k_rr(Dev D, const double2* __restrict__ dI, const double2* __restrict__ dSprev,
+                     const double2* __restrict__ load, const double2* __restrict__ rad,
+                     double2* __restrict__ rr, const Scal* sc) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ncoef) return;
+  const int l = D.lidx[i];
+  const double2 a = dI[i], b = dSprev[i], c = load[i], v = rad[i];
+  const double th = D.ttlhe[l], t = D.ttl[l];
+  double re = __dadd_rn(__dadd_rn(__dmul_rn(a.x, D.rhoi), __dmul_rn(b.x, D.rhow)), __dmul_rn(c.x, D.rhow));
+  double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(b.y, D.rhow)), __dmul_rn(c.y, D.rhow));
+  re = __dadd_rn(__dmul_rn(re, th), __dmul_rn(v.x, t));
+  im = __dadd_rn(__dmul_rn(im, th), __dmul_rn(v.y, t));
+  if (D.tpw) {
+    int q = -1;
+    if (i == D.i20) q = 0;
+    else if (i == D.i21) q = 1;
+    else if (i == D.i22) q = 2;
+    if (q >= 0) {
+      re = __dadd_rn(re, sc->rr_rot[2 * q]);
+      im = __dadd_rn(im, sc->rr_rot[2 * q + 1]);
+    }
+  }
+  rr[i] = make_double2(re, im);
+}
+
+// commit (solver.py:1080-1096): cur = rhoi dice + rhow load (l = 0 zeroed); p_load += cur;
+// p_ice = dI ; p_ocean = dS_cur ; prev_ice = I*_lm ; extrap history h_new = load
+__global__ void k_commit(Dev D, const double2* __restrict__ dice, const double2* __restrict__ load,
+                         const double2* __restrict__ dI, const double2* __restrict__ dScur,
+                         const double2* __restrict__ icelm, double2* __restrict__ p_load,
+                         double2* __restrict__ p_ice, double2* __restrict__ p_ocean,
+                         double2* __restrict__ prev_ice, double2* __restrict__ hist_new) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ncoef) return;
+  const int l = D.lidx[i];
+  double2 cur = make_double2(0.0, 0.0);
+  const double2 ld = load[i];
+  if (l != 0) {
+    const double2 d = dice[i];
+    cur = make_double2(__dadd_rn(__dmul_rn(d.x, D.rhoi), __dmul_rn(ld.x, D.rhow)),
+                       __dadd_rn(__dmul_rn(d.y, D.rhoi), __dmul_rn(ld.y, D.rhow)));
+  }
+  const double2 p = p_load[i];
+  p_load[i] = make_double2(__dadd_rn(p.x, cur.x), __dadd_rn(p.y, cur.y));
+  p_ice[i] = dI[i];
+  p_ocean[i] = dScur[i];
+  prev_ice[i] = icelm[i];
+  if (hist_new) hist_new[i] = ld;
+}
+
+__global__ void k_rot_commit(Scal* sc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int q = 0; q < 9; ++q) sc->p_il[q] = __dadd_rn(sc->p_il[q], sc->dil[q]);
+  for (int q = 0; q < 3; ++q) sc->p_m[q] = __dadd_rn(sc->p_m[q], sc->dm[q]);
+  for (int q = 0; q < 6; ++q) sc->p_lambda[q] = __dadd_rn(sc->p_lambda[q], sc->dlam_cur2[q]);
+}
+
+// Post-step topography / ocean function (solver.py:1099-1101) and, for the diag option, the
+// row sums of the four degree-0 diagnostics (solver_opt.py:893-916): block per row.
+__global__ void k_post_grid(Dev D, const double* __restrict__ tinit, const double* __restrict__ deltasl,
+                            const double* __restrict__ beta, double* __restrict__ topo,
+                            double* __restrict__ topo_prev, double* __restrict__ cxy,
+                            double* __restrict__ slc, double* __restrict__ slcb, double* __restrict__ cstar,
+                            double* __restrict__ rows /* [4][nlat] or null */) {
+  __shared__ double sh[32];
+  const int j = blockIdx.x;
+  double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
+  for (int t = threadIdx.x; t < D.nlon; t += blockDim.x) {
+    const size_t i = (size_t)j * D.nlon + t;
+    const double ds = deltasl[i];
+    const double tp = __dsub_rn(tinit[i], ds);
+    topo[i] = tp;
+    topo_prev[i] = tp;
+    const double o = (tp < 0.0) ? 1.0 : 0.0;
+    cxy[i] = o;
+    const double s1 = __dmul_rn(ds, o);
+    const double bb = beta[i];
+    const double s2 = __dmul_rn(s1, bb);
+    const double cs = __dmul_rn(o, bb);
+    if (slc) {
+      slc[i] = s1;
+      slcb[i] = s2;
+      cstar[i] = cs;
+    }
+    a += s1;
+    b += o;
+    c += s2;
+    d += cs;
+  }
+  if (!rows) return;
+  a = block_sum(a, sh);
+  b = block_sum(b, sh);
+  c = block_sum(c, sh);
+  d = block_sum(d, sh);
+  if (threadIdx.x == 0) {
+    rows[j] = a;
+    rows[D.nlat + j] = b;
+    rows[2 * D.nlat + j] = c;
+    rows[3 * D.nlat + j] = d;
+  }
+}
+
+// degree-0 coefficient U00 = sum_j P~_00 w_j rowsum_j / (nlon 1.41421356), P~_00 = sqrt(0.5)
+__global__ void k_degree0(Dev D, const double* rows, const double* w, Scal* sc) {
+  __shared__ double sh[32];
+  for (int q = 0; q < 4; ++q) {
+    double acc = 0.0;
+    for (int j = threadIdx.x; j < D.nlat; j += blockDim.x) acc += w[j] * rows[q * D.nlat + j];
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) sc->diag[q] = sqrt(0.5) * acc / (double)D.nlon / SQRT2_LEGACY;
+    __syncthreads();
+  }
+}
+
+__global__ void k_grid_add(long long n, const double* a, const double* b, double* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = __dadd_rn(a[i], b[i]);
+}
+
+__global__ void k_init_grid(Dev D, const double* __restrict__ tinit, const double* __restrict__ ice0,
+                            double* __restrict__ cxy0, double* __restrict__ beta0, double* __restrict__ cstar0,
+                            double* __restrict__ cxy, double* __restrict__ topo_prev, double* __restrict__ ic0) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ng) return;
+  const double t = tinit[i];
+  const double c = (t < 0.0) ? 1.0 : 0.0;
+  cxy0[i] = c;
+  cxy[i] = c;
+  topo_prev[i] = t;
+  const double v = ice0[i];
+  const double g = D.checkmarine ? icestar_on(v, t, D.rhow, D.rhoi) : v;
+  ic0[i] = g;
+  const double b = (g < EPS0) ? 1.0 : 0.0;
+  beta0[i] = b;
+  cstar0[i] = __dmul_rn(c, b);
+}
+
+__global__ void k_finite(long long n, const double* a, unsigned int* bad) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !isfinite(a[i])) atomicOr(bad, 1u);
+}
+
+}  // namespace sle
+
+// ============================================================================ handle
+using namespace sle;
+
+struct sle_solver {
+  sle_config cfg;
+  sle_sht* plan;
+  cudaStream_t st;
+  Dev D;
+  RotConst C;
+  int K, nmod2;
+  // earth
+  double *s_kl, *decay, *omd, *a_sl, *a_rr, *ttl, *ttlekhl, *ttlhe, *a_il, *a_m, *a_tsl, *a_trr;
+  int* nmod;
+  double *r_il, *r_m, *r_lam;
+  // grids
+  double *tinit, *cxy0, *beta0, *cstar0, *cxy, *topo_prev, *icestar, *beta, *cstar, *tO, *rO, *dsl, *deltasl,
+      *topo, *rr, *grnew, *ice, *ice_prev, *tmpg, *gbuf3, *gbuf4, *rows;
+  // spectra (packed)
+  double2 *R, *p_load, *p_ice, *p_ocean, *prev_ice, *visc, *rad, *icelm, *oldice, *dice, *dI, *cstarlm, *tOlm,
+      *rOlm, *load, *dScur, *sl, *sltot, *rrlm, *h1, *h2, *spare[4];
+  Scal* sc;
+  Scal* hsc;  // pinned mirror
+  double* partials;
+  unsigned int* counter;
+  unsigned int* badflag;
+  double K00;
+  int iter, inited, nhist;
+  double dt_cur, dt_hist[2];
+  double ocean_area0, oceanBeta_area0, ice_volume0;
+  sle_step_info last;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), (n ? n : 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(%zu bytes) failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    *p = nullptr;
+    return SLE_ERR_OOM;
+  }
+  return SLE_OK;
+}
+
+inline unsigned nb(long long n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
+
+void solver_free(sle_solver* s) {
+  if (!s) return;
+  void* ptrs[] = {s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr, s->ttl, s->ttlekhl, s->ttlhe, s->a_il, s->a_m,
+                  s->a_tsl, s->a_trr, s->nmod, s->r_il, s->r_m, s->r_lam, s->tinit, s->cxy0, s->beta0,
+                  s->cstar0, s->cxy, s->topo_prev, s->icestar, s->beta, s->cstar, s->tO, s->rO, s->dsl,
+                  s->deltasl, s->topo, s->rr, s->grnew, s->ice, s->ice_prev, s->tmpg, s->gbuf3, s->gbuf4,
+                  s->rows, s->R, s->p_load, s->p_ice, s->p_ocean, s->prev_ice, s->visc, s->rad, s->icelm,
+                  s->oldice, s->dice, s->dI, s->cstarlm, s->tOlm, s->rOlm, s->load, s->dScur, s->sl,
+                  s->sltot, s->rrlm, s->h1, s->h2, s->spare[0], s->spare[1], s->spare[2], s->spare[3],
+                  s->sc, s->partials, s->counter, s->badflag};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (s->hsc) cudaFreeHost(s->hsc);
+  if (s->st) cudaStreamDestroy(s->st);
+  if (s->plan) sle_sht_destroy(s->plan);
+  delete s;
+}
+
+int upload(void* dst, const void* src, size_t bytes, int on_device, cudaStream_t st) {
+  SLE_CUDA(cudaMemcpyAsync(dst, src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  return SLE_OK;
+}
+
+int sync_scal(sle_solver* s) {
+  SLE_CUDA(cudaMemcpyAsync(s->hsc, s->sc, sizeof(Scal), cudaMemcpyDeviceToHost, s->st));
+  SLE_CUDA(cudaStreamSynchronize(s->st));
+  return SLE_OK;
+}
+
+int check_finite(sle_solver* s, const double* dev, long long n, const char* what) {
+  SLE_CUDA(cudaMemsetAsync(s->badflag, 0, sizeof(unsigned int), s->st));
+  k_finite<<<nb(n), 256, 0, s->st>>>(n, dev, s->badflag);
+  unsigned int bad = 0;
+  SLE_CUDA(cudaMemcpyAsync(&bad, s->badflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
+  SLE_CUDA(cudaStreamSynchronize(s->st));
+  if (bad) {
+    set_error("%s contains NaN or Inf", what);
+    return SLE_ERR_NONFINITE;
+  }
+  return SLE_OK;
+}
+
+int set_dt(sle_solver* s, double dt) {
+  if (dt == s->dt_cur) return SLE_OK;
+  k_set_decay<<<nb((long long)s->K * s->D.nl), 256, 0, s->st>>>(s->K, s->D.nl, s->s_kl, s->nmod, dt, s->decay,
+                                                               s->omd);
+  SLE_CUDA(cudaGetLastError());
+  s->dt_cur = dt;
+  return SLE_OK;
+}
+
+int ana(sle_solver* s, int nf, const double* g0, double2* o0, const double* g1 = nullptr, double2* o1 = nullptr,
+        const double* g2 = nullptr, double2* o2 = nullptr, const double* g3 = nullptr, double2* o3 = nullptr) {
+  const double* g[4] = {g0, g1, g2, g3};
+  double2* o[4] = {o0, o1, o2, o3};
+  return sht_analysis_packed(s->plan, nf, g, o, s->st);
+}
+
+int syn(sle_solver* s, const double2* c, double* g, const SynEpilogue* epi = nullptr) {
+  const double2* cc[1] = {c};
+  double* gg[1] = {g};
+  return sht_synthesis_packed(s->plan, 1, cc, gg, epi, s->st);
+}
+
+double fourpiR2(const sle_solver* s, double x) {
+  // x * 4 * PI * radius**2 with the reference's left-to-right association
+  return ((x * 4.0) * PI_LEGACY) * std::pow(s->cfg.radius, 2);
+}
+
+}  // namespace
+
+extern "C" int sle_solver_create(const sle_config* cfg, const sle_earth* earth, sle_solver** out) {
+  if (!cfg || !earth || !out) {
+    set_error("sle_solver_create: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  if (earth->nmodes < 0 || earth->nmodes > 4096) {
+    set_error("sle_solver_create: nmodes out of range");
+    return SLE_ERR_BAD_ARG;
+  }
+  sle_solver* s = new sle_solver();
+  std::memset(s, 0, sizeof(sle_solver));
+  s->cfg = *cfg;
+  int rc = sle_sht_create(cfg->nlat, cfg->nlon, cfg->lmax, &s->plan);
+  if (rc != SLE_OK) {
+    delete s;
+    return rc;
+  }
+#define TRY(x)                \
+  do {                        \
+    rc = (x);                 \
+    if (rc != SLE_OK) {       \
+      solver_free(s);         \
+      return rc;              \
+    }                         \
+  } while (0)
+#define TRYC(x)                                                                       \
+  do {                                                                                \
+    cudaError_t e_ = (x);                                                             \
+    if (e_ != cudaSuccess) {                                                          \
+      set_error("%s failed: %s", #x, cudaGetErrorString(e_));                          \
+      solver_free(s);                                                                 \
+      return SLE_ERR_CUDA;                                                            \
+    }                                                                                 \
+  } while (0)
+  TRYC(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  const int nl = cfg->lmax + 1;
+  const long long ng = (long long)cfg->nlat * cfg->nlon;
+  const long long nc = s->plan->d.ncoef;
+  const int K = earth->nmodes;
+  s->K = K;
+  // earth
+  TRY(dalloc(&s->s_kl, (size_t)K * nl));
+  TRY(dalloc(&s->decay, (size_t)K * nl));
+  TRY(dalloc(&s->omd, (size_t)K * nl));
+  TRY(dalloc(&s->a_sl, (size_t)K * nl));
+  TRY(dalloc(&s->a_rr, (size_t)K * nl));
+  TRY(dalloc(&s->ttl, nl));
+  TRY(dalloc(&s->ttlekhl, nl));
+  TRY(dalloc(&s->ttlhe, nl));
+  TRY(dalloc(&s->a_il, K));
+  TRY(dalloc(&s->a_m, K));
+  TRY(dalloc(&s->a_tsl, K));
+  TRY(dalloc(&s->a_trr, K));
+  TRY(dalloc(&s->nmod, nl));
+  TRY(dalloc(&s->r_il, (size_t)K * 9));
+  TRY(dalloc(&s->r_m, (size_t)K * 3));
+  TRY(dalloc(&s->r_lam, (size_t)K * 6));
+  TRYC(cudaMemcpy(s->s_kl, earth->s, sizeof(double) * K * nl, cudaMemcpyHostToDevice));
+  TRYC(cudaMemcpy(s->a_sl, earth->a_sl, sizeof(double) * K * nl, cudaMemcpyHostToDevice));
+  TRYC(cudaMemcpy(s->a_rr, earth->a_rr, sizeof(double) * K * nl, cudaMemcpyHostToDevice));
+  TRYC(cudaMemcpy(s->ttl, earth->ttl, sizeof(double) * nl, cudaMemcpyHostToDevice));
+  TRYC(cudaMemcpy(s->ttlekhl, earth->ttlekhl, sizeof(double) * nl, cudaMemcpyHostToDevice));
+  TRYC(cudaMemcpy(s->ttlhe, earth->ttlhe, sizeof(double) * nl, cudaMemcpyHostToDevice));
+  if (K > 0) {
+    TRYC(cudaMemcpy(s->a_il, earth->a_il, sizeof(double) * K, cudaMemcpyHostToDevice));
+    TRYC(cudaMemcpy(s->a_m, earth->a_m, sizeof(double) * K, cudaMemcpyHostToDevice));
+    TRYC(cudaMemcpy(s->a_tsl, earth->a_tsl, sizeof(double) * K, cudaMemcpyHostToDevice));
+    TRYC(cudaMemcpy(s->a_trr, earth->a_trr, sizeof(double) * K, cudaMemcpyHostToDevice));
+  }
+  std::vector<int> nm(earth->nmod, earth->nmod + nl);
+  for (int l = 0; l < nl; ++l) {
+    if (nm[l] < 0 || nm[l] > K) {
+      set_error("sle_solver_create: nmod[%d]=%d outside 0..%d", l, nm[l], K);
+      solver_free(s);
+      return SLE_ERR_BAD_ARG;
+    }
+  }
+  TRYC(cudaMemcpy(s->nmod, nm.data(), sizeof(int) * nl, cudaMemcpyHostToDevice));
+  s->nmod2 = nl > 2 ? nm[2] : 0;
+  // grids
+  double** grids[] = {&s->tinit, &s->cxy0, &s->beta0, &s->cstar0, &s->cxy, &s->topo_prev, &s->icestar, &s->beta,
+                      &s->cstar, &s->tO, &s->rO, &s->dsl, &s->deltasl, &s->topo, &s->rr, &s->grnew, &s->ice,
+                      &s->ice_prev, &s->tmpg, &s->gbuf3, &s->gbuf4};
+  for (double** g : grids) TRY(dalloc(g, ng));
+  TRY(dalloc(&s->rows, (size_t)4 * cfg->nlat));
+  double2** specs[] = {&s->p_load, &s->p_ice, &s->p_ocean, &s->prev_ice, &s->visc, &s->rad, &s->icelm,
+                       &s->oldice, &s->dice, &s->dI, &s->cstarlm, &s->tOlm, &s->rOlm, &s->load, &s->dScur,
+                       &s->sl, &s->sltot, &s->rrlm, &s->h1, &s->h2, &s->spare[0], &s->spare[1], &s->spare[2],
+                       &s->spare[3]};
+  for (double2** p : specs) TRY(dalloc(p, nc));
+  TRY(dalloc(&s->R, (size_t)K * nc + 1));
+  TRY(dalloc(&s->sc, 1));
+  TRY(dalloc(&s->partials, 4096));
+  TRY(dalloc(&s->counter, 4));
+  TRY(dalloc(&s->badflag, 1));
+  TRYC(cudaMallocHost(reinterpret_cast<void**>(&s->hsc), sizeof(Scal)));
+  TRYC(cudaMemset(s->counter, 0, 4 * sizeof(unsigned int)));
+  // device view
+  Dev& D = s->D;
+  D.nlat = cfg->nlat;
+  D.nlon = cfg->nlon;
+  D.nl = nl;
+  D.ng = ng;
+  D.ncoef = nc;
+  D.K = K;
+  D.lidx = s->plan->d.lidx;
+  D.nmod = s->nmod;
+  D.decay = s->decay;
+  D.omd = s->omd;
+  D.a_sl = s->a_sl;
+  D.a_rr = s->a_rr;
+  D.ttl = s->ttl;
+  D.ttlekhl = s->ttlekhl;
+  D.ttlhe = s->ttlhe;
+  D.a_il = s->a_il;
+  D.a_m = s->a_m;
+  D.a_tsl = s->a_tsl;
+  D.a_trr = s->a_trr;
+  D.nmod2 = s->nmod2;
+  D.rhoi = cfg->rhoi;
+  D.rhow = cfg->rhow;
+  D.epsilon1 = cfg->epsilon1;
+  D.checkmarine = cfg->checkmarine;
+  D.tpw = cfg->tpw && nl > 2;
+  D.calcRG = cfg->calcRG;
+  D.opt_dsl = cfg->opt_dsl;
+  const int L = cfg->lmax;
+  D.i20 = 2;
+  D.i21 = (long long)(L + 1) + 1;
+  D.i22 = (long long)2 * (L + 1) - 1 + 0;
+  // rotation constants (solver.py:910-975), same expressions as the reference
+  RotConst& C = s->C;
+  const double a4 = std::pow(cfg->radius, 4);
+  C.c_il22 = (-8 * PI_LEGACY * a4) / (3 * std::sqrt(5.0));
+  C.c_il02 = (-8 * PI_LEGACY * a4) / std::sqrt(30.0);
+  C.c_il12 = (8 * PI_LEGACY * a4) / std::sqrt(30.0);
+  C.alpha = 1 / (1 - earth->kTE2 / cfg->kf);
+  C.inv_CmA = 1 / (cfg->moiC - cfg->moiA);
+  C.inv_kf = 1 / cfg->kf;
+  C.inv_C = 1.0 / cfg->moiC;
+  C.onepk = 1 + earth->kE2;
+  const double r2w2 = std::pow(cfg->radius, 2) * std::pow(cfg->omega, 2);
+  C.r2w2_3 = r2w2 / 3.0;
+  C.r2w2_6s5 = r2w2 / (6.0 * std::sqrt(5.0));
+  C.r2w2_s30 = r2w2 / std::sqrt(30.0);
+  C.r2w2_s120 = r2w2 / std::sqrt(5.0 * 24.0);
+  C.ekhTE = 1 + earth->kTE2 - earth->hTE2;
+  C.hTE2 = earth->hTE2;
+  C.gacc = cfg->gacc;
+  C.rhoi = cfg->rhoi;
+  C.rhow = cfg->rhow;
+  s->dt_cur = -1.0;
+  TRY(set_dt(s, cfg->dt_years));
+  TRYC(cudaStreamSynchronize(s->st));
+  *out = s;
+  return SLE_OK;
+#undef TRY
+#undef TRYC
+}
+
+extern "C" int sle_solver_destroy(sle_solver* s) {
+  if (s) cudaStreamSynchronize(s->st);
+  solver_free(s);
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_stream(sle_solver* s, void** stream) {
+  if (!s || !stream) {
+    set_error("sle_solver_stream: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  *stream = reinterpret_cast<void*>(s->st);
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_init(sle_solver* s, const double* topo0, const double* ice0, int on_device,
+                               double* ocean_area0, double* oceanBeta_area0, double* ice_volume0) {
+  if (!s || !topo0 || !ice0) {
+    set_error("sle_solver_init: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  const Dev& D = s->D;
+  const size_t gb = sizeof(double) * D.ng;
+  cudaStream_t st = s->st;
+  SLE_TRY(upload(s->tinit, topo0, gb, on_device, st));
+  SLE_TRY(upload(s->ice_prev, ice0, gb, on_device, st));
+  SLE_TRY(check_finite(s, s->tinit, D.ng, "topography"));
+  SLE_TRY(check_finite(s, s->ice_prev, D.ng, "initial ice"));
+  k_init_grid<<<nb(D.ng), 256, 0, st>>>(D, s->tinit, s->ice_prev, s->cxy0, s->beta0, s->cstar0, s->cxy,
+                                        s->topo_prev, s->icestar);
+  SLE_CUDA(cudaGetLastError());
+  // step-0 areas and volume from full analyses (solver.py:571-581)
+  SLE_TRY(ana(s, 3, s->cxy0, s->spare[0], s->cstar0, s->spare[1], s->icestar, s->spare[2]));
+  double2 v[3];
+  for (int q = 0; q < 3; ++q)
+    SLE_CUDA(cudaMemcpyAsync(&v[q], s->spare[q], sizeof(double2), cudaMemcpyDeviceToHost, st));
+  // modal and rotational state start at zero
+  const long long nc = D.ncoef;
+  SLE_CUDA(cudaMemsetAsync(s->R, 0, sizeof(double2) * ((size_t)s->K * nc + 1), st));
+  double2* zero_specs[] = {s->p_load, s->p_ice, s->p_ocean, s->prev_ice, s->h1, s->h2};
+  for (double2* z : zero_specs) SLE_CUDA(cudaMemsetAsync(z, 0, sizeof(double2) * nc, st));
+  SLE_CUDA(cudaMemsetAsync(s->r_il, 0, sizeof(double) * 9 * (s->K ? s->K : 1), st));
+  SLE_CUDA(cudaMemsetAsync(s->r_m, 0, sizeof(double) * 3 * (s->K ? s->K : 1), st));
+  SLE_CUDA(cudaMemsetAsync(s->r_lam, 0, sizeof(double) * 6 * (s->K ? s->K : 1), st));
+  SLE_CUDA(cudaMemsetAsync(s->sc, 0, sizeof(Scal), st));
+  // K00 = synth(e00)[0,0] (solver_opt.py:320-325)
+  s->K00 = 0.0;
+  if (s->cfg.opt_dsl) {
+    SLE_CUDA(cudaMemsetAsync(s->spare[3], 0, sizeof(double2) * nc, st));
+    const double2 one = make_double2(1.0, 0.0);
+    SLE_CUDA(cudaMemcpyAsync(s->spare[3], &one, sizeof(double2), cudaMemcpyHostToDevice, st));
+    SLE_TRY(syn(s, s->spare[3], s->tmpg));
+    SLE_CUDA(cudaMemcpyAsync(&s->K00, s->tmpg, sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  SLE_CUDA(cudaStreamSynchronize(st));
+  SLE_CUDA(cudaMemcpy(&s->sc->K00, &s->K00, sizeof(double), cudaMemcpyHostToDevice));
+  s->ocean_area0 = fourpiR2(s, v[0].x);
+  s->oceanBeta_area0 = fourpiR2(s, v[1].x);
+  s->ice_volume0 = fourpiR2(s, v[2].x);
+  if (ocean_area0) *ocean_area0 = s->ocean_area0;
+  if (oceanBeta_area0) *oceanBeta_area0 = s->oceanBeta_area0;
+  if (ice_volume0) *ice_volume0 = s->ice_volume0;
+  s->iter = 0;
+  s->nhist = 0;
+  s->dt_hist[0] = s->dt_hist[1] = s->cfg.dt_years;
+  s->inited = 1;
+  std::memset(&s->last, 0, sizeof(s->last));
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, double dt_years,
+                               sle_step_info* info) {
+  if (!s || !ice) {
+    set_error("sle_solver_step: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (!s->inited) {
+    set_error("sle_solver_step: call sle_solver_init first");
+    return SLE_ERR_STATE;
+  }
+  const Dev& D = s->D;
+  cudaStream_t st = s->st;
+  const long long nc = D.ncoef, ng = D.ng;
+  double dt = s->cfg.dt_years;
+  if (dt_years > 0.0) {
+    dt = dt_years;
+    s->cfg.dt_years = dt;
+  }
+  SLE_TRY(set_dt(s, dt));
+  s->iter += 1;
+  const int it = s->iter;
+  SLE_TRY(upload(s->ice, ice, sizeof(double) * ng, on_device, st));
+
+  // ---- modal advance (solver.py:835)
+  k_advance<<<nb(nc), 256, 0, st>>>(D, s->R, s->p_load, s->visc, s->rad);
+  k_rot_advance<<<1, 1, 0, st>>>(D, s->sc, s->r_il, s->r_m, s->r_lam);
+  // ---- ice and ocean grids, their analyses
+  k_ice_grid<<<nb(ng), 256, 0, st>>>(D, s->ice, s->topo_prev, s->cxy, s->tinit, s->cstar0, s->icestar, s->beta,
+                                     s->cstar, s->tO, s->ice_prev, it == 1 ? s->tmpg : nullptr, s->sc);
+  SLE_CUDA(cudaGetLastError());
+  if (it == 1) {
+    SLE_TRY(ana(s, 4, s->icestar, s->icelm, s->cstar, s->cstarlm, s->tO, s->tOlm, s->tmpg, s->oldice));
+  } else {
+    SLE_TRY(ana(s, 3, s->icestar, s->icelm, s->cstar, s->cstarlm, s->tO, s->tOlm));
+    SLE_CUDA(cudaMemcpyAsync(s->oldice, s->prev_ice, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, st));
+  }
+  // ---- first guess
+  int mode = 0;
+  double c1 = 0.0, c2 = 0.0;
+  if (s->cfg.inner_extrap && s->nhist >= 2) {
+    const double dt0 = dt, dt1 = s->dt_hist[0], dt2 = s->dt_hist[1];
+    if (dt0 == dt1 && dt1 == dt2) {
+      mode = 1;
+    } else {
+      mode = 2;
+      const double w = (dt0 + dt1) / (dt1 + dt2);
+      c1 = dt0 / dt1 * (1.0 + w);
+      c2 = dt0 / dt2 * w;
+    }
+  }
+  const unsigned red_blocks = std::min<unsigned>(RED_BLOCKS, nb(nc));
+  k_pre_spec<<<red_blocks, 256, 0, st>>>(D, s->icelm, s->oldice, s->p_ice, s->cstarlm, s->p_ocean, s->h1, s->h2,
+                                         mode, c1, c2, s->dice, s->dI, s->load, s->dScur, s->sc, s->partials,
+                                         s->counter);
+  SLE_CUDA(cudaGetLastError());
+
+  // ---- inner fixed-point loop (solver.py:907-1051)
+  const unsigned red_grid = std::min<unsigned>(RED_BLOCKS, nb(ng));
+  for (int host_iter = 0;; ++host_iter) {
+    if (host_iter > MAX_INNER + 2) {  // the device flag must have stopped the loop by now
+      set_error("inner loop control lost (device iteration counter did not advance)");
+      return SLE_ERR_STATE;
+    }
+    k_b18<<<nb(nc), 256, 0, st>>>(D, s->C, s->dI, s->p_ocean, s->load, s->visc, s->dScur, s->sl, s->sc);
+    SynEpilogue epi{s->rO, s->cstar};
+    SLE_TRY(syn(s, s->sl, s->dsl, &epi));
+    SLE_TRY(ana(s, 1, s->rO, s->rOlm));
+    k_update<<<red_blocks, 256, 0, st>>>(D, s->p_ocean, s->rOlm, s->cstarlm, s->tOlm, s->dI, s->load, s->dScur,
+                                         s->sc, s->partials, s->counter);
+    if (!s->cfg.opt_dsl) {
+      k_sltot<<<nb(nc), 256, 0, st>>>(D, s->sl, s->sltot, s->sc);
+      SLE_TRY(syn(s, s->sltot, s->deltasl));
+    }
+    k_refresh1<<<red_grid, 256, 0, st>>>(D, s->dsl, s->deltasl, s->tinit, s->topo, s->cxy, s->ice, s->beta,
+                                         s->grnew, s->sc, s->partials + 2048, s->counter + 1);
+    SLE_CUDA(cudaGetLastError());
+    SLE_TRY(sync_scal(s));
+    const Scal& h = *s->hsc;
+    if (h.converged || h.status != 0) break;
+    const int changed = h.gr_changed;
+    k_refresh2<<<nb(ng), 256, 0, st>>>(D, s->cxy, s->tinit, s->cstar0, s->grnew, s->icestar, s->beta, s->cstar,
+                                       s->tO, changed);
+    if (changed) {
+      SLE_TRY(ana(s, 3, s->icestar, s->icelm, s->cstar, s->cstarlm, s->tO, s->tOlm));
+      k_dice<<<nb(nc), 256, 0, st>>>(D, s->icelm, s->oldice, s->p_ice, s->dice, s->dI);
+      SLE_CUDA(cudaMemsetAsync(&s->sc->gr_changed, 0, sizeof(int), st));
+    } else {
+      SLE_TRY(ana(s, 2, s->cstar, s->cstarlm, s->tO, s->tOlm));
+    }
+    SLE_CUDA(cudaGetLastError());
+  }
+  const Scal& h = *s->hsc;
+  if (h.status != SLE_OK) {
+    if (h.status == SLE_ERR_NONCONVERGED)
+      set_error("inner loop failed to converge, xi=%.17g", h.xi);
+    else
+      set_error("non-finite value in the inner loop (xi=%g)", h.xi);
+    s->last.status = h.status;
+    return h.status;
+  }
+
+  // ---- radial displacement (solver.py:1054-1072)
+  if (s->cfg.calcRG) {
+    k_rr<<<nb(nc), 256, 0, st>>>(D, s->dI, s->p_ocean, s->load, s->rad, s->rrlm, s->sc);
+    SLE_TRY(syn(s, s->rrlm, s->rr));
+  }
+  // ---- commit (solver.py:1080-1096); extrap history (solver_opt.py:817-822)
+  double2* hist_new = s->cfg.inner_extrap ? s->h2 : nullptr;
+  k_commit<<<nb(nc), 256, 0, st>>>(D, s->dice, s->load, s->dI, s->dScur, s->icelm, s->p_load, s->p_ice, s->p_ocean,
+                                   s->prev_ice, hist_new);
+  if (D.tpw) k_rot_commit<<<1, 1, 0, st>>>(s->sc);
+  if (s->cfg.inner_extrap) {
+    double2* t = s->h1;
+    s->h1 = s->h2;
+    s->h2 = t;
+    s->dt_hist[1] = s->dt_hist[0];
+    s->dt_hist[0] = dt;
+    s->nhist = std::min(2, s->nhist + 1);
+  }
+  // ---- topography / ocean function and the degree-0 diagnostics
+  if (s->cfg.opt_diag) {
+    k_post_grid<<<D.nlat, 256, 0, st>>>(D, s->tinit, s->deltasl, s->beta, s->topo, s->topo_prev, s->cxy, nullptr,
+                                        nullptr, nullptr, s->rows);
+    k_degree0<<<1, 256, 0, st>>>(D, s->rows, s->plan->d.w, s->sc);
+  } else {
+    k_post_grid<<<D.nlat, 256, 0, st>>>(D, s->tinit, s->deltasl, s->beta, s->topo, s->topo_prev, s->cxy, s->tmpg,
+                                        s->gbuf3, s->gbuf4, nullptr);
+    SLE_TRY(ana(s, 4, s->tmpg, s->spare[0], s->cxy, s->spare[1], s->gbuf3, s->spare[2], s->gbuf4, s->spare[3]));
+  }
+  SLE_CUDA(cudaGetLastError());
+  double2 d4[4];
+  if (!s->cfg.opt_diag)
+    for (int q = 0; q < 4; ++q)
+      SLE_CUDA(cudaMemcpyAsync(&d4[q], s->spare[q], sizeof(double2), cudaMemcpyDeviceToHost, st));
+  double2 ice00;
+  SLE_CUDA(cudaMemcpyAsync(&ice00, s->icelm, sizeof(double2), cudaMemcpyDeviceToHost, st));
+  SLE_TRY(sync_scal(s));
+  const Scal& f = *s->hsc;
+  double slc_ocn00, c00, slc_b00, cst00;
+  if (s->cfg.opt_diag) {
+    slc_ocn00 = f.diag[0];
+    c00 = f.diag[1];
+    slc_b00 = f.diag[2];
+    cst00 = f.diag[3];
+  } else {
+    slc_ocn00 = d4[0].x;
+    c00 = d4[1].x;
+    slc_b00 = d4[2].x;
+    cst00 = d4[3].x;
+  }
+  sle_step_info& o = s->last;
+  o.iter = it;
+  o.numiter = f.numiter;
+  o.status = SLE_OK;
+  o.gr_reguess = f.gr_reguess;
+  o.gr_ice_analyses = f.gr_ice_an;
+  o.xi = f.xi;
+  if (s->cfg.opt_diag) {
+    // float arithmetic of solver_opt.py:909-914
+    const double a4 = 4 * PI_LEGACY * std::pow(s->cfg.radius, 2);
+    o.ocean_area = c00 * a4;
+    o.oceanBeta_area = cst00 * a4;
+    o.gmslc_ocn = slc_ocn00 / c00;
+    o.gmslc_ocnBeta = slc_b00 / cst00;
+  } else {
+    // complex [0,0] ratios of solver.py:1105-1113 (imaginary parts are exactly zero)
+    o.ocean_area = fourpiR2(s, c00);
+    o.oceanBeta_area = fourpiR2(s, cst00);
+    o.gmslc_ocn = slc_ocn00 * (1.0 / c00);
+    o.gmslc_ocnBeta = slc_b00 * (1.0 / cst00);
+  }
+  o.ice_volume = fourpiR2(s, ice00.x);
+  std::memcpy(o.il, f.il, sizeof(o.il));
+  std::memcpy(o.mm, f.mm, sizeof(o.mm));
+  std::memcpy(o.lam, f.lam, sizeof(o.lam));
+  if (info) *info = o;
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device) {
+  if (!s || !dst) {
+    set_error("sle_solver_get: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  const Dev& D = s->D;
+  const size_t gb = sizeof(double) * D.ng;
+  const cudaMemcpyKind kind = dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const double* src = nullptr;
+  switch (field) {
+    case SLE_F_TGRID: src = s->topo; break;
+    case SLE_F_OCEAN: src = s->cxy; break;
+    case SLE_F_BETA: src = s->beta; break;
+    case SLE_F_R: src = s->rr; break;
+    case SLE_F_DELTASL: src = s->deltasl; break;
+    case SLE_F_ICESTAR: src = s->icestar; break;
+    case SLE_F_OCEAN0: src = s->cxy0; break;
+    case SLE_F_BETA0: src = s->beta0; break;
+    case SLE_F_G:
+      k_grid_add<<<nb(D.ng), 256, 0, s->st>>>(D.ng, s->deltasl, s->rr, s->tmpg);
+      SLE_CUDA(cudaGetLastError());
+      src = s->tmpg;
+      break;
+    case SLE_F_DS_CONVERGED:
+    case SLE_F_LOAD_INC: {
+      const double2* p = (field == SLE_F_DS_CONVERGED) ? s->p_ocean : s->load;
+      double2* dense = s->plan->packbuf;  // staging (nm*nm <= 4*ncoef)
+      SLE_TRY(sht_unpack(s->plan, p, dense, s->st));
+      const size_t bytes = sizeof(double2) * (size_t)D.nl * D.nl;
+      SLE_CUDA(cudaMemcpyAsync(dst, dense, bytes, kind, s->st));
+      SLE_CUDA(cudaStreamSynchronize(s->st));
+      return SLE_OK;
+    }
+    default:
+      set_error("sle_solver_get: unknown field %d", field);
+      return SLE_ERR_BAD_ARG;
+  }
+  SLE_CUDA(cudaMemcpyAsync(dst, src, gb, kind, s->st));
+  SLE_CUDA(cudaStreamSynchronize(s->st));
+  return SLE_OK;
+}

@@ -1,0 +1,314 @@
+"""GPU sea-level solver behind the reference's solver interface.
+
+``SeaLevelSolver`` mirrors SLEvolve ``python/slevolve/solver.py:518-1144`` (constructor
+arguments, ``step(icexy_cur, profile=False, dt=None, rates=False) -> dict``, step-0 attributes)
+and ``OptSeaLevelSolver`` mirrors ``solver_opt.py:267-979`` (``opt`` set, ``inner``), so that the
+forward driver (run_ais.py:322) and the outer driver (run_outer.py:216) can construct them in
+place of the reference classes.  The whole step runs on the device (``libslevolve_b200.so``);
+grids in the returned dict are copied to host memory on first access and alias per-solver host
+buffers that the next step overwrites, as the reference's do (tests/test_small_case.py:110 of the
+reference copies them for that reason).
+
+Branches of the reference that this build does not provide raise ``NotImplementedError``: the
+second-order ramp placement, the axial-rotation options, Anderson mixing, analytic rates, the
+horizontal read-out and cross-pass reuse.  The ``raw`` option needs a raw-mode backend and raises
+``ValueError`` as in the reference (solver_opt.py:299-301).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _lib
+from .love import mode_arrays
+
+PI = 3.1415926535898   # truncated legacy literal (solver.py:31)
+EPS0 = float(np.finfo(np.float64).eps)
+
+
+class Planet:
+    """Constants of ``planets_mod::earth_init`` (solver.py:98-110)."""
+
+    def __init__(self):
+        self.radius = 6.371e6
+        self.mass = 5.976e24
+        self.rhoi = 920.0
+        self.rhow = 1000.0
+        self.gacc = 9.80665
+        self.omega = 7.292e-5
+        self.moiA = 0.3296145 * self.mass * self.radius ** 2
+        self.moiC = 0.3307007 * self.mass * self.radius ** 2
+        self.kf = 0.9342 + 0.008
+
+
+def degree_weights(love, norder, planet):
+    """T_l, T_l (1 + k_l - h_l), T_l h_l with the reference's expressions (solver.py:596-603)."""
+    nl = norder + 1
+    l = np.arange(nl, dtype=np.float64)
+    ttl = np.zeros(nl)
+    ttl[1:] = (4.0 * PI * (planet.radius ** 3)) / (planet.mass * (2 * l[1:] + 1.0))
+    ekhl = np.zeros(nl)
+    ekhl[1:] = 1 + np.asarray(love.ke)[1:nl] - np.asarray(love.he)[1:nl]
+    he = np.zeros(nl)
+    he[1:] = np.asarray(love.he)[1:nl]
+    return ttl, ttl * ekhl, ttl * he
+
+
+class _StepResult(dict):
+    """Step outputs; grid and spectrum entries are fetched from the device on first access."""
+
+    _GRIDS = {"tgrid": _lib.F_TGRID, "ocean": _lib.F_OCEAN, "beta": _lib.F_BETA, "R": _lib.F_R,
+              "G": _lib.F_G, "deltasl": _lib.F_DELTASL, "icestar": _lib.F_ICESTAR}
+    _SPECS = {"dS_converged": _lib.F_DS_CONVERGED, "load_inc": _lib.F_LOAD_INC}
+
+    def __init__(self, solver, scalars):
+        super().__init__(scalars)
+        self._solver = solver
+
+    def __missing__(self, key):
+        if key in self._GRIDS:
+            if key in ("R", "G") and not self._solver.calcRG:
+                return None
+            v = self._solver._fetch(key, self._GRIDS[key])
+        elif key in self._SPECS:
+            v = self._solver._fetch(key, self._SPECS[key], spectral=True)
+        else:
+            raise KeyError(key)
+        self[key] = v
+        return v
+
+    def get(self, key, default=None):
+        try:
+            return self[key]
+        except KeyError:
+            return default
+
+    def __contains__(self, key):
+        return dict.__contains__(self, key) or key in self._GRIDS or key in self._SPECS
+
+
+class SeaLevelSolver:
+    """Exact-memory sea-level solver on the GPU (the reference's plain path, FP64)."""
+
+    _opt_default = ()
+    _inner_default = "off"
+
+    def __init__(self, sht, love, topo0, ice0, *, norder=512, dt=1, tpw=True, checkmarine=True,
+                 calcRG=True, epsilon1=1.0e-5, planet=None, mem_threads=1, ramp=False,
+                 axial_rotation="off", axial_tau_c=None, opt=None, inner=None, reuse="off",
+                 reuse_store=None, anderson_depth=3, max_mask_refresh=3, anderson_freeze=2,
+                 anderson_keep=False):
+        opt = set(self._opt_default if opt is None else opt)
+        inner = self._inner_default if inner is None else inner
+        if ramp:
+            raise NotImplementedError("ramp placement is not provided by the GPU solver")
+        if axial_rotation != "off":
+            raise NotImplementedError("axial_rotation options are not provided by the GPU solver")
+        if inner not in ("off", "extrap", "anderson"):
+            raise ValueError(f"inner must be one of ('off', 'extrap', 'anderson'), got {inner!r}")
+        if inner == "anderson":
+            raise NotImplementedError("Anderson mixing is not provided by the GPU solver")
+        if reuse not in ("off", "warm", "warm+ice", "warm+corr", "warm+corr2"):
+            raise ValueError(f"reuse must be off|warm|warm+ice|warm+corr|warm+corr2, got {reuse!r}")
+        if reuse != "off":
+            raise NotImplementedError("cross-pass reuse is not provided by the GPU solver")
+        unknown = opt - {"raw", "diag", "dsl", "numba", "sums"}
+        if unknown:
+            raise ValueError(f"unknown opt {sorted(unknown)}")
+        if "raw" in opt:
+            raise ValueError("--opt raw must be used with a raw-mode SHT backend")
+        topo0 = np.ascontiguousarray(topo0, dtype=np.float64)
+        nlat, nlon = topo0.shape
+        norder = int(norder)
+        if sht is not None:
+            for attr, val in (("nlat", nlat), ("nlon", nlon), ("lmax", norder)):
+                got = getattr(sht, attr, val)
+                if got != val:
+                    raise ValueError(f"sht.{attr}={got} does not match the solver ({val})")
+        self.sht = sht
+        self.love = love
+        self.norder = norder
+        self.nl = norder + 1
+        self.dt = float(dt)
+        self.tpw = bool(tpw)
+        self.checkmarine = bool(checkmarine)
+        self.calcRG = bool(calcRG)
+        self.horizontal = False
+        self.epsilon1 = float(epsilon1)
+        self.p = planet or Planet()
+        self.nlat, self.nlon = nlat, nlon
+        self.opt = opt
+        self.inner = inner
+        self.reuse = reuse
+        self.reuse_store = reuse_store if reuse_store is not None else {}
+        self.inner_stats = {"mixed": 0, "plain": 0, "fallback": 0, "singular": 0,
+                            "mask_refresh": 0, "frozen_iters": 0}
+        self.gr_counts = {"reguess": 0, "ice_analyses": 0}
+        self.prof = {}
+        self.iter = 0
+
+        L = _lib.lib()
+        self._L = L
+        p = self.p
+        cfg = _lib.SleConfig(nlat=nlat, nlon=nlon, lmax=norder, dt_years=self.dt,
+                             epsilon1=self.epsilon1, tpw=int(self.tpw),
+                             checkmarine=int(self.checkmarine), calcRG=int(self.calcRG),
+                             opt_dsl=int("dsl" in opt), opt_diag=int("diag" in opt),
+                             inner_extrap=int(inner == "extrap"), radius=p.radius, mass=p.mass,
+                             rhoi=p.rhoi, rhow=p.rhow, gacc=p.gacc, omega=p.omega, moiA=p.moiA,
+                             moiC=p.moiC, kf=p.kf)
+        ma = mode_arrays(love, norder)
+        ttl, ttlekhl, ttlhe = degree_weights(love, norder, p)
+        self._earth_arrays = keep = {
+            "nmod": np.ascontiguousarray(ma["nmod"], dtype=np.int32),
+            "s": np.ascontiguousarray(ma["s"]), "a_sl": np.ascontiguousarray(ma["a_sl"]),
+            "a_rr": np.ascontiguousarray(ma["a_rr"]), "ttl": ttl, "ttlekhl": ttlekhl,
+            "ttlhe": ttlhe, "a_il": ma["a_il"], "a_m": ma["a_m"], "a_tsl": ma["a_tsl"],
+            "a_trr": ma["a_trr"]}
+
+        def dp(a):
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+
+        kTE2 = float(love.kTE[2]) if self.nl > 2 else 0.0
+        hTE2 = float(love.hTE[2]) if self.nl > 2 else 0.0
+        kE2 = float(love.ke[2]) if self.nl > 2 else 0.0
+        earth = _lib.SleEarth(nmodes=int(ma["K"]),
+                              nmod=keep["nmod"].ctypes.data_as(C.POINTER(C.c_int)),
+                              s=dp(keep["s"]), a_sl=dp(keep["a_sl"]), a_rr=dp(keep["a_rr"]),
+                              ttl=dp(ttl), ttlekhl=dp(ttlekhl), ttlhe=dp(ttlhe),
+                              a_il=dp(keep["a_il"]), a_m=dp(keep["a_m"]), a_tsl=dp(keep["a_tsl"]),
+                              a_trr=dp(keep["a_trr"]), kTE2=kTE2, hTE2=hTE2, kE2=kE2)
+        h = C.c_void_p()
+        _lib.check(L.sle_solver_create(C.byref(cfg), C.byref(earth), C.byref(h)), "sle_solver_create")
+        self._h = h
+        self._host = {}
+        self.tinit_0 = topo0
+        self.tinit = topo0
+        ice0 = np.ascontiguousarray(ice0, dtype=np.float64)
+        if ice0.shape != topo0.shape:
+            raise ValueError(f"ice0 shape {ice0.shape} != topography shape {topo0.shape}")
+        a0, b0, v0 = C.c_double(), C.c_double(), C.c_double()
+        _lib.check(L.sle_solver_init(h, topo0.ctypes.data, ice0.ctypes.data, 0, C.byref(a0),
+                                     C.byref(b0), C.byref(v0)), "sle_solver_init")
+        self.ocean_area0 = a0.value
+        self.oceanBeta_area0 = b0.value
+        self.ice_volume0 = v0.value
+        self.cxy0 = self._fetch("_ocean0", _lib.F_OCEAN0).copy()
+        self.beta0 = self._fetch("_beta0", _lib.F_BETA0).copy()
+        self.cstar0 = self.cxy0 * self.beta0
+        self._info = _lib.SleStepInfo()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._L.sle_solver_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ---------------------------------------------------------------- helpers
+    def _host_buffer(self, key, shape, dtype):
+        buf = self._host.get(key)
+        if buf is None:
+            try:
+                import torch
+
+                t = torch.empty(shape, dtype=torch.float64 if dtype == np.float64 else torch.complex128)
+                t = t.pin_memory()
+                buf = (t, t.numpy())
+            except Exception:
+                arr = np.empty(shape, dtype=dtype)
+                buf = (None, arr)
+            self._host[key] = buf
+        return buf[1]
+
+    def _fetch(self, key, field, spectral=False):
+        if spectral:
+            arr = self._host_buffer(key, (self.nl, self.nl), np.complex128)
+        else:
+            arr = self._host_buffer(key, (self.nlat, self.nlon), np.float64)
+        _lib.check(self._L.sle_solver_get(self._h, int(field), arr.ctypes.data, 0), "sle_solver_get")
+        return arr
+
+    def stream_handle(self):
+        s = C.c_void_p()
+        _lib.check(self._L.sle_solver_stream(self._h, C.byref(s)), "sle_solver_stream")
+        return s.value
+
+    def set_step_dt(self, dt):
+        if dt is not None:
+            self.dt = float(dt)
+
+    # ------------------------------------------------------------------ step
+    def step_device(self, ice_ptr, on_device, dt=None):
+        """One step from a raw pointer (host or device); returns the step info record."""
+        self.set_step_dt(dt)
+        rc = self._L.sle_solver_step(self._h, C.c_void_p(ice_ptr), int(on_device),
+                                     float(self.dt), C.byref(self._info))
+        _lib.check(rc, "sle_solver_step")
+        self.iter = self._info.iter
+        self.gr_counts["reguess"] += self._info.gr_reguess
+        self.gr_counts["ice_analyses"] += self._info.gr_ice_analyses
+        return self._info
+
+    def step(self, icexy_cur, profile=False, dt=None, rates=False):
+        if rates:
+            raise NotImplementedError("analytic rates are not provided by the GPU solver")
+        t0 = time.perf_counter()
+        try:
+            import torch
+
+            is_dev = isinstance(icexy_cur, torch.Tensor) and icexy_cur.is_cuda
+        except ImportError:  # pragma: no cover
+            is_dev = False
+        if is_dev:
+            ice = icexy_cur.to(torch.float64).contiguous()
+            if tuple(ice.shape) != (self.nlat, self.nlon):
+                raise ValueError(f"ice shape {tuple(ice.shape)} != {(self.nlat, self.nlon)}")
+            torch.cuda.current_stream().synchronize()
+            info = self.step_device(ice.data_ptr(), 1, dt)
+        else:
+            ice = np.ascontiguousarray(icexy_cur, dtype=np.float64)
+            if ice.shape != (self.nlat, self.nlon):
+                raise ValueError(f"ice shape {ice.shape} != {(self.nlat, self.nlon)}")
+            info = self.step_device(ice.ctypes.data, 0, dt)
+        wall = time.perf_counter() - t0
+        lam = np.array(info.lam[:]).reshape(3, 3, 2)
+        scal = {
+            "iter": info.iter,
+            "numiter": info.numiter,
+            "horiz": None,
+            "ocean_area": info.ocean_area,
+            "oceanBeta_area": info.oceanBeta_area,
+            "gmslc_ocn": info.gmslc_ocn,
+            "gmslc_ocnBeta": info.gmslc_ocnBeta,
+            "ice_volume": info.ice_volume,
+            "il": np.array(info.il[:]).reshape(3, 3),
+            "mm": np.array(info.mm[:]),
+            "lambda": lam[..., 0] + 1j * lam[..., 1],
+            "rates": None,
+            "wall": wall,
+            "xi": info.xi,
+            "prof": {"total": wall} if profile else None,
+        }
+        if isinstance(self, OptSeaLevelSolver):
+            scal["inner_stats"] = dict(self.inner_stats)
+        if profile:
+            self.prof = scal["prof"]
+        return _StepResult(self, scal)
+
+
+class OptSeaLevelSolver(SeaLevelSolver):
+    """GPU counterpart of the reference's ``OptSeaLevelSolver`` (solver_opt.py:267-360):
+    the ``opt`` set (``dsl``, ``diag`` change the work; ``numba``, ``sums`` are accepted) and
+    ``inner`` in {"off", "extrap"}."""
+
+    _opt_default = ()
+    _inner_default = "off"
+
+
+GpuSeaLevelSolver = SeaLevelSolver

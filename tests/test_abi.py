@@ -1,0 +1,127 @@
+"""CPU-side checks of the C ABI and the host wrappers (no GPU needed)."""
+
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+
+HEADER = os.path.join(REPO, "include", "slevolve_b200.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(sle_\w+)\s*\(", txt, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from slevolve_b200 import _lib
+
+    lib = _lib.lib()
+    assert lib.sle_abi_version() == 1
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [s for s in declared_symbols() if s not in exported]
+    assert not missing, missing
+    # the ctypes table binds exactly the declared entry points
+    assert set(_lib.exported_symbols()) <= set(declared_symbols())
+
+
+def test_error_mapping():
+    from slevolve_b200 import _lib
+
+    lib = _lib.lib()
+    # argument validation happens before any device call
+    import ctypes as C
+
+    h = C.c_void_p()
+    with pytest.raises(ValueError, match="nlat must be even"):
+        _lib.check(lib.sle_sht_create(15, 32, 15, C.byref(h)), "create")
+    with pytest.raises(ValueError, match="lmax must be <= nlon/2"):
+        _lib.check(lib.sle_sht_create(16, 32, 17, C.byref(h)), "create")
+    with pytest.raises(ValueError, match="power of two"):
+        _lib.check(lib.sle_sht_create(16, 48, 15, C.byref(h)), "create")
+
+
+def test_solver_rejects_unprovided_options():
+    from slevolve_b200 import OptSeaLevelSolver, SeaLevelSolver, SyntheticEarth
+
+    love = SyntheticEarth(15, 2, 1)
+    topo = np.full((16, 32), -1000.0)
+    ice = np.zeros((16, 32))
+    with pytest.raises(NotImplementedError):
+        SeaLevelSolver(None, love, topo, ice, norder=15, ramp=True)
+    with pytest.raises(NotImplementedError):
+        SeaLevelSolver(None, love, topo, ice, norder=15, axial_rotation="deg2")
+    with pytest.raises(NotImplementedError):
+        OptSeaLevelSolver(None, love, topo, ice, norder=15, inner="anderson")
+    with pytest.raises(ValueError):
+        OptSeaLevelSolver(None, love, topo, ice, norder=15, inner="bogus")
+    with pytest.raises(ValueError):
+        OptSeaLevelSolver(None, love, topo, ice, norder=15, opt={"raw"})
+    with pytest.raises(ValueError):
+        OptSeaLevelSolver(None, love, topo, ice, norder=15, opt={"fast"})
+
+
+def test_make_sht_unknown_backend():
+    from slevolve_b200 import make_sht
+
+    with pytest.raises(ValueError, match="unknown SHT backend"):
+        make_sht("numpy", 16, 32, 15)
+
+
+def test_degree_weights_match_oracle():
+    from oracle.solver import OracleSolver  # noqa: F401  (constants restated there)
+    from slevolve_b200.solver import Planet, degree_weights
+    from slevolve_b200 import SyntheticEarth
+
+    love = SyntheticEarth(31, 3, 5)
+    p = Planet()
+    ttl, tek, the = degree_weights(love, 31, p)
+    l = np.arange(32, dtype=np.float64)
+    ref = np.zeros(32)
+    ref[1:] = (4.0 * 3.1415926535898 * (p.radius ** 3)) / (p.mass * (2 * l[1:] + 1.0))
+    assert np.array_equal(ttl, ref)
+    assert np.array_equal(tek[1:], ref[1:] * (1 + love.ke[1:] - love.he[1:]))
+
+
+def test_love_reader_roundtrip(tmp_path):
+    """Write a small Love file in the reference's text format and read it back."""
+    from slevolve_b200 import LoveNumbers
+
+    lmax, K = 4, 3
+    rng = np.random.default_rng(3)
+    s = rng.uniform(0.1, 10, (K, lmax + 1))
+    lines = ["header"]
+    vals = {}
+    for l in range(1, lmax + 1):
+        lines.append(f"{l} {K}")
+        lines.append(" ".join(f"{x:.8E}" for x in s[:, l]))
+        el = rng.normal(size=5)
+        fl = rng.normal(size=5)
+        rh, rl, rk = (rng.normal(size=K) for _ in range(3))
+        vals[l] = (el, rh, rk)
+        lines.append(" ".join(f"{x:.8E}" for x in el))
+        lines.append(" ".join(f"{x:.8E}" for x in fl))
+        for r in (rh, rl, rk):
+            lines.append(" ".join(f"{x:.8E}" for x in r))
+        if l >= 2:
+            for _ in range(2):
+                lines.append(" ".join(f"{x:.8E}" for x in rng.normal(size=5)))
+            for _ in range(3):
+                lines.append(" ".join(f"{x:.8E}" for x in rng.normal(size=K)))
+    path = tmp_path / "love.txt"
+    path.write_text("\n".join(lines) + "\n")
+    L = LoveNumbers(str(path), lmax)
+    for l in range(1, lmax + 1):
+        el, rh, rk = vals[l]
+        assert np.allclose(L.s[:K, l], s[:, l], rtol=1e-8)
+        assert np.isclose(L.he[l], el[0], rtol=1e-8)
+        assert np.isclose(L.ke[l], el[4] / l, rtol=1e-8)
+        assert np.allclose(L.r[:K, l], rh, rtol=1e-8)
+        assert np.allclose(L.rprime[:K, l], rk / l, rtol=1e-8)
+    assert L.max_modes == K

@@ -1,0 +1,169 @@
+"""The CUDA time step against the reference's own outputs and the CPU oracle.
+
+Bar (the reference's own, tests/test_fortran_python.sh:37-47): topography and radial displacement
+within 1e-9 m at every compared step, identical inner-iteration counts, identical ocean and
+grounded-ice masks; degree-0 diagnostics within 1e-9 relative.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import FixtureLove, load_golden
+
+pytestmark = pytest.mark.gpu
+TOL_M = 1e-9
+
+
+def _unpack(bits, shape):
+    return np.unpackbits(bits)[: int(np.prod(shape))].reshape(shape) != 0
+
+
+def _check_against_fixture(slv, fx, prefix, ice_fn, nsteps):
+    numiter = []
+    for k in range(1, nsteps + 1):
+        r = slv.step(ice_fn(k))
+        numiter.append(r["numiter"])
+        if f"{prefix}tgrid_{k}" in fx:
+            dt = np.abs(r["tgrid"] - fx[f"{prefix}tgrid_{k}"]).max()
+            assert dt <= TOL_M, (k, dt)
+            if f"{prefix}R_{k}" in fx:
+                dr = np.abs(r["R"] - fx[f"{prefix}R_{k}"]).max()
+                assert dr <= TOL_M, (k, dr)
+            if f"{prefix}ocean_{k}" in fx:
+                assert np.array_equal(r["ocean"] != 0, _unpack(fx[f"{prefix}ocean_{k}"], r["ocean"].shape)), k
+                assert np.array_equal(r["beta"] != 0, _unpack(fx[f"{prefix}beta_{k}"], r["beta"].shape)), k
+        if f"{prefix}gmslc_ocn" in fx:
+            for key in ("gmslc_ocn", "gmslc_ocnBeta", "ocean_area", "oceanBeta_area", "ice_volume"):
+                ref = fx[f"{prefix}{key}"][k - 1]
+                assert abs(r[key] - ref) <= 1e-9 * max(1.0, abs(ref)), (k, key, r[key], ref)
+    assert numiter == list(fx[f"{prefix}numiter"]), numiter
+
+
+def test_c0_plain_100_steps():
+    from slevolve_b200 import SeaLevelSolver
+    from slevolve_b200.synthetic import case_c0
+    from oracle.sht import OracleSHT
+
+    fx = load_golden("step_c0.npz")
+    love = FixtureLove(fx)
+    topo = fx["topo_mm"] / 1000.0
+    case = case_c0(OracleSHT(64, 128, 63))
+    assert np.array_equal(case.topo, topo)
+    slv = SeaLevelSolver(None, love, topo, case.ice(0), norder=63, dt=1.0)
+    a0, b0, v0 = fx["plain_step0_scalars"]
+    assert abs(slv.ocean_area0 - a0) <= 1e-9 * abs(a0)
+    assert abs(slv.ice_volume0 - v0) <= 1e-9 * abs(v0)
+    _check_against_fixture(slv, fx, "plain_", case.ice, 100)
+
+
+def test_c0_extrap_dsl_100_steps():
+    from slevolve_b200 import OptSeaLevelSolver
+    from slevolve_b200.synthetic import case_c0
+    from oracle.sht import OracleSHT
+
+    fx = load_golden("step_c0.npz")
+    love = FixtureLove(fx)
+    topo = fx["topo_mm"] / 1000.0
+    case = case_c0(OracleSHT(64, 128, 63))
+    slv = OptSeaLevelSolver(None, love, topo, case.ice(0), norder=63, dt=1.0,
+                            opt={"numba", "sums", "dsl"}, inner="extrap")
+    _check_against_fixture(slv, fx, "extrap_", case.ice, 100)
+
+
+def test_marine_cap():
+    from slevolve_b200 import SeaLevelSolver
+    from tests_helpers import marine_ice
+    from oracle.sht import gauss_nodes
+
+    fx = load_golden("step_marine.npz")
+    love = FixtureLove(fx)
+    mu, _ = gauss_nodes(64)
+    ice = marine_ice(mu, 128, fx["ice_heights"])
+    slv = SeaLevelSolver(None, love, fx["topo"], ice[0], norder=63, dt=1000.0)
+    _check_against_fixture(slv, fx, "plain_", lambda k: ice[k], 8)
+
+
+def test_c1_small_grounding_line():
+    from slevolve_b200 import SeaLevelSolver
+    from slevolve_b200.synthetic import case_c1
+    from oracle.sht import OracleSHT
+
+    fx = load_golden("step_c1s.npz")
+    love = FixtureLove(fx)
+    case = case_c1(OracleSHT(64, 128, 63), nsteps=60)
+    slv = SeaLevelSolver(None, love, case.topo, case.ice(0), norder=63, dt=1.0)
+    _check_against_fixture(slv, fx, "plain_", case.ice, 60)
+    assert slv.gr_counts["ice_analyses"] > 0
+
+
+def test_reference_synthetic_512_golden():
+    """The reference's shipped L=511 golden grid (8 steps, --opt all --inner extrap)."""
+    from slevolve_b200 import OptSeaLevelSolver, make_sht
+    from tests_helpers import synthetic512_ice
+
+    fx = load_golden("synthetic512.npz")
+    love = FixtureLove(fx)
+    topo = fx["topo_mm"].astype(np.float64) / 1000.0
+    sht = make_sht("cuda", 512, 1024, 511)
+    ice = synthetic512_ice(sht.gaulats, topo, 1024, fx["polar"], fx["midlat"])
+    if "ice_abs_sums" in fx:
+        assert np.array_equal(np.array([float(np.abs(x).sum()) for x in ice]), fx["ice_abs_sums"])
+    slv = OptSeaLevelSolver(sht, love, topo, ice[0], norder=511, dt=1.0,
+                            opt={"numba", "sums", "dsl"}, inner="extrap")
+    ni = []
+    for k in range(1, 9):
+        r = slv.step(ice[k])
+        ni.append(r["numiter"])
+    tg = r["tgrid"]
+    assert ni == list(fx["numiter_doc"])
+    assert np.abs(tg[::8, ::8] - fx["tgrid8_sub"]).max() <= TOL_M
+    assert np.abs(tg.sum(axis=1) - fx["tgrid8_rowsum"]).max() <= 1024 * TOL_M
+    assert np.abs(tg.sum(axis=0) - fx["tgrid8_colsum"]).max() <= 512 * TOL_M
+
+
+@pytest.mark.parametrize("steps", [6])
+def test_c1_full_size_prefix_against_oracle(steps):
+    """c1 at its benchmark size (256 x 512, L = 255): the GPU step vs the CPU oracle."""
+    from slevolve_b200 import SeaLevelSolver
+    from slevolve_b200.synthetic import case_c1
+    from oracle.sht import OracleSHT
+    from oracle.solver import OracleSolver
+
+    osht = OracleSHT(256, 512, 255)
+    case = case_c1(osht, nsteps=550)
+    orc = OracleSolver(osht, case.love, case.topo, case.ice(0), norder=255, dt=1.0)
+    slv = SeaLevelSolver(None, case.love, case.topo, case.ice(0), norder=255, dt=1.0)
+    for k in range(1, steps + 1):
+        o = orc.step(case.ice(k))
+        r = slv.step(case.ice(k))
+        assert r["numiter"] == o["numiter"], k
+        assert np.abs(r["tgrid"] - o["tgrid"]).max() <= TOL_M, k
+        assert np.abs(r["R"] - o["R"]).max() <= TOL_M, k
+        assert np.array_equal(r["ocean"], o["ocean"]), k
+        assert np.array_equal(r["beta"], o["beta"]), k
+
+
+def test_nonfinite_ice_is_reported_not_faulted():
+    from slevolve_b200 import SeaLevelSolver, SyntheticEarth
+
+    love = SyntheticEarth(15, 3, 2)
+    topo = np.where(np.arange(32)[None, :] < 16, -1000.0, 500.0) * np.ones((16, 1))
+    slv = SeaLevelSolver(None, love, topo, np.zeros((16, 32)), norder=15)
+    bad = np.zeros((16, 32))
+    bad[3, 4] = np.nan
+    with pytest.raises(RuntimeError, match="non-finite"):
+        slv.step(bad)
+
+
+def test_nonconvergence_cap():
+    """epsilon1 < 0 can never be met: the device loop stops at 9999 iterations with an error."""
+    from slevolve_b200 import SeaLevelSolver, SyntheticEarth
+
+    love = SyntheticEarth(15, 3, 2)
+    topo = np.where(np.arange(32)[None, :] < 16, -1000.0, 500.0) * np.ones((16, 1))
+    ice = np.zeros((16, 32))
+    slv = SeaLevelSolver(None, love, topo, ice, norder=15, epsilon1=-1.0)
+    ice1 = ice.copy()
+    ice1[2:5, 20:24] = 100.0
+    with pytest.raises(RuntimeError, match="failed to converge"):
+        slv.step(ice1)
