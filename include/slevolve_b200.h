@@ -147,6 +147,20 @@ int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device);
 /* the solver's own CUDA stream (as void*) */
 int sle_solver_stream(sle_solver* s, void** stream);
 
+/* ------------------------------------------------------- measurement */
+/* Kernel classes timed by sle_prof_*: 0 row FFT + fold, 1 Legendre analysis, 2 Legendre
+ * synthesis, 3 inverse FFT + unfold, 4 modal-state advance.  Timing is off by default; when on,
+ * each launch of these classes is bracketed by CUDA events on its own stream. */
+int sle_prof_enable(int on);
+int sle_prof_collect(void);        /* wait for recorded events and accumulate */
+int sle_prof_reset(void);          /* also resets the launch counter */
+/* accumulated device milliseconds, launch count and fields processed ("units") of a class */
+int sle_prof_read(int cls, double* ms, long long* count, double* units);
+/* kernels launched by this library since the last sle_prof_reset() */
+long long sle_launch_count(void);
+/* FP64 FMA throughput of the current device (TFLOP/s), from a timed dependent-free FMA kernel */
+int sle_probe_fp64_tflops(double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,7 +82,15 @@ _SIGS = {
                                   C.POINTER(SleStepInfo)]),
     "sle_solver_get": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "sle_solver_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "sle_prof_enable": (C.c_int, [C.c_int]),
+    "sle_prof_collect": (C.c_int, []),
+    "sle_prof_reset": (C.c_int, []),
+    "sle_prof_read": (C.c_int, [C.c_int, _DP, C.POINTER(C.c_longlong), _DP]),
+    "sle_launch_count": (C.c_longlong, []),
+    "sle_probe_fp64_tflops": (C.c_int, [_DP]),
 }
+
+PROF_FFT, PROF_LEG_ANA, PROF_LEG_SYN, PROF_IFFT, PROF_ADVANCE = range(5)
 
 _lib = None
 

@@ -84,6 +84,18 @@ struct sle_sht {
 };
 
 namespace sle {
+// Launch accounting / per-kernel event timing (sle_prof.cu).
+enum ProfClass { PROF_FFT = 0, PROF_LEG_ANA = 1, PROF_LEG_SYN = 2, PROF_IFFT = 3, PROF_ADVANCE = 4,
+                 PROF_NCLS = 5 };
+struct ProfToken {
+  int cls;
+  double units;
+  void* a;
+};
+void note_launch(int n = 1);
+ProfToken prof_begin(int cls, double units, cudaStream_t st);
+void prof_end(const ProfToken& t, cudaStream_t st);
+
 // Launch helpers implemented in sle_sht.cu, used by the solver.
 int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, double2* const* out,
                         cudaStream_t st);

@@ -575,10 +575,15 @@ int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, doubl
     g.p[f] = grids[f];
     o.p[f] = out[f];
   }
+  ProfToken t0 = prof_begin(PROF_FFT, nf, st);
   k_fft_fold<<<d.nh, 256, fft_smem(d), st>>>(d, nf, g);
+  prof_end(t0, st);
   const int warps_per_block = 4;
   dim3 grid((d.nseg + warps_per_block - 1) / warps_per_block, nf);
+  ProfToken t1 = prof_begin(PROF_LEG_ANA, nf, st);
   k_leg_ana<<<grid, 32 * warps_per_block, 0, st>>>(d, o);
+  prof_end(t1, st);
+  note_launch(2);
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
 }
@@ -597,9 +602,14 @@ int sht_synthesis_packed(sle_sht* plan, int nf, const double2* const* coeffs, do
     g.p[f] = grids[f];
   }
   const int npairs = (d.nm + 1) / 2;
+  ProfToken t0 = prof_begin(PROF_LEG_SYN, nf, st);
   k_leg_syn<<<dim3(npairs, nf), 32 * d.ngrp, syn_smem(d), st>>>(d, c);
+  prof_end(t0, st);
   SynEpilogue e = epi ? *epi : SynEpilogue{nullptr, nullptr};
+  ProfToken t1 = prof_begin(PROF_IFFT, nf, st);
   k_ifft_unfold<<<d.nh, 256, fft_smem(d), st>>>(d, nf, g, e);
+  prof_end(t1, st);
+  note_launch(2);
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
 }
@@ -607,6 +617,7 @@ int sht_synthesis_packed(sle_sht* plan, int nf, const double2* const* coeffs, do
 int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t st) {
   const long long n = (long long)plan->d.nm * plan->d.nm;
   k_pack<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(plan->d, dense, packed);
+  note_launch();
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
 }
@@ -614,6 +625,7 @@ int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t 
 int sht_unpack(sle_sht* plan, const double2* packed, double2* dense, cudaStream_t st) {
   const long long n = (long long)plan->d.nm * plan->d.nm;
   k_unpack<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(plan->d, packed, dense);
+  note_launch();
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
 }

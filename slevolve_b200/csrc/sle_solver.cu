@@ -756,6 +756,7 @@ int sync_scal(sle_solver* s) {
 
 int check_finite(sle_solver* s, const double* dev, long long n, const char* what) {
   SLE_CUDA(cudaMemsetAsync(s->badflag, 0, sizeof(unsigned int), s->st));
+  note_launch();
   k_finite<<<nb(n), 256, 0, s->st>>>(n, dev, s->badflag);
   unsigned int bad = 0;
   SLE_CUDA(cudaMemcpyAsync(&bad, s->badflag, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->st));
@@ -769,6 +770,7 @@ int check_finite(sle_solver* s, const double* dev, long long n, const char* what
 
 int set_dt(sle_solver* s, double dt) {
   if (dt == s->dt_cur) return SLE_OK;
+  note_launch();
   k_set_decay<<<nb((long long)s->K * s->D.nl), 256, 0, s->st>>>(s->K, s->D.nl, s->s_kl, s->nmod, dt, s->decay,
                                                                s->omd);
   SLE_CUDA(cudaGetLastError());
@@ -985,6 +987,7 @@ extern "C" int sle_solver_init(sle_solver* s, const double* topo0, const double*
   SLE_TRY(upload(s->ice_prev, ice0, gb, on_device, st));
   SLE_TRY(check_finite(s, s->tinit, D.ng, "topography"));
   SLE_TRY(check_finite(s, s->ice_prev, D.ng, "initial ice"));
+  note_launch();
   k_init_grid<<<nb(D.ng), 256, 0, st>>>(D, s->tinit, s->ice_prev, s->cxy0, s->beta0, s->cstar0, s->cxy,
                                         s->topo_prev, s->icestar);
   SLE_CUDA(cudaGetLastError());
@@ -1051,9 +1054,14 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
   SLE_TRY(upload(s->ice, ice, sizeof(double) * ng, on_device, st));
 
   // ---- modal advance (solver.py:835)
+  note_launch();
+  ProfToken tadv = prof_begin(PROF_ADVANCE, 1, st);
   k_advance<<<nb(nc), 256, 0, st>>>(D, s->R, s->p_load, s->visc, s->rad);
+  prof_end(tadv, st);
+  note_launch();
   k_rot_advance<<<1, 1, 0, st>>>(D, s->sc, s->r_il, s->r_m, s->r_lam);
   // ---- ice and ocean grids, their analyses
+  note_launch();
   k_ice_grid<<<nb(ng), 256, 0, st>>>(D, s->ice, s->topo_prev, s->cxy, s->tinit, s->cstar0, s->icestar, s->beta,
                                      s->cstar, s->tO, s->ice_prev, it == 1 ? s->tmpg : nullptr, s->sc);
   SLE_CUDA(cudaGetLastError());
@@ -1078,6 +1086,7 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
     }
   }
   const unsigned red_blocks = std::min<unsigned>(RED_BLOCKS, nb(nc));
+  note_launch();
   k_pre_spec<<<red_blocks, 256, 0, st>>>(D, s->icelm, s->oldice, s->p_ice, s->cstarlm, s->p_ocean, s->h1, s->h2,
                                          mode, c1, c2, s->dice, s->dI, s->load, s->dScur, s->sc, s->partials,
                                          s->counter);
@@ -1090,16 +1099,20 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
       set_error("inner loop control lost (device iteration counter did not advance)");
       return SLE_ERR_STATE;
     }
+    note_launch();
     k_b18<<<nb(nc), 256, 0, st>>>(D, s->C, s->dI, s->p_ocean, s->load, s->visc, s->dScur, s->sl, s->sc);
     SynEpilogue epi{s->rO, s->cstar};
     SLE_TRY(syn(s, s->sl, s->dsl, &epi));
     SLE_TRY(ana(s, 1, s->rO, s->rOlm));
+    note_launch();
     k_update<<<red_blocks, 256, 0, st>>>(D, s->p_ocean, s->rOlm, s->cstarlm, s->tOlm, s->dI, s->load, s->dScur,
                                          s->sc, s->partials, s->counter);
     if (!s->cfg.opt_dsl) {
+      note_launch();
       k_sltot<<<nb(nc), 256, 0, st>>>(D, s->sl, s->sltot, s->sc);
       SLE_TRY(syn(s, s->sltot, s->deltasl));
     }
+    note_launch();
     k_refresh1<<<red_grid, 256, 0, st>>>(D, s->dsl, s->deltasl, s->tinit, s->topo, s->cxy, s->ice, s->beta,
                                          s->grnew, s->sc, s->partials + 2048, s->counter + 1);
     SLE_CUDA(cudaGetLastError());
@@ -1107,10 +1120,12 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
     const Scal& h = *s->hsc;
     if (h.converged || h.status != 0) break;
     const int changed = h.gr_changed;
+    note_launch();
     k_refresh2<<<nb(ng), 256, 0, st>>>(D, s->cxy, s->tinit, s->cstar0, s->grnew, s->icestar, s->beta, s->cstar,
                                        s->tO, changed);
     if (changed) {
       SLE_TRY(ana(s, 3, s->icestar, s->icelm, s->cstar, s->cstarlm, s->tO, s->tOlm));
+      note_launch();
       k_dice<<<nb(nc), 256, 0, st>>>(D, s->icelm, s->oldice, s->p_ice, s->dice, s->dI);
       SLE_CUDA(cudaMemsetAsync(&s->sc->gr_changed, 0, sizeof(int), st));
     } else {
@@ -1130,13 +1145,16 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
 
   // ---- radial displacement (solver.py:1054-1072)
   if (s->cfg.calcRG) {
+    note_launch();
     k_rr<<<nb(nc), 256, 0, st>>>(D, s->dI, s->p_ocean, s->load, s->rad, s->rrlm, s->sc);
     SLE_TRY(syn(s, s->rrlm, s->rr));
   }
   // ---- commit (solver.py:1080-1096); extrap history (solver_opt.py:817-822)
   double2* hist_new = s->cfg.inner_extrap ? s->h2 : nullptr;
+  note_launch();
   k_commit<<<nb(nc), 256, 0, st>>>(D, s->dice, s->load, s->dI, s->dScur, s->icelm, s->p_load, s->p_ice, s->p_ocean,
                                    s->prev_ice, hist_new);
+  if (D.tpw) note_launch();
   if (D.tpw) k_rot_commit<<<1, 1, 0, st>>>(s->sc);
   if (s->cfg.inner_extrap) {
     double2* t = s->h1;
@@ -1148,10 +1166,13 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
   }
   // ---- topography / ocean function and the degree-0 diagnostics
   if (s->cfg.opt_diag) {
+    note_launch();
     k_post_grid<<<D.nlat, 256, 0, st>>>(D, s->tinit, s->deltasl, s->beta, s->topo, s->topo_prev, s->cxy, nullptr,
                                         nullptr, nullptr, s->rows);
+    note_launch();
     k_degree0<<<1, 256, 0, st>>>(D, s->rows, s->plan->d.w, s->sc);
   } else {
+    note_launch();
     k_post_grid<<<D.nlat, 256, 0, st>>>(D, s->tinit, s->deltasl, s->beta, s->topo, s->topo_prev, s->cxy, s->tmpg,
                                         s->gbuf3, s->gbuf4, nullptr);
     SLE_TRY(ana(s, 4, s->tmpg, s->spare[0], s->cxy, s->spare[1], s->gbuf3, s->spare[2], s->gbuf4, s->spare[3]));
@@ -1225,6 +1246,7 @@ extern "C" int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_de
     case SLE_F_OCEAN0: src = s->cxy0; break;
     case SLE_F_BETA0: src = s->beta0; break;
     case SLE_F_G:
+      note_launch();
       k_grid_add<<<nb(D.ng), 256, 0, s->st>>>(D.ng, s->deltasl, s->rr, s->tmpg);
       SLE_CUDA(cudaGetLastError());
       src = s->tmpg;

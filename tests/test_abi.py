@@ -14,7 +14,7 @@ HEADER = os.path.join(REPO, "include", "slevolve_b200.h")
 
 def declared_symbols():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(sle_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|const char\*)\s+(sle_\w+)\s*\(", txt, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
