@@ -70,6 +70,17 @@ int sle_sht_analysis(sle_sht* plan, int nfields, const double* const* grids_dev,
 /* sht.py:305-343.  Im of the m = 0 coefficients is ignored (irfft semantics). */
 int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* coeffs_dev, int layout,
                       double* const* grids_dev, void* stream);
+/* Analysis of one grid into packed coefficients without any device allocation.  No counterpart
+ * in the reference.  For hosts that reserve the GPU's memory for their own allocator and do not
+ * let a library call cudaMalloc once they run: they create the plan while setting up and then
+ * analyse through this call, whose scratch is a 4 MiB array compiled into this library (held by
+ * every GPU that loads it, until exit) instead of memory from cudaMalloc.  Limits: at most 512
+ * latitudes and lmax 511, else SLE_ERR_BAD_SHAPE.  The first call on a device looks up the
+ * array's device address and should come before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other threads) race and must be ordered
+ * by the caller. */
+int sle_sht_analysis_noalloc(sle_sht* plan, const double* grid_dev, void* coeffs_packed_dev,
+                             void* stream);
 /* dense <-> packed conversion of one complex128 spectrum (device buffers) */
 int sle_sht_pack(sle_sht* plan, const void* dense_dev, void* packed_dev, void* stream);
 int sle_sht_unpack(sle_sht* plan, const void* packed_dev, void* dense_dev, void* stream);

@@ -72,6 +72,7 @@ _SIGS = {
                                    C.c_void_p]),
     "sle_sht_synthesis": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                     C.c_void_p]),
+    "sle_sht_analysis_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_sht_pack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_sht_unpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_solver_create": (C.c_int, [C.POINTER(SleConfig), C.POINTER(SleEarth),

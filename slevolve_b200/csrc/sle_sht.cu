@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
@@ -784,10 +785,26 @@ static int plan_build(sle_sht* p, int nlat, int nlon, int lmax) {
   return SLE_OK;
 }
 
+// ------------------------------------------------------------ allocation-free analysis
+// Scratch of sle_sht_analysis_noalloc: the folded row FFT (S and D) of one field for grids of
+// up to 512 latitudes and lmax up to 511, 2 x 512 x 256 complex128 = 4 MiB.  It is part of the
+// module image, so every GPU that loads this library holds it until the process exits.
+constexpr int NOALLOC_MAX_NM = 512;
+constexpr int NOALLOC_MAX_NH = 256;
+static __device__ __align__(256) double2 g_noalloc_fold[2 * NOALLOC_MAX_NM * NOALLOC_MAX_NH];
+
 }  // namespace sle
 
 // ============================================================================ C ABI
 using namespace sle;
+
+namespace {
+// Device address of g_noalloc_fold per device, looked up once per device (the host-side name of
+// a __device__ array is not a device address and must never be passed to a kernel).
+std::mutex g_noalloc_mu;
+constexpr int NOALLOC_MAX_DEVICES = 128;
+double2* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+}  // namespace
 
 extern "C" int sle_abi_version(void) { return SLE_ABI_VERSION; }
 extern "C" const char* sle_last_error(void) { return g_err; }
@@ -935,4 +952,56 @@ extern "C" int sle_sht_unpack(sle_sht* plan, const void* packed_dev, void* dense
   }
   return sht_unpack(plan, reinterpret_cast<const double2*>(packed_dev), reinterpret_cast<double2*>(dense_dev),
                     reinterpret_cast<cudaStream_t>(stream));
+}
+
+// One analysis (one field, packed output) whose scratch is the fixed array g_noalloc_fold instead
+// of memory from cudaMalloc.  The call launches the same two kernels as sle_sht_analysis; the
+// first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
+// device current.  No element of the scratch needs clearing: every element the second kernel
+// reads is written earlier in the same call by the first.
+extern "C" int sle_sht_analysis_noalloc(sle_sht* plan, const double* grid_dev, void* coeffs_packed_dev,
+                                        void* stream) {
+  if (!plan) {
+    set_error("sle_sht_analysis_noalloc: NULL plan");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (!aligned16(grid_dev) || !aligned16(coeffs_packed_dev)) {
+    set_error("sle_sht_analysis_noalloc: device buffers must be non-NULL and 16-byte aligned");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (plan->d.nm > NOALLOC_MAX_NM || plan->d.nh > NOALLOC_MAX_NH) {
+    set_error("sle_sht_analysis_noalloc: grid %d x %d with lmax %d exceeds the fixed scratch "
+              "(at most 512 latitudes and lmax 511); use sle_sht_analysis",
+              plan->d.nlat, plan->d.nlon, plan->d.lmax);
+    return SLE_ERR_BAD_SHAPE;
+  }
+  int dev = -1;
+  SLE_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+    set_error("sle_sht_analysis_noalloc: device ordinal %d out of range", dev);
+    return SLE_ERR_BAD_ARG;
+  }
+  double2* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      SLE_CUDA(cudaGetSymbolAddress(&p, g_noalloc_fold));
+      g_noalloc_addr[dev] = reinterpret_cast<double2*>(p);
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  ShtDev d = plan->d;
+  d.X = scratch;
+  GridPtrs g{};
+  g.p[0] = grid_dev;
+  SpecPtrs o{};
+  o.p[0] = reinterpret_cast<double2*>(coeffs_packed_dev);
+  k_fft_fold<<<d.nh, 256, fft_smem(d), st>>>(d, 1, g);
+  const int warps_per_block = 4;
+  k_leg_ana<<<dim3((d.nseg + warps_per_block - 1) / warps_per_block, 1), 32 * warps_per_block, 0, st>>>(d, o);
+  SLE_CUDA(cudaGetLastError());
+  note_launch(2);
+  return SLE_OK;
 }
