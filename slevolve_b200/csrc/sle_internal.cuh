@@ -60,6 +60,24 @@ struct ShtDev {
   const double2* tw;          // [n2] exp(-2 pi i t / nlon)
   double2* X;                 // [MAXF][2][nm][nh] folded rFFT (S then D) of analysed grids
   double2* EO;                // [MAXF][2][nm][nh] even/odd Legendre sums of synthesised fields
+  // Optional per-field gates of an analysis launch (device flags read at kernel entry): field f
+  // is skipped when bit f of gate_conv_mask is set and *gate_conv != 0, or when bit f of
+  // gate_chg_mask is set and *gate_chg == 0.
+  const int* gate_conv;
+  const int* gate_chg;
+  unsigned gate_conv_mask, gate_chg_mask;
+};
+
+__device__ __forceinline__ bool field_gated_off(const ShtDev& P, int f) {
+  if (((P.gate_conv_mask >> f) & 1u) && *P.gate_conv != 0) return true;
+  if (((P.gate_chg_mask >> f) & 1u) && *P.gate_chg == 0) return true;
+  return false;
+}
+
+struct AnaGate {
+  const int* conv;
+  const int* chg;
+  unsigned conv_mask, chg_mask;
 };
 
 // Epilogue of the inverse-FFT kernel: out2 = g * mul2 (e.g. rO = dsl * C*).
@@ -93,12 +111,13 @@ struct ProfToken {
   void* a;
 };
 void note_launch(int n = 1);
+bool prof_enabled();
 ProfToken prof_begin(int cls, double units, cudaStream_t st);
 void prof_end(const ProfToken& t, cudaStream_t st);
 
 // Launch helpers implemented in sle_sht.cu, used by the solver.
 int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, double2* const* out,
-                        cudaStream_t st);
+                        cudaStream_t st, const AnaGate* gate = nullptr);
 int sht_synthesis_packed(sle_sht* plan, int nf, const double2* const* coeffs, double* const* grids,
                          const SynEpilogue* epi, cudaStream_t st);
 int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t st);

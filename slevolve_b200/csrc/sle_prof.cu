@@ -42,11 +42,17 @@ cudaEvent_t take_event() {
 }
 }  // namespace
 
-void note_launch(int n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+bool prof_enabled() { return g_prof.enabled; }
+
+void note_launch(int n) {
+  __atomic_fetch_add(&g_launches, (unsigned long long)(long long)n, __ATOMIC_RELAXED);
+}
 
 ProfToken prof_begin(int cls, double units, cudaStream_t st) {
   ProfToken t{cls, units, nullptr};
   if (!g_prof.enabled) return t;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return t;
   std::lock_guard<std::mutex> lk(g_prof.mu);
   t.a = take_event();
   cudaEventRecord(reinterpret_cast<cudaEvent_t>(t.a), st);

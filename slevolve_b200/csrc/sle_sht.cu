@@ -101,8 +101,12 @@ __global__ void k_gauss_nodes(int n, double tol, double* mu, double* w, int* fai
   w[i] = __ddiv_rn(2.0, __dmul_rn(__dmul_rn(__dsub_rn(1.0, __dmul_rn(zfin, zfin)), ppfin), ppfin));
 }
 
-// Seeds (Q_l0, Q_l0+1) of every (segment, latitude) and the per-(segment, group) maximum of
-// |P~|.  P~ follows the reference LEGEND recursion (sht.py:105-144) operation by operation.
+// Seeds of every (segment, latitude) and the per-(segment, group) maximum of |P~|.  P~ follows
+// the reference LEGEND recursion (sht.py:105-144) operation by operation.  A segment starting at
+// degree l0 > m stores (Q_{l0-2}, Q_{l0-1}) in its own scale (P~_l = cf_l Q_l with cf_l0 = 1,
+// so Q_{l0-1} = P~_{l0-1} / eps_l0 and Q_{l0-2} = P~_{l0-2} / (eps_l0 eps_{l0-1})); the first
+// segment (l0 = m) stores (P~_mm, 0) and uses be_m = 1.  Every degree of every segment then
+// follows the same update Q_l = mu Q_{l-1} + be_l Q_{l-2}.
 __global__ void k_legendre_tables(sle::ShtDev P, double2* seeds, double* segmax) {
   const int m = blockIdx.x, g = blockIdx.y, lane = threadIdx.x;
   const int j = g * 32 + lane;
@@ -121,9 +125,8 @@ __global__ void k_legendre_tables(sle::ShtDev P, double2* seeds, double* segmax)
   const int np1 = m + 1;
   const double eps_m1 = __dsqrt_rn(__ddiv_rn((double)(np1 * np1 - m * m), (double)(4 * np1 * np1 - 1)));
   double t = __dsub_rn(__dmul_rn(x, pm1), __dmul_rn(eps_m1, pmm));  // x P_{n-1} - eps_{n-1} P_{n-2}
-  double prev1 = 0.0;
+  double prev1 = 0.0, prev2 = 0.0, eps_prev = 0.0;
   double smax = 0.0;
-  double2 seed = make_double2(0.0, 0.0);
   int seg = P.segoff[m];
   for (int l = m; l <= L; ++l) {
     double pl, eps_l;
@@ -139,24 +142,31 @@ __global__ void k_legendre_tables(sle::ShtDev P, double2* seeds, double* segmax)
       t = __dsub_rn(__dmul_rn(x, pl), __dmul_rn(eps_l, prev1));
     }
     const int r = (l - m) % SEG;
-    if (r == 0) seed.x = pl;
-    if (r == 1) seed.y = __dmul_rn(pl, eps_l);
+    if (r == 0 && ok) {
+      double2 sd;
+      if (l == m) {
+        sd = make_double2(pmm, 0.0);
+      } else {
+        sd = make_double2(__ddiv_rn(prev2, __dmul_rn(eps_l, eps_prev)), __ddiv_rn(prev1, eps_l));
+      }
+      seeds[(size_t)seg * P.nh + j] = sd;
+    }
     smax = fmax(smax, ok ? fabs(pl) : 0.0);
     if (r == SEG - 1 || l == L) {
       double v = smax;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-      if (ok) seeds[(size_t)seg * P.nh + j] = seed;
       if (lane == 0) segmax[(size_t)seg * P.ngrp + g] = v;
-      seed = make_double2(0.0, 0.0);
       smax = 0.0;
       ++seg;
     }
+    prev2 = prev1;
     prev1 = pl;
+    eps_prev = eps_l;
   }
 }
 
-// Recurrence coefficients in segment scale: cf (P~ = cf Q) and be = -eps_{l-1}^2.
+// Recurrence coefficients in segment scale: cf (P~ = cf Q) and be_l = -eps_{l-1}^2 (be_m = 1).
 __global__ void k_legendre_coef(sle::ShtDev P, double* be, double* cf) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= P.nseg) return;
@@ -165,7 +175,12 @@ __global__ void k_legendre_coef(sle::ShtDev P, double* be, double* cf) {
   const long long base = P.moff[m] + (l0 - m);
   double c = 1.0;
   cf[base] = 1.0;
-  be[base] = 0.0;
+  if (l0 == m) {
+    be[base] = 1.0;  // Q_m = be_m * P~_mm with the first segment's seeds (P~_mm, 0)
+  } else {
+    const int k = l0 - 1;
+    be[base] = -__ddiv_rn((double)(k * k - m * m), (double)(4 * k * k - 1));
+  }
   for (int l = l0 + 1; l < l1; ++l) {
     const double eps = __dsqrt_rn(__ddiv_rn((double)(l * l - m * m), (double)(4 * l * l - 1)));
     c = __ddiv_rn(c, eps);
@@ -190,35 +205,100 @@ __global__ void k_lidx(sle::ShtDev P, int* lidx) {
 }
 
 // ----------------------------------------------------------------------------- FFTs
-// Radix-2 Stockham FFT of `rows` length-n2 sequences laid out back to back in A (B is
-// scratch).  tw[t] = exp(-2 pi i t / (2 n2)); the stage twiddle exp(-+2 pi i k / (2 Ns)) is
-// tw[k n2 / Ns].  Returns the buffer holding the result.
-__device__ double2* stockham(double2* A, double2* B, int n2, int log2n2, int rows,
-                             const double2* tw, bool inverse) {
-  const int half = n2 >> 1;
-  const int tot = rows * half;
-  for (int st = 0; st < log2n2; ++st) {
-    const int Ns = 1 << st;
-    const int tws = n2 >> st;
-    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
-      const int r = idx >> (log2n2 - 1);
-      const int jj = idx & (half - 1);
-      const int k = jj & (Ns - 1);
-      const double2 a = A[r * n2 + jj];
-      const double2 b = A[r * n2 + jj + half];
-      double2 w = tw[k * tws];
-      if (inverse) w.y = -w.y;
-      const double2 bw = cmul(b, w);
-      const int d = ((jj - k) << 1) + k;
-      B[r * n2 + d] = cadd(a, bw);
-      B[r * n2 + d + Ns] = csub(a, bw);
+// Stockham FFT of length n2 = nlon/2 on complex rows in shared memory: radix-8 passes while at
+// least 8 points remain per sub-transform, then one radix-4 or radix-2 pass.  A pass of radix R
+// with current sub-transform size Ns maps in[j + r q] (q = n2/R, k = j mod Ns) through the
+// twiddles exp(-+2 pi i r k/(Ns R)) and an R-point DFT in registers to
+// out[(j - k) R + k + r Ns].  tw[t] = exp(-2 pi i t / (2 n2)) for t < n2; larger t use
+// tw[t - n2] = -exp(...).
+__device__ __forceinline__ double2 twiddle(const double2* tw, int n2, int t, bool inv) {
+  double2 w = (t < n2) ? tw[t] : make_double2(-tw[t - n2].x, -tw[t - n2].y);
+  if (inv) w.y = -w.y;
+  return w;
+}
+
+__device__ __forceinline__ double2 mul_mi(double2 a, bool inv) {  // a * (-i), or a * (+i) when inv
+  return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+__device__ __forceinline__ void dft8(double2 (&v)[8], bool inv) {
+  const double h = 0.70710678118654752440;  // cos(pi/4)
+  double2 a0 = cadd(v[0], v[4]), a4 = csub(v[0], v[4]);
+  double2 a1 = cadd(v[1], v[5]), a5 = csub(v[1], v[5]);
+  double2 a2 = cadd(v[2], v[6]), a6 = csub(v[2], v[6]);
+  double2 a3 = cadd(v[3], v[7]), a7 = csub(v[3], v[7]);
+  // a5 *= W, a6 *= W^2, a7 *= W^3 with W = exp(-+2 pi i / 8)
+  const double s = inv ? h : -h;
+  a5 = make_double2(h * a5.x - s * a5.y, h * a5.y + s * a5.x);
+  a6 = mul_mi(a6, inv);
+  a7 = make_double2(-h * a7.x - s * a7.y, -h * a7.y + s * a7.x);
+  double2 b0 = cadd(a0, a2), b2 = csub(a0, a2), b1 = cadd(a1, a3), b3 = mul_mi(csub(a1, a3), inv);
+  double2 b4 = cadd(a4, a6), b6 = csub(a4, a6), b5 = cadd(a5, a7), b7 = mul_mi(csub(a5, a7), inv);
+  v[0] = cadd(b0, b1);
+  v[1] = cadd(b4, b5);
+  v[2] = cadd(b2, b3);
+  v[3] = cadd(b6, b7);
+  v[4] = csub(b0, b1);
+  v[5] = csub(b4, b5);
+  v[6] = csub(b2, b3);
+  v[7] = csub(b6, b7);
+}
+
+// One Stockham pass of radix R on two rows of N points (compile-time sizes: all index
+// arithmetic folds to shifts and masks).  Sub-transform size before the pass: NS.
+template <int N, int R, int NS, bool INV>
+__device__ __forceinline__ void fft_pass_c(const double2* __restrict__ in, double2* __restrict__ out,
+                                           const double2* __restrict__ tw) {
+  constexpr int Q = N / R;
+  constexpr int TSTEP = 2 * N / (NS * R);
+  for (int idx = threadIdx.x; idx < 2 * Q; idx += blockDim.x) {
+    const int r = idx / Q, j = idx % Q;
+    const int k = j % NS;
+    const double2* src = in + r * N;
+    double2 v[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) v[u] = src[j + u * Q];
+    if (NS > 1) {
+#pragma unroll
+      for (int u = 1; u < R; ++u) {
+        const int t = u * k * TSTEP;
+        double2 w = (t < N) ? tw[t] : make_double2(-tw[t - N].x, -tw[t - N].y);
+        if (INV) w.y = -w.y;
+        v[u] = cmul(v[u], w);
+      }
     }
-    __syncthreads();
-    double2* tmp = A;
-    A = B;
-    B = tmp;
+    if (R == 8) {
+      dft8(reinterpret_cast<double2(&)[8]>(v), INV);
+    } else if (R == 4) {
+      const double2 a0 = cadd(v[0], v[2]), a2 = csub(v[0], v[2]);
+      const double2 a1 = cadd(v[1], v[3]), a3 = mul_mi(csub(v[1], v[3]), INV);
+      v[0] = cadd(a0, a1);
+      v[1] = cadd(a2, a3);
+      v[2] = csub(a0, a1);
+      v[3] = csub(a2, a3);
+    } else {
+      const double2 a0 = cadd(v[0], v[1]), a1 = csub(v[0], v[1]);
+      v[0] = a0;
+      v[1] = a1;
+    }
+    double2* dst = out + r * N + (j - k) * R + k;
+#pragma unroll
+    for (int u = 0; u < R; ++u) dst[u * NS] = v[u];
   }
-  return A;
+}
+
+// Radix-8 passes while at least 8 points remain per sub-transform, then one radix-4 or 2 pass.
+template <int N, int NS, bool INV>
+__device__ __forceinline__ double2* stockham_c(double2* A, double2* B, const double2* tw) {
+  if constexpr (NS >= N) {
+    return A;
+  } else {
+    constexpr int REM = N / NS;
+    constexpr int R = (REM >= 8) ? 8 : REM;
+    fft_pass_c<N, R, NS, INV>(A, B, tw);
+    __syncthreads();
+    return stockham_c<N, NS * R, INV>(B, A, tw);
+  }
 }
 
 struct GridPtrs {
@@ -234,140 +314,199 @@ struct CSpecPtrs {
   const double2* p[MAXF];
 };
 
-// Row rFFT of the north row j and south row nlat-1-j of every field, then the fold
+// Row rFFT of the north row j and south row nlat-1-j of field blockIdx.y, then the fold
 // S = F_N w_j/nlon + F_S w_j/nlon, D = F_N w_j/nlon - F_S w_j/nlon for m <= lmax
-// (sht.py:277-287).  X layout [f][0=S,1=D][m][j].
-__global__ void __launch_bounds__(256) k_fft_fold(sle::ShtDev P, int nf, GridPtrs g) {
+// (sht.py:277-287).  X layout [f][0=S,1=D][m][j].  N = nlon/2 complex points per row.
+template <int N>
+__global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fft_fold(sle::ShtDev P, GridPtrs g) {
   extern __shared__ double2 sm[];
-  const int n2 = P.n2;
   double2* tw = sm;
-  double2* A = sm + n2;
-  double2* B = A + 2 * n2;
-  for (int t = threadIdx.x; t < n2; t += blockDim.x) tw[t] = P.tw[t];
-  const int j = blockIdx.x;
+  double2* A = sm + N;
+  double2* B = A + 2 * N;
+  const int j = blockIdx.x, f = blockIdx.y;
+  if (field_gated_off(P, f)) return;
   const int js = P.nlat - 1 - j;
+  const double2* rn = reinterpret_cast<const double2*>(g.p[f] + (size_t)j * (2 * N));
+  const double2* rs = reinterpret_cast<const double2*>(g.p[f] + (size_t)js * (2 * N));
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    tw[t] = P.tw[t];
+    A[t] = rn[t];
+    A[N + t] = rs[t];
+  }
+  __syncthreads();
+  const double2* Z = stockham_c<N, 1, false>(A, B, tw);
   const double wn = P.wn[j], ws = P.ws[j];
-  for (int f = 0; f < nf; ++f) {
-    const double2* rn = reinterpret_cast<const double2*>(g.p[f] + (size_t)j * P.nlon);
-    const double2* rs = reinterpret_cast<const double2*>(g.p[f] + (size_t)js * P.nlon);
-    for (int t = threadIdx.x; t < n2; t += blockDim.x) {
-      A[t] = rn[t];
-      A[n2 + t] = rs[t];
-    }
-    __syncthreads();
-    const double2* Z = stockham(A, B, n2, P.log2n2, 2, tw, false);
-    double2* XS = P.X + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
-    double2* XD = P.X + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
-    for (int m = threadIdx.x; m < P.nm; m += blockDim.x) {
-      double2 xr[2];
+  double2* XS = P.X + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
+  double2* XD = P.X + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
+  for (int m = threadIdx.x; m < P.nm; m += blockDim.x) {
+    double2 xr[2];
 #pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const double2* z = Z + r * n2;
-        if (m == 0) {
-          xr[r] = make_double2(z[0].x + z[0].y, 0.0);
-        } else if (m == n2) {
-          xr[r] = make_double2(z[0].x - z[0].y, 0.0);
-        } else {
-          const double2 zm = z[m];
-          const double2 zc = make_double2(z[n2 - m].x, -z[n2 - m].y);
-          const double2 e = cscale(cadd(zm, zc), 0.5);
-          const double2 dz = csub(zm, zc);
-          const double2 o = make_double2(0.5 * dz.y, -0.5 * dz.x);  // (zm - zc) / (2i)
-          xr[r] = cadd(e, cmul(tw[m], o));
-        }
+    for (int r = 0; r < 2; ++r) {
+      const double2* z = Z + r * N;
+      if (m == 0) {
+        xr[r] = make_double2(z[0].x + z[0].y, 0.0);
+      } else if (m == N) {
+        xr[r] = make_double2(z[0].x - z[0].y, 0.0);
+      } else {
+        const double2 zm = z[m];
+        const double2 zc = make_double2(z[N - m].x, -z[N - m].y);
+        const double2 e = cscale(cadd(zm, zc), 0.5);
+        const double2 dz = csub(zm, zc);
+        const double2 o = make_double2(0.5 * dz.y, -0.5 * dz.x);  // (zm - zc) / (2i)
+        xr[r] = cadd(e, cmul(tw[m], o));
       }
-      const double2 a = cscale(xr[0], wn);
-      const double2 b = cscale(xr[1], ws);
-      XS[(size_t)m * P.nh + j] = cadd(a, b);
-      XD[(size_t)m * P.nh + j] = csub(a, b);
     }
-    __syncthreads();
+    const double2 a = cscale(xr[0], wn);
+    const double2 b = cscale(xr[1], ws);
+    XS[(size_t)m * P.nh + j] = cadd(a, b);
+    XD[(size_t)m * P.nh + j] = csub(a, b);
   }
 }
 
 // Inverse: north spectrum E + O, south E - O (m <= lmax, 0 above), unnormalised inverse
-// real FFT of both rows (sht.py:330-339 with the nlon scaling folded out).
-__global__ void __launch_bounds__(256) k_ifft_unfold(sle::ShtDev P, int nf, OutGridPtrs g,
-                                                     SynEpilogue epi) {
+// real FFT of both rows (sht.py:330-339 with the nlon scaling folded out); field blockIdx.y.
+template <int N>
+__global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_ifft_unfold(sle::ShtDev P, OutGridPtrs g,
+                                                                          SynEpilogue epi) {
   extern __shared__ double2 sm[];
   __shared__ double2 nyq[2];
-  const int n2 = P.n2;
   double2* tw = sm;
-  double2* A = sm + n2;
-  double2* B = A + 2 * n2;
-  for (int t = threadIdx.x; t < n2; t += blockDim.x) tw[t] = P.tw[t];
-  const int j = blockIdx.x;
+  double2* A = sm + N;
+  double2* B = A + 2 * N;
+  const int j = blockIdx.x, f = blockIdx.y;
   const int js = P.nlat - 1 - j;
-  for (int f = 0; f < nf; ++f) {
-    const double2* E = P.EO + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
-    const double2* O = P.EO + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
-    // stage G into B (rows north, south); G[n2] (Nyquist, only when lmax == n2) in nyq
-    for (int m = threadIdx.x; m <= n2; m += blockDim.x) {
-      double2 gn = make_double2(0.0, 0.0), gs = gn;
-      if (m < P.nm) {
-        const double2 e = E[(size_t)m * P.nh + j];
-        const double2 o = O[(size_t)m * P.nh + j];
-        gn = cadd(e, o);
-        gs = csub(e, o);
-      }
-      if (m < n2) {
-        B[m] = gn;
-        B[n2 + m] = gs;
-      } else {
-        nyq[0] = gn;
-        nyq[1] = gs;
-      }
+  const double2* E = P.EO + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
+  const double2* O = P.EO + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = P.tw[t];
+  // stage G into B (rows north, south); G[N] (Nyquist, only when lmax == N) in nyq
+  for (int m = threadIdx.x; m <= N; m += blockDim.x) {
+    double2 gn = make_double2(0.0, 0.0), gs = gn;
+    if (m < P.nm) {
+      const double2 e = E[(size_t)m * P.nh + j];
+      const double2 o = O[(size_t)m * P.nh + j];
+      gn = cadd(e, o);
+      gs = csub(e, o);
     }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < 2 * n2; idx += blockDim.x) {
-      const int r = idx / n2;
-      const int m = idx - r * n2;
-      double2 a, b;
-      if (m == 0) {
-        a = make_double2(B[r * n2].x, 0.0);
-        b = make_double2(nyq[r].x, 0.0);
-      } else {
-        a = B[r * n2 + m];
-        const double2 c = B[r * n2 + n2 - m];
-        b = make_double2(c.x, -c.y);
-      }
-      const double2 e = cadd(a, b);
-      const double2 wc = make_double2(tw[m].x, -tw[m].y);  // exp(+2 pi i m / nlon)
-      const double2 o = cmul(csub(a, b), wc);
-      A[r * n2 + m] = make_double2(e.x - o.y, e.y + o.x);  // e + i o
+    if (m < N) {
+      B[m] = gn;
+      B[N + m] = gs;
+    } else {
+      nyq[0] = gn;
+      nyq[1] = gs;
     }
-    __syncthreads();
-    const double2* Z = stockham(A, B, n2, P.log2n2, 2, tw, true);
-    double2* rn = reinterpret_cast<double2*>(g.p[f] + (size_t)j * P.nlon);
-    double2* rs = reinterpret_cast<double2*>(g.p[f] + (size_t)js * P.nlon);
-    for (int t = threadIdx.x; t < n2; t += blockDim.x) {
-      const double2 vn = Z[t], vs = Z[n2 + t];
-      rn[t] = vn;
-      rs[t] = vs;
-      if (f == 0 && epi.out2) {
-        const double2 mn = reinterpret_cast<const double2*>(epi.mul2 + (size_t)j * P.nlon)[t];
-        const double2 ms = reinterpret_cast<const double2*>(epi.mul2 + (size_t)js * P.nlon)[t];
-        reinterpret_cast<double2*>(epi.out2 + (size_t)j * P.nlon)[t] = make_double2(vn.x * mn.x, vn.y * mn.y);
-        reinterpret_cast<double2*>(epi.out2 + (size_t)js * P.nlon)[t] = make_double2(vs.x * ms.x, vs.y * ms.y);
-      }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 2 * N; idx += blockDim.x) {
+    const int r = idx / N;
+    const int m = idx % N;
+    double2 a, b;
+    if (m == 0) {
+      a = make_double2(B[r * N].x, 0.0);
+      b = make_double2(nyq[r].x, 0.0);
+    } else {
+      a = B[r * N + m];
+      const double2 c = B[r * N + N - m];
+      b = make_double2(c.x, -c.y);
     }
-    __syncthreads();
+    const double2 e = cadd(a, b);
+    const double2 wc = make_double2(tw[m].x, -tw[m].y);  // exp(+2 pi i m / nlon)
+    const double2 o = cmul(csub(a, b), wc);
+    A[r * N + m] = make_double2(e.x - o.y, e.y + o.x);  // e + i o
+  }
+  __syncthreads();
+  const double2* Z = stockham_c<N, 1, true>(A, B, tw);
+  double2* rn = reinterpret_cast<double2*>(g.p[f] + (size_t)j * (2 * N));
+  double2* rs = reinterpret_cast<double2*>(g.p[f] + (size_t)js * (2 * N));
+  const bool ep = (f == 0) && epi.out2;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    const double2 vn = Z[t], vs = Z[N + t];
+    rn[t] = vn;
+    rs[t] = vs;
+    if (ep) {
+      const double2 mn = reinterpret_cast<const double2*>(epi.mul2 + (size_t)j * (2 * N))[t];
+      const double2 ms = reinterpret_cast<const double2*>(epi.mul2 + (size_t)js * (2 * N))[t];
+      reinterpret_cast<double2*>(epi.out2 + (size_t)j * (2 * N))[t] = make_double2(vn.x * mn.x, vn.y * mn.y);
+      reinterpret_cast<double2*>(epi.out2 + (size_t)js * (2 * N))[t] = make_double2(vs.x * ms.x, vs.y * ms.y);
+    }
   }
 }
 
-// ------------------------------------------------------------------ Legendre analysis
-constexpr int ANA_TL = 8;      // degrees per warp reduction
-constexpr int ANA_NAMAX = 8;   // latitude groups per lane in one pass
+// launch over the supported sizes N = 4 .. 2048 (nlon = 8 .. 4096)
+#define SLE_FFT_SWITCH(N2, CALL) \
+  switch (N2) {                  \
+    case 4: CALL(4); break;      \
+    case 8: CALL(8); break;      \
+    case 16: CALL(16); break;    \
+    case 32: CALL(32); break;    \
+    case 64: CALL(64); break;    \
+    case 128: CALL(128); break;  \
+    case 256: CALL(256); break;  \
+    case 512: CALL(512); break;  \
+    case 1024: CALL(1024); break; \
+    default: CALL(2048); break;  \
+  }
 
+static int fft_threads(int n2) { return n2 / 4 > 32 ? n2 / 4 : 32; }
+
+// ------------------------------------------------------------------ Legendre analysis
+constexpr int ANA_TL = 4;      // degrees per warp reduction
+constexpr int ANA_NAMAX = 8;   // latitude groups per lane in one pass
+constexpr int ANA_WARPS = 4;   // warps (independent segments) per block
+
+// One batch of TL consecutive degrees: advance the recurrence of the NA latitudes of this lane,
+// form the per-lane products with the folded input of the degree's parity, and reduce over
+// the warp.  Degree t of the batch has parity t (segments start at even l - m).
+template <int NA>
+__device__ __forceinline__ void ana_batch(const double* __restrict__ sbe, const double (&mu)[NA],
+                                          double (&qa)[NA], double (&qb)[NA], const double2 (&xs)[NA],
+                                          const double2 (&xd)[NA], double (&v)[2 * ANA_TL], int lane) {
+  // the latitude sum of each degree uses up to four independent partial sums (short chains)
+  constexpr int NP = (NA >= 4) ? 4 : NA;
+#pragma unroll
+  for (int t = 0; t < ANA_TL; ++t) {
+    double re[NP], im[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) re[p] = im[p] = 0.0;
+    const double b = sbe[t];
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+      const double q = fma(mu[i], qb[i], b * qa[i]);
+      qa[i] = qb[i];
+      qb[i] = q;
+      const double2 x = (t & 1) ? xd[i] : xs[i];
+      re[i % NP] = fma(q, x.x, re[i % NP]);
+      im[i % NP] = fma(q, x.y, im[i % NP]);
+    }
+    double sr = re[0], si = im[0];
+    if (NP == 4) {
+      sr = (re[0] + re[1]) + (re[2] + re[3]);
+      si = (im[0] + im[1]) + (im[2] + im[3]);
+    } else if (NP == 2) {
+      sr = re[0] + re[1];
+      si = im[0] + im[1];
+    }
+    v[2 * t] = sr;
+    v[2 * t + 1] = si;
+  }
+  warp_transpose_reduce<2 * ANA_TL>(v, lane);
+}
+
+// Degrees l0 .. l0+len-1 of segment s over the latitude groups g0 .. g0+NA-1 (groups at or
+// beyond ngrp hold no latitudes).  The staged recurrence coefficients are zero-padded to a
+// whole number of batches; the extra degrees are computed and discarded.
 template <int NA>
 __device__ __forceinline__ void ana_segment(const sle::ShtDev& P, int s, int g0, const double2* __restrict__ Xf,
-                                            double2* __restrict__ Uf, int lane, bool accumulate) {
-  constexpr int TL = ANA_TL;
-  constexpr int V = 2 * TL;
-  constexpr int SHIFT = 5 - 4;  // log2(V) = 4
+                                            double2* __restrict__ Uf, int lane, bool accumulate,
+                                            double* __restrict__ sbe, double* __restrict__ scf) {
+  constexpr int SHIFT = (ANA_TL == 8) ? 1 : (ANA_TL == 4) ? 2 : 3;  // 5 - log2(2 ANA_TL)
   const int m = P.seg_m[s], l0 = P.seg_l0[s];
-  const int l1 = min(l0 + SEG, P.lmax + 1);
+  const int len = min(SEG, P.lmax + 1 - l0);
   const int nh = P.nh;
+  const long long base = P.moff[m] + (l0 - m);
+  for (int t = lane; t < SEG; t += 32) {
+    sbe[t] = (t < len) ? P.be[base + t] : 0.0;
+    scf[t] = (t < len) ? P.cf[base + t] : 0.0;
+  }
   const double2* XS = Xf + (size_t)m * nh;
   const double2* XD = Xf + (size_t)(P.nm + m) * nh;
   double mu[NA], qa[NA], qb[NA];
@@ -383,49 +522,20 @@ __device__ __forceinline__ void ana_segment(const sle::ShtDev& P, int s, int g0,
     xs[i] = ok ? XS[j] : make_double2(0.0, 0.0);
     xd[i] = ok ? XD[j] : make_double2(0.0, 0.0);
   }
-  const long long base = P.moff[m] + (l0 - m);
-  for (int lb = l0; lb < l1; lb += TL) {
-    double v[V];
-#pragma unroll
-    for (int t = 0; t < TL; ++t) {
-      const int l = lb + t;
-      double re = 0.0, im = 0.0;
-      if (l < l1) {
-        if (t < 2 && lb == l0) {
-#pragma unroll
-          for (int i = 0; i < NA; ++i) {
-            const double q = (t == 0) ? qa[i] : qb[i];
-            const double2 x = (t & 1) ? xd[i] : xs[i];
-            re = fma(q, x.x, re);
-            im = fma(q, x.y, im);
-          }
-        } else {
-          const double b = __ldg(P.be + base + (l - l0));
-#pragma unroll
-          for (int i = 0; i < NA; ++i) {
-            const double q = fma(mu[i], qb[i], b * qa[i]);
-            qa[i] = qb[i];
-            qb[i] = q;
-            const double2 x = (t & 1) ? xd[i] : xs[i];
-            re = fma(q, x.x, re);
-            im = fma(q, x.y, im);
-          }
-        }
-      }
-      v[2 * t] = re;
-      v[2 * t + 1] = im;
-    }
-    warp_transpose_reduce<V>(v, lane);
-    const int idx = lane >> SHIFT;
-    const int t = idx >> 1, c = idx & 1;
-    const int l = lb + t;
-    if ((lane & ((1 << SHIFT) - 1)) == 0 && l < l1) {
-      const long long pi = base + (l - l0);
-      const double val = __ddiv_rn(v[0] * __ldg(P.cf + pi), SQRT2_LEGACY);
-      double* dst = reinterpret_cast<double*>(Uf + pi) + c;
+  __syncwarp();
+  const int idx = lane >> SHIFT;
+  const int tw_ = idx >> 1, c = idx & 1;
+  const bool writer = (lane & ((1 << SHIFT) - 1)) == 0;
+  for (int off = 0; off < len; off += ANA_TL) {
+    double v[2 * ANA_TL];
+    ana_batch<NA>(sbe + off, mu, qa, qb, xs, xd, v, lane);
+    if (writer && off + tw_ < len) {
+      const double val = __ddiv_rn(v[0] * scf[off + tw_], SQRT2_LEGACY);
+      double* dst = reinterpret_cast<double*>(Uf + base + off + tw_) + c;
       *dst = accumulate ? (*dst + val) : val;
     }
   }
+  __syncwarp();
 }
 
 __device__ void ana_zero_segment(const sle::ShtDev& P, int s, double2* Uf, int lane) {
@@ -435,44 +545,51 @@ __device__ void ana_zero_segment(const sle::ShtDev& P, int s, double2* Uf, int l
   for (int l = l0 + lane; l < l1; l += 32) Uf[base + (l - l0)] = make_double2(0.0, 0.0);
 }
 
-__global__ void __launch_bounds__(128) k_leg_ana(sle::ShtDev P, SpecPtrs out) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void __launch_bounds__(32 * ANA_WARPS, 3) k_leg_ana(sle::ShtDev P, SpecPtrs out) {
+  __shared__ double scoef[ANA_WARPS][2][SEG];
+  const int wib = threadIdx.x >> 5;
+  const int warp = blockIdx.x * ANA_WARPS + wib;
   const int lane = threadIdx.x & 31;
   if (warp >= P.nseg) return;
   const int f = blockIdx.y;
+  if (field_gated_off(P, f)) return;
   const double2* Xf = P.X + (size_t)f * 2 * P.nm * P.nh;
   double2* Uf = out.p[f];
   const int s = P.ana_order[warp];
-  int g0 = P.istart[s];
-  int na = P.ngrp - g0;
-  if (na <= 0) {
+  int gfirst = P.istart[s];
+  if (gfirst >= P.ngrp) {
     ana_zero_segment(P, s, Uf, lane);
     return;
   }
+  double* sbe = scoef[wib][0];
+  double* scf = scoef[wib][1];
+  // latitude groups gfirst .. ngrp-1 in passes of up to ANA_NAMAX groups; a pass of na groups
+  // runs the smallest instance NA >= na.  The first pass starts NA - na groups closer to the
+  // pole when that stays inside the grid (those groups hold negligible but valid values and no
+  // other pass covers them); later passes start where the previous one ended and mask groups
+  // beyond the grid.
   bool acc = false;
-  while (na > 0) {
-    const int nn = na > ANA_NAMAX ? ANA_NAMAX : na;
-    switch (nn) {
-      case 1: ana_segment<1>(P, s, g0, Xf, Uf, lane, acc); break;
-      case 2: ana_segment<2>(P, s, g0, Xf, Uf, lane, acc); break;
-      case 3: ana_segment<3>(P, s, g0, Xf, Uf, lane, acc); break;
-      case 4: ana_segment<4>(P, s, g0, Xf, Uf, lane, acc); break;
-      case 5: ana_segment<5>(P, s, g0, Xf, Uf, lane, acc); break;
-      case 6: ana_segment<6>(P, s, g0, Xf, Uf, lane, acc); break;
-      case 7: ana_segment<7>(P, s, g0, Xf, Uf, lane, acc); break;
-      default: ana_segment<8>(P, s, g0, Xf, Uf, lane, acc); break;
+  int g = gfirst;
+  while (g < P.ngrp) {
+    const int na = min(P.ngrp - g, ANA_NAMAX);
+    const int NA = (na > 4) ? 8 : (na > 2) ? 4 : na;
+    const int g0 = acc ? g : max(0, min(g, P.ngrp - NA));
+    switch (NA) {
+      case 1: ana_segment<1>(P, s, g0, Xf, Uf, lane, acc, sbe, scf); break;
+      case 2: ana_segment<2>(P, s, g0, Xf, Uf, lane, acc, sbe, scf); break;
+      case 4: ana_segment<4>(P, s, g0, Xf, Uf, lane, acc, sbe, scf); break;
+      default: ana_segment<8>(P, s, g0, Xf, Uf, lane, acc, sbe, scf); break;
     }
-    __syncwarp();
     acc = true;
-    g0 += nn;
-    na -= nn;
+    g = g0 + NA;
   }
 }
 
 // ----------------------------------------------------------------- Legendre synthesis
-// Block per pair of orders (p, lmax-p); warp per 32-latitude group; E (even l-m) and O
-// (odd l-m) sums of cf_l * 1.41421356 * U_l * Q_l over the significant segments.
-__global__ void __launch_bounds__(1024) k_leg_syn(sle::ShtDev P, CSpecPtrs in) {
+// Block per pair of orders (p, lmax-p); warp per 64 latitudes (two per lane); E (even l-m) and
+// O (odd l-m) sums of cf_l * 1.41421356 * U_l * Q_l over the segments where the warp's outer
+// latitude group is significant.
+__global__ void __launch_bounds__(512, 1) k_leg_syn(sle::ShtDev P, CSpecPtrs in) {
   extern __shared__ double smd[];
   const int f = blockIdx.y;
   const int p = blockIdx.x;
@@ -481,9 +598,10 @@ __global__ void __launch_bounds__(1024) k_leg_syn(sle::ShtDev P, CSpecPtrs in) {
   double* bes = smd + 2 * P.nm;                            // [nm]
   const double2* U = in.p[f];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int j = w * 32 + lane;
-  const bool ok = j < P.nh;
-  const double x = ok ? P.mu[j] : 0.0;
+  const int j0 = w * 64 + lane, j1 = j0 + 32;
+  const bool ok0 = j0 < P.nh, ok1 = j1 < P.nh;
+  const double x0 = ok0 ? P.mu[j0] : 0.0, x1 = ok1 ? P.mu[j1] : 0.0;
+  const int gouter = min(2 * w + 1, P.ngrp - 1);
   double2* Ef = P.EO + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
   double2* Of = P.EO + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
   for (int pass = 0; pass < 2; ++pass) {
@@ -499,45 +617,46 @@ __global__ void __launch_bounds__(1024) k_leg_syn(sle::ShtDev P, CSpecPtrs in) {
       bes[t] = P.be[base + t];
     }
     __syncthreads();
-    double2 E = make_double2(0.0, 0.0), O = make_double2(0.0, 0.0);
+    double2 E0 = make_double2(0.0, 0.0), O0 = E0, E1 = E0, O1 = E0;
     for (int s = P.segoff[m]; s < P.segoff[m + 1]; ++s) {
-      if (w < (int)P.istart[s]) continue;
+      if (gouter < (int)P.istart[s]) continue;
       const int l0 = P.seg_l0[s];
       const int l1 = min(l0 + SEG, L + 1);
-      const double2 sd = ok ? P.seeds[(size_t)s * P.nh + j] : make_double2(0.0, 0.0);
-      double qa = sd.x, qb = sd.y;
+      const double2 s0 = ok0 ? P.seeds[(size_t)s * P.nh + j0] : make_double2(0.0, 0.0);
+      const double2 s1 = ok1 ? P.seeds[(size_t)s * P.nh + j1] : make_double2(0.0, 0.0);
+      double qa0 = s0.x, qb0 = s0.y, qa1 = s1.x, qb1 = s1.y;
       int r = l0 - m;
-      {
-        const double2 u = Uc[r];
-        E.x = fma(u.x, qa, E.x);
-        E.y = fma(u.y, qa, E.y);
-      }
-      if (l0 + 1 < l1) {
-        const double2 u = Uc[r + 1];
-        O.x = fma(u.x, qb, O.x);
-        O.y = fma(u.y, qb, O.y);
-      }
-      for (int l = l0 + 2; l < l1; l += 2) {
-        r = l - m;
-        double q = fma(x, qb, bes[r] * qa);
-        qa = qb;
-        qb = q;
+      const int rend = l1 - m;
+      for (; r + 2 <= rend; r += 2) {
         double2 u = Uc[r];
-        E.x = fma(u.x, q, E.x);
-        E.y = fma(u.y, q, E.y);
-        if (l + 1 < l1) {
-          q = fma(x, qb, bes[r + 1] * qa);
-          qa = qb;
-          qb = q;
-          u = Uc[r + 1];
-          O.x = fma(u.x, q, O.x);
-          O.y = fma(u.y, q, O.y);
-        }
+        double b = bes[r];
+        double q0 = fma(x0, qb0, b * qa0), q1 = fma(x1, qb1, b * qa1);
+        qa0 = qb0; qb0 = q0; qa1 = qb1; qb1 = q1;
+        E0.x = fma(u.x, q0, E0.x); E0.y = fma(u.y, q0, E0.y);
+        E1.x = fma(u.x, q1, E1.x); E1.y = fma(u.y, q1, E1.y);
+        u = Uc[r + 1];
+        b = bes[r + 1];
+        q0 = fma(x0, qb0, b * qa0);
+        q1 = fma(x1, qb1, b * qa1);
+        qa0 = qb0; qb0 = q0; qa1 = qb1; qb1 = q1;
+        O0.x = fma(u.x, q0, O0.x); O0.y = fma(u.y, q0, O0.y);
+        O1.x = fma(u.x, q1, O1.x); O1.y = fma(u.y, q1, O1.y);
+      }
+      if (r < rend) {  // odd-length tail: one more even degree
+        const double2 u = Uc[r];
+        const double b = bes[r];
+        const double q0 = fma(x0, qb0, b * qa0), q1 = fma(x1, qb1, b * qa1);
+        E0.x = fma(u.x, q0, E0.x); E0.y = fma(u.y, q0, E0.y);
+        E1.x = fma(u.x, q1, E1.x); E1.y = fma(u.y, q1, E1.y);
       }
     }
-    if (ok) {
-      Ef[(size_t)m * P.nh + j] = E;
-      Of[(size_t)m * P.nh + j] = O;
+    if (ok0) {
+      Ef[(size_t)m * P.nh + j0] = E0;
+      Of[(size_t)m * P.nh + j0] = O0;
+    }
+    if (ok1) {
+      Ef[(size_t)m * P.nh + j1] = E1;
+      Of[(size_t)m * P.nh + j1] = O1;
     }
   }
 }
@@ -561,11 +680,18 @@ __global__ void k_unpack(sle::ShtDev P, const double2* packed, double2* dense) {
 
 // ------------------------------------------------------------------------ launchers
 static size_t fft_smem(const ShtDev& d) { return (size_t)5 * d.n2 * sizeof(double2); }
+static int syn_threads(const ShtDev& d) { return 32 * ((d.ngrp + 1) / 2); }
 static size_t syn_smem(const ShtDev& d) { return (size_t)3 * d.nm * sizeof(double); }
 
 int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, double2* const* out,
-                        cudaStream_t st) {
-  const ShtDev& d = plan->d;
+                        cudaStream_t st, const AnaGate* gate) {
+  ShtDev d = plan->d;
+  if (gate) {
+    d.gate_conv = gate->conv;
+    d.gate_chg = gate->chg;
+    d.gate_conv_mask = gate->conv_mask;
+    d.gate_chg_mask = gate->chg_mask;
+  }
   if (nf < 1 || nf > MAXF) {
     set_error("analysis: nfields must be 1..%d", MAXF);
     return SLE_ERR_BAD_ARG;
@@ -577,9 +703,11 @@ int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, doubl
     o.p[f] = out[f];
   }
   ProfToken t0 = prof_begin(PROF_FFT, nf, st);
-  k_fft_fold<<<d.nh, 256, fft_smem(d), st>>>(d, nf, g);
+#define SLE_LAUNCH_FOLD(NN) k_fft_fold<NN><<<dim3(d.nh, nf), fft_threads(NN), fft_smem(d), st>>>(d, g)
+  SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_FOLD)
+#undef SLE_LAUNCH_FOLD
   prof_end(t0, st);
-  const int warps_per_block = 4;
+  const int warps_per_block = ANA_WARPS;
   dim3 grid((d.nseg + warps_per_block - 1) / warps_per_block, nf);
   ProfToken t1 = prof_begin(PROF_LEG_ANA, nf, st);
   k_leg_ana<<<grid, 32 * warps_per_block, 0, st>>>(d, o);
@@ -604,11 +732,13 @@ int sht_synthesis_packed(sle_sht* plan, int nf, const double2* const* coeffs, do
   }
   const int npairs = (d.nm + 1) / 2;
   ProfToken t0 = prof_begin(PROF_LEG_SYN, nf, st);
-  k_leg_syn<<<dim3(npairs, nf), 32 * d.ngrp, syn_smem(d), st>>>(d, c);
+  k_leg_syn<<<dim3(npairs, nf), syn_threads(d), syn_smem(d), st>>>(d, c);
   prof_end(t0, st);
   SynEpilogue e = epi ? *epi : SynEpilogue{nullptr, nullptr};
   ProfToken t1 = prof_begin(PROF_IFFT, nf, st);
-  k_ifft_unfold<<<d.nh, 256, fft_smem(d), st>>>(d, nf, g, e);
+#define SLE_LAUNCH_IFFT(NN) k_ifft_unfold<NN><<<dim3(d.nh, nf), fft_threads(NN), fft_smem(d), st>>>(d, g, e)
+  SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_IFFT)
+#undef SLE_LAUNCH_IFFT
   prof_end(t1, st);
   note_launch(2);
   SLE_CUDA(cudaGetLastError());
@@ -778,8 +908,13 @@ static int plan_build(sle_sht* p, int nlat, int nlon, int lmax) {
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
   SLE_CUDA(cudaMemcpy(p->ana_order, order.data(), d.nseg * sizeof(int), cudaMemcpyHostToDevice));
 
-  SLE_CUDA(cudaFuncSetAttribute(k_fft_fold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(d)));
-  SLE_CUDA(cudaFuncSetAttribute(k_ifft_unfold, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(d)));
+#define SLE_ATTR_FFT(NN)                                                                              \
+  do {                                                                                                \
+    SLE_CUDA(cudaFuncSetAttribute(k_fft_fold<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(d)));    \
+    SLE_CUDA(cudaFuncSetAttribute(k_ifft_unfold<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(d))); \
+  } while (0)
+  SLE_FFT_SWITCH(d.n2, SLE_ATTR_FFT)
+#undef SLE_ATTR_FFT
   SLE_CUDA(cudaFuncSetAttribute(k_leg_syn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)syn_smem(d)));
   SLE_CUDA(cudaDeviceSynchronize());
   return SLE_OK;
@@ -998,9 +1133,10 @@ extern "C" int sle_sht_analysis_noalloc(sle_sht* plan, const double* grid_dev, v
   g.p[0] = grid_dev;
   SpecPtrs o{};
   o.p[0] = reinterpret_cast<double2*>(coeffs_packed_dev);
-  k_fft_fold<<<d.nh, 256, fft_smem(d), st>>>(d, 1, g);
-  const int warps_per_block = 4;
-  k_leg_ana<<<dim3((d.nseg + warps_per_block - 1) / warps_per_block, 1), 32 * warps_per_block, 0, st>>>(d, o);
+#define SLE_LAUNCH_FOLD1(NN) k_fft_fold<NN><<<dim3(d.nh, 1), fft_threads(NN), fft_smem(d), st>>>(d, g)
+  SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_FOLD1)
+#undef SLE_LAUNCH_FOLD1
+  k_leg_ana<<<dim3((d.nseg + ANA_WARPS - 1) / ANA_WARPS, 1), 32 * ANA_WARPS, 0, st>>>(d, o);
   SLE_CUDA(cudaGetLastError());
   note_launch(2);
   return SLE_OK;

@@ -9,6 +9,7 @@
 #include "sle_internal.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -18,7 +19,6 @@ constexpr double EPS0 = 2.220446049250313e-16;   // numpy finfo(float64).eps (so
 constexpr double PI_LEGACY = 3.1415926535898;    // truncated literal (solver.py:31)
 constexpr int GR_MAXACC = 3;                      // solver.py:38
 constexpr int MAX_INNER = 9999;                   // solver.py:1049
-constexpr int RED_BLOCKS = 296;                   // 2 x 148 SMs: reduction grid (fixed partition)
 
 // Constants of the rotation block (solver.py:910-975), computed on the host with the
 // reference's expressions.
@@ -90,6 +90,8 @@ __device__ double block_sum(double v, double* sh) {
 __device__ bool last_block_total(double part, double* partials, unsigned int* counter, double* total,
                                  double* sh) {
   __shared__ bool is_last;
+  __threadfence();  // every thread's earlier global writes are visible before the block's ticket
+  __syncthreads();
   if (threadIdx.x == 0) {
     partials[blockIdx.x] = part;
     __threadfence();
@@ -132,6 +134,26 @@ __device__ __forceinline__ double2 np_cmul(double2 a, double2 b) {
 }
 
 // ------------------------------------------------------------------------- kernels
+// Grid kernels process two neighbouring cells per thread (16-byte loads; nlon is even) over a
+// full-width grid; spectral kernels one coefficient per thread.  Reductions: block partial
+// sums, then the last block to finish sums the partials in index order.
+
+// true in all threads of the last block to finish (after every block passed this point)
+__device__ bool last_block(unsigned int* counter) {
+  __shared__ bool is_last;
+  __threadfence();  // every thread's earlier global writes are visible before the block's ticket
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int t = atomicAdd(counter, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
 __global__ void k_set_decay(int K, int nl, const double* s, const int* nmod, double dt, double* decay,
                             double* omd) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -143,81 +165,121 @@ __global__ void k_set_decay(int K, int nl, const double* s, const int* nmod, dou
   omd[i] = __dsub_rn(1.0, d);
 }
 
+// degree-2 rotational states and their sums (solver.py:409-421): one thread per component
+// (9 il, 3 m, 6 lambda re/im), modes summed in ascending order, inputs staged in shared memory;
+// then the per-step resets and the snapshot of the committed rotational loads (oldil, oldm,
+// dlambda_prev2; solver.py:837-839).  Run by the last block of k_advance (32 threads used).
+__device__ void rot_advance_block(const Dev& D, Scal* sc, double* r_il, double* r_m, double* r_lam) {
+  __shared__ double sd[64], sa[4][64], sp[18];
+  const int q = threadIdx.x;
+  const int n2 = (D.nl > 2) ? min(D.nmod2, 64) : 0;
+  for (int k = q; k < n2; k += blockDim.x) {
+    sd[k] = D.decay[k * D.nl + 2];
+    sa[0][k] = D.a_il[k];
+    sa[1][k] = D.a_m[k];
+    sa[2][k] = D.a_tsl[k];
+    sa[3][k] = D.a_trr[k];
+  }
+  if (q < 9) sp[q] = sc->p_il[q];
+  else if (q < 12) sp[q] = sc->p_m[q - 9];
+  else if (q < 18) sp[q] = sc->p_lambda[q - 12];
+  __syncthreads();
+  if (q < 18) {
+    double* r = (q < 9) ? r_il + q : (q < 12) ? r_m + (q - 9) : r_lam + (q - 12);
+    const int stride = (q < 9) ? 9 : (q < 12) ? 3 : 6;
+    const double p = sp[q];
+    double acc = 0.0, acc2 = 0.0;
+    for (int k = 0; k < n2; ++k) {
+      const double d = sd[k];
+      const double o = __dsub_rn(1.0, d);
+      const double x = __dadd_rn(__dmul_rn(d, r[k * stride]), __dmul_rn(o, p));
+      r[k * stride] = x;
+      if (q < 9) {
+        acc = __dadd_rn(acc, __dmul_rn(sa[0][k], x));
+      } else if (q < 12) {
+        acc = __dadd_rn(acc, __dmul_rn(sa[1][k], x));
+      } else {
+        acc = __dadd_rn(acc, __dmul_rn(sa[2][k], x));
+        acc2 = __dadd_rn(acc2, __dmul_rn(sa[3][k], x));
+      }
+    }
+    if (q < 9) sc->sum_il[q] = acc;
+    else if (q < 12) sc->sum_m[q - 9] = acc;
+    else {
+      sc->sum_tsl[q - 12] = acc;
+      sc->sum_trr[q - 12] = acc2;
+    }
+  }
+  if (q == 0) {
+    sc->numiter = 0;
+    sc->converged = 0;
+    sc->status = 0;
+    sc->gr_nacc = 0;
+    sc->gr_changed = 0;
+    sc->gr_reguess = 0;
+    sc->gr_ice_an = 0;
+    for (int i = 0; i < 9; ++i) sc->oldil[i] = sp[i];
+    for (int i = 0; i < 3; ++i) sc->oldm[i] = sp[9 + i];
+    for (int i = 0; i < 6; ++i) sc->dlam_prev2[i] = sp[12 + i];
+    for (int i = 0; i < 6; ++i) sc->dsl_rot[i] = sc->rr_rot[i] = sc->dlam_cur2[i] = 0.0;
+    for (int i = 0; i < 9; ++i) sc->dil[i] = 0.0;
+    for (int i = 0; i < 3; ++i) sc->dm[i] = 0.0;
+  }
+}
+
 // R_k <- d R_k + (1-d) P ; visc = sum_k a_sl R_k ; rad = sum_k a_rr R_k   (solver.py:386-407)
-__global__ void k_advance(Dev D, double2* __restrict__ R, const double2* __restrict__ P,
-                          double2* __restrict__ visc, double2* __restrict__ rad) {
+// The last block advances the degree-2 rotational state instead.
+__global__ void __launch_bounds__(256) k_advance(Dev D, double2* __restrict__ R, const double2* __restrict__ P,
+                                                 double2* __restrict__ visc, double2* __restrict__ rad, Scal* sc,
+                                                 double* r_il, double* r_m, double* r_lam) {
+  if (blockIdx.x == gridDim.x - 1) {
+    rot_advance_block(D, sc, r_il, r_m, r_lam);
+    return;
+  }
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef) return;
   const int l = D.lidx[i];
   const double2 p = P[i];
   double2 v = make_double2(0.0, 0.0), r = v;
   const int nk = D.nmod[l];
-  for (int k = 0; k < nk; ++k) {
-    const int kl = k * D.nl + l;
-    const double d = D.decay[kl], o = D.omd[kl], as = D.a_sl[kl], ar = D.a_rr[kl];
-    double2 x = R[(size_t)k * D.ncoef + i];
-    x.x = __dadd_rn(__dmul_rn(x.x, d), __dmul_rn(p.x, o));
-    x.y = __dadd_rn(__dmul_rn(x.y, d), __dmul_rn(p.y, o));
-    R[(size_t)k * D.ncoef + i] = x;
-    v.x = __dadd_rn(v.x, __dmul_rn(x.x, as));
-    v.y = __dadd_rn(v.y, __dmul_rn(x.y, as));
-    r.x = __dadd_rn(r.x, __dmul_rn(x.x, ar));
-    r.y = __dadd_rn(r.y, __dmul_rn(x.y, ar));
-  }
-  visc[i] = v;
-  rad[i] = r;
-}
-
-// degree-2 rotational states and their sums (solver.py:409-421); also snapshot the
-// committed rotational loads (oldil, oldm, dlambda_prev2; solver.py:837-839)
-__global__ void k_rot_advance(Dev D, Scal* sc, double* r_il, double* r_m, double* r_lam) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int q = 0; q < 9; ++q) sc->sum_il[q] = 0.0;
-  for (int q = 0; q < 3; ++q) sc->sum_m[q] = 0.0;
-  for (int q = 0; q < 6; ++q) sc->sum_tsl[q] = sc->sum_trr[q] = 0.0;
-  if (D.nl > 2) {
-    for (int k = 0; k < D.nmod2; ++k) {
-      const double d = D.decay[k * D.nl + 2];
-      const double o = __dsub_rn(1.0, d);
-      for (int q = 0; q < 9; ++q) {
-        const double x = __dadd_rn(__dmul_rn(d, r_il[k * 9 + q]), __dmul_rn(o, sc->p_il[q]));
-        r_il[k * 9 + q] = x;
-      }
-      for (int q = 0; q < 3; ++q) {
-        const double x = __dadd_rn(__dmul_rn(d, r_m[k * 3 + q]), __dmul_rn(o, sc->p_m[q]));
-        r_m[k * 3 + q] = x;
-      }
-      for (int q = 0; q < 6; ++q) {
-        const double x = __dadd_rn(__dmul_rn(d, r_lam[k * 6 + q]), __dmul_rn(o, sc->p_lambda[q]));
-        r_lam[k * 6 + q] = x;
-      }
-      for (int q = 0; q < 9; ++q) sc->sum_il[q] = __dadd_rn(sc->sum_il[q], __dmul_rn(D.a_il[k], r_il[k * 9 + q]));
-      for (int q = 0; q < 3; ++q) sc->sum_m[q] = __dadd_rn(sc->sum_m[q], __dmul_rn(D.a_m[k], r_m[k * 3 + q]));
-      for (int q = 0; q < 6; ++q) {
-        sc->sum_tsl[q] = __dadd_rn(sc->sum_tsl[q], __dmul_rn(D.a_tsl[k], r_lam[k * 6 + q]));
-        sc->sum_trr[q] = __dadd_rn(sc->sum_trr[q], __dmul_rn(D.a_trr[k], r_lam[k * 6 + q]));
+  constexpr int U = 4;
+  for (int k0 = 0; k0 < nk; k0 += U) {
+    double2 x[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (k0 + u < nk) x[u] = R[(size_t)(k0 + u) * D.ncoef + i];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = k0 + u;
+      if (k < nk) {
+        const int kl = k * D.nl + l;
+        const double d = D.decay[kl], o = D.omd[kl], as = D.a_sl[kl], ar = D.a_rr[kl];
+        double2 y;
+        y.x = __dadd_rn(__dmul_rn(x[u].x, d), __dmul_rn(p.x, o));
+        y.y = __dadd_rn(__dmul_rn(x[u].y, d), __dmul_rn(p.y, o));
+        R[(size_t)k * D.ncoef + i] = y;
+        v.x = __dadd_rn(v.x, __dmul_rn(y.x, as));
+        v.y = __dadd_rn(v.y, __dmul_rn(y.y, as));
+        r.x = __dadd_rn(r.x, __dmul_rn(y.x, ar));
+        r.y = __dadd_rn(r.y, __dmul_rn(y.y, ar));
       }
     }
   }
-  sc->numiter = 0;
-  sc->converged = 0;
-  sc->status = 0;
-  sc->gr_nacc = 0;
-  sc->gr_changed = 0;
-  sc->gr_reguess = 0;
-  sc->gr_ice_an = 0;
-  for (int q = 0; q < 9; ++q) sc->oldil[q] = sc->p_il[q];
-  for (int q = 0; q < 3; ++q) sc->oldm[q] = sc->p_m[q];
-  for (int q = 0; q < 6; ++q) sc->dlam_prev2[q] = sc->p_lambda[q];
-  for (int q = 0; q < 6; ++q) sc->dsl_rot[q] = sc->rr_rot[q] = sc->dlam_cur2[q] = 0.0;
-  for (int q = 0; q < 9; ++q) sc->dil[q] = 0.0;
-  for (int q = 0; q < 3; ++q) sc->dm[q] = 0.0;
+  visc[i] = v;
+  rad[i] = r;
 }
 
 // grounded ice on topography `topo` (flotation test, solver.py:655-659)
 __device__ __forceinline__ double icestar_on(double ice, double topo, double rhow, double rhoi) {
   const bool keep = (topo > 0.0) || (ice > __ddiv_rn(__dmul_rn(fabs(topo), rhow), rhoi));
   return keep ? ice : __dmul_rn(ice, 0.0);
+}
+
+__device__ __forceinline__ double2 ld2(const double* p, long long i) {
+  return reinterpret_cast<const double2*>(p)[i];
+}
+__device__ __forceinline__ void st2(double* p, long long i, double a, double b) {
+  reinterpret_cast<double2*>(p)[i] = make_double2(a, b);
 }
 
 // Step prologue on the grid (solver.py:853-887): I* on the previous topography, beta,
@@ -227,77 +289,38 @@ __global__ void k_ice_grid(Dev D, const double* __restrict__ ice, const double* 
                            const double* __restrict__ cstar0, double* __restrict__ icestar,
                            double* __restrict__ beta, double* __restrict__ cstar, double* __restrict__ tO,
                            const double* __restrict__ ice_prev, double* __restrict__ oldsrc, Scal* sc) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= D.ng) return;
-  const double v = ice[i];
-  if (!isfinite(v)) sc->status = SLE_ERR_NONFINITE;
-  const double is = D.checkmarine ? icestar_on(v, topo_prev[i], D.rhow, D.rhoi) : v;
-  icestar[i] = is;
-  const double b = (is < EPS0) ? 1.0 : 0.0;
-  beta[i] = b;
-  const double c = __dmul_rn(cxy[i], b);
-  cstar[i] = c;
-  tO[i] = __dmul_rn(tinit[i], __dsub_rn(c, cstar0[i]));
+  const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (2 * h >= D.ng) return;
+  const double2 v = ld2(ice, h), tp = ld2(topo_prev, h), cx = ld2(cxy, h), ti = ld2(tinit, h), c0 = ld2(cstar0, h);
+  if (!isfinite(v.x) || !isfinite(v.y)) sc->status = SLE_ERR_NONFINITE;
+  double is[2], b[2], c[2], t[2];
+  const double vv[2] = {v.x, v.y}, tt[2] = {tp.x, tp.y}, cc[2] = {cx.x, cx.y}, ii[2] = {ti.x, ti.y},
+               zz[2] = {c0.x, c0.y};
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    is[u] = D.checkmarine ? icestar_on(vv[u], tt[u], D.rhow, D.rhoi) : vv[u];
+    b[u] = (is[u] < EPS0) ? 1.0 : 0.0;
+    c[u] = __dmul_rn(cc[u], b[u]);
+    t[u] = __dmul_rn(ii[u], __dsub_rn(c[u], zz[u]));
+  }
+  st2(icestar, h, is[0], is[1]);
+  st2(beta, h, b[0], b[1]);
+  st2(cstar, h, c[0], c[1]);
+  st2(tO, h, t[0], t[1]);
   if (oldsrc) {
-    const double vp = ice_prev[i];
-    oldsrc[i] = D.checkmarine ? icestar_on(vp, tinit[i], D.rhow, D.rhoi) : vp;
+    const double2 vp = ld2(ice_prev, h);
+    const double o0 = D.checkmarine ? icestar_on(vp.x, ti.x, D.rhow, D.rhoi) : vp.x;
+    const double o1 = D.checkmarine ? icestar_on(vp.y, ti.y, D.rhow, D.rhoi) : vp.y;
+    st2(oldsrc, h, o0, o1);
   }
 }
 
-// dice = I*_lm - old ; dI = p_ice + dice ; first guess of the load increment ; dS_cur ;
-// so = sum|load_inc|  (solver.py:868-905; extrap solver_opt.py:504-513)
-// mode: 0 eustatic, 1 extrap uniform (2 h1 - h2), 2 extrap variable (c1 h1 - c2 h2)
-__global__ void k_pre_spec(Dev D, const double2* __restrict__ icelm, const double2* __restrict__ oldice,
-                           const double2* __restrict__ p_ice, const double2* __restrict__ cstarlm,
-                           const double2* __restrict__ dSprev, const double2* __restrict__ h1,
-                           const double2* __restrict__ h2, int mode, double c1, double c2,
-                           double2* __restrict__ dice, double2* __restrict__ dI, double2* __restrict__ load,
-                           double2* __restrict__ dScur, Scal* sc, double* partials, unsigned int* counter) {
-  __shared__ double sh[32];
-  double acc = 0.0;
-  const double2 dice00 = make_double2(__dsub_rn(icelm[0].x, oldice[0].x), __dsub_rn(icelm[0].y, oldice[0].y));
-  const double2 c00 = cstarlm[0];
-  const double fr = -D.rhoi / D.rhow;
-  const double2 s00 = make_double2(__dmul_rn(fr, dice00.x), __dmul_rn(fr, dice00.y));
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < D.ncoef;
-       i += (long long)gridDim.x * blockDim.x) {
-    const double2 a = icelm[i], o = oldice[i];
-    const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
-    dice[i] = d;
-    const double2 pi = p_ice[i];
-    dI[i] = make_double2(__dadd_rn(pi.x, d.x), __dadd_rn(pi.y, d.y));
-    double2 g;
-    if (mode == 0) {
-      g = np_cmul(np_cdiv(cstarlm[i], c00), s00);
-    } else if (mode == 1) {
-      const double2 u = h1[i], v = h2[i];
-      g = make_double2(__dsub_rn(__dmul_rn(u.x, 2.0), v.x), __dsub_rn(__dmul_rn(u.y, 2.0), v.y));
-    } else {
-      const double2 u = h1[i], v = h2[i];
-      g = make_double2(__dsub_rn(__dmul_rn(u.x, c1), __dmul_rn(c2, v.x)),
-                       __dsub_rn(__dmul_rn(u.y, c1), __dmul_rn(c2, v.y)));
-    }
-    load[i] = g;
-    if (mode == 0) {
-      dScur[i] = make_double2(0.0, 0.0);
-    } else {
-      const double2 p = dSprev[i];
-      dScur[i] = make_double2(__dadd_rn(p.x, g.x), __dadd_rn(p.y, g.y));
-    }
-    acc += cabs_(g);
-  }
-  const double part = block_sum(acc, sh);
-  double tot;
-  if (last_block_total(part, partials, counter, &tot, sh)) {
-    if (threadIdx.x == 0) sc->so = tot;
-  }
-}
-
-// The rotation block (solver.py:910-975), one thread.
-__device__ void rotation_block(const Dev& D, const RotConst& C, const double2* dScur, const double2* dI,
-                               Scal* sc, double2 rot_out[3], double2 rr_out[3], bool write_state) {
-  const double2 s20 = dScur[D.i20], s21 = dScur[D.i21];
-  const double2 i20 = dI[D.i20], i21 = dI[D.i21];
+// The rotation block (solver.py:910-975) for the coming inner iteration, one thread; writes
+// il, m, Lambda, their increments and the degree-2 rotational sea-level / radial terms.
+__device__ void rotation_block(const Dev& D, const RotConst& C, const double2* dScur, const double2* dI, Scal* sc) {
+  // written by other blocks of the same kernel: read through L2
+  const double2 s20 = __ldcg(dScur + D.i20), s21 = __ldcg(dScur + D.i21);
+  const double2 i20 = __ldcg(dI + D.i20), i21 = __ldcg(dI + D.i21);
   const double z20r = __dadd_rn(__dmul_rn(C.rhow, s20.x), __dmul_rn(C.rhoi, i20.x));
   const double z21r = __dadd_rn(__dmul_rn(C.rhow, s21.x), __dmul_rn(C.rhoi, i21.x));
   const double z21i = __dadd_rn(__dmul_rn(C.rhow, s21.y), __dmul_rn(C.rhoi, i21.y));
@@ -317,17 +340,11 @@ __device__ void rotation_block(const Dev& D, const RotConst& C, const double2* d
   const double m1s = __dmul_rn(m1, m1), m2s = __dmul_rn(m2, m2), m3s = __dmul_rn(m3, m3);
   double lam[18];
   for (int q = 0; q < 18; ++q) lam[q] = 0.0;
-  // lam[0,0]
   lam[0] = __dmul_rn(C.r2w2_3, __dadd_rn(__dadd_rn(__dadd_rn(m1s, m2s), m3s), __dmul_rn(2.0, m3)));
-  lam[1] = 0.0;
-  // lam[2,0] at flat (2*3+0)*2
   lam[12] = __dmul_rn(C.r2w2_6s5, __dsub_rn(__dsub_rn(__dadd_rn(m1s, m2s), __dmul_rn(2.0, m3s)), __dmul_rn(4.0, m3)));
-  lam[13] = 0.0;
-  // lam[2,1] = -(r2w2/sqrt30) * ((m1 - i m2) * (1 + m3))
   const double op = __dadd_rn(1.0, m3);
   lam[14] = __dmul_rn(-C.r2w2_s30, __dmul_rn(m1, op));
   lam[15] = __dmul_rn(-C.r2w2_s30, __dmul_rn(-m2, op));
-  // lam[2,2] = (r2w2/sqrt120) * ((m2^2 - m1^2) + 2 i m1 m2)
   lam[16] = __dmul_rn(C.r2w2_s120, __dsub_rn(m2s, m1s));
   lam[17] = __dmul_rn(C.r2w2_s120, __dmul_rn(__dmul_rn(2.0, m1), m2));
   for (int q = 0; q < 3; ++q) {
@@ -335,41 +352,83 @@ __device__ void rotation_block(const Dev& D, const RotConst& C, const double2* d
     const double di = __dsub_rn(lam[13 + 2 * q], sc->dlam_prev2[2 * q + 1]);
     const double tr = __dadd_rn(sc->dlam_prev2[2 * q], dr);
     const double ti = __dadd_rn(sc->dlam_prev2[2 * q + 1], di);
-    rot_out[q] = make_double2(__ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, tr), sc->sum_tsl[2 * q]), C.gacc),
-                              __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, ti), sc->sum_tsl[2 * q + 1]), C.gacc));
-    rr_out[q] = make_double2(__ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, tr), sc->sum_trr[2 * q]), C.gacc),
-                             __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, ti), sc->sum_trr[2 * q + 1]), C.gacc));
-    if (write_state) {
-      sc->dlam_cur2[2 * q] = dr;
-      sc->dlam_cur2[2 * q + 1] = di;
-    }
+    sc->dsl_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, tr), sc->sum_tsl[2 * q]), C.gacc);
+    sc->dsl_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, ti), sc->sum_tsl[2 * q + 1]), C.gacc);
+    sc->rr_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, tr), sc->sum_trr[2 * q]), C.gacc);
+    sc->rr_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, ti), sc->sum_trr[2 * q + 1]), C.gacc);
+    sc->dlam_cur2[2 * q] = dr;
+    sc->dlam_cur2[2 * q + 1] = di;
   }
-  if (write_state) {
-    for (int q = 0; q < 9; ++q) {
-      sc->il[q] = il[q];
-      sc->dil[q] = __dsub_rn(il[q], sc->oldil[q]);
+  for (int q = 0; q < 9; ++q) {
+    sc->il[q] = il[q];
+    sc->dil[q] = __dsub_rn(il[q], sc->oldil[q]);
+  }
+  for (int q = 0; q < 3; ++q) {
+    sc->mm[q] = mm[q];
+    sc->dm[q] = __dsub_rn(mm[q], sc->oldm[q]);
+  }
+  for (int q = 0; q < 18; ++q) sc->lam[q] = lam[q];
+}
+
+// dice = I*_lm - old ; dI = p_ice + dice ; first guess of the load increment ; dS_cur ;
+// so = sum|load_inc|  (solver.py:868-905; extrap solver_opt.py:504-513); the last block also
+// evaluates the rotation block for the first inner iteration.
+// mode: 0 eustatic, 1 extrap uniform (2 h1 - h2), 2 extrap variable (c1 h1 - c2 h2)
+__global__ void k_pre_spec(Dev D, RotConst C, const double2* __restrict__ icelm, const double2* __restrict__ oldice,
+                           const double2* __restrict__ p_ice, const double2* __restrict__ cstarlm,
+                           const double2* __restrict__ dSprev, const double2* __restrict__ h1,
+                           const double2* __restrict__ h2, int mode, double c1, double c2,
+                           double2* __restrict__ dice, double2* __restrict__ dI, double2* __restrict__ load,
+                           double2* __restrict__ dScur, Scal* sc, double* partials, unsigned int* counter) {
+  __shared__ double sh[32];
+  double acc = 0.0;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < D.ncoef) {
+    const double2 dice00 = make_double2(__dsub_rn(icelm[0].x, oldice[0].x), __dsub_rn(icelm[0].y, oldice[0].y));
+    const double fr = -D.rhoi / D.rhow;
+    const double2 s00 = make_double2(__dmul_rn(fr, dice00.x), __dmul_rn(fr, dice00.y));
+    const double2 a = icelm[i], o = oldice[i];
+    const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
+    dice[i] = d;
+    const double2 pi = p_ice[i];
+    dI[i] = make_double2(__dadd_rn(pi.x, d.x), __dadd_rn(pi.y, d.y));
+    double2 g;
+    if (mode == 0) {
+      g = np_cmul(np_cdiv(cstarlm[i], cstarlm[0]), s00);
+    } else if (mode == 1) {
+      const double2 u = h1[i], v = h2[i];
+      g = make_double2(__dsub_rn(__dmul_rn(u.x, 2.0), v.x), __dsub_rn(__dmul_rn(u.y, 2.0), v.y));
+    } else {
+      const double2 u = h1[i], v = h2[i];
+      g = make_double2(__dsub_rn(__dmul_rn(u.x, c1), __dmul_rn(c2, v.x)),
+                       __dsub_rn(__dmul_rn(u.y, c1), __dmul_rn(c2, v.y)));
     }
-    for (int q = 0; q < 3; ++q) {
-      sc->mm[q] = mm[q];
-      sc->dm[q] = __dsub_rn(mm[q], sc->oldm[q]);
+    load[i] = g;
+    if (mode == 0) {
+      dScur[i] = make_double2(0.0, 0.0);
+    } else {
+      const double2 p = dSprev[i];
+      dScur[i] = make_double2(__dadd_rn(p.x, g.x), __dadd_rn(p.y, g.y));
     }
-    for (int q = 0; q < 18; ++q) sc->lam[q] = lam[q];
-    for (int q = 0; q < 3; ++q) {
-      sc->dsl_rot[2 * q] = rot_out[q].x;
-      sc->dsl_rot[2 * q + 1] = rot_out[q].y;
-      sc->rr_rot[2 * q] = rr_out[q].x;
-      sc->rr_rot[2 * q + 1] = rr_out[q].y;
+    acc = cabs_(g);
+  }
+  const double part = block_sum(acc, sh);
+  double tot;
+  if (last_block_total(part, partials, counter, &tot, sh)) {
+    if (threadIdx.x == 0) {
+      sc->so = tot;
+      if (D.tpw) rotation_block(D, C, dScur, dI, sc);
     }
   }
 }
 
-// Eq. B18 (solver.py:977-991) with the rotation block fused: the three threads owning
-// (l=2, m=0..2) evaluate it, the (2,0) thread records the rotational state.
-__global__ void k_b18(Dev D, RotConst C, const double2* __restrict__ dI, const double2* __restrict__ dSprev,
+// Eq. B18 (solver.py:977-991) plus the degree-2 rotational term of the current iteration.
+__global__ void k_b18(Dev D, const double2* __restrict__ dI, const double2* __restrict__ dSprev,
                       const double2* __restrict__ load, const double2* __restrict__ visc,
-                      const double2* __restrict__ dScur, double2* __restrict__ sl, Scal* sc) {
+                      double2* __restrict__ sl, Scal* sc) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef) return;
+  if (i == 0) sc->gr_changed = 0;  // the previous iteration's grounded-mask change is consumed
   const int l = D.lidx[i];
   const double2 a = dI[i], b = dSprev[i], c = load[i], v = visc[i];
   const double te = D.ttlekhl[l], t = D.ttl[l];
@@ -377,22 +436,24 @@ __global__ void k_b18(Dev D, RotConst C, const double2* __restrict__ dI, const d
   double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(b.y, D.rhow)), __dmul_rn(c.y, D.rhow));
   re = __dadd_rn(__dmul_rn(re, te), __dmul_rn(v.x, t));
   im = __dadd_rn(__dmul_rn(im, te), __dmul_rn(v.y, t));
-  if (D.tpw && (i == D.i20 || i == D.i21 || i == D.i22)) {
-    double2 rot[3], rr[3];
-    rotation_block(D, C, dScur, dI, sc, rot, rr, i == D.i20);
-    const int q = (i == D.i20) ? 0 : (i == D.i21) ? 1 : 2;
-    re = __dadd_rn(re, rot[q].x);
-    im = __dadd_rn(im, rot[q].y);
+  if (D.tpw) {
+    const int q = (i == D.i20) ? 0 : (i == D.i21) ? 1 : (i == D.i22) ? 2 : -1;
+    if (q >= 0) {
+      re = __dadd_rn(re, sc->dsl_rot[2 * q]);
+      im = __dadd_rn(im, sc->dsl_rot[2 * q + 1]);
+    }
   }
   sl[i] = make_double2(re, im);
 }
 
 // conserv, the load update and xi (solver.py:1002-1030):
 //   new = ((-dSprev + rO) + C*_lm conserv) - tO ;  dS_cur = dSprev + new ;  sa = sum|new|
-__global__ void k_update(Dev D, const double2* __restrict__ dSprev, const double2* __restrict__ rOlm,
+// The last block decides convergence and sets the graph loop condition.
+__global__ void k_update(Dev D, RotConst C, const double2* __restrict__ dSprev, const double2* __restrict__ rOlm,
                          const double2* __restrict__ cstarlm, const double2* __restrict__ tOlm,
                          const double2* __restrict__ dI, double2* __restrict__ load,
-                         double2* __restrict__ dScur, Scal* sc, double* partials, unsigned int* counter) {
+                         double2* __restrict__ dScur, Scal* sc, double* partials, unsigned int* counter,
+                         cudaGraphConditionalHandle loop) {
   __shared__ double sh[32];
   // conserv = ((1 / C*_00) * (-(rhoi/rhow) dI_00 - rO_00 + tO_00)).real
   const double2 c00 = cstarlm[0];
@@ -403,8 +464,8 @@ __global__ void k_update(Dev D, const double2* __restrict__ dSprev, const double
                                  __dadd_rn(__dsub_rn(__dmul_rn(fr, d00.y), r00.y), t00.y));
   const double conserv = __dsub_rn(__dmul_rn(rinv.x, x.x), __dmul_rn(rinv.y, x.y));
   double acc = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < D.ncoef;
-       i += (long long)gridDim.x * blockDim.x) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < D.ncoef) {
     const double2 p = dSprev[i], r = rOlm[i], c = cstarlm[i], t = tOlm[i];
     double nr = __dadd_rn(-p.x, r.x), ni = __dadd_rn(-p.y, r.y);
     nr = __dadd_rn(nr, __dmul_rn(c.x, conserv));
@@ -413,7 +474,7 @@ __global__ void k_update(Dev D, const double2* __restrict__ dSprev, const double
     ni = __dsub_rn(ni, t.y);
     load[i] = make_double2(nr, ni);
     dScur[i] = make_double2(__dadd_rn(p.x, nr), __dadd_rn(p.y, ni));
-    acc += hypot(nr, ni);
+    acc = hypot(nr, ni);
   }
   const double part = block_sum(acc, sh);
   double sa;
@@ -438,6 +499,7 @@ __global__ void k_update(Dev D, const double2* __restrict__ dSprev, const double
         sc->status = SLE_ERR_NONCONVERGED;
         sc->converged = 1;
       }
+      if (loop) cudaGraphSetConditional(loop, sc->converged ? 0u : 1u);
     }
   }
 }
@@ -452,8 +514,10 @@ __global__ void k_sltot(Dev D, const double2* __restrict__ sl, double2* __restri
 }
 
 // deltasl (dsl identity) and, when not converged, topography / ocean function refresh and
-// the grounded-ice test on the new topography (solver.py:1032-1037, 661-684).
-__global__ void k_refresh1(Dev D, const double* __restrict__ dsl, double* __restrict__ deltasl,
+// the grounded-ice test on the new topography (solver.py:1032-1037, 661-684).  One extra block
+// (the last) evaluates the rotation block of the next iteration meanwhile.
+__global__ void k_refresh1(Dev D, RotConst C, const double2* __restrict__ dScur, const double2* __restrict__ dI,
+                           const double* __restrict__ dsl, double* __restrict__ deltasl,
                            const double* __restrict__ tinit, double* __restrict__ topo,
                            double* __restrict__ cxy, const double* __restrict__ ice,
                            const double* __restrict__ beta, double* __restrict__ grnew, Scal* sc,
@@ -463,24 +527,32 @@ __global__ void k_refresh1(Dev D, const double* __restrict__ dsl, double* __rest
   const bool test = !conv && D.checkmarine && sc->gr_nacc < GR_MAXACC;
   const double cadd = D.opt_dsl ? __dmul_rn(sc->conserv, sc->K00) : 0.0;
   double cnt = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < D.ng;
-       i += (long long)gridDim.x * blockDim.x) {
-    double ds;
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0 && !conv && D.tpw) rotation_block(D, C, dScur, dI, sc);
+  const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (2 * h < D.ng) {
+    double ds[2];
     if (D.opt_dsl) {
-      ds = __dadd_rn(dsl[i], cadd);
-      deltasl[i] = ds;
+      const double2 a = ld2(dsl, h);
+      ds[0] = __dadd_rn(a.x, cadd);
+      ds[1] = __dadd_rn(a.y, cadd);
+      st2(deltasl, h, ds[0], ds[1]);
     } else {
-      ds = deltasl[i];
+      const double2 a = ld2(deltasl, h);
+      ds[0] = a.x;
+      ds[1] = a.y;
     }
     if (!conv) {
-      const double t = __dsub_rn(tinit[i], ds);
-      topo[i] = t;
-      cxy[i] = (t < 0.0) ? 1.0 : 0.0;
+      const double2 ti = ld2(tinit, h);
+      const double t0 = __dsub_rn(ti.x, ds[0]), t1 = __dsub_rn(ti.y, ds[1]);
+      st2(topo, h, t0, t1);
+      st2(cxy, h, (t0 < 0.0) ? 1.0 : 0.0, (t1 < 0.0) ? 1.0 : 0.0);
       if (test) {
-        const double g = icestar_on(ice[i], t, D.rhow, D.rhoi);
-        grnew[i] = g;
-        const bool bnew = g < EPS0;
-        if (bnew != (beta[i] != 0.0)) cnt += 1.0;
+        const double2 ic = ld2(ice, h), be = ld2(beta, h);
+        const double g0 = icestar_on(ic.x, t0, D.rhow, D.rhoi);
+        const double g1 = icestar_on(ic.y, t1, D.rhow, D.rhoi);
+        st2(grnew, h, g0, g1);
+        if ((g0 < EPS0) != (be.x != 0.0)) cnt += 1.0;
+        if ((g1 < EPS0) != (be.y != 0.0)) cnt += 1.0;
       }
     }
   }
@@ -506,31 +578,39 @@ __global__ void k_refresh1(Dev D, const double* __restrict__ dsl, double* __rest
 __global__ void k_refresh2(Dev D, const double* __restrict__ cxy, const double* __restrict__ tinit,
                            const double* __restrict__ cstar0, const double* __restrict__ grnew,
                            double* __restrict__ icestar, double* __restrict__ beta,
-                           double* __restrict__ cstar, double* __restrict__ tO, int changed) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= D.ng) return;
-  double b;
+                           double* __restrict__ cstar, double* __restrict__ tO, const Scal* sc) {
+  const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (2 * h >= D.ng || sc->converged) return;
+  const int changed = sc->gr_changed;
+  double2 b;
   if (changed) {
-    const double g = grnew[i];
-    icestar[i] = g;
-    b = (g < EPS0) ? 1.0 : 0.0;
-    beta[i] = b;
+    const double2 g = ld2(grnew, h);
+    st2(icestar, h, g.x, g.y);
+    b = make_double2((g.x < EPS0) ? 1.0 : 0.0, (g.y < EPS0) ? 1.0 : 0.0);
+    st2(beta, h, b.x, b.y);
   } else {
-    b = beta[i];
+    b = ld2(beta, h);
   }
-  const double c = __dmul_rn(cxy[i], b);
-  cstar[i] = c;
-  tO[i] = __dmul_rn(tinit[i], __dsub_rn(c, cstar0[i]));
+  const double2 cx = ld2(cxy, h), ti = ld2(tinit, h), c0 = ld2(cstar0, h);
+  const double c_0 = __dmul_rn(cx.x, b.x), c_1 = __dmul_rn(cx.y, b.y);
+  st2(cstar, h, c_0, c_1);
+  st2(tO, h, __dmul_rn(ti.x, __dsub_rn(c_0, c0.x)), __dmul_rn(ti.y, __dsub_rn(c_1, c0.y)));
 }
 
-__global__ void k_dice(Dev D, const double2* __restrict__ icelm, const double2* __restrict__ oldice,
-                       const double2* __restrict__ p_ice, double2* __restrict__ dice, double2* __restrict__ dI) {
+// dice, dI after a grounded-mask change; the last block re-evaluates the rotation block
+__global__ void k_dice(Dev D, RotConst C, const double2* __restrict__ icelm, const double2* __restrict__ oldice,
+                       const double2* __restrict__ p_ice, double2* __restrict__ dice, double2* __restrict__ dI,
+                       const double2* __restrict__ dScur, Scal* sc, unsigned int* counter) {
+  if (sc->converged || !sc->gr_changed) return;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= D.ncoef) return;
-  const double2 a = icelm[i], o = oldice[i], p = p_ice[i];
-  const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
-  dice[i] = d;
-  dI[i] = make_double2(__dadd_rn(p.x, d.x), __dadd_rn(p.y, d.y));
+  if (i < D.ncoef) {
+    const double2 a = icelm[i], o = oldice[i], p = p_ice[i];
+    const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
+    dice[i] = d;
+    dI[i] = make_double2(__dadd_rn(p.x, d.x), __dadd_rn(p.y, d.y));
+  }
+  if (!D.tpw) return;
+  if (last_block(counter) && threadIdx.x == 0) rotation_block(D, C, dScur, dI, sc);
 }
 
 // Radial displacement spectrum (solver.py:1054-1069)
@@ -538,7 +618,7 @@ __global__ void k_rr(Dev D, const double2* __restrict__ dI, const double2* __res
                      const double2* __restrict__ load, const double2* __restrict__ rad,
                      double2* __restrict__ rr, const Scal* sc) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= D.ncoef) return;
+  if (i >= D.ncoef || sc->status) return;
   const int l = D.lidx[i];
   const double2 a = dI[i], b = dSprev[i], c = load[i], v = rad[i];
   const double th = D.ttlhe[l], t = D.ttl[l];
@@ -547,10 +627,7 @@ __global__ void k_rr(Dev D, const double2* __restrict__ dI, const double2* __res
   re = __dadd_rn(__dmul_rn(re, th), __dmul_rn(v.x, t));
   im = __dadd_rn(__dmul_rn(im, th), __dmul_rn(v.y, t));
   if (D.tpw) {
-    int q = -1;
-    if (i == D.i20) q = 0;
-    else if (i == D.i21) q = 1;
-    else if (i == D.i22) q = 2;
+    const int q = (i == D.i20) ? 0 : (i == D.i21) ? 1 : (i == D.i22) ? 2 : -1;
     if (q >= 0) {
       re = __dadd_rn(re, sc->rr_rot[2 * q]);
       im = __dadd_rn(im, sc->rr_rot[2 * q + 1]);
@@ -560,14 +637,20 @@ __global__ void k_rr(Dev D, const double2* __restrict__ dI, const double2* __res
 }
 
 // commit (solver.py:1080-1096): cur = rhoi dice + rhow load (l = 0 zeroed); p_load += cur;
-// p_ice = dI ; p_ocean = dS_cur ; prev_ice = I*_lm ; extrap history h_new = load
+// p_ice = dI ; p_ocean = dS_cur ; prev_ice = I*_lm ; extrap history h_new = load; thread 0
+// also commits the rotational increments.
 __global__ void k_commit(Dev D, const double2* __restrict__ dice, const double2* __restrict__ load,
                          const double2* __restrict__ dI, const double2* __restrict__ dScur,
                          const double2* __restrict__ icelm, double2* __restrict__ p_load,
                          double2* __restrict__ p_ice, double2* __restrict__ p_ocean,
-                         double2* __restrict__ prev_ice, double2* __restrict__ hist_new) {
+                         double2* __restrict__ prev_ice, double2* __restrict__ hist_new, Scal* sc) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= D.ncoef) return;
+  if (i >= D.ncoef || sc->status) return;
+  if (i == 0 && D.tpw) {
+    for (int q = 0; q < 9; ++q) sc->p_il[q] = __dadd_rn(sc->p_il[q], sc->dil[q]);
+    for (int q = 0; q < 3; ++q) sc->p_m[q] = __dadd_rn(sc->p_m[q], sc->dm[q]);
+    for (int q = 0; q < 6; ++q) sc->p_lambda[q] = __dadd_rn(sc->p_lambda[q], sc->dlam_cur2[q]);
+  }
   const int l = D.lidx[i];
   double2 cur = make_double2(0.0, 0.0);
   const double2 ld = load[i];
@@ -584,44 +667,45 @@ __global__ void k_commit(Dev D, const double2* __restrict__ dice, const double2*
   if (hist_new) hist_new[i] = ld;
 }
 
-__global__ void k_rot_commit(Scal* sc) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  for (int q = 0; q < 9; ++q) sc->p_il[q] = __dadd_rn(sc->p_il[q], sc->dil[q]);
-  for (int q = 0; q < 3; ++q) sc->p_m[q] = __dadd_rn(sc->p_m[q], sc->dm[q]);
-  for (int q = 0; q < 6; ++q) sc->p_lambda[q] = __dadd_rn(sc->p_lambda[q], sc->dlam_cur2[q]);
-}
-
 // Post-step topography / ocean function (solver.py:1099-1101) and, for the diag option, the
-// row sums of the four degree-0 diagnostics (solver_opt.py:893-916): block per row.
+// row sums of the four degree-0 diagnostics (solver_opt.py:893-916): block per row; the last
+// block forms U00 = sum_j P~_00 w_j rowsum_j / (nlon 1.41421356), P~_00 = sqrt(0.5).
 __global__ void k_post_grid(Dev D, const double* __restrict__ tinit, const double* __restrict__ deltasl,
                             const double* __restrict__ beta, double* __restrict__ topo,
                             double* __restrict__ topo_prev, double* __restrict__ cxy,
                             double* __restrict__ slc, double* __restrict__ slcb, double* __restrict__ cstar,
-                            double* __restrict__ rows /* [4][nlat] or null */) {
+                            double* __restrict__ rows /* [4][nlat] or null */, const double* __restrict__ w,
+                            Scal* sc, unsigned int* counter) {
   __shared__ double sh[32];
   const int j = blockIdx.x;
+  if (sc->status) return;
   double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
-  for (int t = threadIdx.x; t < D.nlon; t += blockDim.x) {
-    const size_t i = (size_t)j * D.nlon + t;
-    const double ds = deltasl[i];
-    const double tp = __dsub_rn(tinit[i], ds);
-    topo[i] = tp;
-    topo_prev[i] = tp;
-    const double o = (tp < 0.0) ? 1.0 : 0.0;
-    cxy[i] = o;
-    const double s1 = __dmul_rn(ds, o);
-    const double bb = beta[i];
-    const double s2 = __dmul_rn(s1, bb);
-    const double cs = __dmul_rn(o, bb);
-    if (slc) {
-      slc[i] = s1;
-      slcb[i] = s2;
-      cstar[i] = cs;
+  const long long row = (long long)j * (D.nlon / 2);
+  for (int t = threadIdx.x; t < D.nlon / 2; t += blockDim.x) {
+    const long long h = row + t;
+    const double2 ds = ld2(deltasl, h), ti = ld2(tinit, h), bb = ld2(beta, h);
+    const double dsv[2] = {ds.x, ds.y}, tiv[2] = {ti.x, ti.y}, bv[2] = {bb.x, bb.y};
+    double tp[2], o[2], s1[2], s2[2], cs[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      tp[u] = __dsub_rn(tiv[u], dsv[u]);
+      o[u] = (tp[u] < 0.0) ? 1.0 : 0.0;
+      s1[u] = __dmul_rn(dsv[u], o[u]);
+      s2[u] = __dmul_rn(s1[u], bv[u]);
+      cs[u] = __dmul_rn(o[u], bv[u]);
+      a += s1[u];
+      b += o[u];
+      c += s2[u];
+      d += cs[u];
     }
-    a += s1;
-    b += o;
-    c += s2;
-    d += cs;
+    st2(topo, h, tp[0], tp[1]);
+    st2(topo_prev, h, tp[0], tp[1]);
+    st2(cxy, h, o[0], o[1]);
+    if (slc) {
+      st2(slc, h, s1[0], s1[1]);
+      st2(slcb, h, s2[0], s2[1]);
+      st2(cstar, h, cs[0], cs[1]);
+    }
   }
   if (!rows) return;
   a = block_sum(a, sh);
@@ -634,14 +718,10 @@ __global__ void k_post_grid(Dev D, const double* __restrict__ tinit, const doubl
     rows[2 * D.nlat + j] = c;
     rows[3 * D.nlat + j] = d;
   }
-}
-
-// degree-0 coefficient U00 = sum_j P~_00 w_j rowsum_j / (nlon 1.41421356), P~_00 = sqrt(0.5)
-__global__ void k_degree0(Dev D, const double* rows, const double* w, Scal* sc) {
-  __shared__ double sh[32];
+  if (!last_block(counter)) return;
   for (int q = 0; q < 4; ++q) {
     double acc = 0.0;
-    for (int j = threadIdx.x; j < D.nlat; j += blockDim.x) acc += w[j] * rows[q * D.nlat + j];
+    for (int jj = threadIdx.x; jj < D.nlat; jj += blockDim.x) acc += w[jj] * ((volatile double*)rows)[q * D.nlat + jj];
     acc = block_sum(acc, sh);
     if (threadIdx.x == 0) sc->diag[q] = sqrt(0.5) * acc / (double)D.nlon / SQRT2_LEGACY;
     __syncthreads();
@@ -701,6 +781,7 @@ struct sle_solver {
   Scal* sc;
   Scal* hsc;  // pinned mirror
   double* partials;
+  long long part_grid;   // offset of the grid-reduction partials
   unsigned int* counter;
   unsigned int* badflag;
   double K00;
@@ -708,6 +789,12 @@ struct sle_solver {
   double dt_cur, dt_hist[2];
   double ocean_area0, oceanBeta_area0, ice_volume0;
   sle_step_info last;
+  // inner loop as a CUDA graph with a device-evaluated WHILE condition
+  cudaGraph_t loop_graph;
+  cudaGraphExec_t loop_exec;
+  cudaGraphConditionalHandle loop_cond;
+  int use_graph;
+  long long body_launches;   // kernels in one iteration of the graph body
 };
 
 namespace {
@@ -738,6 +825,8 @@ void solver_free(sle_solver* s) {
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (s->hsc) cudaFreeHost(s->hsc);
+  if (s->loop_exec) cudaGraphExecDestroy(s->loop_exec);
+  if (s->loop_graph) cudaGraphDestroy(s->loop_graph);
   if (s->st) cudaStreamDestroy(s->st);
   if (s->plan) sle_sht_destroy(s->plan);
   delete s;
@@ -794,6 +883,98 @@ int syn(sle_solver* s, const double2* c, double* g, const SynEpilogue* epi = nul
 double fourpiR2(const sle_solver* s, double x) {
   // x * 4 * PI * radius**2 with the reference's left-to-right association
   return ((x * 4.0) * PI_LEGACY) * std::pow(s->cfg.radius, 2);
+}
+
+// One inner iteration (solver.py:909-1045) as a fixed kernel sequence: every decision is read
+// on the device, so the same sequence serves the host-driven loop and the graph body.
+int enqueue_iteration(sle_solver* s, cudaGraphConditionalHandle loop) {
+  const Dev& D = s->D;
+  cudaStream_t st = s->st;
+  const long long nc = D.ncoef, ng = D.ng;
+  note_launch();
+  k_b18<<<nb(nc), 256, 0, st>>>(D, s->dI, s->p_ocean, s->load, s->visc, s->sl, s->sc);
+  SynEpilogue epi{s->rO, s->cstar};
+  SLE_TRY(syn(s, s->sl, s->dsl, &epi));
+  SLE_TRY(ana(s, 1, s->rO, s->rOlm));
+  note_launch();
+  k_update<<<nb(nc), 256, 0, st>>>(D, s->C, s->p_ocean, s->rOlm, s->cstarlm, s->tOlm, s->dI, s->load, s->dScur,
+                                   s->sc, s->partials, s->counter, loop);
+  if (!s->cfg.opt_dsl) {
+    note_launch();
+    k_sltot<<<nb(nc), 256, 0, st>>>(D, s->sl, s->sltot, s->sc);
+    SLE_TRY(syn(s, s->sltot, s->deltasl));
+  }
+  note_launch(2);
+  k_refresh1<<<nb(ng / 2) + 1, 256, 0, st>>>(D, s->C, s->dScur, s->dI, s->dsl, s->deltasl, s->tinit, s->topo,
+                                             s->cxy, s->ice, s->beta,
+                                         s->grnew, s->sc, s->partials + s->part_grid, s->counter + 1);
+  k_refresh2<<<nb(ng / 2), 256, 0, st>>>(D, s->cxy, s->tinit, s->cstar0, s->grnew, s->icestar, s->beta, s->cstar,
+                                     s->tO, s->sc);
+  // I* (only when the grounded mask changed), C* and tO for the next iteration; skipped once
+  // the iteration has converged
+  AnaGate gate{&s->sc->converged, &s->sc->gr_changed, 0x7u, 0x1u};
+  const double* g3[3] = {s->icestar, s->cstar, s->tO};
+  double2* o3[3] = {s->icelm, s->cstarlm, s->tOlm};
+  SLE_TRY(sht_analysis_packed(s->plan, 3, g3, o3, st, &gate));
+  note_launch();
+  k_dice<<<nb(nc), 256, 0, st>>>(D, s->C, s->icelm, s->oldice, s->p_ice, s->dice, s->dI, s->dScur, s->sc,
+                                 s->counter + 2);
+  SLE_CUDA(cudaGetLastError());
+  return SLE_OK;
+}
+
+int build_loop_graph(sle_solver* s) {
+  cudaGraph_t g = nullptr;
+  SLE_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1u, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_error("cudaGraphConditionalHandleCreate: %s", cudaGetErrorString(e));
+    return SLE_ERR_CUDA;
+  }
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_error("cudaGraphAddNode(conditional): %s", cudaGetErrorString(e));
+    return SLE_ERR_CUDA;
+  }
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(s->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_error("cudaStreamBeginCaptureToGraph: %s", cudaGetErrorString(e));
+    return SLE_ERR_CUDA;
+  }
+  const long long before = sle_launch_count();
+  const int rc = enqueue_iteration(s, h);
+  s->body_launches = sle_launch_count() - before;
+  note_launch(-(int)s->body_launches);  // counted per executed iteration at the end of each step
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(s->st, &captured);
+  if (rc != SLE_OK || e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    if (rc != SLE_OK) return rc;
+    set_error("cudaStreamEndCapture: %s", cudaGetErrorString(e));
+    return SLE_ERR_CUDA;
+  }
+  cudaGraphExec_t ex = nullptr;
+  e = cudaGraphInstantiate(&ex, g, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_error("cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    return SLE_ERR_CUDA;
+  }
+  s->loop_graph = g;
+  s->loop_exec = ex;
+  s->loop_cond = h;
+  return SLE_OK;
 }
 
 }  // namespace
@@ -878,6 +1059,11 @@ extern "C" int sle_solver_create(const sle_config* cfg, const sle_earth* earth, 
   }
   TRYC(cudaMemcpy(s->nmod, nm.data(), sizeof(int) * nl, cudaMemcpyHostToDevice));
   s->nmod2 = nl > 2 ? nm[2] : 0;
+  if (s->nmod2 > 64) {
+    set_error("sle_solver_create: %d relaxation modes at degree 2 (at most 64 supported)", s->nmod2);
+    solver_free(s);
+    return SLE_ERR_UNSUPPORTED;
+  }
   // grids
   double** grids[] = {&s->tinit, &s->cxy0, &s->beta0, &s->cstar0, &s->cxy, &s->topo_prev, &s->icestar, &s->beta,
                       &s->cstar, &s->tO, &s->rO, &s->dsl, &s->deltasl, &s->topo, &s->rr, &s->grnew, &s->ice,
@@ -891,7 +1077,8 @@ extern "C" int sle_solver_create(const sle_config* cfg, const sle_earth* earth, 
   for (double2** p : specs) TRY(dalloc(p, nc));
   TRY(dalloc(&s->R, (size_t)K * nc + 1));
   TRY(dalloc(&s->sc, 1));
-  TRY(dalloc(&s->partials, 4096));
+  s->part_grid = (long long)nb(nc) + 32;
+  TRY(dalloc(&s->partials, (size_t)s->part_grid + nb(ng / 2) + 64));
   TRY(dalloc(&s->counter, 4));
   TRY(dalloc(&s->badflag, 1));
   TRYC(cudaMallocHost(reinterpret_cast<void**>(&s->hsc), sizeof(Scal)));
@@ -951,6 +1138,12 @@ extern "C" int sle_solver_create(const sle_config* cfg, const sle_earth* earth, 
   C.rhoi = cfg->rhoi;
   C.rhow = cfg->rhow;
   s->dt_cur = -1.0;
+  // SLEVOLVE_B200_HOST_LOOP=1 drives the inner loop from the host (same kernels; used to profile
+  // the loop body, whose kernels profilers do not report inside conditional graph nodes)
+  {
+    const char* e = std::getenv("SLEVOLVE_B200_HOST_LOOP");
+    s->use_graph = !(e && e[0] == '1');
+  }
   TRY(set_dt(s, cfg->dt_years));
   TRYC(cudaStreamSynchronize(s->st));
   *out = s;
@@ -1056,13 +1249,11 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
   // ---- modal advance (solver.py:835)
   note_launch();
   ProfToken tadv = prof_begin(PROF_ADVANCE, 1, st);
-  k_advance<<<nb(nc), 256, 0, st>>>(D, s->R, s->p_load, s->visc, s->rad);
+  k_advance<<<nb(nc) + 1, 256, 0, st>>>(D, s->R, s->p_load, s->visc, s->rad, s->sc, s->r_il, s->r_m, s->r_lam);
   prof_end(tadv, st);
-  note_launch();
-  k_rot_advance<<<1, 1, 0, st>>>(D, s->sc, s->r_il, s->r_m, s->r_lam);
   // ---- ice and ocean grids, their analyses
   note_launch();
-  k_ice_grid<<<nb(ng), 256, 0, st>>>(D, s->ice, s->topo_prev, s->cxy, s->tinit, s->cstar0, s->icestar, s->beta,
+  k_ice_grid<<<nb(ng / 2), 256, 0, st>>>(D, s->ice, s->topo_prev, s->cxy, s->tinit, s->cstar0, s->icestar, s->beta,
                                      s->cstar, s->tO, s->ice_prev, it == 1 ? s->tmpg : nullptr, s->sc);
   SLE_CUDA(cudaGetLastError());
   if (it == 1) {
@@ -1085,62 +1276,30 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
       c2 = dt0 / dt2 * w;
     }
   }
-  const unsigned red_blocks = std::min<unsigned>(RED_BLOCKS, nb(nc));
   note_launch();
-  k_pre_spec<<<red_blocks, 256, 0, st>>>(D, s->icelm, s->oldice, s->p_ice, s->cstarlm, s->p_ocean, s->h1, s->h2,
+  k_pre_spec<<<nb(nc), 256, 0, st>>>(D, s->C, s->icelm, s->oldice, s->p_ice, s->cstarlm, s->p_ocean, s->h1, s->h2,
                                          mode, c1, c2, s->dice, s->dI, s->load, s->dScur, s->sc, s->partials,
                                          s->counter);
   SLE_CUDA(cudaGetLastError());
 
-  // ---- inner fixed-point loop (solver.py:907-1051)
-  const unsigned red_grid = std::min<unsigned>(RED_BLOCKS, nb(ng));
-  for (int host_iter = 0;; ++host_iter) {
-    if (host_iter > MAX_INNER + 2) {  // the device flag must have stopped the loop by now
-      set_error("inner loop control lost (device iteration counter did not advance)");
-      return SLE_ERR_STATE;
+  // ---- inner fixed-point loop (solver.py:907-1051): a CUDA graph whose WHILE condition
+  // is set by k_update (converged, 9999-iteration cap or non-finite value all stop it); with
+  // per-kernel profiling on, the same sequence is driven from the host.
+  const bool graph_step = s->use_graph && !prof_enabled();
+  if (graph_step) {
+    if (!s->loop_exec) SLE_TRY(build_loop_graph(s));
+    SLE_CUDA(cudaGraphLaunch(s->loop_exec, st));
+  } else {
+    for (int host_iter = 0;; ++host_iter) {
+      if (host_iter > MAX_INNER + 2) {  // the device flag must have stopped the loop by now
+        set_error("inner loop control lost (device iteration counter did not advance)");
+        return SLE_ERR_STATE;
+      }
+      SLE_TRY(enqueue_iteration(s, 0));
+      SLE_TRY(sync_scal(s));
+      const Scal& h = *s->hsc;
+      if (h.converged || h.status != 0) break;
     }
-    note_launch();
-    k_b18<<<nb(nc), 256, 0, st>>>(D, s->C, s->dI, s->p_ocean, s->load, s->visc, s->dScur, s->sl, s->sc);
-    SynEpilogue epi{s->rO, s->cstar};
-    SLE_TRY(syn(s, s->sl, s->dsl, &epi));
-    SLE_TRY(ana(s, 1, s->rO, s->rOlm));
-    note_launch();
-    k_update<<<red_blocks, 256, 0, st>>>(D, s->p_ocean, s->rOlm, s->cstarlm, s->tOlm, s->dI, s->load, s->dScur,
-                                         s->sc, s->partials, s->counter);
-    if (!s->cfg.opt_dsl) {
-      note_launch();
-      k_sltot<<<nb(nc), 256, 0, st>>>(D, s->sl, s->sltot, s->sc);
-      SLE_TRY(syn(s, s->sltot, s->deltasl));
-    }
-    note_launch();
-    k_refresh1<<<red_grid, 256, 0, st>>>(D, s->dsl, s->deltasl, s->tinit, s->topo, s->cxy, s->ice, s->beta,
-                                         s->grnew, s->sc, s->partials + 2048, s->counter + 1);
-    SLE_CUDA(cudaGetLastError());
-    SLE_TRY(sync_scal(s));
-    const Scal& h = *s->hsc;
-    if (h.converged || h.status != 0) break;
-    const int changed = h.gr_changed;
-    note_launch();
-    k_refresh2<<<nb(ng), 256, 0, st>>>(D, s->cxy, s->tinit, s->cstar0, s->grnew, s->icestar, s->beta, s->cstar,
-                                       s->tO, changed);
-    if (changed) {
-      SLE_TRY(ana(s, 3, s->icestar, s->icelm, s->cstar, s->cstarlm, s->tO, s->tOlm));
-      note_launch();
-      k_dice<<<nb(nc), 256, 0, st>>>(D, s->icelm, s->oldice, s->p_ice, s->dice, s->dI);
-      SLE_CUDA(cudaMemsetAsync(&s->sc->gr_changed, 0, sizeof(int), st));
-    } else {
-      SLE_TRY(ana(s, 2, s->cstar, s->cstarlm, s->tO, s->tOlm));
-    }
-    SLE_CUDA(cudaGetLastError());
-  }
-  const Scal& h = *s->hsc;
-  if (h.status != SLE_OK) {
-    if (h.status == SLE_ERR_NONCONVERGED)
-      set_error("inner loop failed to converge, xi=%.17g", h.xi);
-    else
-      set_error("non-finite value in the inner loop (xi=%g)", h.xi);
-    s->last.status = h.status;
-    return h.status;
   }
 
   // ---- radial displacement (solver.py:1054-1072)
@@ -1153,28 +1312,16 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
   double2* hist_new = s->cfg.inner_extrap ? s->h2 : nullptr;
   note_launch();
   k_commit<<<nb(nc), 256, 0, st>>>(D, s->dice, s->load, s->dI, s->dScur, s->icelm, s->p_load, s->p_ice, s->p_ocean,
-                                   s->prev_ice, hist_new);
-  if (D.tpw) note_launch();
-  if (D.tpw) k_rot_commit<<<1, 1, 0, st>>>(s->sc);
-  if (s->cfg.inner_extrap) {
-    double2* t = s->h1;
-    s->h1 = s->h2;
-    s->h2 = t;
-    s->dt_hist[1] = s->dt_hist[0];
-    s->dt_hist[0] = dt;
-    s->nhist = std::min(2, s->nhist + 1);
-  }
+                                   s->prev_ice, hist_new, s->sc);
   // ---- topography / ocean function and the degree-0 diagnostics
   if (s->cfg.opt_diag) {
     note_launch();
     k_post_grid<<<D.nlat, 256, 0, st>>>(D, s->tinit, s->deltasl, s->beta, s->topo, s->topo_prev, s->cxy, nullptr,
-                                        nullptr, nullptr, s->rows);
-    note_launch();
-    k_degree0<<<1, 256, 0, st>>>(D, s->rows, s->plan->d.w, s->sc);
+                                        nullptr, nullptr, s->rows, s->plan->d.w, s->sc, s->counter + 3);
   } else {
     note_launch();
     k_post_grid<<<D.nlat, 256, 0, st>>>(D, s->tinit, s->deltasl, s->beta, s->topo, s->topo_prev, s->cxy, s->tmpg,
-                                        s->gbuf3, s->gbuf4, nullptr);
+                                        s->gbuf3, s->gbuf4, nullptr, s->plan->d.w, s->sc, s->counter + 3);
     SLE_TRY(ana(s, 4, s->tmpg, s->spare[0], s->cxy, s->spare[1], s->gbuf3, s->spare[2], s->gbuf4, s->spare[3]));
   }
   SLE_CUDA(cudaGetLastError());
@@ -1186,6 +1333,23 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
   SLE_CUDA(cudaMemcpyAsync(&ice00, s->icelm, sizeof(double2), cudaMemcpyDeviceToHost, st));
   SLE_TRY(sync_scal(s));
   const Scal& f = *s->hsc;
+  if (graph_step) note_launch((int)(f.numiter * s->body_launches));
+  if (f.status != SLE_OK) {
+    if (f.status == SLE_ERR_NONCONVERGED)
+      set_error("inner loop failed to converge, xi=%.17g", f.xi);
+    else
+      set_error("non-finite value in the inner loop (xi=%g)", f.xi);
+    s->last.status = f.status;
+    return f.status;
+  }
+  if (s->cfg.inner_extrap) {
+    double2* t = s->h1;
+    s->h1 = s->h2;
+    s->h2 = t;
+    s->dt_hist[1] = s->dt_hist[0];
+    s->dt_hist[0] = dt;
+    s->nhist = std::min(2, s->nhist + 1);
+  }
   double slc_ocn00, c00, slc_b00, cst00;
   if (s->cfg.opt_diag) {
     slc_ocn00 = f.diag[0];

@@ -68,6 +68,22 @@ def test_roundtrip(n, L):
     assert np.abs(g2 - g).max() / np.abs(g).max() < 1e-12
 
 
+def test_more_than_eight_latitude_groups():
+    """640 latitudes = 10 groups of 32: the analysis runs in two passes per segment."""
+    from oracle.sht import OracleSHT
+
+    rng = np.random.default_rng(13)
+    n, nlon, L = 640, 1024, 100
+    s = _sht(n, L, nlon)
+    o = OracleSHT(n, nlon, L)
+    g = rng.standard_normal((n, nlon))
+    ref = o.analysis(g)
+    assert np.abs(s.analysis(g) - ref).max() <= REL * np.abs(ref).max()
+    c = np.tril(rng.standard_normal((L + 1, L + 1)) + 1j * rng.standard_normal((L + 1, L + 1)))
+    ref = o.synthesis(c)
+    assert np.abs(s.synthesis(c) - ref).max() <= REL * np.abs(ref).max()
+
+
 def test_nyquist_order_and_small_lmax():
     """lmax = nlon/2 (the Nyquist order kept by the reference numpy backend) and lmax < nlat-1."""
     from oracle.sht import OracleSHT
