@@ -42,8 +42,16 @@ enum sle_status {
   SLE_ERR_NONCONVERGED = 5,  /* RuntimeError at 9999 inner iterations (solver.py:1049-1050) */
   SLE_ERR_NONFINITE = 6,     /* NaN / Inf met in the inner loop or in the inputs */
   SLE_ERR_UNSUPPORTED = 7,   /* an option of the reference this build does not provide */
-  SLE_ERR_STATE = 8          /* call out of order (e.g. step before init) */
+  SLE_ERR_STATE = 8,         /* call out of order (e.g. step before init) */
+  SLE_ERR_TIMEOUT = 9        /* a device-side wait gave up (bounded waits; results invalid) */
 };
+
+/* Arithmetic of the transforms.  FP64: FP64 end to end (matches the reference to 1e-9 m).
+ * MIXED: Legendre contractions as split-TF32 (3xTF32) tensor-core GEMMs with FP32
+ * accumulation (operands rounded to FP32 before the split); the Legendre recurrence, row FFTs,
+ * Gauss nodes and weights, the degree-0 coefficient and everything outside the transforms stay
+ * FP64. */
+enum sle_precision { SLE_PREC_FP64 = 0, SLE_PREC_MIXED = 1 };
 
 enum sle_layout { SLE_LAYOUT_DENSE = 0, SLE_LAYOUT_PACKED = 1 };
 
@@ -81,6 +89,9 @@ int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* coeffs_dev,
  * by the caller. */
 int sle_sht_analysis_noalloc(sle_sht* plan, const double* grid_dev, void* coeffs_packed_dev,
                              void* stream);
+/* Select the arithmetic of sle_sht_analysis / sle_sht_synthesis on this plan (default FP64).
+ * MIXED needs nlat a multiple of 64 and lmax <= 511; no counterpart in the reference. */
+int sle_sht_set_precision(sle_sht* plan, int precision);
 /* dense <-> packed conversion of one complex128 spectrum (device buffers) */
 int sle_sht_pack(sle_sht* plan, const void* dense_dev, void* packed_dev, void* stream);
 int sle_sht_unpack(sle_sht* plan, const void* packed_dev, void* dense_dev, void* stream);
@@ -100,6 +111,7 @@ typedef struct {
   int inner_extrap;         /* inner="extrap" first guess (solver_opt.py:148-165) */
   /* Planet (solver.py:98-110) */
   double radius, mass, rhoi, rhow, gacc, omega, moiA, moiC, kf;
+  int precision;            /* sle_precision of the step's transforms */
 } sle_config;
 
 typedef struct {
@@ -157,6 +169,38 @@ int sle_solver_step(sle_solver* s, const double* ice, int on_device, double dt_y
 int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device);
 /* the solver's own CUDA stream (as void*) */
 int sle_solver_stream(sle_solver* s, void** stream);
+
+/* ------------------------------------------------------------- batches
+ * A batch holds nslots independent solves ("slots") of one grid size and configuration (the
+ * sle_config flags and precision are shared; Earth model, step length, topography and ice history
+ * are per slot).  One sle_batch_step advances every slot given ice in the call by one time step
+ * with the launches of a single solve; slots converge independently (a converged slot is skipped
+ * by the remaining inner iterations).  A slot's results do not depend on the other slots.  Slots
+ * are loaded, stepped and released at any time between steps (continuous batching).  No
+ * counterpart in the reference, which runs one solve per process; each slot follows
+ * SeaLevelSolver.step (solver.py:814-1144). */
+typedef struct sle_batch sle_batch;
+
+/* max_modes: the largest Earth-model mode count any slot will use. */
+int sle_batch_create(const sle_config* cfg, int nslots, int max_modes, sle_batch** out);
+int sle_batch_destroy(sle_batch* b);
+/* Load a slot: Earth model, step length (yr), then step 0 (solver.py:550-581) on topo0 / ice0. */
+int sle_batch_load(sle_batch* b, int slot, const sle_earth* earth, double dt_years, const double* topo0,
+                   const double* ice0, int on_device, double* ocean_area0, double* oceanBeta_area0,
+                   double* ice_volume0);
+/* The slot no longer steps (its memory is reused by the next load). */
+int sle_batch_release(sle_batch* b, int slot);
+/* One step of every slot with ice[slot] != NULL (ice: array of nslots grid pointers).
+ * dt_years: NULL, or nslots values (> 0 changes that slot's step length).  info: nslots records,
+ * filled for the slots that stepped.  Returns SLE_OK, or the status of the first slot that failed
+ * (its record says which; failed slots are not committed, the others are). */
+int sle_batch_step(sle_batch* b, const double* const* ice, int on_device, const double* dt_years,
+                   sle_step_info* info);
+/* copy one output of a slot's last step (as sle_solver_get) */
+int sle_batch_get(sle_batch* b, int slot, int field, void* dst, int dst_on_device);
+int sle_batch_stream(sle_batch* b, void** stream);
+/* slots, mode capacity and the device bytes the batch's solver state occupies */
+int sle_batch_info(const sle_batch* b, int* nslots, int* max_modes, long long* device_bytes);
 
 /* ------------------------------------------------------- measurement */
 /* Kernel classes timed by sle_prof_*: 0 row FFT + fold, 1 Legendre analysis, 2 Legendre

@@ -21,6 +21,7 @@ SLE_ERR_NONCONVERGED = 5
 SLE_ERR_NONFINITE = 6
 SLE_ERR_UNSUPPORTED = 7
 SLE_ERR_STATE = 8
+SLE_ERR_TIMEOUT = 9
 
 LAYOUT_DENSE = 0
 LAYOUT_PACKED = 1
@@ -36,7 +37,8 @@ class SleConfig(C.Structure):
                 ("opt_dsl", C.c_int), ("opt_diag", C.c_int), ("inner_extrap", C.c_int),
                 ("radius", C.c_double), ("mass", C.c_double), ("rhoi", C.c_double),
                 ("rhow", C.c_double), ("gacc", C.c_double), ("omega", C.c_double),
-                ("moiA", C.c_double), ("moiC", C.c_double), ("kf", C.c_double)]
+                ("moiA", C.c_double), ("moiC", C.c_double), ("kf", C.c_double),
+                ("precision", C.c_int)]
 
 
 _DP = C.POINTER(C.c_double)
@@ -73,6 +75,7 @@ _SIGS = {
     "sle_sht_synthesis": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                     C.c_void_p]),
     "sle_sht_analysis_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sle_sht_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "sle_sht_pack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_sht_unpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_solver_create": (C.c_int, [C.POINTER(SleConfig), C.POINTER(SleEarth),
@@ -83,6 +86,16 @@ _SIGS = {
                                   C.POINTER(SleStepInfo)]),
     "sle_solver_get": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "sle_solver_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "sle_batch_create": (C.c_int, [C.POINTER(SleConfig), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "sle_batch_destroy": (C.c_int, [C.c_void_p]),
+    "sle_batch_load": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(SleEarth), C.c_double, C.c_void_p,
+                                 C.c_void_p, C.c_int, _DP, _DP, _DP]),
+    "sle_batch_release": (C.c_int, [C.c_void_p, C.c_int]),
+    "sle_batch_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "sle_batch_get": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),
+    "sle_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "sle_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_longlong)]),
     "sle_prof_enable": (C.c_int, [C.c_int]),
     "sle_prof_collect": (C.c_int, []),
     "sle_prof_reset": (C.c_int, []),
@@ -92,6 +105,17 @@ _SIGS = {
 }
 
 PROF_FFT, PROF_LEG_ANA, PROF_LEG_SYN, PROF_IFFT, PROF_ADVANCE = range(5)
+PREC_FP64, PREC_MIXED = 0, 1
+PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
+
+
+def precision_code(precision) -> int:
+    """'fp64' / 'mixed' (or the integer code) -> sle_precision; ValueError otherwise."""
+    if isinstance(precision, str) and precision.lower() in PRECISIONS:
+        return PRECISIONS[precision.lower()]
+    if precision in (PREC_FP64, PREC_MIXED):
+        return int(precision)
+    raise ValueError(f"unknown precision {precision!r} (expected 'fp64' or 'mixed')")
 
 _lib = None
 

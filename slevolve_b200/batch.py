@@ -1,0 +1,203 @@
+"""Batches of independent sea-level solves on one GPU (``sle_batch_*`` in the C ABI).
+
+``SolverBatch(nlat, nlon, lmax, nslots, ...)`` holds ``nslots`` solves ("slots") of one grid size
+and one configuration (rotation, marine check, options, precision).  Each slot has its own Earth
+model, step length, topography, ice history and modal state, all resident on the device.  One
+``step`` advances every slot that is given ice by one time step of ``SeaLevelSolver.step``
+(SLEvolve python/slevolve/solver.py:814-1144) with the kernel launches of a single solve; slots
+converge independently and a converged slot drops out of the remaining inner iterations.  Slots
+are loaded, stepped and released between steps in any order, which is what the serving loop
+(``slevolve_b200.serving``) builds continuous batching on.
+
+A slot's results do not depend on which other slots share the batch: every reduction is per slot
+and in a fixed order, and the tensor-core contraction treats each field as its own columns.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .solver import PI, Planet, earth_struct
+
+FIELDS = {"tgrid": _lib.F_TGRID, "ocean": _lib.F_OCEAN, "beta": _lib.F_BETA, "R": _lib.F_R,
+          "G": _lib.F_G, "deltasl": _lib.F_DELTASL, "icestar": _lib.F_ICESTAR}
+
+
+def _is_cuda_tensor(x):
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        return False
+    return isinstance(x, torch.Tensor) and x.is_cuda
+
+
+class SolverBatch:
+    """``nslots`` independent solves of one grid size stepped together on the GPU."""
+
+    def __init__(self, nlat, nlon, lmax, nslots, *, max_modes=8, precision="mixed", tpw=True,
+                 checkmarine=True, calcRG=True, epsilon1=1.0e-5, planet=None, opt=("dsl", "diag"),
+                 inner="extrap"):
+        opt = set(opt)
+        unknown = opt - {"diag", "dsl", "numba", "sums"}
+        if unknown:
+            raise ValueError(f"unknown opt {sorted(unknown)}")
+        if inner not in ("off", "extrap"):
+            raise ValueError(f"inner must be 'off' or 'extrap' for a batch, got {inner!r}")
+        self.nlat, self.nlon, self.lmax = int(nlat), int(nlon), int(lmax)
+        self.nslots = int(nslots)
+        self.p = planet or Planet()
+        self.precision = "mixed" if _lib.precision_code(precision) == _lib.PREC_MIXED else "fp64"
+        p = self.p
+        cfg = _lib.SleConfig(nlat=self.nlat, nlon=self.nlon, lmax=self.lmax, dt_years=1.0,
+                             epsilon1=float(epsilon1), tpw=int(bool(tpw)),
+                             checkmarine=int(bool(checkmarine)), calcRG=int(bool(calcRG)),
+                             opt_dsl=int("dsl" in opt), opt_diag=int("diag" in opt),
+                             inner_extrap=int(inner == "extrap"), radius=p.radius, mass=p.mass,
+                             rhoi=p.rhoi, rhow=p.rhow, gacc=p.gacc, omega=p.omega, moiA=p.moiA,
+                             moiC=p.moiC, kf=p.kf, precision=_lib.precision_code(precision))
+        L = _lib.lib()
+        self._L = L
+        h = C.c_void_p()
+        _lib.check(L.sle_batch_create(C.byref(cfg), self.nslots, int(max_modes), C.byref(h)),
+                   "sle_batch_create")
+        self._h = h
+        self.loaded = [False] * self.nslots
+        self.area0 = [None] * self.nslots
+        self._ice_ptrs = (C.c_void_p * self.nslots)()
+        self._dts = (C.c_double * self.nslots)()
+        self._infos = (_lib.SleStepInfo * self.nslots)()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._L.sle_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ------------------------------------------------------------------ slots
+    @property
+    def device_bytes(self) -> int:
+        n = C.c_longlong()
+        _lib.check(self._L.sle_batch_info(self._h, None, None, C.byref(n)), "sle_batch_info")
+        return int(n.value)
+
+    def free_slots(self):
+        return [i for i, x in enumerate(self.loaded) if not x]
+
+    def load(self, slot, love, topo0, ice0, dt):
+        """Give `slot` an Earth model, a step length (yr) and run step 0 on topo0 / ice0;
+        returns (ocean_area0, oceanBeta_area0, ice_volume0)."""
+        earth, keep = earth_struct(love, self.lmax, self.p)
+        a, b, v = C.c_double(), C.c_double(), C.c_double()
+        if _is_cuda_tensor(topo0):
+            import torch
+
+            t0 = topo0.to(torch.float64).contiguous()
+            i0 = ice0.to(torch.float64).contiguous()
+            torch.cuda.current_stream().synchronize()
+            ptrs, on_dev = (t0.data_ptr(), i0.data_ptr()), 1
+        else:
+            t0 = np.ascontiguousarray(topo0, dtype=np.float64)
+            i0 = np.ascontiguousarray(ice0, dtype=np.float64)
+            if t0.shape != (self.nlat, self.nlon) or i0.shape != t0.shape:
+                raise ValueError(f"grids must be {(self.nlat, self.nlon)}")
+            ptrs, on_dev = (t0.ctypes.data, i0.ctypes.data), 0
+        _lib.check(self._L.sle_batch_load(self._h, int(slot), C.byref(earth), float(dt), C.c_void_p(ptrs[0]),
+                                          C.c_void_p(ptrs[1]), on_dev, C.byref(a), C.byref(b), C.byref(v)),
+                   "sle_batch_load")
+        del keep
+        self.loaded[slot] = True
+        self.area0[slot] = (a.value, b.value, v.value)
+        return self.area0[slot]
+
+    def release(self, slot):
+        _lib.check(self._L.sle_batch_release(self._h, int(slot)), "sle_batch_release")
+        self.loaded[slot] = False
+
+    # ------------------------------------------------------------------- step
+    def step_ptrs(self, ptrs, on_device, dts=None):
+        """One step from raw grid pointers: {slot: pointer}; returns {slot: SleStepInfo}.
+        Raises like the single solver when a slot fails (its record has the status)."""
+        for i in range(self.nslots):
+            self._ice_ptrs[i] = None
+            self._dts[i] = 0.0
+        for slot, ptr in ptrs.items():
+            self._ice_ptrs[slot] = ptr
+            if dts and slot in dts and dts[slot]:
+                self._dts[slot] = float(dts[slot])
+        rc = self._L.sle_batch_step(self._h, self._ice_ptrs, int(on_device), self._dts, self._infos)
+        out = {slot: self._infos[slot] for slot in ptrs}
+        _lib.check(rc, "sle_batch_step")
+        return out
+
+    def step(self, ices, dts=None):
+        """ices: {slot: grid (NumPy array or CUDA tensor)}; returns {slot: info dict}."""
+        if not ices:
+            return {}
+        dev = [_is_cuda_tensor(x) for x in ices.values()]
+        if any(dev) and not all(dev):
+            raise ValueError("all ice grids of one step must be on the same side (host or device)")
+        keep = {}
+        if all(dev):
+            import torch
+
+            for slot, x in ices.items():
+                keep[slot] = x.to(torch.float64).contiguous()
+            torch.cuda.current_stream().synchronize()
+            ptrs = {slot: t.data_ptr() for slot, t in keep.items()}
+            infos = self.step_ptrs(ptrs, 1, dts)
+        else:
+            for slot, x in ices.items():
+                a = np.ascontiguousarray(x, dtype=np.float64)
+                if a.shape != (self.nlat, self.nlon):
+                    raise ValueError(f"ice shape {a.shape} != {(self.nlat, self.nlon)}")
+                keep[slot] = a
+            ptrs = {slot: a.ctypes.data for slot, a in keep.items()}
+            infos = self.step_ptrs(ptrs, 0, dts)
+        return {slot: _info_dict(i) for slot, i in infos.items()}
+
+    def get(self, slot, field, out=None):
+        """A grid of the slot's last step ('tgrid', 'ocean', 'beta', 'R', 'G', 'deltasl',
+        'icestar') as NumPy, or into `out` (a CUDA tensor or a NumPy array)."""
+        code = FIELDS[field]
+        if out is None:
+            out = np.empty((self.nlat, self.nlon))
+        if _is_cuda_tensor(out):
+            _lib.check(self._L.sle_batch_get(self._h, int(slot), code, C.c_void_p(out.data_ptr()), 1),
+                       "sle_batch_get")
+        else:
+            _lib.check(self._L.sle_batch_get(self._h, int(slot), code, C.c_void_p(out.ctypes.data), 0),
+                       "sle_batch_get")
+        return out
+
+    def stream_handle(self):
+        s = C.c_void_p()
+        _lib.check(self._L.sle_batch_stream(self._h, C.byref(s)), "sle_batch_stream")
+        return s.value
+
+
+def _info_dict(info):
+    lam = np.array(info.lam[:]).reshape(3, 3, 2)
+    return {"iter": info.iter, "numiter": info.numiter, "status": info.status, "xi": info.xi,
+            "ocean_area": info.ocean_area, "oceanBeta_area": info.oceanBeta_area,
+            "gmslc_ocn": info.gmslc_ocn, "gmslc_ocnBeta": info.gmslc_ocnBeta,
+            "ice_volume": info.ice_volume, "il": np.array(info.il[:]).reshape(3, 3),
+            "mm": np.array(info.mm[:]), "lambda": lam[..., 0] + 1j * lam[..., 1],
+            "gr_reguess": info.gr_reguess, "gr_ice_analyses": info.gr_ice_analyses}
+
+
+def slot_bytes(nlat, nlon, lmax, max_modes=8):
+    """Device bytes one slot's solver state takes (the admission unit of the serving loop)."""
+    ng = nlat * nlon
+    nc = (lmax + 1) * (lmax + 2) // 2
+    nl = lmax + 1
+    return int(21 * ng * 8 + 24 * nc * 16 + max_modes * nc * 16 + 5 * max_modes * nl * 8 + 3 * nl * 8
+               + 1024 + (nc // 256 + ng // 512 + 128) * 8 + 4 * nlat * 8)
+
+
+__all__ = ["SolverBatch", "slot_bytes", "PI"]

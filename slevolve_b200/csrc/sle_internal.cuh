@@ -37,7 +37,9 @@ constexpr int SEG = 64;
 constexpr double SIG_THRESHOLD = 1.0e-35;
 // The legacy literal of spat2spec / spec2spat (SLEvolve sht.py:60-61), not sqrt(2).
 constexpr double SQRT2_LEGACY = 1.41421356;
-constexpr int MAXF = 4;   // fields per batched transform call
+constexpr int MAXF = 4;   // fields per batched transform call (FP64 path)
+constexpr int MX_MAXF = 32;          // fields per mixed-precision transform launch
+constexpr int MX_NMAX = 2 * MX_MAXF; // B-operand rows (Re, Im per field)
 
 // Device view of a transform plan, passed to kernels by value.
 struct ShtDev {
@@ -60,30 +62,48 @@ struct ShtDev {
   const double2* tw;          // [n2] exp(-2 pi i t / nlon)
   double2* X;                 // [MAXF][2][nm][nh] folded rFFT (S then D) of analysed grids
   double2* EO;                // [MAXF][2][nm][nh] even/odd Legendre sums of synthesised fields
-  // Optional per-field gates of an analysis launch (device flags read at kernel entry): field f
-  // is skipped when bit f of gate_conv_mask is set and *gate_conv != 0, or when bit f of
-  // gate_chg_mask is set and *gate_chg == 0.
-  const int* gate_conv;
-  const int* gate_chg;
-  unsigned gate_conv_mask, gate_chg_mask;
+  // Per-field gates of a launch (device flags read at kernel entry): field f is skipped (its
+  // outputs left as they are) when gset[f] && *gset[f] != 0, or gclr[f] && *gclr[f] == 0.
+  const int* gset[MAXF];
+  const int* gclr[MAXF];
+  // mixed-precision transforms (set once the plan prepared them)
+  float* mx_xf;               // [nm][2][ngrp][MX_NMAX][32] folded FP32 rFFT, analysis B layout
+  float2* mx_gns;             // [MX_MAXF][2][nm][nh] north / south Legendre sums (synthesis)
+  double* mx_s0;              // [MX_MAXF][nh] FP64 fold of the row sums (degree 0)
+  int* mx_abort;              // raised by a tensor-core kernel whose wait timed out
+  const int2* mx_ana_units;   // (m, span) analysis work units, most work first
+  const int2* mx_syn_units;   // (m, latitude tile) synthesis work units, most work first
 };
 
 __device__ __forceinline__ bool field_gated_off(const ShtDev& P, int f) {
-  if (((P.gate_conv_mask >> f) & 1u) && *P.gate_conv != 0) return true;
-  if (((P.gate_chg_mask >> f) & 1u) && *P.gate_chg == 0) return true;
+  if (P.gset[f] && *P.gset[f] != 0) return true;
+  if (P.gclr[f] && *P.gclr[f] == 0) return true;
   return false;
 }
 
-struct AnaGate {
-  const int* conv;
-  const int* chg;
-  unsigned conv_mask, chg_mask;
+// One field of a transform call: input and output, optional gates (see ShtDev::gset/gclr) and,
+// for synthesis, the optional epilogue epi_out = grid * epi_mul.
+struct FieldSpec {
+  double* grid;
+  double2* spec;
+  const int* skip_set;
+  const int* skip_clear;
+  double* epi_out;
+  const double* epi_mul;
 };
 
-// Epilogue of the inverse-FFT kernel: out2 = g * mul2 (e.g. rO = dsl * C*).
-struct SynEpilogue {
-  double* out2;
-  const double* mul2;
+// Fields of one mixed-precision transform launch.  Field f is skipped (its outputs left as
+// they are) when *skip_set[f] != 0 or *skip_clear[f] == 0 (null pointers never skip).
+// Synthesis epilogue: epi_out[f] = grid[f] * epi_mul[f] when epi_out[f] is set.
+struct MxFieldArgs {
+  int nf;
+  int ncols;                       // MMA N: 0 = smallest multiple of 16 >= 2 nf
+  double* grid[MX_MAXF];           // analysis input / synthesis output
+  double2* spec[MX_MAXF];          // analysis output / synthesis input (packed)
+  const int* skip_set[MX_MAXF];
+  const int* skip_clear[MX_MAXF];
+  double* epi_out[MX_MAXF];
+  const double* epi_mul[MX_MAXF];
 };
 
 }  // namespace sle
@@ -99,6 +119,16 @@ struct sle_sht {
   double2* packbuf;           // [MAXF][ncoef] packed staging for dense-layout calls
   double* skipped_frac;       // host value: fraction of (l, m, j) work skipped
   double work_frac;
+  int precision;              // SLE_PREC_FP64 or SLE_PREC_MIXED
+  int* mx_status;             // device status word raised on a tensor-core timeout (may be null)
+  // mixed-precision transform buffers (allocated on first use)
+  int mx_ready;
+  float* mx_xf;
+  float2* mx_gns;
+  double* mx_s0;
+  int* mx_abort;
+  int2 *mx_ana_units, *mx_syn_units;
+  int n_ana_units, n_syn_units;
 };
 
 namespace sle {
@@ -115,11 +145,17 @@ bool prof_enabled();
 ProfToken prof_begin(int cls, double units, cudaStream_t st);
 void prof_end(const ProfToken& t, cudaStream_t st);
 
-// Launch helpers implemented in sle_sht.cu, used by the solver.
-int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, double2* const* out,
-                        cudaStream_t st, const AnaGate* gate = nullptr);
-int sht_synthesis_packed(sle_sht* plan, int nf, const double2* const* coeffs, double* const* grids,
-                         const SynEpilogue* epi, cudaStream_t st);
+// Transforms of a list of fields (packed spectra), launched in groups of MAXF (FP64) or
+// MX_MAXF (mixed) fields with the precision of the plan (sle_sht.cu).
+int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st);
+int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st);
 int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t st);
+// Mixed-precision transforms (sle_mx.cu).  `status` (device int, may be null) receives
+// SLE_ERR_TIMEOUT if a tensor-core kernel gave up waiting.
+int sht_mx_prepare(sle_sht* plan);
+int sht_mx_analysis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st);
+int sht_mx_synthesis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st);
+int sht_mx_abort_flag(sle_sht* plan, int* flag);
+int mx_cols(int nf);
 int sht_unpack(sle_sht* plan, const double2* packed, double2* dense, cudaStream_t st);
 }  // namespace sle

@@ -19,6 +19,7 @@
 //   * (segment, latitude-group) blocks whose |P~| never exceeds 1e-35 (near the poles at high
 //     m) are skipped.
 #include "sle_internal.cuh"
+#include "sle_fft.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -39,12 +40,7 @@ void set_error(const char* fmt, ...) {
 }
 
 // --------------------------------------------------------------------------- helpers
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// (complex helpers and the Stockham FFT: sle_fft.cuh)
 
 // Sum a per-lane vector v[0..V) over the 32 lanes of a warp.  After the call lane `l` holds
 // in v[0] the warp total of value index (l >> (5 - log2 V)).  log2(V) exchange stages each
@@ -204,108 +200,13 @@ __global__ void k_lidx(sle::ShtDev P, int* lidx) {
   for (int l = m + threadIdx.x; l <= P.lmax; l += blockDim.x) lidx[base + (l - m)] = l;
 }
 
-// ----------------------------------------------------------------------------- FFTs
-// Stockham FFT of length n2 = nlon/2 on complex rows in shared memory: radix-8 passes while at
-// least 8 points remain per sub-transform, then one radix-4 or radix-2 pass.  A pass of radix R
-// with current sub-transform size Ns maps in[j + r q] (q = n2/R, k = j mod Ns) through the
-// twiddles exp(-+2 pi i r k/(Ns R)) and an R-point DFT in registers to
-// out[(j - k) R + k + r Ns].  tw[t] = exp(-2 pi i t / (2 n2)) for t < n2; larger t use
-// tw[t - n2] = -exp(...).
-__device__ __forceinline__ double2 twiddle(const double2* tw, int n2, int t, bool inv) {
-  double2 w = (t < n2) ? tw[t] : make_double2(-tw[t - n2].x, -tw[t - n2].y);
-  if (inv) w.y = -w.y;
-  return w;
-}
-
-__device__ __forceinline__ double2 mul_mi(double2 a, bool inv) {  // a * (-i), or a * (+i) when inv
-  return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
-}
-
-__device__ __forceinline__ void dft8(double2 (&v)[8], bool inv) {
-  const double h = 0.70710678118654752440;  // cos(pi/4)
-  double2 a0 = cadd(v[0], v[4]), a4 = csub(v[0], v[4]);
-  double2 a1 = cadd(v[1], v[5]), a5 = csub(v[1], v[5]);
-  double2 a2 = cadd(v[2], v[6]), a6 = csub(v[2], v[6]);
-  double2 a3 = cadd(v[3], v[7]), a7 = csub(v[3], v[7]);
-  // a5 *= W, a6 *= W^2, a7 *= W^3 with W = exp(-+2 pi i / 8)
-  const double s = inv ? h : -h;
-  a5 = make_double2(h * a5.x - s * a5.y, h * a5.y + s * a5.x);
-  a6 = mul_mi(a6, inv);
-  a7 = make_double2(-h * a7.x - s * a7.y, -h * a7.y + s * a7.x);
-  double2 b0 = cadd(a0, a2), b2 = csub(a0, a2), b1 = cadd(a1, a3), b3 = mul_mi(csub(a1, a3), inv);
-  double2 b4 = cadd(a4, a6), b6 = csub(a4, a6), b5 = cadd(a5, a7), b7 = mul_mi(csub(a5, a7), inv);
-  v[0] = cadd(b0, b1);
-  v[1] = cadd(b4, b5);
-  v[2] = cadd(b2, b3);
-  v[3] = cadd(b6, b7);
-  v[4] = csub(b0, b1);
-  v[5] = csub(b4, b5);
-  v[6] = csub(b2, b3);
-  v[7] = csub(b6, b7);
-}
-
-// One Stockham pass of radix R on two rows of N points (compile-time sizes: all index
-// arithmetic folds to shifts and masks).  Sub-transform size before the pass: NS.
-template <int N, int R, int NS, bool INV>
-__device__ __forceinline__ void fft_pass_c(const double2* __restrict__ in, double2* __restrict__ out,
-                                           const double2* __restrict__ tw) {
-  constexpr int Q = N / R;
-  constexpr int TSTEP = 2 * N / (NS * R);
-  for (int idx = threadIdx.x; idx < 2 * Q; idx += blockDim.x) {
-    const int r = idx / Q, j = idx % Q;
-    const int k = j % NS;
-    const double2* src = in + r * N;
-    double2 v[R];
-#pragma unroll
-    for (int u = 0; u < R; ++u) v[u] = src[j + u * Q];
-    if (NS > 1) {
-#pragma unroll
-      for (int u = 1; u < R; ++u) {
-        const int t = u * k * TSTEP;
-        double2 w = (t < N) ? tw[t] : make_double2(-tw[t - N].x, -tw[t - N].y);
-        if (INV) w.y = -w.y;
-        v[u] = cmul(v[u], w);
-      }
-    }
-    if (R == 8) {
-      dft8(reinterpret_cast<double2(&)[8]>(v), INV);
-    } else if (R == 4) {
-      const double2 a0 = cadd(v[0], v[2]), a2 = csub(v[0], v[2]);
-      const double2 a1 = cadd(v[1], v[3]), a3 = mul_mi(csub(v[1], v[3]), INV);
-      v[0] = cadd(a0, a1);
-      v[1] = cadd(a2, a3);
-      v[2] = csub(a0, a1);
-      v[3] = csub(a2, a3);
-    } else {
-      const double2 a0 = cadd(v[0], v[1]), a1 = csub(v[0], v[1]);
-      v[0] = a0;
-      v[1] = a1;
-    }
-    double2* dst = out + r * N + (j - k) * R + k;
-#pragma unroll
-    for (int u = 0; u < R; ++u) dst[u * NS] = v[u];
-  }
-}
-
-// Radix-8 passes while at least 8 points remain per sub-transform, then one radix-4 or 2 pass.
-template <int N, int NS, bool INV>
-__device__ __forceinline__ double2* stockham_c(double2* A, double2* B, const double2* tw) {
-  if constexpr (NS >= N) {
-    return A;
-  } else {
-    constexpr int REM = N / NS;
-    constexpr int R = (REM >= 8) ? 8 : REM;
-    fft_pass_c<N, R, NS, INV>(A, B, tw);
-    __syncthreads();
-    return stockham_c<N, NS * R, INV>(B, A, tw);
-  }
-}
-
 struct GridPtrs {
   const double* p[MAXF];
 };
 struct OutGridPtrs {
   double* p[MAXF];
+  double* out2[MAXF];        // optional epilogue out2 = grid * mul2
+  const double* mul2[MAXF];
 };
 struct SpecPtrs {
   double2* p[MAXF];
@@ -366,14 +267,14 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fft_fold(sle::Sht
 // Inverse: north spectrum E + O, south E - O (m <= lmax, 0 above), unnormalised inverse
 // real FFT of both rows (sht.py:330-339 with the nlon scaling folded out); field blockIdx.y.
 template <int N>
-__global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_ifft_unfold(sle::ShtDev P, OutGridPtrs g,
-                                                                          SynEpilogue epi) {
+__global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_ifft_unfold(sle::ShtDev P, OutGridPtrs g) {
   extern __shared__ double2 sm[];
   __shared__ double2 nyq[2];
   double2* tw = sm;
   double2* A = sm + N;
   double2* B = A + 2 * N;
   const int j = blockIdx.x, f = blockIdx.y;
+  if (field_gated_off(P, f)) return;
   const int js = P.nlat - 1 - j;
   const double2* E = P.EO + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
   const double2* O = P.EO + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
@@ -417,36 +318,22 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_ifft_unfold(sle::
   const double2* Z = stockham_c<N, 1, true>(A, B, tw);
   double2* rn = reinterpret_cast<double2*>(g.p[f] + (size_t)j * (2 * N));
   double2* rs = reinterpret_cast<double2*>(g.p[f] + (size_t)js * (2 * N));
-  const bool ep = (f == 0) && epi.out2;
+  double* out2 = g.out2[f];
+  const double* mul2 = g.mul2[f];
   for (int t = threadIdx.x; t < N; t += blockDim.x) {
     const double2 vn = Z[t], vs = Z[N + t];
     rn[t] = vn;
     rs[t] = vs;
-    if (ep) {
-      const double2 mn = reinterpret_cast<const double2*>(epi.mul2 + (size_t)j * (2 * N))[t];
-      const double2 ms = reinterpret_cast<const double2*>(epi.mul2 + (size_t)js * (2 * N))[t];
-      reinterpret_cast<double2*>(epi.out2 + (size_t)j * (2 * N))[t] = make_double2(vn.x * mn.x, vn.y * mn.y);
-      reinterpret_cast<double2*>(epi.out2 + (size_t)js * (2 * N))[t] = make_double2(vs.x * ms.x, vs.y * ms.y);
+    if (out2) {
+      const double2 mn = reinterpret_cast<const double2*>(mul2 + (size_t)j * (2 * N))[t];
+      const double2 ms = reinterpret_cast<const double2*>(mul2 + (size_t)js * (2 * N))[t];
+      reinterpret_cast<double2*>(out2 + (size_t)j * (2 * N))[t] = make_double2(vn.x * mn.x, vn.y * mn.y);
+      reinterpret_cast<double2*>(out2 + (size_t)js * (2 * N))[t] = make_double2(vs.x * ms.x, vs.y * ms.y);
     }
   }
 }
 
-// launch over the supported sizes N = 4 .. 2048 (nlon = 8 .. 4096)
-#define SLE_FFT_SWITCH(N2, CALL) \
-  switch (N2) {                  \
-    case 4: CALL(4); break;      \
-    case 8: CALL(8); break;      \
-    case 16: CALL(16); break;    \
-    case 32: CALL(32); break;    \
-    case 64: CALL(64); break;    \
-    case 128: CALL(128); break;  \
-    case 256: CALL(256); break;  \
-    case 512: CALL(512); break;  \
-    case 1024: CALL(1024); break; \
-    default: CALL(2048); break;  \
-  }
 
-static int fft_threads(int n2) { return n2 / 4 > 32 ? n2 / 4 : 32; }
 
 // ------------------------------------------------------------------ Legendre analysis
 constexpr int ANA_TL = 4;      // degrees per warp reduction
@@ -592,6 +479,7 @@ __global__ void __launch_bounds__(32 * ANA_WARPS, 3) k_leg_ana(sle::ShtDev P, Sp
 __global__ void __launch_bounds__(512, 1) k_leg_syn(sle::ShtDev P, CSpecPtrs in) {
   extern __shared__ double smd[];
   const int f = blockIdx.y;
+  if (field_gated_off(P, f)) return;
   const int p = blockIdx.x;
   const int L = P.lmax;
   double2* Uc = reinterpret_cast<double2*>(smd);          // [nm]
@@ -683,24 +571,16 @@ static size_t fft_smem(const ShtDev& d) { return (size_t)5 * d.n2 * sizeof(doubl
 static int syn_threads(const ShtDev& d) { return 32 * ((d.ngrp + 1) / 2); }
 static size_t syn_smem(const ShtDev& d) { return (size_t)3 * d.nm * sizeof(double); }
 
-int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, double2* const* out,
-                        cudaStream_t st, const AnaGate* gate) {
+// One FP64 launch group (1..MAXF fields).
+static int fp64_analysis(sle_sht* plan, const FieldSpec* fs, int nf, cudaStream_t st) {
   ShtDev d = plan->d;
-  if (gate) {
-    d.gate_conv = gate->conv;
-    d.gate_chg = gate->chg;
-    d.gate_conv_mask = gate->conv_mask;
-    d.gate_chg_mask = gate->chg_mask;
-  }
-  if (nf < 1 || nf > MAXF) {
-    set_error("analysis: nfields must be 1..%d", MAXF);
-    return SLE_ERR_BAD_ARG;
-  }
   GridPtrs g{};
   SpecPtrs o{};
   for (int f = 0; f < nf; ++f) {
-    g.p[f] = grids[f];
-    o.p[f] = out[f];
+    g.p[f] = fs[f].grid;
+    o.p[f] = fs[f].spec;
+    d.gset[f] = fs[f].skip_set;
+    d.gclr[f] = fs[f].skip_clear;
   }
   ProfToken t0 = prof_begin(PROF_FFT, nf, st);
 #define SLE_LAUNCH_FOLD(NN) k_fft_fold<NN><<<dim3(d.nh, nf), fft_threads(NN), fft_smem(d), st>>>(d, g)
@@ -717,31 +597,76 @@ int sht_analysis_packed(sle_sht* plan, int nf, const double* const* grids, doubl
   return SLE_OK;
 }
 
-int sht_synthesis_packed(sle_sht* plan, int nf, const double2* const* coeffs, double* const* grids,
-                         const SynEpilogue* epi, cudaStream_t st) {
-  const ShtDev& d = plan->d;
-  if (nf < 1 || nf > MAXF) {
-    set_error("synthesis: nfields must be 1..%d", MAXF);
-    return SLE_ERR_BAD_ARG;
-  }
+static int fp64_synthesis(sle_sht* plan, const FieldSpec* fs, int nf, cudaStream_t st) {
+  ShtDev d = plan->d;
   CSpecPtrs c{};
   OutGridPtrs g{};
   for (int f = 0; f < nf; ++f) {
-    c.p[f] = coeffs[f];
-    g.p[f] = grids[f];
+    c.p[f] = fs[f].spec;
+    g.p[f] = fs[f].grid;
+    g.out2[f] = fs[f].epi_out;
+    g.mul2[f] = fs[f].epi_mul;
+    d.gset[f] = fs[f].skip_set;
+    d.gclr[f] = fs[f].skip_clear;
   }
   const int npairs = (d.nm + 1) / 2;
   ProfToken t0 = prof_begin(PROF_LEG_SYN, nf, st);
   k_leg_syn<<<dim3(npairs, nf), syn_threads(d), syn_smem(d), st>>>(d, c);
   prof_end(t0, st);
-  SynEpilogue e = epi ? *epi : SynEpilogue{nullptr, nullptr};
   ProfToken t1 = prof_begin(PROF_IFFT, nf, st);
-#define SLE_LAUNCH_IFFT(NN) k_ifft_unfold<NN><<<dim3(d.nh, nf), fft_threads(NN), fft_smem(d), st>>>(d, g, e)
+#define SLE_LAUNCH_IFFT(NN) k_ifft_unfold<NN><<<dim3(d.nh, nf), fft_threads(NN), fft_smem(d), st>>>(d, g)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_IFFT)
 #undef SLE_LAUNCH_IFFT
   prof_end(t1, st);
   note_launch(2);
   SLE_CUDA(cudaGetLastError());
+  return SLE_OK;
+}
+
+static MxFieldArgs mx_args(const FieldSpec* fs, int nf) {
+  MxFieldArgs a{};
+  a.nf = nf;
+  for (int f = 0; f < nf; ++f) {
+    a.grid[f] = fs[f].grid;
+    a.spec[f] = fs[f].spec;
+    a.skip_set[f] = fs[f].skip_set;
+    a.skip_clear[f] = fs[f].skip_clear;
+    a.epi_out[f] = fs[f].epi_out;
+    a.epi_mul[f] = fs[f].epi_mul;
+  }
+  return a;
+}
+
+int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st) {
+  if (n < 1) return SLE_OK;
+  const bool mx = plan->precision == SLE_PREC_MIXED;
+  const int group = mx ? MX_MAXF : MAXF;
+  // equal groups (the tensor-core kernels' cost depends on the launch, not on its width)
+  const int ngroups = (n + group - 1) / group;
+  for (int g = 0; g < ngroups; ++g) {
+    const int lo = (int)((long long)n * g / ngroups), hi = (int)((long long)n * (g + 1) / ngroups);
+    if (mx) {
+      SLE_TRY(sht_mx_analysis(plan, mx_args(f + lo, hi - lo), plan->mx_status, st));
+    } else {
+      SLE_TRY(fp64_analysis(plan, f + lo, hi - lo, st));
+    }
+  }
+  return SLE_OK;
+}
+
+int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st) {
+  if (n < 1) return SLE_OK;
+  const bool mx = plan->precision == SLE_PREC_MIXED;
+  const int group = mx ? MX_MAXF : MAXF;
+  const int ngroups = (n + group - 1) / group;
+  for (int g = 0; g < ngroups; ++g) {
+    const int lo = (int)((long long)n * g / ngroups), hi = (int)((long long)n * (g + 1) / ngroups);
+    if (mx) {
+      SLE_TRY(sht_mx_synthesis(plan, mx_args(f + lo, hi - lo), plan->mx_status, st));
+    } else {
+      SLE_TRY(fp64_synthesis(plan, f + lo, hi - lo, st));
+    }
+  }
   return SLE_OK;
 }
 
@@ -777,7 +702,8 @@ static void plan_free(sle_sht* p) {
   if (!p) return;
   void* ptrs[] = {p->mu, p->w, p->wn, p->ws, p->be, p->cf, p->moff, p->lidx, p->segoff,
                   p->seg_m, p->seg_l0, p->ana_order, p->seeds, p->tw, p->X, p->EO, p->istart,
-                  p->packbuf};
+                  p->packbuf, p->mx_xf, p->mx_gns, p->mx_s0, p->mx_abort,
+                  p->mx_ana_units, p->mx_syn_units};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -1015,6 +941,19 @@ extern "C" int sle_sht_gauss(const sle_sht* plan, double* mu_host, double* w_hos
 
 static bool aligned16(const void* p) { return p && (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// A mixed-precision kernel that timed out leaves the plan's abort flag raised: report it (the
+// check synchronises only on plans that use the tensor-core path).
+static int check_abort(sle_sht* plan) {
+  if (plan->precision != SLE_PREC_MIXED) return SLE_OK;
+  int flag = 0;
+  SLE_TRY(sht_mx_abort_flag(plan, &flag));
+  if (flag) {
+    set_error("a tensor-core transform kernel timed out waiting on its pipeline");
+    return SLE_ERR_TIMEOUT;
+  }
+  return SLE_OK;
+}
+
 extern "C" int sle_sht_analysis(sle_sht* plan, int nfields, const double* const* grids_dev,
                                 void* const* coeffs_dev, int layout, void* stream) {
   if (!plan || !grids_dev || !coeffs_dev) {
@@ -1035,7 +974,13 @@ extern "C" int sle_sht_analysis(sle_sht* plan, int nfields, const double* const*
   for (int f = 0; f < nfields; ++f)
     outp[f] = (layout == SLE_LAYOUT_PACKED) ? reinterpret_cast<double2*>(coeffs_dev[f])
                                             : plan->packbuf + (size_t)f * plan->d.ncoef;
-  SLE_TRY(sht_analysis_packed(plan, nfields, grids_dev, outp, st));
+  FieldSpec fs[MAXF] = {};
+  for (int f = 0; f < nfields; ++f) {
+    fs[f].grid = const_cast<double*>(grids_dev[f]);
+    fs[f].spec = outp[f];
+  }
+  SLE_TRY(sht_analysis_list(plan, fs, nfields, st));
+  SLE_TRY(check_abort(plan));
   if (layout != SLE_LAYOUT_PACKED)
     for (int f = 0; f < nfields; ++f)
       SLE_TRY(sht_unpack(plan, outp[f], reinterpret_cast<double2*>(coeffs_dev[f]), st));
@@ -1068,7 +1013,27 @@ extern "C" int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* 
       inp[f] = pb;
     }
   }
-  return sht_synthesis_packed(plan, nfields, inp, grids_dev, nullptr, st);
+  FieldSpec fs[MAXF] = {};
+  for (int f = 0; f < nfields; ++f) {
+    fs[f].grid = grids_dev[f];
+    fs[f].spec = const_cast<double2*>(inp[f]);
+  }
+  SLE_TRY(sht_synthesis_list(plan, fs, nfields, st));
+  return check_abort(plan);
+}
+
+extern "C" int sle_sht_set_precision(sle_sht* plan, int precision) {
+  if (!plan) {
+    set_error("sle_sht_set_precision: NULL plan");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (precision != SLE_PREC_FP64 && precision != SLE_PREC_MIXED) {
+    set_error("sle_sht_set_precision: unknown precision %d", precision);
+    return SLE_ERR_BAD_ARG;
+  }
+  if (precision == SLE_PREC_MIXED) SLE_TRY(sht_mx_prepare(plan));
+  plan->precision = precision;
+  return SLE_OK;
 }
 
 extern "C" int sle_sht_pack(sle_sht* plan, const void* dense_dev, void* packed_dev, void* stream) {

@@ -1,13 +1,23 @@
-// The SLEvolve time step on the device, FP64 (SLEvolve python/slevolve/solver.py:521-1144).
+// The SLEvolve time step on the device (SLEvolve python/slevolve/solver.py:521-1144) for a batch
+// of independent solves ("slots") on one grid size, FP64 or mixed-precision transforms.
 //
-// All solver state lives in HBM for the life of the handle: grids [nlat][nlon] float64,
-// spectra in the packed order-major triangle (complex128), the modal state R[k][packed].
-// Elementwise kernels reproduce the reference's NumPy statement order with explicitly
-// rounded operations (no FMA contraction), reductions are deterministic (fixed partition,
-// last-block finalisation in index order).  The inner fixed-point loop runs its kernels
-// back to back and reads one small status record per iteration to decide whether to go on.
+// Every slot has its own Earth model, step length, topography, ice history, modal state and
+// convergence; the kernels cover all slots of the batch in one launch (blockIdx.y = slot), so a
+// step of B solves costs the launches of one.  All state lives in HBM for the life of the
+// handle, laid out buffer-major: grid buffer g of slot b at grid + (g * nslot + b) * ng, spectra
+// in the packed order-major triangle (complex128) likewise, the modal state R[slot][k][packed].
+// Elementwise kernels reproduce the reference's NumPy statement order with explicitly rounded
+// operations (no FMA contraction); reductions are deterministic (fixed partition, last-block
+// finalisation in index order), so a slot's results do not depend on the other slots.
+//
+// The inner fixed-point loop is a CUDA graph with a device-evaluated WHILE condition: it runs
+// while any stepping slot is unconverged; a slot that converged is marked done at the end of
+// that iteration and every kernel of later iterations skips it.
+//
+// The single-solve C API (sle_solver_*) is a batch of one slot.
 #include "sle_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -21,7 +31,7 @@ constexpr int GR_MAXACC = 3;                      // solver.py:38
 constexpr int MAX_INNER = 9999;                   // solver.py:1049
 
 // Constants of the rotation block (solver.py:910-975), computed on the host with the
-// reference's expressions.
+// reference's expressions, one record per slot (they depend on the slot's Earth model).
 struct RotConst {
   double c_il22, c_il02, c_il12;   // -8 PI a^4/(3 sqrt5), -8 PI a^4/sqrt30, 8 PI a^4/sqrt30
   double alpha;                    // 1 / (1 - kTE2/kf)
@@ -32,11 +42,11 @@ struct RotConst {
   double rhoi, rhow;
 };
 
-// Small per-step record, mirrored to pinned host memory once per inner iteration.
+// Per-slot step record, mirrored to pinned host memory.
 struct Scal {
   double conserv, sa, so, xi;
   double K00;
-  int numiter, converged, status, gr_nacc, gr_changed, gr_reguess, gr_ice_an, pad0;
+  int numiter, converged, status, gr_nacc, gr_changed, gr_reguess, gr_ice_an, done;
   unsigned int nd;
   unsigned int pad1;
   double diag[5];        // slc_ocn00, c00, slc_b00, cst00 (real parts), ice00
@@ -49,18 +59,51 @@ struct Scal {
   double p_il[9], p_m[3], p_lambda[6];
 };
 
+// Per-slot parameters of one step, uploaded before the step's kernels.
+struct SlotStep {
+  int active;   // the slot steps in this call
+  int first;    // its first step (old-ice analysis on T0, solver.py:868-873)
+  int mode;     // first guess: 0 eustatic, 1 extrap uniform, 2 extrap variable
+  int hsel;     // which extrap history buffer holds the most recent load increment
+  double c1, c2;
+};
+
+enum GridId {
+  G_TINIT, G_CXY0, G_BETA0, G_CSTAR0, G_CXY, G_TOPO_PREV, G_ICESTAR, G_BETA, G_CSTAR, G_TO, G_RO,
+  G_DSL, G_DELTASL, G_TOPO, G_RR, G_GRNEW, G_ICE, G_ICE_PREV, G_TMP, G_TMP3, G_TMP4, NGRID
+};
+enum SpecId {
+  S_P_LOAD, S_P_ICE, S_P_OCEAN, S_PREV_ICE, S_VISC, S_RAD, S_ICELM, S_OLDICE, S_DICE, S_DI, S_CSTARLM,
+  S_TOLM, S_ROLM, S_LOAD, S_DSCUR, S_SL, S_SLTOT, S_RRLM, S_HA, S_HB, S_SP0, S_SP1, S_SP2, S_SP3, NSPEC
+};
+
 struct Dev {
-  int nlat, nlon, nl;
+  int nlat, nlon, nl, nslot, K;
   long long ng, ncoef;
-  int K;
   const int* lidx;
-  const int* nmod;
-  const double *decay, *omd, *a_sl, *a_rr, *ttl, *ttlekhl, *ttlhe;
-  const double *a_il, *a_m, *a_tsl, *a_trr;
-  int nmod2;
+  double* grid;                 // [NGRID][nslot][ng]
+  double2* spec;                // [NSPEC][nslot][ncoef]
+  double2* R;                   // [nslot][K][ncoef]
+  const int* nmod;              // [nslot][nl]
+  const double *s_kl, *decay, *omd, *a_sl, *a_rr;   // [nslot][K][nl]
+  const double *ttl, *ttlekhl, *ttlhe;             // [nslot][nl]
+  const double *a_il, *a_m, *a_tsl, *a_trr;        // [nslot][K]
+  const RotConst* rc;           // [nslot]
+  double *r_il, *r_m, *r_lam;   // [nslot][K][9 | 3 | 6]
+  Scal* sc;                     // [nslot]
+  const SlotStep* ss;           // [nslot]
+  double* partials;             // [nslot][npart]
+  long long npart, part_grid;
+  unsigned int* counter;        // [nslot][4]
+  double* rows;                 // [nslot][4][nlat]
+  const double* w;              // Gauss weights
   double rhoi, rhow, epsilon1;
   int checkmarine, tpw, calcRG, opt_dsl;
-  long long i20, i21, i22;   // packed indices of (l=2, m=0..2)
+  long long i20, i21, i22;      // packed indices of (l=2, m=0..2)
+  int slot0;                    // slot of blockIdx.y == 0
+  __host__ __device__ double* g(int id, int b) const { return grid + ((size_t)id * nslot + b) * ng; }
+  __host__ __device__ double2* sp(int id, int b) const { return spec + ((size_t)id * nslot + b) * ncoef; }
+  __host__ __device__ size_t kl(int b) const { return (size_t)b * K * nl; }
 };
 
 // ------------------------------------------------------------------ reduction helpers
@@ -85,8 +128,8 @@ __device__ double block_sum(double v, double* sh) {
   return t;  // valid in warp 0
 }
 
-// After each block stored its partial, the last block to arrive sums the partials in index
-// order and returns true (in all its threads) with *total set; others return false.
+// After each block of the slot stored its partial, the last block to arrive sums the partials in
+// index order and returns true (in all its threads) with *total set; others return false.
 __device__ bool last_block_total(double part, double* partials, unsigned int* counter, double* total,
                                  double* sh) {
   __shared__ bool is_last;
@@ -112,6 +155,22 @@ __device__ bool last_block_total(double part, double* partials, unsigned int* co
   return true;
 }
 
+// true in all threads of the slot's last block to finish (after every block passed this point)
+__device__ bool last_block(unsigned int* counter) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int t = atomicAdd(counter, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
 __device__ __forceinline__ double cabs_(double2 z) { return hypot(z.x, z.y); }
 
 // numpy complex division a / b (Smith's method with a reciprocal scale, loops.c.src)
@@ -133,57 +192,88 @@ __device__ __forceinline__ double2 np_cmul(double2 a, double2 b) {
                       __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
 }
 
+__device__ __forceinline__ double2 ld2(const double* p, long long i) {
+  return reinterpret_cast<const double2*>(p)[i];
+}
+__device__ __forceinline__ void st2(double* p, long long i, double a, double b) {
+  reinterpret_cast<double2*>(p)[i] = make_double2(a, b);
+}
+
+// grounded ice on topography `topo` (flotation test, solver.py:655-659)
+__device__ __forceinline__ double icestar_on(double ice, double topo, double rhow, double rhoi) {
+  const bool keep = (topo > 0.0) || (ice > __ddiv_rn(__dmul_rn(fabs(topo), rhow), rhoi));
+  return keep ? ice : __dmul_rn(ice, 0.0);
+}
+
 // ------------------------------------------------------------------------- kernels
-// Grid kernels process two neighbouring cells per thread (16-byte loads; nlon is even) over a
-// full-width grid; spectral kernels one coefficient per thread.  Reductions: block partial
-// sums, then the last block to finish sums the partials in index order.
+// Grid kernels process two neighbouring cells per thread (16-byte loads; nlon is even),
+// spectral kernels one coefficient per thread; blockIdx.y selects the slot.  Every kernel of a
+// step returns at once for a slot marked done (not stepping, or converged earlier).
 
-// true in all threads of the last block to finish (after every block passed this point)
-__device__ bool last_block(unsigned int* counter) {
-  __shared__ bool is_last;
-  __threadfence();  // every thread's earlier global writes are visible before the block's ticket
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned int t = atomicAdd(counter, 1u);
-    is_last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!is_last) return false;
-  __threadfence();
-  if (threadIdx.x == 0) *counter = 0u;
-  return true;
-}
+#define SLOT_OR_RETURN()                        \
+  const int b = D.slot0 + (int)blockIdx.y;      \
+  Scal* sc = D.sc + b;                          \
+  if (sc->done) return;
 
-__global__ void k_set_decay(int K, int nl, const double* s, const int* nmod, double dt, double* decay,
-                            double* omd) {
+__global__ void k_set_decay(Dev D, int b, double dt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= K * nl) return;
-  const int k = i / nl, l = i - k * nl;
+  if (i >= D.K * D.nl) return;
+  const int k = i / D.nl, l = i - k * D.nl;
+  const size_t o = D.kl(b);
   double d = 0.0;
-  if (l >= 1 && k < nmod[l]) d = exp(__ddiv_rn(__dmul_rn(-s[i], dt), 1000.0));
-  decay[i] = d;
-  omd[i] = __dsub_rn(1.0, d);
+  if (l >= 1 && k < D.nmod[(size_t)b * D.nl + l]) d = exp(__ddiv_rn(__dmul_rn(-D.s_kl[o + i], dt), 1000.0));
+  const_cast<double*>(D.decay)[o + i] = d;
+  const_cast<double*>(D.omd)[o + i] = __dsub_rn(1.0, d);
 }
 
-// degree-2 rotational states and their sums (solver.py:409-421): one thread per component
-// (9 il, 3 m, 6 lambda re/im), modes summed in ascending order, inputs staged in shared memory;
-// then the per-step resets and the snapshot of the committed rotational loads (oldil, oldm,
-// dlambda_prev2; solver.py:837-839).  Run by the last block of k_advance (32 threads used).
-__device__ void rot_advance_block(const Dev& D, Scal* sc, double* r_il, double* r_m, double* r_lam) {
+// Step prologue of every slot: stepping slots get their per-step counters reset; the others are
+// marked done (and converged) so that every kernel of the step skips them.
+__global__ void k_step_begin(Dev D) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= D.nslot) return;
+  Scal* sc = D.sc + b;
+  if (D.ss[b].active) {
+    sc->numiter = 0;
+    sc->converged = 0;
+    sc->status = 0;
+    sc->gr_nacc = 0;
+    sc->gr_changed = 0;
+    sc->gr_reguess = 0;
+    sc->gr_ice_an = 0;
+    sc->done = 0;
+  } else {
+    sc->done = 1;
+    sc->converged = 1;
+  }
+}
+
+// Degree-2 rotational states and their sums (solver.py:409-421): one thread per component
+// (9 il, 3 m, 6 lambda re/im), modes summed in ascending order; then the snapshot of the
+// committed rotational loads (oldil, oldm, dlambda_prev2; solver.py:837-839).
+__device__ void rot_advance_block(const Dev& D, int b, Scal* sc) {
   __shared__ double sd[64], sa[4][64], sp[18];
   const int q = threadIdx.x;
-  const int n2 = (D.nl > 2) ? min(D.nmod2, 64) : 0;
+  const int nmod2 = (D.nl > 2) ? D.nmod[(size_t)b * D.nl + 2] : 0;
+  const int n2 = (D.nl > 2) ? min(nmod2, 64) : 0;
+  const size_t o = D.kl(b);
+  const double* al = D.a_il + (size_t)b * D.K;
+  const double* am = D.a_m + (size_t)b * D.K;
+  const double* at = D.a_tsl + (size_t)b * D.K;
+  const double* ar = D.a_trr + (size_t)b * D.K;
   for (int k = q; k < n2; k += blockDim.x) {
-    sd[k] = D.decay[k * D.nl + 2];
-    sa[0][k] = D.a_il[k];
-    sa[1][k] = D.a_m[k];
-    sa[2][k] = D.a_tsl[k];
-    sa[3][k] = D.a_trr[k];
+    sd[k] = D.decay[o + (size_t)k * D.nl + 2];
+    sa[0][k] = al[k];
+    sa[1][k] = am[k];
+    sa[2][k] = at[k];
+    sa[3][k] = ar[k];
   }
   if (q < 9) sp[q] = sc->p_il[q];
   else if (q < 12) sp[q] = sc->p_m[q - 9];
   else if (q < 18) sp[q] = sc->p_lambda[q - 12];
   __syncthreads();
+  double* r_il = D.r_il + (size_t)b * D.K * 9;
+  double* r_m = D.r_m + (size_t)b * D.K * 3;
+  double* r_lam = D.r_lam + (size_t)b * D.K * 6;
   if (q < 18) {
     double* r = (q < 9) ? r_il + q : (q < 12) ? r_m + (q - 9) : r_lam + (q - 12);
     const int stride = (q < 9) ? 9 : (q < 12) ? 3 : 6;
@@ -191,8 +281,8 @@ __device__ void rot_advance_block(const Dev& D, Scal* sc, double* r_il, double* 
     double acc = 0.0, acc2 = 0.0;
     for (int k = 0; k < n2; ++k) {
       const double d = sd[k];
-      const double o = __dsub_rn(1.0, d);
-      const double x = __dadd_rn(__dmul_rn(d, r[k * stride]), __dmul_rn(o, p));
+      const double om = __dsub_rn(1.0, d);
+      const double x = __dadd_rn(__dmul_rn(d, r[k * stride]), __dmul_rn(om, p));
       r[k * stride] = x;
       if (q < 9) {
         acc = __dadd_rn(acc, __dmul_rn(sa[0][k], x));
@@ -211,13 +301,6 @@ __device__ void rot_advance_block(const Dev& D, Scal* sc, double* r_il, double* 
     }
   }
   if (q == 0) {
-    sc->numiter = 0;
-    sc->converged = 0;
-    sc->status = 0;
-    sc->gr_nacc = 0;
-    sc->gr_changed = 0;
-    sc->gr_reguess = 0;
-    sc->gr_ice_an = 0;
     for (int i = 0; i < 9; ++i) sc->oldil[i] = sp[i];
     for (int i = 0; i < 3; ++i) sc->oldm[i] = sp[9 + i];
     for (int i = 0; i < 6; ++i) sc->dlam_prev2[i] = sp[12 + i];
@@ -228,20 +311,21 @@ __device__ void rot_advance_block(const Dev& D, Scal* sc, double* r_il, double* 
 }
 
 // R_k <- d R_k + (1-d) P ; visc = sum_k a_sl R_k ; rad = sum_k a_rr R_k   (solver.py:386-407)
-// The last block advances the degree-2 rotational state instead.
-__global__ void __launch_bounds__(256) k_advance(Dev D, double2* __restrict__ R, const double2* __restrict__ P,
-                                                 double2* __restrict__ visc, double2* __restrict__ rad, Scal* sc,
-                                                 double* r_il, double* r_m, double* r_lam) {
+// The last block of each slot advances the degree-2 rotational state instead.
+__global__ void __launch_bounds__(256) k_advance(Dev D) {
+  SLOT_OR_RETURN();
   if (blockIdx.x == gridDim.x - 1) {
-    rot_advance_block(D, sc, r_il, r_m, r_lam);
+    rot_advance_block(D, b, sc);
     return;
   }
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef) return;
+  double2* R = D.R + (size_t)b * D.K * D.ncoef;
   const int l = D.lidx[i];
-  const double2 p = P[i];
+  const double2 p = D.sp(S_P_LOAD, b)[i];
+  const size_t o = D.kl(b);
   double2 v = make_double2(0.0, 0.0), r = v;
-  const int nk = D.nmod[l];
+  const int nk = D.nmod[(size_t)b * D.nl + l];
   constexpr int U = 4;
   for (int k0 = 0; k0 < nk; k0 += U) {
     double2 x[U];
@@ -252,11 +336,11 @@ __global__ void __launch_bounds__(256) k_advance(Dev D, double2* __restrict__ R,
     for (int u = 0; u < U; ++u) {
       const int k = k0 + u;
       if (k < nk) {
-        const int kl = k * D.nl + l;
-        const double d = D.decay[kl], o = D.omd[kl], as = D.a_sl[kl], ar = D.a_rr[kl];
+        const size_t kl = o + (size_t)k * D.nl + l;
+        const double d = D.decay[kl], om = D.omd[kl], as = D.a_sl[kl], ar = D.a_rr[kl];
         double2 y;
-        y.x = __dadd_rn(__dmul_rn(x[u].x, d), __dmul_rn(p.x, o));
-        y.y = __dadd_rn(__dmul_rn(x[u].y, d), __dmul_rn(p.y, o));
+        y.x = __dadd_rn(__dmul_rn(x[u].x, d), __dmul_rn(p.x, om));
+        y.y = __dadd_rn(__dmul_rn(x[u].y, d), __dmul_rn(p.y, om));
         R[(size_t)k * D.ncoef + i] = y;
         v.x = __dadd_rn(v.x, __dmul_rn(y.x, as));
         v.y = __dadd_rn(v.y, __dmul_rn(y.y, as));
@@ -265,59 +349,47 @@ __global__ void __launch_bounds__(256) k_advance(Dev D, double2* __restrict__ R,
       }
     }
   }
-  visc[i] = v;
-  rad[i] = r;
-}
-
-// grounded ice on topography `topo` (flotation test, solver.py:655-659)
-__device__ __forceinline__ double icestar_on(double ice, double topo, double rhow, double rhoi) {
-  const bool keep = (topo > 0.0) || (ice > __ddiv_rn(__dmul_rn(fabs(topo), rhow), rhoi));
-  return keep ? ice : __dmul_rn(ice, 0.0);
-}
-
-__device__ __forceinline__ double2 ld2(const double* p, long long i) {
-  return reinterpret_cast<const double2*>(p)[i];
-}
-__device__ __forceinline__ void st2(double* p, long long i, double a, double b) {
-  reinterpret_cast<double2*>(p)[i] = make_double2(a, b);
+  D.sp(S_VISC, b)[i] = v;
+  D.sp(S_RAD, b)[i] = r;
 }
 
 // Step prologue on the grid (solver.py:853-887): I* on the previous topography, beta,
-// C* = C beta, tO = T0 (C* - C*0); at step 1 also I* of the previous ice on T0.
-__global__ void k_ice_grid(Dev D, const double* __restrict__ ice, const double* __restrict__ topo_prev,
-                           const double* __restrict__ cxy, const double* __restrict__ tinit,
-                           const double* __restrict__ cstar0, double* __restrict__ icestar,
-                           double* __restrict__ beta, double* __restrict__ cstar, double* __restrict__ tO,
-                           const double* __restrict__ ice_prev, double* __restrict__ oldsrc, Scal* sc) {
+// C* = C beta, tO = T0 (C* - C*0); at the slot's first step also I* of the previous ice on T0.
+__global__ void k_ice_grid(Dev D) {
+  SLOT_OR_RETURN();
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h >= D.ng) return;
-  const double2 v = ld2(ice, h), tp = ld2(topo_prev, h), cx = ld2(cxy, h), ti = ld2(tinit, h), c0 = ld2(cstar0, h);
+  const double2 v = ld2(D.g(G_ICE, b), h), tp = ld2(D.g(G_TOPO_PREV, b), h), cx = ld2(D.g(G_CXY, b), h);
+  const double2 ti = ld2(D.g(G_TINIT, b), h), c0 = ld2(D.g(G_CSTAR0, b), h);
   if (!isfinite(v.x) || !isfinite(v.y)) sc->status = SLE_ERR_NONFINITE;
-  double is[2], b[2], c[2], t[2];
+  double is[2], bt[2], c[2], t[2];
   const double vv[2] = {v.x, v.y}, tt[2] = {tp.x, tp.y}, cc[2] = {cx.x, cx.y}, ii[2] = {ti.x, ti.y},
                zz[2] = {c0.x, c0.y};
 #pragma unroll
   for (int u = 0; u < 2; ++u) {
     is[u] = D.checkmarine ? icestar_on(vv[u], tt[u], D.rhow, D.rhoi) : vv[u];
-    b[u] = (is[u] < EPS0) ? 1.0 : 0.0;
-    c[u] = __dmul_rn(cc[u], b[u]);
+    bt[u] = (is[u] < EPS0) ? 1.0 : 0.0;
+    c[u] = __dmul_rn(cc[u], bt[u]);
     t[u] = __dmul_rn(ii[u], __dsub_rn(c[u], zz[u]));
   }
-  st2(icestar, h, is[0], is[1]);
-  st2(beta, h, b[0], b[1]);
-  st2(cstar, h, c[0], c[1]);
-  st2(tO, h, t[0], t[1]);
-  if (oldsrc) {
-    const double2 vp = ld2(ice_prev, h);
+  st2(D.g(G_ICESTAR, b), h, is[0], is[1]);
+  st2(D.g(G_BETA, b), h, bt[0], bt[1]);
+  st2(D.g(G_CSTAR, b), h, c[0], c[1]);
+  st2(D.g(G_TO, b), h, t[0], t[1]);
+  if (D.ss[b].first) {
+    const double2 vp = ld2(D.g(G_ICE_PREV, b), h);
     const double o0 = D.checkmarine ? icestar_on(vp.x, ti.x, D.rhow, D.rhoi) : vp.x;
     const double o1 = D.checkmarine ? icestar_on(vp.y, ti.y, D.rhow, D.rhoi) : vp.y;
-    st2(oldsrc, h, o0, o1);
+    st2(D.g(G_TMP, b), h, o0, o1);
   }
 }
 
 // The rotation block (solver.py:910-975) for the coming inner iteration, one thread; writes
 // il, m, Lambda, their increments and the degree-2 rotational sea-level / radial terms.
-__device__ void rotation_block(const Dev& D, const RotConst& C, const double2* dScur, const double2* dI, Scal* sc) {
+__device__ void rotation_block(const Dev& D, int b, Scal* sc) {
+  const RotConst& C = D.rc[b];
+  const double2* dScur = D.sp(S_DSCUR, b);
+  const double2* dI = D.sp(S_DI, b);
   // written by other blocks of the same kernel: read through L2
   const double2 s20 = __ldcg(dScur + D.i20), s21 = __ldcg(dScur + D.i21);
   const double2 i20 = __ldcg(dI + D.i20), i21 = __ldcg(dI + D.i21);
@@ -371,69 +443,74 @@ __device__ void rotation_block(const Dev& D, const RotConst& C, const double2* d
 }
 
 // dice = I*_lm - old ; dI = p_ice + dice ; first guess of the load increment ; dS_cur ;
-// so = sum|load_inc|  (solver.py:868-905; extrap solver_opt.py:504-513); the last block also
-// evaluates the rotation block for the first inner iteration.
-// mode: 0 eustatic, 1 extrap uniform (2 h1 - h2), 2 extrap variable (c1 h1 - c2 h2)
-__global__ void k_pre_spec(Dev D, RotConst C, const double2* __restrict__ icelm, const double2* __restrict__ oldice,
-                           const double2* __restrict__ p_ice, const double2* __restrict__ cstarlm,
-                           const double2* __restrict__ dSprev, const double2* __restrict__ h1,
-                           const double2* __restrict__ h2, int mode, double c1, double c2,
-                           double2* __restrict__ dice, double2* __restrict__ dI, double2* __restrict__ load,
-                           double2* __restrict__ dScur, Scal* sc, double* partials, unsigned int* counter) {
+// so = sum|load_inc|  (solver.py:868-905; extrap solver_opt.py:504-513).  old = the analysed
+// previous ice at the slot's first step, else the committed I*_lm of the last step (copied into
+// oldice here).  The last block evaluates the rotation block for the first inner iteration.
+__global__ void k_pre_spec(Dev D) {
+  SLOT_OR_RETURN();
   __shared__ double sh[32];
+  const SlotStep ss = D.ss[b];
+  const double2* icelm = D.sp(S_ICELM, b);
+  double2* oldice = D.sp(S_OLDICE, b);
+  const double2* osrc = ss.first ? oldice : D.sp(S_PREV_ICE, b);
+  const double2* h1 = D.sp(ss.hsel ? S_HB : S_HA, b);
+  const double2* h2 = D.sp(ss.hsel ? S_HA : S_HB, b);
+  const double2* cstarlm = D.sp(S_CSTARLM, b);
   double acc = 0.0;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < D.ncoef) {
-    const double2 dice00 = make_double2(__dsub_rn(icelm[0].x, oldice[0].x), __dsub_rn(icelm[0].y, oldice[0].y));
+    const double2 o0 = osrc[0];
+    const double2 dice00 = make_double2(__dsub_rn(icelm[0].x, o0.x), __dsub_rn(icelm[0].y, o0.y));
     const double fr = -D.rhoi / D.rhow;
     const double2 s00 = make_double2(__dmul_rn(fr, dice00.x), __dmul_rn(fr, dice00.y));
-    const double2 a = icelm[i], o = oldice[i];
+    const double2 a = icelm[i], o = osrc[i];
+    if (!ss.first) oldice[i] = o;
     const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
-    dice[i] = d;
-    const double2 pi = p_ice[i];
-    dI[i] = make_double2(__dadd_rn(pi.x, d.x), __dadd_rn(pi.y, d.y));
+    D.sp(S_DICE, b)[i] = d;
+    const double2 pi = D.sp(S_P_ICE, b)[i];
+    D.sp(S_DI, b)[i] = make_double2(__dadd_rn(pi.x, d.x), __dadd_rn(pi.y, d.y));
     double2 g;
-    if (mode == 0) {
+    if (ss.mode == 0) {
       g = np_cmul(np_cdiv(cstarlm[i], cstarlm[0]), s00);
-    } else if (mode == 1) {
+    } else if (ss.mode == 1) {
       const double2 u = h1[i], v = h2[i];
       g = make_double2(__dsub_rn(__dmul_rn(u.x, 2.0), v.x), __dsub_rn(__dmul_rn(u.y, 2.0), v.y));
     } else {
       const double2 u = h1[i], v = h2[i];
-      g = make_double2(__dsub_rn(__dmul_rn(u.x, c1), __dmul_rn(c2, v.x)),
-                       __dsub_rn(__dmul_rn(u.y, c1), __dmul_rn(c2, v.y)));
+      g = make_double2(__dsub_rn(__dmul_rn(u.x, ss.c1), __dmul_rn(ss.c2, v.x)),
+                       __dsub_rn(__dmul_rn(u.y, ss.c1), __dmul_rn(ss.c2, v.y)));
     }
-    load[i] = g;
-    if (mode == 0) {
-      dScur[i] = make_double2(0.0, 0.0);
+    D.sp(S_LOAD, b)[i] = g;
+    if (ss.mode == 0) {
+      D.sp(S_DSCUR, b)[i] = make_double2(0.0, 0.0);
     } else {
-      const double2 p = dSprev[i];
-      dScur[i] = make_double2(__dadd_rn(p.x, g.x), __dadd_rn(p.y, g.y));
+      const double2 p = D.sp(S_P_OCEAN, b)[i];
+      D.sp(S_DSCUR, b)[i] = make_double2(__dadd_rn(p.x, g.x), __dadd_rn(p.y, g.y));
     }
     acc = cabs_(g);
   }
   const double part = block_sum(acc, sh);
   double tot;
-  if (last_block_total(part, partials, counter, &tot, sh)) {
+  if (last_block_total(part, D.partials + (size_t)b * D.npart, D.counter + 4 * b, &tot, sh)) {
     if (threadIdx.x == 0) {
       sc->so = tot;
-      if (D.tpw) rotation_block(D, C, dScur, dI, sc);
+      if (D.tpw) rotation_block(D, b, sc);
     }
   }
 }
 
 // Eq. B18 (solver.py:977-991) plus the degree-2 rotational term of the current iteration.
-__global__ void k_b18(Dev D, const double2* __restrict__ dI, const double2* __restrict__ dSprev,
-                      const double2* __restrict__ load, const double2* __restrict__ visc,
-                      double2* __restrict__ sl, Scal* sc) {
+__global__ void k_b18(Dev D) {
+  SLOT_OR_RETURN();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef) return;
   if (i == 0) sc->gr_changed = 0;  // the previous iteration's grounded-mask change is consumed
   const int l = D.lidx[i];
-  const double2 a = dI[i], b = dSprev[i], c = load[i], v = visc[i];
-  const double te = D.ttlekhl[l], t = D.ttl[l];
-  double re = __dadd_rn(__dadd_rn(__dmul_rn(a.x, D.rhoi), __dmul_rn(b.x, D.rhow)), __dmul_rn(c.x, D.rhow));
-  double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(b.y, D.rhow)), __dmul_rn(c.y, D.rhow));
+  const double2 a = D.sp(S_DI, b)[i], bb = D.sp(S_P_OCEAN, b)[i], c = D.sp(S_LOAD, b)[i];
+  const double2 v = D.sp(S_VISC, b)[i];
+  const double te = D.ttlekhl[(size_t)b * D.nl + l], t = D.ttl[(size_t)b * D.nl + l];
+  double re = __dadd_rn(__dadd_rn(__dmul_rn(a.x, D.rhoi), __dmul_rn(bb.x, D.rhow)), __dmul_rn(c.x, D.rhow));
+  double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(bb.y, D.rhow)), __dmul_rn(c.y, D.rhow));
   re = __dadd_rn(__dmul_rn(re, te), __dmul_rn(v.x, t));
   im = __dadd_rn(__dmul_rn(im, te), __dmul_rn(v.y, t));
   if (D.tpw) {
@@ -443,18 +520,20 @@ __global__ void k_b18(Dev D, const double2* __restrict__ dI, const double2* __re
       im = __dadd_rn(im, sc->dsl_rot[2 * q + 1]);
     }
   }
-  sl[i] = make_double2(re, im);
+  D.sp(S_SL, b)[i] = make_double2(re, im);
 }
 
 // conserv, the load update and xi (solver.py:1002-1030):
 //   new = ((-dSprev + rO) + C*_lm conserv) - tO ;  dS_cur = dSprev + new ;  sa = sum|new|
-// The last block decides convergence and sets the graph loop condition.
-__global__ void k_update(Dev D, RotConst C, const double2* __restrict__ dSprev, const double2* __restrict__ rOlm,
-                         const double2* __restrict__ cstarlm, const double2* __restrict__ tOlm,
-                         const double2* __restrict__ dI, double2* __restrict__ load,
-                         double2* __restrict__ dScur, Scal* sc, double* partials, unsigned int* counter,
-                         cudaGraphConditionalHandle loop) {
+// The slot's last block decides its convergence.
+__global__ void k_update(Dev D) {
+  SLOT_OR_RETURN();
   __shared__ double sh[32];
+  const double2* dSprev = D.sp(S_P_OCEAN, b);
+  const double2* rOlm = D.sp(S_ROLM, b);
+  const double2* cstarlm = D.sp(S_CSTARLM, b);
+  const double2* tOlm = D.sp(S_TOLM, b);
+  const double2* dI = D.sp(S_DI, b);
   // conserv = ((1 / C*_00) * (-(rhoi/rhow) dI_00 - rO_00 + tO_00)).real
   const double2 c00 = cstarlm[0];
   const double2 rinv = np_cdiv(make_double2(1.0, 0.0), c00);
@@ -472,13 +551,13 @@ __global__ void k_update(Dev D, RotConst C, const double2* __restrict__ dSprev, 
     ni = __dadd_rn(ni, __dmul_rn(c.y, conserv));
     nr = __dsub_rn(nr, t.x);
     ni = __dsub_rn(ni, t.y);
-    load[i] = make_double2(nr, ni);
-    dScur[i] = make_double2(__dadd_rn(p.x, nr), __dadd_rn(p.y, ni));
+    D.sp(S_LOAD, b)[i] = make_double2(nr, ni);
+    D.sp(S_DSCUR, b)[i] = make_double2(__dadd_rn(p.x, nr), __dadd_rn(p.y, ni));
     acc = hypot(nr, ni);
   }
   const double part = block_sum(acc, sh);
   double sa;
-  if (last_block_total(part, partials, counter, &sa, sh)) {
+  if (last_block_total(part, D.partials + (size_t)b * D.npart, D.counter + 4 * b, &sa, sh)) {
     if (threadIdx.x == 0) {
       const double so = sc->so;
       double xi;
@@ -491,7 +570,7 @@ __global__ void k_update(Dev D, RotConst C, const double2* __restrict__ dSprev, 
       sc->so = sa;
       sc->numiter += 1;
       if (sc->status != 0 || !(xi == xi) || !isfinite(sa)) {
-        sc->status = SLE_ERR_NONFINITE;
+        if (sc->status == 0) sc->status = SLE_ERR_NONFINITE;
         sc->converged = 1;
       } else if (xi <= D.epsilon1) {
         sc->converged = 1;
@@ -499,40 +578,37 @@ __global__ void k_update(Dev D, RotConst C, const double2* __restrict__ dSprev, 
         sc->status = SLE_ERR_NONCONVERGED;
         sc->converged = 1;
       }
-      if (loop) cudaGraphSetConditional(loop, sc->converged ? 0u : 1u);
     }
   }
 }
 
 // sl_tot = sl_inc with conserv added to (0,0) (plain path, solver.py:1017-1021)
-__global__ void k_sltot(Dev D, const double2* __restrict__ sl, double2* __restrict__ sltot, const Scal* sc) {
+__global__ void k_sltot(Dev D) {
+  SLOT_OR_RETURN();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef) return;
-  double2 v = sl[i];
+  double2 v = D.sp(S_SL, b)[i];
   if (i == 0) v.x = __dadd_rn(v.x, sc->conserv);
-  sltot[i] = v;
+  D.sp(S_SLTOT, b)[i] = v;
 }
 
 // deltasl (dsl identity) and, when not converged, topography / ocean function refresh and
 // the grounded-ice test on the new topography (solver.py:1032-1037, 661-684).  One extra block
-// (the last) evaluates the rotation block of the next iteration meanwhile.
-__global__ void k_refresh1(Dev D, RotConst C, const double2* __restrict__ dScur, const double2* __restrict__ dI,
-                           const double* __restrict__ dsl, double* __restrict__ deltasl,
-                           const double* __restrict__ tinit, double* __restrict__ topo,
-                           double* __restrict__ cxy, const double* __restrict__ ice,
-                           const double* __restrict__ beta, double* __restrict__ grnew, Scal* sc,
-                           double* partials, unsigned int* counter) {
+// per slot (the last) evaluates the rotation block of the next iteration meanwhile.
+__global__ void k_refresh1(Dev D) {
+  SLOT_OR_RETURN();
   __shared__ double sh[32];
   const bool conv = sc->converged != 0;
   const bool test = !conv && D.checkmarine && sc->gr_nacc < GR_MAXACC;
   const double cadd = D.opt_dsl ? __dmul_rn(sc->conserv, sc->K00) : 0.0;
   double cnt = 0.0;
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0 && !conv && D.tpw) rotation_block(D, C, dScur, dI, sc);
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0 && !conv && D.tpw) rotation_block(D, b, sc);
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h < D.ng) {
     double ds[2];
+    double* deltasl = D.g(G_DELTASL, b);
     if (D.opt_dsl) {
-      const double2 a = ld2(dsl, h);
+      const double2 a = ld2(D.g(G_DSL, b), h);
       ds[0] = __dadd_rn(a.x, cadd);
       ds[1] = __dadd_rn(a.y, cadd);
       st2(deltasl, h, ds[0], ds[1]);
@@ -542,15 +618,15 @@ __global__ void k_refresh1(Dev D, RotConst C, const double2* __restrict__ dScur,
       ds[1] = a.y;
     }
     if (!conv) {
-      const double2 ti = ld2(tinit, h);
+      const double2 ti = ld2(D.g(G_TINIT, b), h);
       const double t0 = __dsub_rn(ti.x, ds[0]), t1 = __dsub_rn(ti.y, ds[1]);
-      st2(topo, h, t0, t1);
-      st2(cxy, h, (t0 < 0.0) ? 1.0 : 0.0, (t1 < 0.0) ? 1.0 : 0.0);
+      st2(D.g(G_TOPO, b), h, t0, t1);
+      st2(D.g(G_CXY, b), h, (t0 < 0.0) ? 1.0 : 0.0, (t1 < 0.0) ? 1.0 : 0.0);
       if (test) {
-        const double2 ic = ld2(ice, h), be = ld2(beta, h);
+        const double2 ic = ld2(D.g(G_ICE, b), h), be = ld2(D.g(G_BETA, b), h);
         const double g0 = icestar_on(ic.x, t0, D.rhow, D.rhoi);
         const double g1 = icestar_on(ic.y, t1, D.rhow, D.rhoi);
-        st2(grnew, h, g0, g1);
+        st2(D.g(G_GRNEW, b), h, g0, g1);
         if ((g0 < EPS0) != (be.x != 0.0)) cnt += 1.0;
         if ((g1 < EPS0) != (be.y != 0.0)) cnt += 1.0;
       }
@@ -559,7 +635,7 @@ __global__ void k_refresh1(Dev D, RotConst C, const double2* __restrict__ dScur,
   if (!test) return;
   const double part = block_sum(cnt, sh);
   double tot;
-  if (last_block_total(part, partials, counter, &tot, sh)) {
+  if (last_block_total(part, D.partials + (size_t)b * D.npart + D.part_grid, D.counter + 4 * b + 1, &tot, sh)) {
     if (threadIdx.x == 0) {
       sc->gr_reguess += 1;
       sc->nd = (unsigned int)tot;
@@ -575,55 +651,80 @@ __global__ void k_refresh1(Dev D, RotConst C, const double2* __restrict__ dScur,
 }
 
 // C* and tO on the refreshed ocean function; accepted grounded-ice mask (solver.py:664-684)
-__global__ void k_refresh2(Dev D, const double* __restrict__ cxy, const double* __restrict__ tinit,
-                           const double* __restrict__ cstar0, const double* __restrict__ grnew,
-                           double* __restrict__ icestar, double* __restrict__ beta,
-                           double* __restrict__ cstar, double* __restrict__ tO, const Scal* sc) {
+__global__ void k_refresh2(Dev D) {
+  SLOT_OR_RETURN();
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h >= D.ng || sc->converged) return;
   const int changed = sc->gr_changed;
-  double2 b;
+  double2 bt;
   if (changed) {
-    const double2 g = ld2(grnew, h);
-    st2(icestar, h, g.x, g.y);
-    b = make_double2((g.x < EPS0) ? 1.0 : 0.0, (g.y < EPS0) ? 1.0 : 0.0);
-    st2(beta, h, b.x, b.y);
+    const double2 g = ld2(D.g(G_GRNEW, b), h);
+    st2(D.g(G_ICESTAR, b), h, g.x, g.y);
+    bt = make_double2((g.x < EPS0) ? 1.0 : 0.0, (g.y < EPS0) ? 1.0 : 0.0);
+    st2(D.g(G_BETA, b), h, bt.x, bt.y);
   } else {
-    b = ld2(beta, h);
+    bt = ld2(D.g(G_BETA, b), h);
   }
-  const double2 cx = ld2(cxy, h), ti = ld2(tinit, h), c0 = ld2(cstar0, h);
-  const double c_0 = __dmul_rn(cx.x, b.x), c_1 = __dmul_rn(cx.y, b.y);
-  st2(cstar, h, c_0, c_1);
-  st2(tO, h, __dmul_rn(ti.x, __dsub_rn(c_0, c0.x)), __dmul_rn(ti.y, __dsub_rn(c_1, c0.y)));
+  const double2 cx = ld2(D.g(G_CXY, b), h), ti = ld2(D.g(G_TINIT, b), h), c0 = ld2(D.g(G_CSTAR0, b), h);
+  const double c_0 = __dmul_rn(cx.x, bt.x), c_1 = __dmul_rn(cx.y, bt.y);
+  st2(D.g(G_CSTAR, b), h, c_0, c_1);
+  st2(D.g(G_TO, b), h, __dmul_rn(ti.x, __dsub_rn(c_0, c0.x)), __dmul_rn(ti.y, __dsub_rn(c_1, c0.y)));
 }
 
-// dice, dI after a grounded-mask change; the last block re-evaluates the rotation block
-__global__ void k_dice(Dev D, RotConst C, const double2* __restrict__ icelm, const double2* __restrict__ oldice,
-                       const double2* __restrict__ p_ice, double2* __restrict__ dice, double2* __restrict__ dI,
-                       const double2* __restrict__ dScur, Scal* sc, unsigned int* counter) {
+// dice, dI after a grounded-mask change; the slot's last block re-evaluates the rotation block
+__global__ void k_dice(Dev D) {
+  SLOT_OR_RETURN();
   if (sc->converged || !sc->gr_changed) return;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < D.ncoef) {
-    const double2 a = icelm[i], o = oldice[i], p = p_ice[i];
+    const double2 a = D.sp(S_ICELM, b)[i], o = D.sp(S_OLDICE, b)[i], p = D.sp(S_P_ICE, b)[i];
     const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
-    dice[i] = d;
-    dI[i] = make_double2(__dadd_rn(p.x, d.x), __dadd_rn(p.y, d.y));
+    D.sp(S_DICE, b)[i] = d;
+    D.sp(S_DI, b)[i] = make_double2(__dadd_rn(p.x, d.x), __dadd_rn(p.y, d.y));
   }
   if (!D.tpw) return;
-  if (last_block(counter) && threadIdx.x == 0) rotation_block(D, C, dScur, dI, sc);
+  if (last_block(D.counter + 4 * b + 2) && threadIdx.x == 0) rotation_block(D, b, sc);
+}
+
+// End of an inner iteration: slots that converged (or failed) are done from the next iteration
+// on; the loop goes on while any slot is not.  A raised tensor-core timeout ends every slot.
+__global__ void k_loop_cond(Dev D, const int* bstatus, cudaGraphConditionalHandle loop) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  const int bs = *bstatus;
+  for (int b = threadIdx.x; b < D.nslot; b += blockDim.x) {
+    Scal* sc = D.sc + b;
+    if (sc->done) continue;
+    if (bs != 0) {
+      if (sc->status == 0) sc->status = bs;
+      sc->converged = 1;
+    }
+    if (sc->converged) sc->done = 1;
+    else atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && loop) cudaGraphSetConditional(loop, any ? 1u : 0u);
+}
+
+// After the loop: re-open the slots that step in this call for the post-loop kernels.
+__global__ void k_reopen(Dev D) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= D.nslot) return;
+  if (D.ss[b].active) D.sc[b].done = 0;
 }
 
 // Radial displacement spectrum (solver.py:1054-1069)
-__global__ void k_rr(Dev D, const double2* __restrict__ dI, const double2* __restrict__ dSprev,
-                     const double2* __restrict__ load, const double2* __restrict__ rad,
-                     double2* __restrict__ rr, const Scal* sc) {
+__global__ void k_rr(Dev D) {
+  SLOT_OR_RETURN();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef || sc->status) return;
   const int l = D.lidx[i];
-  const double2 a = dI[i], b = dSprev[i], c = load[i], v = rad[i];
-  const double th = D.ttlhe[l], t = D.ttl[l];
-  double re = __dadd_rn(__dadd_rn(__dmul_rn(a.x, D.rhoi), __dmul_rn(b.x, D.rhow)), __dmul_rn(c.x, D.rhow));
-  double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(b.y, D.rhow)), __dmul_rn(c.y, D.rhow));
+  const double2 a = D.sp(S_DI, b)[i], bb = D.sp(S_P_OCEAN, b)[i], c = D.sp(S_LOAD, b)[i];
+  const double2 v = D.sp(S_RAD, b)[i];
+  const double th = D.ttlhe[(size_t)b * D.nl + l], t = D.ttl[(size_t)b * D.nl + l];
+  double re = __dadd_rn(__dadd_rn(__dmul_rn(a.x, D.rhoi), __dmul_rn(bb.x, D.rhow)), __dmul_rn(c.x, D.rhow));
+  double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(bb.y, D.rhow)), __dmul_rn(c.y, D.rhow));
   re = __dadd_rn(__dmul_rn(re, th), __dmul_rn(v.x, t));
   im = __dadd_rn(__dmul_rn(im, th), __dmul_rn(v.y, t));
   if (D.tpw) {
@@ -633,54 +734,55 @@ __global__ void k_rr(Dev D, const double2* __restrict__ dI, const double2* __res
       im = __dadd_rn(im, sc->rr_rot[2 * q + 1]);
     }
   }
-  rr[i] = make_double2(re, im);
+  D.sp(S_RRLM, b)[i] = make_double2(re, im);
 }
 
 // commit (solver.py:1080-1096): cur = rhoi dice + rhow load (l = 0 zeroed); p_load += cur;
-// p_ice = dI ; p_ocean = dS_cur ; prev_ice = I*_lm ; extrap history h_new = load; thread 0
-// also commits the rotational increments.
-__global__ void k_commit(Dev D, const double2* __restrict__ dice, const double2* __restrict__ load,
-                         const double2* __restrict__ dI, const double2* __restrict__ dScur,
-                         const double2* __restrict__ icelm, double2* __restrict__ p_load,
-                         double2* __restrict__ p_ice, double2* __restrict__ p_ocean,
-                         double2* __restrict__ prev_ice, double2* __restrict__ hist_new, Scal* sc) {
+// p_ice = dI ; p_ocean = dS_cur ; prev_ice = I*_lm ; extrap history (the older buffer) = load;
+// thread 0 also commits the rotational increments and records I*_00.
+__global__ void k_commit(Dev D, int extrap) {
+  SLOT_OR_RETURN();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef || sc->status) return;
-  if (i == 0 && D.tpw) {
-    for (int q = 0; q < 9; ++q) sc->p_il[q] = __dadd_rn(sc->p_il[q], sc->dil[q]);
-    for (int q = 0; q < 3; ++q) sc->p_m[q] = __dadd_rn(sc->p_m[q], sc->dm[q]);
-    for (int q = 0; q < 6; ++q) sc->p_lambda[q] = __dadd_rn(sc->p_lambda[q], sc->dlam_cur2[q]);
+  if (i == 0) {
+    if (D.tpw) {
+      for (int q = 0; q < 9; ++q) sc->p_il[q] = __dadd_rn(sc->p_il[q], sc->dil[q]);
+      for (int q = 0; q < 3; ++q) sc->p_m[q] = __dadd_rn(sc->p_m[q], sc->dm[q]);
+      for (int q = 0; q < 6; ++q) sc->p_lambda[q] = __dadd_rn(sc->p_lambda[q], sc->dlam_cur2[q]);
+    }
+    sc->diag[4] = D.sp(S_ICELM, b)[0].x;
   }
   const int l = D.lidx[i];
   double2 cur = make_double2(0.0, 0.0);
-  const double2 ld = load[i];
+  const double2 ld = D.sp(S_LOAD, b)[i];
   if (l != 0) {
-    const double2 d = dice[i];
+    const double2 d = D.sp(S_DICE, b)[i];
     cur = make_double2(__dadd_rn(__dmul_rn(d.x, D.rhoi), __dmul_rn(ld.x, D.rhow)),
                        __dadd_rn(__dmul_rn(d.y, D.rhoi), __dmul_rn(ld.y, D.rhow)));
   }
+  double2* p_load = D.sp(S_P_LOAD, b);
   const double2 p = p_load[i];
   p_load[i] = make_double2(__dadd_rn(p.x, cur.x), __dadd_rn(p.y, cur.y));
-  p_ice[i] = dI[i];
-  p_ocean[i] = dScur[i];
-  prev_ice[i] = icelm[i];
-  if (hist_new) hist_new[i] = ld;
+  D.sp(S_P_ICE, b)[i] = D.sp(S_DI, b)[i];
+  D.sp(S_P_OCEAN, b)[i] = D.sp(S_DSCUR, b)[i];
+  D.sp(S_PREV_ICE, b)[i] = D.sp(S_ICELM, b)[i];
+  if (extrap) D.sp(D.ss[b].hsel ? S_HA : S_HB, b)[i] = ld;
 }
 
 // Post-step topography / ocean function (solver.py:1099-1101) and, for the diag option, the
-// row sums of the four degree-0 diagnostics (solver_opt.py:893-916): block per row; the last
-// block forms U00 = sum_j P~_00 w_j rowsum_j / (nlon 1.41421356), P~_00 = sqrt(0.5).
-__global__ void k_post_grid(Dev D, const double* __restrict__ tinit, const double* __restrict__ deltasl,
-                            const double* __restrict__ beta, double* __restrict__ topo,
-                            double* __restrict__ topo_prev, double* __restrict__ cxy,
-                            double* __restrict__ slc, double* __restrict__ slcb, double* __restrict__ cstar,
-                            double* __restrict__ rows /* [4][nlat] or null */, const double* __restrict__ w,
-                            Scal* sc, unsigned int* counter) {
+// row sums of the four degree-0 diagnostics (solver_opt.py:893-916): block per row; the slot's
+// last block forms U00 = sum_j P~_00 w_j rowsum_j / (nlon 1.41421356), P~_00 = sqrt(0.5).
+// Without diag the three diagnostic grids are written for full analyses instead.
+__global__ void k_post_grid(Dev D, int diag) {
+  SLOT_OR_RETURN();
   __shared__ double sh[32];
   const int j = blockIdx.x;
   if (sc->status) return;
-  double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
+  double a = 0.0, bs = 0.0, c = 0.0, d = 0.0;
   const long long row = (long long)j * (D.nlon / 2);
+  const double *deltasl = D.g(G_DELTASL, b), *tinit = D.g(G_TINIT, b), *beta = D.g(G_BETA, b);
+  double *topo = D.g(G_TOPO, b), *topo_prev = D.g(G_TOPO_PREV, b), *cxy = D.g(G_CXY, b);
+  double *slc = D.g(G_TMP, b), *slcb = D.g(G_TMP3, b), *cstar = D.g(G_TMP4, b);
   for (int t = threadIdx.x; t < D.nlon / 2; t += blockDim.x) {
     const long long h = row + t;
     const double2 ds = ld2(deltasl, h), ti = ld2(tinit, h), bb = ld2(beta, h);
@@ -694,61 +796,71 @@ __global__ void k_post_grid(Dev D, const double* __restrict__ tinit, const doubl
       s2[u] = __dmul_rn(s1[u], bv[u]);
       cs[u] = __dmul_rn(o[u], bv[u]);
       a += s1[u];
-      b += o[u];
+      bs += o[u];
       c += s2[u];
       d += cs[u];
     }
     st2(topo, h, tp[0], tp[1]);
     st2(topo_prev, h, tp[0], tp[1]);
     st2(cxy, h, o[0], o[1]);
-    if (slc) {
+    if (!diag) {
       st2(slc, h, s1[0], s1[1]);
       st2(slcb, h, s2[0], s2[1]);
       st2(cstar, h, cs[0], cs[1]);
     }
   }
-  if (!rows) return;
+  if (!diag) return;
+  double* rows = D.rows + (size_t)b * 4 * D.nlat;
   a = block_sum(a, sh);
-  b = block_sum(b, sh);
+  bs = block_sum(bs, sh);
   c = block_sum(c, sh);
   d = block_sum(d, sh);
   if (threadIdx.x == 0) {
     rows[j] = a;
-    rows[D.nlat + j] = b;
+    rows[D.nlat + j] = bs;
     rows[2 * D.nlat + j] = c;
     rows[3 * D.nlat + j] = d;
   }
-  if (!last_block(counter)) return;
+  if (!last_block(D.counter + 4 * b + 3)) return;
   for (int q = 0; q < 4; ++q) {
     double acc = 0.0;
-    for (int jj = threadIdx.x; jj < D.nlat; jj += blockDim.x) acc += w[jj] * ((volatile double*)rows)[q * D.nlat + jj];
+    for (int jj = threadIdx.x; jj < D.nlat; jj += blockDim.x) acc += D.w[jj] * ((volatile double*)rows)[q * D.nlat + jj];
     acc = block_sum(acc, sh);
     if (threadIdx.x == 0) sc->diag[q] = sqrt(0.5) * acc / (double)D.nlon / SQRT2_LEGACY;
     __syncthreads();
   }
 }
 
-__global__ void k_grid_add(long long n, const double* a, const double* b, double* out) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = __dadd_rn(a[i], b[i]);
+// Without the diag option: the (0,0) coefficients of the four diagnostic analyses
+__global__ void k_diag00(Dev D) {
+  const int b = D.slot0 + (int)blockIdx.x;
+  Scal* sc = D.sc + b;
+  if (sc->done || sc->status || threadIdx.x != 0) return;
+  sc->diag[0] = D.sp(S_SP0, b)[0].x;
+  sc->diag[1] = D.sp(S_SP1, b)[0].x;
+  sc->diag[2] = D.sp(S_SP2, b)[0].x;
+  sc->diag[3] = D.sp(S_SP3, b)[0].x;
 }
 
-__global__ void k_init_grid(Dev D, const double* __restrict__ tinit, const double* __restrict__ ice0,
-                            double* __restrict__ cxy0, double* __restrict__ beta0, double* __restrict__ cstar0,
-                            double* __restrict__ cxy, double* __restrict__ topo_prev, double* __restrict__ ic0) {
+__global__ void k_grid_add(long long n, const double* a, const double* c, double* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = __dadd_rn(a[i], c[i]);
+}
+
+__global__ void k_init_grid(Dev D, int b) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ng) return;
-  const double t = tinit[i];
+  const double t = D.g(G_TINIT, b)[i];
   const double c = (t < 0.0) ? 1.0 : 0.0;
-  cxy0[i] = c;
-  cxy[i] = c;
-  topo_prev[i] = t;
-  const double v = ice0[i];
-  const double g = D.checkmarine ? icestar_on(v, t, D.rhow, D.rhoi) : v;
-  ic0[i] = g;
-  const double b = (g < EPS0) ? 1.0 : 0.0;
-  beta0[i] = b;
-  cstar0[i] = __dmul_rn(c, b);
+  D.g(G_CXY0, b)[i] = c;
+  D.g(G_CXY, b)[i] = c;
+  D.g(G_TOPO_PREV, b)[i] = t;
+  const double v = D.g(G_ICE_PREV, b)[i];
+  const double gg = D.checkmarine ? icestar_on(v, t, D.rhow, D.rhoi) : v;
+  D.g(G_ICESTAR, b)[i] = gg;
+  const double bt = (gg < EPS0) ? 1.0 : 0.0;
+  D.g(G_BETA0, b)[i] = bt;
+  D.g(G_CSTAR0, b)[i] = __dmul_rn(c, bt);
 }
 
 __global__ void k_finite(long long n, const double* a, unsigned int* bad) {
@@ -756,45 +868,69 @@ __global__ void k_finite(long long n, const double* a, unsigned int* bad) {
   if (i < n && !isfinite(a[i])) atomicOr(bad, 1u);
 }
 
+// Slot record after loading: not stepping, K00 of the grid.
+__global__ void k_slot_reset(Dev D, int b, double K00) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  Scal* sc = D.sc + b;
+  memset(sc, 0, sizeof(Scal));
+  sc->K00 = K00;
+  sc->converged = 1;
+  sc->done = 1;
+}
+
 }  // namespace sle
 
 // ============================================================================ handle
 using namespace sle;
 
-struct sle_solver {
+namespace {
+
+struct SlotHost {
+  int loaded, inited;
+  int iter, nhist, hsel;
+  double dt, dt_cur, dt_hist[2];
+  double ocean_area0, oceanBeta_area0, ice_volume0;
+  sle_step_info last;
+};
+
+}  // namespace
+
+struct sle_batch {
   sle_config cfg;
+  int nslot, K;
   sle_sht* plan;
   cudaStream_t st;
   Dev D;
-  RotConst C;
-  int K, nmod2;
-  // earth
-  double *s_kl, *decay, *omd, *a_sl, *a_rr, *ttl, *ttlekhl, *ttlhe, *a_il, *a_m, *a_tsl, *a_trr;
+  // device allocations
+  double* grid;
+  double2 *spec, *R;
   int* nmod;
+  double *s_kl, *decay, *omd, *a_sl, *a_rr, *ttl, *ttlekhl, *ttlhe, *a_il, *a_m, *a_tsl, *a_trr;
+  RotConst* rc;
   double *r_il, *r_m, *r_lam;
-  // grids
-  double *tinit, *cxy0, *beta0, *cstar0, *cxy, *topo_prev, *icestar, *beta, *cstar, *tO, *rO, *dsl, *deltasl,
-      *topo, *rr, *grnew, *ice, *ice_prev, *tmpg, *gbuf3, *gbuf4, *rows;
-  // spectra (packed)
-  double2 *R, *p_load, *p_ice, *p_ocean, *prev_ice, *visc, *rad, *icelm, *oldice, *dice, *dI, *cstarlm, *tOlm,
-      *rOlm, *load, *dScur, *sl, *sltot, *rrlm, *h1, *h2, *spare[4];
   Scal* sc;
-  Scal* hsc;  // pinned mirror
+  SlotStep* ss;
   double* partials;
-  long long part_grid;   // offset of the grid-reduction partials
   unsigned int* counter;
+  double* rows;
   unsigned int* badflag;
+  int* bstatus;            // batch-wide status raised by a tensor-core timeout
+  // pinned mirrors
+  Scal* hsc;
+  SlotStep* hss;
+  std::vector<SlotHost> slot;
   double K00;
-  int iter, inited, nhist;
-  double dt_cur, dt_hist[2];
-  double ocean_area0, oceanBeta_area0, ice_volume0;
-  sle_step_info last;
   // inner loop as a CUDA graph with a device-evaluated WHILE condition
   cudaGraph_t loop_graph;
   cudaGraphExec_t loop_exec;
-  cudaGraphConditionalHandle loop_cond;
   int use_graph;
   long long body_launches;   // kernels in one iteration of the graph body
+  // static field lists of the loop body
+  std::vector<FieldSpec> f_syn_sl, f_ana_ro, f_syn_sltot, f_ana_refresh;
+};
+
+struct sle_solver {
+  sle_batch* b;
 };
 
 namespace {
@@ -812,19 +948,15 @@ int dalloc(T** p, size_t n) {
 
 inline unsigned nb(long long n, int bs = 256) { return (unsigned)((n + bs - 1) / bs); }
 
-void solver_free(sle_solver* s) {
+void batch_free(sle_batch* s) {
   if (!s) return;
-  void* ptrs[] = {s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr, s->ttl, s->ttlekhl, s->ttlhe, s->a_il, s->a_m,
-                  s->a_tsl, s->a_trr, s->nmod, s->r_il, s->r_m, s->r_lam, s->tinit, s->cxy0, s->beta0,
-                  s->cstar0, s->cxy, s->topo_prev, s->icestar, s->beta, s->cstar, s->tO, s->rO, s->dsl,
-                  s->deltasl, s->topo, s->rr, s->grnew, s->ice, s->ice_prev, s->tmpg, s->gbuf3, s->gbuf4,
-                  s->rows, s->R, s->p_load, s->p_ice, s->p_ocean, s->prev_ice, s->visc, s->rad, s->icelm,
-                  s->oldice, s->dice, s->dI, s->cstarlm, s->tOlm, s->rOlm, s->load, s->dScur, s->sl,
-                  s->sltot, s->rrlm, s->h1, s->h2, s->spare[0], s->spare[1], s->spare[2], s->spare[3],
-                  s->sc, s->partials, s->counter, s->badflag};
+  void* ptrs[] = {s->grid, s->spec, s->R, s->nmod, s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr, s->ttl,
+                  s->ttlekhl, s->ttlhe, s->a_il, s->a_m, s->a_tsl, s->a_trr, s->rc, s->r_il, s->r_m,
+                  s->r_lam, s->sc, s->ss, s->partials, s->counter, s->rows, s->badflag, s->bstatus};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (s->hsc) cudaFreeHost(s->hsc);
+  if (s->hss) cudaFreeHost(s->hss);
   if (s->loop_exec) cudaGraphExecDestroy(s->loop_exec);
   if (s->loop_graph) cudaGraphDestroy(s->loop_graph);
   if (s->st) cudaStreamDestroy(s->st);
@@ -837,13 +969,13 @@ int upload(void* dst, const void* src, size_t bytes, int on_device, cudaStream_t
   return SLE_OK;
 }
 
-int sync_scal(sle_solver* s) {
-  SLE_CUDA(cudaMemcpyAsync(s->hsc, s->sc, sizeof(Scal), cudaMemcpyDeviceToHost, s->st));
+int sync_scal(sle_batch* s) {
+  SLE_CUDA(cudaMemcpyAsync(s->hsc, s->sc, sizeof(Scal) * s->nslot, cudaMemcpyDeviceToHost, s->st));
   SLE_CUDA(cudaStreamSynchronize(s->st));
   return SLE_OK;
 }
 
-int check_finite(sle_solver* s, const double* dev, long long n, const char* what) {
+int check_finite(sle_batch* s, const double* dev, long long n, const char* what) {
   SLE_CUDA(cudaMemsetAsync(s->badflag, 0, sizeof(unsigned int), s->st));
   note_launch();
   k_finite<<<nb(n), 256, 0, s->st>>>(n, dev, s->badflag);
@@ -857,73 +989,59 @@ int check_finite(sle_solver* s, const double* dev, long long n, const char* what
   return SLE_OK;
 }
 
-int set_dt(sle_solver* s, double dt) {
-  if (dt == s->dt_cur) return SLE_OK;
+int set_dt(sle_batch* s, int b, double dt) {
+  SlotHost& h = s->slot[b];
+  if (dt == h.dt_cur) return SLE_OK;
   note_launch();
-  k_set_decay<<<nb((long long)s->K * s->D.nl), 256, 0, s->st>>>(s->K, s->D.nl, s->s_kl, s->nmod, dt, s->decay,
-                                                               s->omd);
+  k_set_decay<<<nb((long long)s->K * s->D.nl), 256, 0, s->st>>>(s->D, b, dt);
   SLE_CUDA(cudaGetLastError());
-  s->dt_cur = dt;
+  h.dt_cur = dt;
   return SLE_OK;
 }
 
-int ana(sle_solver* s, int nf, const double* g0, double2* o0, const double* g1 = nullptr, double2* o1 = nullptr,
-        const double* g2 = nullptr, double2* o2 = nullptr, const double* g3 = nullptr, double2* o3 = nullptr) {
-  const double* g[4] = {g0, g1, g2, g3};
-  double2* o[4] = {o0, o1, o2, o3};
-  return sht_analysis_packed(s->plan, nf, g, o, s->st);
+FieldSpec fspec(double* grid, double2* spec, const int* skip_set = nullptr, const int* skip_clear = nullptr,
+                double* epi_out = nullptr, const double* epi_mul = nullptr) {
+  return FieldSpec{grid, spec, skip_set, skip_clear, epi_out, epi_mul};
 }
 
-int syn(sle_solver* s, const double2* c, double* g, const SynEpilogue* epi = nullptr) {
-  const double2* cc[1] = {c};
-  double* gg[1] = {g};
-  return sht_synthesis_packed(s->plan, 1, cc, gg, epi, s->st);
-}
-
-double fourpiR2(const sle_solver* s, double x) {
+double fourpiR2(const sle_batch* s, double x) {
   // x * 4 * PI * radius**2 with the reference's left-to-right association
   return ((x * 4.0) * PI_LEGACY) * std::pow(s->cfg.radius, 2);
 }
 
-// One inner iteration (solver.py:909-1045) as a fixed kernel sequence: every decision is read
-// on the device, so the same sequence serves the host-driven loop and the graph body.
-int enqueue_iteration(sle_solver* s, cudaGraphConditionalHandle loop) {
+// One inner iteration (solver.py:909-1045) for every slot as a fixed kernel sequence: every
+// decision is read on the device, so the same sequence serves the host-driven loop and the
+// graph body.
+int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   const Dev& D = s->D;
   cudaStream_t st = s->st;
   const long long nc = D.ncoef, ng = D.ng;
+  const unsigned B = (unsigned)s->nslot;
   note_launch();
-  k_b18<<<nb(nc), 256, 0, st>>>(D, s->dI, s->p_ocean, s->load, s->visc, s->sl, s->sc);
-  SynEpilogue epi{s->rO, s->cstar};
-  SLE_TRY(syn(s, s->sl, s->dsl, &epi));
-  SLE_TRY(ana(s, 1, s->rO, s->rOlm));
+  k_b18<<<dim3(nb(nc), B), 256, 0, st>>>(D);
+  SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sl.data(), (int)s->f_syn_sl.size(), st));
+  SLE_TRY(sht_analysis_list(s->plan, s->f_ana_ro.data(), (int)s->f_ana_ro.size(), st));
   note_launch();
-  k_update<<<nb(nc), 256, 0, st>>>(D, s->C, s->p_ocean, s->rOlm, s->cstarlm, s->tOlm, s->dI, s->load, s->dScur,
-                                   s->sc, s->partials, s->counter, loop);
+  k_update<<<dim3(nb(nc), B), 256, 0, st>>>(D);
   if (!s->cfg.opt_dsl) {
     note_launch();
-    k_sltot<<<nb(nc), 256, 0, st>>>(D, s->sl, s->sltot, s->sc);
-    SLE_TRY(syn(s, s->sltot, s->deltasl));
+    k_sltot<<<dim3(nb(nc), B), 256, 0, st>>>(D);
+    SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sltot.data(), (int)s->f_syn_sltot.size(), st));
   }
   note_launch(2);
-  k_refresh1<<<nb(ng / 2) + 1, 256, 0, st>>>(D, s->C, s->dScur, s->dI, s->dsl, s->deltasl, s->tinit, s->topo,
-                                             s->cxy, s->ice, s->beta,
-                                         s->grnew, s->sc, s->partials + s->part_grid, s->counter + 1);
-  k_refresh2<<<nb(ng / 2), 256, 0, st>>>(D, s->cxy, s->tinit, s->cstar0, s->grnew, s->icestar, s->beta, s->cstar,
-                                     s->tO, s->sc);
-  // I* (only when the grounded mask changed), C* and tO for the next iteration; skipped once
-  // the iteration has converged
-  AnaGate gate{&s->sc->converged, &s->sc->gr_changed, 0x7u, 0x1u};
-  const double* g3[3] = {s->icestar, s->cstar, s->tO};
-  double2* o3[3] = {s->icelm, s->cstarlm, s->tOlm};
-  SLE_TRY(sht_analysis_packed(s->plan, 3, g3, o3, st, &gate));
-  note_launch();
-  k_dice<<<nb(nc), 256, 0, st>>>(D, s->C, s->icelm, s->oldice, s->p_ice, s->dice, s->dI, s->dScur, s->sc,
-                                 s->counter + 2);
+  k_refresh1<<<dim3(nb(ng / 2) + 1, B), 256, 0, st>>>(D);
+  k_refresh2<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
+  // I* (only when the grounded mask changed), C* and tO for the next iteration; skipped for
+  // slots that converged
+  SLE_TRY(sht_analysis_list(s->plan, s->f_ana_refresh.data(), (int)s->f_ana_refresh.size(), st));
+  note_launch(2);
+  k_dice<<<dim3(nb(nc), B), 256, 0, st>>>(D);
+  k_loop_cond<<<1, 128, 0, st>>>(D, s->bstatus, loop);
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
 }
 
-int build_loop_graph(sle_solver* s) {
+int build_loop_graph(sle_batch* s) {
   cudaGraph_t g = nullptr;
   SLE_CUDA(cudaGraphCreate(&g, 0));
   cudaGraphConditionalHandle h;
@@ -973,151 +1091,68 @@ int build_loop_graph(sle_solver* s) {
   }
   s->loop_graph = g;
   s->loop_exec = ex;
-  s->loop_cond = h;
   return SLE_OK;
 }
 
-}  // namespace
+int check_slot(const sle_batch* s, int slot, const char* what) {
+  if (slot < 0 || slot >= s->nslot) {
+    set_error("%s: slot %d outside 0..%d", what, slot, s->nslot - 1);
+    return SLE_ERR_BAD_ARG;
+  }
+  return SLE_OK;
+}
 
-extern "C" int sle_solver_create(const sle_config* cfg, const sle_earth* earth, sle_solver** out) {
-  if (!cfg || !earth || !out) {
-    set_error("sle_solver_create: NULL argument");
+// Earth model of one slot: arrays, per-slot rotation constants, decay for dt.
+int set_earth(sle_batch* s, int b, const sle_earth* earth, double dt) {
+  const int nl = s->D.nl, K = s->K;
+  if (!earth) {
+    set_error("sle_batch_load: NULL earth");
     return SLE_ERR_BAD_ARG;
   }
-  *out = nullptr;
-  if (earth->nmodes < 0 || earth->nmodes > 4096) {
-    set_error("sle_solver_create: nmodes out of range");
+  if (earth->nmodes < 0 || earth->nmodes > K) {
+    set_error("sle_batch_load: %d modes, the batch holds at most %d", earth->nmodes, K);
     return SLE_ERR_BAD_ARG;
   }
-  sle_solver* s = new sle_solver();
-  std::memset(s, 0, sizeof(sle_solver));
-  s->cfg = *cfg;
-  int rc = sle_sht_create(cfg->nlat, cfg->nlon, cfg->lmax, &s->plan);
-  if (rc != SLE_OK) {
-    delete s;
-    return rc;
-  }
-#define TRY(x)                \
-  do {                        \
-    rc = (x);                 \
-    if (rc != SLE_OK) {       \
-      solver_free(s);         \
-      return rc;              \
-    }                         \
-  } while (0)
-#define TRYC(x)                                                                       \
-  do {                                                                                \
-    cudaError_t e_ = (x);                                                             \
-    if (e_ != cudaSuccess) {                                                          \
-      set_error("%s failed: %s", #x, cudaGetErrorString(e_));                          \
-      solver_free(s);                                                                 \
-      return SLE_ERR_CUDA;                                                            \
-    }                                                                                 \
-  } while (0)
-  TRYC(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
-  const int nl = cfg->lmax + 1;
-  const long long ng = (long long)cfg->nlat * cfg->nlon;
-  const long long nc = s->plan->d.ncoef;
-  const int K = earth->nmodes;
-  s->K = K;
-  // earth
-  TRY(dalloc(&s->s_kl, (size_t)K * nl));
-  TRY(dalloc(&s->decay, (size_t)K * nl));
-  TRY(dalloc(&s->omd, (size_t)K * nl));
-  TRY(dalloc(&s->a_sl, (size_t)K * nl));
-  TRY(dalloc(&s->a_rr, (size_t)K * nl));
-  TRY(dalloc(&s->ttl, nl));
-  TRY(dalloc(&s->ttlekhl, nl));
-  TRY(dalloc(&s->ttlhe, nl));
-  TRY(dalloc(&s->a_il, K));
-  TRY(dalloc(&s->a_m, K));
-  TRY(dalloc(&s->a_tsl, K));
-  TRY(dalloc(&s->a_trr, K));
-  TRY(dalloc(&s->nmod, nl));
-  TRY(dalloc(&s->r_il, (size_t)K * 9));
-  TRY(dalloc(&s->r_m, (size_t)K * 3));
-  TRY(dalloc(&s->r_lam, (size_t)K * 6));
-  TRYC(cudaMemcpy(s->s_kl, earth->s, sizeof(double) * K * nl, cudaMemcpyHostToDevice));
-  TRYC(cudaMemcpy(s->a_sl, earth->a_sl, sizeof(double) * K * nl, cudaMemcpyHostToDevice));
-  TRYC(cudaMemcpy(s->a_rr, earth->a_rr, sizeof(double) * K * nl, cudaMemcpyHostToDevice));
-  TRYC(cudaMemcpy(s->ttl, earth->ttl, sizeof(double) * nl, cudaMemcpyHostToDevice));
-  TRYC(cudaMemcpy(s->ttlekhl, earth->ttlekhl, sizeof(double) * nl, cudaMemcpyHostToDevice));
-  TRYC(cudaMemcpy(s->ttlhe, earth->ttlhe, sizeof(double) * nl, cudaMemcpyHostToDevice));
-  if (K > 0) {
-    TRYC(cudaMemcpy(s->a_il, earth->a_il, sizeof(double) * K, cudaMemcpyHostToDevice));
-    TRYC(cudaMemcpy(s->a_m, earth->a_m, sizeof(double) * K, cudaMemcpyHostToDevice));
-    TRYC(cudaMemcpy(s->a_tsl, earth->a_tsl, sizeof(double) * K, cudaMemcpyHostToDevice));
-    TRYC(cudaMemcpy(s->a_trr, earth->a_trr, sizeof(double) * K, cudaMemcpyHostToDevice));
-  }
+  const int Ke = earth->nmodes;
   std::vector<int> nm(earth->nmod, earth->nmod + nl);
   for (int l = 0; l < nl; ++l) {
-    if (nm[l] < 0 || nm[l] > K) {
-      set_error("sle_solver_create: nmod[%d]=%d outside 0..%d", l, nm[l], K);
-      solver_free(s);
+    if (nm[l] < 0 || nm[l] > Ke) {
+      set_error("sle_batch_load: nmod[%d]=%d outside 0..%d", l, nm[l], Ke);
       return SLE_ERR_BAD_ARG;
     }
   }
-  TRYC(cudaMemcpy(s->nmod, nm.data(), sizeof(int) * nl, cudaMemcpyHostToDevice));
-  s->nmod2 = nl > 2 ? nm[2] : 0;
-  if (s->nmod2 > 64) {
-    set_error("sle_solver_create: %d relaxation modes at degree 2 (at most 64 supported)", s->nmod2);
-    solver_free(s);
+  if (nl > 2 && nm[2] > 64) {
+    set_error("sle_batch_load: %d relaxation modes at degree 2 (at most 64 supported)", nm[2]);
     return SLE_ERR_UNSUPPORTED;
   }
-  // grids
-  double** grids[] = {&s->tinit, &s->cxy0, &s->beta0, &s->cstar0, &s->cxy, &s->topo_prev, &s->icestar, &s->beta,
-                      &s->cstar, &s->tO, &s->rO, &s->dsl, &s->deltasl, &s->topo, &s->rr, &s->grnew, &s->ice,
-                      &s->ice_prev, &s->tmpg, &s->gbuf3, &s->gbuf4};
-  for (double** g : grids) TRY(dalloc(g, ng));
-  TRY(dalloc(&s->rows, (size_t)4 * cfg->nlat));
-  double2** specs[] = {&s->p_load, &s->p_ice, &s->p_ocean, &s->prev_ice, &s->visc, &s->rad, &s->icelm,
-                       &s->oldice, &s->dice, &s->dI, &s->cstarlm, &s->tOlm, &s->rOlm, &s->load, &s->dScur,
-                       &s->sl, &s->sltot, &s->rrlm, &s->h1, &s->h2, &s->spare[0], &s->spare[1], &s->spare[2],
-                       &s->spare[3]};
-  for (double2** p : specs) TRY(dalloc(p, nc));
-  TRY(dalloc(&s->R, (size_t)K * nc + 1));
-  TRY(dalloc(&s->sc, 1));
-  s->part_grid = (long long)nb(nc) + 32;
-  TRY(dalloc(&s->partials, (size_t)s->part_grid + nb(ng / 2) + 64));
-  TRY(dalloc(&s->counter, 4));
-  TRY(dalloc(&s->badflag, 1));
-  TRYC(cudaMallocHost(reinterpret_cast<void**>(&s->hsc), sizeof(Scal)));
-  TRYC(cudaMemset(s->counter, 0, 4 * sizeof(unsigned int)));
-  // device view
-  Dev& D = s->D;
-  D.nlat = cfg->nlat;
-  D.nlon = cfg->nlon;
-  D.nl = nl;
-  D.ng = ng;
-  D.ncoef = nc;
-  D.K = K;
-  D.lidx = s->plan->d.lidx;
-  D.nmod = s->nmod;
-  D.decay = s->decay;
-  D.omd = s->omd;
-  D.a_sl = s->a_sl;
-  D.a_rr = s->a_rr;
-  D.ttl = s->ttl;
-  D.ttlekhl = s->ttlekhl;
-  D.ttlhe = s->ttlhe;
-  D.a_il = s->a_il;
-  D.a_m = s->a_m;
-  D.a_tsl = s->a_tsl;
-  D.a_trr = s->a_trr;
-  D.nmod2 = s->nmod2;
-  D.rhoi = cfg->rhoi;
-  D.rhow = cfg->rhow;
-  D.epsilon1 = cfg->epsilon1;
-  D.checkmarine = cfg->checkmarine;
-  D.tpw = cfg->tpw && nl > 2;
-  D.calcRG = cfg->calcRG;
-  D.opt_dsl = cfg->opt_dsl;
-  const int L = cfg->lmax;
-  D.i20 = 2;
-  D.i21 = (long long)(L + 1) + 1;
-  D.i22 = (long long)2 * (L + 1) - 1 + 0;
+  // [K][nl] arrays padded from the slot's Ke modes to the batch's K
+  std::vector<double> sk((size_t)K * nl, 0.0), asl((size_t)K * nl, 0.0), arr((size_t)K * nl, 0.0);
+  std::copy(earth->s, earth->s + (size_t)Ke * nl, sk.begin());
+  std::copy(earth->a_sl, earth->a_sl + (size_t)Ke * nl, asl.begin());
+  std::copy(earth->a_rr, earth->a_rr + (size_t)Ke * nl, arr.begin());
+  std::vector<double> ail(K, 0.0), am(K, 0.0), atsl(K, 0.0), atrr(K, 0.0);
+  if (Ke > 0) {
+    std::copy(earth->a_il, earth->a_il + Ke, ail.begin());
+    std::copy(earth->a_m, earth->a_m + Ke, am.begin());
+    std::copy(earth->a_tsl, earth->a_tsl + Ke, atsl.begin());
+    std::copy(earth->a_trr, earth->a_trr + Ke, atrr.begin());
+  }
+  const size_t o = s->D.kl(b);
+  cudaStream_t st = s->st;
+  SLE_CUDA(cudaMemcpyAsync(s->s_kl + o, sk.data(), sizeof(double) * K * nl, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->a_sl + o, asl.data(), sizeof(double) * K * nl, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->a_rr + o, arr.data(), sizeof(double) * K * nl, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->ttl + (size_t)b * nl, earth->ttl, sizeof(double) * nl, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->ttlekhl + (size_t)b * nl, earth->ttlekhl, sizeof(double) * nl, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->ttlhe + (size_t)b * nl, earth->ttlhe, sizeof(double) * nl, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->a_il + (size_t)b * K, ail.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->a_m + (size_t)b * K, am.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->a_tsl + (size_t)b * K, atsl.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->a_trr + (size_t)b * K, atrr.data(), sizeof(double) * K, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemcpyAsync(s->nmod + (size_t)b * nl, nm.data(), sizeof(int) * nl, cudaMemcpyHostToDevice, st));
   // rotation constants (solver.py:910-975), same expressions as the reference
-  RotConst& C = s->C;
+  const sle_config* cfg = &s->cfg;
+  RotConst C;
   const double a4 = std::pow(cfg->radius, 4);
   C.c_il22 = (-8 * PI_LEGACY * a4) / (3 * std::sqrt(5.0));
   C.c_il02 = (-8 * PI_LEGACY * a4) / std::sqrt(30.0);
@@ -1137,14 +1172,238 @@ extern "C" int sle_solver_create(const sle_config* cfg, const sle_earth* earth, 
   C.gacc = cfg->gacc;
   C.rhoi = cfg->rhoi;
   C.rhow = cfg->rhow;
-  s->dt_cur = -1.0;
+  SLE_CUDA(cudaMemcpyAsync(s->rc + b, &C, sizeof(RotConst), cudaMemcpyHostToDevice, st));
+  SlotHost& h = s->slot[b];
+  h.dt = dt;
+  h.dt_cur = -1.0;
+  SLE_TRY(set_dt(s, b, dt));
+  SLE_CUDA(cudaStreamSynchronize(st));
+  h.loaded = 1;
+  h.inited = 0;
+  return SLE_OK;
+}
+
+// Step 0 of one slot (solver.py:550-581): masks, areas and volume; zero modal and history state.
+int init_slot(sle_batch* s, int b, const double* topo0, const double* ice0, int on_device, double* ocean_area0,
+              double* oceanBeta_area0, double* ice_volume0) {
+  const Dev& D = s->D;
+  const size_t gb = sizeof(double) * D.ng;
+  cudaStream_t st = s->st;
+  SlotHost& h = s->slot[b];
+  if (!h.loaded) {
+    set_error("slot %d has no Earth model", b);
+    return SLE_ERR_STATE;
+  }
+  SLE_TRY(upload(D.g(G_TINIT, b), topo0, gb, on_device, st));
+  SLE_TRY(upload(D.g(G_ICE_PREV, b), ice0, gb, on_device, st));
+  SLE_TRY(check_finite(s, D.g(G_TINIT, b), D.ng, "topography"));
+  SLE_TRY(check_finite(s, D.g(G_ICE_PREV, b), D.ng, "initial ice"));
+  note_launch();
+  k_init_grid<<<nb(D.ng), 256, 0, st>>>(D, b);
+  SLE_CUDA(cudaGetLastError());
+  // step-0 areas and volume from full analyses (solver.py:571-581)
+  const FieldSpec f3[3] = {fspec(D.g(G_CXY0, b), D.sp(S_SP0, b)), fspec(D.g(G_CSTAR0, b), D.sp(S_SP1, b)),
+                           fspec(D.g(G_ICESTAR, b), D.sp(S_SP2, b))};
+  SLE_TRY(sht_analysis_list(s->plan, f3, 3, st));
+  double2 v[3];
+  SLE_CUDA(cudaMemcpyAsync(&v[0], D.sp(S_SP0, b), sizeof(double2), cudaMemcpyDeviceToHost, st));
+  SLE_CUDA(cudaMemcpyAsync(&v[1], D.sp(S_SP1, b), sizeof(double2), cudaMemcpyDeviceToHost, st));
+  SLE_CUDA(cudaMemcpyAsync(&v[2], D.sp(S_SP2, b), sizeof(double2), cudaMemcpyDeviceToHost, st));
+  // modal, rotational and history state start at zero
+  const long long nc = D.ncoef;
+  SLE_CUDA(cudaMemsetAsync(D.R + (size_t)b * s->K * nc, 0, sizeof(double2) * s->K * nc, st));
+  const int zero_specs[] = {S_P_LOAD, S_P_ICE, S_P_OCEAN, S_PREV_ICE, S_HA, S_HB};
+  for (int z : zero_specs) SLE_CUDA(cudaMemsetAsync(D.sp(z, b), 0, sizeof(double2) * nc, st));
+  const size_t K = s->K ? s->K : 1;
+  SLE_CUDA(cudaMemsetAsync(s->r_il + (size_t)b * s->K * 9, 0, sizeof(double) * 9 * K, st));
+  SLE_CUDA(cudaMemsetAsync(s->r_m + (size_t)b * s->K * 3, 0, sizeof(double) * 3 * K, st));
+  SLE_CUDA(cudaMemsetAsync(s->r_lam + (size_t)b * s->K * 6, 0, sizeof(double) * 6 * K, st));
+  note_launch();
+  k_slot_reset<<<1, 32, 0, st>>>(D, b, s->K00);
+  SLE_CUDA(cudaGetLastError());
+  SLE_CUDA(cudaStreamSynchronize(st));
+  h.ocean_area0 = fourpiR2(s, v[0].x);
+  h.oceanBeta_area0 = fourpiR2(s, v[1].x);
+  h.ice_volume0 = fourpiR2(s, v[2].x);
+  if (ocean_area0) *ocean_area0 = h.ocean_area0;
+  if (oceanBeta_area0) *oceanBeta_area0 = h.oceanBeta_area0;
+  if (ice_volume0) *ice_volume0 = h.ice_volume0;
+  h.iter = 0;
+  h.nhist = 0;
+  h.hsel = 0;
+  h.dt_hist[0] = h.dt_hist[1] = h.dt;
+  h.inited = 1;
+  std::memset(&h.last, 0, sizeof(h.last));
+  return SLE_OK;
+}
+
+int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
+  if (!cfg || !out) {
+    set_error("sle_batch_create: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  if (nslot < 1 || nslot > 4096) {
+    set_error("sle_batch_create: nslots must be 1..4096 (got %d)", nslot);
+    return SLE_ERR_BAD_ARG;
+  }
+  if (kmax < 0 || kmax > 4096) {
+    set_error("sle_batch_create: max_modes out of range");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (cfg->precision != SLE_PREC_FP64 && cfg->precision != SLE_PREC_MIXED) {
+    set_error("sle_batch_create: unknown precision %d", cfg->precision);
+    return SLE_ERR_BAD_ARG;
+  }
+  sle_batch* s = new sle_batch();
+  s->cfg = *cfg;
+  s->nslot = nslot;
+  s->K = kmax;
+  int rc = sle_sht_create(cfg->nlat, cfg->nlon, cfg->lmax, &s->plan);
+  if (rc != SLE_OK) {
+    delete s;
+    return rc;
+  }
+#define TRY(x)                \
+  do {                        \
+    rc = (x);                 \
+    if (rc != SLE_OK) {       \
+      batch_free(s);          \
+      return rc;              \
+    }                         \
+  } while (0)
+#define TRYC(x)                                                                       \
+  do {                                                                                \
+    cudaError_t e_ = (x);                                                             \
+    if (e_ != cudaSuccess) {                                                          \
+      set_error("%s failed: %s", #x, cudaGetErrorString(e_));                          \
+      batch_free(s);                                                                  \
+      return SLE_ERR_CUDA;                                                            \
+    }                                                                                 \
+  } while (0)
+  TRYC(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  const int nl = cfg->lmax + 1;
+  const long long ng = (long long)cfg->nlat * cfg->nlon;
+  const long long nc = s->plan->d.ncoef;
+  const int K = kmax;
+  const size_t B = (size_t)nslot;
+  TRY(dalloc(&s->grid, (size_t)NGRID * B * ng));
+  TRY(dalloc(&s->spec, (size_t)NSPEC * B * nc));
+  TRY(dalloc(&s->R, B * K * nc + 1));
+  TRY(dalloc(&s->nmod, B * nl));
+  double** kl_arrays[] = {&s->s_kl, &s->decay, &s->omd, &s->a_sl, &s->a_rr};
+  for (double** p : kl_arrays) TRY(dalloc(p, B * K * nl + 1));
+  double** l_arrays[] = {&s->ttl, &s->ttlekhl, &s->ttlhe};
+  for (double** p : l_arrays) TRY(dalloc(p, B * nl));
+  double** k_arrays[] = {&s->a_il, &s->a_m, &s->a_tsl, &s->a_trr};
+  for (double** p : k_arrays) TRY(dalloc(p, B * K + 1));
+  TRY(dalloc(&s->rc, B));
+  TRY(dalloc(&s->r_il, B * K * 9 + 1));
+  TRY(dalloc(&s->r_m, B * K * 3 + 1));
+  TRY(dalloc(&s->r_lam, B * K * 6 + 1));
+  TRY(dalloc(&s->sc, B));
+  TRY(dalloc(&s->ss, B));
+  const long long part_grid = (long long)nb(nc) + 32;
+  const long long npart = part_grid + nb(ng / 2) + 64;
+  TRY(dalloc(&s->partials, B * npart));
+  TRY(dalloc(&s->counter, B * 4));
+  TRY(dalloc(&s->rows, B * 4 * cfg->nlat));
+  TRY(dalloc(&s->badflag, 1));
+  TRY(dalloc(&s->bstatus, 1));
+  TRYC(cudaMallocHost(reinterpret_cast<void**>(&s->hsc), sizeof(Scal) * B));
+  TRYC(cudaMallocHost(reinterpret_cast<void**>(&s->hss), sizeof(SlotStep) * B));
+  TRYC(cudaMemset(s->counter, 0, sizeof(unsigned int) * 4 * B));
+  TRYC(cudaMemset(s->bstatus, 0, sizeof(int)));
+  TRYC(cudaMemset(s->sc, 0, sizeof(Scal) * B));
+  TRYC(cudaMemset(s->ss, 0, sizeof(SlotStep) * B));
+  TRYC(cudaMemset(s->nmod, 0, sizeof(int) * B * nl));
+  s->slot.assign(B, SlotHost{});
+  if (cfg->precision == SLE_PREC_MIXED) {
+    TRY(sle_sht_set_precision(s->plan, SLE_PREC_MIXED));
+    s->plan->mx_status = s->bstatus;   // a tensor-core timeout ends the step with SLE_ERR_TIMEOUT
+  }
+  // device view
+  Dev& D = s->D;
+  D.nlat = cfg->nlat;
+  D.nlon = cfg->nlon;
+  D.nl = nl;
+  D.nslot = nslot;
+  D.K = K;
+  D.ng = ng;
+  D.ncoef = nc;
+  D.lidx = s->plan->d.lidx;
+  D.grid = s->grid;
+  D.spec = s->spec;
+  D.R = s->R;
+  D.nmod = s->nmod;
+  D.s_kl = s->s_kl;
+  D.decay = s->decay;
+  D.omd = s->omd;
+  D.a_sl = s->a_sl;
+  D.a_rr = s->a_rr;
+  D.ttl = s->ttl;
+  D.ttlekhl = s->ttlekhl;
+  D.ttlhe = s->ttlhe;
+  D.a_il = s->a_il;
+  D.a_m = s->a_m;
+  D.a_tsl = s->a_tsl;
+  D.a_trr = s->a_trr;
+  D.rc = s->rc;
+  D.r_il = s->r_il;
+  D.r_m = s->r_m;
+  D.r_lam = s->r_lam;
+  D.sc = s->sc;
+  D.ss = s->ss;
+  D.partials = s->partials;
+  D.npart = npart;
+  D.part_grid = part_grid;
+  D.counter = s->counter;
+  D.rows = s->rows;
+  D.w = s->plan->d.w;
+  D.rhoi = cfg->rhoi;
+  D.rhow = cfg->rhow;
+  D.epsilon1 = cfg->epsilon1;
+  D.checkmarine = cfg->checkmarine;
+  D.tpw = cfg->tpw && nl > 2;
+  D.calcRG = cfg->calcRG;
+  D.opt_dsl = cfg->opt_dsl;
+  D.slot0 = 0;
+  const int L = cfg->lmax;
+  D.i20 = 2;
+  D.i21 = (long long)(L + 1) + 1;
+  D.i22 = (long long)2 * (L + 1) - 1 + 0;
+  // static field lists of the loop body: every slot, gated by its flags
+  for (int b = 0; b < nslot; ++b) {
+    Scal* sb = s->sc + b;
+    s->f_syn_sl.push_back(fspec(D.g(G_DSL, b), D.sp(S_SL, b), &sb->done, nullptr, D.g(G_RO, b), D.g(G_CSTAR, b)));
+    s->f_ana_ro.push_back(fspec(D.g(G_RO, b), D.sp(S_ROLM, b), &sb->done));
+    s->f_syn_sltot.push_back(fspec(D.g(G_DELTASL, b), D.sp(S_SLTOT, b), &sb->done));
+  }
+  for (int b = 0; b < nslot; ++b) {
+    Scal* sb = s->sc + b;
+    s->f_ana_refresh.push_back(fspec(D.g(G_ICESTAR, b), D.sp(S_ICELM, b), &sb->converged, &sb->gr_changed));
+    s->f_ana_refresh.push_back(fspec(D.g(G_CSTAR, b), D.sp(S_CSTARLM, b), &sb->converged));
+    s->f_ana_refresh.push_back(fspec(D.g(G_TO, b), D.sp(S_TOLM, b), &sb->converged));
+  }
   // SLEVOLVE_B200_HOST_LOOP=1 drives the inner loop from the host (same kernels; used to profile
   // the loop body, whose kernels profilers do not report inside conditional graph nodes)
   {
     const char* e = std::getenv("SLEVOLVE_B200_HOST_LOOP");
     s->use_graph = !(e && e[0] == '1');
   }
-  TRY(set_dt(s, cfg->dt_years));
+  // K00 = synth(e00)[0,0] (solver_opt.py:320-325): the same for every slot of the grid
+  s->K00 = 0.0;
+  if (cfg->opt_dsl) {
+    double2* e00 = D.sp(S_SP3, 0);
+    double* g0 = D.g(G_TMP, 0);
+    TRYC(cudaMemset(e00, 0, sizeof(double2) * nc));
+    const double2 one = make_double2(1.0, 0.0);
+    TRYC(cudaMemcpy(e00, &one, sizeof(double2), cudaMemcpyHostToDevice));
+    const FieldSpec f1 = fspec(g0, e00);
+    TRY(sht_synthesis_list(s->plan, &f1, 1, s->st));
+    TRYC(cudaStreamSynchronize(s->st));
+    TRYC(cudaMemcpy(&s->K00, g0, sizeof(double), cudaMemcpyDeviceToHost));
+  }
   TRYC(cudaStreamSynchronize(s->st));
   *out = s;
   return SLE_OK;
@@ -1152,272 +1411,211 @@ extern "C" int sle_solver_create(const sle_config* cfg, const sle_earth* earth, 
 #undef TRYC
 }
 
-extern "C" int sle_solver_destroy(sle_solver* s) {
-  if (s) cudaStreamSynchronize(s->st);
-  solver_free(s);
-  return SLE_OK;
-}
-
-extern "C" int sle_solver_stream(sle_solver* s, void** stream) {
-  if (!s || !stream) {
-    set_error("sle_solver_stream: NULL argument");
-    return SLE_ERR_BAD_ARG;
-  }
-  *stream = reinterpret_cast<void*>(s->st);
-  return SLE_OK;
-}
-
-extern "C" int sle_solver_init(sle_solver* s, const double* topo0, const double* ice0, int on_device,
-                               double* ocean_area0, double* oceanBeta_area0, double* ice_volume0) {
-  if (!s || !topo0 || !ice0) {
-    set_error("sle_solver_init: NULL argument");
-    return SLE_ERR_BAD_ARG;
-  }
-  const Dev& D = s->D;
-  const size_t gb = sizeof(double) * D.ng;
-  cudaStream_t st = s->st;
-  SLE_TRY(upload(s->tinit, topo0, gb, on_device, st));
-  SLE_TRY(upload(s->ice_prev, ice0, gb, on_device, st));
-  SLE_TRY(check_finite(s, s->tinit, D.ng, "topography"));
-  SLE_TRY(check_finite(s, s->ice_prev, D.ng, "initial ice"));
-  note_launch();
-  k_init_grid<<<nb(D.ng), 256, 0, st>>>(D, s->tinit, s->ice_prev, s->cxy0, s->beta0, s->cstar0, s->cxy,
-                                        s->topo_prev, s->icestar);
-  SLE_CUDA(cudaGetLastError());
-  // step-0 areas and volume from full analyses (solver.py:571-581)
-  SLE_TRY(ana(s, 3, s->cxy0, s->spare[0], s->cstar0, s->spare[1], s->icestar, s->spare[2]));
-  double2 v[3];
-  for (int q = 0; q < 3; ++q)
-    SLE_CUDA(cudaMemcpyAsync(&v[q], s->spare[q], sizeof(double2), cudaMemcpyDeviceToHost, st));
-  // modal and rotational state start at zero
-  const long long nc = D.ncoef;
-  SLE_CUDA(cudaMemsetAsync(s->R, 0, sizeof(double2) * ((size_t)s->K * nc + 1), st));
-  double2* zero_specs[] = {s->p_load, s->p_ice, s->p_ocean, s->prev_ice, s->h1, s->h2};
-  for (double2* z : zero_specs) SLE_CUDA(cudaMemsetAsync(z, 0, sizeof(double2) * nc, st));
-  SLE_CUDA(cudaMemsetAsync(s->r_il, 0, sizeof(double) * 9 * (s->K ? s->K : 1), st));
-  SLE_CUDA(cudaMemsetAsync(s->r_m, 0, sizeof(double) * 3 * (s->K ? s->K : 1), st));
-  SLE_CUDA(cudaMemsetAsync(s->r_lam, 0, sizeof(double) * 6 * (s->K ? s->K : 1), st));
-  SLE_CUDA(cudaMemsetAsync(s->sc, 0, sizeof(Scal), st));
-  // K00 = synth(e00)[0,0] (solver_opt.py:320-325)
-  s->K00 = 0.0;
-  if (s->cfg.opt_dsl) {
-    SLE_CUDA(cudaMemsetAsync(s->spare[3], 0, sizeof(double2) * nc, st));
-    const double2 one = make_double2(1.0, 0.0);
-    SLE_CUDA(cudaMemcpyAsync(s->spare[3], &one, sizeof(double2), cudaMemcpyHostToDevice, st));
-    SLE_TRY(syn(s, s->spare[3], s->tmpg));
-    SLE_CUDA(cudaMemcpyAsync(&s->K00, s->tmpg, sizeof(double), cudaMemcpyDeviceToHost, st));
-  }
-  SLE_CUDA(cudaStreamSynchronize(st));
-  SLE_CUDA(cudaMemcpy(&s->sc->K00, &s->K00, sizeof(double), cudaMemcpyHostToDevice));
-  s->ocean_area0 = fourpiR2(s, v[0].x);
-  s->oceanBeta_area0 = fourpiR2(s, v[1].x);
-  s->ice_volume0 = fourpiR2(s, v[2].x);
-  if (ocean_area0) *ocean_area0 = s->ocean_area0;
-  if (oceanBeta_area0) *oceanBeta_area0 = s->oceanBeta_area0;
-  if (ice_volume0) *ice_volume0 = s->ice_volume0;
-  s->iter = 0;
-  s->nhist = 0;
-  s->dt_hist[0] = s->dt_hist[1] = s->cfg.dt_years;
-  s->inited = 1;
-  std::memset(&s->last, 0, sizeof(s->last));
-  return SLE_OK;
-}
-
-extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, double dt_years,
-                               sle_step_info* info) {
-  if (!s || !ice) {
-    set_error("sle_solver_step: NULL argument");
-    return SLE_ERR_BAD_ARG;
-  }
-  if (!s->inited) {
-    set_error("sle_solver_step: call sle_solver_init first");
-    return SLE_ERR_STATE;
-  }
+// One time step of the slots with ice[b] != NULL.
+int batch_step(sle_batch* s, const double* const* ice, int on_device, const double* dt_years,
+               sle_step_info* info) {
   const Dev& D = s->D;
   cudaStream_t st = s->st;
   const long long nc = D.ncoef, ng = D.ng;
-  double dt = s->cfg.dt_years;
-  if (dt_years > 0.0) {
-    dt = dt_years;
-    s->cfg.dt_years = dt;
+  const int B = s->nslot;
+  std::vector<int> act;
+  for (int b = 0; b < B; ++b) {
+    if (!ice[b]) continue;
+    if (!s->slot[b].inited) {
+      set_error("sle_batch_step: slot %d is not initialised", b);
+      return SLE_ERR_STATE;
+    }
+    act.push_back(b);
   }
-  SLE_TRY(set_dt(s, dt));
-  s->iter += 1;
-  const int it = s->iter;
-  SLE_TRY(upload(s->ice, ice, sizeof(double) * ng, on_device, st));
-
+  if (act.empty()) return SLE_OK;
+  // per-slot step parameters
+  for (int b = 0; b < B; ++b) s->hss[b] = SlotStep{0, 0, 0, 0, 0.0, 0.0};
+  for (int b : act) {
+    SlotHost& h = s->slot[b];
+    double dt = h.dt;
+    if (dt_years && dt_years[b] > 0.0) {
+      dt = dt_years[b];
+      h.dt = dt;
+    }
+    SLE_TRY(set_dt(s, b, dt));
+    h.iter += 1;
+    SlotStep& p = s->hss[b];
+    p.active = 1;
+    p.first = h.iter == 1;
+    p.hsel = h.hsel;
+    if (s->cfg.inner_extrap && h.nhist >= 2) {
+      const double dt0 = dt, dt1 = h.dt_hist[0], dt2 = h.dt_hist[1];
+      if (dt0 == dt1 && dt1 == dt2) {
+        p.mode = 1;
+      } else {
+        p.mode = 2;
+        const double w = (dt0 + dt1) / (dt1 + dt2);
+        p.c1 = dt0 / dt1 * (1.0 + w);
+        p.c2 = dt0 / dt2 * w;
+      }
+    }
+    SLE_TRY(upload(D.g(G_ICE, b), ice[b], sizeof(double) * ng, on_device, st));
+  }
+  SLE_CUDA(cudaMemcpyAsync(s->ss, s->hss, sizeof(SlotStep) * B, cudaMemcpyHostToDevice, st));
+  SLE_CUDA(cudaMemsetAsync(s->bstatus, 0, sizeof(int), st));
+  const unsigned UB = (unsigned)B;
+  note_launch(3);
+  k_step_begin<<<nb(B, 128), 128, 0, st>>>(D);
   // ---- modal advance (solver.py:835)
-  note_launch();
-  ProfToken tadv = prof_begin(PROF_ADVANCE, 1, st);
-  k_advance<<<nb(nc) + 1, 256, 0, st>>>(D, s->R, s->p_load, s->visc, s->rad, s->sc, s->r_il, s->r_m, s->r_lam);
+  ProfToken tadv = prof_begin(PROF_ADVANCE, (double)act.size(), st);
+  k_advance<<<dim3(nb(nc) + 1, UB), 256, 0, st>>>(D);
   prof_end(tadv, st);
-  // ---- ice and ocean grids, their analyses
-  note_launch();
-  k_ice_grid<<<nb(ng / 2), 256, 0, st>>>(D, s->ice, s->topo_prev, s->cxy, s->tinit, s->cstar0, s->icestar, s->beta,
-                                     s->cstar, s->tO, s->ice_prev, it == 1 ? s->tmpg : nullptr, s->sc);
+  // ---- ice and ocean grids, their analyses (the stepping slots only)
+  k_ice_grid<<<dim3(nb(ng / 2), UB), 256, 0, st>>>(D);
   SLE_CUDA(cudaGetLastError());
-  if (it == 1) {
-    SLE_TRY(ana(s, 4, s->icestar, s->icelm, s->cstar, s->cstarlm, s->tO, s->tOlm, s->tmpg, s->oldice));
-  } else {
-    SLE_TRY(ana(s, 3, s->icestar, s->icelm, s->cstar, s->cstarlm, s->tO, s->tOlm));
-    SLE_CUDA(cudaMemcpyAsync(s->oldice, s->prev_ice, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, st));
+  {
+    std::vector<FieldSpec> f;
+    for (int b : act) {
+      f.push_back(fspec(D.g(G_ICESTAR, b), D.sp(S_ICELM, b)));
+      f.push_back(fspec(D.g(G_CSTAR, b), D.sp(S_CSTARLM, b)));
+      f.push_back(fspec(D.g(G_TO, b), D.sp(S_TOLM, b)));
+      if (s->hss[b].first) f.push_back(fspec(D.g(G_TMP, b), D.sp(S_OLDICE, b)));
+    }
+    SLE_TRY(sht_analysis_list(s->plan, f.data(), (int)f.size(), st));
   }
   // ---- first guess
-  int mode = 0;
-  double c1 = 0.0, c2 = 0.0;
-  if (s->cfg.inner_extrap && s->nhist >= 2) {
-    const double dt0 = dt, dt1 = s->dt_hist[0], dt2 = s->dt_hist[1];
-    if (dt0 == dt1 && dt1 == dt2) {
-      mode = 1;
-    } else {
-      mode = 2;
-      const double w = (dt0 + dt1) / (dt1 + dt2);
-      c1 = dt0 / dt1 * (1.0 + w);
-      c2 = dt0 / dt2 * w;
-    }
-  }
   note_launch();
-  k_pre_spec<<<nb(nc), 256, 0, st>>>(D, s->C, s->icelm, s->oldice, s->p_ice, s->cstarlm, s->p_ocean, s->h1, s->h2,
-                                         mode, c1, c2, s->dice, s->dI, s->load, s->dScur, s->sc, s->partials,
-                                         s->counter);
+  k_pre_spec<<<dim3(nb(nc), UB), 256, 0, st>>>(D);
   SLE_CUDA(cudaGetLastError());
 
-  // ---- inner fixed-point loop (solver.py:907-1051): a CUDA graph whose WHILE condition
-  // is set by k_update (converged, 9999-iteration cap or non-finite value all stop it); with
-  // per-kernel profiling on, the same sequence is driven from the host.
+  // ---- inner fixed-point loop (solver.py:907-1051): a CUDA graph whose WHILE condition is set
+  // at the end of each iteration (any slot unconverged); with per-kernel profiling on, the same
+  // sequence is driven from the host.
   const bool graph_step = s->use_graph && !prof_enabled();
   if (graph_step) {
     if (!s->loop_exec) SLE_TRY(build_loop_graph(s));
     SLE_CUDA(cudaGraphLaunch(s->loop_exec, st));
   } else {
     for (int host_iter = 0;; ++host_iter) {
-      if (host_iter > MAX_INNER + 2) {  // the device flag must have stopped the loop by now
+      if (host_iter > MAX_INNER + 2) {  // the device flags must have stopped the loop by now
         set_error("inner loop control lost (device iteration counter did not advance)");
         return SLE_ERR_STATE;
       }
       SLE_TRY(enqueue_iteration(s, 0));
       SLE_TRY(sync_scal(s));
-      const Scal& h = *s->hsc;
-      if (h.converged || h.status != 0) break;
+      bool any = false;
+      for (int b : act) any |= !s->hsc[b].done;
+      if (!any) break;
     }
   }
+  note_launch();
+  k_reopen<<<nb(B, 128), 128, 0, st>>>(D);
 
   // ---- radial displacement (solver.py:1054-1072)
   if (s->cfg.calcRG) {
     note_launch();
-    k_rr<<<nb(nc), 256, 0, st>>>(D, s->dI, s->p_ocean, s->load, s->rad, s->rrlm, s->sc);
-    SLE_TRY(syn(s, s->rrlm, s->rr));
+    k_rr<<<dim3(nb(nc), UB), 256, 0, st>>>(D);
+    std::vector<FieldSpec> f;
+    for (int b : act) f.push_back(fspec(D.g(G_RR, b), D.sp(S_RRLM, b), &s->sc[b].status));
+    SLE_TRY(sht_synthesis_list(s->plan, f.data(), (int)f.size(), st));
   }
   // ---- commit (solver.py:1080-1096); extrap history (solver_opt.py:817-822)
-  double2* hist_new = s->cfg.inner_extrap ? s->h2 : nullptr;
   note_launch();
-  k_commit<<<nb(nc), 256, 0, st>>>(D, s->dice, s->load, s->dI, s->dScur, s->icelm, s->p_load, s->p_ice, s->p_ocean,
-                                   s->prev_ice, hist_new, s->sc);
+  k_commit<<<dim3(nb(nc), UB), 256, 0, st>>>(D, s->cfg.inner_extrap);
   // ---- topography / ocean function and the degree-0 diagnostics
-  if (s->cfg.opt_diag) {
+  note_launch();
+  k_post_grid<<<dim3(D.nlat, UB), 256, 0, st>>>(D, s->cfg.opt_diag);
+  if (!s->cfg.opt_diag) {
+    std::vector<FieldSpec> f;
+    for (int b : act) {
+      const int* gs = &s->sc[b].status;
+      f.push_back(fspec(D.g(G_TMP, b), D.sp(S_SP0, b), gs));
+      f.push_back(fspec(D.g(G_CXY, b), D.sp(S_SP1, b), gs));
+      f.push_back(fspec(D.g(G_TMP3, b), D.sp(S_SP2, b), gs));
+      f.push_back(fspec(D.g(G_TMP4, b), D.sp(S_SP3, b), gs));
+    }
+    SLE_TRY(sht_analysis_list(s->plan, f.data(), (int)f.size(), st));
     note_launch();
-    k_post_grid<<<D.nlat, 256, 0, st>>>(D, s->tinit, s->deltasl, s->beta, s->topo, s->topo_prev, s->cxy, nullptr,
-                                        nullptr, nullptr, s->rows, s->plan->d.w, s->sc, s->counter + 3);
-  } else {
-    note_launch();
-    k_post_grid<<<D.nlat, 256, 0, st>>>(D, s->tinit, s->deltasl, s->beta, s->topo, s->topo_prev, s->cxy, s->tmpg,
-                                        s->gbuf3, s->gbuf4, nullptr, s->plan->d.w, s->sc, s->counter + 3);
-    SLE_TRY(ana(s, 4, s->tmpg, s->spare[0], s->cxy, s->spare[1], s->gbuf3, s->spare[2], s->gbuf4, s->spare[3]));
+    k_diag00<<<UB, 32, 0, st>>>(D);
   }
   SLE_CUDA(cudaGetLastError());
-  double2 d4[4];
-  if (!s->cfg.opt_diag)
-    for (int q = 0; q < 4; ++q)
-      SLE_CUDA(cudaMemcpyAsync(&d4[q], s->spare[q], sizeof(double2), cudaMemcpyDeviceToHost, st));
-  double2 ice00;
-  SLE_CUDA(cudaMemcpyAsync(&ice00, s->icelm, sizeof(double2), cudaMemcpyDeviceToHost, st));
   SLE_TRY(sync_scal(s));
-  const Scal& f = *s->hsc;
-  if (graph_step) note_launch((int)(f.numiter * s->body_launches));
-  if (f.status != SLE_OK) {
-    if (f.status == SLE_ERR_NONCONVERGED)
-      set_error("inner loop failed to converge, xi=%.17g", f.xi);
-    else
-      set_error("non-finite value in the inner loop (xi=%g)", f.xi);
-    s->last.status = f.status;
-    return f.status;
+  int first_bad = SLE_OK;
+  int maxiter = 0;
+  for (int b : act) maxiter = std::max(maxiter, s->hsc[b].numiter);
+  if (graph_step) note_launch((int)(maxiter * s->body_launches));
+  for (int b : act) {
+    SlotHost& h = s->slot[b];
+    const Scal& f = s->hsc[b];
+    sle_step_info& o = h.last;
+    std::memset(&o, 0, sizeof(o));
+    o.iter = h.iter;
+    o.numiter = f.numiter;
+    o.status = f.status;
+    o.xi = f.xi;
+    o.gr_reguess = f.gr_reguess;
+    o.gr_ice_analyses = f.gr_ice_an;
+    if (f.status != SLE_OK) {
+      if (first_bad == SLE_OK) {
+        first_bad = f.status;
+        if (f.status == SLE_ERR_NONCONVERGED)
+          set_error("inner loop failed to converge, xi=%.17g", f.xi);
+        else if (f.status == SLE_ERR_TIMEOUT)
+          set_error("a tensor-core transform kernel timed out waiting on its pipeline");
+        else
+          set_error("non-finite value in the inner loop (xi=%g)", f.xi);
+      }
+      if (info) info[b] = o;
+      continue;
+    }
+    if (s->cfg.inner_extrap) {
+      h.hsel ^= 1;
+      h.dt_hist[1] = h.dt_hist[0];
+      h.dt_hist[0] = h.dt;
+      h.nhist = std::min(2, h.nhist + 1);
+    }
+    const double slc_ocn00 = f.diag[0], c00 = f.diag[1], slc_b00 = f.diag[2], cst00 = f.diag[3];
+    if (s->cfg.opt_diag) {
+      // float arithmetic of solver_opt.py:909-914
+      const double a4 = 4 * PI_LEGACY * std::pow(s->cfg.radius, 2);
+      o.ocean_area = c00 * a4;
+      o.oceanBeta_area = cst00 * a4;
+      o.gmslc_ocn = slc_ocn00 / c00;
+      o.gmslc_ocnBeta = slc_b00 / cst00;
+    } else {
+      // complex [0,0] ratios of solver.py:1105-1113 (imaginary parts are exactly zero)
+      o.ocean_area = fourpiR2(s, c00);
+      o.oceanBeta_area = fourpiR2(s, cst00);
+      o.gmslc_ocn = slc_ocn00 * (1.0 / c00);
+      o.gmslc_ocnBeta = slc_b00 * (1.0 / cst00);
+    }
+    o.ice_volume = fourpiR2(s, f.diag[4]);
+    std::memcpy(o.il, f.il, sizeof(o.il));
+    std::memcpy(o.mm, f.mm, sizeof(o.mm));
+    std::memcpy(o.lam, f.lam, sizeof(o.lam));
+    if (info) info[b] = o;
   }
-  if (s->cfg.inner_extrap) {
-    double2* t = s->h1;
-    s->h1 = s->h2;
-    s->h2 = t;
-    s->dt_hist[1] = s->dt_hist[0];
-    s->dt_hist[0] = dt;
-    s->nhist = std::min(2, s->nhist + 1);
-  }
-  double slc_ocn00, c00, slc_b00, cst00;
-  if (s->cfg.opt_diag) {
-    slc_ocn00 = f.diag[0];
-    c00 = f.diag[1];
-    slc_b00 = f.diag[2];
-    cst00 = f.diag[3];
-  } else {
-    slc_ocn00 = d4[0].x;
-    c00 = d4[1].x;
-    slc_b00 = d4[2].x;
-    cst00 = d4[3].x;
-  }
-  sle_step_info& o = s->last;
-  o.iter = it;
-  o.numiter = f.numiter;
-  o.status = SLE_OK;
-  o.gr_reguess = f.gr_reguess;
-  o.gr_ice_analyses = f.gr_ice_an;
-  o.xi = f.xi;
-  if (s->cfg.opt_diag) {
-    // float arithmetic of solver_opt.py:909-914
-    const double a4 = 4 * PI_LEGACY * std::pow(s->cfg.radius, 2);
-    o.ocean_area = c00 * a4;
-    o.oceanBeta_area = cst00 * a4;
-    o.gmslc_ocn = slc_ocn00 / c00;
-    o.gmslc_ocnBeta = slc_b00 / cst00;
-  } else {
-    // complex [0,0] ratios of solver.py:1105-1113 (imaginary parts are exactly zero)
-    o.ocean_area = fourpiR2(s, c00);
-    o.oceanBeta_area = fourpiR2(s, cst00);
-    o.gmslc_ocn = slc_ocn00 * (1.0 / c00);
-    o.gmslc_ocnBeta = slc_b00 * (1.0 / cst00);
-  }
-  o.ice_volume = fourpiR2(s, ice00.x);
-  std::memcpy(o.il, f.il, sizeof(o.il));
-  std::memcpy(o.mm, f.mm, sizeof(o.mm));
-  std::memcpy(o.lam, f.lam, sizeof(o.lam));
-  if (info) *info = o;
-  return SLE_OK;
+  return first_bad;
 }
 
-extern "C" int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device) {
-  if (!s || !dst) {
-    set_error("sle_solver_get: NULL argument");
-    return SLE_ERR_BAD_ARG;
-  }
+int batch_get(sle_batch* s, int b, int field, void* dst, int dst_on_device) {
   const Dev& D = s->D;
   const size_t gb = sizeof(double) * D.ng;
   const cudaMemcpyKind kind = dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   const double* src = nullptr;
   switch (field) {
-    case SLE_F_TGRID: src = s->topo; break;
-    case SLE_F_OCEAN: src = s->cxy; break;
-    case SLE_F_BETA: src = s->beta; break;
-    case SLE_F_R: src = s->rr; break;
-    case SLE_F_DELTASL: src = s->deltasl; break;
-    case SLE_F_ICESTAR: src = s->icestar; break;
-    case SLE_F_OCEAN0: src = s->cxy0; break;
-    case SLE_F_BETA0: src = s->beta0; break;
+    case SLE_F_TGRID: src = D.g(G_TOPO, b); break;
+    case SLE_F_OCEAN: src = D.g(G_CXY, b); break;
+    case SLE_F_BETA: src = D.g(G_BETA, b); break;
+    case SLE_F_R: src = D.g(G_RR, b); break;
+    case SLE_F_DELTASL: src = D.g(G_DELTASL, b); break;
+    case SLE_F_ICESTAR: src = D.g(G_ICESTAR, b); break;
+    case SLE_F_OCEAN0: src = D.g(G_CXY0, b); break;
+    case SLE_F_BETA0: src = D.g(G_BETA0, b); break;
     case SLE_F_G:
       note_launch();
-      k_grid_add<<<nb(D.ng), 256, 0, s->st>>>(D.ng, s->deltasl, s->rr, s->tmpg);
+      k_grid_add<<<nb(D.ng), 256, 0, s->st>>>(D.ng, D.g(G_DELTASL, b), D.g(G_RR, b), D.g(G_TMP, b));
       SLE_CUDA(cudaGetLastError());
-      src = s->tmpg;
+      src = D.g(G_TMP, b);
       break;
     case SLE_F_DS_CONVERGED:
     case SLE_F_LOAD_INC: {
-      const double2* p = (field == SLE_F_DS_CONVERGED) ? s->p_ocean : s->load;
+      const double2* p = (field == SLE_F_DS_CONVERGED) ? D.sp(S_P_OCEAN, b) : D.sp(S_LOAD, b);
       double2* dense = s->plan->packbuf;  // staging (nm*nm <= 4*ncoef)
       SLE_TRY(sht_unpack(s->plan, p, dense, s->st));
       const size_t bytes = sizeof(double2) * (size_t)D.nl * D.nl;
@@ -1432,4 +1630,161 @@ extern "C" int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_de
   SLE_CUDA(cudaMemcpyAsync(dst, src, gb, kind, s->st));
   SLE_CUDA(cudaStreamSynchronize(s->st));
   return SLE_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ batch C ABI
+extern "C" int sle_batch_create(const sle_config* cfg, int nslots, int max_modes, sle_batch** out) {
+  return batch_create(cfg, nslots, max_modes, out);
+}
+
+extern "C" int sle_batch_destroy(sle_batch* b) {
+  if (b) cudaStreamSynchronize(b->st);
+  batch_free(b);
+  return SLE_OK;
+}
+
+extern "C" int sle_batch_load(sle_batch* b, int slot, const sle_earth* earth, double dt_years, const double* topo0,
+                              const double* ice0, int on_device, double* ocean_area0, double* oceanBeta_area0,
+                              double* ice_volume0) {
+  if (!b || !topo0 || !ice0) {
+    set_error("sle_batch_load: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  SLE_TRY(check_slot(b, slot, "sle_batch_load"));
+  if (!(dt_years > 0.0)) {
+    set_error("sle_batch_load: dt_years must be > 0");
+    return SLE_ERR_BAD_ARG;
+  }
+  SLE_TRY(set_earth(b, slot, earth, dt_years));
+  return init_slot(b, slot, topo0, ice0, on_device, ocean_area0, oceanBeta_area0, ice_volume0);
+}
+
+extern "C" int sle_batch_release(sle_batch* b, int slot) {
+  if (!b) {
+    set_error("sle_batch_release: NULL batch");
+    return SLE_ERR_BAD_ARG;
+  }
+  SLE_TRY(check_slot(b, slot, "sle_batch_release"));
+  b->slot[slot].loaded = 0;
+  b->slot[slot].inited = 0;
+  return SLE_OK;
+}
+
+extern "C" int sle_batch_step(sle_batch* b, const double* const* ice, int on_device, const double* dt_years,
+                              sle_step_info* info) {
+  if (!b || !ice) {
+    set_error("sle_batch_step: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  return batch_step(b, ice, on_device, dt_years, info);
+}
+
+extern "C" int sle_batch_get(sle_batch* b, int slot, int field, void* dst, int dst_on_device) {
+  if (!b || !dst) {
+    set_error("sle_batch_get: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  SLE_TRY(check_slot(b, slot, "sle_batch_get"));
+  return batch_get(b, slot, field, dst, dst_on_device);
+}
+
+extern "C" int sle_batch_stream(sle_batch* b, void** stream) {
+  if (!b || !stream) {
+    set_error("sle_batch_stream: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  *stream = reinterpret_cast<void*>(b->st);
+  return SLE_OK;
+}
+
+extern "C" int sle_batch_info(const sle_batch* b, int* nslots, int* max_modes, long long* device_bytes) {
+  if (!b) {
+    set_error("sle_batch_info: NULL batch");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (nslots) *nslots = b->nslot;
+  if (max_modes) *max_modes = b->K;
+  if (device_bytes) {
+    const long long B = b->nslot, ng = b->D.ng, nc = b->D.ncoef, K = b->K, nl = b->D.nl;
+    *device_bytes = B * (NGRID * ng * 8 + NSPEC * nc * 16 + K * nc * 16 + 5 * K * nl * 8 + 3 * nl * 8 +
+                         (long long)sizeof(Scal) + b->D.npart * 8 + 4LL * b->cfg.nlat * 8);
+  }
+  return SLE_OK;
+}
+
+// ----------------------------------------------------- single-solve C ABI (one slot)
+extern "C" int sle_solver_create(const sle_config* cfg, const sle_earth* earth, sle_solver** out) {
+  if (!cfg || !earth || !out) {
+    set_error("sle_solver_create: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  if (earth->nmodes < 0 || earth->nmodes > 4096) {
+    set_error("sle_solver_create: nmodes out of range");
+    return SLE_ERR_BAD_ARG;
+  }
+  sle_batch* b = nullptr;
+  SLE_TRY(batch_create(cfg, 1, earth->nmodes, &b));
+  const int rc = set_earth(b, 0, earth, cfg->dt_years);
+  if (rc != SLE_OK) {
+    batch_free(b);
+    return rc;
+  }
+  sle_solver* s = new sle_solver();
+  s->b = b;
+  *out = s;
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_destroy(sle_solver* s) {
+  if (!s) return SLE_OK;
+  sle_batch_destroy(s->b);
+  delete s;
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_stream(sle_solver* s, void** stream) {
+  if (!s || !stream) {
+    set_error("sle_solver_stream: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  *stream = reinterpret_cast<void*>(s->b->st);
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_init(sle_solver* s, const double* topo0, const double* ice0, int on_device,
+                               double* ocean_area0, double* oceanBeta_area0, double* ice_volume0) {
+  if (!s || !topo0 || !ice0) {
+    set_error("sle_solver_init: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  return init_slot(s->b, 0, topo0, ice0, on_device, ocean_area0, oceanBeta_area0, ice_volume0);
+}
+
+extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, double dt_years,
+                               sle_step_info* info) {
+  if (!s || !ice) {
+    set_error("sle_solver_step: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (!s->b->slot[0].inited) {
+    set_error("sle_solver_step: call sle_solver_init first");
+    return SLE_ERR_STATE;
+  }
+  const double* ices[1] = {ice};
+  const double dts[1] = {dt_years};
+  sle_step_info o;
+  const int rc = batch_step(s->b, ices, on_device, dts, &o);
+  if (info) *info = o;
+  return rc;
+}
+
+extern "C" int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device) {
+  if (!s || !dst) {
+    set_error("sle_solver_get: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  return batch_get(s->b, 0, field, dst, dst_on_device);
 }

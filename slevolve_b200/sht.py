@@ -5,6 +5,10 @@ transform interface (SLEvolve ``python/slevolve/sht.py:43-46``, ``sht_ducc.py:20
     ``analysis(grid[nlat, nlon] float64, out=None) -> coeffs[lmax+1, lmax+1] complex128``
     ``synthesis(coeffs, out=None) -> grid``
 
+``precision="mixed"`` runs the Legendre contractions as split-TF32 tensor-core GEMMs with FP32
+accumulation (FP64 recurrence, row FFTs and degree-0 coefficient); the default ``"fp64"`` matches
+the reference to round-off.
+
 Inputs may be NumPy arrays (copied to the device and back) or CUDA ``torch`` tensors (used in
 place, results stay on the device).  With ``out=None`` the NumPy path returns an internal buffer
 that the next call overwrites, exactly like the reference (sht.py:297-302, 339-343).
@@ -41,7 +45,7 @@ class CudaSHT:
     backend = "cuda"
 
     def __init__(self, nlat: int, nlon: int, lmax: int, workers: int = 1, chunk: int = 16,
-                 raw: bool = False):
+                 raw: bool = False, precision: str = "fp64"):
         if raw:
             raise ValueError("raw (sign-free) mode is only implemented for the ducc backend")
         if nlat % 2 != 0:
@@ -54,6 +58,8 @@ class CudaSHT:
         _lib.check(L.sle_sht_create(int(nlat), int(nlon), int(lmax), C.byref(h)), "sle_sht_create")
         self._h = h
         self._L = L
+        self.precision = "mixed" if _lib.precision_code(precision) == _lib.PREC_MIXED else "fp64"
+        _lib.check(L.sle_sht_set_precision(h, _lib.precision_code(precision)), "sle_sht_set_precision")
         self.nlat, self.nlon, self.lmax = int(nlat), int(nlon), int(lmax)
         self.nm = self.lmax + 1
         self.nh = self.nlat // 2
@@ -163,10 +169,10 @@ class CudaSHT:
 
 
 def make_sht(backend: str, nlat: int, nlon: int, lmax: int, workers: int = 1, chunk: int = 16,
-             raw: bool = False):
+             raw: bool = False, precision: str = "fp64"):
     """Transform factory with the reference's signature (sht_ducc.py:206-217); this package
     provides the ``"cuda"`` backend only and raises ValueError for any other name."""
     if backend == "cuda":
-        return CudaSHT(nlat, nlon, lmax, workers=workers, chunk=chunk, raw=raw)
+        return CudaSHT(nlat, nlon, lmax, workers=workers, chunk=chunk, raw=raw, precision=precision)
     raise ValueError(f"unknown SHT backend {backend!r} (slevolve_b200 provides 'cuda'; the 'numpy' "
                      "and 'ducc' backends belong to the reference package)")

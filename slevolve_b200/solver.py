@@ -57,6 +57,36 @@ def degree_weights(love, norder, planet):
     return ttl, ttl * ekhl, ttl * he
 
 
+def earth_struct(love, norder, planet):
+    """The C ABI's Earth record for `love` truncated at `norder` (solver.py:252-368, 596-603).
+
+    Returns (SleEarth, keep): `keep` owns the arrays the record points to and must outlive every
+    call that reads the record."""
+    ma = mode_arrays(love, norder)
+    ttl, ttlekhl, ttlhe = degree_weights(love, norder, planet)
+    keep = {
+        "nmod": np.ascontiguousarray(ma["nmod"], dtype=np.int32),
+        "s": np.ascontiguousarray(ma["s"]), "a_sl": np.ascontiguousarray(ma["a_sl"]),
+        "a_rr": np.ascontiguousarray(ma["a_rr"]), "ttl": ttl, "ttlekhl": ttlekhl,
+        "ttlhe": ttlhe, "a_il": np.ascontiguousarray(ma["a_il"]), "a_m": np.ascontiguousarray(ma["a_m"]),
+        "a_tsl": np.ascontiguousarray(ma["a_tsl"]), "a_trr": np.ascontiguousarray(ma["a_trr"])}
+
+    def dp(a):
+        return a.ctypes.data_as(C.POINTER(C.c_double))
+
+    nl = norder + 1
+    kTE2 = float(love.kTE[2]) if nl > 2 else 0.0
+    hTE2 = float(love.hTE[2]) if nl > 2 else 0.0
+    kE2 = float(love.ke[2]) if nl > 2 else 0.0
+    earth = _lib.SleEarth(nmodes=int(ma["K"]),
+                          nmod=keep["nmod"].ctypes.data_as(C.POINTER(C.c_int)),
+                          s=dp(keep["s"]), a_sl=dp(keep["a_sl"]), a_rr=dp(keep["a_rr"]),
+                          ttl=dp(ttl), ttlekhl=dp(ttlekhl), ttlhe=dp(ttlhe),
+                          a_il=dp(keep["a_il"]), a_m=dp(keep["a_m"]), a_tsl=dp(keep["a_tsl"]),
+                          a_trr=dp(keep["a_trr"]), kTE2=kTE2, hTE2=hTE2, kE2=kE2)
+    return earth, keep
+
+
 class _StepResult(dict):
     """Step outputs; grid and spectrum entries are fetched from the device on first access."""
 
@@ -100,8 +130,9 @@ class SeaLevelSolver:
                  calcRG=True, epsilon1=1.0e-5, planet=None, mem_threads=1, ramp=False,
                  axial_rotation="off", axial_tau_c=None, opt=None, inner=None, reuse="off",
                  reuse_store=None, anderson_depth=3, max_mask_refresh=3, anderson_freeze=2,
-                 anderson_keep=False):
+                 anderson_keep=False, precision="fp64"):
         opt = set(self._opt_default if opt is None else opt)
+        prec = _lib.precision_code(precision)
         inner = self._inner_default if inner is None else inner
         if ramp:
             raise NotImplementedError("ramp placement is not provided by the GPU solver")
@@ -159,28 +190,9 @@ class SeaLevelSolver:
                              opt_dsl=int("dsl" in opt), opt_diag=int("diag" in opt),
                              inner_extrap=int(inner == "extrap"), radius=p.radius, mass=p.mass,
                              rhoi=p.rhoi, rhow=p.rhow, gacc=p.gacc, omega=p.omega, moiA=p.moiA,
-                             moiC=p.moiC, kf=p.kf)
-        ma = mode_arrays(love, norder)
-        ttl, ttlekhl, ttlhe = degree_weights(love, norder, p)
-        self._earth_arrays = keep = {
-            "nmod": np.ascontiguousarray(ma["nmod"], dtype=np.int32),
-            "s": np.ascontiguousarray(ma["s"]), "a_sl": np.ascontiguousarray(ma["a_sl"]),
-            "a_rr": np.ascontiguousarray(ma["a_rr"]), "ttl": ttl, "ttlekhl": ttlekhl,
-            "ttlhe": ttlhe, "a_il": ma["a_il"], "a_m": ma["a_m"], "a_tsl": ma["a_tsl"],
-            "a_trr": ma["a_trr"]}
-
-        def dp(a):
-            return a.ctypes.data_as(C.POINTER(C.c_double))
-
-        kTE2 = float(love.kTE[2]) if self.nl > 2 else 0.0
-        hTE2 = float(love.hTE[2]) if self.nl > 2 else 0.0
-        kE2 = float(love.ke[2]) if self.nl > 2 else 0.0
-        earth = _lib.SleEarth(nmodes=int(ma["K"]),
-                              nmod=keep["nmod"].ctypes.data_as(C.POINTER(C.c_int)),
-                              s=dp(keep["s"]), a_sl=dp(keep["a_sl"]), a_rr=dp(keep["a_rr"]),
-                              ttl=dp(ttl), ttlekhl=dp(ttlekhl), ttlhe=dp(ttlhe),
-                              a_il=dp(keep["a_il"]), a_m=dp(keep["a_m"]), a_tsl=dp(keep["a_tsl"]),
-                              a_trr=dp(keep["a_trr"]), kTE2=kTE2, hTE2=hTE2, kE2=kE2)
+                             moiC=p.moiC, kf=p.kf, precision=prec)
+        self.precision = "mixed" if prec == _lib.PREC_MIXED else "fp64"
+        earth, self._earth_arrays = earth_struct(love, norder, p)
         h = C.c_void_p()
         _lib.check(L.sle_solver_create(C.byref(cfg), C.byref(earth), C.byref(h)), "sle_solver_create")
         self._h = h
