@@ -67,12 +67,16 @@ struct ShtDev {
   const int* gset[MAXF];
   const int* gclr[MAXF];
   // mixed-precision transforms (set once the plan prepared them)
-  float* mx_xf;               // [nm][2][ngrp][MX_NMAX][32] folded FP32 rFFT, analysis B layout
-  float2* mx_gns;             // [MX_MAXF][2][nm][nh] north / south Legendre sums (synthesis)
+  float* mx_xf;               // [MX_MAXF][nh][nm][4] folded FP32 rFFT (S.re, S.im, D.re, D.im)
+  float2* mx_gns;             // [MX_MAXF][nh][nm][2] north / south Legendre sums (synthesis)
+  float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (tile order)
   double* mx_s0;              // [MX_MAXF][nh] FP64 fold of the row sums (degree 0)
   int* mx_abort;              // raised by a tensor-core kernel whose wait timed out
-  const int2* mx_ana_units;   // (m, span) analysis work units, most work first
-  const int2* mx_syn_units;   // (m, latitude tile) synthesis work units, most work first
+  const int4* mx_ana_units;   // (m, span, first chunk, table slot) analysis units, most work first
+  const int4* mx_syn_units;   // (m, latitude tile, chunks, table slot) synthesis units
+  const int* mx_syn_seg;      // segment of each synthesis table slot
+  const uint32_t* mx_tab_ana; // Legendre tables: [slot][par][hi/lo][128][32] TF32, tile order
+  const uint32_t* mx_tab_syn;
 };
 
 __device__ __forceinline__ bool field_gated_off(const ShtDev& P, int f) {
@@ -125,9 +129,14 @@ struct sle_sht {
   int mx_ready;
   float* mx_xf;
   float2* mx_gns;
+  float* mx_bsyn;
   double* mx_s0;
   int* mx_abort;
-  int2 *mx_ana_units, *mx_syn_units;
+  int4 *mx_ana_units, *mx_syn_units;
+  int* mx_syn_seg;
+  uint32_t *mx_tab_ana, *mx_tab_syn;
+  alignas(64) unsigned char mx_tmap[3][128];   // TMA maps of mx_xf (boxes of 8, 16, 32 fields)
+  double mx_table_bytes;
   int n_ana_units, n_syn_units;
 };
 

@@ -10,24 +10,30 @@
 //   synthesis  D[j][n] = sum_l  P[l][j]  B[n][l],   B = coefficients of one parity
 // with each operand split into TF32 hi + lo and D += Ahi Bhi + Ahi Blo + Alo Bhi in FP32.
 //
-// Row FFTs, folds and the degree-0 coefficient are FP64; the fold output is rounded to FP32
-// before the split and the synthesis accumulators are read back as FP32.
-// What stays FP64: the Legendre recurrence (regenerated on the fly in every CTA from the FP64
-// seeds of the plan, Q_l = mu Q_{l-1} + be_l Q_{l-2}, P~ = cf Q, then split), the Gauss nodes and
-// weights, and the degree-0 coefficient: analysis computes U_00 from FP64 row sums of the input
-// grid; synthesis leaves l = 0 out of the tensor-core sum and adds its uniform contribution to
-// the output grid in FP64.
+// Precision: the Legendre values come from the FP64 recurrence of the plan
+// (Q_l = mu Q_{l-1} + be_l Q_{l-2}, P~ = cf Q) and are split once, when the plan is prepared,
+// into TF32 hi + lo tables stored in the tensor cores' shared-memory tile order; the B operands
+// are rounded to FP32 and split in shared memory.  Row FFTs, folds and the degree-0 coefficient
+// are FP64: analysis computes U_00 from FP64 row sums of the input grid; synthesis leaves l = 0
+// out of the tensor-core sum and adds its uniform contribution to the output grid in FP64.  The
+// tensor core's FP32 accumulation truncates, so the large products are spread over fresh TMEM
+// accumulators that the epilogue adds in FP64.
 //
-// Kernel structure (one CTA per work unit, 11 warps):
-//   warps 0-7   produce the A operand (Legendre values) of K-chunk stages 0 and 1 (4 warps each),
-//               warps 0-3 then read the accumulators out of TMEM (epilogue)
+// Kernel structure (one CTA per work unit, 10 warps, two pipeline stages):
+//   warp 9      loader: per K-chunk, one bulk copy of the A tiles (64 KB) and the B data
+//               (analysis: one 3-D TMA tensor load of the folded FFT; synthesis: bulk copies)
+//   warps 0-7   stage 0 / 1 splitters: B -> TF32 hi / lo tiles; warps 0-3 then read the
+//               accumulators out of TMEM (epilogue)
 //   warp 8      allocates TMEM and issues the MMAs from one thread
-//   warps 9-10  stage and split the B operand of stages 0 and 1
 // Stages hand over through mbarriers; tcgen05.commit releases a stage when its MMAs are done.
 // Every wait is bounded: on timeout the CTA raises the plan's abort flag (and the caller's status
-// word), stops waiting and releases its TMEM.
+// word), stops waiting, lets issued MMAs drain and releases its TMEM.  No load uses cluster
+// multicast; every copy reads this GPU's own memory.
 #include "sle_internal.cuh"
 #include "sle_fft.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -37,15 +43,18 @@ namespace sle {
 namespace {
 
 constexpr int KC = 32;                        // K elements per chunk: one 128-byte row of TF32
-constexpr int TILE_A = 128 * 128;             // 128 rows x 128 bytes
-constexpr int TILE_B = MX_NMAX * 128;         // MX_NMAX rows x 128 bytes
+constexpr int TILE_F = 128 * KC;              // words of one A tile (128 rows x 32)
+constexpr int TILE_A = TILE_F * 4;            // 16 KB
+constexpr int TILE_B = MX_NMAX * 128;         // MX_NMAX rows x 128 bytes = 8 KB
 constexpr int STAGE_BYTES = 4 * TILE_A + 4 * TILE_B;
 constexpr int NSTAGE = 2;
-constexpr int MISC_BYTES = 8192 + 1024;       // coefficients + barriers + bookkeeping
+constexpr int MISC_BYTES = 1024;              // barriers + bookkeeping
 constexpr int MX_SMEM = 1024 + NSTAGE * STAGE_BYTES + MISC_BYTES;
-constexpr int MX_THREADS = 11 * 32;
+constexpr int TC_THREADS = 10 * 32;
 constexpr int ANA_SPAN = 256;                 // degrees per analysis unit (128 per parity)
 constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wait gives up
+constexpr uint32_t TMEM_COLS = 512;
+constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
 
 static_assert(MX_SMEM <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
 
@@ -62,6 +71,10 @@ __device__ __forceinline__ void mbar_arrive(uint32_t a) {
   asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(a) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -73,12 +86,33 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t a, uint32_t parity) {
   return ok != 0;
 }
 
+// Bulk copy global -> this CTA's shared memory (no multicast), completion counted on `mbar`.
+// Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
+// 3-D TMA tensor load (tile mode, no multicast) of the tensor map's box at (x, y, z).
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(mbar)
+      : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
 __device__ __forceinline__ void tc_alloc(uint32_t holder, uint32_t ncols) {
@@ -129,20 +163,9 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// Byte offset of element (row, k) (4-byte elements, k < 32) in a 128-byte-swizzled K-major tile.
-__device__ __forceinline__ uint32_t sw128(int row, int k) {
-  return (uint32_t)(row * 128 + ((((k >> 2) ^ (row & 7)) << 4) | ((k & 3) << 2)));
-}
-// Byte offset of the 16-byte chunk c of row `row`.
-__device__ __forceinline__ uint32_t sw128_chunk(int row, int c) {
-  return (uint32_t)(row * 128 + ((c ^ (row & 7)) << 4));
-}
-
-__device__ __forceinline__ void sts32(uint32_t a, uint32_t v) {
-  asm volatile("st.shared.b32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
-}
-__device__ __forceinline__ void sts128(uint32_t a, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
-  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(a), "r"(x), "r"(y), "r"(z), "r"(w) : "memory");
+// Offset (in 4-byte elements) of (row, k), k < 32, in a 128-byte-swizzled K-major tile.
+__host__ __device__ __forceinline__ int sw_off(int row, int k) {
+  return row * KC + ((((k >> 2) ^ (row & 7)) << 2) | (k & 3));
 }
 
 // ------------------------------------------------------------- precision splits
@@ -204,7 +227,9 @@ __device__ __forceinline__ bool field_off(const MxFieldArgs& a, int f) {
   return false;
 }
 
-// Shared-memory layout common to both contraction kernels.
+// Shared memory of a stage: A tiles [par0 hi][par0 lo][par1 hi][par1 lo] (the order of a
+// Legendre table slot, so one bulk copy fills them), then B tiles [par0 hi][par1 hi][par0 lo]
+// [par1 lo] (the lo pair is where the raw B data lands).
 struct Smem {
   uint8_t* base;        // generic pointer, 1024-aligned
   uint32_t sbase;       // shared-window address of base
@@ -212,7 +237,10 @@ struct Smem {
     return sbase + stage * STAGE_BYTES + (par * 2 + lo) * TILE_A;
   }
   __device__ uint32_t b_tile(int stage, int par, int lo) const {
-    return sbase + stage * STAGE_BYTES + 4 * TILE_A + (par * 2 + lo) * TILE_B;
+    return sbase + stage * STAGE_BYTES + 4 * TILE_A + (lo * 2 + par) * TILE_B;
+  }
+  __device__ uint8_t* b_ptr(int stage, int par, int lo) const {
+    return base + stage * STAGE_BYTES + 4 * TILE_A + (lo * 2 + par) * TILE_B;
   }
   __device__ uint8_t* misc() const { return base + NSTAGE * STAGE_BYTES; }
 };
@@ -223,42 +251,30 @@ __device__ __forceinline__ Smem smem_layout(uint8_t* raw) {
   return Smem{raw + (al - s), al};
 }
 
-// misc region: [0, 8192) coefficients (double2), then barriers and bookkeeping
 struct Misc {
-  double2* coef;
-  uint64_t* bar;        // full[2], empty[2], accum, drain
+  uint64_t* bar;        // full[2], empty[2], accum, drain, raw[2]
   uint32_t* tmem_holder;
   int* active;          // [MX_MAXF]
-  int* chunks;          // [64]
-  int* nch;
   int* any;
 };
 __device__ __forceinline__ Misc misc_layout(const Smem& S) {
   uint8_t* p = S.misc();
   Misc m;
-  m.coef = reinterpret_cast<double2*>(p);
-  m.bar = reinterpret_cast<uint64_t*>(p + 8192);
-  m.tmem_holder = reinterpret_cast<uint32_t*>(p + 8192 + 64);
-  m.active = reinterpret_cast<int*>(p + 8192 + 128);
-  m.chunks = reinterpret_cast<int*>(p + 8192 + 128 + 4 * MX_MAXF);
-  m.nch = reinterpret_cast<int*>(p + 8192 + 128 + 4 * MX_MAXF + 4 * 64);
-  m.any = m.nch + 1;
+  m.bar = reinterpret_cast<uint64_t*>(p);
+  m.tmem_holder = reinterpret_cast<uint32_t*>(p + 64);
+  m.active = reinterpret_cast<int*>(p + 128);
+  m.any = reinterpret_cast<int*>(p + 128 + 4 * MX_MAXF);
   return m;
 }
 
-
 // TMEM use (512 columns): [0, 2N) correction accumulator (Ahi*Blo + Alo*Bhi of every chunk),
 // then nbuf main accumulators of 2N columns (Ahi*Bhi), chunk i into buffer i % nbuf; each
-// accumulator holds [even parity N columns][odd parity N columns].  The tensor core's FP32
-// accumulation truncates, so its error grows with the number of MMAs summed into one
-// accumulator: the main products (the large ones) are spread over fresh buffers and the
-// buffers are added in FP64 by the epilogue.
-constexpr uint32_t TMEM_COLS = 512;
+// accumulator holds [even parity N columns][odd parity N columns].
 __device__ __forceinline__ int main_buffers(int nch, int ncols) {
   return max(1, min(nch, ((int)TMEM_COLS - 2 * ncols) / (2 * ncols)));
 }
 
-// MMA issue loop shared by both kernels: chunk i uses stage i & 1.
+// MMA issue loop: chunk i uses stage i & 1.
 __device__ void mma_loop(const Smem& S, const Misc& M, uint32_t tmem, int nch, int ncols, const Abort& ab) {
   const uint32_t idesc = idesc_tf32(128, ncols);
   const uint32_t full0 = smem_u32(&M.bar[0]), empty0 = smem_u32(&M.bar[2]), accum = smem_u32(&M.bar[4]);
@@ -326,20 +342,22 @@ __device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int ncols, 
 }
 
 // Common prologue: barriers, gates, TMEM.  Returns the TMEM base (all threads).
-__device__ uint32_t prologue(const Misc& M, const MxFieldArgs& a, uint32_t tcols) {
+__device__ uint32_t prologue(const Misc& M, const MxFieldArgs& a) {
   const int warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
-    mbar_init(smem_u32(&M.bar[0]), 5);   // full: 4 producer warps + 1 loader warp
-    mbar_init(smem_u32(&M.bar[1]), 5);
+    mbar_init(smem_u32(&M.bar[0]), 4);   // full: the 4 splitter warps of the stage
+    mbar_init(smem_u32(&M.bar[1]), 4);
     mbar_init(smem_u32(&M.bar[2]), 1);   // empty: one tcgen05.commit
     mbar_init(smem_u32(&M.bar[3]), 1);
     mbar_init(smem_u32(&M.bar[4]), 1);   // accumulators complete
     mbar_init(smem_u32(&M.bar[5]), 1);   // drain after an abort
+    mbar_init(smem_u32(&M.bar[6]), 1);   // raw A and B data of stage 0 / 1 landed
+    mbar_init(smem_u32(&M.bar[7]), 1);
     fence_mbar_init();
   }
   if (threadIdx.x < MX_MAXF) M.active[threadIdx.x] = (threadIdx.x < a.nf) && !field_off(a, threadIdx.x);
   if (warp == 8) {
-    tc_alloc(smem_u32(M.tmem_holder), tcols);
+    tc_alloc(smem_u32(M.tmem_holder), TMEM_COLS);
     tc_relinquish();
   }
   tc_fence_before();
@@ -355,315 +373,206 @@ __device__ uint32_t prologue(const Misc& M, const MxFieldArgs& a, uint32_t tcols
   return t;
 }
 
-__device__ void epilogue_release(uint32_t tmem, uint32_t tcols) {
+__device__ void epilogue_release(uint32_t tmem) {
   tc_fence_before();
   __syncthreads();
   if ((threadIdx.x >> 5) == 8) {
     tc_fence_after();
-    tc_dealloc(tmem, tcols);
+    tc_dealloc(tmem, TMEM_COLS);
   }
 }
 
-// ==================================================================== analysis
-// Unit (m, s): degrees lbase = m + 256 s .. lbase + 255 (clipped at lmax), rows r of the even /
-// odd tile are degrees lbase + 2r / lbase + 2r + 1.  K = latitudes in chunks of 32 starting at
-// the first chunk any of the unit's four segments needs.
-__global__ void __launch_bounds__(MX_THREADS, 1) k_ana_tc(ShtDev P, MxFieldArgs a, int* status) {
-  extern __shared__ uint8_t smraw[];
-  const Smem S = smem_layout(smraw);
-  const Misc M = misc_layout(S);
-  const Abort ab{P.mx_abort, status};
+// ===================================================== Legendre tables (once per plan)
+// The A operand of every chunk is precomputed from the FP64 recurrence and split into TF32
+// hi / lo in the tile order of the shared-memory stage: slot = [par0 hi][par0 lo][par1 hi]
+// [par1 lo], each 128 rows x 32 (4 TILE_F words).  Entries below the significance threshold of
+// their (segment, latitude group) and rows or columns outside the unit stay zero (the table is
+// zeroed first).
+
+// Analysis unit (m, span s): rows r of parity p = degree lbase + 2r + p, K = latitudes
+// 32c .. 32c + 31 for the chunks c = kstart .. ngrp - 1.  Warp (segment q, chunk parity g).
+__global__ void __launch_bounds__(256) k_tab_ana(ShtDev P, uint32_t* tab) {
+  const int4 unit = P.mx_ana_units[blockIdx.x];
+  const int m = unit.x, s = unit.y, kstart = unit.z;
+  const long long off = unit.w;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int2 unit = P.mx_ana_units[blockIdx.x];
-  const int m = unit.x, s = unit.y, L = P.lmax;
+  const int q = warp & 3, g = warp >> 2;
+  const int L = P.lmax;
   const int lbase = m + ANA_SPAN * s;
   const int nd = min(ANA_SPAN, L + 1 - lbase);
-  const int nsegu = (nd + SEG - 1) / SEG;
-  const int seg0 = P.segoff[m] + (ANA_SPAN / SEG) * s;
-  int kstart = P.ngrp;
-  for (int q = 0; q < nsegu; ++q) kstart = min(kstart, (int)P.istart[seg0 + q]);
-  const int nch = P.ngrp - kstart;
-  const int ncols = a.ncols;
-  const uint32_t tcols = TMEM_COLS;
-  const long long cbase = P.moff[m] + (lbase - m);
-  for (int t = threadIdx.x; t < nd; t += blockDim.x) M.coef[t] = make_double2(P.be[cbase + t], P.cf[cbase + t]);
-  const uint32_t tmem = prologue(M, a, tcols);
-  if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
-    const uint32_t empty0 = smem_u32(&M.bar[2]), full0 = smem_u32(&M.bar[0]);
-    if (warp < 8) {
-      // ---- producers: segment q of the unit, stage g
-      const int g = warp >> 2, q = warp & 3;
-      const bool valid = q < nsegu;
-      const int seg = seg0 + q;
-      const int ist = valid ? (int)P.istart[seg] : P.ngrp;
-      const int len = valid ? min(SEG, nd - SEG * q) : 0;
-      int round = 0;
-      for (int i = g; i < nch; i += 2, ++round) {
-        const int c = kstart + i;
-        if (!mbar_wait(empty0 + 8 * g, (uint32_t)((round & 1) ^ 1), ab)) break;
-        if (valid) {
-          const uint32_t aeh = S.a_tile(g, 0, 0), ael = S.a_tile(g, 0, 1);
-          const uint32_t aoh = S.a_tile(g, 1, 0), aol = S.a_tile(g, 1, 1);
-          if (c < ist) {
-            // negligible block: zero rows 32q .. 32q+31 of all four tiles
-            for (int e = lane; e < 32 * 8; e += 32) {
-              const int row = SEG / 2 * q + (e >> 3), ch = e & 7;
-              const uint32_t o = sw128_chunk(row, ch);
-              sts128(aeh + o, 0, 0, 0, 0);
-              sts128(ael + o, 0, 0, 0, 0);
-              sts128(aoh + o, 0, 0, 0, 0);
-              sts128(aol + o, 0, 0, 0, 0);
-            }
-          } else {
-            const int j = KC * c + lane;
-            const double mu = P.mu[j];
-            const double2 sd = P.seeds[(size_t)seg * P.nh + j];
-            double qa = sd.x, qb = sd.y;
-            const double2* cf = M.coef + SEG * q;
-            for (int t = 0; t < len; t += 2) {
-              const int row = SEG / 2 * q + (t >> 1);
-              const uint32_t o = sw128(row, lane);
-              double2 bc = cf[t];
-              double qn = fma(mu, qb, bc.x * qa);
-              qa = qb;
-              qb = qn;
-              uint32_t h, l;
-              split_f64(bc.y * qn, h, l);
-              sts32(aeh + o, h);
-              sts32(ael + o, l);
-              if (t + 1 < len) {
-                bc = cf[t + 1];
-                qn = fma(mu, qb, bc.x * qa);
-                qa = qb;
-                qb = qn;
-                split_f64(bc.y * qn, h, l);
-                sts32(aoh + o, h);
-                sts32(aol + o, l);
-              }
-            }
-          }
-        }
-        fence_proxy_async();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(full0 + 8 * g);
-      }
-    } else if (warp == 8) {
-      if (lane == 0) mma_loop(S, M, tmem, nch, ncols, ab);
-      __syncwarp();
-    } else {
-      // ---- B loader: folded FFT chunk (S rows, D rows) split into TF32 hi / lo
-      const int lw = warp - 9;
-      const int nrow = 2 * a.nf;
-      int round = 0;
-      for (int i = lw; i < nch; i += 2, ++round) {
-        const int c = kstart + i;
-        if (!mbar_wait(empty0 + 8 * lw, (uint32_t)((round & 1) ^ 1), ab)) break;
-#pragma unroll
-        for (int par = 0; par < 2; ++par) {
-          const float* src = P.mx_xf + (((size_t)m * 2 + par) * P.ngrp + c) * (size_t)(MX_NMAX * KC);
-          const uint32_t bh = S.b_tile(lw, par, 0), bl = S.b_tile(lw, par, 1);
-          for (int n = 0; n < nrow; n += 4) {
-            float v[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) v[u] = (n + u < nrow) ? __ldg(src + (n + u) * KC + lane) : 0.0f;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              if (n + u < nrow) {
-                uint32_t h, l;
-                split_f32(v[u], h, l);
-                const uint32_t o = sw128(n + u, lane);
-                sts32(bh + o, h);
-                sts32(bl + o, l);
-              }
-            }
-          }
-        }
-        fence_proxy_async();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(full0 + 8 * lw);
-      }
-    }
-    // ---- epilogue: warps 0-3 own TMEM lanes 0-127 = rows of both parity tiles
-    if (warp < 4) {
-      const int r = 32 * warp + lane;
-      const int le = lbase + 2 * r;
-      bool ok = true;
-      if (nch > 0) {
-        ok = mbar_wait(smem_u32(&M.bar[4]), 0u, ab);
-        tc_fence_after();
-      }
-      ok = __all_sync(0xffffffffu, ok);
-      if (ok) {
-        const double inv = 1.0 / SQRT2_LEGACY;
-        const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
-        for (int cb = 0; cb < (2 * a.nf + 15) / 16; ++cb) {
-          double ve[16], vo[16];
-          if (nch > 0) {
-            acc_read(lanebase, nch, ncols, cb, ve, vo);
-          } else {
-#pragma unroll
-            for (int u = 0; u < 16; ++u) ve[u] = vo[u] = 0.0;
-          }
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const int f = 8 * cb + u;
-            if (f < a.nf && M.active[f] && le <= L) {
-              double2* dst = a.spec[f] + P.moff[m] + (le - m);
-              const double2 ev = make_double2(ve[2 * u] * inv, ve[2 * u + 1] * inv);
-              if (le + 1 <= L) {
-                dst[0] = ev;
-                dst[1] = make_double2(vo[2 * u] * inv, vo[2 * u + 1] * inv);
-              } else {
-                dst[0] = ev;
-              }
-            }
-          }
-        }
-        // degree 0 in FP64 from the row sums of the fold: U_00 = sqrt(0.5) sum_j S_0(j) / 1.41421356
-        __syncwarp();
-        if (m == 0 && s == 0 && warp == 0 && lane < a.nf && M.active[lane]) {
-          const double* s0 = P.mx_s0 + (size_t)lane * P.nh;
-          double acc = 0.0;
-          for (int j = 0; j < P.nh; ++j) acc += s0[j];
-          a.spec[lane][0] = make_double2(__dmul_rn(__dsqrt_rn(0.5), acc) / SQRT2_LEGACY, 0.0);
-        }
-      }
+  if (SEG * q >= nd) return;
+  const int seg = P.segoff[m] + (ANA_SPAN / SEG) * s + q;
+  const int len = min(SEG, nd - SEG * q);
+  const long long cbase = P.moff[m] + (lbase - m) + SEG * q;
+  for (int c = kstart + g; c < P.ngrp; c += 2) {
+    if (c < (int)P.istart[seg]) continue;
+    uint32_t* slot = tab + (off + (c - kstart)) * 4 * TILE_F;
+    const int j = KC * c + lane;
+    const double mu = P.mu[j];
+    const double2 sd = P.seeds[(size_t)seg * P.nh + j];
+    double qa = sd.x, qb = sd.y;
+    for (int t = 0; t < len; ++t) {
+      const double qn = fma(mu, qb, P.be[cbase + t] * qa);
+      qa = qb;
+      qb = qn;
+      uint32_t h, l;
+      split_f64(P.cf[cbase + t] * qn, h, l);
+      const int o = sw_off(SEG / 2 * q + (t >> 1), lane);
+      uint32_t* tp = slot + (t & 1) * 2 * TILE_F;
+      tp[o] = h;
+      tp[TILE_F + o] = l;
     }
   }
-  epilogue_release(tmem, tcols);
 }
 
-// =================================================================== synthesis
-// Unit (m, t): latitudes 128 t .. 128 t + 127 (rows; clipped at nh), K = degrees of m in
-// segments of 64 (32 even + 32 odd), skipping segments negligible on the whole tile.
-__global__ void __launch_bounds__(MX_THREADS, 1) k_syn_tc(ShtDev P, MxFieldArgs a, int* status) {
+// Synthesis unit (m, latitude tile t): rows = latitudes 128 t + row, chunk i = segment
+// seg_list[off + i] of m (K = the degree's index in its parity).  Thread per latitude row.
+__global__ void __launch_bounds__(128) k_tab_syn(ShtDev P, uint32_t* tab) {
+  const int4 unit = P.mx_syn_units[blockIdx.x];
+  const int m = unit.x, t = unit.y, nch = unit.z;
+  const long long off = unit.w;
+  const int row = threadIdx.x;
+  const int j = 128 * t + row;
+  if (j >= P.nh) return;
+  const int grp = j >> 5;
+  const double mu = P.mu[j];
+  for (int i = 0; i < nch; ++i) {
+    const int seg = P.mx_syn_seg[off + i];
+    if (grp < (int)P.istart[seg]) continue;
+    const int l0 = P.seg_l0[seg];
+    const int len = min(SEG, P.lmax + 1 - l0);
+    const long long cbase = P.moff[m] + (l0 - m);
+    uint32_t* slot = tab + (off + i) * 4 * TILE_F;
+    const double2 sd = P.seeds[(size_t)seg * P.nh + j];
+    double qa = sd.x, qb = sd.y;
+    for (int tt = 0; tt < len; ++tt) {
+      const double qn = fma(mu, qb, P.be[cbase + tt] * qa);
+      qa = qb;
+      qb = qn;
+      uint32_t h, l;
+      split_f64(P.cf[cbase + tt] * qn, h, l);
+      const int o = sw_off(row, tt >> 1);
+      uint32_t* tp = slot + (tt & 1) * 2 * TILE_F;
+      tp[o] = h;
+      tp[TILE_F + o] = l;
+    }
+  }
+}
+
+// ============================================================ Legendre contraction
+// Analysis B data: the TMA box of the folded FFT is [field][32 latitudes][S.re, S.im, D.re, D.im]
+// (16 bytes per entry) in the stage's B lo tiles; the 4 splitter warps read it, synchronise,
+// and write rows 2f / 2f+1 of the parity-0 (S) and parity-1 (D) tiles.
+__device__ __forceinline__ void split_b_ana(const Smem& S, int st, int nf, int tid, int bar_id) {
+  const float4* box = reinterpret_cast<const float4*>(S.b_ptr(st, 0, 1));
+  float4 v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int e = tid + 128 * u;
+    v[u] = ((e >> 5) < nf) ? box[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  named_bar(bar_id, 128);
+  uint32_t* h0 = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0, 0));
+  uint32_t* h1 = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1, 0));
+  uint32_t* l0 = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0, 1));
+  uint32_t* l1 = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1, 1));
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int e = tid + 128 * u;
+    const int f = e >> 5, k = e & 31;
+    if (f >= nf) continue;
+    const int o0 = sw_off(2 * f, k), o1 = sw_off(2 * f + 1, k);
+    uint32_t h, l;
+    split_f32(v[u].x, h, l);
+    h0[o0] = h;
+    l0[o0] = l;
+    split_f32(v[u].y, h, l);
+    h0[o1] = h;
+    l0[o1] = l;
+    split_f32(v[u].z, h, l);
+    h1[o0] = h;
+    l1[o0] = l;
+    split_f32(v[u].w, h, l);
+    h1[o1] = h;
+    l1[o1] = l;
+  }
+}
+
+// Synthesis B data: raw blocks already in the tile order; split in place.
+__device__ __forceinline__ void split_b_syn(const Smem& S, int st, int nrow, int tid) {
+#pragma unroll
+  for (int par = 0; par < 2; ++par) {
+    uint32_t* hp = reinterpret_cast<uint32_t*>(S.b_ptr(st, par, 0));
+    uint32_t* lp = reinterpret_cast<uint32_t*>(S.b_ptr(st, par, 1));
+    for (int e = tid; e < nrow * KC; e += 128) {
+      uint32_t h, l;
+      split_f32(__uint_as_float(lp[e]), h, l);
+      hp[e] = h;
+      lp[e] = l;
+    }
+  }
+}
+
+// One CTA per work unit.  Analysis: rows of D = degrees, columns = (Re, Im) of the fields;
+// synthesis: rows = latitudes.
+template <bool SYN>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox) {
   extern __shared__ uint8_t smraw[];
   const Smem S = smem_layout(smraw);
   const Misc M = misc_layout(S);
   const Abort ab{P.mx_abort, status};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int2 unit = P.mx_syn_units[blockIdx.x];
-  const int m = unit.x, t = unit.y, L = P.lmax;
+  const int4 unit = SYN ? P.mx_syn_units[blockIdx.x] : P.mx_ana_units[blockIdx.x];
+  const int m = unit.x, L = P.lmax;
+  const long long toff = unit.w;
+  const int nch = SYN ? unit.z : P.ngrp - unit.z;
   const int ncols = a.ncols;
-  const uint32_t tcols = TMEM_COLS;
-  const int nl = L - m + 1;
-  const long long cbase = P.moff[m];
-  for (int u = threadIdx.x; u < nl; u += blockDim.x) M.coef[u] = make_double2(P.be[cbase + u], P.cf[cbase + u]);
-  if (threadIdx.x == 0) {
-    const int glast = min(P.ngrp, 4 * t + 4) - 1;
-    int n = 0;
-    for (int q = 0; q < P.segoff[m + 1] - P.segoff[m]; ++q)
-      if ((int)P.istart[P.segoff[m] + q] <= glast) M.chunks[n++] = q;
-    *M.nch = n;
-  }
-  const uint32_t tmem = prologue(M, a, tcols);
-  const int nch = *M.nch;
+  const uint32_t* tab = SYN ? P.mx_tab_syn : P.mx_tab_ana;
+  const uint32_t tmem = prologue(M, a);
   if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
     const uint32_t empty0 = smem_u32(&M.bar[2]), full0 = smem_u32(&M.bar[0]);
-    if (warp < 8) {
-      // ---- producers: rows 32 wq .. 32 wq + 31 of the tile, stage g
-      const int g = warp >> 2, wq = warp & 3;
-      const int row = 32 * wq + lane;
-      const int j = 128 * t + row;
-      const int grp = j >> 5;
-      const bool okrow = j < P.nh;
-      const double mu = okrow ? P.mu[j] : 0.0;
-      int round = 0;
-      for (int i = g; i < nch; i += 2, ++round) {
-        if (!mbar_wait(empty0 + 8 * g, (uint32_t)((round & 1) ^ 1), ab)) break;
-        const int q = M.chunks[i];
-        const int seg = P.segoff[m] + q;
-        const int l0 = m + SEG * q;
-        const int len = min(SEG, L + 1 - l0);
-        const uint32_t aeh = S.a_tile(g, 0, 0), ael = S.a_tile(g, 0, 1);
-        const uint32_t aoh = S.a_tile(g, 1, 0), aol = S.a_tile(g, 1, 1);
-        if (okrow) {
-          if (grp < (int)P.istart[seg]) {
-#pragma unroll
-            for (int ch = 0; ch < 8; ++ch) {
-              const uint32_t o = sw128_chunk(row, ch);
-              sts128(aeh + o, 0, 0, 0, 0);
-              sts128(ael + o, 0, 0, 0, 0);
-              sts128(aoh + o, 0, 0, 0, 0);
-              sts128(aol + o, 0, 0, 0, 0);
-            }
+    const int nrow = 2 * a.nf;
+    if (warp == 9) {
+      // ---- loader: A slot and B data of chunk i into stage i & 1
+      if (lane == 0) {
+        const uint32_t bbytes = SYN ? 2u * (uint32_t)nrow * 128u : (uint32_t)zbox * 32u * 16u;
+        for (int i = 0; i < nch; ++i) {
+          const int st = i & 1;
+          if (!mbar_wait(empty0 + 8 * st, (uint32_t)(((i >> 1) & 1) ^ 1), ab)) break;
+          const uint32_t raw = smem_u32(&M.bar[6 + st]);
+          mbar_arrive_expect_tx(raw, 4u * TILE_A + bbytes);
+          bulk_g2s(S.a_tile(st, 0, 0), tab + (toff + i) * 4 * TILE_F, 4u * TILE_A, raw);
+          if (SYN) {
+            const int seg = P.mx_syn_seg[toff + i];
+            bulk_g2s(S.b_tile(st, 0, 1), P.mx_bsyn + ((size_t)seg * 2 + 0) * BBLOCK, (uint32_t)nrow * 128u, raw);
+            bulk_g2s(S.b_tile(st, 1, 1), P.mx_bsyn + ((size_t)seg * 2 + 1) * BBLOCK, (uint32_t)nrow * 128u, raw);
           } else {
-            const double2 sd = P.seeds[(size_t)seg * P.nh + j];
-            double qa = sd.x, qb = sd.y;
-            const double2* cf = M.coef + SEG * q;
-            for (int ch = 0; ch < 8; ++ch) {
-              uint32_t eh[4], el[4], oh[4], ol[4];
-#pragma unroll
-              for (int v = 0; v < 4; ++v) {
-                const int te = 8 * ch + 2 * v;
-                eh[v] = el[v] = oh[v] = ol[v] = 0u;
-                if (te < len) {
-                  const double2 bc = cf[te];
-                  const double qn = fma(mu, qb, bc.x * qa);
-                  qa = qb;
-                  qb = qn;
-                  split_f64(bc.y * qn, eh[v], el[v]);
-                }
-                if (te + 1 < len) {
-                  const double2 bc = cf[te + 1];
-                  const double qn = fma(mu, qb, bc.x * qa);
-                  qa = qb;
-                  qb = qn;
-                  split_f64(bc.y * qn, oh[v], ol[v]);
-                }
-              }
-              const uint32_t o = sw128_chunk(row, ch);
-              sts128(aeh + o, eh[0], eh[1], eh[2], eh[3]);
-              sts128(ael + o, el[0], el[1], el[2], el[3]);
-              sts128(aoh + o, oh[0], oh[1], oh[2], oh[3]);
-              sts128(aol + o, ol[0], ol[1], ol[2], ol[3]);
-            }
+            tma_load_3d(S.b_tile(st, 0, 1), &tmx, 4 * m, KC * (unit.z + i), 0, raw);
           }
         }
-        fence_proxy_async();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(full0 + 8 * g);
       }
+      __syncwarp();
     } else if (warp == 8) {
       if (lane == 0) mma_loop(S, M, tmem, nch, ncols, ab);
       __syncwarp();
     } else {
-      // ---- B loader: 1.41421356 U[l, m] of the segment, rows 2f (Re) and 2f+1 (Im), K = the
-      // degree's index in its parity; l = 0 is left out (added in FP64 by the inverse FFT)
-      const int lw = warp - 9;
+      // ---- splitters: group g = stage g
+      const int g = warp >> 2, tid = threadIdx.x & 127;
       int round = 0;
-      for (int i = lw; i < nch; i += 2, ++round) {
-        if (!mbar_wait(empty0 + 8 * lw, (uint32_t)((round & 1) ^ 1), ab)) break;
-        const int q = M.chunks[i];
-        const int l0 = m + SEG * q;
-        const int len = min(SEG, L + 1 - l0);
-        for (int f = 0; f < a.nf; ++f) {
-          const double2* U = a.spec[f] + cbase + (l0 - m);
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int tt = lane + 32 * h;
-            double2 u = make_double2(0.0, 0.0);
-            if (tt < len && !(m == 0 && l0 + tt == 0) && M.active[f]) u = U[tt];
-            const int par = tt & 1, k = tt >> 1;
-            uint32_t rh, rl, ih, il;
-            split_f64(u.x * SQRT2_LEGACY, rh, rl);
-            split_f64(u.y * SQRT2_LEGACY, ih, il);
-            const uint32_t bh = S.b_tile(lw, par, 0), bl = S.b_tile(lw, par, 1);
-            sts32(bh + sw128(2 * f, k), rh);
-            sts32(bl + sw128(2 * f, k), rl);
-            sts32(bh + sw128(2 * f + 1, k), ih);
-            sts32(bl + sw128(2 * f + 1, k), il);
-          }
-        }
+      for (int i = g; i < nch; i += 2, ++round) {
+        const bool ok = mbar_wait(smem_u32(&M.bar[6 + g]), (uint32_t)(round & 1), ab);
+        if (!__all_sync(0xffffffffu, ok)) break;
+        if (SYN) split_b_syn(S, g, nrow, tid);
+        else split_b_ana(S, g, a.nf, tid, 1 + g);
         fence_proxy_async();
         __syncwarp();
-        if (lane == 0) mbar_arrive(full0 + 8 * lw);
+        if (lane == 0) mbar_arrive(full0 + 8 * g);
       }
     }
-    // ---- epilogue: north = E + O, south = E - O for the tile's latitudes
+    // ---- epilogue: warps 0-3 own TMEM lanes 0-127
     if (warp < 4) {
       const int r = 32 * warp + lane;
-      const int j = 128 * t + r;
       bool ok = true;
       if (nch > 0) {
         ok = mbar_wait(smem_u32(&M.bar[4]), 0u, ab);
@@ -672,6 +581,9 @@ __global__ void __launch_bounds__(MX_THREADS, 1) k_syn_tc(ShtDev P, MxFieldArgs 
       ok = __all_sync(0xffffffffu, ok);
       if (ok) {
         const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
+        const double inv = 1.0 / SQRT2_LEGACY;
+        const int le = m + ANA_SPAN * unit.y + 2 * r;   // analysis: even degree of row r
+        const int j = 128 * unit.y + r;                 // synthesis: latitude of row r
         for (int cb = 0; cb < (2 * a.nf + 15) / 16; ++cb) {
           double ve[16], vo[16];
           if (nch > 0) {
@@ -683,25 +595,41 @@ __global__ void __launch_bounds__(MX_THREADS, 1) k_syn_tc(ShtDev P, MxFieldArgs 
 #pragma unroll
           for (int u = 0; u < 8; ++u) {
             const int f = 8 * cb + u;
-            if (f < a.nf && M.active[f] && j < P.nh) {
-              float2* gn = P.mx_gns + ((size_t)(2 * f) * P.nm + m) * P.nh;
-              float2* gs = P.mx_gns + ((size_t)(2 * f + 1) * P.nm + m) * P.nh;
-              gn[j] = make_float2((float)(ve[2 * u] + vo[2 * u]), (float)(ve[2 * u + 1] + vo[2 * u + 1]));
-              gs[j] = make_float2((float)(ve[2 * u] - vo[2 * u]), (float)(ve[2 * u + 1] - vo[2 * u + 1]));
+            if (f >= a.nf || !M.active[f]) continue;
+            if (SYN) {
+              if (j < P.nh) {
+                float4* gq = reinterpret_cast<float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm + m;
+                *gq = make_float4((float)(ve[2 * u] + vo[2 * u]), (float)(ve[2 * u + 1] + vo[2 * u + 1]),
+                                  (float)(ve[2 * u] - vo[2 * u]), (float)(ve[2 * u + 1] - vo[2 * u + 1]));
+              }
+            } else if (le <= L) {
+              double2* dst = a.spec[f] + P.moff[m] + (le - m);
+              dst[0] = make_double2(ve[2 * u] * inv, ve[2 * u + 1] * inv);
+              if (le + 1 <= L) dst[1] = make_double2(vo[2 * u] * inv, vo[2 * u + 1] * inv);
             }
+          }
+        }
+        if (!SYN) {
+          // degree 0 in FP64 from the row sums of the fold: U_00 = sqrt(0.5) sum_j S_0(j) / 1.41421356
+          __syncwarp();
+          if (m == 0 && unit.y == 0 && warp == 0 && lane < a.nf && M.active[lane]) {
+            const double* s0 = P.mx_s0 + (size_t)lane * P.nh;
+            double acc = 0.0;
+            for (int jj = 0; jj < P.nh; ++jj) acc += s0[jj];
+            a.spec[lane][0] = make_double2(__dmul_rn(__dsqrt_rn(0.5), acc) / SQRT2_LEGACY, 0.0);
           }
         }
       }
     }
   }
-  epilogue_release(tmem, tcols);
+  epilogue_release(tmem);
 }
 
 // ============================================================== row FFT kernels
 // Row rFFT (FP64) of the north row j and south row nlat-1-j of field blockIdx.y, fold with the
-// weights (FP64), output rounded to FP32 in the analysis B layout X[m][par][chunk][row][k]
-// (row 2f = Re, 2f+1 = Im, chunk = j / 32, k = j % 32).  The m = 0 fold (row sums) is also kept
-// in FP64 in s0[f][j] for the FP64 degree-0 coefficient.
+// weights (FP64), output rounded to FP32: X[f][j][m] = (S.re, S.im, D.re, D.im), one 16-byte
+// entry per order (coalesced), the layout the analysis kernel's TMA box reads.  The m = 0 fold
+// (row sums) is also kept in FP64 in s0[f][j] for the FP64 degree-0 coefficient.
 template <int N>
 __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ double2 smd2[];
@@ -721,7 +649,7 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fold_mx(ShtDev P,
   __syncthreads();
   const double2* Z = stockham_c<N, 1, false>(A, B, tw);
   const double wn = P.wn[j], ws = P.ws[j];
-  const int c = j >> 5, k = j & 31;
+  float4* X = reinterpret_cast<float4*>(P.mx_xf) + ((size_t)f * P.nh + j) * P.nm;
   for (int m = threadIdx.x; m < P.nm; m += blockDim.x) {
     double2 xr[2];
 #pragma unroll
@@ -742,18 +670,13 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fold_mx(ShtDev P,
     }
     const double2 an = cscale(xr[0], wn), bs = cscale(xr[1], ws);
     if (m == 0) P.mx_s0[(size_t)f * P.nh + j] = an.x + bs.x;
-    float* xs = P.mx_xf + ((((size_t)m * 2 + 0) * P.ngrp + c) * MX_NMAX + 2 * f) * KC + k;
-    float* xd = P.mx_xf + ((((size_t)m * 2 + 1) * P.ngrp + c) * MX_NMAX + 2 * f) * KC + k;
-    xs[0] = (float)(an.x + bs.x);
-    xs[KC] = (float)(an.y + bs.y);
-    xd[0] = (float)(an.x - bs.x);
-    xd[KC] = (float)(an.y - bs.y);
+    X[m] = make_float4((float)(an.x + bs.x), (float)(an.y + bs.y), (float)(an.x - bs.x), (float)(an.y - bs.y));
   }
 }
 
 // Inverse: north and south Legendre sums of field blockIdx.y (FP32 accumulators, m <= lmax, 0
-// above), unnormalised inverse real FFT in FP64, plus the FP64 degree-0 term
-// 1.41421356 sqrt(0.5) Re U_00 in every cell; optional epilogue out2 = grid * mul2.
+// above; one 16-byte entry per order), unnormalised inverse real FFT in FP64, plus the FP64
+// degree-0 term 1.41421356 sqrt(0.5) Re U_00 in every cell; optional epilogue out2 = grid * mul2.
 template <int N>
 __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_unfold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ double2 smd2[];
@@ -764,16 +687,15 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_unfold_mx(ShtDev 
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
   const int js = P.nlat - 1 - j;
-  const float2* GN = P.mx_gns + (size_t)(2 * f) * P.nm * P.nh;
-  const float2* GS = P.mx_gns + (size_t)(2 * f + 1) * P.nm * P.nh;
+  const float4* G = reinterpret_cast<const float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm;
   const double c00 = __dmul_rn(__dmul_rn(SQRT2_LEGACY, a.spec[f][0].x), __dsqrt_rn(0.5));
   for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = P.tw[t];
   for (int m = threadIdx.x; m <= N; m += blockDim.x) {
     double2 gn = make_double2(0.0, 0.0), gs = gn;
     if (m < P.nm) {
-      const float2 vn = GN[(size_t)m * P.nh + j], vs = GS[(size_t)m * P.nh + j];
-      gn = make_double2(vn.x, vn.y);
-      gs = make_double2(vs.x, vs.y);
+      const float4 v = G[m];
+      gn = make_double2(v.x, v.y);
+      gs = make_double2(v.z, v.w);
     }
     if (m == 0) {
       gn.x += c00;
@@ -824,6 +746,25 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_unfold_mx(ShtDev 
   }
 }
 
+// Synthesis B operand: per segment s (order m, degrees l0..l0+63) and parity, rows 2f / 2f+1 =
+// Re / Im of 1.41421356 U_f[l, m] rounded to FP32, k = the degree's index in its parity, in the
+// tile order (MX_NMAX x 32 per block).  l = 0 is left out (the inverse FFT adds it in FP64);
+// degrees beyond lmax are zero.  Block (segment, group of 4 fields), 64 threads per field.
+__global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
+  const int s = blockIdx.x;
+  const int f = 4 * blockIdx.y + (threadIdx.x >> 6);
+  const int t = threadIdx.x & 63;
+  if (f >= a.nf || field_off(a, f)) return;
+  const int m = P.seg_m[s], l0 = P.seg_l0[s];
+  const int len = min(SEG, P.lmax + 1 - l0);
+  double2 u = make_double2(0.0, 0.0);
+  if (t < len && !(m == 0 && l0 + t == 0)) u = a.spec[f][P.moff[m] + (l0 - m) + t];
+  float* blk = P.mx_bsyn + ((size_t)s * 2 + (t & 1)) * BBLOCK;
+  const int k = t >> 1;
+  blk[sw_off(2 * f, k)] = (float)(u.x * SQRT2_LEGACY);
+  blk[sw_off(2 * f + 1, k)] = (float)(u.y * SQRT2_LEGACY);
+}
+
 size_t mx_fft_smem(const ShtDev& d) { return (size_t)5 * d.n2 * sizeof(double2); }
 
 template <typename T>
@@ -837,6 +778,21 @@ int mx_alloc(T** p, size_t n) {
   }
   return SLE_OK;
 }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link-time libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+constexpr int ZBOX[3] = {8, 16, 32};
 
 }  // namespace
 
@@ -852,66 +808,110 @@ int sht_mx_prepare(sle_sht* p) {
     set_error("mixed precision supports lmax <= 511 (got %d)", d.lmax);
     return SLE_ERR_BAD_SHAPE;
   }
-  const size_t nxf = (size_t)d.nm * 2 * d.ngrp * MX_NMAX * KC;
-  SLE_TRY(mx_alloc(&p->mx_xf, nxf));
-  SLE_TRY(mx_alloc(&p->mx_gns, (size_t)2 * MX_MAXF * d.nm * d.nh));
+  const size_t nx4 = (size_t)MX_MAXF * d.nh * d.nm;   // 16-byte entries of X and of the sums
+  SLE_TRY(mx_alloc(&p->mx_xf, 4 * nx4));
+  SLE_TRY(mx_alloc(&p->mx_gns, 2 * nx4));
+  SLE_TRY(mx_alloc(&p->mx_bsyn, (size_t)d.nseg * 2 * BBLOCK));
   SLE_TRY(mx_alloc(&p->mx_s0, (size_t)MX_MAXF * d.nh));
   SLE_TRY(mx_alloc(&p->mx_abort, 1));
-  SLE_CUDA(cudaMemset(p->mx_xf, 0, nxf * sizeof(float)));
-  SLE_CUDA(cudaMemset(p->mx_gns, 0, (size_t)2 * MX_MAXF * d.nm * d.nh * sizeof(float2)));
+  SLE_CUDA(cudaMemset(p->mx_xf, 0, 4 * nx4 * sizeof(float)));
+  SLE_CUDA(cudaMemset(p->mx_gns, 0, 2 * nx4 * sizeof(float2)));
+  SLE_CUDA(cudaMemset(p->mx_bsyn, 0, (size_t)d.nseg * 2 * BBLOCK * sizeof(float)));
   SLE_CUDA(cudaMemset(p->mx_abort, 0, sizeof(int)));
-  // work units, most work first (generation work ~ degrees x significant latitude groups)
+  // work units, most work first; each unit's chunks are contiguous slots of its Legendre table
   std::vector<unsigned char> ist(d.nseg);
   std::vector<int> segoff(d.nm + 1);
   SLE_CUDA(cudaMemcpy(ist.data(), p->istart, d.nseg, cudaMemcpyDeviceToHost));
   SLE_CUDA(cudaMemcpy(segoff.data(), p->segoff, (d.nm + 1) * sizeof(int), cudaMemcpyDeviceToHost));
   const int L = d.lmax;
-  std::vector<std::pair<long long, int2>> au, su;
+  struct AU { long long w; int m, s, kstart; };
+  struct SU { long long w; int m, t; std::vector<int> segs; };
+  std::vector<AU> au;
+  std::vector<SU> su;
   for (int m = 0; m <= L; ++m) {
     const int nl = L - m + 1;
     for (int s = 0; s * ANA_SPAN < nl; ++s) {
-      long long w = 1;
       const int nd = std::min(ANA_SPAN, nl - ANA_SPAN * s);
-      for (int q = 0; q * SEG < nd; ++q) {
-        const int seg = segoff[m] + (ANA_SPAN / SEG) * s + q;
-        w += (long long)std::min(SEG, nd - SEG * q) * (d.ngrp - ist[seg]);
-      }
-      au.push_back({w, make_int2(m, s)});
+      int kstart = d.ngrp;
+      for (int q = 0; q * SEG < nd; ++q) kstart = std::min(kstart, (int)ist[segoff[m] + (ANA_SPAN / SEG) * s + q]);
+      au.push_back({(long long)(d.ngrp - kstart) * 64 + nd, m, s, kstart});
     }
     const int ntile = (d.nh + 127) / 128;
     for (int t = 0; t < ntile; ++t) {
-      long long w = 1;
-      for (int seg = segoff[m]; seg < segoff[m + 1]; ++seg) {
-        const int l0 = m + SEG * (seg - segoff[m]);
-        const int g0 = 4 * t, g1 = std::min(d.ngrp, 4 * t + 4);
-        const int sig = std::max(0, g1 - std::max(g0, (int)ist[seg]));
-        w += (long long)std::min(SEG, L + 1 - l0) * sig;
-      }
-      su.push_back({w, make_int2(m, t)});
+      SU u{0, m, t, {}};
+      const int glast = std::min(d.ngrp, 4 * t + 4) - 1;
+      for (int seg = segoff[m]; seg < segoff[m + 1]; ++seg)
+        if ((int)ist[seg] <= glast) u.segs.push_back(seg);
+      u.w = (long long)u.segs.size() * 64 + 1;
+      su.push_back(u);
     }
   }
-  auto by_work = [](const std::pair<long long, int2>& x, const std::pair<long long, int2>& y) {
-    return x.first > y.first;
-  };
-  std::stable_sort(au.begin(), au.end(), by_work);
-  std::stable_sort(su.begin(), su.end(), by_work);
-  std::vector<int2> av, sv;
-  for (auto& e : au) av.push_back(e.second);
-  for (auto& e : su) sv.push_back(e.second);
+  std::stable_sort(au.begin(), au.end(), [](const AU& x, const AU& y) { return x.w > y.w; });
+  std::stable_sort(su.begin(), su.end(), [](const SU& x, const SU& y) { return x.w > y.w; });
+  std::vector<int4> av, sv;
+  std::vector<int> segs;
+  long long na = 0, ns = 0;
+  for (const AU& u : au) {
+    av.push_back(make_int4(u.m, u.s, u.kstart, (int)na));
+    na += d.ngrp - u.kstart;
+  }
+  for (const SU& u : su) {
+    sv.push_back(make_int4(u.m, u.t, (int)u.segs.size(), (int)ns));
+    for (int sg : u.segs) segs.push_back(sg);
+    ns += (long long)u.segs.size();
+  }
   SLE_TRY(mx_alloc(&p->mx_ana_units, av.size()));
   SLE_TRY(mx_alloc(&p->mx_syn_units, sv.size()));
-  SLE_CUDA(cudaMemcpy(p->mx_ana_units, av.data(), av.size() * sizeof(int2), cudaMemcpyHostToDevice));
-  SLE_CUDA(cudaMemcpy(p->mx_syn_units, sv.data(), sv.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  SLE_TRY(mx_alloc(&p->mx_syn_seg, segs.size() + 1));
+  SLE_CUDA(cudaMemcpy(p->mx_ana_units, av.data(), av.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  SLE_CUDA(cudaMemcpy(p->mx_syn_units, sv.data(), sv.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  if (!segs.empty())
+    SLE_CUDA(cudaMemcpy(p->mx_syn_seg, segs.data(), segs.size() * sizeof(int), cudaMemcpyHostToDevice));
   p->n_ana_units = (int)av.size();
   p->n_syn_units = (int)sv.size();
+  // Legendre tables: FP64 recurrence, split into TF32 hi / lo, zero where negligible
+  const size_t tab_a = (size_t)na * 4 * TILE_F, tab_s = (size_t)ns * 4 * TILE_F;
+  SLE_TRY(mx_alloc(&p->mx_tab_ana, tab_a + 1));
+  SLE_TRY(mx_alloc(&p->mx_tab_syn, tab_s + 1));
+  SLE_CUDA(cudaMemset(p->mx_tab_ana, 0, tab_a * sizeof(uint32_t)));
+  SLE_CUDA(cudaMemset(p->mx_tab_syn, 0, tab_s * sizeof(uint32_t)));
+  p->mx_table_bytes = (double)(tab_a + tab_s) * sizeof(uint32_t);
   d.mx_xf = p->mx_xf;
   d.mx_gns = p->mx_gns;
+  d.mx_bsyn = p->mx_bsyn;
   d.mx_s0 = p->mx_s0;
   d.mx_abort = p->mx_abort;
   d.mx_ana_units = p->mx_ana_units;
   d.mx_syn_units = p->mx_syn_units;
-  SLE_CUDA(cudaFuncSetAttribute(k_ana_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
-  SLE_CUDA(cudaFuncSetAttribute(k_syn_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
+  d.mx_syn_seg = p->mx_syn_seg;
+  d.mx_tab_ana = p->mx_tab_ana;
+  d.mx_tab_syn = p->mx_tab_syn;
+  k_tab_ana<<<p->n_ana_units, 256>>>(d, p->mx_tab_ana);
+  k_tab_syn<<<p->n_syn_units, 128>>>(d, p->mx_tab_syn);
+  SLE_CUDA(cudaGetLastError());
+  SLE_CUDA(cudaDeviceSynchronize());
+  // TMA maps of X: dims (4 nm floats, nh latitudes, MX_MAXF fields), boxes (4, 32, 8 | 16 | 32)
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return SLE_ERR_CUDA;
+  }
+  for (int zi = 0; zi < 3; ++zi) {
+    const cuuint64_t dims[3] = {(cuuint64_t)4 * d.nm, (cuuint64_t)d.nh, (cuuint64_t)MX_MAXF};
+    const cuuint64_t strides[2] = {(cuuint64_t)16 * d.nm, (cuuint64_t)16 * d.nm * d.nh};
+    const cuuint32_t box[3] = {4, (cuuint32_t)KC, (cuuint32_t)ZBOX[zi]};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(reinterpret_cast<CUtensorMap*>(p->mx_tmap[zi]), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                           p->mx_xf, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+      return SLE_ERR_CUDA;
+    }
+  }
+  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
+  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
 #define SLE_ATTR_MX(NN)                                                                                        \
   do {                                                                                                         \
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_fft_smem(d))); \
@@ -948,8 +948,10 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXF)
 #undef SLE_LAUNCH_MXF
   prof_end(t0, st);
+  const int zi = (a.nf <= ZBOX[0]) ? 0 : (a.nf <= ZBOX[1]) ? 1 : 2;
+  const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[zi]);
   ProfToken t1 = prof_begin(PROF_LEG_ANA, a.nf, st);
-  k_ana_tc<<<p->n_ana_units, MX_THREADS, MX_SMEM, st>>>(d, a, status);
+  k_leg_tc<false><<<p->n_ana_units, TC_THREADS, MX_SMEM, st>>>(d, a, status, *map, ZBOX[zi]);
   prof_end(t1, st);
   note_launch(2);
   SLE_CUDA(cudaGetLastError());
@@ -962,15 +964,17 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_
   if (a.ncols == 0) a.ncols = mx_cols(a.nf);
   SLE_TRY(mx_check_args(a, "mixed synthesis"));
   const ShtDev& d = p->d;
+  const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[0]);
   ProfToken t0 = prof_begin(PROF_LEG_SYN, a.nf, st);
-  k_syn_tc<<<p->n_syn_units, MX_THREADS, MX_SMEM, st>>>(d, a, status);
+  k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
+  k_leg_tc<true><<<p->n_syn_units, TC_THREADS, MX_SMEM, st>>>(d, a, status, *map, 0);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
 #define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(NN), mx_fft_smem(d), st>>>(d, a)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXU)
 #undef SLE_LAUNCH_MXU
   prof_end(t1, st);
-  note_launch(2);
+  note_launch(3);
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
 }

@@ -48,7 +48,7 @@ struct Scal {
   double K00;
   int numiter, converged, status, gr_nacc, gr_changed, gr_reguess, gr_ice_an, done;
   unsigned int nd;
-  unsigned int pad1;
+  int cs_changed;        // C* (hence tO) changed in this iteration's refresh
   double diag[5];        // slc_ocn00, c00, slc_b00, cst00 (real parts), ice00
   // rotation
   double il[9], mm[3], lam[18];
@@ -504,7 +504,10 @@ __global__ void k_b18(Dev D) {
   SLOT_OR_RETURN();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef) return;
-  if (i == 0) sc->gr_changed = 0;  // the previous iteration's grounded-mask change is consumed
+  if (i == 0) {
+    sc->gr_changed = 0;  // the previous iteration's mask changes are consumed
+    sc->cs_changed = 0;
+  }
   const int l = D.lidx[i];
   const double2 a = D.sp(S_DI, b)[i], bb = D.sp(S_P_OCEAN, b)[i], c = D.sp(S_LOAD, b)[i];
   const double2 v = D.sp(S_VISC, b)[i];
@@ -667,6 +670,10 @@ __global__ void k_refresh2(Dev D) {
   }
   const double2 cx = ld2(D.g(G_CXY, b), h), ti = ld2(D.g(G_TINIT, b), h), c0 = ld2(D.g(G_CSTAR0, b), h);
   const double c_0 = __dmul_rn(cx.x, bt.x), c_1 = __dmul_rn(cx.y, bt.y);
+  // C* and tO = T0 (C* - C*0) only change where a cell of C* flips; without a flip their
+  // re-analyses are skipped (the inputs, hence the spectra, are bit-identical to the last ones)
+  const double2 prev = ld2(D.g(G_CSTAR, b), h);
+  if (prev.x != c_0 || prev.y != c_1) sc->cs_changed = 1;
   st2(D.g(G_CSTAR, b), h, c_0, c_1);
   st2(D.g(G_TO, b), h, __dmul_rn(ti.x, __dsub_rn(c_0, c0.x)), __dmul_rn(ti.y, __dsub_rn(c_1, c0.y)));
 }
@@ -1382,8 +1389,8 @@ int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
   for (int b = 0; b < nslot; ++b) {
     Scal* sb = s->sc + b;
     s->f_ana_refresh.push_back(fspec(D.g(G_ICESTAR, b), D.sp(S_ICELM, b), &sb->converged, &sb->gr_changed));
-    s->f_ana_refresh.push_back(fspec(D.g(G_CSTAR, b), D.sp(S_CSTARLM, b), &sb->converged));
-    s->f_ana_refresh.push_back(fspec(D.g(G_TO, b), D.sp(S_TOLM, b), &sb->converged));
+    s->f_ana_refresh.push_back(fspec(D.g(G_CSTAR, b), D.sp(S_CSTARLM, b), &sb->converged, &sb->cs_changed));
+    s->f_ana_refresh.push_back(fspec(D.g(G_TO, b), D.sp(S_TOLM, b), &sb->converged, &sb->cs_changed));
   }
   // SLEVOLVE_B200_HOST_LOOP=1 drives the inner loop from the host (same kernels; used to profile
   // the loop body, whose kernels profilers do not report inside conditional graph nodes)
