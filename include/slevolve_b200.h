@@ -167,6 +167,13 @@ int sle_solver_step(sle_solver* s, const double* ice, int on_device, double dt_y
                     sle_step_info* info);
 /* copy one output of the last step; dst is host or device memory. */
 int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device);
+/* Cross-pass warm start, reuse="warm" (solver_opt.py:400-403, 514-528, 932-947): a store in
+ * device memory kept by the caller across solves of the same ice history (outer iterations,
+ * run_outer.py).  ds_store: [capacity][ncoef] complex128 (packed), 16-byte aligned; mask_store:
+ * [capacity][nlat*nlon] bytes.  Step k (1-based, k <= capacity) records its converged load
+ * increment and ocean function at entry k-1; when k <= valid (entries of an earlier pass) the step
+ * first starts from them instead of the eustatic / extrapolated guess.  ds_store = NULL: off. */
+int sle_solver_set_reuse(sle_solver* s, void* ds_store, void* mask_store, int capacity, int valid);
 /* the solver's own CUDA stream (as void*) */
 int sle_solver_stream(sle_solver* s, void** stream);
 
@@ -188,8 +195,10 @@ int sle_batch_destroy(sle_batch* b);
 int sle_batch_load(sle_batch* b, int slot, const sle_earth* earth, double dt_years, const double* topo0,
                    const double* ice0, int on_device, double* ocean_area0, double* oceanBeta_area0,
                    double* ice_volume0);
-/* The slot no longer steps (its memory is reused by the next load). */
+/* The slot no longer steps (its memory is reused by the next load; its reuse store is dropped). */
 int sle_batch_release(sle_batch* b, int slot);
+/* reuse store of a slot, as sle_solver_set_reuse; kept across sle_batch_load of the slot */
+int sle_batch_set_reuse(sle_batch* b, int slot, void* ds_store, void* mask_store, int capacity, int valid);
 /* One step of every slot with ice[slot] != NULL (ice: array of nslots grid pointers).
  * dt_years: NULL, or nslots values (> 0 changes that slot's step length).  info: nslots records,
  * filled for the slots that stepped.  Returns SLE_OK, or the status of the first slot that failed

@@ -91,6 +91,8 @@ _SIGS = {
     "sle_batch_load": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(SleEarth), C.c_double, C.c_void_p,
                                  C.c_void_p, C.c_int, _DP, _DP, _DP]),
     "sle_batch_release": (C.c_int, [C.c_void_p, C.c_int]),
+    "sle_batch_set_reuse": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "sle_solver_set_reuse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
     "sle_batch_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "sle_batch_get": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),
     "sle_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),

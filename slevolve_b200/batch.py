@@ -94,11 +94,13 @@ class SolverBatch:
         returns (ocean_area0, oceanBeta_area0, ice_volume0)."""
         earth, keep = earth_struct(love, self.lmax, self.p)
         a, b, v = C.c_double(), C.c_double(), C.c_double()
-        if _is_cuda_tensor(topo0):
+        if _is_cuda_tensor(topo0) or _is_cuda_tensor(ice0):
             import torch
 
-            t0 = topo0.to(torch.float64).contiguous()
-            i0 = ice0.to(torch.float64).contiguous()
+            t0 = torch.as_tensor(topo0, dtype=torch.float64, device="cuda").contiguous()
+            i0 = torch.as_tensor(ice0, dtype=torch.float64, device="cuda").contiguous()
+            if tuple(t0.shape) != (self.nlat, self.nlon) or tuple(i0.shape) != tuple(t0.shape):
+                raise ValueError(f"grids must be {(self.nlat, self.nlon)}")
             torch.cuda.current_stream().synchronize()
             ptrs, on_dev = (t0.data_ptr(), i0.data_ptr()), 1
         else:
@@ -114,6 +116,17 @@ class SolverBatch:
         self.loaded[slot] = True
         self.area0[slot] = (a.value, b.value, v.value)
         return self.area0[slot]
+
+    def set_reuse(self, slot, store, valid=None):
+        """Attach a ``ReuseStore`` (warm start across passes, reuse="warm") to `slot`; entries
+        0 .. valid-1 (default: all recorded ones) hold an earlier pass.  None detaches."""
+        if store is None:
+            _lib.check(self._L.sle_batch_set_reuse(self._h, int(slot), None, None, 0, 0), "sle_batch_set_reuse")
+            return
+        ds, mask = store.pointers()
+        v = store.recorded if valid is None else int(valid)
+        _lib.check(self._L.sle_batch_set_reuse(self._h, int(slot), ds, mask, store.capacity, min(v, store.capacity)),
+                   "sle_batch_set_reuse")
 
     def release(self, slot):
         _lib.check(self._L.sle_batch_release(self._h, int(slot)), "sle_batch_release")

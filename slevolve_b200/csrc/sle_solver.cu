@@ -66,6 +66,12 @@ struct SlotStep {
   int mode;     // first guess: 0 eustatic, 1 extrap uniform, 2 extrap variable
   int hsel;     // which extrap history buffer holds the most recent load increment
   double c1, c2;
+  // cross-pass warm start (solver_opt.py:400-403, 514-528, 932-947): this step's entry of the
+  // slot's reuse store, read before the step (null = no entry yet) and written at its end
+  const double2* warm_ds;          // converged load increment of this step, previous pass
+  const unsigned char* warm_mask;  // converged ocean function of this step, previous pass
+  double2* rec_ds;                 // where this pass's converged increment goes
+  unsigned char* rec_mask;         // where this pass's converged ocean function goes
 };
 
 enum GridId {
@@ -359,8 +365,14 @@ __global__ void k_ice_grid(Dev D) {
   SLOT_OR_RETURN();
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h >= D.ng) return;
-  const double2 v = ld2(D.g(G_ICE, b), h), tp = ld2(D.g(G_TOPO_PREV, b), h), cx = ld2(D.g(G_CXY, b), h);
+  const double2 v = ld2(D.g(G_ICE, b), h), tp = ld2(D.g(G_TOPO_PREV, b), h);
+  double2 cx = ld2(D.g(G_CXY, b), h);
   const double2 ti = ld2(D.g(G_TINIT, b), h), c0 = ld2(D.g(G_CSTAR0, b), h);
+  const unsigned char* wm = D.ss[b].warm_mask;
+  if (wm) {  // warm start: the converged ocean function of this step in the previous pass
+    cx = make_double2(wm[2 * h] ? 1.0 : 0.0, wm[2 * h + 1] ? 1.0 : 0.0);
+    st2(D.g(G_CXY, b), h, cx.x, cx.y);
+  }
   if (!isfinite(v.x) || !isfinite(v.y)) sc->status = SLE_ERR_NONFINITE;
   double is[2], bt[2], c[2], t[2];
   const double vv[2] = {v.x, v.y}, tt[2] = {tp.x, tp.y}, cc[2] = {cx.x, cx.y}, ii[2] = {ti.x, ti.y},
@@ -470,7 +482,9 @@ __global__ void k_pre_spec(Dev D) {
     const double2 pi = D.sp(S_P_ICE, b)[i];
     D.sp(S_DI, b)[i] = make_double2(__dadd_rn(pi.x, d.x), __dadd_rn(pi.y, d.y));
     double2 g;
-    if (ss.mode == 0) {
+    if (ss.warm_ds) {
+      g = ss.warm_ds[i];   // warm start replaces the eustatic / extrapolated guess
+    } else if (ss.mode == 0) {
       g = np_cmul(np_cdiv(cstarlm[i], cstarlm[0]), s00);
     } else if (ss.mode == 1) {
       const double2 u = h1[i], v = h2[i];
@@ -481,7 +495,7 @@ __global__ void k_pre_spec(Dev D) {
                        __dsub_rn(__dmul_rn(u.y, ss.c1), __dmul_rn(ss.c2, v.y)));
     }
     D.sp(S_LOAD, b)[i] = g;
-    if (ss.mode == 0) {
+    if (ss.mode == 0 && !ss.warm_ds) {
       D.sp(S_DSCUR, b)[i] = make_double2(0.0, 0.0);
     } else {
       const double2 p = D.sp(S_P_OCEAN, b)[i];
@@ -774,6 +788,7 @@ __global__ void k_commit(Dev D, int extrap) {
   D.sp(S_P_OCEAN, b)[i] = D.sp(S_DSCUR, b)[i];
   D.sp(S_PREV_ICE, b)[i] = D.sp(S_ICELM, b)[i];
   if (extrap) D.sp(D.ss[b].hsel ? S_HA : S_HB, b)[i] = ld;
+  if (D.ss[b].rec_ds) D.ss[b].rec_ds[i] = ld;
 }
 
 // Post-step topography / ocean function (solver.py:1099-1101) and, for the diag option, the
@@ -790,6 +805,7 @@ __global__ void k_post_grid(Dev D, int diag) {
   const double *deltasl = D.g(G_DELTASL, b), *tinit = D.g(G_TINIT, b), *beta = D.g(G_BETA, b);
   double *topo = D.g(G_TOPO, b), *topo_prev = D.g(G_TOPO_PREV, b), *cxy = D.g(G_CXY, b);
   double *slc = D.g(G_TMP, b), *slcb = D.g(G_TMP3, b), *cstar = D.g(G_TMP4, b);
+  unsigned char* rec_mask = D.ss[b].rec_mask;
   for (int t = threadIdx.x; t < D.nlon / 2; t += blockDim.x) {
     const long long h = row + t;
     const double2 ds = ld2(deltasl, h), ti = ld2(tinit, h), bb = ld2(beta, h);
@@ -810,6 +826,10 @@ __global__ void k_post_grid(Dev D, int diag) {
     st2(topo, h, tp[0], tp[1]);
     st2(topo_prev, h, tp[0], tp[1]);
     st2(cxy, h, o[0], o[1]);
+    if (rec_mask) {
+      rec_mask[2 * h] = o[0] != 0.0;
+      rec_mask[2 * h + 1] = o[1] != 0.0;
+    }
     if (!diag) {
       st2(slc, h, s1[0], s1[1]);
       st2(slcb, h, s2[0], s2[1]);
@@ -894,6 +914,11 @@ namespace {
 
 struct SlotHost {
   int loaded, inited;
+  // reuse store (device): [capacity][ncoef] increments and [capacity][ng] masks; the first
+  // `valid` steps hold entries of an earlier pass
+  double2* rs_ds;
+  unsigned char* rs_mask;
+  int rs_cap, rs_valid;
   int iter, nhist, hsel;
   double dt, dt_cur, dt_hist[2];
   double ocean_area0, oceanBeta_area0, ice_volume0;
@@ -1436,7 +1461,7 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
   }
   if (act.empty()) return SLE_OK;
   // per-slot step parameters
-  for (int b = 0; b < B; ++b) s->hss[b] = SlotStep{0, 0, 0, 0, 0.0, 0.0};
+  for (int b = 0; b < B; ++b) s->hss[b] = SlotStep{0, 0, 0, 0, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr};
   for (int b : act) {
     SlotHost& h = s->slot[b];
     double dt = h.dt;
@@ -1459,6 +1484,15 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
         const double w = (dt0 + dt1) / (dt1 + dt2);
         p.c1 = dt0 / dt1 * (1.0 + w);
         p.c2 = dt0 / dt2 * w;
+      }
+    }
+    if (h.rs_ds && h.iter <= h.rs_cap) {
+      const size_t e = (size_t)(h.iter - 1);
+      p.rec_ds = h.rs_ds + e * nc;
+      p.rec_mask = h.rs_mask + e * ng;
+      if (h.iter <= h.rs_valid) {
+        p.warm_ds = p.rec_ds;
+        p.warm_mask = p.rec_mask;
       }
     }
     SLE_TRY(upload(D.g(G_ICE, b), ice[b], sizeof(double) * ng, on_device, st));
@@ -1676,6 +1710,32 @@ extern "C" int sle_batch_release(sle_batch* b, int slot) {
   SLE_TRY(check_slot(b, slot, "sle_batch_release"));
   b->slot[slot].loaded = 0;
   b->slot[slot].inited = 0;
+  b->slot[slot].rs_ds = nullptr;
+  b->slot[slot].rs_mask = nullptr;
+  b->slot[slot].rs_cap = b->slot[slot].rs_valid = 0;
+  return SLE_OK;
+}
+
+extern "C" int sle_batch_set_reuse(sle_batch* b, int slot, void* ds_store, void* mask_store, int capacity,
+                                   int valid) {
+  if (!b) {
+    set_error("sle_batch_set_reuse: NULL batch");
+    return SLE_ERR_BAD_ARG;
+  }
+  SLE_TRY(check_slot(b, slot, "sle_batch_set_reuse"));
+  if (ds_store && (!mask_store || capacity < 1 || valid < 0 || valid > capacity)) {
+    set_error("sle_batch_set_reuse: need both stores, capacity >= 1 and 0 <= valid <= capacity");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (ds_store && (reinterpret_cast<uintptr_t>(ds_store) & 15)) {
+    set_error("sle_batch_set_reuse: the increment store must be 16-byte aligned");
+    return SLE_ERR_BAD_ARG;
+  }
+  SlotHost& h = b->slot[slot];
+  h.rs_ds = reinterpret_cast<double2*>(ds_store);
+  h.rs_mask = reinterpret_cast<unsigned char*>(mask_store);
+  h.rs_cap = ds_store ? capacity : 0;
+  h.rs_valid = ds_store ? valid : 0;
   return SLE_OK;
 }
 
@@ -1786,6 +1846,14 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
   const int rc = batch_step(s->b, ices, on_device, dts, &o);
   if (info) *info = o;
   return rc;
+}
+
+extern "C" int sle_solver_set_reuse(sle_solver* s, void* ds_store, void* mask_store, int capacity, int valid) {
+  if (!s) {
+    set_error("sle_solver_set_reuse: NULL solver");
+    return SLE_ERR_BAD_ARG;
+  }
+  return sle_batch_set_reuse(s->b, 0, ds_store, mask_store, capacity, valid);
 }
 
 extern "C" int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device) {

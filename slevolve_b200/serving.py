@@ -1,0 +1,272 @@
+"""Serving loop: continuous batching of sea-level solves on one GPU.
+
+A request is one forward solve (an Earth model, a truncation degree L, a topography, an ice
+history, a step count and a step length) or an ice-age outer-iteration request: several forward
+passes over the same ice history, each starting from the initial topography updated by the
+reference's Picard rule ``T0 <- T0 - (predicted present topography - observed)``
+(SLEvolve python/slevolve/run_outer.py:243-273), warm-started from the previous pass's
+converged state (``reuse="warm"``, solver_opt.py:400-403, 514-528, 932-947).
+
+The server keeps one slot batch (``SolverBatch``) per truncation degree.  Each batch has its own
+host thread: between two of its batch steps it retires finished solves, admits queued requests
+while a slot is free and the device-memory budget holds their footprint (solver state of one
+slot plus, for outer requests, the reuse store), and then advances every admitted solve by one
+time step in one batched step.  Batches of different degrees run concurrently on their own CUDA
+streams, so their kernels overlap on the device.  All solver state stays on the device from
+admission to completion; the ice of each step is generated on the device.
+
+A solve's result does not depend on what else is in its batch (per-slot reductions in a fixed
+order, per-field tensor-core columns), so a request gives the same answer alone and in the mix.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+import threading
+import time
+from typing import Callable, Optional
+
+import numpy as np
+
+from .batch import SolverBatch, slot_bytes
+from .reuse import ReuseStore
+
+
+@dataclasses.dataclass
+class Request:
+    """One solve.  ``ice(k)`` returns the ice grid of step k (a CUDA float64 tensor or NumPy
+    array of the request's grid); ``outer_passes > 1`` makes it an outer-iteration request whose
+    observed present topography is ``obs`` (default: ``topo``)."""
+
+    rid: int
+    lmax: int
+    love: object
+    topo: np.ndarray
+    ice: Callable[[int], object]
+    nsteps: int
+    dt: float
+    arrival: float = 0.0
+    outer_passes: int = 1
+    obs: Optional[np.ndarray] = None
+    # filled in by the server
+    t_admit: float = math.nan
+    t_done: float = math.nan
+    numiter: int = 0
+    passes_done: int = 0
+    warm_steps: int = 0
+    result: dict = dataclasses.field(default_factory=dict)
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.arrival
+
+
+def footprint(req: Request, max_modes=8) -> int:
+    """Device bytes a request holds while admitted (admission unit)."""
+    n = req.lmax + 1
+    b = slot_bytes(n, 2 * n, req.lmax, max_modes)
+    if req.outer_passes > 1:
+        nc = n * (n + 1) // 2
+        b += req.nsteps * (16 * nc + n * 2 * n)
+    return b
+
+
+class _Running:
+    def __init__(self, req, slot):
+        self.req = req
+        self.slot = slot
+        self.k = 0          # steps done in the current pass
+        self.store = None   # ReuseStore of an outer request
+        self.T0 = None      # current initial topography (device) of an outer request
+        self.obs = None
+
+
+class Server:
+    """groups: {lmax: slots}.  budget_bytes: device memory the admitted requests may hold."""
+
+    def __init__(self, groups, precision="mixed", budget_bytes=None, max_modes=8, opt=("dsl", "diag"),
+                 inner="extrap", record=("deltasl", "tgrid")):
+        self.precision = precision
+        self.max_modes = max_modes
+        self.record = tuple(record)
+        self.batches = {int(L): SolverBatch(L + 1, 2 * (L + 1), L, int(n), max_modes=max_modes,
+                                            precision=precision, opt=opt, inner=inner)
+                        for L, n in groups.items()}
+        self.budget = budget_bytes if budget_bytes is not None else float("inf")
+        self.used = 0
+        self.peak_used = 0
+        self.lock = threading.Lock()
+        self.queue = {L: [] for L in self.batches}
+        self.done = []
+        self.steps = {L: 0 for L in self.batches}        # member-steps executed per group
+        self.batch_steps = {L: 0 for L in self.batches}  # batched steps per group
+
+    # ---------------------------------------------------------------- helpers
+    def _admit(self, L, running, now):
+        bt = self.batches[L]
+        free = [s for s in range(bt.nslots) if s not in running]
+        q = self.queue[L]
+        while free and q and q[0].arrival <= now:
+            req = q[0]
+            fp = footprint(req, self.max_modes)
+            with self.lock:
+                if self.used + fp > self.budget:
+                    return
+                self.used += fp
+                self.peak_used = max(self.peak_used, self.used)
+            q.pop(0)
+            slot = free.pop(0)
+            run = _Running(req, slot)
+            req.t_admit = time.perf_counter() - self._t0
+            if req.outer_passes > 1:
+                import torch
+
+                n = req.lmax + 1
+                run.store = ReuseStore(n * (n + 1) // 2, n * 2 * n, capacity=req.nsteps)
+                run.T0 = torch.as_tensor(np.ascontiguousarray(req.topo), dtype=torch.float64, device="cuda")
+                obs = req.obs if req.obs is not None else req.topo
+                run.obs = torch.as_tensor(np.ascontiguousarray(obs), dtype=torch.float64, device="cuda")
+            self._load(bt, run)
+            running[slot] = run
+
+    def _load(self, bt, run):
+        req = run.req
+        topo = run.T0 if run.T0 is not None else req.topo
+        bt.load(run.slot, req.love, topo, req.ice(0), req.dt)
+        if run.store is not None:
+            bt.set_reuse(run.slot, run.store, valid=run.store.recorded)
+        run.k = 0
+
+    def _finish_pass(self, L, bt, run, running):
+        """End of a forward pass: next pass (outer request) or completion."""
+        req = run.req
+        req.passes_done += 1
+        if run.store is not None:
+            run.store.recorded = max(run.store.recorded, run.k)
+        if req.passes_done < req.outer_passes:
+            import torch
+
+            pred = torch.empty_like(run.T0)
+            bt.get(run.slot, "tgrid", out=pred)
+            run.T0 = run.T0 - (pred - run.obs)   # Picard update of the initial topography
+            self._load(bt, run)
+            return
+        for f in self.record:
+            req.result[f] = bt.get(run.slot, f).copy()
+        if run.T0 is not None:
+            req.result["T0"] = run.T0.cpu().numpy()
+        req.t_done = time.perf_counter() - self._t0
+        bt.release(run.slot)
+        del running[run.slot]
+        with self.lock:
+            self.used -= footprint(req, self.max_modes)
+            self.done.append(req)
+
+    def _group_loop(self, L):
+        bt = self.batches[L]
+        running = {}
+        while True:
+            now = time.perf_counter() - self._t0
+            self._admit(L, running, now)
+            if not running:
+                q = self.queue[L]
+                if not q:
+                    return
+                time.sleep(min(0.002, max(0.0, q[0].arrival - now)))
+                continue
+            ices = {s: r.req.ice(r.k + 1) for s, r in running.items()}
+            infos = bt.step(ices)
+            self.batch_steps[L] += 1
+            self.steps[L] += len(ices)
+            for s, info in infos.items():
+                r = running[s]
+                r.k += 1
+                r.req.numiter += info["numiter"]
+                if r.store is not None and r.req.passes_done > 0 and r.k <= r.store.recorded:
+                    r.req.warm_steps += 1
+            for s in list(running):
+                r = running[s]
+                if r.k >= r.req.nsteps:
+                    self._finish_pass(L, bt, r, running)
+
+    # -------------------------------------------------------------------- API
+    def run(self, requests):
+        """Serve `requests` (arrival times in seconds from now); returns them with their
+        admission / completion times, iteration counts and recorded results."""
+        for r in sorted(requests, key=lambda r: (r.arrival, r.rid)):
+            if r.lmax not in self.batches:
+                raise ValueError(f"no slot batch for lmax {r.lmax}")
+            self.queue[r.lmax].append(r)
+        self._t0 = time.perf_counter()
+        threads = [threading.Thread(target=self._group_loop, args=(L,), daemon=True) for L in self.batches]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        self.wall = time.perf_counter() - self._t0
+        return requests
+
+    def stats(self, requests):
+        lat = np.array([r.latency for r in requests])
+        steps = sum(self.steps.values())
+        return {"requests": len(requests), "wall_s": self.wall, "member_steps": steps,
+                "member_steps_per_s": steps / self.wall,
+                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                "peak_bytes": int(self.peak_used), "budget_bytes": self.budget,
+                "batch_steps": dict(self.batch_steps)}
+
+
+# ------------------------------------------------------------- synthetic members
+class MemberFactory:
+    """Seeded members of the uneven ensembles: L, Earth model (relaxation times scaled by a
+    factor log-uniform in [0.3, 3]), topography from the seeded generator of the grid, ice from
+    the two-cap melt history or the three-sheet 100-kyr sawtooth scaled by U[0.5, 1.5]."""
+
+    def __init__(self, seed=20261206):
+        self.rng = np.random.default_rng(seed)
+        self._grid = {}
+
+    def grid(self, L):
+        if L not in self._grid:
+            import torch
+
+            from . import make_sht
+            from .synthetic import (SHEETS_C2, angular_distance, grid_latlon, random_topography,
+                                    vialov)
+
+            n = L + 1
+            sht = make_sht("cuda", n, 2 * n, L)
+            topo = random_topography(sht, 20261203 + L)
+            LAT, LON = grid_latlon(sht.gaulats, 2 * n)
+            cap = (vialov(angular_distance(LAT, LON, -90.0, 0.0), 15.0)
+                   + vialov(angular_distance(LAT, LON, 56.0, 132.0), 15.0)) * (topo > -500.0)
+            nh = np.zeros_like(topo)
+            for la, lo, R in SHEETS_C2:
+                nh = np.maximum(nh, vialov(angular_distance(LAT, LON, la, lo), R))
+            self._grid[L] = (topo, torch.as_tensor(cap, device="cuda"), torch.as_tensor(nh, device="cuda"))
+        return self._grid[L]
+
+    def make(self, rid, L, nsteps, arrival=0.0, outer_passes=1, kind=None):
+        import torch
+
+        from .love import SyntheticEarth
+        from .synthetic import sawtooth
+
+        topo, cap, nh = self.grid(L)
+        f = float(np.exp(self.rng.uniform(np.log(0.3), np.log(3.0))))
+        amp = float(self.rng.uniform(0.5, 1.5))
+        kind = kind or ("melt" if self.rng.uniform() < 0.5 else "sawtooth")
+        love = SyntheticEarth(L, 8, 20261203 + rid, relax_scale=f)
+        if kind == "melt":
+            dt = 1.0
+
+            def ice(k, amp=amp, n=nsteps, shape=cap):
+                return torch.round(amp * (3000.0 * (1.0 - k / n)) * shape * 1000.0) / 1000.0
+        else:
+            dt = 200.0
+
+            def ice(k, amp=amp, shape=nh):
+                return torch.round(amp * (3500.0 * float(sawtooth(k * 200.0 / 1000.0))) * shape * 1000.0) / 1000.0
+        return Request(rid=rid, lmax=L, love=love, topo=topo, ice=ice, nsteps=nsteps, dt=dt, arrival=arrival,
+                       outer_passes=outer_passes)

@@ -11,7 +11,7 @@ reference copies them for that reason).
 
 Branches of the reference that this build does not provide raise ``NotImplementedError``: the
 second-order ramp placement, the axial-rotation options, Anderson mixing, analytic rates, the
-horizontal read-out and cross-pass reuse.  The ``raw`` option needs a raw-mode backend and raises
+horizontal read-out and the reuse variants other than ``"warm"``.  The ``raw`` option needs a raw-mode backend and raises
 ``ValueError`` as in the reference (solver_opt.py:299-301).
 """
 
@@ -144,8 +144,8 @@ class SeaLevelSolver:
             raise NotImplementedError("Anderson mixing is not provided by the GPU solver")
         if reuse not in ("off", "warm", "warm+ice", "warm+corr", "warm+corr2"):
             raise ValueError(f"reuse must be off|warm|warm+ice|warm+corr|warm+corr2, got {reuse!r}")
-        if reuse != "off":
-            raise NotImplementedError("cross-pass reuse is not provided by the GPU solver")
+        if reuse not in ("off", "warm"):
+            raise NotImplementedError(f"reuse={reuse!r} is not provided by the GPU solver (off, warm are)")
         unknown = opt - {"raw", "diag", "dsl", "numba", "sums"}
         if unknown:
             raise ValueError(f"unknown opt {sorted(unknown)}")
@@ -175,6 +175,7 @@ class SeaLevelSolver:
         self.inner = inner
         self.reuse = reuse
         self.reuse_store = reuse_store if reuse_store is not None else {}
+        self.reuse_stats = {"warm_steps": 0, "ice_reused": 0, "ice_recomputed": 0}
         self.inner_stats = {"mixed": 0, "plain": 0, "fallback": 0, "singular": 0,
                             "mask_refresh": 0, "frozen_iters": 0}
         self.gr_counts = {"reguess": 0, "ice_analyses": 0}
@@ -256,12 +257,34 @@ class SeaLevelSolver:
             self.dt = float(dt)
 
     # ------------------------------------------------------------------ step
+    def _reuse_register(self, k):
+        """Device reuse store for step k (reuse="warm"): kept in ``reuse_store`` across the
+        solvers of successive outer passes."""
+        from .reuse import ReuseStore
+
+        st = self.reuse_store.get("_device_store")
+        if st is None:
+            nc = (self.nl * (self.nl + 1)) // 2
+            st = self.reuse_store["_device_store"] = ReuseStore(nc, self.nlat * self.nlon)
+        if k == 1:
+            self._reuse_valid = st.recorded   # entries of the previous pass
+        st.ensure(k)
+        ds, mask = st.pointers()
+        _lib.check(self._L.sle_solver_set_reuse(self._h, ds, mask, st.capacity, self._reuse_valid),
+                   "sle_solver_set_reuse")
+        return st
+
     def step_device(self, ice_ptr, on_device, dt=None):
         """One step from a raw pointer (host or device); returns the step info record."""
         self.set_step_dt(dt)
+        st = self._reuse_register(self.iter + 1) if self.reuse == "warm" else None
         rc = self._L.sle_solver_step(self._h, C.c_void_p(ice_ptr), int(on_device),
                                      float(self.dt), C.byref(self._info))
         _lib.check(rc, "sle_solver_step")
+        if st is not None:
+            if self._info.iter <= self._reuse_valid:
+                self.reuse_stats["warm_steps"] += 1
+            st.recorded = max(st.recorded, self._info.iter)
         self.iter = self._info.iter
         self.gr_counts["reguess"] += self._info.gr_reguess
         self.gr_counts["ice_analyses"] += self._info.gr_ice_analyses

@@ -59,6 +59,8 @@ def test_solver_rejects_unprovided_options():
         SeaLevelSolver(None, love, topo, ice, norder=15, axial_rotation="deg2")
     with pytest.raises(NotImplementedError):
         OptSeaLevelSolver(None, love, topo, ice, norder=15, inner="anderson")
+    with pytest.raises(NotImplementedError):
+        OptSeaLevelSolver(None, love, topo, ice, norder=15, reuse="warm+corr")
     with pytest.raises(ValueError):
         OptSeaLevelSolver(None, love, topo, ice, norder=15, inner="bogus")
     with pytest.raises(ValueError):

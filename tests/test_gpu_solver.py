@@ -167,3 +167,33 @@ def test_nonconvergence_cap():
     ice1[2:5, 20:24] = 100.0
     with pytest.raises(RuntimeError, match="failed to converge"):
         slv.step(ice1)
+
+
+def test_outer_passes_with_warm_reuse_against_oracle():
+    """Three outer (ice-age) passes over the c0 shape with the reference's Picard update of the
+    initial topography (run_outer.py) and reuse="warm": every step of every pass against the
+    CPU oracle driven the same way (same iteration counts, topography within 1e-9 m)."""
+    from slevolve_b200 import OptSeaLevelSolver
+    from slevolve_b200.synthetic import case_c0
+    from oracle.sht import OracleSHT
+    from oracle.solver import OracleSolver
+
+    osht = OracleSHT(64, 128, 63)
+    case = case_c0(osht, nsteps=12)
+    obs = case.topo.copy()
+    T_gpu, T_orc = case.topo.copy(), case.topo.copy()
+    store_gpu, store_orc = {}, {}
+    warm = 0
+    for it in range(3):
+        kw = dict(norder=63, dt=1.0, opt={"dsl"}, inner="extrap", reuse="warm")
+        slv = OptSeaLevelSolver(None, case.love, T_gpu, case.ice(0), reuse_store=store_gpu, **kw)
+        orc = OracleSolver(osht, case.love, T_orc, case.ice(0), reuse_store=store_orc, **kw)
+        for k in range(1, 13):
+            r = slv.step(case.ice(k))
+            o = orc.step(case.ice(k))
+            assert r["numiter"] == o["numiter"], (it, k)
+            assert np.abs(r["tgrid"] - o["tgrid"]).max() <= TOL_M, (it, k)
+        warm += slv.reuse_stats["warm_steps"]
+        T_gpu = T_gpu - (np.array(r["tgrid"]) - obs)
+        T_orc = T_orc - (o["tgrid"] - obs)
+    assert warm == 24   # passes 2 and 3 start every step from the stored state
