@@ -213,8 +213,10 @@ int sle_batch_info(const sle_batch* b, int* nslots, int* max_modes, long long* d
 
 /* ------------------------------------------------------- measurement */
 /* Kernel classes timed by sle_prof_*: 0 row FFT + fold, 1 Legendre analysis, 2 Legendre
- * synthesis, 3 inverse FFT + unfold, 4 modal-state advance.  Timing is off by default; when on,
- * each launch of these classes is bracketed by CUDA events on its own stream. */
+ * synthesis, 3 inverse FFT + unfold, 4 modal-state advance, 5 the Legendre analysis of the inner
+ * iteration's rO field (every stepping slot's field active; class 1 has the other analyses).
+ * Timing is off by default; when on, each launch of these classes is bracketed by CUDA events on
+ * its own stream. */
 int sle_prof_enable(int on);
 int sle_prof_collect(void);        /* wait for recorded events and accumulate */
 int sle_prof_reset(void);          /* also resets the launch counter */

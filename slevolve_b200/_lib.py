@@ -106,7 +106,7 @@ _SIGS = {
     "sle_probe_fp64_tflops": (C.c_int, [_DP]),
 }
 
-PROF_FFT, PROF_LEG_ANA, PROF_LEG_SYN, PROF_IFFT, PROF_ADVANCE = range(5)
+PROF_FFT, PROF_LEG_ANA, PROF_LEG_SYN, PROF_IFFT, PROF_ADVANCE, PROF_ANA_STEP = range(6)
 PREC_FP64, PREC_MIXED = 0, 1
 PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
 

@@ -142,8 +142,9 @@ struct sle_sht {
 
 namespace sle {
 // Launch accounting / per-kernel event timing (sle_prof.cu).
+// PROF_ANA_STEP: the Legendre analysis of the inner iteration's rO (every stepping field active).
 enum ProfClass { PROF_FFT = 0, PROF_LEG_ANA = 1, PROF_LEG_SYN = 2, PROF_IFFT = 3, PROF_ADVANCE = 4,
-                 PROF_NCLS = 5 };
+                 PROF_ANA_STEP = 5, PROF_NCLS = 6 };
 struct ProfToken {
   int cls;
   double units;
@@ -156,13 +157,14 @@ void prof_end(const ProfToken& t, cudaStream_t st);
 
 // Transforms of a list of fields (packed spectra), launched in groups of MAXF (FP64) or
 // MX_MAXF (mixed) fields with the precision of the plan (sle_sht.cu).
-int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st);
+int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st, int prof_cls = PROF_LEG_ANA);
 int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st);
 int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t st);
 // Mixed-precision transforms (sle_mx.cu).  `status` (device int, may be null) receives
 // SLE_ERR_TIMEOUT if a tensor-core kernel gave up waiting.
 int sht_mx_prepare(sle_sht* plan);
-int sht_mx_analysis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st);
+int sht_mx_analysis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st,
+                    int prof_cls = PROF_LEG_ANA);
 int sht_mx_synthesis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st);
 int sht_mx_abort_flag(sle_sht* plan, int* flag);
 int mx_cols(int nf);

@@ -937,7 +937,7 @@ static int mx_check_args(const MxFieldArgs& a, const char* what) {
 
 int mx_cols(int nf) { return std::max(16, (2 * nf + 15) / 16 * 16); }
 
-int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t st) {
+int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t st, int prof_cls) {
   SLE_TRY(sht_mx_prepare(p));
   MxFieldArgs a = a0;
   if (a.ncols == 0) a.ncols = mx_cols(a.nf);
@@ -950,7 +950,7 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t
   prof_end(t0, st);
   const int zi = (a.nf <= ZBOX[0]) ? 0 : (a.nf <= ZBOX[1]) ? 1 : 2;
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[zi]);
-  ProfToken t1 = prof_begin(PROF_LEG_ANA, a.nf, st);
+  ProfToken t1 = prof_begin(prof_cls, a.nf, st);
   k_leg_tc<false><<<p->n_ana_units, TC_THREADS, MX_SMEM, st>>>(d, a, status, *map, ZBOX[zi]);
   prof_end(t1, st);
   note_launch(2);

@@ -572,7 +572,7 @@ static int syn_threads(const ShtDev& d) { return 32 * ((d.ngrp + 1) / 2); }
 static size_t syn_smem(const ShtDev& d) { return (size_t)3 * d.nm * sizeof(double); }
 
 // One FP64 launch group (1..MAXF fields).
-static int fp64_analysis(sle_sht* plan, const FieldSpec* fs, int nf, cudaStream_t st) {
+static int fp64_analysis(sle_sht* plan, const FieldSpec* fs, int nf, cudaStream_t st, int prof_cls) {
   ShtDev d = plan->d;
   GridPtrs g{};
   SpecPtrs o{};
@@ -589,7 +589,7 @@ static int fp64_analysis(sle_sht* plan, const FieldSpec* fs, int nf, cudaStream_
   prof_end(t0, st);
   const int warps_per_block = ANA_WARPS;
   dim3 grid((d.nseg + warps_per_block - 1) / warps_per_block, nf);
-  ProfToken t1 = prof_begin(PROF_LEG_ANA, nf, st);
+  ProfToken t1 = prof_begin(prof_cls, nf, st);
   k_leg_ana<<<grid, 32 * warps_per_block, 0, st>>>(d, o);
   prof_end(t1, st);
   note_launch(2);
@@ -637,7 +637,7 @@ static MxFieldArgs mx_args(const FieldSpec* fs, int nf) {
   return a;
 }
 
-int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st) {
+int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st, int prof_cls) {
   if (n < 1) return SLE_OK;
   const bool mx = plan->precision == SLE_PREC_MIXED;
   const int group = mx ? MX_MAXF : MAXF;
@@ -646,9 +646,9 @@ int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st)
   for (int g = 0; g < ngroups; ++g) {
     const int lo = (int)((long long)n * g / ngroups), hi = (int)((long long)n * (g + 1) / ngroups);
     if (mx) {
-      SLE_TRY(sht_mx_analysis(plan, mx_args(f + lo, hi - lo), plan->mx_status, st));
+      SLE_TRY(sht_mx_analysis(plan, mx_args(f + lo, hi - lo), plan->mx_status, st, prof_cls));
     } else {
-      SLE_TRY(fp64_analysis(plan, f + lo, hi - lo, st));
+      SLE_TRY(fp64_analysis(plan, f + lo, hi - lo, st, prof_cls));
     }
   }
   return SLE_OK;

@@ -1052,7 +1052,7 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   note_launch();
   k_b18<<<dim3(nb(nc), B), 256, 0, st>>>(D);
   SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sl.data(), (int)s->f_syn_sl.size(), st));
-  SLE_TRY(sht_analysis_list(s->plan, s->f_ana_ro.data(), (int)s->f_ana_ro.size(), st));
+  SLE_TRY(sht_analysis_list(s->plan, s->f_ana_ro.data(), (int)s->f_ana_ro.size(), st, PROF_ANA_STEP));
   note_launch();
   k_update<<<dim3(nb(nc), B), 256, 0, st>>>(D);
   if (!s->cfg.opt_dsl) {
