@@ -29,14 +29,17 @@ __device__ __forceinline__ V mul_mi(V a, bool inv) {
   return inv ? mkc(-a.y, a.x) : mkc(a.y, -a.x);
 }
 
-// Stockham FFT of length N = nlon/2 on complex rows in shared memory: radix-8 passes while at
-// least 8 points remain per sub-transform, then one radix-4 or radix-2 pass.  A pass of radix R
-// with current sub-transform size Ns maps in[j + r q] (q = N/R, k = j mod Ns) through the
-// twiddles exp(-+2 pi i r k/(Ns R)) and an R-point DFT in registers to
-// out[(j - k) R + k + r Ns].  tw[t] = exp(-2 pi i t / (2 N)) for t < N; larger t use
-// tw[t - N] = -exp(...).
-template <typename V>
-__device__ __forceinline__ void dft8(V (&v)[8], bool inv) {
+// Stockham FFT of length N = nlon/2 on the two complex rows (north, south) of a block, in place
+// in shared memory: radix-8 passes while at least 8 points remain per sub-transform, then one
+// radix-4 or radix-2 pass.  A pass of radix R with current sub-transform size Ns maps
+// in[j + r q] (q = N/R, k = j mod Ns) through the twiddles exp(-+2 pi i r k/(Ns R)) and an
+// R-point DFT in registers to out[(j - k) R + k + r Ns].  Every thread reads its inputs into
+// registers before the block synchronises and overwrites the row, so one buffer of 2N points
+// suffices.  tw[t] = exp(-2 pi i t / (2 N)) for t < N (global memory, read through the
+// read-only cache); larger t use tw[t - N] = -exp(...).  The first pass may read from any
+// source (global rows, a fused pre-processing step) and the last may write to any sink.
+template <bool INV, typename V>
+__device__ __forceinline__ void dft8(V (&v)[8]) {
   using S = typename ScalarOf<V>::type;
   const S h = (S)0.70710678118654752440;  // cos(pi/4)
   V a0 = cadd(v[0], v[4]), a4 = csub(v[0], v[4]);
@@ -44,12 +47,12 @@ __device__ __forceinline__ void dft8(V (&v)[8], bool inv) {
   V a2 = cadd(v[2], v[6]), a6 = csub(v[2], v[6]);
   V a3 = cadd(v[3], v[7]), a7 = csub(v[3], v[7]);
   // a5 *= W, a6 *= W^2, a7 *= W^3 with W = exp(-+2 pi i / 8)
-  const S s = inv ? h : -h;
+  const S s = INV ? h : -h;
   a5 = mkc(h * a5.x - s * a5.y, h * a5.y + s * a5.x);
-  a6 = mul_mi(a6, inv);
+  a6 = mul_mi(a6, INV);
   a7 = mkc(-h * a7.x - s * a7.y, -h * a7.y + s * a7.x);
-  V b0 = cadd(a0, a2), b2 = csub(a0, a2), b1 = cadd(a1, a3), b3 = mul_mi(csub(a1, a3), inv);
-  V b4 = cadd(a4, a6), b6 = csub(a4, a6), b5 = cadd(a5, a7), b7 = mul_mi(csub(a5, a7), inv);
+  V b0 = cadd(a0, a2), b2 = csub(a0, a2), b1 = cadd(a1, a3), b3 = mul_mi(csub(a1, a3), INV);
+  V b4 = cadd(a4, a6), b6 = csub(a4, a6), b5 = cadd(a5, a7), b7 = mul_mi(csub(a5, a7), INV);
   v[0] = cadd(b0, b1);
   v[1] = cadd(b4, b5);
   v[2] = cadd(b2, b3);
@@ -60,60 +63,139 @@ __device__ __forceinline__ void dft8(V (&v)[8], bool inv) {
   v[7] = csub(b6, b7);
 }
 
-// One Stockham pass of radix R on two rows of N points (compile-time sizes: all index
-// arithmetic folds to shifts and masks).  Sub-transform size before the pass: NS.
-template <int N, int R, int NS, bool INV, typename V>
-__device__ __forceinline__ void fft_pass_c(const V* __restrict__ in, V* __restrict__ out,
-                                           const V* __restrict__ tw) {
-  constexpr int Q = N / R;
-  constexpr int TSTEP = 2 * N / (NS * R);
-  for (int idx = threadIdx.x; idx < 2 * Q; idx += blockDim.x) {
-    const int r = idx / Q, j = idx % Q;
-    const int k = j % NS;
-    const V* src = in + r * N;
-    V v[R];
-#pragma unroll
-    for (int u = 0; u < R; ++u) v[u] = src[j + u * Q];
-    if (NS > 1) {
-#pragma unroll
-      for (int u = 1; u < R; ++u) {
-        const int t = u * k * TSTEP;
-        V w = (t < N) ? tw[t] : mkc(-tw[t - N].x, -tw[t - N].y);
-        if (INV) w.y = -w.y;
-        v[u] = cmul(v[u], w);
-      }
-    }
-    if (R == 8) {
-      dft8(reinterpret_cast<V(&)[8]>(v), INV);
-    } else if (R == 4) {
-      const V a0 = cadd(v[0], v[2]), a2 = csub(v[0], v[2]);
-      const V a1 = cadd(v[1], v[3]), a3 = mul_mi(csub(v[1], v[3]), INV);
-      v[0] = cadd(a0, a1);
-      v[1] = cadd(a2, a3);
-      v[2] = csub(a0, a1);
-      v[3] = csub(a2, a3);
-    } else {
-      const V a0 = cadd(v[0], v[1]), a1 = csub(v[0], v[1]);
-      v[0] = a0;
-      v[1] = a1;
-    }
-    V* dst = out + r * N + (j - k) * R + k;
-#pragma unroll
-    for (int u = 0; u < R; ++u) dst[u * NS] = v[u];
+template <int R, bool INV, typename V>
+__device__ __forceinline__ void dft_r(V (&v)[R]) {
+  if constexpr (R == 8) {
+    dft8<INV>(v);
+  } else if constexpr (R == 4) {
+    const V a0 = cadd(v[0], v[2]), a2 = csub(v[0], v[2]);
+    const V a1 = cadd(v[1], v[3]), a3 = mul_mi(csub(v[1], v[3]), INV);
+    v[0] = cadd(a0, a1);
+    v[1] = cadd(a2, a3);
+    v[2] = csub(a0, a1);
+    v[3] = csub(a2, a3);
+  } else {
+    const V a0 = cadd(v[0], v[1]), a1 = csub(v[0], v[1]);
+    v[0] = a0;
+    v[1] = a1;
   }
 }
 
-// Radix-8 passes while at least 8 points remain per sub-transform, then one radix-4 or 2 pass.
-template <int N, int NS, bool INV, typename V>
-__device__ __forceinline__ V* stockham_c(V* A, V* B, const V* tw) {
-  if constexpr (NS >= N) {
-    return A;
+// threads per block of the row-FFT kernels (two rows of N points)
+__host__ __device__ constexpr int fft_nt(int n2) { return n2 / 4 > 32 ? n2 / 4 : 32; }
+inline int fft_threads(int n2) { return fft_nt(n2); }
+
+// Sources and sinks of a pass: (row r in {0 north, 1 south}, index i) -> value.
+template <int N, typename V>
+struct SmemRows {
+  V* a;
+  __device__ __forceinline__ V operator()(int r, int i) const { return a[r * N + i]; }
+  __device__ __forceinline__ void put(int r, int i, V v) const { a[r * N + i] = v; }
+};
+template <typename V>
+struct GlobalRows {
+  const V* n;
+  const V* s;
+  __device__ __forceinline__ V operator()(int r, int i) const { return __ldg((r ? s : n) + i); }
+};
+
+// Output rows of an inverse transform (north row, south row of the grid), with the optional
+// epilogue out2 = grid * mul2 on the same rows (null: none).
+struct GridRowsOut {
+  double2* rn;
+  double2* rs;
+  double2* on;
+  double2* os;
+  const double2* mn;
+  const double2* ms;
+  __device__ __forceinline__ void put(int r, int i, double2 v) const {
+    (r ? rs : rn)[i] = v;
+    if (on) {
+      const double2 w = __ldg((r ? ms : mn) + i);
+      (r ? os : on)[i] = make_double2(v.x * w.x, v.y * w.y);
+    }
+  }
+};
+
+// One pass of radix R, sub-transform size NS before the pass.  ALIAS: the source is the
+// destination buffer (synchronise between the reads and the writes).
+template <int N, int R, int NS, bool INV, bool ALIAS, typename V, typename Src, typename Dst>
+__device__ __forceinline__ void fft_pass(const Src& src, const Dst& dst, const V* __restrict__ tw) {
+  constexpr int NT = fft_nt(N);
+  constexpr int Q = N / R;
+  constexpr int IT = (2 * Q + NT - 1) / NT;
+  constexpr int TSTEP = 2 * N / (NS * R);
+  V v[IT][R];
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = threadIdx.x + it * NT;
+    if ((2 * Q) % NT == 0 || idx < 2 * Q) {
+      const int r = idx / Q, j = idx % Q;
+      const int k = j % NS;
+#pragma unroll
+      for (int u = 0; u < R; ++u) v[it][u] = src(r, j + u * Q);
+      if (NS > 1) {
+#pragma unroll
+        for (int u = 1; u < R; ++u) {
+          const int t = u * k * TSTEP;
+          V w;
+          if (t < N) {
+            w = __ldg(tw + t);
+          } else {
+            w = __ldg(tw + (t - N));
+            w = mkc(-w.x, -w.y);
+          }
+          if (INV) w.y = -w.y;
+          v[it][u] = cmul(v[it][u], w);
+        }
+      }
+    }
+  }
+  if (ALIAS) __syncthreads();
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int idx = threadIdx.x + it * NT;
+    if ((2 * Q) % NT == 0 || idx < 2 * Q) {
+      const int r = idx / Q, j = idx % Q;
+      const int k = j % NS;
+      dft_r<R, INV>(v[it]);
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int u = 0; u < R; ++u) dst.put(r, base + u * NS, v[it][u]);
+    }
+  }
+  __syncthreads();
+}
+
+template <int N, int NS>
+struct FftRadix {
+  static constexpr int R = (N / NS >= 8) ? 8 : N / NS;
+};
+
+// Passes NS .. N of the transform held in A (shared memory), the last one into `sink`.
+template <int N, int NS, bool INV, typename V, typename Sink>
+__device__ __forceinline__ void fft_rest(V* A, const V* tw, const Sink& sink) {
+  if constexpr (NS < N) {
+    constexpr int R = FftRadix<N, NS>::R;
+    if constexpr (NS * R >= N) {
+      fft_pass<N, R, NS, INV, false>(SmemRows<N, V>{A}, sink, tw);
+    } else {
+      fft_pass<N, R, NS, INV, true>(SmemRows<N, V>{A}, SmemRows<N, V>{A}, tw);
+      fft_rest<N, NS * R, INV>(A, tw, sink);
+    }
+  }
+}
+
+// Whole transform: first pass from `src` into A, the rest in place, the last pass into `sink`
+// (SmemRows{A} to keep the result in A).  N >= 2.
+template <int N, bool INV, typename V, typename Src, typename Sink>
+__device__ __forceinline__ void fft_rows(const Src& src, V* A, const V* tw, const Sink& sink) {
+  constexpr int R = FftRadix<N, 1>::R;
+  if constexpr (R >= N) {
+    fft_pass<N, R, 1, INV, false>(src, sink, tw);
   } else {
-    constexpr int REM = N / NS;
-    constexpr int R = (REM >= 8) ? 8 : REM;
-    fft_pass_c<N, R, NS, INV, V>(A, B, tw);
-    __syncthreads();
-    return stockham_c<N, NS * R, INV, V>(B, A, tw);
+    fft_pass<N, R, 1, INV, false>(src, SmemRows<N, V>{A}, tw);
+    fft_rest<N, R, INV>(A, tw, sink);
   }
 }
 
@@ -132,6 +214,5 @@ __device__ __forceinline__ V* stockham_c(V* A, V* B, const V* tw) {
     default: CALL(2048); break;  \
   }
 
-inline int fft_threads(int n2) { return n2 / 4 > 32 ? n2 / 4 : 32; }
 
 }  // namespace sle

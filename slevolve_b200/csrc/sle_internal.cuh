@@ -138,6 +138,7 @@ struct sle_sht {
   alignas(64) unsigned char mx_tmap[3][128];   // TMA maps of mx_xf (boxes of 8, 16, 32 fields)
   double mx_table_bytes;
   int n_ana_units, n_syn_units;
+  int n_sm;                      // SMs of the device (persistent transform grid)
 };
 
 namespace sle {

@@ -45,15 +45,21 @@ namespace {
 constexpr int KC = 32;                        // K elements per chunk: one 128-byte row of TF32
 constexpr int TILE_F = 128 * KC;              // words of one A tile (128 rows x 32)
 constexpr int TILE_A = TILE_F * 4;            // 16 KB
+constexpr int SLOT_WORDS = 2 * TILE_F;        // Legendre table slot: FP32 A tiles of both parities
+constexpr uint32_t SLOT_BYTES = 4u * SLOT_WORDS;
 constexpr int TILE_B = MX_NMAX * 128;         // MX_NMAX rows x 128 bytes = 8 KB
 constexpr int STAGE_BYTES = 4 * TILE_A + 4 * TILE_B;
 constexpr int NSTAGE = 2;
 constexpr int MISC_BYTES = 1024;              // barriers + bookkeeping
 constexpr int MX_SMEM = 1024 + NSTAGE * STAGE_BYTES + MISC_BYTES;
-constexpr int TC_THREADS = 10 * 32;
+constexpr int W_SPL = 4;                      // warps 4..11: splitters (two groups of four)
+constexpr int W_MMA = 12;                     // TMEM owner, MMA issue
+constexpr int W_LOAD = 13;                    // bulk / TMA loads
+constexpr int TC_THREADS = 14 * 32;           // warps 0..3: epilogue
 constexpr int ANA_SPAN = 256;                 // degrees per analysis unit (128 per parity)
 constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wait gives up
 constexpr uint32_t TMEM_COLS = 512;
+constexpr uint32_t SET_COLS = 256;            // two accumulator sets (units alternate)
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
 
 static_assert(MX_SMEM <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
@@ -115,6 +121,18 @@ __device__ __forceinline__ void named_bar(int id, int nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
+// AND of `v` over the `n` threads that reach named barrier `id` (all of them must).
+__device__ __forceinline__ bool bar_and(int id, int n, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, %2, %3, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+
 __device__ __forceinline__ void tc_alloc(uint32_t holder, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(holder), "r"(ncols)
                : "memory");
@@ -169,24 +187,8 @@ __host__ __device__ __forceinline__ int sw_off(int row, int k) {
 }
 
 // ------------------------------------------------------------- precision splits
-// TF32 bit pattern of a double whose mantissa below its top 10 bits is zero, given its high
-// word; magnitudes below FP32's normal range (2^-126) become zero.
-__device__ __forceinline__ uint32_t tf32_from_dhi(uint32_t a) {
-  const uint32_t e = (a >> 20) & 0x7FFu;
-  const uint32_t f = (a & 0x80000000u) | ((e - 896u) << 23) | ((a & 0x000FFC00u) << 3);
-  return (e < 897u) ? 0u : f;
-}
-
-// p = hi + lo with hi the nearest TF32 (ties away from zero, decided on the high word) and lo
-// the nearest TF32 of the exact remainder: |p - hi - lo| <= 2^-22 |p| for |p| >= 2^-100.
-__device__ __forceinline__ void split_f64(double p, uint32_t& hi, uint32_t& lo) {
-  const uint32_t a = ((uint32_t)__double2hiint(p) + 0x200u) & 0xFFFFFC00u;
-  const double r = p - __hiloint2double((int)a, 0);
-  const uint32_t b = ((uint32_t)__double2hiint(r) + 0x200u) & 0xFFFFFC00u;
-  hi = tf32_from_dhi(a);
-  lo = tf32_from_dhi(b);
-}
-
+// x = hi + lo with hi the nearest TF32 of x (ties away from zero) and lo the nearest TF32 of
+// the exact remainder: |x - hi - lo| <= 2^-22 |x| for normal x.
 __device__ __forceinline__ void split_f32(float x, uint32_t& hi, uint32_t& lo) {
   hi = (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
   const float r = x - __uint_as_float(hi);
@@ -227,14 +229,17 @@ __device__ __forceinline__ bool field_off(const MxFieldArgs& a, int f) {
   return false;
 }
 
-// Shared memory of a stage: A tiles [par0 hi][par0 lo][par1 hi][par1 lo] (the order of a
-// Legendre table slot, so one bulk copy fills them), then B tiles [par0 hi][par1 hi][par0 lo]
-// [par1 lo] (the lo pair is where the raw B data lands).
+// Shared memory of a stage: A tiles [par0 hi][par1 hi][par0 lo][par1 lo] (a Legendre table
+// slot, FP32, lands in the hi pair and is split in place), then B tiles [par0 hi][par1 hi]
+// [par0 lo][par1 lo] (the raw B data lands in the lo pair).
 struct Smem {
   uint8_t* base;        // generic pointer, 1024-aligned
   uint32_t sbase;       // shared-window address of base
   __device__ uint32_t a_tile(int stage, int par, int lo) const {
-    return sbase + stage * STAGE_BYTES + (par * 2 + lo) * TILE_A;
+    return sbase + stage * STAGE_BYTES + (lo * 2 + par) * TILE_A;
+  }
+  __device__ uint8_t* a_ptr(int stage, int par, int lo) const {
+    return base + stage * STAGE_BYTES + (lo * 2 + par) * TILE_A;
   }
   __device__ uint32_t b_tile(int stage, int par, int lo) const {
     return sbase + stage * STAGE_BYTES + 4 * TILE_A + (lo * 2 + par) * TILE_B;
@@ -251,71 +256,59 @@ __device__ __forceinline__ Smem smem_layout(uint8_t* raw) {
   return Smem{raw + (al - s), al};
 }
 
+// Barriers: full[2] (splitters -> MMA), empty[2] (MMA commit -> loader), raw[2] (copies
+// landed -> splitters), accum[2] (a unit's MMAs done -> epilogue, per TMEM set), tfree[2]
+// (epilogue done with a TMEM set -> MMA), drain (MMAs issued before an abort).
+enum { BAR_FULL = 0, BAR_EMPTY = 2, BAR_RAW = 4, BAR_ACCUM = 6, BAR_TFREE = 8, BAR_DRAIN = 10 };
 struct Misc {
-  uint64_t* bar;        // full[2], empty[2], accum, drain, raw[2]
+  uint64_t* bar;
   uint32_t* tmem_holder;
   int* active;          // [MX_MAXF]
   int* any;
+  __device__ uint32_t b(int i) const { return smem_u32(bar + i); }
 };
 __device__ __forceinline__ Misc misc_layout(const Smem& S) {
   uint8_t* p = S.misc();
   Misc m;
   m.bar = reinterpret_cast<uint64_t*>(p);
-  m.tmem_holder = reinterpret_cast<uint32_t*>(p + 64);
-  m.active = reinterpret_cast<int*>(p + 128);
-  m.any = reinterpret_cast<int*>(p + 128 + 4 * MX_MAXF);
+  m.tmem_holder = reinterpret_cast<uint32_t*>(p + 128);
+  m.active = reinterpret_cast<int*>(p + 256);
+  m.any = reinterpret_cast<int*>(p + 256 + 4 * MX_MAXF);
   return m;
 }
 
-// TMEM use (512 columns): [0, 2N) correction accumulator (Ahi*Blo + Alo*Bhi of every chunk),
-// then nbuf main accumulators of 2N columns (Ahi*Bhi), chunk i into buffer i % nbuf; each
-// accumulator holds [even parity N columns][odd parity N columns].
+// TMEM use (512 columns): two sets of 256, consecutive units alternate between them so that
+// the epilogue of one unit overlaps the MMAs of the next.  In a set: [0, 2N) correction
+// accumulator (Ahi*Blo + Alo*Bhi of every chunk), then nbuf main accumulators of 2N columns
+// (Ahi*Bhi), chunk i into buffer i % nbuf; each accumulator holds [even parity N columns][odd
+// parity N columns].
 __device__ __forceinline__ int main_buffers(int nch, int ncols) {
-  return max(1, min(nch, ((int)TMEM_COLS - 2 * ncols) / (2 * ncols)));
+  return max(1, min(nch, ((int)SET_COLS - 2 * ncols) / (2 * ncols)));
 }
 
-// MMA issue loop: chunk i uses stage i & 1.
-__device__ void mma_loop(const Smem& S, const Misc& M, uint32_t tmem, int nch, int ncols, const Abort& ab) {
+// MMAs of one chunk (stage st) into the set at `set_base`; chunk k of its unit.
+__device__ __forceinline__ void mma_chunk(const Smem& S, uint32_t set_base, int st, int k, int nbuf, int ncols) {
   const uint32_t idesc = idesc_tf32(128, ncols);
-  const uint32_t full0 = smem_u32(&M.bar[0]), empty0 = smem_u32(&M.bar[2]), accum = smem_u32(&M.bar[4]);
-  const int nbuf = main_buffers(nch, ncols);
-  for (int i = 0; i < nch; ++i) {
-    const int st = i & 1;
-    if (!mbar_wait(full0 + 8 * st, (uint32_t)((i >> 1) & 1), ab)) {
-      // aborted: let the MMAs already issued finish (bounded) before TMEM is released
-      if (i > 0) {
-        const uint32_t drain = smem_u32(&M.bar[5]);
-        tc_commit(drain);
-        const long long t0 = clock64();
-        while (!mbar_try_wait(drain, 0u) && clock64() - t0 < WAIT_LIMIT) {
-        }
-      }
-      return;
-    }
-    tc_fence_after();
-    const uint32_t dmain = tmem + (uint32_t)(2 * ncols * (1 + i % nbuf));
-    const bool fresh = i < nbuf;
+  const uint32_t dmain = set_base + (uint32_t)(2 * ncols * (1 + k % nbuf));
+  const bool fresh = k < nbuf;
 #pragma unroll
-    for (int kk = 0; kk < KC / 8; ++kk) {
+  for (int kk = 0; kk < KC / 8; ++kk) {
 #pragma unroll
-      for (int par = 0; par < 2; ++par) {
-        const uint64_t ah = sdesc_sw128(S.a_tile(st, par, 0) + 32 * kk);
-        const uint64_t al = sdesc_sw128(S.a_tile(st, par, 1) + 32 * kk);
-        const uint64_t bh = sdesc_sw128(S.b_tile(st, par, 0) + 32 * kk);
-        const uint64_t bl = sdesc_sw128(S.b_tile(st, par, 1) + 32 * kk);
-        const uint32_t off = (uint32_t)(par * ncols);
-        tc_mma_tf32(dmain + off, ah, bh, idesc, (fresh && kk == 0) ? 0u : 1u);
-        tc_mma_tf32(tmem + off, ah, bl, idesc, (i == 0 && kk == 0) ? 0u : 1u);
-        tc_mma_tf32(tmem + off, al, bh, idesc, 1u);
-      }
+    for (int par = 0; par < 2; ++par) {
+      const uint64_t ah = sdesc_sw128(S.a_tile(st, par, 0) + 32 * kk);
+      const uint64_t al = sdesc_sw128(S.a_tile(st, par, 1) + 32 * kk);
+      const uint64_t bh = sdesc_sw128(S.b_tile(st, par, 0) + 32 * kk);
+      const uint64_t bl = sdesc_sw128(S.b_tile(st, par, 1) + 32 * kk);
+      const uint32_t off = (uint32_t)(par * ncols);
+      tc_mma_tf32(dmain + off, ah, bh, idesc, (fresh && kk == 0) ? 0u : 1u);
+      tc_mma_tf32(set_base + off, ah, bl, idesc, (k == 0 && kk == 0) ? 0u : 1u);
+      tc_mma_tf32(set_base + off, al, bh, idesc, 1u);
     }
-    tc_commit(empty0 + 8 * st);
   }
-  if (nch > 0) tc_commit(accum);
 }
 
 // Accumulator columns [16 cb, 16 cb + 16) of both parities for this thread's TMEM lane, summed
-// over the correction and main buffers in FP64 (in that order).
+// over the correction and main buffers of the set in FP64 (in that order).
 __device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int ncols, int cb, double (&ev)[16],
                                          double (&od)[16]) {
   uint32_t re[16], ro[16];
@@ -327,7 +320,7 @@ __device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int ncols, 
     ev[u] = (double)__uint_as_float(re[u]);
     od[u] = (double)__uint_as_float(ro[u]);
   }
-  const int nb = min(nch, main_buffers(nch, ncols));
+  const int nb = main_buffers(nch, ncols);
   for (int b = 0; b < nb; ++b) {
     const uint32_t base = lanebase + (uint32_t)(2 * ncols * (1 + b));
     tc_ld16(base + (uint32_t)(16 * cb), re);
@@ -345,18 +338,18 @@ __device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int ncols, 
 __device__ uint32_t prologue(const Misc& M, const MxFieldArgs& a) {
   const int warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
-    mbar_init(smem_u32(&M.bar[0]), 4);   // full: the 4 splitter warps of the stage
-    mbar_init(smem_u32(&M.bar[1]), 4);
-    mbar_init(smem_u32(&M.bar[2]), 1);   // empty: one tcgen05.commit
-    mbar_init(smem_u32(&M.bar[3]), 1);
-    mbar_init(smem_u32(&M.bar[4]), 1);   // accumulators complete
-    mbar_init(smem_u32(&M.bar[5]), 1);   // drain after an abort
-    mbar_init(smem_u32(&M.bar[6]), 1);   // raw A and B data of stage 0 / 1 landed
-    mbar_init(smem_u32(&M.bar[7]), 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(M.b(BAR_FULL + i), 4);    // the 4 splitter warps of the stage
+      mbar_init(M.b(BAR_EMPTY + i), 1);   // one tcgen05.commit
+      mbar_init(M.b(BAR_RAW + i), 1);     // loader's expect_tx
+      mbar_init(M.b(BAR_ACCUM + i), 1);   // one tcgen05.commit (or arrive for an empty unit)
+      mbar_init(M.b(BAR_TFREE + i), 4);   // the 4 epilogue warps
+    }
+    mbar_init(M.b(BAR_DRAIN), 1);
     fence_mbar_init();
   }
   if (threadIdx.x < MX_MAXF) M.active[threadIdx.x] = (threadIdx.x < a.nf) && !field_off(a, threadIdx.x);
-  if (warp == 8) {
+  if (warp == W_MMA) {
     tc_alloc(smem_u32(M.tmem_holder), TMEM_COLS);
     tc_relinquish();
   }
@@ -376,18 +369,27 @@ __device__ uint32_t prologue(const Misc& M, const MxFieldArgs& a) {
 __device__ void epilogue_release(uint32_t tmem) {
   tc_fence_before();
   __syncthreads();
-  if ((threadIdx.x >> 5) == 8) {
+  if ((threadIdx.x >> 5) == W_MMA) {
     tc_fence_after();
     tc_dealloc(tmem, TMEM_COLS);
   }
 }
 
+// Wait for a phase with only the time limit (not the abort flag): used to let copies already
+// in flight land before the CTA exits.
+__device__ __noinline__ void mbar_wait_drain(uint32_t a, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(a, parity)) {
+    if (clock64() - t0 > WAIT_LIMIT) return;
+  }
+}
+
 // ===================================================== Legendre tables (once per plan)
-// The A operand of every chunk is precomputed from the FP64 recurrence and split into TF32
-// hi / lo in the tile order of the shared-memory stage: slot = [par0 hi][par0 lo][par1 hi]
-// [par1 lo], each 128 rows x 32 (4 TILE_F words).  Entries below the significance threshold of
-// their (segment, latitude group) and rows or columns outside the unit stay zero (the table is
-// zeroed first).
+// The A operand of every chunk is precomputed from the FP64 recurrence, rounded to FP32 and
+// stored in the tile order of the shared-memory stage: slot = [par0][par1], each 128 rows x 32
+// (2 TILE_F words); the transform kernel splits it into TF32 hi / lo.  Entries below the
+// significance threshold of their (segment, latitude group) and rows or columns outside the
+// unit stay zero (the table is zeroed first).
 
 // Analysis unit (m, span s): rows r of parity p = degree lbase + 2r + p, K = latitudes
 // 32c .. 32c + 31 for the chunks c = kstart .. ngrp - 1.  Warp (segment q, chunk parity g).
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(256) k_tab_ana(ShtDev P, uint32_t* tab) {
   const long long cbase = P.moff[m] + (lbase - m) + SEG * q;
   for (int c = kstart + g; c < P.ngrp; c += 2) {
     if (c < (int)P.istart[seg]) continue;
-    uint32_t* slot = tab + (off + (c - kstart)) * 4 * TILE_F;
+    uint32_t* slot = tab + (off + (c - kstart)) * SLOT_WORDS;
     const int j = KC * c + lane;
     const double mu = P.mu[j];
     const double2 sd = P.seeds[(size_t)seg * P.nh + j];
@@ -415,12 +417,8 @@ __global__ void __launch_bounds__(256) k_tab_ana(ShtDev P, uint32_t* tab) {
       const double qn = fma(mu, qb, P.be[cbase + t] * qa);
       qa = qb;
       qb = qn;
-      uint32_t h, l;
-      split_f64(P.cf[cbase + t] * qn, h, l);
       const int o = sw_off(SEG / 2 * q + (t >> 1), lane);
-      uint32_t* tp = slot + (t & 1) * 2 * TILE_F;
-      tp[o] = h;
-      tp[TILE_F + o] = l;
+      slot[(t & 1) * TILE_F + o] = __float_as_uint(__double2float_rn(P.cf[cbase + t] * qn));
     }
   }
 }
@@ -442,24 +440,38 @@ __global__ void __launch_bounds__(128) k_tab_syn(ShtDev P, uint32_t* tab) {
     const int l0 = P.seg_l0[seg];
     const int len = min(SEG, P.lmax + 1 - l0);
     const long long cbase = P.moff[m] + (l0 - m);
-    uint32_t* slot = tab + (off + i) * 4 * TILE_F;
+    uint32_t* slot = tab + (off + i) * SLOT_WORDS;
     const double2 sd = P.seeds[(size_t)seg * P.nh + j];
     double qa = sd.x, qb = sd.y;
     for (int tt = 0; tt < len; ++tt) {
       const double qn = fma(mu, qb, P.be[cbase + tt] * qa);
       qa = qb;
       qb = qn;
-      uint32_t h, l;
-      split_f64(P.cf[cbase + tt] * qn, h, l);
       const int o = sw_off(row, tt >> 1);
-      uint32_t* tp = slot + (tt & 1) * 2 * TILE_F;
-      tp[o] = h;
-      tp[TILE_F + o] = l;
+      slot[(tt & 1) * TILE_F + o] = __float_as_uint(__double2float_rn(P.cf[cbase + tt] * qn));
     }
   }
 }
 
 // ============================================================ Legendre contraction
+// A split: the FP32 Legendre values landed in the hi tiles of the stage; hi <- TF32(x) in
+// place, lo tile <- TF32(x - hi).  Elementwise, so the tile order does not matter.
+__device__ __forceinline__ void split_a(const Smem& S, int st, int tid) {
+  uint4* hp = reinterpret_cast<uint4*>(S.a_ptr(st, 0, 0));
+  uint4* lp = reinterpret_cast<uint4*>(S.a_ptr(st, 0, 1));
+#pragma unroll 4
+  for (int e = tid; e < SLOT_WORDS / 4; e += 128) {
+    const uint4 v = hp[e];
+    uint4 h, l;
+    split_f32(__uint_as_float(v.x), h.x, l.x);
+    split_f32(__uint_as_float(v.y), h.y, l.y);
+    split_f32(__uint_as_float(v.z), h.z, l.z);
+    split_f32(__uint_as_float(v.w), h.w, l.w);
+    hp[e] = h;
+    lp[e] = l;
+  }
+}
+
 // Analysis B data: the TMA box of the folded FFT is [field][32 latitudes][S.re, S.im, D.re, D.im]
 // (16 bytes per entry) in the stage's B lo tiles; the 4 splitter warps read it, synchronise,
 // and write rows 2f / 2f+1 of the parity-0 (S) and parity-1 (D) tiles.
@@ -513,75 +525,142 @@ __device__ __forceinline__ void split_b_syn(const Smem& S, int st, int nrow, int
   }
 }
 
-// One CTA per work unit.  Analysis: rows of D = degrees, columns = (Re, Im) of the fields;
-// synthesis: rows = latitudes.
+// Work unit u: (m, span | latitude tile, chunk count, first table slot).
+template <bool SYN>
+__device__ __forceinline__ void unit_info(const ShtDev& P, int u, int4& unit, int& nch) {
+  unit = SYN ? P.mx_syn_units[u] : P.mx_ana_units[u];
+  nch = SYN ? unit.z : P.ngrp - unit.z;
+}
+
+// Persistent CTAs (one per SM) over the work units u = blockIdx.x + i gridDim.x.  Analysis
+// units: rows of D = degrees, columns = (Re, Im) of the fields; synthesis: rows = latitudes.
+// Roles: warp 13 streams the chunks of all the CTA's units through the two stages; warps 4-11
+// split stage g = (warp - 4) / 4; warp 12 issues the MMAs of unit i into TMEM set i & 1;
+// warps 0-3 drain set i & 1 for unit i while the MMAs of unit i + 1 run.
 template <bool SYN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox) {
+    k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox, int nunits) {
   extern __shared__ uint8_t smraw[];
   const Smem S = smem_layout(smraw);
   const Misc M = misc_layout(S);
   const Abort ab{P.mx_abort, status};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int4 unit = SYN ? P.mx_syn_units[blockIdx.x] : P.mx_ana_units[blockIdx.x];
-  const int m = unit.x, L = P.lmax;
-  const long long toff = unit.w;
-  const int nch = SYN ? unit.z : P.ngrp - unit.z;
+  const int L = P.lmax;
   const int ncols = a.ncols;
   const uint32_t* tab = SYN ? P.mx_tab_syn : P.mx_tab_ana;
   const uint32_t tmem = prologue(M, a);
   if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
-    const uint32_t empty0 = smem_u32(&M.bar[2]), full0 = smem_u32(&M.bar[0]);
     const int nrow = 2 * a.nf;
-    if (warp == 9) {
-      // ---- loader: A slot and B data of chunk i into stage i & 1
+    if (warp == W_LOAD) {
+      // ---- loader: chunk c of the CTA's sequence into stage c & 1
       if (lane == 0) {
         const uint32_t bbytes = SYN ? 2u * (uint32_t)nrow * 128u : (uint32_t)zbox * 32u * 16u;
-        for (int i = 0; i < nch; ++i) {
-          const int st = i & 1;
-          if (!mbar_wait(empty0 + 8 * st, (uint32_t)(((i >> 1) & 1) ^ 1), ab)) break;
-          const uint32_t raw = smem_u32(&M.bar[6 + st]);
-          mbar_arrive_expect_tx(raw, 4u * TILE_A + bbytes);
-          bulk_g2s(S.a_tile(st, 0, 0), tab + (toff + i) * 4 * TILE_F, 4u * TILE_A, raw);
-          if (SYN) {
-            const int seg = P.mx_syn_seg[toff + i];
-            bulk_g2s(S.b_tile(st, 0, 1), P.mx_bsyn + ((size_t)seg * 2 + 0) * BBLOCK, (uint32_t)nrow * 128u, raw);
-            bulk_g2s(S.b_tile(st, 1, 1), P.mx_bsyn + ((size_t)seg * 2 + 1) * BBLOCK, (uint32_t)nrow * 128u, raw);
-          } else {
-            tma_load_3d(S.b_tile(st, 0, 1), &tmx, 4 * m, KC * (unit.z + i), 0, raw);
+        int c = 0;
+        bool ok = true;
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+          int4 unit;
+          int nch;
+          unit_info<SYN>(P, u, unit, nch);
+          for (int k = 0; k < nch; ++k, ++c) {
+            const int st = c & 1;
+            if (!mbar_wait(M.b(BAR_EMPTY + st), (uint32_t)(((c >> 1) & 1) ^ 1), ab)) {
+              ok = false;
+              break;
+            }
+            const uint32_t raw = M.b(BAR_RAW + st);
+            mbar_arrive_expect_tx(raw, SLOT_BYTES + bbytes);
+            bulk_g2s(S.a_tile(st, 0, 0), tab + ((long long)unit.w + k) * SLOT_WORDS, SLOT_BYTES, raw);
+            if (SYN) {
+              const int seg = P.mx_syn_seg[unit.w + k];
+              bulk_g2s(S.b_tile(st, 0, 1), P.mx_bsyn + ((size_t)seg * 2 + 0) * BBLOCK, (uint32_t)nrow * 128u, raw);
+              bulk_g2s(S.b_tile(st, 1, 1), P.mx_bsyn + ((size_t)seg * 2 + 1) * BBLOCK, (uint32_t)nrow * 128u, raw);
+            } else {
+              tma_load_3d(S.b_tile(st, 0, 1), &tmx, 4 * unit.x, KC * (unit.z + k), 0, raw);
+            }
           }
+        }
+        // copies in flight land before the CTA exits: the last phase issued on each stage
+        for (int st = 0; st < 2; ++st) {
+          const int n_st = (c + 1 - st) / 2;   // loads issued on stage st
+          if (n_st > 0) mbar_wait_drain(M.b(BAR_RAW + st), (uint32_t)((n_st - 1) & 1));
         }
       }
       __syncwarp();
-    } else if (warp == 8) {
-      if (lane == 0) mma_loop(S, M, tmem, nch, ncols, ab);
+    } else if (warp == W_MMA) {
+      if (lane == 0) {
+        int c = 0, i = 0;
+        bool ok = true, issued = false;
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
+          int4 unit;
+          int nch;
+          unit_info<SYN>(P, u, unit, nch);
+          const int set = i & 1;
+          if (!mbar_wait(M.b(BAR_TFREE + set), (uint32_t)(((i >> 1) & 1) ^ 1), ab)) break;
+          tc_fence_after();
+          const uint32_t base = tmem + SET_COLS * (uint32_t)set;
+          const int nbuf = main_buffers(nch, ncols);
+          for (int k = 0; k < nch; ++k, ++c) {
+            const int st = c & 1;
+            if (!mbar_wait(M.b(BAR_FULL + st), (uint32_t)((c >> 1) & 1), ab)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            mma_chunk(S, base, st, k, nbuf, ncols);
+            issued = true;
+            tc_commit(M.b(BAR_EMPTY + st));
+          }
+          if (!ok) break;
+          if (nch > 0) tc_commit(M.b(BAR_ACCUM + set));
+          else mbar_arrive(M.b(BAR_ACCUM + set));
+        }
+        if (!ok && issued) {
+          // aborted: let the MMAs already issued finish (bounded) before TMEM is released
+          tc_commit(M.b(BAR_DRAIN));
+          mbar_wait_drain(M.b(BAR_DRAIN), 0u);
+        }
+      }
       __syncwarp();
-    } else {
+    } else if (warp >= W_SPL) {
       // ---- splitters: group g = stage g
-      const int g = warp >> 2, tid = threadIdx.x & 127;
-      int round = 0;
-      for (int i = g; i < nch; i += 2, ++round) {
-        const bool ok = mbar_wait(smem_u32(&M.bar[6 + g]), (uint32_t)(round & 1), ab);
-        if (!__all_sync(0xffffffffu, ok)) break;
-        if (SYN) split_b_syn(S, g, nrow, tid);
-        else split_b_ana(S, g, a.nf, tid, 1 + g);
-        fence_proxy_async();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(full0 + 8 * g);
-      }
-    }
-    // ---- epilogue: warps 0-3 own TMEM lanes 0-127
-    if (warp < 4) {
-      const int r = 32 * warp + lane;
+      const int g = (warp - W_SPL) >> 2, tid = threadIdx.x - 32 * W_SPL - 128 * g;
+      int c = 0;
       bool ok = true;
-      if (nch > 0) {
-        ok = mbar_wait(smem_u32(&M.bar[4]), 0u, ab);
-        tc_fence_after();
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        int4 unit;
+        int nch;
+        unit_info<SYN>(P, u, unit, nch);
+        for (int k = 0; k < nch; ++k, ++c) {
+          if ((c & 1) != g) continue;
+          // every wait is bounded, so all four warps of the group reach the vote; they go on
+          // (and meet at the named barrier of the B split) only together
+          const bool w = mbar_wait(M.b(BAR_RAW + g), (uint32_t)((c >> 1) & 1), ab);
+          if (!bar_and(1 + g, 128, w)) {
+            ok = false;
+            break;
+          }
+          split_a(S, g, tid);
+          if (SYN) split_b_syn(S, g, nrow, tid);
+          else split_b_ana(S, g, a.nf, tid, 1 + g);
+          fence_proxy_async();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(M.b(BAR_FULL + g));
+        }
       }
-      ok = __all_sync(0xffffffffu, ok);
-      if (ok) {
-        const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
-        const double inv = 1.0 / SQRT2_LEGACY;
+    } else {
+      // ---- epilogue: warps 0-3 own TMEM lanes 0-127
+      const int r = 32 * warp + lane;
+      const double inv = 1.0 / SQRT2_LEGACY;
+      int i = 0;
+      for (int u = blockIdx.x; u < nunits; u += gridDim.x, ++i) {
+        int4 unit;
+        int nch;
+        unit_info<SYN>(P, u, unit, nch);
+        const int set = i & 1, m = unit.x;
+        const bool w = mbar_wait(M.b(BAR_ACCUM + set), (uint32_t)((i >> 1) & 1), ab);
+        if (!__all_sync(0xffffffffu, w)) break;
+        tc_fence_after();
+        const uint32_t lanebase = tmem + SET_COLS * (uint32_t)set + ((uint32_t)(32 * warp) << 16);
         const int le = m + ANA_SPAN * unit.y + 2 * r;   // analysis: even degree of row r
         const int j = 128 * unit.y + r;                 // synthesis: latitude of row r
         for (int cb = 0; cb < (2 * a.nf + 15) / 16; ++cb) {
@@ -590,22 +669,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             acc_read(lanebase, nch, ncols, cb, ve, vo);
           } else {
 #pragma unroll
-            for (int u = 0; u < 16; ++u) ve[u] = vo[u] = 0.0;
+            for (int q = 0; q < 16; ++q) ve[q] = vo[q] = 0.0;
           }
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const int f = 8 * cb + u;
+          for (int q = 0; q < 8; ++q) {
+            const int f = 8 * cb + q;
             if (f >= a.nf || !M.active[f]) continue;
             if (SYN) {
               if (j < P.nh) {
                 float4* gq = reinterpret_cast<float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm + m;
-                *gq = make_float4((float)(ve[2 * u] + vo[2 * u]), (float)(ve[2 * u + 1] + vo[2 * u + 1]),
-                                  (float)(ve[2 * u] - vo[2 * u]), (float)(ve[2 * u + 1] - vo[2 * u + 1]));
+                *gq = make_float4((float)(ve[2 * q] + vo[2 * q]), (float)(ve[2 * q + 1] + vo[2 * q + 1]),
+                                  (float)(ve[2 * q] - vo[2 * q]), (float)(ve[2 * q + 1] - vo[2 * q + 1]));
               }
             } else if (le <= L) {
               double2* dst = a.spec[f] + P.moff[m] + (le - m);
-              dst[0] = make_double2(ve[2 * u] * inv, ve[2 * u + 1] * inv);
-              if (le + 1 <= L) dst[1] = make_double2(vo[2 * u] * inv, vo[2 * u + 1] * inv);
+              dst[0] = make_double2(ve[2 * q] * inv, ve[2 * q + 1] * inv);
+              if (le + 1 <= L) dst[1] = make_double2(vo[2 * q] * inv, vo[2 * q + 1] * inv);
             }
           }
         }
@@ -619,6 +698,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             a.spec[lane][0] = make_double2(__dmul_rn(__dsqrt_rn(0.5), acc) / SQRT2_LEGACY, 0.0);
           }
         }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(M.b(BAR_TFREE + set));
       }
     }
   }
@@ -631,27 +713,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // entry per order (coalesced), the layout the analysis kernel's TMA box reads.  The m = 0 fold
 // (row sums) is also kept in FP64 in s0[f][j] for the FP64 degree-0 coefficient.
 template <int N>
-__global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fold_mx(ShtDev P, MxFieldArgs a) {
+__global__ void __launch_bounds__(fft_nt(N)) k_fold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ double2 smd2[];
-  double2* tw = smd2;
-  double2* A = smd2 + N;
-  double2* B = A + 2 * N;
+  double2* A = smd2;
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
   const int js = P.nlat - 1 - j;
   const double2* rn = reinterpret_cast<const double2*>(a.grid[f] + (size_t)j * (2 * N));
   const double2* rs = reinterpret_cast<const double2*>(a.grid[f] + (size_t)js * (2 * N));
-  for (int t = threadIdx.x; t < N; t += blockDim.x) {
-    tw[t] = P.tw[t];
-    A[t] = rn[t];
-    A[N + t] = rs[t];
-  }
-  __syncthreads();
-  const double2* Z = stockham_c<N, 1, false>(A, B, tw);
+  fft_rows<N, false>(GlobalRows<double2>{rn, rs}, A, P.tw, SmemRows<N, double2>{A});
+  const double2* Z = A;
   const double wn = P.wn[j], ws = P.ws[j];
   float4* X = reinterpret_cast<float4*>(P.mx_xf) + ((size_t)f * P.nh + j) * P.nm;
   for (int m = threadIdx.x; m < P.nm; m += blockDim.x) {
     double2 xr[2];
+    const double2 twm = (m > 0 && m < N) ? __ldg(P.tw + m) : make_double2(1.0, 0.0);
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       const double2* z = Z + r * N;
@@ -665,7 +741,7 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fold_mx(ShtDev P,
         const double2 e = cscale(cadd(zm, zc), 0.5);
         const double2 dz = csub(zm, zc);
         const double2 o = make_double2(0.5 * dz.y, -0.5 * dz.x);  // (zm - zc) / (2i)
-        xr[r] = cadd(e, cmul(tw[m], o));
+        xr[r] = cadd(e, cmul(twm, o));
       }
     }
     const double2 an = cscale(xr[0], wn), bs = cscale(xr[1], ws);
@@ -677,73 +753,59 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fold_mx(ShtDev P,
 // Inverse: north and south Legendre sums of field blockIdx.y (FP32 accumulators, m <= lmax, 0
 // above; one 16-byte entry per order), unnormalised inverse real FFT in FP64, plus the FP64
 // degree-0 term 1.41421356 sqrt(0.5) Re U_00 in every cell; optional epilogue out2 = grid * mul2.
+// The half-length complex packing of the real inverse transform is computed while the first
+// FFT pass reads its inputs; the last pass writes the output rows.
 template <int N>
-__global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_unfold_mx(ShtDev P, MxFieldArgs a) {
+struct UnfoldSrcMx {
+  const float4* G;   // [m] of this latitude pair
+  const double2* tw;
+  int nm;
+  double c00;
+  __device__ __forceinline__ double2 g(int r, int m) const {
+    double2 x = make_double2(0.0, 0.0);
+    if (m < nm) {
+      const float4 v = __ldg(G + m);
+      x = r ? make_double2(v.z, v.w) : make_double2(v.x, v.y);
+    }
+    if (m == 0) x.x += c00;
+    return x;
+  }
+  __device__ __forceinline__ double2 operator()(int r, int m) const {
+    double2 x, y;
+    if (m == 0) {
+      x = make_double2(g(r, 0).x, 0.0);
+      y = make_double2(g(r, N).x, 0.0);
+    } else {
+      x = g(r, m);
+      const double2 c = g(r, N - m);
+      y = make_double2(c.x, -c.y);
+    }
+    const double2 e = cadd(x, y);
+    const double2 t = __ldg(tw + m);
+    const double2 wc = make_double2(t.x, -t.y);  // exp(+2 pi i m / nlon)
+    const double2 o = cmul(csub(x, y), wc);
+    return make_double2(e.x - o.y, e.y + o.x);  // e + i o
+  }
+};
+
+template <int N>
+__global__ void __launch_bounds__(fft_nt(N)) k_unfold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ double2 smd2[];
-  __shared__ double2 nyq[2];
-  double2* tw = smd2;
-  double2* A = smd2 + N;
-  double2* B = A + 2 * N;
+  double2* A = smd2;
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
   const int js = P.nlat - 1 - j;
   const float4* G = reinterpret_cast<const float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm;
   const double c00 = __dmul_rn(__dmul_rn(SQRT2_LEGACY, a.spec[f][0].x), __dsqrt_rn(0.5));
-  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = P.tw[t];
-  for (int m = threadIdx.x; m <= N; m += blockDim.x) {
-    double2 gn = make_double2(0.0, 0.0), gs = gn;
-    if (m < P.nm) {
-      const float4 v = G[m];
-      gn = make_double2(v.x, v.y);
-      gs = make_double2(v.z, v.w);
-    }
-    if (m == 0) {
-      gn.x += c00;
-      gs.x += c00;
-    }
-    if (m < N) {
-      B[m] = gn;
-      B[N + m] = gs;
-    } else {
-      nyq[0] = gn;
-      nyq[1] = gs;
-    }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < 2 * N; idx += blockDim.x) {
-    const int r = idx / N;
-    const int m = idx % N;
-    double2 x, y;
-    if (m == 0) {
-      x = make_double2(B[r * N].x, 0.0);
-      y = make_double2(nyq[r].x, 0.0);
-    } else {
-      x = B[r * N + m];
-      const double2 c = B[r * N + N - m];
-      y = make_double2(c.x, -c.y);
-    }
-    const double2 e = cadd(x, y);
-    const double2 wc = make_double2(tw[m].x, -tw[m].y);  // exp(+2 pi i m / nlon)
-    const double2 o = cmul(csub(x, y), wc);
-    A[r * N + m] = make_double2(e.x - o.y, e.y + o.x);  // e + i o
-  }
-  __syncthreads();
-  const double2* Z = stockham_c<N, 1, true>(A, B, tw);
-  double2* rn = reinterpret_cast<double2*>(a.grid[f] + (size_t)j * (2 * N));
-  double2* rs = reinterpret_cast<double2*>(a.grid[f] + (size_t)js * (2 * N));
+  const size_t ro = (size_t)j * (2 * N), rso = (size_t)js * (2 * N);
   double* out2 = a.epi_out[f];
   const double* mul2 = a.epi_mul[f];
-  for (int t = threadIdx.x; t < N; t += blockDim.x) {
-    const double2 vn = Z[t], vs = Z[N + t];
-    rn[t] = vn;
-    rs[t] = vs;
-    if (out2) {
-      const double2 mn = reinterpret_cast<const double2*>(mul2 + (size_t)j * (2 * N))[t];
-      const double2 ms = reinterpret_cast<const double2*>(mul2 + (size_t)js * (2 * N))[t];
-      reinterpret_cast<double2*>(out2 + (size_t)j * (2 * N))[t] = make_double2(vn.x * mn.x, vn.y * mn.y);
-      reinterpret_cast<double2*>(out2 + (size_t)js * (2 * N))[t] = make_double2(vs.x * ms.x, vs.y * ms.y);
-    }
-  }
+  GridRowsOut sink{reinterpret_cast<double2*>(a.grid[f] + ro), reinterpret_cast<double2*>(a.grid[f] + rso),
+                   out2 ? reinterpret_cast<double2*>(out2 + ro) : nullptr,
+                   out2 ? reinterpret_cast<double2*>(out2 + rso) : nullptr,
+                   out2 ? reinterpret_cast<const double2*>(mul2 + ro) : nullptr,
+                   out2 ? reinterpret_cast<const double2*>(mul2 + rso) : nullptr};
+  fft_rows<N, true>(UnfoldSrcMx<N>{G, P.tw, P.nm, c00}, A, P.tw, sink);
 }
 
 // Synthesis B operand: per segment s (order m, degrees l0..l0+63) and parity, rows 2f / 2f+1 =
@@ -765,7 +827,7 @@ __global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
   blk[sw_off(2 * f + 1, k)] = (float)(u.y * SQRT2_LEGACY);
 }
 
-size_t mx_fft_smem(const ShtDev& d) { return (size_t)5 * d.n2 * sizeof(double2); }
+size_t mx_fft_smem(const ShtDev& d) { return (size_t)2 * d.n2 * sizeof(double2); }
 
 template <typename T>
 int mx_alloc(T** p, size_t n) {
@@ -870,7 +932,7 @@ int sht_mx_prepare(sle_sht* p) {
   p->n_ana_units = (int)av.size();
   p->n_syn_units = (int)sv.size();
   // Legendre tables: FP64 recurrence, split into TF32 hi / lo, zero where negligible
-  const size_t tab_a = (size_t)na * 4 * TILE_F, tab_s = (size_t)ns * 4 * TILE_F;
+  const size_t tab_a = (size_t)na * SLOT_WORDS, tab_s = (size_t)ns * SLOT_WORDS;
   SLE_TRY(mx_alloc(&p->mx_tab_ana, tab_a + 1));
   SLE_TRY(mx_alloc(&p->mx_tab_syn, tab_s + 1));
   SLE_CUDA(cudaMemset(p->mx_tab_ana, 0, tab_a * sizeof(uint32_t)));
@@ -909,6 +971,12 @@ int sht_mx_prepare(sle_sht* p) {
       set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
       return SLE_ERR_CUDA;
     }
+  }
+  {
+    int dev = 0, nsm = 0;
+    SLE_CUDA(cudaGetDevice(&dev));
+    SLE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    p->n_sm = std::max(1, nsm);
   }
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
@@ -951,7 +1019,8 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t
   const int zi = (a.nf <= ZBOX[0]) ? 0 : (a.nf <= ZBOX[1]) ? 1 : 2;
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[zi]);
   ProfToken t1 = prof_begin(prof_cls, a.nf, st);
-  k_leg_tc<false><<<p->n_ana_units, TC_THREADS, MX_SMEM, st>>>(d, a, status, *map, ZBOX[zi]);
+  k_leg_tc<false><<<std::min(p->n_ana_units, p->n_sm), TC_THREADS, MX_SMEM, st>>>(d, a, status, *map, ZBOX[zi],
+                                                                                p->n_ana_units);
   prof_end(t1, st);
   note_launch(2);
   SLE_CUDA(cudaGetLastError());
@@ -967,7 +1036,8 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[0]);
   ProfToken t0 = prof_begin(PROF_LEG_SYN, a.nf, st);
   k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
-  k_leg_tc<true><<<p->n_syn_units, TC_THREADS, MX_SMEM, st>>>(d, a, status, *map, 0);
+  k_leg_tc<true><<<std::min(p->n_syn_units, p->n_sm), TC_THREADS, MX_SMEM, st>>>(d, a, status, *map, 0,
+                                                                             p->n_syn_units);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
 #define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(NN), mx_fft_smem(d), st>>>(d, a)

@@ -219,28 +219,22 @@ struct CSpecPtrs {
 // S = F_N w_j/nlon + F_S w_j/nlon, D = F_N w_j/nlon - F_S w_j/nlon for m <= lmax
 // (sht.py:277-287).  X layout [f][0=S,1=D][m][j].  N = nlon/2 complex points per row.
 template <int N>
-__global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fft_fold(sle::ShtDev P, GridPtrs g) {
+__global__ void __launch_bounds__(fft_nt(N)) k_fft_fold(sle::ShtDev P, GridPtrs g) {
   extern __shared__ double2 sm[];
-  double2* tw = sm;
-  double2* A = sm + N;
-  double2* B = A + 2 * N;
+  double2* A = sm;
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_gated_off(P, f)) return;
   const int js = P.nlat - 1 - j;
   const double2* rn = reinterpret_cast<const double2*>(g.p[f] + (size_t)j * (2 * N));
   const double2* rs = reinterpret_cast<const double2*>(g.p[f] + (size_t)js * (2 * N));
-  for (int t = threadIdx.x; t < N; t += blockDim.x) {
-    tw[t] = P.tw[t];
-    A[t] = rn[t];
-    A[N + t] = rs[t];
-  }
-  __syncthreads();
-  const double2* Z = stockham_c<N, 1, false>(A, B, tw);
+  fft_rows<N, false>(GlobalRows<double2>{rn, rs}, A, P.tw, SmemRows<N, double2>{A});
+  const double2* Z = A;
   const double wn = P.wn[j], ws = P.ws[j];
   double2* XS = P.X + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
   double2* XD = P.X + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
   for (int m = threadIdx.x; m < P.nm; m += blockDim.x) {
     double2 xr[2];
+    const double2 twm = (m > 0 && m < N) ? __ldg(P.tw + m) : make_double2(1.0, 0.0);
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       const double2* z = Z + r * N;
@@ -254,7 +248,7 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fft_fold(sle::Sht
         const double2 e = cscale(cadd(zm, zc), 0.5);
         const double2 dz = csub(zm, zc);
         const double2 o = make_double2(0.5 * dz.y, -0.5 * dz.x);  // (zm - zc) / (2i)
-        xr[r] = cadd(e, cmul(tw[m], o));
+        xr[r] = cadd(e, cmul(twm, o));
       }
     }
     const double2 a = cscale(xr[0], wn);
@@ -266,71 +260,55 @@ __global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_fft_fold(sle::Sht
 
 // Inverse: north spectrum E + O, south E - O (m <= lmax, 0 above), unnormalised inverse
 // real FFT of both rows (sht.py:330-339 with the nlon scaling folded out); field blockIdx.y.
+// The half-length complex packing is formed while the first FFT pass reads its inputs; the last
+// pass writes the output rows (and the optional epilogue out2 = grid * mul2).
 template <int N>
-__global__ void __launch_bounds__((N / 4 > 32) ? N / 4 : 32) k_ifft_unfold(sle::ShtDev P, OutGridPtrs g) {
+struct UnfoldSrc64 {
+  const double2* E;   // [m][j] planes of the field, at latitude j
+  const double2* O;
+  const double2* tw;
+  int nm, nh;
+  __device__ __forceinline__ double2 g(int r, int m) const {
+    if (m >= nm) return make_double2(0.0, 0.0);
+    const double2 e = E[(size_t)m * nh], o = O[(size_t)m * nh];
+    return r ? csub(e, o) : cadd(e, o);
+  }
+  __device__ __forceinline__ double2 operator()(int r, int m) const {
+    double2 x, y;
+    if (m == 0) {
+      x = make_double2(g(r, 0).x, 0.0);
+      y = make_double2(g(r, N).x, 0.0);
+    } else {
+      x = g(r, m);
+      const double2 c = g(r, N - m);
+      y = make_double2(c.x, -c.y);
+    }
+    const double2 e = cadd(x, y);
+    const double2 t = __ldg(tw + m);
+    const double2 wc = make_double2(t.x, -t.y);  // exp(+2 pi i m / nlon)
+    const double2 o = cmul(csub(x, y), wc);
+    return make_double2(e.x - o.y, e.y + o.x);  // e + i o
+  }
+};
+
+template <int N>
+__global__ void __launch_bounds__(fft_nt(N)) k_ifft_unfold(sle::ShtDev P, OutGridPtrs g) {
   extern __shared__ double2 sm[];
-  __shared__ double2 nyq[2];
-  double2* tw = sm;
-  double2* A = sm + N;
-  double2* B = A + 2 * N;
+  double2* A = sm;
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_gated_off(P, f)) return;
   const int js = P.nlat - 1 - j;
-  const double2* E = P.EO + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
-  const double2* O = P.EO + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
-  for (int t = threadIdx.x; t < N; t += blockDim.x) tw[t] = P.tw[t];
-  // stage G into B (rows north, south); G[N] (Nyquist, only when lmax == N) in nyq
-  for (int m = threadIdx.x; m <= N; m += blockDim.x) {
-    double2 gn = make_double2(0.0, 0.0), gs = gn;
-    if (m < P.nm) {
-      const double2 e = E[(size_t)m * P.nh + j];
-      const double2 o = O[(size_t)m * P.nh + j];
-      gn = cadd(e, o);
-      gs = csub(e, o);
-    }
-    if (m < N) {
-      B[m] = gn;
-      B[N + m] = gs;
-    } else {
-      nyq[0] = gn;
-      nyq[1] = gs;
-    }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < 2 * N; idx += blockDim.x) {
-    const int r = idx / N;
-    const int m = idx % N;
-    double2 a, b;
-    if (m == 0) {
-      a = make_double2(B[r * N].x, 0.0);
-      b = make_double2(nyq[r].x, 0.0);
-    } else {
-      a = B[r * N + m];
-      const double2 c = B[r * N + N - m];
-      b = make_double2(c.x, -c.y);
-    }
-    const double2 e = cadd(a, b);
-    const double2 wc = make_double2(tw[m].x, -tw[m].y);  // exp(+2 pi i m / nlon)
-    const double2 o = cmul(csub(a, b), wc);
-    A[r * N + m] = make_double2(e.x - o.y, e.y + o.x);  // e + i o
-  }
-  __syncthreads();
-  const double2* Z = stockham_c<N, 1, true>(A, B, tw);
-  double2* rn = reinterpret_cast<double2*>(g.p[f] + (size_t)j * (2 * N));
-  double2* rs = reinterpret_cast<double2*>(g.p[f] + (size_t)js * (2 * N));
+  const double2* E = P.EO + ((size_t)(f * 2 + 0) * P.nm) * P.nh + j;
+  const double2* O = P.EO + ((size_t)(f * 2 + 1) * P.nm) * P.nh + j;
+  const size_t ro = (size_t)j * (2 * N), rso = (size_t)js * (2 * N);
   double* out2 = g.out2[f];
   const double* mul2 = g.mul2[f];
-  for (int t = threadIdx.x; t < N; t += blockDim.x) {
-    const double2 vn = Z[t], vs = Z[N + t];
-    rn[t] = vn;
-    rs[t] = vs;
-    if (out2) {
-      const double2 mn = reinterpret_cast<const double2*>(mul2 + (size_t)j * (2 * N))[t];
-      const double2 ms = reinterpret_cast<const double2*>(mul2 + (size_t)js * (2 * N))[t];
-      reinterpret_cast<double2*>(out2 + (size_t)j * (2 * N))[t] = make_double2(vn.x * mn.x, vn.y * mn.y);
-      reinterpret_cast<double2*>(out2 + (size_t)js * (2 * N))[t] = make_double2(vs.x * ms.x, vs.y * ms.y);
-    }
-  }
+  GridRowsOut sink{reinterpret_cast<double2*>(g.p[f] + ro), reinterpret_cast<double2*>(g.p[f] + rso),
+                     out2 ? reinterpret_cast<double2*>(out2 + ro) : nullptr,
+                     out2 ? reinterpret_cast<double2*>(out2 + rso) : nullptr,
+                     out2 ? reinterpret_cast<const double2*>(mul2 + ro) : nullptr,
+                     out2 ? reinterpret_cast<const double2*>(mul2 + rso) : nullptr};
+  fft_rows<N, true>(UnfoldSrc64<N>{E, O, P.tw, P.nm, P.nh}, A, P.tw, sink);
 }
 
 
@@ -567,7 +545,7 @@ __global__ void k_unpack(sle::ShtDev P, const double2* packed, double2* dense) {
 }
 
 // ------------------------------------------------------------------------ launchers
-static size_t fft_smem(const ShtDev& d) { return (size_t)5 * d.n2 * sizeof(double2); }
+static size_t fft_smem(const ShtDev& d) { return (size_t)2 * d.n2 * sizeof(double2); }
 static int syn_threads(const ShtDev& d) { return 32 * ((d.ngrp + 1) / 2); }
 static size_t syn_smem(const ShtDev& d) { return (size_t)3 * d.nm * sizeof(double); }
 

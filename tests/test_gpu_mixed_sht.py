@@ -1,0 +1,50 @@
+"""Mixed-precision transforms (split-TF32 tensor-core Legendre contraction) against the FP64 ones.
+
+Bar: 1e-6 of the largest coefficient / grid value for the contraction (3xTF32 with FP32
+accumulation: about 1e-7 in practice), and the FP64 degree-0 coefficient of the analysis and the
+degree-0 term of the synthesis within 1e-13 relative (they bypass the tensor cores).
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+REL_TC = 1e-6
+
+
+def _pair(n, L):
+    from slevolve_b200 import make_sht
+
+    return make_sht("cuda", n, 2 * n, L), make_sht("cuda", n, 2 * n, L, precision="mixed")
+
+
+@pytest.mark.parametrize("n,L", [(64, 63), (128, 127), (256, 255), (512, 511)])
+def test_mixed_analysis_synthesis_against_fp64(n, L):
+    from slevolve_b200.synthetic import band_limited_field
+
+    f64, mx = _pair(n, L)
+    g = band_limited_field(f64, 7, 1, L, 2.0) * 1000.0 + 300.0
+    a64 = f64.analysis(g).copy()
+    amx = mx.analysis(g).copy()
+    ref = np.abs(a64).max()
+    assert np.abs(amx - a64).max() <= REL_TC * ref
+    assert abs(amx[0, 0].real - a64[0, 0].real) <= 1e-13 * abs(a64[0, 0].real)
+    s64 = f64.synthesis(a64).copy()
+    smx = mx.synthesis(a64).copy()
+    assert np.abs(smx - s64).max() <= REL_TC * np.abs(s64).max()
+
+
+def test_mixed_degree0_only_is_fp64():
+    """A field with only the (0,0) coefficient: the mixed synthesis adds it in FP64, so the grid
+    equals the FP64 one to rounding; the mixed analysis of a constant grid gives U_00 in FP64."""
+    f64, mx = _pair(128, 127)
+    c = np.zeros((128, 128), dtype=np.complex128)
+    c[0, 0] = 123.456
+    s64 = f64.synthesis(c).copy()
+    smx = mx.synthesis(c).copy()
+    assert np.abs(smx - s64).max() <= 1e-13 * np.abs(s64).max()
+    g = np.full((128, 256), -3.25)
+    a64 = f64.analysis(g).copy()
+    amx = mx.analysis(g).copy()
+    assert abs(amx[0, 0].real - a64[0, 0].real) <= 1e-13 * abs(a64[0, 0].real)
+    assert np.abs(amx[1:, :]).max() <= 1e-6 * abs(a64[0, 0].real)
