@@ -81,26 +81,42 @@ __device__ __forceinline__ void dft_r(V (&v)[R]) {
   }
 }
 
-// threads per block of the row-FFT kernels (two rows of N points)
-__host__ __device__ constexpr int fft_nt(int n2) { return n2 / 4 > 32 ? n2 / 4 : 32; }
-inline int fft_threads(int n2) { return fft_nt(n2); }
+// Row-FFT blocks transform NR rows of N points (NR = 2: the north and south rows of one
+// latitude pair; NR = 4: two pairs); one radix-8 butterfly per thread and pass.
+__host__ __device__ constexpr int fft_nt(int nr, int n2) { return nr * n2 / 8 > 32 ? nr * n2 / 8 : 32; }
+inline int fft_threads(int nr, int n2) { return fft_nt(nr, n2); }
 
-// Sources and sinks of a pass: (row r in {0 north, 1 south}, index i) -> value.
+// Shared-memory rows are padded by one entry every 8 (16-byte entries), and row r starts r
+// entries further on: the stride-8 writes of the first pass, the unit-stride accesses of the
+// others and same-index accesses to different rows are then free of bank conflicts.
+__host__ __device__ constexpr int fpad(int p) { return p + (p >> 3); }
+inline size_t fft_smem_bytes(int nr, int n2, size_t entry) { return (size_t)(fpad(nr * n2) + 4 * nr + 1) * entry; }
+
+// Sources and sinks of a pass: (row r, index i) -> value.  The row offset is one 16-byte entry
+// (8 per 128-byte bank row) or four 8-byte entries (16 per bank row): rows two apart then land
+// in disjoint halves of the banks.
 template <int N, typename V>
 struct SmemRows {
+  static constexpr int ROFF = sizeof(V) == 16 ? 1 : 4;
   V* a;
-  __device__ __forceinline__ V operator()(int r, int i) const { return a[r * N + i]; }
-  __device__ __forceinline__ void put(int r, int i, V v) const { a[r * N + i] = v; }
+  __device__ __forceinline__ V operator()(int r, int i) const { return a[fpad(r * N + i) + ROFF * r]; }
+  __device__ __forceinline__ void put(int r, int i, V v) const { a[fpad(r * N + i) + ROFF * r] = v; }
 };
+// Grid rows of latitude pairs j0, j0 + 1, ...: row r = north (r even) or south (r odd) row of
+// pair r / 2.  `rowlen` points per row.
 template <typename V>
-struct GlobalRows {
-  const V* n;
-  const V* s;
-  __device__ __forceinline__ V operator()(int r, int i) const { return __ldg((r ? s : n) + i); }
+struct GlobalPairRows {
+  const V* g;
+  int j0, nlat, rowlen;
+  __device__ __forceinline__ V operator()(int r, int i) const {
+    const int j = j0 + (r >> 1);
+    const int row = (r & 1) ? nlat - 1 - j : j;
+    return __ldg(g + (size_t)row * rowlen + i);
+  }
 };
 
-// Output rows of an inverse transform (north row, south row of the grid), with the optional
-// epilogue out2 = grid * mul2 on the same rows (null: none).
+// Output rows of an inverse transform (north row, south row of latitude pair j), with the
+// optional epilogue out2 = grid * mul2 on the same rows (null: none).
 struct GridRowsOut {
   double2* rn;
   double2* rs;
@@ -117,37 +133,40 @@ struct GridRowsOut {
   }
 };
 
-// One pass of radix R, sub-transform size NS before the pass.  ALIAS: the source is the
-// destination buffer (synchronise between the reads and the writes).
-template <int N, int R, int NS, bool INV, bool ALIAS, typename V, typename Src, typename Dst>
+// One pass of radix R over NR rows, sub-transform size NS before the pass.  ALIAS: the source
+// is the destination buffer (synchronise between the reads and the writes).
+template <int NR, int N, int R, int NS, bool INV, bool ALIAS, typename V, typename Src, typename Dst>
 __device__ __forceinline__ void fft_pass(const Src& src, const Dst& dst, const V* __restrict__ tw) {
-  constexpr int NT = fft_nt(N);
+  constexpr int NT = fft_nt(NR, N);
   constexpr int Q = N / R;
-  constexpr int IT = (2 * Q + NT - 1) / NT;
+  constexpr int IT = (NR * Q + NT - 1) / NT;
   constexpr int TSTEP = 2 * N / (NS * R);
   V v[IT][R];
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
     const int idx = threadIdx.x + it * NT;
-    if ((2 * Q) % NT == 0 || idx < 2 * Q) {
+    if ((NR * Q) % NT == 0 || idx < NR * Q) {
       const int r = idx / Q, j = idx % Q;
       const int k = j % NS;
-#pragma unroll
-      for (int u = 0; u < R; ++u) v[it][u] = src(r, j + u * Q);
+      V w[R];
       if (NS > 1) {
 #pragma unroll
         for (int u = 1; u < R; ++u) {
           const int t = u * k * TSTEP;
-          V w;
           if (t < N) {
-            w = __ldg(tw + t);
+            w[u] = __ldg(tw + t);
           } else {
-            w = __ldg(tw + (t - N));
-            w = mkc(-w.x, -w.y);
+            w[u] = __ldg(tw + (t - N));
+            w[u] = mkc(-w[u].x, -w[u].y);
           }
-          if (INV) w.y = -w.y;
-          v[it][u] = cmul(v[it][u], w);
+          if (INV) w[u].y = -w[u].y;
         }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) v[it][u] = src(r, j + u * Q);
+      if (NS > 1) {
+#pragma unroll
+        for (int u = 1; u < R; ++u) v[it][u] = cmul(v[it][u], w[u]);
       }
     }
   }
@@ -155,7 +174,7 @@ __device__ __forceinline__ void fft_pass(const Src& src, const Dst& dst, const V
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
     const int idx = threadIdx.x + it * NT;
-    if ((2 * Q) % NT == 0 || idx < 2 * Q) {
+    if ((NR * Q) % NT == 0 || idx < NR * Q) {
       const int r = idx / Q, j = idx % Q;
       const int k = j % NS;
       dft_r<R, INV>(v[it]);
@@ -173,29 +192,29 @@ struct FftRadix {
 };
 
 // Passes NS .. N of the transform held in A (shared memory), the last one into `sink`.
-template <int N, int NS, bool INV, typename V, typename Sink>
+template <int NR, int N, int NS, bool INV, typename V, typename Sink>
 __device__ __forceinline__ void fft_rest(V* A, const V* tw, const Sink& sink) {
   if constexpr (NS < N) {
     constexpr int R = FftRadix<N, NS>::R;
     if constexpr (NS * R >= N) {
-      fft_pass<N, R, NS, INV, false>(SmemRows<N, V>{A}, sink, tw);
+      fft_pass<NR, N, R, NS, INV, false>(SmemRows<N, V>{A}, sink, tw);
     } else {
-      fft_pass<N, R, NS, INV, true>(SmemRows<N, V>{A}, SmemRows<N, V>{A}, tw);
-      fft_rest<N, NS * R, INV>(A, tw, sink);
+      fft_pass<NR, N, R, NS, INV, true>(SmemRows<N, V>{A}, SmemRows<N, V>{A}, tw);
+      fft_rest<NR, N, NS * R, INV>(A, tw, sink);
     }
   }
 }
 
-// Whole transform: first pass from `src` into A, the rest in place, the last pass into `sink`
-// (SmemRows{A} to keep the result in A).  N >= 2.
-template <int N, bool INV, typename V, typename Src, typename Sink>
+// Whole transform of NR rows: first pass from `src` into A, the rest in place, the last pass
+// into `sink` (SmemRows{A} to keep the result in A).  N >= 2.
+template <int NR, int N, bool INV, typename V, typename Src, typename Sink>
 __device__ __forceinline__ void fft_rows(const Src& src, V* A, const V* tw, const Sink& sink) {
   constexpr int R = FftRadix<N, 1>::R;
   if constexpr (R >= N) {
-    fft_pass<N, R, 1, INV, false>(src, sink, tw);
+    fft_pass<NR, N, R, 1, INV, false>(src, sink, tw);
   } else {
-    fft_pass<N, R, 1, INV, false>(src, SmemRows<N, V>{A}, tw);
-    fft_rest<N, R, INV>(A, tw, sink);
+    fft_pass<NR, N, R, 1, INV, false>(src, SmemRows<N, V>{A}, tw);
+    fft_rest<NR, N, R, INV>(A, tw, sink);
   }
 }
 

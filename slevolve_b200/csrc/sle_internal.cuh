@@ -67,7 +67,8 @@ struct ShtDev {
   const int* gset[MAXF];
   const int* gclr[MAXF];
   // mixed-precision transforms (set once the plan prepared them)
-  float* mx_xf;               // [MX_MAXF][nh][nm][4] folded FP32 rFFT (S.re, S.im, D.re, D.im)
+  const float2* twf;          // [n2] FP32 twiddles of the mixed-precision row FFTs
+  float* mx_xf;               // [MX_MAXF][nm][nh][4] folded FP32 rFFT (S.re, S.im, D.re, D.im)
   float2* mx_gns;             // [MX_MAXF][nh][nm][2] north / south Legendre sums (synthesis)
   float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (tile order)
   double* mx_s0;              // [MX_MAXF][nh] FP64 fold of the row sums (degree 0)
@@ -75,7 +76,7 @@ struct ShtDev {
   const int4* mx_ana_units;   // (m, span, first chunk, table slot) analysis units, most work first
   const int4* mx_syn_units;   // (m, latitude tile, chunks, table slot) synthesis units
   const int* mx_syn_seg;      // segment of each synthesis table slot
-  const uint32_t* mx_tab_ana; // Legendre tables: [slot][par][hi/lo][128][32] TF32, tile order
+  const uint32_t* mx_tab_ana; // Legendre tables: [slot][par][128][32] FP32, tile order
   const uint32_t* mx_tab_syn;
 };
 
@@ -128,6 +129,7 @@ struct sle_sht {
   // mixed-precision transform buffers (allocated on first use)
   int mx_ready;
   float* mx_xf;
+  float2* mx_twf;
   float2* mx_gns;
   float* mx_bsyn;
   double* mx_s0;

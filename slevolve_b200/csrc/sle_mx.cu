@@ -61,6 +61,8 @@ constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wa
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t SET_COLS = 256;            // two accumulator sets (units alternate)
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
+constexpr int MAX_CTA_UNITS = 16;             // work units per CTA staged in shared memory
+static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
 
 static_assert(MX_SMEM <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
 
@@ -265,6 +267,7 @@ struct Misc {
   uint32_t* tmem_holder;
   int* active;          // [MX_MAXF]
   int* any;
+  int4* units;          // [MAX_CTA_UNITS]: this CTA's work units, staged by the prologue
   __device__ uint32_t b(int i) const { return smem_u32(bar + i); }
 };
 __device__ __forceinline__ Misc misc_layout(const Smem& S) {
@@ -274,6 +277,7 @@ __device__ __forceinline__ Misc misc_layout(const Smem& S) {
   m.tmem_holder = reinterpret_cast<uint32_t*>(p + 128);
   m.active = reinterpret_cast<int*>(p + 256);
   m.any = reinterpret_cast<int*>(p + 256 + 4 * MX_MAXF);
+  m.units = reinterpret_cast<int4*>(p + 512);
   return m;
 }
 
@@ -286,23 +290,29 @@ __device__ __forceinline__ int main_buffers(int nch, int ncols) {
   return max(1, min(nch, ((int)SET_COLS - 2 * ncols) / (2 * ncols)));
 }
 
-// MMAs of one chunk (stage st) into the set at `set_base`; chunk k of its unit.
+// MMAs of one chunk (stage st) into the set at `set_base`; chunk k of its unit.  The K sub-block
+// kk starts 32 kk bytes into the tile rows: +2 kk in the descriptor's start-address field.
 __device__ __forceinline__ void mma_chunk(const Smem& S, uint32_t set_base, int st, int k, int nbuf, int ncols) {
   const uint32_t idesc = idesc_tf32(128, ncols);
   const uint32_t dmain = set_base + (uint32_t)(2 * ncols * (1 + k % nbuf));
   const bool fresh = k < nbuf;
+  uint64_t ah[2], al[2], bh[2], bl[2];
+#pragma unroll
+  for (int par = 0; par < 2; ++par) {
+    ah[par] = sdesc_sw128(S.a_tile(st, par, 0));
+    al[par] = sdesc_sw128(S.a_tile(st, par, 1));
+    bh[par] = sdesc_sw128(S.b_tile(st, par, 0));
+    bl[par] = sdesc_sw128(S.b_tile(st, par, 1));
+  }
 #pragma unroll
   for (int kk = 0; kk < KC / 8; ++kk) {
 #pragma unroll
     for (int par = 0; par < 2; ++par) {
-      const uint64_t ah = sdesc_sw128(S.a_tile(st, par, 0) + 32 * kk);
-      const uint64_t al = sdesc_sw128(S.a_tile(st, par, 1) + 32 * kk);
-      const uint64_t bh = sdesc_sw128(S.b_tile(st, par, 0) + 32 * kk);
-      const uint64_t bl = sdesc_sw128(S.b_tile(st, par, 1) + 32 * kk);
+      const uint64_t d = (uint64_t)(2 * kk);
       const uint32_t off = (uint32_t)(par * ncols);
-      tc_mma_tf32(dmain + off, ah, bh, idesc, (fresh && kk == 0) ? 0u : 1u);
-      tc_mma_tf32(set_base + off, ah, bl, idesc, (k == 0 && kk == 0) ? 0u : 1u);
-      tc_mma_tf32(set_base + off, al, bh, idesc, 1u);
+      tc_mma_tf32(dmain + off, ah[par] + d, bh[par] + d, idesc, (fresh && kk == 0) ? 0u : 1u);
+      tc_mma_tf32(set_base + off, ah[par] + d, bl[par] + d, idesc, (k == 0 && kk == 0) ? 0u : 1u);
+      tc_mma_tf32(set_base + off, al[par] + d, bh[par] + d, idesc, 1u);
     }
   }
 }
@@ -335,8 +345,12 @@ __device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int ncols, 
 }
 
 // Common prologue: barriers, gates, TMEM.  Returns the TMEM base (all threads).
-__device__ uint32_t prologue(const Misc& M, const MxFieldArgs& a) {
+__device__ uint32_t prologue(const Misc& M, const MxFieldArgs& a, const int4* units, int nunits) {
   const int warp = threadIdx.x >> 5;
+  if (threadIdx.x < MAX_CTA_UNITS) {
+    const int u = blockIdx.x + threadIdx.x * gridDim.x;
+    if (u < nunits) M.units[threadIdx.x] = units[u];
+  }
   if (threadIdx.x == 0) {
     for (int i = 0; i < 2; ++i) {
       mbar_init(M.b(BAR_FULL + i), 4);    // the 4 splitter warps of the stage
@@ -457,18 +471,21 @@ __global__ void __launch_bounds__(128) k_tab_syn(ShtDev P, uint32_t* tab) {
 // A split: the FP32 Legendre values landed in the hi tiles of the stage; hi <- TF32(x) in
 // place, lo tile <- TF32(x - hi).  Elementwise, so the tile order does not matter.
 __device__ __forceinline__ void split_a(const Smem& S, int st, int tid) {
+  constexpr int NV = SLOT_WORDS / 4 / 128;   // 16-byte vectors per thread
   uint4* hp = reinterpret_cast<uint4*>(S.a_ptr(st, 0, 0));
   uint4* lp = reinterpret_cast<uint4*>(S.a_ptr(st, 0, 1));
-#pragma unroll 4
-  for (int e = tid; e < SLOT_WORDS / 4; e += 128) {
-    const uint4 v = hp[e];
+  uint4 v[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = hp[tid + 128 * q];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
     uint4 h, l;
-    split_f32(__uint_as_float(v.x), h.x, l.x);
-    split_f32(__uint_as_float(v.y), h.y, l.y);
-    split_f32(__uint_as_float(v.z), h.z, l.z);
-    split_f32(__uint_as_float(v.w), h.w, l.w);
-    hp[e] = h;
-    lp[e] = l;
+    split_f32(__uint_as_float(v[q].x), h.x, l.x);
+    split_f32(__uint_as_float(v[q].y), h.y, l.y);
+    split_f32(__uint_as_float(v[q].z), h.z, l.z);
+    split_f32(__uint_as_float(v[q].w), h.w, l.w);
+    hp[tid + 128 * q] = h;
+    lp[tid + 128 * q] = l;
   }
 }
 
@@ -525,10 +542,10 @@ __device__ __forceinline__ void split_b_syn(const Smem& S, int st, int nrow, int
   }
 }
 
-// Work unit u: (m, span | latitude tile, chunk count, first table slot).
+// Work unit u (the CTA's i-th): (m, span | latitude tile, chunk count, first table slot).
 template <bool SYN>
-__device__ __forceinline__ void unit_info(const ShtDev& P, int u, int4& unit, int& nch) {
-  unit = SYN ? P.mx_syn_units[u] : P.mx_ana_units[u];
+__device__ __forceinline__ void unit_info(const ShtDev& P, const Misc& M, int u, int i, int4& unit, int& nch) {
+  unit = (i < MAX_CTA_UNITS) ? M.units[i] : (SYN ? P.mx_syn_units[u] : P.mx_ana_units[u]);
   nch = SYN ? unit.z : P.ngrp - unit.z;
 }
 
@@ -548,19 +565,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int L = P.lmax;
   const int ncols = a.ncols;
   const uint32_t* tab = SYN ? P.mx_tab_syn : P.mx_tab_ana;
-  const uint32_t tmem = prologue(M, a);
+  const uint32_t tmem = prologue(M, a, SYN ? P.mx_syn_units : P.mx_ana_units, nunits);
   if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
     const int nrow = 2 * a.nf;
     if (warp == W_LOAD) {
       // ---- loader: chunk c of the CTA's sequence into stage c & 1
       if (lane == 0) {
         const uint32_t bbytes = SYN ? 2u * (uint32_t)nrow * 128u : (uint32_t)zbox * 32u * 16u;
-        int c = 0;
+        int c = 0, i = 0;
         bool ok = true;
-        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
           int4 unit;
           int nch;
-          unit_info<SYN>(P, u, unit, nch);
+          unit_info<SYN>(P, M, u, i, unit, nch);
           for (int k = 0; k < nch; ++k, ++c) {
             const int st = c & 1;
             if (!mbar_wait(M.b(BAR_EMPTY + st), (uint32_t)(((c >> 1) & 1) ^ 1), ab)) {
@@ -575,7 +592,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
               bulk_g2s(S.b_tile(st, 0, 1), P.mx_bsyn + ((size_t)seg * 2 + 0) * BBLOCK, (uint32_t)nrow * 128u, raw);
               bulk_g2s(S.b_tile(st, 1, 1), P.mx_bsyn + ((size_t)seg * 2 + 1) * BBLOCK, (uint32_t)nrow * 128u, raw);
             } else {
-              tma_load_3d(S.b_tile(st, 0, 1), &tmx, 4 * unit.x, KC * (unit.z + k), 0, raw);
+              tma_load_3d(S.b_tile(st, 0, 1), &tmx, 4 * KC * (unit.z + k), unit.x, 0, raw);
             }
           }
         }
@@ -593,7 +610,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
           int4 unit;
           int nch;
-          unit_info<SYN>(P, u, unit, nch);
+          unit_info<SYN>(P, M, u, i, unit, nch);
           const int set = i & 1;
           if (!mbar_wait(M.b(BAR_TFREE + set), (uint32_t)(((i >> 1) & 1) ^ 1), ab)) break;
           tc_fence_after();
@@ -624,12 +641,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else if (warp >= W_SPL) {
       // ---- splitters: group g = stage g
       const int g = (warp - W_SPL) >> 2, tid = threadIdx.x - 32 * W_SPL - 128 * g;
-      int c = 0;
+      int c = 0, i = 0;
       bool ok = true;
-      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
         int4 unit;
         int nch;
-        unit_info<SYN>(P, u, unit, nch);
+        unit_info<SYN>(P, M, u, i, unit, nch);
         for (int k = 0; k < nch; ++k, ++c) {
           if ((c & 1) != g) continue;
           // every wait is bounded, so all four warps of the group reach the vote; they go on
@@ -655,7 +672,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       for (int u = blockIdx.x; u < nunits; u += gridDim.x, ++i) {
         int4 unit;
         int nch;
-        unit_info<SYN>(P, u, unit, nch);
+        unit_info<SYN>(P, M, u, i, unit, nch);
         const int set = i & 1, m = unit.x;
         const bool w = mbar_wait(M.b(BAR_ACCUM + set), (uint32_t)((i >> 1) & 1), ab);
         if (!__all_sync(0xffffffffu, w)) break;
@@ -688,14 +705,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
           }
         }
-        if (!SYN) {
-          // degree 0 in FP64 from the row sums of the fold: U_00 = sqrt(0.5) sum_j S_0(j) / 1.41421356
+        if (!SYN && m == 0 && unit.y == 0) {
+          // degree 0 in FP64 from the row sums of the fold: U_00 = sqrt(0.5) sum_j S_0(j) / 1.41421356;
+          // warp w sums the fields w, w + 4, ... (lane-strided partial sums, then a fixed
+          // butterfly: the same order in every launch)
           __syncwarp();
-          if (m == 0 && unit.y == 0 && warp == 0 && lane < a.nf && M.active[lane]) {
-            const double* s0 = P.mx_s0 + (size_t)lane * P.nh;
+          for (int f = warp; f < a.nf; f += 4) {
+            if (!M.active[f]) continue;
+            const double* s0 = P.mx_s0 + (size_t)f * P.nh;
             double acc = 0.0;
-            for (int jj = 0; jj < P.nh; ++jj) acc += s0[jj];
-            a.spec[lane][0] = make_double2(__dmul_rn(__dsqrt_rn(0.5), acc) / SQRT2_LEGACY, 0.0);
+            for (int jj = lane; jj < P.nh; jj += 32) acc += s0[jj];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) a.spec[f][0] = make_double2(__dmul_rn(__dsqrt_rn(0.5), acc) / SQRT2_LEGACY, 0.0);
           }
         }
         tc_fence_before();
@@ -708,90 +730,141 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 // ============================================================== row FFT kernels
-// Row rFFT (FP64) of the north row j and south row nlat-1-j of field blockIdx.y, fold with the
-// weights (FP64), output rounded to FP32: X[f][j][m] = (S.re, S.im, D.re, D.im), one 16-byte
-// entry per order (coalesced), the layout the analysis kernel's TMA box reads.  The m = 0 fold
-// (row sums) is also kept in FP64 in s0[f][j] for the FP64 degree-0 coefficient.
-template <int N>
-__global__ void __launch_bounds__(fft_nt(N)) k_fold_mx(ShtDev P, MxFieldArgs a) {
-  extern __shared__ double2 smd2[];
-  double2* A = smd2;
-  const int j = blockIdx.x, f = blockIdx.y;
-  if (field_off(a, f)) return;
-  const int js = P.nlat - 1 - j;
-  const double2* rn = reinterpret_cast<const double2*>(a.grid[f] + (size_t)j * (2 * N));
-  const double2* rs = reinterpret_cast<const double2*>(a.grid[f] + (size_t)js * (2 * N));
-  fft_rows<N, false>(GlobalRows<double2>{rn, rs}, A, P.tw, SmemRows<N, double2>{A});
-  const double2* Z = A;
-  const double wn = P.wn[j], ws = P.ws[j];
-  float4* X = reinterpret_cast<float4*>(P.mx_xf) + ((size_t)f * P.nh + j) * P.nm;
-  for (int m = threadIdx.x; m < P.nm; m += blockDim.x) {
-    double2 xr[2];
-    const double2 twm = (m > 0 && m < N) ? __ldg(P.tw + m) : make_double2(1.0, 0.0);
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const double2* z = Z + r * N;
-      if (m == 0) {
-        xr[r] = make_double2(z[0].x + z[0].y, 0.0);
-      } else if (m == N) {
-        xr[r] = make_double2(z[0].x - z[0].y, 0.0);
-      } else {
-        const double2 zm = z[m];
-        const double2 zc = make_double2(z[N - m].x, -z[N - m].y);
-        const double2 e = cscale(cadd(zm, zc), 0.5);
-        const double2 dz = csub(zm, zc);
-        const double2 o = make_double2(0.5 * dz.y, -0.5 * dz.x);  // (zm - zc) / (2i)
-        xr[r] = cadd(e, cmul(twm, o));
-      }
-    }
-    const double2 an = cscale(xr[0], wn), bs = cscale(xr[1], ws);
-    if (m == 0) P.mx_s0[(size_t)f * P.nh + j] = an.x + bs.x;
-    X[m] = make_float4((float)(an.x + bs.x), (float)(an.y + bs.y), (float)(an.x - bs.x), (float)(an.y - bs.y));
-  }
-}
-
-// Inverse: north and south Legendre sums of field blockIdx.y (FP32 accumulators, m <= lmax, 0
-// above; one 16-byte entry per order), unnormalised inverse real FFT in FP64, plus the FP64
-// degree-0 term 1.41421356 sqrt(0.5) Re U_00 in every cell; optional epilogue out2 = grid * mul2.
-// The half-length complex packing of the real inverse transform is computed while the first
-// FFT pass reads its inputs; the last pass writes the output rows.
-template <int N>
-struct UnfoldSrcMx {
-  const float4* G;   // [m] of this latitude pair
-  const double2* tw;
-  int nm;
-  double c00;
-  __device__ __forceinline__ double2 g(int r, int m) const {
-    double2 x = make_double2(0.0, 0.0);
-    if (m < nm) {
-      const float4 v = __ldg(G + m);
-      x = r ? make_double2(v.z, v.w) : make_double2(v.x, v.y);
-    }
-    if (m == 0) x.x += c00;
-    return x;
-  }
-  __device__ __forceinline__ double2 operator()(int r, int m) const {
-    double2 x, y;
-    if (m == 0) {
-      x = make_double2(g(r, 0).x, 0.0);
-      y = make_double2(g(r, N).x, 0.0);
-    } else {
-      x = g(r, m);
-      const double2 c = g(r, N - m);
-      y = make_double2(c.x, -c.y);
-    }
-    const double2 e = cadd(x, y);
-    const double2 t = __ldg(tw + m);
-    const double2 wc = make_double2(t.x, -t.y);  // exp(+2 pi i m / nlon)
-    const double2 o = cmul(csub(x, y), wc);
-    return make_double2(e.x - o.y, e.y + o.x);  // e + i o
+// Row rFFT in FP32 of the north and south rows of latitudes j0 = 2 blockIdx.x and j0 + 1 of
+// field blockIdx.y and the fold with the weights, output FP32: X[f][m][j] = (S.re, S.im, D.re,
+// D.im), 16 bytes per entry, latitude fastest (the two latitudes of a block fill one 32-byte
+// sector), the layout whose 32-latitude rows the analysis kernel's TMA box reads.  The m = 0
+// fold (the weighted row sums) is formed in FP64 from the FP64 grid values, in s0[f][j], for the
+// FP64 degree-0 coefficient.
+struct FoldSrcMx {
+  const double2* g;
+  int j0, nlat, rowlen;
+  double* acc;          // this thread's FP64 sum of the values it reads (one row per thread)
+  __device__ __forceinline__ float2 operator()(int r, int i) const {
+    const int j = j0 + (r >> 1);
+    const int row = (r & 1) ? nlat - 1 - j : j;
+    const double2 v = __ldg(g + (size_t)row * rowlen + i);
+    *acc = (*acc + v.x) + v.y;
+    return make_float2((float)v.x, (float)v.y);
   }
 };
 
 template <int N>
-__global__ void __launch_bounds__(fft_nt(N)) k_unfold_mx(ShtDev P, MxFieldArgs a) {
-  extern __shared__ double2 smd2[];
-  double2* A = smd2;
+__global__ void __launch_bounds__(fft_nt(4, N)) k_fold_mx(ShtDev P, MxFieldArgs a) {
+  extern __shared__ float2 smf2[];
+  float2* A = smf2;
+  const int j0 = 2 * blockIdx.x, f = blockIdx.y;
+  if (field_off(a, f)) return;
+  constexpr int NT = fft_nt(4, N);
+  constexpr int Q = N / FftRadix<N, 1>::R;   // first-pass items per row: one per thread
+  double acc = 0.0;
+  fft_rows<4, N, false>(FoldSrcMx{reinterpret_cast<const double2*>(a.grid[f]), j0, P.nlat, N, &acc}, A, P.twf,
+                        SmemRows<N, float2>{A});
+  // FP64 row sums: the Q threads r Q .. r Q + Q - 1 hold the partial sums of row r (Q a power
+  // of two): a butterfly within aligned groups of min(Q, 32) lanes, then the warps of a row in
+  // order
+  __shared__ double rowtot[4];
+  {
+    const int t = threadIdx.x;
+    double v = (t < 4 * Q) ? acc : 0.0;
+    constexpr int W = Q < 32 ? Q : 32;
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if constexpr (Q <= 32) {
+      if (t < 4 * Q && t % Q == 0) rowtot[t / Q] = v;
+    } else {
+      __shared__ double wsum[NT / 32];
+      if ((t & 31) == 0) wsum[t >> 5] = v;
+      __syncthreads();
+      if (t < 4) {
+        double sum = 0.0;
+        for (int w = t * (Q / 32); w < (t + 1) * (Q / 32); ++w) sum += wsum[w];
+        rowtot[t] = sum;
+      }
+    }
+    __syncthreads();
+  }
+  const SmemRows<N, float2> Z{A};
+  float4* X = reinterpret_cast<float4*>(P.mx_xf) + (size_t)f * P.nm * P.nh;
+  for (int e = threadIdx.x; e < 2 * P.nm; e += NT) {
+    // consecutive threads: the two latitudes of one order (one 32-byte sector of X)
+    const int m = e >> 1, q = e & 1, j = j0 + q;
+    float2 xr[2];
+    const float2 twm = (m > 0 && m < N) ? __ldg(P.twf + m) : make_float2(1.f, 0.f);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = 2 * q + h;
+      const float2 z0 = Z(r, 0);
+      if (m == 0) {
+        xr[h] = make_float2(z0.x + z0.y, 0.f);
+      } else if (m == N) {
+        xr[h] = make_float2(z0.x - z0.y, 0.f);
+      } else {
+        const float2 zm = Z(r, m);
+        const float2 zn = Z(r, N - m);
+        const float2 zc = make_float2(zn.x, -zn.y);
+        const float2 ev = cscale(cadd(zm, zc), 0.5f);
+        const float2 dz = csub(zm, zc);
+        const float2 o = make_float2(0.5f * dz.y, -0.5f * dz.x);  // (zm - zc) / (2i)
+        xr[h] = cadd(ev, cmul(twm, o));
+      }
+    }
+    const double wn = P.wn[j], ws = P.ws[j];
+    const float2 an = cscale(xr[0], (float)wn), bs = cscale(xr[1], (float)ws);
+    if (m == 0) {
+      // S_0(j) in FP64: the weighted sums of the north and south rows of latitude j
+      P.mx_s0[(size_t)f * P.nh + j] = wn * rowtot[2 * q] + ws * rowtot[2 * q + 1];
+    }
+    X[(size_t)m * P.nh + j] = make_float4(an.x + bs.x, an.y + bs.y, an.x - bs.x, an.y - bs.y);
+  }
+}
+
+// Inverse: north and south Legendre sums of field blockIdx.y (FP32, m <= lmax, 0 above; one
+// 16-byte entry per order), unnormalised inverse real FFT in FP32; the output rows get the FP64
+// degree-0 term 1.41421356 sqrt(0.5) Re U_00 added in FP64; optional epilogue out2 = grid * mul2.
+// The half-length complex packing of the real inverse transform is formed while the first FFT
+// pass reads its inputs; the last pass writes the output rows.
+template <int N>
+struct UnfoldSrcMx {
+  const float4* G;   // [m] of this latitude pair
+  const float2* tw;
+  int nm;
+  __device__ __forceinline__ float2 g(int r, int m) const {
+    if (m >= nm) return make_float2(0.f, 0.f);
+    const float4 v = __ldg(G + m);
+    return r ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+  }
+  __device__ __forceinline__ float2 operator()(int r, int m) const {
+    float2 x, y;
+    if (m == 0) {
+      x = make_float2(g(r, 0).x, 0.f);
+      y = make_float2(g(r, N).x, 0.f);
+    } else {
+      x = g(r, m);
+      const float2 c = g(r, N - m);
+      y = make_float2(c.x, -c.y);
+    }
+    const float2 e = cadd(x, y);
+    const float2 t = __ldg(tw + m);
+    const float2 wc = make_float2(t.x, -t.y);  // exp(+2 pi i m / nlon)
+    const float2 o = cmul(csub(x, y), wc);
+    return make_float2(e.x - o.y, e.y + o.x);  // e + i o
+  }
+};
+
+// FP32 values of the inverse FFT -> FP64 grid rows plus the degree-0 term.
+struct GridRowsOutMx {
+  GridRowsOut out;
+  double c00;
+  __device__ __forceinline__ void put(int r, int i, float2 v) const {
+    out.put(r, i, make_double2((double)v.x + c00, (double)v.y + c00));
+  }
+};
+
+template <int N>
+__global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArgs a) {
+  extern __shared__ float2 smf2[];
+  float2* A = smf2;
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
   const int js = P.nlat - 1 - j;
@@ -800,12 +873,12 @@ __global__ void __launch_bounds__(fft_nt(N)) k_unfold_mx(ShtDev P, MxFieldArgs a
   const size_t ro = (size_t)j * (2 * N), rso = (size_t)js * (2 * N);
   double* out2 = a.epi_out[f];
   const double* mul2 = a.epi_mul[f];
-  GridRowsOut sink{reinterpret_cast<double2*>(a.grid[f] + ro), reinterpret_cast<double2*>(a.grid[f] + rso),
-                   out2 ? reinterpret_cast<double2*>(out2 + ro) : nullptr,
-                   out2 ? reinterpret_cast<double2*>(out2 + rso) : nullptr,
-                   out2 ? reinterpret_cast<const double2*>(mul2 + ro) : nullptr,
-                   out2 ? reinterpret_cast<const double2*>(mul2 + rso) : nullptr};
-  fft_rows<N, true>(UnfoldSrcMx<N>{G, P.tw, P.nm, c00}, A, P.tw, sink);
+  const GridRowsOut rows{reinterpret_cast<double2*>(a.grid[f] + ro), reinterpret_cast<double2*>(a.grid[f] + rso),
+                         out2 ? reinterpret_cast<double2*>(out2 + ro) : nullptr,
+                         out2 ? reinterpret_cast<double2*>(out2 + rso) : nullptr,
+                         out2 ? reinterpret_cast<const double2*>(mul2 + ro) : nullptr,
+                         out2 ? reinterpret_cast<const double2*>(mul2 + rso) : nullptr};
+  fft_rows<2, N, true>(UnfoldSrcMx<N>{G, P.twf, P.nm}, A, P.twf, GridRowsOutMx{rows, c00});
 }
 
 // Synthesis B operand: per segment s (order m, degrees l0..l0+63) and parity, rows 2f / 2f+1 =
@@ -827,7 +900,8 @@ __global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
   blk[sw_off(2 * f + 1, k)] = (float)(u.y * SQRT2_LEGACY);
 }
 
-size_t mx_fft_smem(const ShtDev& d) { return (size_t)2 * d.n2 * sizeof(double2); }
+size_t mx_fold_smem(const ShtDev& d) { return fft_smem_bytes(4, d.n2, sizeof(float2)); }
+size_t mx_unfold_smem(const ShtDev& d) { return fft_smem_bytes(2, d.n2, sizeof(float2)); }
 
 template <typename T>
 int mx_alloc(T** p, size_t n) {
@@ -880,6 +954,15 @@ int sht_mx_prepare(sle_sht* p) {
   SLE_CUDA(cudaMemset(p->mx_gns, 0, 2 * nx4 * sizeof(float2)));
   SLE_CUDA(cudaMemset(p->mx_bsyn, 0, (size_t)d.nseg * 2 * BBLOCK * sizeof(float)));
   SLE_CUDA(cudaMemset(p->mx_abort, 0, sizeof(int)));
+  {
+    // FP32 twiddles exp(-2 pi i t / nlon), rounded from the plan's FP64 ones
+    std::vector<double2> tw64(d.n2);
+    std::vector<float2> tw32(d.n2);
+    SLE_CUDA(cudaMemcpy(tw64.data(), p->tw, d.n2 * sizeof(double2), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < d.n2; ++t) tw32[t] = make_float2((float)tw64[t].x, (float)tw64[t].y);
+    SLE_TRY(mx_alloc(&p->mx_twf, (size_t)d.n2));
+    SLE_CUDA(cudaMemcpy(p->mx_twf, tw32.data(), d.n2 * sizeof(float2), cudaMemcpyHostToDevice));
+  }
   // work units, most work first; each unit's chunks are contiguous slots of its Legendre table
   std::vector<unsigned char> ist(d.nseg);
   std::vector<int> segoff(d.nm + 1);
@@ -938,6 +1021,7 @@ int sht_mx_prepare(sle_sht* p) {
   SLE_CUDA(cudaMemset(p->mx_tab_ana, 0, tab_a * sizeof(uint32_t)));
   SLE_CUDA(cudaMemset(p->mx_tab_syn, 0, tab_s * sizeof(uint32_t)));
   p->mx_table_bytes = (double)(tab_a + tab_s) * sizeof(uint32_t);
+  d.twf = p->mx_twf;
   d.mx_xf = p->mx_xf;
   d.mx_gns = p->mx_gns;
   d.mx_bsyn = p->mx_bsyn;
@@ -952,16 +1036,17 @@ int sht_mx_prepare(sle_sht* p) {
   k_tab_syn<<<p->n_syn_units, 128>>>(d, p->mx_tab_syn);
   SLE_CUDA(cudaGetLastError());
   SLE_CUDA(cudaDeviceSynchronize());
-  // TMA maps of X: dims (4 nm floats, nh latitudes, MX_MAXF fields), boxes (4, 32, 8 | 16 | 32)
+  // TMA maps of X[f][m][j][4]: dims (4 nh floats, nm orders, MX_MAXF fields), boxes (4 x 32
+  // latitudes, 1 order, 8 | 16 | 32 fields)
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled is not available from the driver");
     return SLE_ERR_CUDA;
   }
   for (int zi = 0; zi < 3; ++zi) {
-    const cuuint64_t dims[3] = {(cuuint64_t)4 * d.nm, (cuuint64_t)d.nh, (cuuint64_t)MX_MAXF};
-    const cuuint64_t strides[2] = {(cuuint64_t)16 * d.nm, (cuuint64_t)16 * d.nm * d.nh};
-    const cuuint32_t box[3] = {4, (cuuint32_t)KC, (cuuint32_t)ZBOX[zi]};
+    const cuuint64_t dims[3] = {(cuuint64_t)4 * d.nh, (cuuint64_t)d.nm, (cuuint64_t)MX_MAXF};
+    const cuuint64_t strides[2] = {(cuuint64_t)16 * d.nh, (cuuint64_t)16 * d.nh * d.nm};
+    const cuuint32_t box[3] = {4 * KC, 1, (cuuint32_t)ZBOX[zi]};
     const cuuint32_t estr[3] = {1, 1, 1};
     const CUresult r = enc(reinterpret_cast<CUtensorMap*>(p->mx_tmap[zi]), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
                            p->mx_xf, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -982,8 +1067,10 @@ int sht_mx_prepare(sle_sht* p) {
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
 #define SLE_ATTR_MX(NN)                                                                                        \
   do {                                                                                                         \
-    SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_fft_smem(d))); \
-    SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_fft_smem(d))); \
+    SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_fold_smem(d)));          \
+    SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
+    SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_unfold_smem(d)));      \
+    SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
   } while (0)
   SLE_FFT_SWITCH(d.n2, SLE_ATTR_MX)
 #undef SLE_ATTR_MX
@@ -1012,7 +1099,7 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t
   SLE_TRY(mx_check_args(a, "mixed analysis"));
   const ShtDev& d = p->d;
   ProfToken t0 = prof_begin(PROF_FFT, a.nf, st);
-#define SLE_LAUNCH_MXF(NN) k_fold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(NN), mx_fft_smem(d), st>>>(d, a)
+#define SLE_LAUNCH_MXF(NN) k_fold_mx<NN><<<dim3(d.nh / 2, a.nf), fft_threads(4, NN), mx_fold_smem(d), st>>>(d, a)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXF)
 #undef SLE_LAUNCH_MXF
   prof_end(t0, st);
@@ -1040,7 +1127,7 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_
                                                                              p->n_syn_units);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
-#define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(NN), mx_fft_smem(d), st>>>(d, a)
+#define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXU)
 #undef SLE_LAUNCH_MXU
   prof_end(t1, st);

@@ -219,16 +219,14 @@ struct CSpecPtrs {
 // S = F_N w_j/nlon + F_S w_j/nlon, D = F_N w_j/nlon - F_S w_j/nlon for m <= lmax
 // (sht.py:277-287).  X layout [f][0=S,1=D][m][j].  N = nlon/2 complex points per row.
 template <int N>
-__global__ void __launch_bounds__(fft_nt(N)) k_fft_fold(sle::ShtDev P, GridPtrs g) {
+__global__ void __launch_bounds__(fft_nt(2, N)) k_fft_fold(sle::ShtDev P, GridPtrs g) {
   extern __shared__ double2 sm[];
   double2* A = sm;
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_gated_off(P, f)) return;
-  const int js = P.nlat - 1 - j;
-  const double2* rn = reinterpret_cast<const double2*>(g.p[f] + (size_t)j * (2 * N));
-  const double2* rs = reinterpret_cast<const double2*>(g.p[f] + (size_t)js * (2 * N));
-  fft_rows<N, false>(GlobalRows<double2>{rn, rs}, A, P.tw, SmemRows<N, double2>{A});
-  const double2* Z = A;
+  fft_rows<2, N, false>(GlobalPairRows<double2>{reinterpret_cast<const double2*>(g.p[f]), j, P.nlat, N}, A, P.tw,
+                        SmemRows<N, double2>{A});
+  const SmemRows<N, double2> Z{A};
   const double wn = P.wn[j], ws = P.ws[j];
   double2* XS = P.X + ((size_t)(f * 2 + 0) * P.nm) * P.nh;
   double2* XD = P.X + ((size_t)(f * 2 + 1) * P.nm) * P.nh;
@@ -237,14 +235,15 @@ __global__ void __launch_bounds__(fft_nt(N)) k_fft_fold(sle::ShtDev P, GridPtrs 
     const double2 twm = (m > 0 && m < N) ? __ldg(P.tw + m) : make_double2(1.0, 0.0);
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
-      const double2* z = Z + r * N;
+      const double2 z0 = Z(r, 0);
       if (m == 0) {
-        xr[r] = make_double2(z[0].x + z[0].y, 0.0);
+        xr[r] = make_double2(z0.x + z0.y, 0.0);
       } else if (m == N) {
-        xr[r] = make_double2(z[0].x - z[0].y, 0.0);
+        xr[r] = make_double2(z0.x - z0.y, 0.0);
       } else {
-        const double2 zm = z[m];
-        const double2 zc = make_double2(z[N - m].x, -z[N - m].y);
+        const double2 zm = Z(r, m);
+        const double2 zn = Z(r, N - m);
+        const double2 zc = make_double2(zn.x, -zn.y);
         const double2 e = cscale(cadd(zm, zc), 0.5);
         const double2 dz = csub(zm, zc);
         const double2 o = make_double2(0.5 * dz.y, -0.5 * dz.x);  // (zm - zc) / (2i)
@@ -292,7 +291,7 @@ struct UnfoldSrc64 {
 };
 
 template <int N>
-__global__ void __launch_bounds__(fft_nt(N)) k_ifft_unfold(sle::ShtDev P, OutGridPtrs g) {
+__global__ void __launch_bounds__(fft_nt(2, N)) k_ifft_unfold(sle::ShtDev P, OutGridPtrs g) {
   extern __shared__ double2 sm[];
   double2* A = sm;
   const int j = blockIdx.x, f = blockIdx.y;
@@ -308,7 +307,7 @@ __global__ void __launch_bounds__(fft_nt(N)) k_ifft_unfold(sle::ShtDev P, OutGri
                      out2 ? reinterpret_cast<double2*>(out2 + rso) : nullptr,
                      out2 ? reinterpret_cast<const double2*>(mul2 + ro) : nullptr,
                      out2 ? reinterpret_cast<const double2*>(mul2 + rso) : nullptr};
-  fft_rows<N, true>(UnfoldSrc64<N>{E, O, P.tw, P.nm, P.nh}, A, P.tw, sink);
+  fft_rows<2, N, true>(UnfoldSrc64<N>{E, O, P.tw, P.nm, P.nh}, A, P.tw, sink);
 }
 
 
@@ -545,7 +544,7 @@ __global__ void k_unpack(sle::ShtDev P, const double2* packed, double2* dense) {
 }
 
 // ------------------------------------------------------------------------ launchers
-static size_t fft_smem(const ShtDev& d) { return (size_t)2 * d.n2 * sizeof(double2); }
+static size_t fft_smem(const ShtDev& d) { return fft_smem_bytes(2, d.n2, sizeof(double2)); }
 static int syn_threads(const ShtDev& d) { return 32 * ((d.ngrp + 1) / 2); }
 static size_t syn_smem(const ShtDev& d) { return (size_t)3 * d.nm * sizeof(double); }
 
@@ -561,7 +560,7 @@ static int fp64_analysis(sle_sht* plan, const FieldSpec* fs, int nf, cudaStream_
     d.gclr[f] = fs[f].skip_clear;
   }
   ProfToken t0 = prof_begin(PROF_FFT, nf, st);
-#define SLE_LAUNCH_FOLD(NN) k_fft_fold<NN><<<dim3(d.nh, nf), fft_threads(NN), fft_smem(d), st>>>(d, g)
+#define SLE_LAUNCH_FOLD(NN) k_fft_fold<NN><<<dim3(d.nh, nf), fft_threads(2, NN), fft_smem(d), st>>>(d, g)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_FOLD)
 #undef SLE_LAUNCH_FOLD
   prof_end(t0, st);
@@ -592,7 +591,7 @@ static int fp64_synthesis(sle_sht* plan, const FieldSpec* fs, int nf, cudaStream
   k_leg_syn<<<dim3(npairs, nf), syn_threads(d), syn_smem(d), st>>>(d, c);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, nf, st);
-#define SLE_LAUNCH_IFFT(NN) k_ifft_unfold<NN><<<dim3(d.nh, nf), fft_threads(NN), fft_smem(d), st>>>(d, g)
+#define SLE_LAUNCH_IFFT(NN) k_ifft_unfold<NN><<<dim3(d.nh, nf), fft_threads(2, NN), fft_smem(d), st>>>(d, g)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_IFFT)
 #undef SLE_LAUNCH_IFFT
   prof_end(t1, st);
@@ -680,7 +679,7 @@ static void plan_free(sle_sht* p) {
   if (!p) return;
   void* ptrs[] = {p->mu, p->w, p->wn, p->ws, p->be, p->cf, p->moff, p->lidx, p->segoff,
                   p->seg_m, p->seg_l0, p->ana_order, p->seeds, p->tw, p->X, p->EO, p->istart,
-                  p->packbuf, p->mx_xf, p->mx_gns, p->mx_bsyn, p->mx_s0, p->mx_abort,
+                  p->packbuf, p->mx_xf, p->mx_twf, p->mx_gns, p->mx_bsyn, p->mx_s0, p->mx_abort,
                   p->mx_ana_units, p->mx_syn_units, p->mx_syn_seg, p->mx_tab_ana, p->mx_tab_syn};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -816,6 +815,8 @@ static int plan_build(sle_sht* p, int nlat, int nlon, int lmax) {
   do {                                                                                                \
     SLE_CUDA(cudaFuncSetAttribute(k_fft_fold<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(d)));    \
     SLE_CUDA(cudaFuncSetAttribute(k_ifft_unfold<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fft_smem(d))); \
+    SLE_CUDA(cudaFuncSetAttribute(k_fft_fold<NN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));               \
+    SLE_CUDA(cudaFuncSetAttribute(k_ifft_unfold<NN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));            \
   } while (0)
   SLE_FFT_SWITCH(d.n2, SLE_ATTR_FFT)
 #undef SLE_ATTR_FFT
@@ -1076,7 +1077,7 @@ extern "C" int sle_sht_analysis_noalloc(sle_sht* plan, const double* grid_dev, v
   g.p[0] = grid_dev;
   SpecPtrs o{};
   o.p[0] = reinterpret_cast<double2*>(coeffs_packed_dev);
-#define SLE_LAUNCH_FOLD1(NN) k_fft_fold<NN><<<dim3(d.nh, 1), fft_threads(NN), fft_smem(d), st>>>(d, g)
+#define SLE_LAUNCH_FOLD1(NN) k_fft_fold<NN><<<dim3(d.nh, 1), fft_threads(2, NN), fft_smem(d), st>>>(d, g)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_FOLD1)
 #undef SLE_LAUNCH_FOLD1
   k_leg_ana<<<dim3((d.nseg + ANA_WARPS - 1) / ANA_WARPS, 1), 32 * ANA_WARPS, 0, st>>>(d, o);
