@@ -48,9 +48,9 @@ enum sle_status {
 
 /* Arithmetic of the transforms.  FP64: FP64 end to end (matches the reference to 1e-9 m).
  * MIXED: Legendre contractions as split-TF32 (3xTF32) tensor-core GEMMs with FP32
- * accumulation (operands rounded to FP32 before the split); the Legendre recurrence, row FFTs,
- * Gauss nodes and weights, the degree-0 coefficient and everything outside the transforms stay
- * FP64. */
+ * accumulation (operands rounded to FP32 before the split) and FP32 row FFTs; the Legendre
+ * recurrence (tables computed in FP64), Gauss nodes and weights, the degree-0 coefficient of
+ * every analysis and synthesis and everything outside the transforms stay FP64. */
 enum sle_precision { SLE_PREC_FP64 = 0, SLE_PREC_MIXED = 1 };
 
 enum sle_layout { SLE_LAYOUT_DENSE = 0, SLE_LAYOUT_PACKED = 1 };

@@ -11,24 +11,25 @@
 // with each operand split into TF32 hi + lo and D += Ahi Bhi + Ahi Blo + Alo Bhi in FP32.
 //
 // Precision: the Legendre values come from the FP64 recurrence of the plan
-// (Q_l = mu Q_{l-1} + be_l Q_{l-2}, P~ = cf Q) and are split once, when the plan is prepared,
-// into TF32 hi + lo tables stored in the tensor cores' shared-memory tile order; the B operands
-// are rounded to FP32 and split in shared memory.  Row FFTs, folds and the degree-0 coefficient
-// are FP64: analysis computes U_00 from FP64 row sums of the input grid; synthesis leaves l = 0
-// out of the tensor-core sum and adds its uniform contribution to the output grid in FP64.  The
-// tensor core's FP32 accumulation truncates, so the large products are spread over fresh TMEM
-// accumulators that the epilogue adds in FP64.
+// (Q_l = mu Q_{l-1} + be_l Q_{l-2}, P~ = cf Q), rounded once to FP32 when the plan is prepared
+// and stored in the tensor cores' shared-memory tile order; the kernel splits them, and the B
+// operands, into TF32 hi + lo in shared memory.  The row FFTs of this form run in FP32; the
+// degree-0 terms are FP64: analysis computes U_00 from FP64 row sums of the input grid,
+// synthesis leaves l = 0 out of the tensor-core sum and adds its uniform contribution to the
+// output grid in FP64.  The tensor core's FP32 accumulation truncates, so the large products are
+// spread over fresh TMEM accumulators that the epilogue adds in FP64.
 //
-// Kernel structure (one CTA per work unit, 10 warps, two pipeline stages):
-//   warp 9      loader: per K-chunk, one bulk copy of the A tiles (64 KB) and the B data
-//               (analysis: one 3-D TMA tensor load of the folded FFT; synthesis: bulk copies)
-//   warps 0-7   stage 0 / 1 splitters: B -> TF32 hi / lo tiles; warps 0-3 then read the
-//               accumulators out of TMEM (epilogue)
-//   warp 8      allocates TMEM and issues the MMAs from one thread
+// Kernel structure (persistent: one CTA per SM over the work units, 14 warps, two stages):
+//   warp 13     loader: per K-chunk of every unit of the CTA, one bulk copy of the FP32 A tiles
+//               (32 KB) and the B data (analysis: one 3-D TMA tensor load of the folded FFT;
+//               synthesis: bulk copies) into stage c & 1
+//   warps 4-11  stage 0 / 1 splitters: A and B -> TF32 hi / lo tiles
+//   warp 12     allocates TMEM and issues the MMAs from one thread, unit i into TMEM set i & 1
+//   warps 0-3   epilogue: read set i & 1 out of TMEM while the MMAs of unit i + 1 run
 // Stages hand over through mbarriers; tcgen05.commit releases a stage when its MMAs are done.
 // Every wait is bounded: on timeout the CTA raises the plan's abort flag (and the caller's status
-// word), stops waiting, lets issued MMAs drain and releases its TMEM.  No load uses cluster
-// multicast; every copy reads this GPU's own memory.
+// word), stops waiting, lets issued MMAs and copies land and releases its TMEM.  No load uses
+// cluster multicast; every copy reads this GPU's own memory.
 #include "sle_internal.cuh"
 #include "sle_fft.cuh"
 

@@ -270,3 +270,70 @@ class MemberFactory:
                 return torch.round(amp * (3500.0 * float(sawtooth(k * 200.0 / 1000.0))) * shape * 1000.0) / 1000.0
         return Request(rid=rid, lmax=L, love=love, topo=topo, ice=ice, nsteps=nsteps, dt=dt, arrival=arrival,
                        outer_passes=outer_passes)
+
+
+# ---------------------------------------------------------------- ensembles
+def autotune_slots(lmax, candidates=(8, 16, 32), precision="mixed", probe_steps=2, seed=20261209):
+    """Slot count of the highest member-steps/s for degree ``lmax``: each candidate batch is
+    loaded with seeded members (sawtooth ice), stepped once untimed (plan tables, graph capture),
+    then ``probe_steps`` times under CUDA events.  Returns (best, {candidate: member-steps/s})."""
+    import torch
+
+    mf = MemberFactory(seed)
+    rates = {}
+    for n in candidates:
+        reqs = [mf.make(i, lmax, probe_steps + 1, kind="sawtooth") for i in range(n)]
+        bt = SolverBatch(lmax + 1, 2 * (lmax + 1), lmax, n, precision=precision)
+        for s, r in enumerate(reqs):
+            bt.load(s, r.love, r.topo, r.ice(0), r.dt)
+        bt.step({s: r.ice(1) for s, r in enumerate(reqs)})
+        ices = [{s: r.ice(k) for s, r in enumerate(reqs)} for k in range(2, probe_steps + 2)]
+        st = torch.cuda.ExternalStream(bt.stream_handle())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for ice in ices:
+            bt.step(ice)
+        e1.record(st)
+        torch.cuda.synchronize()
+        rates[n] = n * probe_steps / (e0.elapsed_time(e1) / 1000.0)
+        del bt
+    return max(rates, key=rates.get), rates
+
+
+def uneven_ensemble(n=64, degrees=(127, 255, 511), steps=(50, 1200), seed=20261210):
+    """The uneven ensemble of seeded members: degree uniform over ``degrees``, step count uniform
+    in ``steps``, Earth relaxation scale log-uniform in [0.3, 3], ice from the melting caps or the
+    sawtooth sheets scaled by U[0.5, 1.5]; every member arrives at time 0."""
+    rng = np.random.default_rng(seed)
+    mf = MemberFactory(seed)
+    Ls = rng.choice(list(degrees), size=n)
+    ks = rng.integers(steps[0], steps[1] + 1, size=n)
+    return [mf.make(i, int(L), int(k)) for i, (L, k) in enumerate(zip(Ls, ks))]
+
+
+def run_ensemble(requests, precision="mixed", slots=None, autotune=True, candidates=(8, 16, 32)):
+    """Run a set of requests to completion with one slot batch per degree (continuous batching:
+    a member that finishes frees its slot for the next one of its degree).  ``slots``: {lmax:
+    slot count}; missing degrees are autotuned (or get min(32, members)).  Returns the server
+    statistics plus the slot choice and the autotune measurements."""
+    degrees = sorted({r.lmax for r in requests})
+    slots = dict(slots or {})
+    tuned = {}
+    for L in degrees:
+        if L in slots:
+            continue
+        count = sum(1 for r in requests if r.lmax == L)
+        if autotune:
+            cand = tuple(c for c in candidates if c <= max(count, min(candidates)))
+            best, rates = autotune_slots(L, cand, precision)
+            tuned[str(L)] = {str(k): v for k, v in rates.items()}
+            slots[L] = best
+        else:
+            slots[L] = min(32, count)
+    srv = Server(slots, precision=precision)
+    srv.run(requests)
+    st = srv.stats(requests)
+    st.update({"slots": {str(k): v for k, v in slots.items()}, "autotune_member_steps_per_s": tuned,
+               "members": {str(L): sum(1 for r in requests if r.lmax == L) for L in degrees}})
+    return st
