@@ -209,7 +209,7 @@ def slot_bytes(nlat, nlon, lmax, max_modes=8):
     ng = nlat * nlon
     nc = (lmax + 1) * (lmax + 2) // 2
     nl = lmax + 1
-    return int(21 * ng * 8 + 24 * nc * 16 + max_modes * nc * 16 + 5 * max_modes * nl * 8 + 3 * nl * 8
+    return int(11 * ng * 8 + 8 * ng + 24 * nc * 16 + max_modes * nc * 16 + 5 * max_modes * nl * 8 + 3 * nl * 8
                + 1024 + (nc // 256 + ng // 512 + 128) * 8 + 4 * nlat * 8)
 
 

@@ -86,8 +86,14 @@ __device__ __forceinline__ bool field_gated_off(const ShtDev& P, int f) {
   return false;
 }
 
-// One field of a transform call: input and output, optional gates (see ShtDev::gset/gclr) and,
-// for synthesis, the optional epilogue epi_out = grid * epi_mul.
+// What an analysis reads for a field (cell c): SRC_GRID grid[c]; SRC_MASK the 0/1 byte m0[c];
+// SRC_ICE m0[c] ? grid[c] : grid[c] * 0 (ice on its grounded mask); SRC_TO
+// grid[c] * (m0[c] - m1[c]) (T0 (C* - C*0)); SRC_PROD grid[c] * m0[c] (dsl C*).  The products are
+// the ones the step would otherwise write out as FP64 grids, in the same arithmetic.
+enum SrcKind { SRC_GRID = 0, SRC_MASK = 1, SRC_ICE = 2, SRC_TO = 3, SRC_PROD = 4 };
+
+// One field of a transform call: input and output, optional gates (see ShtDev::gset/gclr), the
+// analysis source kind and, for synthesis, the optional epilogue epi_out = grid * epi_mul.
 struct FieldSpec {
   double* grid;
   double2* spec;
@@ -95,7 +101,26 @@ struct FieldSpec {
   const int* skip_clear;
   double* epi_out;
   const double* epi_mul;
+  int kind;
+  const unsigned char* m0;
+  const unsigned char* m1;
 };
+
+// Two neighbouring cells c, c + 1 (c even) of an analysis source.
+__device__ __forceinline__ double2 src_pair(int kind, const double* g, const unsigned char* m0,
+                                            const unsigned char* m1, size_t c) {
+  if (kind == SRC_GRID) return __ldg(reinterpret_cast<const double2*>(g + c));
+  const uchar2 a = *reinterpret_cast<const uchar2*>(m0 + c);
+  if (kind == SRC_MASK) return make_double2(a.x ? 1.0 : 0.0, a.y ? 1.0 : 0.0);
+  const double2 v = __ldg(reinterpret_cast<const double2*>(g + c));
+  if (kind == SRC_ICE) return make_double2(a.x ? v.x : __dmul_rn(v.x, 0.0), a.y ? v.y : __dmul_rn(v.y, 0.0));
+  if (kind == SRC_TO) {
+    const uchar2 z = *reinterpret_cast<const uchar2*>(m1 + c);
+    return make_double2(__dmul_rn(v.x, __dsub_rn(a.x ? 1.0 : 0.0, z.x ? 1.0 : 0.0)),
+                        __dmul_rn(v.y, __dsub_rn(a.y ? 1.0 : 0.0, z.y ? 1.0 : 0.0)));
+  }
+  return make_double2(__dmul_rn(v.x, a.x ? 1.0 : 0.0), __dmul_rn(v.y, a.y ? 1.0 : 0.0));
+}
 
 // Fields of one mixed-precision transform launch.  Field f is skipped (its outputs left as
 // they are) when *skip_set[f] != 0 or *skip_clear[f] == 0 (null pointers never skip).
@@ -109,6 +134,9 @@ struct MxFieldArgs {
   const int* skip_clear[MX_MAXF];
   double* epi_out[MX_MAXF];
   const double* epi_mul[MX_MAXF];
+  int kind[MX_MAXF];               // analysis source (SrcKind)
+  const unsigned char* m0[MX_MAXF];
+  const unsigned char* m1[MX_MAXF];
 };
 
 }  // namespace sle

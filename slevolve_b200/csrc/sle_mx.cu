@@ -738,13 +738,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // fold (the weighted row sums) is formed in FP64 from the FP64 grid values, in s0[f][j], for the
 // FP64 degree-0 coefficient.
 struct FoldSrcMx {
-  const double2* g;
-  int j0, nlat, rowlen;
+  TypedPairRows src;
   double* acc;          // this thread's FP64 sum of the values it reads (one row per thread)
   __device__ __forceinline__ float2 operator()(int r, int i) const {
-    const int j = j0 + (r >> 1);
-    const int row = (r & 1) ? nlat - 1 - j : j;
-    const double2 v = __ldg(g + (size_t)row * rowlen + i);
+    const double2 v = src(r, i);
     *acc = (*acc + v.x) + v.y;
     return make_float2((float)v.x, (float)v.y);
   }
@@ -759,8 +756,8 @@ __global__ void __launch_bounds__(fft_nt(4, N)) k_fold_mx(ShtDev P, MxFieldArgs 
   constexpr int NT = fft_nt(4, N);
   constexpr int Q = N / FftRadix<N, 1>::R;   // first-pass items per row: one per thread
   double acc = 0.0;
-  fft_rows<4, N, false>(FoldSrcMx{reinterpret_cast<const double2*>(a.grid[f]), j0, P.nlat, N, &acc}, A, P.twf,
-                        SmemRows<N, float2>{A});
+  fft_rows<4, N, false>(FoldSrcMx{TypedPairRows{a.kind[f], a.grid[f], a.m0[f], a.m1[f], j0, P.nlat, 2 * N}, &acc},
+                        A, P.twf, SmemRows<N, float2>{A});
   // FP64 row sums: the Q threads r Q .. r Q + Q - 1 hold the partial sums of row r (Q a power
   // of two): a butterfly within aligned groups of min(Q, 32) lanes, then the warps of a row in
   // order

@@ -202,6 +202,9 @@ __global__ void k_lidx(sle::ShtDev P, int* lidx) {
 
 struct GridPtrs {
   const double* p[MAXF];
+  int kind[MAXF];                  // analysis source (SrcKind)
+  const unsigned char* m0[MAXF];
+  const unsigned char* m1[MAXF];
 };
 struct OutGridPtrs {
   double* p[MAXF];
@@ -224,7 +227,7 @@ __global__ void __launch_bounds__(fft_nt(2, N)) k_fft_fold(sle::ShtDev P, GridPt
   double2* A = sm;
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_gated_off(P, f)) return;
-  fft_rows<2, N, false>(GlobalPairRows<double2>{reinterpret_cast<const double2*>(g.p[f]), j, P.nlat, N}, A, P.tw,
+  fft_rows<2, N, false>(TypedPairRows{g.kind[f], g.p[f], g.m0[f], g.m1[f], j, P.nlat, 2 * N}, A, P.tw,
                         SmemRows<N, double2>{A});
   const SmemRows<N, double2> Z{A};
   const double wn = P.wn[j], ws = P.ws[j];
@@ -555,6 +558,9 @@ static int fp64_analysis(sle_sht* plan, const FieldSpec* fs, int nf, cudaStream_
   SpecPtrs o{};
   for (int f = 0; f < nf; ++f) {
     g.p[f] = fs[f].grid;
+    g.kind[f] = fs[f].kind;
+    g.m0[f] = fs[f].m0;
+    g.m1[f] = fs[f].m1;
     o.p[f] = fs[f].spec;
     d.gset[f] = fs[f].skip_set;
     d.gclr[f] = fs[f].skip_clear;
@@ -610,6 +616,9 @@ static MxFieldArgs mx_args(const FieldSpec* fs, int nf) {
     a.skip_clear[f] = fs[f].skip_clear;
     a.epi_out[f] = fs[f].epi_out;
     a.epi_mul[f] = fs[f].epi_mul;
+    a.kind[f] = fs[f].kind;
+    a.m0[f] = fs[f].m0;
+    a.m1[f] = fs[f].m1;
   }
   return a;
 }

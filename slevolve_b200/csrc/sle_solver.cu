@@ -75,9 +75,14 @@ struct SlotStep {
 };
 
 enum GridId {
-  G_TINIT, G_CXY0, G_BETA0, G_CSTAR0, G_CXY, G_TOPO_PREV, G_ICESTAR, G_BETA, G_CSTAR, G_TO, G_RO,
-  G_DSL, G_DELTASL, G_TOPO, G_RR, G_GRNEW, G_ICE, G_ICE_PREV, G_TMP, G_TMP3, G_TMP4, NGRID
+  G_TINIT, G_TOPO_PREV, G_DSL, G_DELTASL, G_TOPO, G_RR, G_ICE, G_ICE_PREV, G_TMP, G_TMP3, G_TMP4, NGRID
 };
+// 0/1 grids as bytes: ocean function (step 0 and current), beta = grounded-ice complement
+// (step 0 and current), C* (step 0 and current), the grounded ("keep") mask of the current I*
+// (I* = keep ? ice : ice * 0) and the candidate keep mask of a grounded re-guess.  The FP64
+// fields derived from them (C*, I*, tO = T0 (C* - C*0), rO = dsl C*) are formed by the transforms
+// as they read them (SrcKind) instead of being written out.
+enum MaskId { M_CXY0, M_BETA0, M_CSTAR0, M_CXY, M_GR, M_BETA, M_CSTAR, M_GRNEW, NMASK };
 enum SpecId {
   S_P_LOAD, S_P_ICE, S_P_OCEAN, S_PREV_ICE, S_VISC, S_RAD, S_ICELM, S_OLDICE, S_DICE, S_DI, S_CSTARLM,
   S_TOLM, S_ROLM, S_LOAD, S_DSCUR, S_SL, S_SLTOT, S_RRLM, S_HA, S_HB, S_SP0, S_SP1, S_SP2, S_SP3, NSPEC
@@ -88,6 +93,7 @@ struct Dev {
   long long ng, ncoef;
   const int* lidx;
   double* grid;                 // [NGRID][nslot][ng]
+  unsigned char* mask;          // [NMASK][nslot][ng]
   double2* spec;                // [NSPEC][nslot][ncoef]
   double2* R;                   // [nslot][K][ncoef]
   const int* nmod;              // [nslot][nl]
@@ -108,6 +114,7 @@ struct Dev {
   long long i20, i21, i22;      // packed indices of (l=2, m=0..2)
   int slot0;                    // slot of blockIdx.y == 0
   __host__ __device__ double* g(int id, int b) const { return grid + ((size_t)id * nslot + b) * ng; }
+  __host__ __device__ unsigned char* m(int id, int b) const { return mask + ((size_t)id * nslot + b) * ng; }
   __host__ __device__ double2* sp(int id, int b) const { return spec + ((size_t)id * nslot + b) * ncoef; }
   __host__ __device__ size_t kl(int b) const { return (size_t)b * K * nl; }
 };
@@ -204,11 +211,20 @@ __device__ __forceinline__ double2 ld2(const double* p, long long i) {
 __device__ __forceinline__ void st2(double* p, long long i, double a, double b) {
   reinterpret_cast<double2*>(p)[i] = make_double2(a, b);
 }
+// mask cells 2i, 2i + 1
+__device__ __forceinline__ uchar2 ldm2(const unsigned char* p, long long i) {
+  return reinterpret_cast<const uchar2*>(p)[i];
+}
+__device__ __forceinline__ void stm2(unsigned char* p, long long i, bool a, bool b) {
+  reinterpret_cast<uchar2*>(p)[i] = make_uchar2(a ? 1 : 0, b ? 1 : 0);
+}
 
 // grounded ice on topography `topo` (flotation test, solver.py:655-659)
+__device__ __forceinline__ bool icestar_keep(double ice, double topo, double rhow, double rhoi) {
+  return (topo > 0.0) || (ice > __ddiv_rn(__dmul_rn(fabs(topo), rhow), rhoi));
+}
 __device__ __forceinline__ double icestar_on(double ice, double topo, double rhow, double rhoi) {
-  const bool keep = (topo > 0.0) || (ice > __ddiv_rn(__dmul_rn(fabs(topo), rhow), rhoi));
-  return keep ? ice : __dmul_rn(ice, 0.0);
+  return icestar_keep(ice, topo, rhow, rhoi) ? ice : __dmul_rn(ice, 0.0);
 }
 
 // ------------------------------------------------------------------------- kernels
@@ -359,37 +375,34 @@ __global__ void __launch_bounds__(256) k_advance(Dev D) {
   D.sp(S_RAD, b)[i] = r;
 }
 
-// Step prologue on the grid (solver.py:853-887): I* on the previous topography, beta,
-// C* = C beta, tO = T0 (C* - C*0); at the slot's first step also I* of the previous ice on T0.
+// Step prologue on the grid (solver.py:853-887): I* on the previous topography (its keep mask),
+// beta, C* = C beta (tO = T0 (C* - C*0) is formed by its analysis); at the slot's first step also
+// I* of the previous ice on T0.
 __global__ void k_ice_grid(Dev D) {
   SLOT_OR_RETURN();
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h >= D.ng) return;
   const double2 v = ld2(D.g(G_ICE, b), h), tp = ld2(D.g(G_TOPO_PREV, b), h);
-  double2 cx = ld2(D.g(G_CXY, b), h);
-  const double2 ti = ld2(D.g(G_TINIT, b), h), c0 = ld2(D.g(G_CSTAR0, b), h);
+  uchar2 cx = ldm2(D.m(M_CXY, b), h);
   const unsigned char* wm = D.ss[b].warm_mask;
   if (wm) {  // warm start: the converged ocean function of this step in the previous pass
-    cx = make_double2(wm[2 * h] ? 1.0 : 0.0, wm[2 * h + 1] ? 1.0 : 0.0);
-    st2(D.g(G_CXY, b), h, cx.x, cx.y);
+    cx = make_uchar2(wm[2 * h] ? 1 : 0, wm[2 * h + 1] ? 1 : 0);
+    stm2(D.m(M_CXY, b), h, cx.x, cx.y);
   }
   if (!isfinite(v.x) || !isfinite(v.y)) sc->status = SLE_ERR_NONFINITE;
-  double is[2], bt[2], c[2], t[2];
-  const double vv[2] = {v.x, v.y}, tt[2] = {tp.x, tp.y}, cc[2] = {cx.x, cx.y}, ii[2] = {ti.x, ti.y},
-               zz[2] = {c0.x, c0.y};
+  bool keep[2], bt[2];
+  const double vv[2] = {v.x, v.y}, tt[2] = {tp.x, tp.y};
 #pragma unroll
   for (int u = 0; u < 2; ++u) {
-    is[u] = D.checkmarine ? icestar_on(vv[u], tt[u], D.rhow, D.rhoi) : vv[u];
-    bt[u] = (is[u] < EPS0) ? 1.0 : 0.0;
-    c[u] = __dmul_rn(cc[u], bt[u]);
-    t[u] = __dmul_rn(ii[u], __dsub_rn(c[u], zz[u]));
+    keep[u] = !D.checkmarine || icestar_keep(vv[u], tt[u], D.rhow, D.rhoi);
+    const double is = keep[u] ? vv[u] : __dmul_rn(vv[u], 0.0);
+    bt[u] = is < EPS0;
   }
-  st2(D.g(G_ICESTAR, b), h, is[0], is[1]);
-  st2(D.g(G_BETA, b), h, bt[0], bt[1]);
-  st2(D.g(G_CSTAR, b), h, c[0], c[1]);
-  st2(D.g(G_TO, b), h, t[0], t[1]);
+  stm2(D.m(M_GR, b), h, keep[0], keep[1]);
+  stm2(D.m(M_BETA, b), h, bt[0], bt[1]);
+  stm2(D.m(M_CSTAR, b), h, cx.x && bt[0], cx.y && bt[1]);
   if (D.ss[b].first) {
-    const double2 vp = ld2(D.g(G_ICE_PREV, b), h);
+    const double2 vp = ld2(D.g(G_ICE_PREV, b), h), ti = ld2(D.g(G_TINIT, b), h);
     const double o0 = D.checkmarine ? icestar_on(vp.x, ti.x, D.rhow, D.rhoi) : vp.x;
     const double o1 = D.checkmarine ? icestar_on(vp.y, ti.y, D.rhow, D.rhoi) : vp.y;
     st2(D.g(G_TMP, b), h, o0, o1);
@@ -609,8 +622,8 @@ __global__ void k_sltot(Dev D) {
   D.sp(S_SLTOT, b)[i] = v;
 }
 
-// deltasl (dsl identity) and, when not converged, topography / ocean function refresh and
-// the grounded-ice test on the new topography (solver.py:1032-1037, 661-684).  One extra block
+// deltasl (dsl identity) and, when not converged, the ocean function of the refreshed
+// topography and the grounded-ice test on it (solver.py:1032-1037, 661-684).  One extra block
 // per slot (the last) evaluates the rotation block of the next iteration meanwhile.
 __global__ void k_refresh1(Dev D) {
   SLOT_OR_RETURN();
@@ -637,15 +650,15 @@ __global__ void k_refresh1(Dev D) {
     if (!conv) {
       const double2 ti = ld2(D.g(G_TINIT, b), h);
       const double t0 = __dsub_rn(ti.x, ds[0]), t1 = __dsub_rn(ti.y, ds[1]);
-      st2(D.g(G_TOPO, b), h, t0, t1);
-      st2(D.g(G_CXY, b), h, (t0 < 0.0) ? 1.0 : 0.0, (t1 < 0.0) ? 1.0 : 0.0);
+      stm2(D.m(M_CXY, b), h, t0 < 0.0, t1 < 0.0);
       if (test) {
-        const double2 ic = ld2(D.g(G_ICE, b), h), be = ld2(D.g(G_BETA, b), h);
-        const double g0 = icestar_on(ic.x, t0, D.rhow, D.rhoi);
-        const double g1 = icestar_on(ic.y, t1, D.rhow, D.rhoi);
-        st2(D.g(G_GRNEW, b), h, g0, g1);
-        if ((g0 < EPS0) != (be.x != 0.0)) cnt += 1.0;
-        if ((g1 < EPS0) != (be.y != 0.0)) cnt += 1.0;
+        const double2 ic = ld2(D.g(G_ICE, b), h);
+        const uchar2 be = ldm2(D.m(M_BETA, b), h);
+        const bool k0 = icestar_keep(ic.x, t0, D.rhow, D.rhoi), k1 = icestar_keep(ic.y, t1, D.rhow, D.rhoi);
+        const double g0 = k0 ? ic.x : __dmul_rn(ic.x, 0.0), g1 = k1 ? ic.y : __dmul_rn(ic.y, 0.0);
+        stm2(D.m(M_GRNEW, b), h, k0, k1);
+        if ((g0 < EPS0) != (be.x != 0)) cnt += 1.0;
+        if ((g1 < EPS0) != (be.y != 0)) cnt += 1.0;
       }
     }
   }
@@ -667,29 +680,32 @@ __global__ void k_refresh1(Dev D) {
   }
 }
 
-// C* and tO on the refreshed ocean function; accepted grounded-ice mask (solver.py:664-684)
+// C* on the refreshed ocean function; accepted grounded-ice mask (solver.py:664-684).  tO =
+// T0 (C* - C*0) is formed by its analysis.
 __global__ void k_refresh2(Dev D) {
   SLOT_OR_RETURN();
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h >= D.ng || sc->converged) return;
-  const int changed = sc->gr_changed;
-  double2 bt;
-  if (changed) {
-    const double2 g = ld2(D.g(G_GRNEW, b), h);
-    st2(D.g(G_ICESTAR, b), h, g.x, g.y);
-    bt = make_double2((g.x < EPS0) ? 1.0 : 0.0, (g.y < EPS0) ? 1.0 : 0.0);
-    st2(D.g(G_BETA, b), h, bt.x, bt.y);
+  uchar2 bt;
+  if (sc->gr_changed) {
+    const uchar2 k = ldm2(D.m(M_GRNEW, b), h);
+    const double2 ic = ld2(D.g(G_ICE, b), h);
+    const double g0 = k.x ? ic.x : __dmul_rn(ic.x, 0.0), g1 = k.y ? ic.y : __dmul_rn(ic.y, 0.0);
+    reinterpret_cast<uchar2*>(D.m(M_GR, b))[h] = k;
+    bt = make_uchar2(g0 < EPS0, g1 < EPS0);
+    reinterpret_cast<uchar2*>(D.m(M_BETA, b))[h] = bt;
   } else {
-    bt = ld2(D.g(G_BETA, b), h);
+    bt = ldm2(D.m(M_BETA, b), h);
   }
-  const double2 cx = ld2(D.g(G_CXY, b), h), ti = ld2(D.g(G_TINIT, b), h), c0 = ld2(D.g(G_CSTAR0, b), h);
-  const double c_0 = __dmul_rn(cx.x, bt.x), c_1 = __dmul_rn(cx.y, bt.y);
-  // C* and tO = T0 (C* - C*0) only change where a cell of C* flips; without a flip their
-  // re-analyses are skipped (the inputs, hence the spectra, are bit-identical to the last ones)
-  const double2 prev = ld2(D.g(G_CSTAR, b), h);
-  if (prev.x != c_0 || prev.y != c_1) sc->cs_changed = 1;
-  st2(D.g(G_CSTAR, b), h, c_0, c_1);
-  st2(D.g(G_TO, b), h, __dmul_rn(ti.x, __dsub_rn(c_0, c0.x)), __dmul_rn(ti.y, __dsub_rn(c_1, c0.y)));
+  const uchar2 cx = ldm2(D.m(M_CXY, b), h);
+  const uchar2 c = make_uchar2(cx.x && bt.x, cx.y && bt.y);
+  // C* and tO only change where a cell of C* flips; without a flip their re-analyses are
+  // skipped (the inputs, hence the spectra, are bit-identical to the last ones)
+  const uchar2 prev = ldm2(D.m(M_CSTAR, b), h);
+  if (prev.x != c.x || prev.y != c.y) {
+    sc->cs_changed = 1;
+    reinterpret_cast<uchar2*>(D.m(M_CSTAR, b))[h] = c;
+  }
 }
 
 // dice, dI after a grounded-mask change; the slot's last block re-evaluates the rotation block
@@ -802,14 +818,17 @@ __global__ void k_post_grid(Dev D, int diag) {
   if (sc->status) return;
   double a = 0.0, bs = 0.0, c = 0.0, d = 0.0;
   const long long row = (long long)j * (D.nlon / 2);
-  const double *deltasl = D.g(G_DELTASL, b), *tinit = D.g(G_TINIT, b), *beta = D.g(G_BETA, b);
-  double *topo = D.g(G_TOPO, b), *topo_prev = D.g(G_TOPO_PREV, b), *cxy = D.g(G_CXY, b);
+  const double *deltasl = D.g(G_DELTASL, b), *tinit = D.g(G_TINIT, b);
+  const unsigned char* beta = D.m(M_BETA, b);
+  double *topo = D.g(G_TOPO, b), *topo_prev = D.g(G_TOPO_PREV, b);
+  unsigned char* cxy = D.m(M_CXY, b);
   double *slc = D.g(G_TMP, b), *slcb = D.g(G_TMP3, b), *cstar = D.g(G_TMP4, b);
   unsigned char* rec_mask = D.ss[b].rec_mask;
   for (int t = threadIdx.x; t < D.nlon / 2; t += blockDim.x) {
     const long long h = row + t;
-    const double2 ds = ld2(deltasl, h), ti = ld2(tinit, h), bb = ld2(beta, h);
-    const double dsv[2] = {ds.x, ds.y}, tiv[2] = {ti.x, ti.y}, bv[2] = {bb.x, bb.y};
+    const double2 ds = ld2(deltasl, h), ti = ld2(tinit, h);
+    const uchar2 bb = ldm2(beta, h);
+    const double dsv[2] = {ds.x, ds.y}, tiv[2] = {ti.x, ti.y}, bv[2] = {bb.x ? 1.0 : 0.0, bb.y ? 1.0 : 0.0};
     double tp[2], o[2], s1[2], s2[2], cs[2];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
@@ -825,7 +844,7 @@ __global__ void k_post_grid(Dev D, int diag) {
     }
     st2(topo, h, tp[0], tp[1]);
     st2(topo_prev, h, tp[0], tp[1]);
-    st2(cxy, h, o[0], o[1]);
+    stm2(cxy, h, o[0] != 0.0, o[1] != 0.0);
     if (rec_mask) {
       rec_mask[2 * h] = o[0] != 0.0;
       rec_mask[2 * h + 1] = o[1] != 0.0;
@@ -878,16 +897,24 @@ __global__ void k_init_grid(Dev D, int b) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ng) return;
   const double t = D.g(G_TINIT, b)[i];
-  const double c = (t < 0.0) ? 1.0 : 0.0;
-  D.g(G_CXY0, b)[i] = c;
-  D.g(G_CXY, b)[i] = c;
+  const bool c = t < 0.0;
+  D.m(M_CXY0, b)[i] = c;
+  D.m(M_CXY, b)[i] = c;
   D.g(G_TOPO_PREV, b)[i] = t;
   const double v = D.g(G_ICE_PREV, b)[i];
-  const double gg = D.checkmarine ? icestar_on(v, t, D.rhow, D.rhoi) : v;
-  D.g(G_ICESTAR, b)[i] = gg;
-  const double bt = (gg < EPS0) ? 1.0 : 0.0;
-  D.g(G_BETA0, b)[i] = bt;
-  D.g(G_CSTAR0, b)[i] = __dmul_rn(c, bt);
+  const bool keep = !D.checkmarine || icestar_keep(v, t, D.rhow, D.rhoi);
+  const double gg = keep ? v : __dmul_rn(v, 0.0);
+  D.m(M_GR, b)[i] = keep;
+  const bool bt = gg < EPS0;
+  D.m(M_BETA0, b)[i] = bt;
+  D.m(M_CSTAR0, b)[i] = c && bt;
+}
+
+// FP64 grid of a mask (0/1) or of I* = keep ? ice : ice * 0, for the getters.
+__global__ void k_mask_grid(long long n, const unsigned char* m, const double* ice, double* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = ice ? (m[i] ? ice[i] : __dmul_rn(ice[i], 0.0)) : (m[i] ? 1.0 : 0.0);
 }
 
 __global__ void k_finite(long long n, const double* a, unsigned int* bad) {
@@ -935,6 +962,7 @@ struct sle_batch {
   Dev D;
   // device allocations
   double* grid;
+  unsigned char* mask;
   double2 *spec, *R;
   int* nmod;
   double *s_kl, *decay, *omd, *a_sl, *a_rr, *ttl, *ttlekhl, *ttlhe, *a_il, *a_m, *a_tsl, *a_trr;
@@ -982,7 +1010,7 @@ inline unsigned nb(long long n, int bs = 256) { return (unsigned)((n + bs - 1) /
 
 void batch_free(sle_batch* s) {
   if (!s) return;
-  void* ptrs[] = {s->grid, s->spec, s->R, s->nmod, s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr, s->ttl,
+  void* ptrs[] = {s->grid, s->mask, s->spec, s->R, s->nmod, s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr, s->ttl,
                   s->ttlekhl, s->ttlhe, s->a_il, s->a_m, s->a_tsl, s->a_trr, s->rc, s->r_il, s->r_m,
                   s->r_lam, s->sc, s->ss, s->partials, s->counter, s->rows, s->badflag, s->bstatus};
   for (void* q : ptrs)
@@ -1033,7 +1061,25 @@ int set_dt(sle_batch* s, int b, double dt) {
 
 FieldSpec fspec(double* grid, double2* spec, const int* skip_set = nullptr, const int* skip_clear = nullptr,
                 double* epi_out = nullptr, const double* epi_mul = nullptr) {
-  return FieldSpec{grid, spec, skip_set, skip_clear, epi_out, epi_mul};
+  return FieldSpec{grid, spec, skip_set, skip_clear, epi_out, epi_mul, SRC_GRID, nullptr, nullptr};
+}
+// analysis inputs formed from masks (SrcKind): a 0/1 mask, ice on its keep mask, T0 (C* - C*0),
+// a grid times a mask
+FieldSpec fmask(const unsigned char* m, double2* spec, const int* skip_set = nullptr,
+                const int* skip_clear = nullptr) {
+  return FieldSpec{nullptr, spec, skip_set, skip_clear, nullptr, nullptr, SRC_MASK, m, nullptr};
+}
+FieldSpec fice(double* ice, const unsigned char* keep, double2* spec, const int* skip_set = nullptr,
+               const int* skip_clear = nullptr) {
+  return FieldSpec{ice, spec, skip_set, skip_clear, nullptr, nullptr, SRC_ICE, keep, nullptr};
+}
+FieldSpec fto(double* tinit, const unsigned char* cstar, const unsigned char* cstar0, double2* spec,
+              const int* skip_set = nullptr, const int* skip_clear = nullptr) {
+  return FieldSpec{tinit, spec, skip_set, skip_clear, nullptr, nullptr, SRC_TO, cstar, cstar0};
+}
+FieldSpec fprod(double* grid, const unsigned char* m, double2* spec, const int* skip_set = nullptr,
+                const int* skip_clear = nullptr) {
+  return FieldSpec{grid, spec, skip_set, skip_clear, nullptr, nullptr, SRC_PROD, m, nullptr};
 }
 
 double fourpiR2(const sle_batch* s, double x) {
@@ -1234,8 +1280,8 @@ int init_slot(sle_batch* s, int b, const double* topo0, const double* ice0, int 
   k_init_grid<<<nb(D.ng), 256, 0, st>>>(D, b);
   SLE_CUDA(cudaGetLastError());
   // step-0 areas and volume from full analyses (solver.py:571-581)
-  const FieldSpec f3[3] = {fspec(D.g(G_CXY0, b), D.sp(S_SP0, b)), fspec(D.g(G_CSTAR0, b), D.sp(S_SP1, b)),
-                           fspec(D.g(G_ICESTAR, b), D.sp(S_SP2, b))};
+  const FieldSpec f3[3] = {fmask(D.m(M_CXY0, b), D.sp(S_SP0, b)), fmask(D.m(M_CSTAR0, b), D.sp(S_SP1, b)),
+                           fice(D.g(G_ICE_PREV, b), D.m(M_GR, b), D.sp(S_SP2, b))};
   SLE_TRY(sht_analysis_list(s->plan, f3, 3, st));
   double2 v[3];
   SLE_CUDA(cudaMemcpyAsync(&v[0], D.sp(S_SP0, b), sizeof(double2), cudaMemcpyDeviceToHost, st));
@@ -1320,6 +1366,7 @@ int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
   const int K = kmax;
   const size_t B = (size_t)nslot;
   TRY(dalloc(&s->grid, (size_t)NGRID * B * ng));
+  TRY(dalloc(&s->mask, (size_t)NMASK * B * ng));
   TRY(dalloc(&s->spec, (size_t)NSPEC * B * nc));
   TRY(dalloc(&s->R, B * K * nc + 1));
   TRY(dalloc(&s->nmod, B * nl));
@@ -1365,6 +1412,7 @@ int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
   D.ncoef = nc;
   D.lidx = s->plan->d.lidx;
   D.grid = s->grid;
+  D.mask = s->mask;
   D.spec = s->spec;
   D.R = s->R;
   D.nmod = s->nmod;
@@ -1407,15 +1455,17 @@ int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
   // static field lists of the loop body: every slot, gated by its flags
   for (int b = 0; b < nslot; ++b) {
     Scal* sb = s->sc + b;
-    s->f_syn_sl.push_back(fspec(D.g(G_DSL, b), D.sp(S_SL, b), &sb->done, nullptr, D.g(G_RO, b), D.g(G_CSTAR, b)));
-    s->f_ana_ro.push_back(fspec(D.g(G_RO, b), D.sp(S_ROLM, b), &sb->done));
+    s->f_syn_sl.push_back(fspec(D.g(G_DSL, b), D.sp(S_SL, b), &sb->done));
+    s->f_ana_ro.push_back(fprod(D.g(G_DSL, b), D.m(M_CSTAR, b), D.sp(S_ROLM, b), &sb->done));
     s->f_syn_sltot.push_back(fspec(D.g(G_DELTASL, b), D.sp(S_SLTOT, b), &sb->done));
   }
   for (int b = 0; b < nslot; ++b) {
     Scal* sb = s->sc + b;
-    s->f_ana_refresh.push_back(fspec(D.g(G_ICESTAR, b), D.sp(S_ICELM, b), &sb->converged, &sb->gr_changed));
-    s->f_ana_refresh.push_back(fspec(D.g(G_CSTAR, b), D.sp(S_CSTARLM, b), &sb->converged, &sb->cs_changed));
-    s->f_ana_refresh.push_back(fspec(D.g(G_TO, b), D.sp(S_TOLM, b), &sb->converged, &sb->cs_changed));
+    s->f_ana_refresh.push_back(
+        fice(D.g(G_ICE, b), D.m(M_GR, b), D.sp(S_ICELM, b), &sb->converged, &sb->gr_changed));
+    s->f_ana_refresh.push_back(fmask(D.m(M_CSTAR, b), D.sp(S_CSTARLM, b), &sb->converged, &sb->cs_changed));
+    s->f_ana_refresh.push_back(fto(D.g(G_TINIT, b), D.m(M_CSTAR, b), D.m(M_CSTAR0, b), D.sp(S_TOLM, b),
+                                   &sb->converged, &sb->cs_changed));
   }
   // SLEVOLVE_B200_HOST_LOOP=1 drives the inner loop from the host (same kernels; used to profile
   // the loop body, whose kernels profilers do not report inside conditional graph nodes)
@@ -1512,9 +1562,9 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
   {
     std::vector<FieldSpec> f;
     for (int b : act) {
-      f.push_back(fspec(D.g(G_ICESTAR, b), D.sp(S_ICELM, b)));
-      f.push_back(fspec(D.g(G_CSTAR, b), D.sp(S_CSTARLM, b)));
-      f.push_back(fspec(D.g(G_TO, b), D.sp(S_TOLM, b)));
+      f.push_back(fice(D.g(G_ICE, b), D.m(M_GR, b), D.sp(S_ICELM, b)));
+      f.push_back(fmask(D.m(M_CSTAR, b), D.sp(S_CSTARLM, b)));
+      f.push_back(fto(D.g(G_TINIT, b), D.m(M_CSTAR, b), D.m(M_CSTAR0, b), D.sp(S_TOLM, b)));
       if (s->hss[b].first) f.push_back(fspec(D.g(G_TMP, b), D.sp(S_OLDICE, b)));
     }
     SLE_TRY(sht_analysis_list(s->plan, f.data(), (int)f.size(), st));
@@ -1566,7 +1616,7 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
     for (int b : act) {
       const int* gs = &s->sc[b].status;
       f.push_back(fspec(D.g(G_TMP, b), D.sp(S_SP0, b), gs));
-      f.push_back(fspec(D.g(G_CXY, b), D.sp(S_SP1, b), gs));
+      f.push_back(fmask(D.m(M_CXY, b), D.sp(S_SP1, b), gs));
       f.push_back(fspec(D.g(G_TMP3, b), D.sp(S_SP2, b), gs));
       f.push_back(fspec(D.g(G_TMP4, b), D.sp(S_SP3, b), gs));
     }
@@ -1641,13 +1691,27 @@ int batch_get(sle_batch* s, int b, int field, void* dst, int dst_on_device) {
   const double* src = nullptr;
   switch (field) {
     case SLE_F_TGRID: src = D.g(G_TOPO, b); break;
-    case SLE_F_OCEAN: src = D.g(G_CXY, b); break;
-    case SLE_F_BETA: src = D.g(G_BETA, b); break;
+    case SLE_F_OCEAN:
+    case SLE_F_BETA:
+    case SLE_F_ICESTAR:
+    case SLE_F_OCEAN0:
+    case SLE_F_BETA0: {
+      const int mid = field == SLE_F_OCEAN ? M_CXY : field == SLE_F_BETA ? M_BETA : field == SLE_F_ICESTAR ? M_GR
+                      : field == SLE_F_OCEAN0 ? M_CXY0 : M_BETA0;
+      double* out = dst_on_device ? static_cast<double*>(dst) : D.g(G_TMP4, b);
+      note_launch();
+      k_mask_grid<<<nb(D.ng), 256, 0, s->st>>>(D.ng, D.m(mid, b), field == SLE_F_ICESTAR ? D.g(G_ICE, b) : nullptr,
+                                              out);
+      SLE_CUDA(cudaGetLastError());
+      if (dst_on_device) {
+        SLE_CUDA(cudaStreamSynchronize(s->st));
+        return SLE_OK;
+      }
+      src = out;
+      break;
+    }
     case SLE_F_R: src = D.g(G_RR, b); break;
     case SLE_F_DELTASL: src = D.g(G_DELTASL, b); break;
-    case SLE_F_ICESTAR: src = D.g(G_ICESTAR, b); break;
-    case SLE_F_OCEAN0: src = D.g(G_CXY0, b); break;
-    case SLE_F_BETA0: src = D.g(G_BETA0, b); break;
     case SLE_F_G:
       note_launch();
       k_grid_add<<<nb(D.ng), 256, 0, s->st>>>(D.ng, D.g(G_DELTASL, b), D.g(G_RR, b), D.g(G_TMP, b));
@@ -1775,7 +1839,7 @@ extern "C" int sle_batch_info(const sle_batch* b, int* nslots, int* max_modes, l
   if (max_modes) *max_modes = b->K;
   if (device_bytes) {
     const long long B = b->nslot, ng = b->D.ng, nc = b->D.ncoef, K = b->K, nl = b->D.nl;
-    *device_bytes = B * (NGRID * ng * 8 + NSPEC * nc * 16 + K * nc * 16 + 5 * K * nl * 8 + 3 * nl * 8 +
+    *device_bytes = B * (NGRID * ng * 8 + NMASK * ng + NSPEC * nc * 16 + K * nc * 16 + 5 * K * nl * 8 + 3 * nl * 8 +
                          (long long)sizeof(Scal) + b->D.npart * 8 + 4LL * b->cfg.nlat * 8);
   }
   return SLE_OK;
