@@ -117,8 +117,8 @@ struct GlobalPairRows {
 
 // Rows of an analysis source (FieldSpec kinds: grid, mask, ice on a mask, T0 (C* - C*0),
 // dsl C*) for latitude pairs j0, j0 + 1, ...; two cells per complex point.
+template <int KIND>
 struct TypedPairRows {
-  int kind;
   const double* g;
   const unsigned char* m0;
   const unsigned char* m1;
@@ -126,7 +126,7 @@ struct TypedPairRows {
   __device__ __forceinline__ double2 operator()(int r, int i) const {
     const int j = j0 + (r >> 1);
     const int row = (r & 1) ? nlat - 1 - j : j;
-    return src_pair(kind, g, m0, m1, (size_t)row * nlon + 2 * i);
+    return src_pair<KIND>(g, m0, m1, (size_t)row * nlon + 2 * i);
   }
 };
 

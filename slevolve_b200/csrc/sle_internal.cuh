@@ -68,7 +68,7 @@ struct ShtDev {
   const int* gclr[MAXF];
   // mixed-precision transforms (set once the plan prepared them)
   const float2* twf;          // [n2] FP32 twiddles of the mixed-precision row FFTs
-  float* mx_xf;               // [MX_MAXF][nm][nh][4] folded FP32 rFFT (S.re, S.im, D.re, D.im)
+  float* mx_xf;               // [MX_MAXF][nm][2][nh][2] folded FP32 rFFT: S, D (complex) per order
   float2* mx_gns;             // [MX_MAXF][nh][nm][2] north / south Legendre sums (synthesis)
   float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (tile order)
   double* mx_s0;              // [MX_MAXF][nh] FP64 fold of the row sums (degree 0)
@@ -106,20 +106,41 @@ struct FieldSpec {
   const unsigned char* m1;
 };
 
-// Two neighbouring cells c, c + 1 (c even) of an analysis source.
-__device__ __forceinline__ double2 src_pair(int kind, const double* g, const unsigned char* m0,
-                                            const unsigned char* m1, size_t c) {
-  if (kind == SRC_GRID) return __ldg(reinterpret_cast<const double2*>(g + c));
-  const uchar2 a = *reinterpret_cast<const uchar2*>(m0 + c);
-  if (kind == SRC_MASK) return make_double2(a.x ? 1.0 : 0.0, a.y ? 1.0 : 0.0);
-  const double2 v = __ldg(reinterpret_cast<const double2*>(g + c));
-  if (kind == SRC_ICE) return make_double2(a.x ? v.x : __dmul_rn(v.x, 0.0), a.y ? v.y : __dmul_rn(v.y, 0.0));
-  if (kind == SRC_TO) {
-    const uchar2 z = *reinterpret_cast<const uchar2*>(m1 + c);
-    return make_double2(__dmul_rn(v.x, __dsub_rn(a.x ? 1.0 : 0.0, z.x ? 1.0 : 0.0)),
-                        __dmul_rn(v.y, __dsub_rn(a.y ? 1.0 : 0.0, z.y ? 1.0 : 0.0)));
+// Two neighbouring cells c, c + 1 (c even) of an analysis source of kind KIND.
+template <int KIND>
+__device__ __forceinline__ double2 src_pair(const double* g, const unsigned char* m0, const unsigned char* m1,
+                                            size_t c) {
+  if constexpr (KIND == SRC_GRID) {
+    return __ldg(reinterpret_cast<const double2*>(g + c));
+  } else if constexpr (KIND == SRC_MASK) {
+    const uchar2 a = *reinterpret_cast<const uchar2*>(m0 + c);
+    return make_double2(a.x ? 1.0 : 0.0, a.y ? 1.0 : 0.0);
+  } else {
+    const uchar2 a = *reinterpret_cast<const uchar2*>(m0 + c);
+    const double2 v = __ldg(reinterpret_cast<const double2*>(g + c));
+    if constexpr (KIND == SRC_ICE) {
+      return make_double2(a.x ? v.x : __dmul_rn(v.x, 0.0), a.y ? v.y : __dmul_rn(v.y, 0.0));
+    } else if constexpr (KIND == SRC_TO) {
+      const uchar2 z = *reinterpret_cast<const uchar2*>(m1 + c);
+      return make_double2(__dmul_rn(v.x, __dsub_rn(a.x ? 1.0 : 0.0, z.x ? 1.0 : 0.0)),
+                          __dmul_rn(v.y, __dsub_rn(a.y ? 1.0 : 0.0, z.y ? 1.0 : 0.0)));
+    } else {
+      return make_double2(__dmul_rn(v.x, a.x ? 1.0 : 0.0), __dmul_rn(v.y, a.y ? 1.0 : 0.0));
+    }
   }
-  return make_double2(__dmul_rn(v.x, a.x ? 1.0 : 0.0), __dmul_rn(v.y, a.y ? 1.0 : 0.0));
+}
+
+// Calls body.template operator()<KIND>() for the run-time source kind (one branch per block, so
+// each kind's loads stay straight-line code).
+template <typename Body>
+__device__ __forceinline__ void with_src_kind(int kind, const Body& body) {
+  switch (kind) {
+    case SRC_MASK: body.template operator()<SRC_MASK>(); break;
+    case SRC_ICE: body.template operator()<SRC_ICE>(); break;
+    case SRC_TO: body.template operator()<SRC_TO>(); break;
+    case SRC_PROD: body.template operator()<SRC_PROD>(); break;
+    default: body.template operator()<SRC_GRID>(); break;
+  }
 }
 
 // Fields of one mixed-precision transform launch.  Field f is skipped (its outputs left as

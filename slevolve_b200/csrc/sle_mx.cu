@@ -49,8 +49,8 @@ constexpr int TILE_A = TILE_F * 4;            // 16 KB
 constexpr int SLOT_WORDS = 2 * TILE_F;        // Legendre table slot: FP32 A tiles of both parities
 constexpr uint32_t SLOT_BYTES = 4u * SLOT_WORDS;
 constexpr int TILE_B = MX_NMAX * 128;         // MX_NMAX rows x 128 bytes = 8 KB
-constexpr int STAGE_BYTES = 4 * TILE_A + 4 * TILE_B;
-constexpr int NSTAGE = 2;
+constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;   // one parity of a chunk: A hi / lo, B hi / lo
+constexpr int NSTAGE = 4;
 constexpr int MISC_BYTES = 1024;              // barriers + bookkeeping
 constexpr int MX_SMEM = 1024 + NSTAGE * STAGE_BYTES + MISC_BYTES;
 constexpr int W_SPL = 4;                      // warps 4..11: splitters (two groups of four)
@@ -103,12 +103,13 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                : "memory");
 }
 
-// 3-D TMA tensor load (tile mode, no multicast) of the tensor map's box at (x, y, z).
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t mbar) {
+// 4-D TMA tensor load (tile mode, no multicast) of the tensor map's box at (x, y, z, w).
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, int w,
+                                            uint32_t mbar) {
   asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
-          "r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(mbar)
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(mbar)
       : "memory");
 }
 
@@ -232,24 +233,18 @@ __device__ __forceinline__ bool field_off(const MxFieldArgs& a, int f) {
   return false;
 }
 
-// Shared memory of a stage: A tiles [par0 hi][par1 hi][par0 lo][par1 lo] (a Legendre table
-// slot, FP32, lands in the hi pair and is split in place), then B tiles [par0 hi][par1 hi]
-// [par0 lo][par1 lo] (the raw B data lands in the lo pair).
+// Shared memory of a stage (one parity of one chunk): A tiles [hi][lo] (the parity's FP32
+// Legendre tile lands in hi and is split in place), then B tiles [hi][lo] (the raw B data lands
+// in lo).
 struct Smem {
   uint8_t* base;        // generic pointer, 1024-aligned
   uint32_t sbase;       // shared-window address of base
-  __device__ uint32_t a_tile(int stage, int par, int lo) const {
-    return sbase + stage * STAGE_BYTES + (lo * 2 + par) * TILE_A;
+  __device__ uint32_t a_tile(int stage, int lo) const { return sbase + stage * STAGE_BYTES + lo * TILE_A; }
+  __device__ uint8_t* a_ptr(int stage, int lo) const { return base + stage * STAGE_BYTES + lo * TILE_A; }
+  __device__ uint32_t b_tile(int stage, int lo) const {
+    return sbase + stage * STAGE_BYTES + 2 * TILE_A + lo * TILE_B;
   }
-  __device__ uint8_t* a_ptr(int stage, int par, int lo) const {
-    return base + stage * STAGE_BYTES + (lo * 2 + par) * TILE_A;
-  }
-  __device__ uint32_t b_tile(int stage, int par, int lo) const {
-    return sbase + stage * STAGE_BYTES + 4 * TILE_A + (lo * 2 + par) * TILE_B;
-  }
-  __device__ uint8_t* b_ptr(int stage, int par, int lo) const {
-    return base + stage * STAGE_BYTES + 4 * TILE_A + (lo * 2 + par) * TILE_B;
-  }
+  __device__ uint8_t* b_ptr(int stage, int lo) const { return base + stage * STAGE_BYTES + 2 * TILE_A + lo * TILE_B; }
   __device__ uint8_t* misc() const { return base + NSTAGE * STAGE_BYTES; }
 };
 
@@ -259,10 +254,10 @@ __device__ __forceinline__ Smem smem_layout(uint8_t* raw) {
   return Smem{raw + (al - s), al};
 }
 
-// Barriers: full[2] (splitters -> MMA), empty[2] (MMA commit -> loader), raw[2] (copies
+// Barriers: full[4] (splitters -> MMA), empty[4] (MMA commit -> loader), raw[4] (copies
 // landed -> splitters), accum[2] (a unit's MMAs done -> epilogue, per TMEM set), tfree[2]
 // (epilogue done with a TMEM set -> MMA), drain (MMAs issued before an abort).
-enum { BAR_FULL = 0, BAR_EMPTY = 2, BAR_RAW = 4, BAR_ACCUM = 6, BAR_TFREE = 8, BAR_DRAIN = 10 };
+enum { BAR_FULL = 0, BAR_EMPTY = 4, BAR_RAW = 8, BAR_ACCUM = 12, BAR_TFREE = 14, BAR_DRAIN = 16 };
 struct Misc {
   uint64_t* bar;
   uint32_t* tmem_holder;
@@ -274,8 +269,8 @@ struct Misc {
 __device__ __forceinline__ Misc misc_layout(const Smem& S) {
   uint8_t* p = S.misc();
   Misc m;
-  m.bar = reinterpret_cast<uint64_t*>(p);
-  m.tmem_holder = reinterpret_cast<uint32_t*>(p + 128);
+  m.bar = reinterpret_cast<uint64_t*>(p);                      // 17 barriers
+  m.tmem_holder = reinterpret_cast<uint32_t*>(p + 192);
   m.active = reinterpret_cast<int*>(p + 256);
   m.any = reinterpret_cast<int*>(p + 256 + 4 * MX_MAXF);
   m.units = reinterpret_cast<int4*>(p + 512);
@@ -291,30 +286,24 @@ __device__ __forceinline__ int main_buffers(int nch, int ncols) {
   return max(1, min(nch, ((int)SET_COLS - 2 * ncols) / (2 * ncols)));
 }
 
-// MMAs of one chunk (stage st) into the set at `set_base`; chunk k of its unit.  The K sub-block
-// kk starts 32 kk bytes into the tile rows: +2 kk in the descriptor's start-address field.
-__device__ __forceinline__ void mma_chunk(const Smem& S, uint32_t set_base, int st, int k, int nbuf, int ncols) {
+// MMAs of one parity `par` of chunk k of a unit (stage st) into the set at `set_base`.  The K
+// sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the descriptor's start-address
+// field.
+__device__ __forceinline__ void mma_half(const Smem& S, uint32_t set_base, int st, int par, int k, int nbuf,
+                                         int ncols) {
   const uint32_t idesc = idesc_tf32(128, ncols);
-  const uint32_t dmain = set_base + (uint32_t)(2 * ncols * (1 + k % nbuf));
+  const uint32_t off = (uint32_t)(par * ncols);
+  const uint32_t dmain = set_base + (uint32_t)(2 * ncols * (1 + k % nbuf)) + off;
+  const uint32_t dcorr = set_base + off;
   const bool fresh = k < nbuf;
-  uint64_t ah[2], al[2], bh[2], bl[2];
-#pragma unroll
-  for (int par = 0; par < 2; ++par) {
-    ah[par] = sdesc_sw128(S.a_tile(st, par, 0));
-    al[par] = sdesc_sw128(S.a_tile(st, par, 1));
-    bh[par] = sdesc_sw128(S.b_tile(st, par, 0));
-    bl[par] = sdesc_sw128(S.b_tile(st, par, 1));
-  }
+  const uint64_t ah = sdesc_sw128(S.a_tile(st, 0)), al = sdesc_sw128(S.a_tile(st, 1));
+  const uint64_t bh = sdesc_sw128(S.b_tile(st, 0)), bl = sdesc_sw128(S.b_tile(st, 1));
 #pragma unroll
   for (int kk = 0; kk < KC / 8; ++kk) {
-#pragma unroll
-    for (int par = 0; par < 2; ++par) {
-      const uint64_t d = (uint64_t)(2 * kk);
-      const uint32_t off = (uint32_t)(par * ncols);
-      tc_mma_tf32(dmain + off, ah[par] + d, bh[par] + d, idesc, (fresh && kk == 0) ? 0u : 1u);
-      tc_mma_tf32(set_base + off, ah[par] + d, bl[par] + d, idesc, (k == 0 && kk == 0) ? 0u : 1u);
-      tc_mma_tf32(set_base + off, al[par] + d, bh[par] + d, idesc, 1u);
-    }
+    const uint64_t d = (uint64_t)(2 * kk);
+    tc_mma_tf32(dmain, ah + d, bh + d, idesc, (fresh && kk == 0) ? 0u : 1u);
+    tc_mma_tf32(dcorr, ah + d, bl + d, idesc, (k == 0 && kk == 0) ? 0u : 1u);
+    tc_mma_tf32(dcorr, al + d, bh + d, idesc, 1u);
   }
 }
 
@@ -353,10 +342,12 @@ __device__ uint32_t prologue(const Misc& M, const MxFieldArgs& a, const int4* un
     if (u < nunits) M.units[threadIdx.x] = units[u];
   }
   if (threadIdx.x == 0) {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < NSTAGE; ++i) {
       mbar_init(M.b(BAR_FULL + i), 4);    // the 4 splitter warps of the stage
       mbar_init(M.b(BAR_EMPTY + i), 1);   // one tcgen05.commit
       mbar_init(M.b(BAR_RAW + i), 1);     // loader's expect_tx
+    }
+    for (int i = 0; i < 2; ++i) {
       mbar_init(M.b(BAR_ACCUM + i), 1);   // one tcgen05.commit (or arrive for an empty unit)
       mbar_init(M.b(BAR_TFREE + i), 4);   // the 4 epilogue warps
     }
@@ -472,9 +463,9 @@ __global__ void __launch_bounds__(128) k_tab_syn(ShtDev P, uint32_t* tab) {
 // A split: the FP32 Legendre values landed in the hi tiles of the stage; hi <- TF32(x) in
 // place, lo tile <- TF32(x - hi).  Elementwise, so the tile order does not matter.
 __device__ __forceinline__ void split_a(const Smem& S, int st, int tid) {
-  constexpr int NV = SLOT_WORDS / 4 / 128;   // 16-byte vectors per thread
-  uint4* hp = reinterpret_cast<uint4*>(S.a_ptr(st, 0, 0));
-  uint4* lp = reinterpret_cast<uint4*>(S.a_ptr(st, 0, 1));
+  constexpr int NV = TILE_F / 4 / 128;   // 16-byte vectors per thread
+  uint4* hp = reinterpret_cast<uint4*>(S.a_ptr(st, 0));
+  uint4* lp = reinterpret_cast<uint4*>(S.a_ptr(st, 1));
   uint4 v[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) v[q] = hp[tid + 128 * q];
@@ -490,22 +481,20 @@ __device__ __forceinline__ void split_a(const Smem& S, int st, int tid) {
   }
 }
 
-// Analysis B data: the TMA box of the folded FFT is [field][32 latitudes][S.re, S.im, D.re, D.im]
-// (16 bytes per entry) in the stage's B lo tiles; the 4 splitter warps read it, synchronise,
-// and write rows 2f / 2f+1 of the parity-0 (S) and parity-1 (D) tiles.
+// Analysis B data of one parity: the TMA box of the folded FFT is [field][32 latitudes][re, im]
+// (8 bytes per entry) in the stage's B lo tile; the 4 splitter warps read it, synchronise, and
+// write rows 2f (re) / 2f+1 (im) of the B hi / lo tiles.
 __device__ __forceinline__ void split_b_ana(const Smem& S, int st, int nf, int tid, int bar_id) {
-  const float4* box = reinterpret_cast<const float4*>(S.b_ptr(st, 0, 1));
-  float4 v[8];
+  const float2* box = reinterpret_cast<const float2*>(S.b_ptr(st, 1));
+  float2 v[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int e = tid + 128 * u;
-    v[u] = ((e >> 5) < nf) ? box[e] : make_float4(0.f, 0.f, 0.f, 0.f);
+    v[u] = ((e >> 5) < nf) ? box[e] : make_float2(0.f, 0.f);
   }
   named_bar(bar_id, 128);
-  uint32_t* h0 = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0, 0));
-  uint32_t* h1 = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1, 0));
-  uint32_t* l0 = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0, 1));
-  uint32_t* l1 = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1, 1));
+  uint32_t* hp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0));
+  uint32_t* lp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1));
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int e = tid + 128 * u;
@@ -514,32 +503,23 @@ __device__ __forceinline__ void split_b_ana(const Smem& S, int st, int nf, int t
     const int o0 = sw_off(2 * f, k), o1 = sw_off(2 * f + 1, k);
     uint32_t h, l;
     split_f32(v[u].x, h, l);
-    h0[o0] = h;
-    l0[o0] = l;
+    hp[o0] = h;
+    lp[o0] = l;
     split_f32(v[u].y, h, l);
-    h0[o1] = h;
-    l0[o1] = l;
-    split_f32(v[u].z, h, l);
-    h1[o0] = h;
-    l1[o0] = l;
-    split_f32(v[u].w, h, l);
-    h1[o1] = h;
-    l1[o1] = l;
+    hp[o1] = h;
+    lp[o1] = l;
   }
 }
 
-// Synthesis B data: raw blocks already in the tile order; split in place.
+// Synthesis B data of one parity: the raw block is already in the tile order; split in place.
 __device__ __forceinline__ void split_b_syn(const Smem& S, int st, int nrow, int tid) {
-#pragma unroll
-  for (int par = 0; par < 2; ++par) {
-    uint32_t* hp = reinterpret_cast<uint32_t*>(S.b_ptr(st, par, 0));
-    uint32_t* lp = reinterpret_cast<uint32_t*>(S.b_ptr(st, par, 1));
-    for (int e = tid; e < nrow * KC; e += 128) {
-      uint32_t h, l;
-      split_f32(__uint_as_float(lp[e]), h, l);
-      hp[e] = h;
-      lp[e] = l;
-    }
+  uint32_t* hp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0));
+  uint32_t* lp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1));
+  for (int e = tid; e < nrow * KC; e += 128) {
+    uint32_t h, l;
+    split_f32(__uint_as_float(lp[e]), h, l);
+    hp[e] = h;
+    lp[e] = l;
   }
 }
 
@@ -552,9 +532,10 @@ __device__ __forceinline__ void unit_info(const ShtDev& P, const Misc& M, int u,
 
 // Persistent CTAs (one per SM) over the work units u = blockIdx.x + i gridDim.x.  Analysis
 // units: rows of D = degrees, columns = (Re, Im) of the fields; synthesis: rows = latitudes.
-// Roles: warp 13 streams the chunks of all the CTA's units through the two stages; warps 4-11
-// split stage g = (warp - 4) / 4; warp 12 issues the MMAs of unit i into TMEM set i & 1;
-// warps 0-3 drain set i & 1 for unit i while the MMAs of unit i + 1 run.
+// The CTA's work is a sequence of halves q = 2 (chunk) + parity: warp 13 streams each half's
+// Legendre tile and B data into stage q % 4; splitter group g = (warp - 4) / 4 splits the halves
+// of parity g; warp 12 issues the MMAs of unit i into TMEM set i & 1; warps 0-3 drain set i & 1
+// for unit i while the MMAs of unit i + 1 run.
 template <bool SYN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox, int nunits) {
@@ -570,43 +551,43 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
     const int nrow = 2 * a.nf;
     if (warp == W_LOAD) {
-      // ---- loader: chunk c of the CTA's sequence into stage c & 1
+      // ---- loader: half q of the CTA's sequence into stage q % NSTAGE
       if (lane == 0) {
-        const uint32_t bbytes = SYN ? 2u * (uint32_t)nrow * 128u : (uint32_t)zbox * 32u * 16u;
-        int c = 0, i = 0;
+        const uint32_t bbytes = SYN ? (uint32_t)nrow * 128u : (uint32_t)zbox * 32u * 8u;
+        int q = 0, i = 0;
         bool ok = true;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
           int4 unit;
           int nch;
           unit_info<SYN>(P, M, u, i, unit, nch);
-          for (int k = 0; k < nch; ++k, ++c) {
-            const int st = c & 1;
-            if (!mbar_wait(M.b(BAR_EMPTY + st), (uint32_t)(((c >> 1) & 1) ^ 1), ab)) {
+          for (int h = 0; h < 2 * nch; ++h, ++q) {
+            const int st = q % NSTAGE, k = h >> 1, par = h & 1;
+            if (!mbar_wait(M.b(BAR_EMPTY + st), (uint32_t)(((q / NSTAGE) & 1) ^ 1), ab)) {
               ok = false;
               break;
             }
             const uint32_t raw = M.b(BAR_RAW + st);
-            mbar_arrive_expect_tx(raw, SLOT_BYTES + bbytes);
-            bulk_g2s(S.a_tile(st, 0, 0), tab + ((long long)unit.w + k) * SLOT_WORDS, SLOT_BYTES, raw);
+            mbar_arrive_expect_tx(raw, (uint32_t)TILE_A + bbytes);
+            bulk_g2s(S.a_tile(st, 0), tab + ((long long)unit.w + k) * SLOT_WORDS + par * TILE_F, (uint32_t)TILE_A,
+                     raw);
             if (SYN) {
               const int seg = P.mx_syn_seg[unit.w + k];
-              bulk_g2s(S.b_tile(st, 0, 1), P.mx_bsyn + ((size_t)seg * 2 + 0) * BBLOCK, (uint32_t)nrow * 128u, raw);
-              bulk_g2s(S.b_tile(st, 1, 1), P.mx_bsyn + ((size_t)seg * 2 + 1) * BBLOCK, (uint32_t)nrow * 128u, raw);
+              bulk_g2s(S.b_tile(st, 1), P.mx_bsyn + ((size_t)seg * 2 + par) * BBLOCK, (uint32_t)nrow * 128u, raw);
             } else {
-              tma_load_3d(S.b_tile(st, 0, 1), &tmx, 4 * KC * (unit.z + k), unit.x, 0, raw);
+              tma_load_4d(S.b_tile(st, 1), &tmx, 2 * KC * (unit.z + k), par, unit.x, 0, raw);
             }
           }
         }
         // copies in flight land before the CTA exits: the last phase issued on each stage
-        for (int st = 0; st < 2; ++st) {
-          const int n_st = (c + 1 - st) / 2;   // loads issued on stage st
+        for (int st = 0; st < NSTAGE; ++st) {
+          const int n_st = (q + NSTAGE - 1 - st) / NSTAGE;   // loads issued on stage st
           if (n_st > 0) mbar_wait_drain(M.b(BAR_RAW + st), (uint32_t)((n_st - 1) & 1));
         }
       }
       __syncwarp();
     } else if (warp == W_MMA) {
       if (lane == 0) {
-        int c = 0, i = 0;
+        int q = 0, i = 0;
         bool ok = true, issued = false;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
           int4 unit;
@@ -617,14 +598,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           tc_fence_after();
           const uint32_t base = tmem + SET_COLS * (uint32_t)set;
           const int nbuf = main_buffers(nch, ncols);
-          for (int k = 0; k < nch; ++k, ++c) {
-            const int st = c & 1;
-            if (!mbar_wait(M.b(BAR_FULL + st), (uint32_t)((c >> 1) & 1), ab)) {
+          for (int h = 0; h < 2 * nch; ++h, ++q) {
+            const int st = q % NSTAGE;
+            if (!mbar_wait(M.b(BAR_FULL + st), (uint32_t)((q / NSTAGE) & 1), ab)) {
               ok = false;
               break;
             }
             tc_fence_after();
-            mma_chunk(S, base, st, k, nbuf, ncols);
+            mma_half(S, base, st, h & 1, h >> 1, nbuf, ncols);
             issued = true;
             tc_commit(M.b(BAR_EMPTY + st));
           }
@@ -640,29 +621,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
       __syncwarp();
     } else if (warp >= W_SPL) {
-      // ---- splitters: group g = stage g
+      // ---- splitters: group g takes the halves of parity g (stages g and g + 2)
       const int g = (warp - W_SPL) >> 2, tid = threadIdx.x - 32 * W_SPL - 128 * g;
-      int c = 0, i = 0;
+      int q = 0, i = 0;
       bool ok = true;
       for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
         int4 unit;
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
-        for (int k = 0; k < nch; ++k, ++c) {
-          if ((c & 1) != g) continue;
+        for (int h = 0; h < 2 * nch; ++h, ++q) {
+          if ((h & 1) != g) continue;
+          const int st = q % NSTAGE;
           // every wait is bounded, so all four warps of the group reach the vote; they go on
           // (and meet at the named barrier of the B split) only together
-          const bool w = mbar_wait(M.b(BAR_RAW + g), (uint32_t)((c >> 1) & 1), ab);
+          const bool w = mbar_wait(M.b(BAR_RAW + st), (uint32_t)((q / NSTAGE) & 1), ab);
           if (!bar_and(1 + g, 128, w)) {
             ok = false;
             break;
           }
-          split_a(S, g, tid);
-          if (SYN) split_b_syn(S, g, nrow, tid);
-          else split_b_ana(S, g, a.nf, tid, 1 + g);
+          split_a(S, st, tid);
+          if (SYN) split_b_syn(S, st, nrow, tid);
+          else split_b_ana(S, st, a.nf, tid, 1 + g);
           fence_proxy_async();
           __syncwarp();
-          if (lane == 0) mbar_arrive(M.b(BAR_FULL + g));
+          if (lane == 0) mbar_arrive(M.b(BAR_FULL + st));
         }
       }
     } else {
@@ -732,18 +714,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
 // ============================================================== row FFT kernels
 // Row rFFT in FP32 of the north and south rows of latitudes j0 = 2 blockIdx.x and j0 + 1 of
-// field blockIdx.y and the fold with the weights, output FP32: X[f][m][j] = (S.re, S.im, D.re,
-// D.im), 16 bytes per entry, latitude fastest (the two latitudes of a block fill one 32-byte
-// sector), the layout whose 32-latitude rows the analysis kernel's TMA box reads.  The m = 0
+// field blockIdx.y and the fold with the weights, output FP32: X[f][m][0][j] = S, X[f][m][1][j]
+// = D (complex, 8 bytes per entry), latitude fastest, the layout whose 32-latitude rows of one
+// parity the analysis kernel's TMA box reads.  The m = 0
 // fold (the weighted row sums) is formed in FP64 from the FP64 grid values, in s0[f][j], for the
 // FP64 degree-0 coefficient.
+template <int K>
 struct FoldSrcMx {
-  TypedPairRows src;
+  TypedPairRows<K> src;
   double* acc;          // this thread's FP64 sum of the values it reads (one row per thread)
   __device__ __forceinline__ float2 operator()(int r, int i) const {
     const double2 v = src(r, i);
     *acc = (*acc + v.x) + v.y;
     return make_float2((float)v.x, (float)v.y);
+  }
+};
+
+// The FP32 row FFTs of two latitude pairs for a source kind known at compile time.
+template <int N>
+struct FoldRowsMx {
+  const double* g;
+  const unsigned char* m0;
+  const unsigned char* m1;
+  int j0, nlat;
+  const float2* tw;
+  float2* A;
+  double* acc;
+  template <int K>
+  __device__ __forceinline__ void operator()() const {
+    fft_rows<4, N, false>(FoldSrcMx<K>{TypedPairRows<K>{g, m0, m1, j0, nlat, 2 * N}, acc}, A, tw,
+                          SmemRows<N, float2>{A});
   }
 };
 
@@ -756,8 +756,7 @@ __global__ void __launch_bounds__(fft_nt(4, N)) k_fold_mx(ShtDev P, MxFieldArgs 
   constexpr int NT = fft_nt(4, N);
   constexpr int Q = N / FftRadix<N, 1>::R;   // first-pass items per row: one per thread
   double acc = 0.0;
-  fft_rows<4, N, false>(FoldSrcMx{TypedPairRows{a.kind[f], a.grid[f], a.m0[f], a.m1[f], j0, P.nlat, 2 * N}, &acc},
-                        A, P.twf, SmemRows<N, float2>{A});
+  with_src_kind(a.kind[f], FoldRowsMx<N>{a.grid[f], a.m0[f], a.m1[f], j0, P.nlat, P.twf, A, &acc});
   // FP64 row sums: the Q threads r Q .. r Q + Q - 1 hold the partial sums of row r (Q a power
   // of two): a butterfly within aligned groups of min(Q, 32) lanes, then the warps of a row in
   // order
@@ -783,7 +782,7 @@ __global__ void __launch_bounds__(fft_nt(4, N)) k_fold_mx(ShtDev P, MxFieldArgs 
     __syncthreads();
   }
   const SmemRows<N, float2> Z{A};
-  float4* X = reinterpret_cast<float4*>(P.mx_xf) + (size_t)f * P.nm * P.nh;
+  float2* X = reinterpret_cast<float2*>(P.mx_xf) + (size_t)f * P.nm * P.nh * 2;
   for (int e = threadIdx.x; e < 2 * P.nm; e += NT) {
     // consecutive threads: the two latitudes of one order (one 32-byte sector of X)
     const int m = e >> 1, q = e & 1, j = j0 + q;
@@ -813,7 +812,8 @@ __global__ void __launch_bounds__(fft_nt(4, N)) k_fold_mx(ShtDev P, MxFieldArgs 
       // S_0(j) in FP64: the weighted sums of the north and south rows of latitude j
       P.mx_s0[(size_t)f * P.nh + j] = wn * rowtot[2 * q] + ws * rowtot[2 * q + 1];
     }
-    X[(size_t)m * P.nh + j] = make_float4(an.x + bs.x, an.y + bs.y, an.x - bs.x, an.y - bs.y);
+    X[((size_t)m * 2 + 0) * P.nh + j] = make_float2(an.x + bs.x, an.y + bs.y);   // S (even l - m)
+    X[((size_t)m * 2 + 1) * P.nh + j] = make_float2(an.x - bs.x, an.y - bs.y);   // D (odd l - m)
   }
 }
 
@@ -1034,19 +1034,19 @@ int sht_mx_prepare(sle_sht* p) {
   k_tab_syn<<<p->n_syn_units, 128>>>(d, p->mx_tab_syn);
   SLE_CUDA(cudaGetLastError());
   SLE_CUDA(cudaDeviceSynchronize());
-  // TMA maps of X[f][m][j][4]: dims (4 nh floats, nm orders, MX_MAXF fields), boxes (4 x 32
-  // latitudes, 1 order, 8 | 16 | 32 fields)
+  // TMA maps of X[f][m][par][j][2]: dims (2 nh floats, 2 parities, nm orders, MX_MAXF fields),
+  // boxes (2 x 32 latitudes, 1, 1, 8 | 16 | 32 fields)
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled is not available from the driver");
     return SLE_ERR_CUDA;
   }
   for (int zi = 0; zi < 3; ++zi) {
-    const cuuint64_t dims[3] = {(cuuint64_t)4 * d.nh, (cuuint64_t)d.nm, (cuuint64_t)MX_MAXF};
-    const cuuint64_t strides[2] = {(cuuint64_t)16 * d.nh, (cuuint64_t)16 * d.nh * d.nm};
-    const cuuint32_t box[3] = {4 * KC, 1, (cuuint32_t)ZBOX[zi]};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = enc(reinterpret_cast<CUtensorMap*>(p->mx_tmap[zi]), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+    const cuuint64_t dims[4] = {(cuuint64_t)2 * d.nh, 2, (cuuint64_t)d.nm, (cuuint64_t)MX_MAXF};
+    const cuuint64_t strides[3] = {(cuuint64_t)8 * d.nh, (cuuint64_t)16 * d.nh, (cuuint64_t)16 * d.nh * d.nm};
+    const cuuint32_t box[4] = {2 * KC, 1, 1, (cuuint32_t)ZBOX[zi]};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = enc(reinterpret_cast<CUtensorMap*>(p->mx_tmap[zi]), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
                            p->mx_xf, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

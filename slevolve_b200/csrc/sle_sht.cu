@@ -221,14 +221,28 @@ struct CSpecPtrs {
 // Row rFFT of the north row j and south row nlat-1-j of field blockIdx.y, then the fold
 // S = F_N w_j/nlon + F_S w_j/nlon, D = F_N w_j/nlon - F_S w_j/nlon for m <= lmax
 // (sht.py:277-287).  X layout [f][0=S,1=D][m][j].  N = nlon/2 complex points per row.
+// The row FFTs of one latitude pair for a source kind known at compile time.
+template <int N>
+struct FoldRows64 {
+  const double* g;
+  const unsigned char* m0;
+  const unsigned char* m1;
+  int j, nlat;
+  const double2* tw;
+  double2* A;
+  template <int K>
+  __device__ __forceinline__ void operator()() const {
+    fft_rows<2, N, false>(TypedPairRows<K>{g, m0, m1, j, nlat, 2 * N}, A, tw, SmemRows<N, double2>{A});
+  }
+};
+
 template <int N>
 __global__ void __launch_bounds__(fft_nt(2, N)) k_fft_fold(sle::ShtDev P, GridPtrs g) {
   extern __shared__ double2 sm[];
   double2* A = sm;
   const int j = blockIdx.x, f = blockIdx.y;
   if (field_gated_off(P, f)) return;
-  fft_rows<2, N, false>(TypedPairRows{g.kind[f], g.p[f], g.m0[f], g.m1[f], j, P.nlat, 2 * N}, A, P.tw,
-                        SmemRows<N, double2>{A});
+  with_src_kind(g.kind[f], FoldRows64<N>{g.p[f], g.m0[f], g.m1[f], j, P.nlat, P.tw, A});
   const SmemRows<N, double2> Z{A};
   const double wn = P.wn[j], ws = P.ws[j];
   double2* XS = P.X + ((size_t)(f * 2 + 0) * P.nm) * P.nh;

@@ -142,11 +142,12 @@ __device__ double block_sum(double v, double* sh) {
 }
 
 // After each block of the slot stored its partial, the last block to arrive sums the partials in
-// index order and returns true (in all its threads) with *total set; others return false.
+// index order and returns true (in all its threads) with *total set; others return false.  Only
+// thread 0's writes (the partial) are fenced before the block's ticket: a thread whose other
+// global writes the last block reads must __threadfence() them itself before calling.
 __device__ bool last_block_total(double part, double* partials, unsigned int* counter, double* total,
                                  double* sh) {
   __shared__ bool is_last;
-  __threadfence();  // every thread's earlier global writes are visible before the block's ticket
   __syncthreads();
   if (threadIdx.x == 0) {
     partials[blockIdx.x] = part;
@@ -169,11 +170,12 @@ __device__ bool last_block_total(double part, double* partials, unsigned int* co
 }
 
 // true in all threads of the slot's last block to finish (after every block passed this point)
+// The last block of the slot to arrive returns true (fencing as last_block_total).
 __device__ bool last_block(unsigned int* counter) {
   __shared__ bool is_last;
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
+    __threadfence();
     const unsigned int t = atomicAdd(counter, 1u);
     is_last = (t == gridDim.x - 1);
   }
@@ -333,14 +335,14 @@ __device__ void rot_advance_block(const Dev& D, int b, Scal* sc) {
 }
 
 // R_k <- d R_k + (1-d) P ; visc = sum_k a_sl R_k ; rad = sum_k a_rr R_k   (solver.py:386-407)
-// The last block of each slot advances the degree-2 rotational state instead.
+// The first block of each slot advances the degree-2 rotational state instead.
 __global__ void __launch_bounds__(256) k_advance(Dev D) {
   SLOT_OR_RETURN();
-  if (blockIdx.x == gridDim.x - 1) {
+  if (blockIdx.x == 0) {   // scheduled first: its serial work overlaps the grid
     rot_advance_block(D, b, sc);
     return;
   }
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = (long long)(blockIdx.x - 1) * blockDim.x + threadIdx.x;
   if (i >= D.ncoef) return;
   double2* R = D.R + (size_t)b * D.K * D.ncoef;
   const int l = D.lidx[i];
@@ -348,7 +350,9 @@ __global__ void __launch_bounds__(256) k_advance(Dev D) {
   const size_t o = D.kl(b);
   double2 v = make_double2(0.0, 0.0), r = v;
   const int nk = D.nmod[(size_t)b * D.nl + l];
-  constexpr int U = 4;
+  // modes in groups of 8: the group's state loads before its stores; the coefficient tables are
+  // read-only (__ldg), so their loads are free to move
+  constexpr int U = 8;
   for (int k0 = 0; k0 < nk; k0 += U) {
     double2 x[U];
 #pragma unroll
@@ -359,7 +363,8 @@ __global__ void __launch_bounds__(256) k_advance(Dev D) {
       const int k = k0 + u;
       if (k < nk) {
         const size_t kl = o + (size_t)k * D.nl + l;
-        const double d = D.decay[kl], om = D.omd[kl], as = D.a_sl[kl], ar = D.a_rr[kl];
+        const double d = __ldg(D.decay + kl), om = __ldg(D.omd + kl), as = __ldg(D.a_sl + kl),
+                     ar = __ldg(D.a_rr + kl);
         double2 y;
         y.x = __dadd_rn(__dmul_rn(x[u].x, d), __dmul_rn(p.x, om));
         y.y = __dadd_rn(__dmul_rn(x[u].y, d), __dmul_rn(p.y, om));
@@ -410,14 +415,30 @@ __global__ void k_ice_grid(Dev D) {
 }
 
 // The rotation block (solver.py:910-975) for the coming inner iteration, one thread; writes
-// il, m, Lambda, their increments and the degree-2 rotational sea-level / radial terms.
+// il, m, Lambda, their increments and the degree-2 rotational sea-level / radial terms.  Runs
+// in the one-block control kernels (k_rotation, k_loop_cond), one thread per slot.
 __device__ void rotation_block(const Dev& D, int b, Scal* sc) {
   const RotConst& C = D.rc[b];
   const double2* dScur = D.sp(S_DSCUR, b);
   const double2* dI = D.sp(S_DI, b);
-  // written by other blocks of the same kernel: read through L2
+  // every input first: the record's fields are global memory and the stores below could alias
+  // them as far as the compiler knows (each load of this serial code is a round trip)
   const double2 s20 = __ldcg(dScur + D.i20), s21 = __ldcg(dScur + D.i21);
   const double2 i20 = __ldcg(dI + D.i20), i21 = __ldcg(dI + D.i21);
+  double sum_il[9], sum_m[3], sum_tsl[6], sum_trr[6], dprev[6], oldil[9], oldm[3];
+  for (int q = 0; q < 9; ++q) {
+    sum_il[q] = sc->sum_il[q];
+    oldil[q] = sc->oldil[q];
+  }
+  for (int q = 0; q < 3; ++q) {
+    sum_m[q] = sc->sum_m[q];
+    oldm[q] = sc->oldm[q];
+  }
+  for (int q = 0; q < 6; ++q) {
+    sum_tsl[q] = sc->sum_tsl[q];
+    sum_trr[q] = sc->sum_trr[q];
+    dprev[q] = sc->dlam_prev2[q];
+  }
   const double z20r = __dadd_rn(__dmul_rn(C.rhow, s20.x), __dmul_rn(C.rhoi, i20.x));
   const double z21r = __dadd_rn(__dmul_rn(C.rhow, s21.x), __dmul_rn(C.rhoi, i21.x));
   const double z21i = __dadd_rn(__dmul_rn(C.rhow, s21.y), __dmul_rn(C.rhoi, i21.y));
@@ -429,10 +450,10 @@ __device__ void rotation_block(const Dev& D, int b, Scal* sc) {
   il[5] = __dmul_rn(C.c_il12, z21i);
   double mm[3];
   for (int i = 0; i < 2; ++i) {
-    const double a = __dadd_rn(__dmul_rn(C.onepk, il[i * 3 + 2]), sc->sum_il[i * 3 + 2]);
-    mm[i] = __dmul_rn(C.alpha, __dadd_rn(__dmul_rn(C.inv_CmA, a), __dmul_rn(C.inv_kf, sc->sum_m[i])));
+    const double a = __dadd_rn(__dmul_rn(C.onepk, il[i * 3 + 2]), sum_il[i * 3 + 2]);
+    mm[i] = __dmul_rn(C.alpha, __dadd_rn(__dmul_rn(C.inv_CmA, a), __dmul_rn(C.inv_kf, sum_m[i])));
   }
-  mm[2] = __dmul_rn(-C.inv_C, __dadd_rn(__dmul_rn(C.onepk, il[8]), sc->sum_il[8]));
+  mm[2] = __dmul_rn(-C.inv_C, __dadd_rn(__dmul_rn(C.onepk, il[8]), sum_il[8]));
   const double m1 = mm[0], m2 = mm[1], m3 = mm[2];
   const double m1s = __dmul_rn(m1, m1), m2s = __dmul_rn(m2, m2), m3s = __dmul_rn(m3, m3);
   double lam[18];
@@ -444,25 +465,31 @@ __device__ void rotation_block(const Dev& D, int b, Scal* sc) {
   lam[15] = __dmul_rn(-C.r2w2_s30, __dmul_rn(-m2, op));
   lam[16] = __dmul_rn(C.r2w2_s120, __dsub_rn(m2s, m1s));
   lam[17] = __dmul_rn(C.r2w2_s120, __dmul_rn(__dmul_rn(2.0, m1), m2));
+  double dsl_rot[6], rr_rot[6], dcur[6];
   for (int q = 0; q < 3; ++q) {
-    const double dr = __dsub_rn(lam[12 + 2 * q], sc->dlam_prev2[2 * q]);
-    const double di = __dsub_rn(lam[13 + 2 * q], sc->dlam_prev2[2 * q + 1]);
-    const double tr = __dadd_rn(sc->dlam_prev2[2 * q], dr);
-    const double ti = __dadd_rn(sc->dlam_prev2[2 * q + 1], di);
-    sc->dsl_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, tr), sc->sum_tsl[2 * q]), C.gacc);
-    sc->dsl_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, ti), sc->sum_tsl[2 * q + 1]), C.gacc);
-    sc->rr_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, tr), sc->sum_trr[2 * q]), C.gacc);
-    sc->rr_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, ti), sc->sum_trr[2 * q + 1]), C.gacc);
-    sc->dlam_cur2[2 * q] = dr;
-    sc->dlam_cur2[2 * q + 1] = di;
+    const double dr = __dsub_rn(lam[12 + 2 * q], dprev[2 * q]);
+    const double di = __dsub_rn(lam[13 + 2 * q], dprev[2 * q + 1]);
+    const double tr = __dadd_rn(dprev[2 * q], dr);
+    const double ti = __dadd_rn(dprev[2 * q + 1], di);
+    dsl_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, tr), sum_tsl[2 * q]), C.gacc);
+    dsl_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, ti), sum_tsl[2 * q + 1]), C.gacc);
+    rr_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, tr), sum_trr[2 * q]), C.gacc);
+    rr_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, ti), sum_trr[2 * q + 1]), C.gacc);
+    dcur[2 * q] = dr;
+    dcur[2 * q + 1] = di;
+  }
+  for (int q = 0; q < 6; ++q) {
+    sc->dsl_rot[q] = dsl_rot[q];
+    sc->rr_rot[q] = rr_rot[q];
+    sc->dlam_cur2[q] = dcur[q];
   }
   for (int q = 0; q < 9; ++q) {
     sc->il[q] = il[q];
-    sc->dil[q] = __dsub_rn(il[q], sc->oldil[q]);
+    sc->dil[q] = __dsub_rn(il[q], oldil[q]);
   }
   for (int q = 0; q < 3; ++q) {
     sc->mm[q] = mm[q];
-    sc->dm[q] = __dsub_rn(mm[q], sc->oldm[q]);
+    sc->dm[q] = __dsub_rn(mm[q], oldm[q]);
   }
   for (int q = 0; q < 18; ++q) sc->lam[q] = lam[q];
 }
@@ -519,10 +546,7 @@ __global__ void k_pre_spec(Dev D) {
   const double part = block_sum(acc, sh);
   double tot;
   if (last_block_total(part, D.partials + (size_t)b * D.npart, D.counter + 4 * b, &tot, sh)) {
-    if (threadIdx.x == 0) {
-      sc->so = tot;
-      if (D.tpw) rotation_block(D, b, sc);
-    }
+    if (threadIdx.x == 0) sc->so = tot;
   }
 }
 
@@ -623,8 +647,7 @@ __global__ void k_sltot(Dev D) {
 }
 
 // deltasl (dsl identity) and, when not converged, the ocean function of the refreshed
-// topography and the grounded-ice test on it (solver.py:1032-1037, 661-684).  One extra block
-// per slot (the last) evaluates the rotation block of the next iteration meanwhile.
+// topography and the grounded-ice test on it (solver.py:1032-1037, 661-684).
 __global__ void k_refresh1(Dev D) {
   SLOT_OR_RETURN();
   __shared__ double sh[32];
@@ -632,28 +655,28 @@ __global__ void k_refresh1(Dev D) {
   const bool test = !conv && D.checkmarine && sc->gr_nacc < GR_MAXACC;
   const double cadd = D.opt_dsl ? __dmul_rn(sc->conserv, sc->K00) : 0.0;
   double cnt = 0.0;
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0 && !conv && D.tpw) rotation_block(D, b, sc);
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h < D.ng) {
-    double ds[2];
+    // every input first (the stores below could alias them as far as the compiler knows)
     double* deltasl = D.g(G_DELTASL, b);
+    const double2 a = ld2(D.opt_dsl ? D.g(G_DSL, b) : deltasl, h);
+    double2 ti = make_double2(0.0, 0.0), ic = ti;
+    uchar2 be = make_uchar2(0, 0);
+    if (!conv) ti = ld2(D.g(G_TINIT, b), h);
+    if (test) {
+      ic = ld2(D.g(G_ICE, b), h);
+      be = ldm2(D.m(M_BETA, b), h);
+    }
+    double ds[2] = {a.x, a.y};
     if (D.opt_dsl) {
-      const double2 a = ld2(D.g(G_DSL, b), h);
       ds[0] = __dadd_rn(a.x, cadd);
       ds[1] = __dadd_rn(a.y, cadd);
       st2(deltasl, h, ds[0], ds[1]);
-    } else {
-      const double2 a = ld2(deltasl, h);
-      ds[0] = a.x;
-      ds[1] = a.y;
     }
     if (!conv) {
-      const double2 ti = ld2(D.g(G_TINIT, b), h);
       const double t0 = __dsub_rn(ti.x, ds[0]), t1 = __dsub_rn(ti.y, ds[1]);
       stm2(D.m(M_CXY, b), h, t0 < 0.0, t1 < 0.0);
       if (test) {
-        const double2 ic = ld2(D.g(G_ICE, b), h);
-        const uchar2 be = ldm2(D.m(M_BETA, b), h);
         const bool k0 = icestar_keep(ic.x, t0, D.rhow, D.rhoi), k1 = icestar_keep(ic.y, t1, D.rhow, D.rhoi);
         const double g0 = k0 ? ic.x : __dmul_rn(ic.x, 0.0), g1 = k1 ? ic.y : __dmul_rn(ic.y, 0.0);
         stm2(D.m(M_GRNEW, b), h, k0, k1);
@@ -686,29 +709,33 @@ __global__ void k_refresh2(Dev D) {
   SLOT_OR_RETURN();
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h >= D.ng || sc->converged) return;
-  uchar2 bt;
-  if (sc->gr_changed) {
-    const uchar2 k = ldm2(D.m(M_GRNEW, b), h);
-    const double2 ic = ld2(D.g(G_ICE, b), h);
+  const bool changed = sc->gr_changed != 0;
+  // every input first (the stores below could alias them as far as the compiler knows)
+  const uchar2 cx = ldm2(D.m(M_CXY, b), h), prev = ldm2(D.m(M_CSTAR, b), h);
+  uchar2 k = make_uchar2(0, 0), bt = make_uchar2(0, 0);
+  double2 ic = make_double2(0.0, 0.0);
+  if (changed) {
+    k = ldm2(D.m(M_GRNEW, b), h);
+    ic = ld2(D.g(G_ICE, b), h);
+  } else {
+    bt = ldm2(D.m(M_BETA, b), h);
+  }
+  if (changed) {
     const double g0 = k.x ? ic.x : __dmul_rn(ic.x, 0.0), g1 = k.y ? ic.y : __dmul_rn(ic.y, 0.0);
     reinterpret_cast<uchar2*>(D.m(M_GR, b))[h] = k;
     bt = make_uchar2(g0 < EPS0, g1 < EPS0);
     reinterpret_cast<uchar2*>(D.m(M_BETA, b))[h] = bt;
-  } else {
-    bt = ldm2(D.m(M_BETA, b), h);
   }
-  const uchar2 cx = ldm2(D.m(M_CXY, b), h);
   const uchar2 c = make_uchar2(cx.x && bt.x, cx.y && bt.y);
   // C* and tO only change where a cell of C* flips; without a flip their re-analyses are
   // skipped (the inputs, hence the spectra, are bit-identical to the last ones)
-  const uchar2 prev = ldm2(D.m(M_CSTAR, b), h);
   if (prev.x != c.x || prev.y != c.y) {
     sc->cs_changed = 1;
     reinterpret_cast<uchar2*>(D.m(M_CSTAR, b))[h] = c;
   }
 }
 
-// dice, dI after a grounded-mask change; the slot's last block re-evaluates the rotation block
+// dice, dI after a grounded-mask change
 __global__ void k_dice(Dev D) {
   SLOT_OR_RETURN();
   if (sc->converged || !sc->gr_changed) return;
@@ -719,12 +746,20 @@ __global__ void k_dice(Dev D) {
     D.sp(S_DICE, b)[i] = d;
     D.sp(S_DI, b)[i] = make_double2(__dadd_rn(p.x, d.x), __dadd_rn(p.y, d.y));
   }
-  if (!D.tpw) return;
-  if (last_block(D.counter + 4 * b + 2) && threadIdx.x == 0) rotation_block(D, b, sc);
 }
 
 // End of an inner iteration: slots that converged (or failed) are done from the next iteration
-// on; the loop goes on while any slot is not.  A raised tensor-core timeout ends every slot.
+// on; the loop goes on while any slot is not, and each such slot (one thread per slot) evaluates
+// the rotation block of its next iteration.  A raised tensor-core timeout ends every slot.
+// The rotation block of the first inner iteration of every stepping slot (one thread per slot),
+// after the step prologue has formed dS_cur and dI.
+__global__ void k_rotation(Dev D) {
+  for (int b = threadIdx.x; b < D.nslot; b += blockDim.x) {
+    Scal* sc = D.sc + b;
+    if (!sc->done && D.tpw) rotation_block(D, b, sc);
+  }
+}
+
 __global__ void k_loop_cond(Dev D, const int* bstatus, cudaGraphConditionalHandle loop) {
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
@@ -737,8 +772,14 @@ __global__ void k_loop_cond(Dev D, const int* bstatus, cudaGraphConditionalHandl
       if (sc->status == 0) sc->status = bs;
       sc->converged = 1;
     }
-    if (sc->converged) sc->done = 1;
-    else atomicOr(&any, 1);
+    if (sc->converged) {
+      sc->done = 1;
+    } else {
+      atomicOr(&any, 1);
+      // the rotation block of the coming iteration (solver.py:910-975) from this iteration's
+      // dS_cur and the current dI (after a grounded re-guess, the re-analysed one)
+      if (D.tpw) rotation_block(D, b, sc);
+    }
   }
   __syncthreads();
   if (threadIdx.x == 0 && loop) cudaGraphSetConditional(loop, any ? 1u : 0u);
@@ -1107,7 +1148,7 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
     SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sltot.data(), (int)s->f_syn_sltot.size(), st));
   }
   note_launch(2);
-  k_refresh1<<<dim3(nb(ng / 2) + 1, B), 256, 0, st>>>(D);
+  k_refresh1<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
   k_refresh2<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
   // I* (only when the grounded mask changed), C* and tO for the next iteration; skipped for
   // slots that converged
@@ -1570,8 +1611,9 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
     SLE_TRY(sht_analysis_list(s->plan, f.data(), (int)f.size(), st));
   }
   // ---- first guess
-  note_launch();
+  note_launch(2);
   k_pre_spec<<<dim3(nb(nc), UB), 256, 0, st>>>(D);
+  k_rotation<<<1, 128, 0, st>>>(D);
   SLE_CUDA(cudaGetLastError());
 
   // ---- inner fixed-point loop (solver.py:907-1051): a CUDA graph whose WHILE condition is set
