@@ -93,11 +93,11 @@ __host__ __device__ constexpr int fpad(int p) { return p + (p >> 3); }
 inline size_t fft_smem_bytes(int nr, int n2, size_t entry) { return (size_t)(fpad(nr * n2) + 4 * nr + 1) * entry; }
 
 // Sources and sinks of a pass: (row r, index i) -> value.  The row offset is one 16-byte entry
-// (8 per 128-byte bank row) or four 8-byte entries (16 per bank row): rows two apart then land
-// in disjoint halves of the banks.
+// (8 per 128-byte bank row) or two 8-byte entries (16 per bank row): the same index of rows two
+// apart then lands in different banks (four such rows, in four disjoint quarters).
 template <int N, typename V>
 struct SmemRows {
-  static constexpr int ROFF = sizeof(V) == 16 ? 1 : 4;
+  static constexpr int ROFF = sizeof(V) == 16 ? 1 : 2;
   V* a;
   __device__ __forceinline__ V operator()(int r, int i) const { return a[fpad(r * N + i) + ROFF * r]; }
   __device__ __forceinline__ void put(int r, int i, V v) const { a[fpad(r * N + i) + ROFF * r] = v; }

@@ -62,7 +62,8 @@ constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wa
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t SET_COLS = 256;            // two accumulator sets (units alternate)
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
-constexpr int MAX_CTA_UNITS = 16;             // work units per CTA staged in shared memory
+constexpr int MAX_CTA_UNITS = 16;
+constexpr int FOLD_NR = 8;                    // rows of a fold block: 4 latitude pairs             // work units per CTA staged in shared memory
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
 
 static_assert(MX_SMEM <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
@@ -713,10 +714,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 // ============================================================== row FFT kernels
-// Row rFFT in FP32 of the north and south rows of latitudes j0 = 2 blockIdx.x and j0 + 1 of
+// Row rFFT in FP32 of the north and south rows of latitudes j0 = 4 blockIdx.x .. j0 + 3 of
 // field blockIdx.y and the fold with the weights, output FP32: X[f][m][0][j] = S, X[f][m][1][j]
-// = D (complex, 8 bytes per entry), latitude fastest, the layout whose 32-latitude rows of one
-// parity the analysis kernel's TMA box reads.  The m = 0
+// = D (complex, 8 bytes per entry), latitude fastest (the four latitudes of a block fill one
+// 32-byte sector of each), the layout whose 32-latitude rows of one parity the analysis
+// kernel's TMA box reads.  The m = 0
 // fold (the weighted row sums) is formed in FP64 from the FP64 grid values, in s0[f][j], for the
 // FP64 degree-0 coefficient.
 template <int K>
@@ -742,38 +744,39 @@ struct FoldRowsMx {
   double* acc;
   template <int K>
   __device__ __forceinline__ void operator()() const {
-    fft_rows<4, N, false>(FoldSrcMx<K>{TypedPairRows<K>{g, m0, m1, j0, nlat, 2 * N}, acc}, A, tw,
-                          SmemRows<N, float2>{A});
+    fft_rows<FOLD_NR, N, false>(FoldSrcMx<K>{TypedPairRows<K>{g, m0, m1, j0, nlat, 2 * N}, acc}, A, tw,
+                                SmemRows<N, float2>{A});
   }
 };
 
 template <int N>
-__global__ void __launch_bounds__(fft_nt(4, N)) k_fold_mx(ShtDev P, MxFieldArgs a) {
+__global__ void __launch_bounds__(fft_nt(FOLD_NR, N)) k_fold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ float2 smf2[];
   float2* A = smf2;
-  const int j0 = 2 * blockIdx.x, f = blockIdx.y;
+  constexpr int NLAT = FOLD_NR / 2;          // latitudes of the block
+  const int j0 = NLAT * blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
-  constexpr int NT = fft_nt(4, N);
+  constexpr int NT = fft_nt(FOLD_NR, N);
   constexpr int Q = N / FftRadix<N, 1>::R;   // first-pass items per row: one per thread
   double acc = 0.0;
   with_src_kind(a.kind[f], FoldRowsMx<N>{a.grid[f], a.m0[f], a.m1[f], j0, P.nlat, P.twf, A, &acc});
   // FP64 row sums: the Q threads r Q .. r Q + Q - 1 hold the partial sums of row r (Q a power
   // of two): a butterfly within aligned groups of min(Q, 32) lanes, then the warps of a row in
   // order
-  __shared__ double rowtot[4];
+  __shared__ double rowtot[FOLD_NR];
   {
     const int t = threadIdx.x;
-    double v = (t < 4 * Q) ? acc : 0.0;
+    double v = (t < FOLD_NR * Q) ? acc : 0.0;
     constexpr int W = Q < 32 ? Q : 32;
 #pragma unroll
     for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if constexpr (Q <= 32) {
-      if (t < 4 * Q && t % Q == 0) rowtot[t / Q] = v;
+      if (t < FOLD_NR * Q && t % Q == 0) rowtot[t / Q] = v;
     } else {
       __shared__ double wsum[NT / 32];
       if ((t & 31) == 0) wsum[t >> 5] = v;
       __syncthreads();
-      if (t < 4) {
+      if (t < FOLD_NR) {
         double sum = 0.0;
         for (int w = t * (Q / 32); w < (t + 1) * (Q / 32); ++w) sum += wsum[w];
         rowtot[t] = sum;
@@ -783,9 +786,9 @@ __global__ void __launch_bounds__(fft_nt(4, N)) k_fold_mx(ShtDev P, MxFieldArgs 
   }
   const SmemRows<N, float2> Z{A};
   float2* X = reinterpret_cast<float2*>(P.mx_xf) + (size_t)f * P.nm * P.nh * 2;
-  for (int e = threadIdx.x; e < 2 * P.nm; e += NT) {
-    // consecutive threads: the two latitudes of one order (one 32-byte sector of X)
-    const int m = e >> 1, q = e & 1, j = j0 + q;
+  for (int e = threadIdx.x; e < NLAT * P.nm; e += NT) {
+    // consecutive threads: the latitudes of one order (one 32-byte sector of each X plane)
+    const int m = e / NLAT, q = e % NLAT, j = j0 + q;
     float2 xr[2];
     const float2 twm = (m > 0 && m < N) ? __ldg(P.twf + m) : make_float2(1.f, 0.f);
 #pragma unroll
@@ -898,7 +901,7 @@ __global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
   blk[sw_off(2 * f + 1, k)] = (float)(u.y * SQRT2_LEGACY);
 }
 
-size_t mx_fold_smem(const ShtDev& d) { return fft_smem_bytes(4, d.n2, sizeof(float2)); }
+size_t mx_fold_smem(const ShtDev& d) { return fft_smem_bytes(FOLD_NR, d.n2, sizeof(float2)); }
 size_t mx_unfold_smem(const ShtDev& d) { return fft_smem_bytes(2, d.n2, sizeof(float2)); }
 
 template <typename T>
@@ -1097,7 +1100,8 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t
   SLE_TRY(mx_check_args(a, "mixed analysis"));
   const ShtDev& d = p->d;
   ProfToken t0 = prof_begin(PROF_FFT, a.nf, st);
-#define SLE_LAUNCH_MXF(NN) k_fold_mx<NN><<<dim3(d.nh / 2, a.nf), fft_threads(4, NN), mx_fold_smem(d), st>>>(d, a)
+#define SLE_LAUNCH_MXF(NN) \
+  k_fold_mx<NN><<<dim3(d.nh / (FOLD_NR / 2), a.nf), fft_threads(FOLD_NR, NN), mx_fold_smem(d), st>>>(d, a)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXF)
 #undef SLE_LAUNCH_MXF
   prof_end(t0, st);
