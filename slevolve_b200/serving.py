@@ -337,3 +337,29 @@ def run_ensemble(requests, precision="mixed", slots=None, autotune=True, candida
     st.update({"slots": {str(k): v for k, v in slots.items()}, "autotune_member_steps_per_s": tuned,
                "members": {str(L): sum(1 for r in requests if r.lmax == L) for L in degrees}})
     return st
+
+
+# ------------------------------------------------------------ several GPUs
+def request_cost(r):
+    """Estimated work of a request: (lmax + 1)^3 per step (the transforms' contraction) x steps x
+    passes."""
+    return (r.lmax + 1) ** 3 * r.nsteps * max(1, getattr(r, "outer_passes", 1))
+
+
+def shard_requests(requests, rank, world):
+    """The requests rank ``rank`` of ``world`` GPUs runs: sorted by estimated work (most first,
+    ties by id) and dealt round robin, so that the shards are disjoint, cover every request and
+    carry similar work.  Independent members: no data moves between ranks."""
+    order = sorted(requests, key=lambda r: (-request_cost(r), r.rid))
+    return [r for i, r in enumerate(order) if i % world == rank]
+
+
+def max_over_ranks(x, dist=None, device="cuda"):
+    """max of ``x`` over the ranks of the default process group (``x`` itself without one)."""
+    if dist is None or not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
