@@ -205,6 +205,13 @@ int sle_batch_set_reuse(sle_batch* b, int slot, void* ds_store, void* mask_store
  * (its record says which; failed slots are not committed, the others are). */
 int sle_batch_step(sle_batch* b, const double* const* ice, int on_device, const double* dt_years,
                    sle_step_info* info);
+/* sle_batch_step in two halves, so that the caller can overlap a step with its own work (e.g.
+ * the upload of the next step's ice on another stream): _begin enqueues the step on the batch's
+ * stream and returns; _end waits for it and fills info as sle_batch_step does.  Between the two,
+ * the ice buffers given to _begin must stay valid and unchanged, and no other sle_batch_* call
+ * on this batch is allowed (they return SLE_ERR_STATE).  No counterpart in the reference. */
+int sle_batch_step_begin(sle_batch* b, const double* const* ice, int on_device, const double* dt_years);
+int sle_batch_step_end(sle_batch* b, sle_step_info* info);
 /* copy one output of a slot's last step (as sle_solver_get) */
 int sle_batch_get(sle_batch* b, int slot, int field, void* dst, int dst_on_device);
 int sle_batch_stream(sle_batch* b, void** stream);

@@ -148,6 +148,70 @@ class SolverBatch:
         _lib.check(rc, "sle_batch_step")
         return out
 
+    def step_begin(self, ptrs, on_device, dts=None):
+        """Enqueue one step from raw grid pointers ({slot: pointer}) and return at once; the
+        grids must stay valid and unchanged until ``step_end``."""
+        for i in range(self.nslots):
+            self._ice_ptrs[i] = None
+            self._dts[i] = 0.0
+        for slot, ptr in ptrs.items():
+            self._ice_ptrs[slot] = ptr
+            if dts and slot in dts and dts[slot]:
+                self._dts[slot] = float(dts[slot])
+        self._pending = list(ptrs)
+        _lib.check(self._L.sle_batch_step_begin(self._h, self._ice_ptrs, int(on_device), self._dts),
+                   "sle_batch_step_begin")
+
+    def step_end(self):
+        """Wait for the step enqueued by ``step_begin``; returns {slot: SleStepInfo} and raises
+        like ``step_ptrs`` when a slot failed."""
+        rc = self._L.sle_batch_step_end(self._h, self._infos)
+        out = {slot: self._infos[slot] for slot in getattr(self, "_pending", [])}
+        self._pending = []
+        _lib.check(rc, "sle_batch_step_end")
+        return out
+
+    def step_host_stream(self, host_steps, dts=None):
+        """Step once per element of ``host_steps`` (a sequence of {slot: host grid}, NumPy arrays or
+        CPU tensors, ideally in pinned memory), uploading step k + 1's ice on a copy stream while
+        step k runs (two device staging grids per slot).  Returns the list of {slot: SleStepInfo}.
+        The results are those of calling ``step`` once per element."""
+        import torch
+
+        n = len(host_steps)
+        if n == 0:
+            return []
+        slots = sorted(host_steps[0])
+        stage = [{s: torch.empty((self.nlat, self.nlon), dtype=torch.float64, device="cuda") for s in slots}
+                 for _ in range(2)]
+        copy = torch.cuda.Stream()
+        batch_stream = torch.cuda.ExternalStream(self.stream_handle())
+        landed = [torch.cuda.Event(), torch.cuda.Event()]
+        copy.wait_stream(torch.cuda.current_stream())
+        copy.wait_stream(batch_stream)
+
+        def upload(k):
+            if sorted(host_steps[k]) != slots:
+                raise ValueError("every step of host_steps must give ice for the same slots")
+            with torch.cuda.stream(copy):
+                for s, h in host_steps[k].items():
+                    src = h if isinstance(h, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(h, np.float64))
+                    if tuple(src.shape) != (self.nlat, self.nlon):
+                        raise ValueError(f"ice shape {tuple(src.shape)} != {(self.nlat, self.nlon)}")
+                    stage[k % 2][s].copy_(src, non_blocking=True)
+                landed[k % 2].record(copy)
+
+        upload(0)
+        out = []
+        for k in range(n):
+            batch_stream.wait_event(landed[k % 2])
+            self.step_begin({s: stage[k % 2][s].data_ptr() for s in slots}, 1, dts)
+            if k + 1 < n:
+                upload(k + 1)   # into the grids step k - 1 read (it has ended)
+            out.append(self.step_end())
+        copy.synchronize()
+        return out
+
     def step(self, ices, dts=None):
         """ices: {slot: grid (NumPy array or CUDA tensor)}; returns {slot: info dict}."""
         if not ices:

@@ -47,7 +47,6 @@ constexpr int KC = 32;                        // K elements per chunk: one 128-b
 constexpr int TILE_F = 128 * KC;              // words of one A tile (128 rows x 32)
 constexpr int TILE_A = TILE_F * 4;            // 16 KB
 constexpr int SLOT_WORDS = 2 * TILE_F;        // Legendre table slot: FP32 A tiles of both parities
-constexpr uint32_t SLOT_BYTES = 4u * SLOT_WORDS;
 constexpr int TILE_B = MX_NMAX * 128;         // MX_NMAX rows x 128 bytes = 8 KB
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;   // one parity of a chunk: A hi / lo, B hi / lo
 constexpr int NSTAGE = 4;
@@ -211,6 +210,17 @@ __device__ __forceinline__ void raise_abort(const Abort& ab) {
   if (ab.status) atomicExch(ab.status, SLE_ERR_TIMEOUT);
 }
 
+__device__ __forceinline__ bool mbar_test_wait(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Wait for the completion of the phase of parity `parity`; false (abort raised) after the time
 // limit or as soon as another CTA raised the abort flag.
 __device__ __noinline__ bool mbar_wait(uint32_t a, uint32_t parity, const Abort& ab) {
@@ -226,6 +236,26 @@ __device__ __noinline__ bool mbar_wait(uint32_t a, uint32_t parity, const Abort&
     }
   }
   return true;
+}
+
+// The same for the single-thread roles (loader, MMA issuer): an inline test first, then a spin
+// on the non-suspending test_wait, so the thread resumes as soon as the phase completes.
+__device__ __noinline__ bool mbar_spin_slow(uint32_t a, uint32_t parity, const Abort& ab) {
+  const long long t0 = clock64();
+  int spins = 0;
+  while (!mbar_test_wait(a, parity)) {
+    if ((++spins & 1023) == 0) {
+      if (*reinterpret_cast<volatile int*>(ab.flag) != 0) return false;
+      if (clock64() - t0 > WAIT_LIMIT) {
+        raise_abort(ab);
+        return false;
+      }
+    }
+  }
+  return true;
+}
+__device__ __forceinline__ bool mbar_spin(uint32_t a, uint32_t parity, const Abort& ab) {
+  return mbar_test_wait(a, parity) || mbar_spin_slow(a, parity, ab);
 }
 
 __device__ __forceinline__ bool field_off(const MxFieldArgs& a, int f) {
@@ -563,7 +593,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           unit_info<SYN>(P, M, u, i, unit, nch);
           for (int h = 0; h < 2 * nch; ++h, ++q) {
             const int st = q % NSTAGE, k = h >> 1, par = h & 1;
-            if (!mbar_wait(M.b(BAR_EMPTY + st), (uint32_t)(((q / NSTAGE) & 1) ^ 1), ab)) {
+            if (!mbar_spin(M.b(BAR_EMPTY + st), (uint32_t)(((q / NSTAGE) & 1) ^ 1), ab)) {
               ok = false;
               break;
             }
@@ -595,13 +625,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           int nch;
           unit_info<SYN>(P, M, u, i, unit, nch);
           const int set = i & 1;
-          if (!mbar_wait(M.b(BAR_TFREE + set), (uint32_t)(((i >> 1) & 1) ^ 1), ab)) break;
+          if (!mbar_spin(M.b(BAR_TFREE + set), (uint32_t)(((i >> 1) & 1) ^ 1), ab)) break;
           tc_fence_after();
           const uint32_t base = tmem + SET_COLS * (uint32_t)set;
           const int nbuf = main_buffers(nch, ncols);
           for (int h = 0; h < 2 * nch; ++h, ++q) {
             const int st = q % NSTAGE;
-            if (!mbar_wait(M.b(BAR_FULL + st), (uint32_t)((q / NSTAGE) & 1), ab)) {
+            if (!mbar_spin(M.b(BAR_FULL + st), (uint32_t)((q / NSTAGE) & 1), ab)) {
               ok = false;
               break;
             }

@@ -1025,6 +1025,10 @@ struct sle_batch {
   cudaGraph_t loop_graph;
   cudaGraphExec_t loop_exec;
   int use_graph;
+  // a step enqueued by batch_step_begin and not yet finished by batch_step_end
+  bool pending = false;
+  bool pending_graph = false;
+  std::vector<int> pending_act;
   long long body_launches;   // kernels in one iteration of the graph body
   // static field lists of the loop body
   std::vector<FieldSpec> f_syn_sl, f_ana_ro, f_syn_sltot, f_ana_refresh;
@@ -1214,6 +1218,10 @@ int build_loop_graph(sle_batch* s) {
 }
 
 int check_slot(const sle_batch* s, int slot, const char* what) {
+  if (s->pending) {
+    set_error("%s: a step is in flight (end it with sle_batch_step_end first)", what);
+    return SLE_ERR_STATE;
+  }
   if (slot < 0 || slot >= s->nslot) {
     set_error("%s: slot %d outside 0..%d", what, slot, s->nslot - 1);
     return SLE_ERR_BAD_ARG;
@@ -1535,8 +1543,13 @@ int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
 }
 
 // One time step of the slots with ice[b] != NULL.
-int batch_step(sle_batch* s, const double* const* ice, int on_device, const double* dt_years,
-               sle_step_info* info) {
+// Enqueue one step of the slots with ice[b] != NULL on the batch's stream; batch_step_end waits
+// for it and reads the slots' records.
+int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, const double* dt_years) {
+  if (s->pending) {
+    set_error("sle_batch_step_begin: the previous step was not ended");
+    return SLE_ERR_STATE;
+  }
   const Dev& D = s->D;
   cudaStream_t st = s->st;
   const long long nc = D.ncoef, ng = D.ng;
@@ -1550,6 +1563,9 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
     }
     act.push_back(b);
   }
+  s->pending_act = act;
+  s->pending_graph = false;
+  s->pending = true;
   if (act.empty()) return SLE_OK;
   // per-slot step parameters
   for (int b = 0; b < B; ++b) s->hss[b] = SlotStep{0, 0, 0, 0, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr};
@@ -1620,6 +1636,7 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
   // at the end of each iteration (any slot unconverged); with per-kernel profiling on, the same
   // sequence is driven from the host.
   const bool graph_step = s->use_graph && !prof_enabled();
+  s->pending_graph = graph_step;
   if (graph_step) {
     if (!s->loop_exec) SLE_TRY(build_loop_graph(s));
     SLE_CUDA(cudaGraphLaunch(s->loop_exec, st));
@@ -1667,6 +1684,18 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
     k_diag00<<<UB, 32, 0, st>>>(D);
   }
   SLE_CUDA(cudaGetLastError());
+  return SLE_OK;
+}
+
+int batch_step_end(sle_batch* s, sle_step_info* info) {
+  if (!s->pending) {
+    set_error("sle_batch_step_end: no step was begun");
+    return SLE_ERR_STATE;
+  }
+  s->pending = false;
+  const std::vector<int> act = s->pending_act;
+  const bool graph_step = s->pending_graph;
+  if (act.empty()) return SLE_OK;
   SLE_TRY(sync_scal(s));
   int first_bad = SLE_OK;
   int maxiter = 0;
@@ -1724,6 +1753,19 @@ int batch_step(sle_batch* s, const double* const* ice, int on_device, const doub
     if (info) info[b] = o;
   }
   return first_bad;
+}
+
+int batch_step(sle_batch* s, const double* const* ice, int on_device, const double* dt_years,
+               sle_step_info* info) {
+  const int rc = batch_step_begin(s, ice, on_device, dt_years);
+  if (rc != SLE_OK) {
+    if (s->pending) {   // a launch failed part-way: wait for what was enqueued before reporting
+      s->pending = false;
+      cudaStreamSynchronize(s->st);
+    }
+    return rc;
+  }
+  return batch_step_end(s, info);
 }
 
 int batch_get(sle_batch* s, int b, int field, void* dst, int dst_on_device) {
@@ -1852,6 +1894,28 @@ extern "C" int sle_batch_step(sle_batch* b, const double* const* ice, int on_dev
     return SLE_ERR_BAD_ARG;
   }
   return batch_step(b, ice, on_device, dt_years, info);
+}
+
+extern "C" int sle_batch_step_begin(sle_batch* b, const double* const* ice, int on_device,
+                                    const double* dt_years) {
+  if (!b || !ice) {
+    set_error("sle_batch_step_begin: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  const int rc = batch_step_begin(b, ice, on_device, dt_years);
+  if (rc != SLE_OK && b->pending) {
+    b->pending = false;
+    cudaStreamSynchronize(b->st);
+  }
+  return rc;
+}
+
+extern "C" int sle_batch_step_end(sle_batch* b, sle_step_info* info) {
+  if (!b) {
+    set_error("sle_batch_step_end: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  return batch_step_end(b, info);
 }
 
 extern "C" int sle_batch_get(sle_batch* b, int slot, int field, void* dst, int dst_on_device) {

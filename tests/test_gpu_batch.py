@@ -135,6 +135,41 @@ def test_mixed_slot_alone_equals_in_mix():
             _same(_snap(bt, s, infos[s]), solo[i][k - 1], (i, k))
 
 
+def test_host_stream_equals_step_by_step():
+    """step_host_stream (uploads overlapping the previous step's compute, begin / end halves of
+    the C step) gives bit for bit the results of one ``step`` call per step; slot calls are
+    refused while a step is in flight."""
+    import torch
+
+    ms = _members()[:3]
+    nsteps = 4
+    host = [{s: torch.from_numpy(np.ascontiguousarray(m["ice"](k))).pin_memory() for s, m in enumerate(ms)}
+            for k in range(1, nsteps + 1)]
+    a = _batch("mixed", 3)
+    b = _batch("mixed", 3)
+    for s, m in enumerate(ms):
+        a.load(s, m["love"], m["topo"], m["ice"](0), m["dt"])
+        b.load(s, m["love"], m["topo"], m["ice"](0), m["dt"])
+    ref = []
+    for k in range(nsteps):
+        infos = a.step({s: host[k][s].numpy() for s in range(3)})
+        ref.append((infos, {s: {f: a.get(s, f).copy() for f in FIELDS} for s in range(3)}))
+    recs = b.step_host_stream(host[:-1])
+    infos = b.step_host_stream(host[-1:])
+    recs += infos
+    for s in range(3):
+        assert recs[-1][s].numiter == ref[-1][0][s]["numiter"]
+        for f in FIELDS:
+            assert np.array_equal(b.get(s, f), ref[-1][1][s][f]), (s, f)
+    assert [[r[s].numiter for s in range(3)] for r in recs] == [[x[0][s]["numiter"] for s in range(3)]
+                                                               for x in ref]
+    ptr = torch.zeros((N, 2 * N), dtype=torch.float64, device="cuda")
+    b.step_begin({0: ptr.data_ptr()}, 1)
+    with pytest.raises(RuntimeError, match="in flight"):
+        b.release(0)
+    b.step_end()
+
+
 def test_mixed_batch_within_1mm_of_fp64():
     """Mixed-precision slots against the FP64 solve of the same member (the 1 mm bar)."""
     ms = _members()[:2]
