@@ -166,7 +166,8 @@ class SolverBatch:
         """Wait for the step enqueued by ``step_begin``; returns {slot: SleStepInfo} and raises
         like ``step_ptrs`` when a slot failed."""
         rc = self._L.sle_batch_step_end(self._h, self._infos)
-        out = {slot: self._infos[slot] for slot in getattr(self, "_pending", [])}
+        # copies: the record buffer is reused by the next step
+        out = {slot: _lib.SleStepInfo.from_buffer_copy(self._infos[slot]) for slot in getattr(self, "_pending", [])}
         self._pending = []
         _lib.check(rc, "sle_batch_step_end")
         return out
