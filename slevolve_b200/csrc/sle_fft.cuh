@@ -35,9 +35,9 @@ __device__ __forceinline__ V mul_mi(V a, bool inv) {
 // in[j + r q] (q = N/R, k = j mod Ns) through the twiddles exp(-+2 pi i r k/(Ns R)) and an
 // R-point DFT in registers to out[(j - k) R + k + r Ns].  Every thread reads its inputs into
 // registers before the block synchronises and overwrites the row, so one buffer of 2N points
-// suffices.  tw[t] = exp(-2 pi i t / (2 N)) for t < N (global memory, read through the
-// read-only cache); larger t use tw[t - N] = -exp(...).  The first pass may read from any
-// source (global rows, a fused pre-processing step) and the last may write to any sink.
+// suffices.  The twiddles come from the table laid out below (global memory, read through the
+// read-only cache).  The first pass may read from any source (global rows, a fused
+// pre-processing step) and the last may write to any sink.
 template <bool INV, typename V>
 __device__ __forceinline__ void dft8(V (&v)[8]) {
   using S = typename ScalarOf<V>::type;
@@ -81,26 +81,44 @@ __device__ __forceinline__ void dft_r(V (&v)[R]) {
   }
 }
 
+// Twiddle table of an N-point transform (nlon = 2N real points).  Entries t < N hold
+// exp(-2 pi i t / (2N)).  After them, for each pass of sub-transform size NS > 1 (NS = 8, 64, ...:
+// every pass before the last has radix 8) and radix R, the factors the pass multiplies by,
+// W(u k 2N / (NS R)) for u = 1 .. R-1 and k < NS, at index N + NS - 8 + (u - 1) NS + k, with
+// W(t) = tw[t] for t < N and -tw[t - N] above: the threads of a warp (consecutive k) read
+// consecutive entries.  tw_table_len(N) entries in all.
+__host__ __device__ constexpr int tw_pass_index(int n, int ns, int u, int k) { return n + ns - 8 + (u - 1) * ns + k; }
+__host__ __device__ constexpr int tw_table_len(int n) { return n >= 8 ? 2 * n - 8 : n; }
+
 // Row-FFT blocks transform NR rows of N points (NR = 2: the north and south rows of one
 // latitude pair; NR = 4: two pairs); one radix-8 butterfly per thread and pass.
 __host__ __device__ constexpr int fft_nt(int nr, int n2) { return nr * n2 / 8 > 32 ? nr * n2 / 8 : 32; }
 inline int fft_threads(int nr, int n2) { return fft_nt(nr, n2); }
 
-// Shared-memory rows are padded by one entry every 8 (16-byte entries), and row r starts r
-// entries further on: the stride-8 writes of the first pass, the unit-stride accesses of the
-// others and same-index accesses to different rows are then free of bank conflicts.
+// Shared-memory row layouts, chosen so that the accesses of the passes are free of bank conflicts
+// (a warp's 16-byte accesses are served eight threads at a time, 8-byte ones sixteen at a time):
+// the stride-8 writes of the first pass, the stride-8 groups of the NS = 8 pass, the unit-stride
+// accesses of the others, and same-index accesses to different rows in the fold's epilogue.
+// 16-byte entries (8 per 128-byte bank row): one padding entry every 8, row r starts r entries
+// further on.  8-byte entries (16 per bank row): row r at r (N + 2), and within a row index i is
+// stored at i XOR s(i), s(i) = bits 4, 5, 6 of i in bits 0, 1, 2 and bit 6 again in bit 3, a
+// permutation within each aligned group of 16 (the identity below 16).
 __host__ __device__ constexpr int fpad(int p) { return p + (p >> 3); }
 inline size_t fft_smem_bytes(int nr, int n2, size_t entry) { return (size_t)(fpad(nr * n2) + 4 * nr + 1) * entry; }
 
-// Sources and sinks of a pass: (row r, index i) -> value.  The row offset is one 16-byte entry
-// (8 per 128-byte bank row) or two 8-byte entries (16 per bank row): the same index of rows two
-// apart then lands in different banks (four such rows, in four disjoint quarters).
+// Sources and sinks of a pass: (row r, index i) -> value.
 template <int N, typename V>
 struct SmemRows {
-  static constexpr int ROFF = sizeof(V) == 16 ? 1 : 2;
   V* a;
-  __device__ __forceinline__ V operator()(int r, int i) const { return a[fpad(r * N + i) + ROFF * r]; }
-  __device__ __forceinline__ void put(int r, int i, V v) const { a[fpad(r * N + i) + ROFF * r] = v; }
+  __device__ __forceinline__ static int slot(int r, int i) {
+    if constexpr (sizeof(V) == 16) {
+      return fpad(r * N + i) + r;
+    } else {
+      return r * (N + 2) + (i ^ (((i >> 4) & 7) | ((i >> 3) & 8)));
+    }
+  }
+  __device__ __forceinline__ V operator()(int r, int i) const { return a[slot(r, i)]; }
+  __device__ __forceinline__ void put(int r, int i, V v) const { a[slot(r, i)] = v; }
 };
 // Grid rows of latitude pairs j0, j0 + 1, ...: row r = north (r even) or south (r odd) row of
 // pair r / 2.  `rowlen` points per row.
@@ -155,7 +173,7 @@ __device__ __forceinline__ void fft_pass(const Src& src, const Dst& dst, const V
   constexpr int NT = fft_nt(NR, N);
   constexpr int Q = N / R;
   constexpr int IT = (NR * Q + NT - 1) / NT;
-  constexpr int TSTEP = 2 * N / (NS * R);
+  static_assert(NS == 1 || NS >= 8, "every pass before the last has radix 8");
   V v[IT][R];
 #pragma unroll
   for (int it = 0; it < IT; ++it) {
@@ -165,15 +183,10 @@ __device__ __forceinline__ void fft_pass(const Src& src, const Dst& dst, const V
       const int k = j % NS;
       V w[R];
       if (NS > 1) {
+        const V* tp = tw + tw_pass_index(N, NS, 1, k);
 #pragma unroll
         for (int u = 1; u < R; ++u) {
-          const int t = u * k * TSTEP;
-          if (t < N) {
-            w[u] = __ldg(tw + t);
-          } else {
-            w[u] = __ldg(tw + (t - N));
-            w[u] = mkc(-w[u].x, -w[u].y);
-          }
+          w[u] = __ldg(tp + (u - 1) * NS);
           if (INV) w[u].y = -w[u].y;
         }
       }

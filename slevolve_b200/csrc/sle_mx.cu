@@ -19,11 +19,12 @@
 // output grid in FP64.  The tensor core's FP32 accumulation truncates, so the large products are
 // spread over fresh TMEM accumulators that the epilogue adds in FP64.
 //
-// Kernel structure (persistent: one CTA per SM over the work units, 14 warps, two stages):
-//   warp 13     loader: per K-chunk of every unit of the CTA, one bulk copy of the FP32 A tiles
-//               (32 KB) and the B data (analysis: one 3-D TMA tensor load of the folded FFT;
-//               synthesis: bulk copies) into stage c & 1
-//   warps 4-11  stage 0 / 1 splitters: A and B -> TF32 hi / lo tiles
+// Kernel structure (persistent: one CTA per SM over the work units, 14 warps, four stages of
+// one half each, a half being one parity of one 32-wide K chunk):
+//   warp 13     loader: per half, one bulk copy of the FP32 A tile (16 KB) and the B data
+//               (analysis: one 4-D TMA tensor load of the folded FFT; synthesis: one bulk copy)
+//               into stage q % 4
+//   warps 4-11  splitters, group g = parity g: A and B -> TF32 hi / lo tiles
 //   warp 12     allocates TMEM and issues the MMAs from one thread, unit i into TMEM set i & 1
 //   warps 0-3   epilogue: read set i & 1 out of TMEM while the MMAs of unit i + 1 run
 // Stages hand over through mbarriers; tcgen05.commit releases a stage when its MMAs are done.
@@ -61,8 +62,8 @@ constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wa
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t SET_COLS = 256;            // two accumulator sets (units alternate)
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
-constexpr int MAX_CTA_UNITS = 16;
-constexpr int FOLD_NR = 8;                    // rows of a fold block: 4 latitude pairs             // work units per CTA staged in shared memory
+constexpr int MAX_CTA_UNITS = 16;            // work units per CTA staged in shared memory
+constexpr int FOLD_NR = 8;                    // rows of a fold block: 4 latitude pairs
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
 
 static_assert(MX_SMEM <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
@@ -780,7 +781,7 @@ struct FoldRowsMx {
 };
 
 template <int N>
-__global__ void __launch_bounds__(fft_nt(FOLD_NR, N)) k_fold_mx(ShtDev P, MxFieldArgs a) {
+__global__ void __launch_bounds__(fft_nt(FOLD_NR, N), fft_nt(FOLD_NR, N) <= 512 ? 3 : 1) k_fold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ float2 smf2[];
   float2* A = smf2;
   constexpr int NLAT = FOLD_NR / 2;          // latitudes of the block
@@ -986,13 +987,14 @@ int sht_mx_prepare(sle_sht* p) {
   SLE_CUDA(cudaMemset(p->mx_bsyn, 0, (size_t)d.nseg * 2 * BBLOCK * sizeof(float)));
   SLE_CUDA(cudaMemset(p->mx_abort, 0, sizeof(int)));
   {
-    // FP32 twiddles exp(-2 pi i t / nlon), rounded from the plan's FP64 ones
-    std::vector<double2> tw64(d.n2);
-    std::vector<float2> tw32(d.n2);
-    SLE_CUDA(cudaMemcpy(tw64.data(), p->tw, d.n2 * sizeof(double2), cudaMemcpyDeviceToHost));
-    for (int t = 0; t < d.n2; ++t) tw32[t] = make_float2((float)tw64[t].x, (float)tw64[t].y);
-    SLE_TRY(mx_alloc(&p->mx_twf, (size_t)d.n2));
-    SLE_CUDA(cudaMemcpy(p->mx_twf, tw32.data(), d.n2 * sizeof(float2), cudaMemcpyHostToDevice));
+    // FP32 twiddle table (same layout), rounded from the plan's FP64 one
+    const int ntw = tw_table_len(d.n2);
+    std::vector<double2> tw64(ntw);
+    std::vector<float2> tw32(ntw);
+    SLE_CUDA(cudaMemcpy(tw64.data(), p->tw, ntw * sizeof(double2), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < ntw; ++t) tw32[t] = make_float2((float)tw64[t].x, (float)tw64[t].y);
+    SLE_TRY(mx_alloc(&p->mx_twf, (size_t)ntw));
+    SLE_CUDA(cudaMemcpy(p->mx_twf, tw32.data(), ntw * sizeof(float2), cudaMemcpyHostToDevice));
   }
   // work units, most work first; each unit's chunks are contiguous slots of its Legendre table
   std::vector<unsigned char> ist(d.nseg);

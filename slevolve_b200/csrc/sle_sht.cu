@@ -749,7 +749,7 @@ static int plan_build(sle_sht* p, int nlat, int nlon, int lmax) {
   SLE_TRY(dalloc(&p->be, d.ncoef));
   SLE_TRY(dalloc(&p->cf, d.ncoef));
   SLE_TRY(dalloc(&p->istart, d.nseg));
-  SLE_TRY(dalloc(&p->tw, d.n2));
+  SLE_TRY(dalloc(&p->tw, tw_table_len(d.n2)));
   SLE_TRY(dalloc(&p->X, (size_t)MAXF * 2 * d.nm * d.nh));
   SLE_TRY(dalloc(&p->EO, (size_t)MAXF * 2 * d.nm * d.nh));
   SLE_TRY(dalloc(&p->packbuf, (size_t)MAXF * d.ncoef));
@@ -762,11 +762,31 @@ static int plan_build(sle_sht* p, int nlat, int nlon, int lmax) {
   SLE_CUDA(cudaMemcpy(p->segoff, segoff.data(), segoff.size() * sizeof(int), cudaMemcpyHostToDevice));
   SLE_CUDA(cudaMemcpy(p->seg_m, seg_m.data(), seg_m.size() * sizeof(int), cudaMemcpyHostToDevice));
   SLE_CUDA(cudaMemcpy(p->seg_l0, seg_l0.data(), seg_l0.size() * sizeof(int), cudaMemcpyHostToDevice));
-  // twiddles exp(-2 pi i t / nlon), from long-double sin/cos rounded once
-  std::vector<double2> tw(d.n2);
+  // twiddles exp(-2 pi i t / nlon), from long-double sin/cos rounded once, then the same values
+  // in the order each FFT pass reads them (layout in sle_fft.cuh)
+  std::vector<double2> tw(tw_table_len(d.n2));
   for (int t = 0; t < d.n2; ++t) {
     const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)nlon;
     tw[t] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  for (int ns = 1, n = d.n2; ns < n;) {
+    const int r = n / ns >= 8 ? 8 : n / ns;
+    if (ns > 1) {
+      for (int u = 1; u < r; ++u) {
+        for (int k = 0; k < ns; ++k) {
+          const int t = u * k * (2 * n / (ns * r));
+          const int at = tw_pass_index(n, ns, u, k);
+          if (at >= (int)tw.size() || t >= 2 * n) {
+            set_error("twiddle table: index %d of %zu out of range", at, tw.size());
+            cudaFree(segmax);
+            cudaFree(fail);
+            return SLE_ERR_STATE;
+          }
+          tw[at] = t < n ? tw[t] : make_double2(-tw[t - n].x, -tw[t - n].y);
+        }
+      }
+    }
+    ns *= r;
   }
   SLE_CUDA(cudaMemcpy(p->tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
 
