@@ -31,7 +31,10 @@ grounded-ice test and rotational feedback on), options ``opt={"dsl", "diag"}``,
 * ``roofline`` the dominant kernel by device time (a profiling pass with CUDA events around every
   transform launch, host-driven inner loop): algorithmic FLOPs of the 3xTF32 Legendre
   contraction (3 MMAs per product, 12 nh ncoef per field) over the measured time, against the
-  dense TF32 rate (half the measured BF16 GEMM rate); ``traffic`` from the committed ncu summary.
+  dense TF32 rate (half the measured BF16 GEMM rate); ``traffic`` from the committed ncu summary;
+  ``step_shares`` the same profile split by bound: all executed transforms (contraction + row FFT
+  work over the transform kernels' time, against the TF32 rate), the modal advance (bytes over its
+  time, against the copy bandwidth), and their time-weighted combination.
 * ``cpu_baseline`` the CPU oracle (NumPy restatement of the reference solver, FP64) on this
   host's cores, 5 timed steps of the c2 run.
 
@@ -217,6 +220,42 @@ def load_peaks():
         return {"hbm_gbs": float(p["hbm_gbs"]), "bf16_tflops": float(p["bf16_tflops"])}, "of measured"
     except (OSError, KeyError, ValueError):
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
+
+
+def step_shares(prof, nprof, peaks, nlat=512, lmax=511, modes=8):
+    """Roofline of the whole step split by bound, from the profiling pass's per-class device time
+    over `nprof` batch steps (`prof[name] = {"ms", "launches", "fields"}`).
+
+    * transforms: algorithmic work of every executed transform, the 3xTF32 contraction counted as
+      three MMAs per product (12 nh ncoef per field) plus the row FFT (2.5 nlon log2(nlon) N),
+      over the time of the fold, Legendre and unfold kernels, against the dense TF32 rate;
+    * modal advance: (2K + 3) 16 ncoef bytes per member over its time, against the copy bandwidth;
+    * combined: the two fractions weighted by their times.
+    The elementwise grid and spectral passes are not in the profiled classes."""
+    nh, nlon = nlat // 2, 2 * nlat
+    ncoef = (lmax + 1) * (lmax + 2) // 2
+    tf32 = peaks["bf16_tflops"] / 2.0
+    tr_names = ("k_fold_mx", "k_leg_tc<analysis of rO>", "k_leg_tc<other analyses>",
+                "k_bsyn_mx + k_leg_tc<synthesis>", "k_unfold_mx")
+    fields = (prof["k_leg_tc<analysis of rO>"]["fields"] + prof["k_leg_tc<other analyses>"]["fields"]
+              + prof["k_bsyn_mx + k_leg_tc<synthesis>"]["fields"])
+    per_transform = 12.0 * nh * ncoef + 2.5 * nlon * np.log2(nlon) * nlat
+    t_tr = sum(prof[n]["ms"] for n in tr_names) / 1000.0
+    tr_ach = fields * per_transform / t_tr / 1e12 if t_tr > 0 else 0.0
+    adv = prof["k_advance"]
+    t_m = adv["ms"] / 1000.0
+    m_ach = (2 * modes + 3) * 16.0 * ncoef * adv["fields"] / t_m / 1e9 if t_m > 0 else 0.0
+    tr_frac, m_frac = tr_ach / tf32, m_ach / peaks["hbm_gbs"]
+    tot = t_tr + t_m
+    return {
+        "transforms": {"transforms_per_step": fields / nprof, "flops_per_transform": per_transform,
+                       "ms_per_step": 1000.0 * t_tr / nprof, "achieved": tr_ach, "unit": "TFLOP/s",
+                       "peak": tf32, "frac": tr_frac},
+        "modal_advance": {"bytes_per_step": (2 * modes + 3) * 16.0 * ncoef * adv["fields"] / nprof,
+                          "ms_per_step": 1000.0 * t_m / nprof, "achieved": m_ach, "unit": "GB/s",
+                          "peak": peaks["hbm_gbs"], "frac": m_frac},
+        "combined_frac": (tr_frac * t_tr + m_frac * t_m) / tot if tot > 0 else 0.0,
+    }
 
 
 def traffic_per_launch(kernel):
@@ -504,6 +543,7 @@ def run_ours(a):
     roof["traffic"] = traffic_per_launch(dominant)
     roof["kernels"] = {k: {"ms_per_batch_step": v["ms"] / nprof, "launches_per_batch_step": v["launches"] / nprof,
                            "fields_per_batch_step": v["fields"] / nprof} for k, v in prof.items()}
+    roof["step_shares"] = step_shares(prof, nprof, peaks)
 
     latency = None
     if a.serve_requests > 0:

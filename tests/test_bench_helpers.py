@@ -1,0 +1,50 @@
+"""Host-side arithmetic of bench.py's roofline split (no GPU): the transform share, the modal
+advance share and their time-weighted combination from a per-class device-time profile."""
+
+import importlib.util
+import math
+import os
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(HERE, "..", "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _prof(nprof=3):
+    per_step = {"k_fold_mx": (1.39, 32.3, 1034.7), "k_leg_tc<analysis of rO>": (0.69, 7.3, 234.7),
+                "k_leg_tc<other analyses>": (1.65, 25.0, 800.0),
+                "k_bsyn_mx + k_leg_tc<synthesis>": (0.97, 8.3, 266.7), "k_unfold_mx": (0.51, 8.3, 266.7),
+                "k_advance": (0.32, 1.0, 32.0)}
+    return {k: {"ms": v[0] * nprof, "launches": v[1] * nprof, "fields": v[2] * nprof} for k, v in per_step.items()}
+
+
+def test_step_shares_arithmetic():
+    b = _bench()
+    peaks = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+    sh = b.step_shares(_prof(), 3, peaks)
+    nh, ncoef = 256, 512 * 513 // 2
+    per = 12.0 * nh * ncoef + 2.5 * 1024 * 10 * 512
+    fields = 234.7 + 800.0 + 266.7
+    t = (1.39 + 0.69 + 1.65 + 0.97 + 0.51) / 1000.0
+    assert sh["transforms"]["achieved"] == pytest.approx(fields * per / t / 1e12, rel=1e-12)
+    assert sh["transforms"]["frac"] == pytest.approx(sh["transforms"]["achieved"] / 795.0, rel=1e-12)
+    adv = 19 * 16.0 * ncoef * 32.0 / 0.32e-3 / 1e9
+    assert sh["modal_advance"]["achieved"] == pytest.approx(adv, rel=1e-12)
+    lo = min(sh["transforms"]["frac"], sh["modal_advance"]["frac"])
+    hi = max(sh["transforms"]["frac"], sh["modal_advance"]["frac"])
+    assert lo <= sh["combined_frac"] <= hi
+    assert sh["transforms"]["ms_per_step"] == pytest.approx(5.21, rel=1e-12)
+
+
+def test_step_shares_empty_profile():
+    b = _bench()
+    prof = {k: {"ms": 0.0, "launches": 0, "fields": 0.0} for k in _prof()}
+    sh = b.step_shares(prof, 1, {"hbm_gbs": 1.0, "bf16_tflops": 2.0})
+    assert sh["combined_frac"] == 0.0 and not math.isnan(sh["transforms"]["frac"])
