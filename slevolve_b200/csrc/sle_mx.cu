@@ -67,6 +67,8 @@ constexpr int FOLD_NR = 8;                    // rows of a fold block: 4 latitud
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
 
 static_assert(MX_SMEM <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
+static_assert(TILE_B == MX_NMAX * 128, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
+static_assert(4 * MX_NMAX <= (int)SET_COLS && 2 * MX_NMAX <= 256, "full-width accumulators exceed a TMEM set");
 
 // ------------------------------------------------------------------ PTX wrappers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -313,23 +315,39 @@ __device__ __forceinline__ Misc misc_layout(const Smem& S) {
 // the epilogue of one unit overlaps the MMAs of the next.  In a set: [0, 2N) correction
 // accumulator (Ahi*Blo + Alo*Bhi of every chunk), then nbuf main accumulators of 2N columns
 // (Ahi*Bhi), chunk i into buffer i % nbuf; each accumulator holds [even parity N columns][odd
-// parity N columns].
+// parity N columns].  Full width (N = MX_NMAX, so nbuf = 1): per parity p the main accumulator at
+// 2Np and the correction right after it at 2Np + N, so that Ahi*Bhi and Ahi*Blo are one MMA of
+// 2N columns over the adjacent B hi and B lo tiles (A hi read from shared memory once per K step
+// instead of twice; each output column is the same dot product in the same order).
 __device__ __forceinline__ int main_buffers(int nch, int ncols) {
   return max(1, min(nch, ((int)SET_COLS - 2 * ncols) / (2 * ncols)));
 }
+__device__ __forceinline__ bool full_width(int ncols) { return ncols == MX_NMAX; }
 
 // MMAs of one parity `par` of chunk k of a unit (stage st) into the set at `set_base`.  The K
 // sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the descriptor's start-address
 // field.
 __device__ __forceinline__ void mma_half(const Smem& S, uint32_t set_base, int st, int par, int k, int nbuf,
                                          int ncols) {
+  const uint64_t ah = sdesc_sw128(S.a_tile(st, 0)), al = sdesc_sw128(S.a_tile(st, 1));
+  const uint64_t bh = sdesc_sw128(S.b_tile(st, 0)), bl = sdesc_sw128(S.b_tile(st, 1));
   const uint32_t idesc = idesc_tf32(128, ncols);
+  if (full_width(ncols)) {
+    // B hi rows [0, N) and B lo rows [0, N) are 2N consecutive rows (TILE_B = N rows)
+    const uint32_t idesc2 = idesc_tf32(128, 2 * ncols);
+    const uint32_t dm = set_base + (uint32_t)(2 * ncols * par), dc = dm + (uint32_t)ncols;
+#pragma unroll
+    for (int kk = 0; kk < KC / 8; ++kk) {
+      const uint64_t d = (uint64_t)(2 * kk);
+      tc_mma_tf32(dm, ah + d, bh + d, idesc2, (k == 0 && kk == 0) ? 0u : 1u);   // [main | corr]
+      tc_mma_tf32(dc, al + d, bh + d, idesc, 1u);
+    }
+    return;
+  }
   const uint32_t off = (uint32_t)(par * ncols);
   const uint32_t dmain = set_base + (uint32_t)(2 * ncols * (1 + k % nbuf)) + off;
   const uint32_t dcorr = set_base + off;
   const bool fresh = k < nbuf;
-  const uint64_t ah = sdesc_sw128(S.a_tile(st, 0)), al = sdesc_sw128(S.a_tile(st, 1));
-  const uint64_t bh = sdesc_sw128(S.b_tile(st, 0)), bl = sdesc_sw128(S.b_tile(st, 1));
 #pragma unroll
   for (int kk = 0; kk < KC / 8; ++kk) {
     const uint64_t d = (uint64_t)(2 * kk);
@@ -344,8 +362,10 @@ __device__ __forceinline__ void mma_half(const Smem& S, uint32_t set_base, int s
 __device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int ncols, int cb, double (&ev)[16],
                                          double (&od)[16]) {
   uint32_t re[16], ro[16];
-  tc_ld16(lanebase + (uint32_t)(16 * cb), re);
-  tc_ld16(lanebase + (uint32_t)(ncols + 16 * cb), ro);
+  const bool fw = full_width(ncols);
+  // correction accumulator of the even / odd parity
+  tc_ld16(lanebase + (uint32_t)((fw ? ncols : 0) + 16 * cb), re);
+  tc_ld16(lanebase + (uint32_t)((fw ? 3 * ncols : ncols) + 16 * cb), ro);
   tc_wait_ld();
 #pragma unroll
   for (int u = 0; u < 16; ++u) {
@@ -354,9 +374,9 @@ __device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int ncols, 
   }
   const int nb = main_buffers(nch, ncols);
   for (int b = 0; b < nb; ++b) {
-    const uint32_t base = lanebase + (uint32_t)(2 * ncols * (1 + b));
+    const uint32_t base = fw ? lanebase : lanebase + (uint32_t)(2 * ncols * (1 + b));
     tc_ld16(base + (uint32_t)(16 * cb), re);
-    tc_ld16(base + (uint32_t)(ncols + 16 * cb), ro);
+    tc_ld16(base + (uint32_t)((fw ? 2 * ncols : ncols) + 16 * cb), ro);
     tc_wait_ld();
 #pragma unroll
     for (int u = 0; u < 16; ++u) {

@@ -186,3 +186,31 @@ def test_mixed_batch_within_1mm_of_fp64():
                 d = np.abs(bt.get(s, f) - alone[s][k - 1][f]).max()
                 worst = max(worst, d)
     assert worst < 1e-3, worst
+
+
+def test_full_width_batch_within_1mm_of_fp64():
+    """32 mixed slots: every analysis of the inner loop carries 32 fields (64 B-operand columns),
+    the width at which the hi*hi and hi*lo products run as one MMA of 128 columns.  Each slot
+    stays within the mixed form's 1 mm bar of its FP64 solve."""
+    from slevolve_b200 import SyntheticEarth, make_sht
+    from slevolve_b200.synthetic import case_c0
+
+    sht = make_sht("cuda", N, 2 * N, L)
+    base = case_c0(sht, nsteps=40)
+    nslot, nsteps = 32, 6
+    ms = []
+    for s in range(nslot):
+        love = SyntheticEarth(L, 8, 20261203 + 40 + s, relax_scale=0.5 + 0.05 * s)
+        ms.append({"love": love, "topo": base.topo, "dt": 1.0 + 0.02 * s,
+                   "ice": (lambda k, a=0.6 + 0.03 * s: np.round(a * base.ice(k), 3))})
+    bt = _batch("mixed", nslot)
+    for s, m in enumerate(ms):
+        bt.load(s, m["love"], m["topo"], m["ice"](0), m["dt"])
+    alone = [_alone_fp64(m, nsteps) for m in ms]
+    worst = 0.0
+    for k in range(1, nsteps + 1):
+        infos = bt.step({s: m["ice"](k) for s, m in enumerate(ms)})
+        for s in range(nslot):
+            for f in ("deltasl", "tgrid", "R"):
+                worst = max(worst, float(np.abs(bt.get(s, f) - alone[s][k - 1][f]).max()))
+    assert worst < 1e-3, worst
