@@ -1046,6 +1046,26 @@ int sht_mx_prepare(sle_sht* p) {
   }
   std::stable_sort(au.begin(), au.end(), [](const AU& x, const AU& y) { return x.w > y.w; });
   std::stable_sort(su.begin(), su.end(), [](const SU& x, const SU& y) { return x.w > y.w; });
+  {
+    int dev = 0, nsm = 0;
+    SLE_CUDA(cudaGetDevice(&dev));
+    SLE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    p->n_sm = std::max(1, nsm);
+  }
+  // CTA b of a launch of G = min(n, SMs) CTAs takes the units at positions b, b + G, ...; lay the
+  // units sorted by work out in snake order (round r of G positions in rank order when r is even,
+  // reversed when odd) so that every CTA's total is close to the mean
+  auto snake = [&](auto& v) {
+    const int n = (int)v.size(), G = std::min(n, p->n_sm);
+    auto out = v;
+    for (int pos = 0; pos < n; ++pos) {
+      const int r = pos / G, b = pos % G, cnt = std::min(G, n - r * G);
+      out[pos] = v[r * G + ((r & 1) ? cnt - 1 - b : b)];
+    }
+    v.swap(out);
+  };
+  snake(au);
+  snake(su);
   std::vector<int4> av, sv;
   std::vector<int> segs;
   long long na = 0, ns = 0;
@@ -1109,12 +1129,6 @@ int sht_mx_prepare(sle_sht* p) {
       set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
       return SLE_ERR_CUDA;
     }
-  }
-  {
-    int dev = 0, nsm = 0;
-    SLE_CUDA(cudaGetDevice(&dev));
-    SLE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    p->n_sm = std::max(1, nsm);
   }
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, MX_SMEM));
