@@ -175,19 +175,24 @@ class SolverBatch:
     def step_host_stream(self, host_steps, dts=None):
         """Step once per element of ``host_steps`` (a sequence of {slot: host grid}, NumPy arrays or
         CPU tensors, ideally in pinned memory), uploading step k + 1's ice on a copy stream while
-        step k runs (two device staging grids per slot).  Returns the list of {slot: SleStepInfo}.
-        The results are those of calling ``step`` once per element."""
+        step k runs (two device staging grids per slot, kept for later calls with the same slots).
+        Returns the list of {slot: SleStepInfo}.  The results are those of calling ``step`` once
+        per element."""
         import torch
 
         n = len(host_steps)
         if n == 0:
             return []
         slots = sorted(host_steps[0])
-        stage = [{s: torch.empty((self.nlat, self.nlon), dtype=torch.float64, device="cuda") for s in slots}
-                 for _ in range(2)]
-        copy = torch.cuda.Stream()
+        # staging grids, copy stream and events are kept for the next call (same slots)
+        hs = getattr(self, "_host_stream", None)
+        if hs is None or hs[0] != slots:
+            stage = [{s: torch.empty((self.nlat, self.nlon), dtype=torch.float64, device="cuda") for s in slots}
+                     for _ in range(2)]
+            hs = (slots, stage, torch.cuda.Stream(), [torch.cuda.Event(), torch.cuda.Event()])
+            self._host_stream = hs
+        _, stage, copy, landed = hs
         batch_stream = torch.cuda.ExternalStream(self.stream_handle())
-        landed = [torch.cuda.Event(), torch.cuda.Event()]
         copy.wait_stream(torch.cuda.current_stream())
         copy.wait_stream(batch_stream)
 
