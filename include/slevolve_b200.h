@@ -218,6 +218,15 @@ int sle_batch_stream(sle_batch* b, void** stream);
 /* slots, mode capacity and the device bytes the batch's solver state occupies */
 int sle_batch_info(const sle_batch* b, int* nslots, int* max_modes, long long* device_bytes);
 
+/* ----------------------------------------------------------- ice history */
+/* out[i] = (1 - w) a[i] + w b[i] for i < n, on the device, with NumPy's elementwise roundings
+ * (1 - w once, two products, one sum, no fused multiply-add): the blended entry "i:j:w" of the
+ * outer driver's custom ice history (run_outer.py:156-174, option --ice-seq), formed from two
+ * snapshots already on the device; out must not overlap a or b.  stream: a cudaStream_t (NULL =
+ * the legacy default stream).
+ * SLE_ERR_BAD_ARG for a negative n or a NULL buffer with n > 0. */
+int sle_ice_blend(double* out, const double* a, const double* b, double w, long long n, void* stream);
+
 /* ------------------------------------------------------- measurement */
 /* Kernel classes timed by sle_prof_*: 0 row FFT + fold, 1 Legendre analysis, 2 Legendre
  * synthesis, 3 inverse FFT + unfold, 4 modal-state advance, 5 the Legendre analysis of the inner

@@ -19,7 +19,7 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libslevolve_b200.so")
-SOURCES = ["sle_sht.cu", "sle_mx.cu", "sle_solver.cu", "sle_prof.cu"]
+SOURCES = ["sle_sht.cu", "sle_mx.cu", "sle_solver.cu", "sle_prof.cu", "sle_ice.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
