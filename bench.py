@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--cpu-steps", type=int, default=5, help="timed oracle steps for cpu_baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--init-topo", action="store_true",
+                    help="instead: time the segmented initial-topography guess (GPU) against the CPU oracle")
     return ap.parse_args()
 
 
@@ -590,10 +592,51 @@ def run_ours(a):
     return 0
 
 
+def run_init_topo(a):
+    """The outer driver's segmented T0 guess on the seeded glacial-cycle case at 512 x 1024,
+    L = 511 (13 ice states, 10-kyr steps): GPU wall time of one guess (after a short warm-up
+    guess), and the CPU oracle (NumPy restatement) on the same inputs beside it."""
+    import torch
+
+    from slevolve_b200 import make_sht
+    from slevolve_b200.init_topo import segmented_guess
+    from slevolve_b200.synthetic import case_glacial
+
+    L = 511
+    topo, ice, love = case_glacial(make_sht("cuda", 512, 1024, L))
+    segmented_guess(topo, ice[:4], love, L, 10.0, maxit=2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    T0, info = segmented_guess(topo, ice, love, L, 10.0)
+    torch.cuda.synchronize()
+    gpu_s = time.perf_counter() - t0
+    line = {"metric": "segmented initial-topography guess, wall time", "value": gpu_s, "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "data": "synthetic", "dtype": "f64",
+            "config": {"workload": "segmented T0 guess of the outer driver: 512x1024, L=511, 13 ice states "
+                                   "(two glacial cycles, three caps), 10-kyr steps, threshold 0.01, tol 1e-3 m"},
+            "iters": info["iters"], "legs": [[s_["a"], s_["b"]] for s_ in info["segments"]], "c_m": info["c"],
+            "cpu_baseline": None}
+    if not a.no_cpu_baseline:
+        from oracle.init_topo import segmented_guess as oracle_guess
+
+        t0 = time.perf_counter()
+        T0c, infoc = oracle_guess(topo, ice, love, L, 10.0)
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": cpu_s, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": "the whole guess on the same inputs (NumPy oracle, threaded FFT/BLAS)"}
+        line["speedup_vs_cpu"] = cpu_s / gpu_s
+        line["max_diff_vs_cpu_m"] = float(np.abs(T0 - T0c).max())
+        line["iters_cpu"] = infoc["iters"]
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         return run_reference(a)
+    if a.init_topo:
+        return run_init_topo(a)
     return run_ours(a)
 
 

@@ -227,6 +227,18 @@ int sle_batch_info(const sle_batch* b, int* nslots, int* max_modes, long long* d
  * SLE_ERR_BAD_ARG for a negative n or a NULL buffer with n > 0. */
 int sle_ice_blend(double* out, const double* a, const double* b, double w, long long n, void* stream);
 
+/* The water-volume residual of the segmented initial-topography guess
+ * (init_topo_segmented.py:84-90) for T0 = (tp + c) + s on an nlat x nlon grid: out2[0] = sum of
+ * max(-T0, 0) C0 area, out2[1] = sum of (I0 g0 - Ip gp) area, with g0 = grounded(i0, T0)
+ * (i0 > 0 and (T0 > 0 or rhoi i0 > rhow |T0|)), C0 = T0 < 0 and not g0, area = wrow[row]; gp the
+ * present grounded mask (bytes).  Deterministic sums (fixed partition, fixed order).  scratch:
+ * sle_topo_scratch_bytes() device bytes, zero before the first call and left so by each call.
+ * Synchronises the stream (the host reads out2). */
+int sle_topo_residual(const double* tp, const double* s, double c, const double* i0, const double* ip,
+                      const unsigned char* gp, const double* wrow, int nlat, int nlon, double rhoi, double rhow,
+                      void* scratch, double* out2, void* stream);
+long long sle_topo_scratch_bytes(void);
+
 /* ------------------------------------------------------- measurement */
 /* Kernel classes timed by sle_prof_*: 0 row FFT + fold, 1 Legendre analysis, 2 Legendre
  * synthesis, 3 inverse FFT + unfold, 4 modal-state advance, 5 the Legendre analysis of the inner

@@ -97,6 +97,10 @@ _SIGS = {
     "sle_batch_step_begin": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "sle_batch_step_end": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sle_ice_blend": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_longlong, C.c_void_p]),
+    "sle_topo_residual": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
+    "sle_topo_scratch_bytes": (C.c_longlong, []),
     "sle_batch_get": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]),
     "sle_batch_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "sle_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),

@@ -159,3 +159,19 @@ def case_c2(sht, nsteps=1200, seed=BASE_SEED + 2, dt=200.0, amp=1.0, relax_scale
 
 
 CASES = {"c0": (64, case_c0), "c1": (256, case_c1), "c2": (512, case_c2)}
+
+
+def case_glacial(sht, nstates=13, seed=BASE_SEED + 5):
+    """Ice states 0..nstates-1 of two glacial cycles (growth, retreat, regrowth, present) on the
+    c0-style topography of this grid: three caps (south pole, 62 N 100 W, 56 N 132 E) scaled by
+    0.35 + 0.65 |sin(2.2 pi t)| (1 - 0.4 t), t in [0, 1]; the input of the segmented T0 guess.
+    Returns (topography, list of ice grids, Earth model)."""
+    nlon, L = sht.nlon, sht.lmax
+    topo = random_topography(sht, seed)
+    LAT, LON = grid_latlon(sht.gaulats, nlon)
+    shape = (1.2 * vialov(angular_distance(LAT, LON, -90.0, 0.0), 15.0)
+             + vialov(angular_distance(LAT, LON, 62.0, -100.0), 20.0)
+             + vialov(angular_distance(LAT, LON, 56.0, 132.0), 15.0)) * (topo > -500.0)
+    t = np.linspace(0.0, 1.0, nstates)
+    amp = 0.35 + 0.65 * np.abs(np.sin(2.2 * np.pi * t)) * (1.0 - 0.4 * t)
+    return topo, [round_mm(3000.0 * a * shape) for a in amp], SyntheticEarth(L, 8, seed)
