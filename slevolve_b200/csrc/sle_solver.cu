@@ -735,6 +735,54 @@ __global__ void k_refresh2(Dev D) {
   }
 }
 
+// The same pass over eight cells per thread (8-byte mask loads and stores, four double2 ice
+// loads), for grids whose cell count is a multiple of 8; per cell the arithmetic of k_refresh2.
+__device__ __forceinline__ unsigned char byte_of(uint2 v, int i) {
+  return (unsigned char)(((i < 4 ? v.x : v.y) >> (8 * (i & 3))) & 0xffu);
+}
+__global__ void k_refresh2_x8(Dev D) {
+  SLOT_OR_RETURN();
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (8 * q >= D.ng || sc->converged) return;
+  const bool changed = sc->gr_changed != 0;
+  const uint2 cx = reinterpret_cast<const uint2*>(D.m(M_CXY, b))[q];
+  const uint2 prev = reinterpret_cast<const uint2*>(D.m(M_CSTAR, b))[q];
+  uint2 k = make_uint2(0u, 0u), bt = make_uint2(0u, 0u);
+  double2 ic[4];
+  if (changed) {
+    k = reinterpret_cast<const uint2*>(D.m(M_GRNEW, b))[q];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) ic[u] = ld2(D.g(G_ICE, b), 4 * q + u);
+  } else {
+    bt = reinterpret_cast<const uint2*>(D.m(M_BETA, b))[q];
+  }
+  if (changed) {
+    unsigned int lo = 0u, hi = 0u;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const double v = (i & 1) ? ic[i >> 1].y : ic[i >> 1].x;
+      const double gi = byte_of(k, i) ? v : __dmul_rn(v, 0.0);
+      const unsigned int bit = (gi < EPS0) ? 1u : 0u;
+      if (i < 4) lo |= bit << (8 * i);
+      else hi |= bit << (8 * (i - 4));
+    }
+    bt = make_uint2(lo, hi);
+    reinterpret_cast<uint2*>(D.m(M_GR, b))[q] = k;
+    reinterpret_cast<uint2*>(D.m(M_BETA, b))[q] = bt;
+  }
+  unsigned int clo = 0u, chi = 0u;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const unsigned int ci = (byte_of(cx, i) && byte_of(bt, i)) ? 1u : 0u;
+    if (i < 4) clo |= ci << (8 * i);
+    else chi |= ci << (8 * (i - 4));
+  }
+  if (clo != prev.x || chi != prev.y) {
+    sc->cs_changed = 1;
+    reinterpret_cast<uint2*>(D.m(M_CSTAR, b))[q] = make_uint2(clo, chi);
+  }
+}
+
 // dice, dI after a grounded-mask change
 __global__ void k_dice(Dev D) {
   SLOT_OR_RETURN();
@@ -1153,7 +1201,8 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   }
   note_launch(2);
   k_refresh1<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
-  k_refresh2<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
+  if (ng % 8 == 0) k_refresh2_x8<<<dim3(nb(ng / 8), B), 256, 0, st>>>(D);
+  else k_refresh2<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
   // I* (only when the grounded mask changed), C* and tO for the next iteration; skipped for
   // slots that converged
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_refresh.data(), (int)s->f_ana_refresh.size(), st));
