@@ -200,16 +200,17 @@ def run_reference(a):
     case = build_case(lambda: OracleSHT(512, 1024, 511, workers=workers))
     r = cpu_oracle_run(case, a.warmup, a.steps, workers)
     sample = f"{a.steps} timed steps after {a.warmup} warm-up steps of the same c2 run"
-    line = {"impl": "reference", "metric": METRIC, "value": r["steps_per_s"], "unit": "steps/s",
+    # one member per step: steps/s of the single solve = member-steps/s, the unit of our arm
+    line = {"impl": "reference", "metric": METRIC, "value": r["steps_per_s"], "unit": "member-steps/s",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": 1000.0 / r["steps_per_s"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": [512, 1024], "lmax": 511, "modes": 8,
                        "precision": "fp64", "numiter_per_step": r["numiter_per_step"],
                        "solver": "CPU oracle (NumPy restatement of the reference SeaLevelSolver)"},
-            "cpu_baseline": {"value": r["steps_per_s"], "unit": "steps/s", "cores": workers,
+            "cpu_baseline": {"value": r["steps_per_s"], "unit": "member-steps/s", "cores": workers,
                              "kind": "port", "sample": sample},
-            "e2e": {"value": r["steps_per_s"], "unit": "steps/s", "h2d_bytes_per_step": 0,
+            "e2e": {"value": r["steps_per_s"], "unit": "member-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -563,7 +564,7 @@ def run_ours(a):
     if not a.no_cpu_baseline:
         workers = os.cpu_count() or 1
         r = cpu_oracle_run(case, 2, a.cpu_steps, workers)
-        cpu = {"value": r["steps_per_s"], "unit": "steps/s", "cores": workers, "kind": "port",
+        cpu = {"value": r["steps_per_s"], "unit": "member-steps/s", "cores": workers, "kind": "port",
                "sample": f"{a.cpu_steps} timed FP64 steps (after 2 warm-up steps) of the c2 run, "
                          f"oracle numiter/step {r['numiter_per_step']:.2f}"}
 
