@@ -197,3 +197,30 @@ def test_outer_passes_with_warm_reuse_against_oracle():
         T_gpu = T_gpu - (np.array(r["tgrid"]) - obs)
         T_orc = T_orc - (o["tgrid"] - obs)
     assert warm == 24   # passes 2 and 3 start every step from the stored state
+
+
+@pytest.mark.parametrize("kind", ["plain", "extrap"])
+def test_variable_step_lengths(kind):
+    """24 steps of varying length through step(ice, dt=...): decay factors per distinct length
+    and the non-uniform extrapolated start, against the reference (make_golden_vardt.py)."""
+    from slevolve_b200 import OptSeaLevelSolver, SeaLevelSolver
+    from slevolve_b200.synthetic import case_c0
+    from oracle.sht import OracleSHT
+
+    fx = load_golden("step_vardt.npz")
+    case = case_c0(OracleSHT(64, 128, 63), nsteps=len(fx["dts"]) + 8)
+    if kind == "plain":
+        slv = SeaLevelSolver(None, case.love, case.topo, case.ice(0), norder=63, dt=1.0)
+    else:
+        slv = OptSeaLevelSolver(None, case.love, case.topo, case.ice(0), norder=63, dt=1.0,
+                                opt={"dsl"}, inner="extrap")
+    numiter = []
+    for k, dt in enumerate(fx["dts"], start=1):
+        r = slv.step(case.ice(k), dt=float(dt))
+        numiter.append(r["numiter"])
+        if f"{kind}_tgrid_{k}" in fx:
+            assert np.abs(r["tgrid"] - fx[f"{kind}_tgrid_{k}"]).max() <= TOL_M, k
+            assert np.abs(r["R"] - fx[f"{kind}_R_{k}"]).max() <= TOL_M, k
+            assert np.array_equal(r["ocean"] != 0, _unpack(fx[f"{kind}_ocean_{k}"], r["ocean"].shape)), k
+            assert np.array_equal(r["beta"] != 0, _unpack(fx[f"{kind}_beta_{k}"], r["beta"].shape)), k
+    assert numiter == list(fx[f"{kind}_numiter"])

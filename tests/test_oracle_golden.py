@@ -136,3 +136,23 @@ def test_synthetic512_oracle_record():
     rec = meta["synthetic512_oracle"]
     assert rec["max_abs_vs_tgrid8_m"] <= TOL_M
     assert rec["numiter"] == [5, 5, 6, 6, 5, 5, 5, 5]
+
+
+@pytest.mark.parametrize("kind", ["plain", "extrap"])
+def test_variable_step_lengths_against_reference(kind):
+    """24 steps of varying length (step(ice, dt=...)): per-length decay factors and, with
+    inner="extrap", the non-uniform extrapolated start (golden: make_golden_vardt.py)."""
+    from slevolve_b200.synthetic import case_c0
+    fx = load_golden("step_vardt.npz")
+    sht = OracleSHT(64, 128, 63)
+    case = case_c0(sht, nsteps=len(fx["dts"]) + 8)
+    kw = {} if kind == "plain" else {"opt": {"dsl"}, "inner": "extrap"}
+    slv = OracleSolver(sht, case.love, case.topo, case.ice(0), norder=63, dt=1.0, **kw)
+    numiter = []
+    for k, dt in enumerate(fx["dts"], start=1):
+        r = slv.step(case.ice(k), dt=float(dt))
+        numiter.append(r["numiter"])
+        if f"{kind}_tgrid_{k}" in fx:
+            assert np.abs(r["tgrid"] - fx[f"{kind}_tgrid_{k}"]).max() <= TOL_M, k
+            assert np.abs(r["R"] - fx[f"{kind}_R_{k}"]).max() <= TOL_M, k
+    assert numiter == list(fx[f"{kind}_numiter"])
