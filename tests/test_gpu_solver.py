@@ -36,6 +36,13 @@ def _check_against_fixture(slv, fx, prefix, ice_fn, nsteps):
             for key in ("gmslc_ocn", "gmslc_ocnBeta", "ocean_area", "oceanBeta_area", "ice_volume"):
                 ref = fx[f"{prefix}{key}"][k - 1]
                 assert abs(r[key] - ref) <= 1e-9 * max(1.0, abs(ref)), (k, key, r[key], ref)
+        # rotational feedback (TPW direction, inertia perturbation, centrifugal potential):
+        # the reference's signs and magnitudes, 1e-9 of the largest entry of the run
+        for key in ("mm", "il", "lambda"):
+            if f"{prefix}{key}" in fx:
+                ref = fx[f"{prefix}{key}"]
+                scale = float(np.abs(ref).max())
+                assert np.abs(np.asarray(r[key]) - ref[k - 1]).max() <= 1e-9 * scale, (k, key)
     assert numiter == list(fx[f"{prefix}numiter"]), numiter
 
 

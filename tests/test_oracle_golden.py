@@ -74,6 +74,10 @@ def _check_run(slv, fx, prefix, ice_fn, nsteps, saved):
         for key in ("gmslc_ocn", "gmslc_ocnBeta", "ocean_area", "oceanBeta_area", "ice_volume"):
             ref = fx[f"{prefix}{key}"][k - 1]
             assert abs(r[key] - ref) <= 1e-9 * max(1.0, abs(ref)), (k, key)
+        for key in ("mm", "il", "lambda"):   # rotational feedback: signs and magnitudes
+            if f"{prefix}{key}" in fx:
+                ref = fx[f"{prefix}{key}"]
+                assert np.abs(np.asarray(r[key]) - ref[k - 1]).max() <= 1e-9 * float(np.abs(ref).max()), (k, key)
     assert numiter == list(fx[f"{prefix}numiter"])
 
 
