@@ -167,6 +167,18 @@ int sle_solver_step(sle_solver* s, const double* ice, int on_device, double dt_y
                     sle_step_info* info);
 /* copy one output of the last step; dst is host or device memory. */
 int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device);
+/* Analytic rates read-out (solver.py:464-484, 722-806; FP64 solves).  set_rate_tables(tab): the
+ * weights of the following steps, host doubles [w_sl (K x (lmax+1)), w_rr (K x (lmax+1)),
+ * ws_sl, ws_rr, wsphi_sl, wsphi_rr (lmax+1 each)] with K the solver's mode capacity (the
+ * reference's ExactMemory.w_sl, w_rr and their sums for the step length, solver.py:293-294,
+ * 347-362); NULL turns the read-out off.  While on, every step also forms, before its commit, the
+ * rate spectra of sea level and radial displacement without the degree-2 rotational terms.
+ * get_rates after a step: dsl, drr dense complex128 [lmax+1][lmax+1] (host); rec (20 doubles:
+ * dI*_00 of the step (re, im), then the rotational totals committed before it: il (9), m (3),
+ * Lambda degree 2 (3 complex)); rot (18 K doubles: the degree-2 modal states after the step's
+ * advance, r_il [K][9], r_m [K][3], r_Lambda [K][3 complex]).  SLE_ERR_STATE without tables. */
+int sle_solver_set_rate_tables(sle_solver* s, const double* tab);
+int sle_solver_get_rates(sle_solver* s, void* dsl, void* drr, double* rec, double* rot);
 /* Cross-pass warm start, reuse="warm" (solver_opt.py:400-403, 514-528, 932-947): a store in
  * device memory kept by the caller across solves of the same ice history (outer iterations,
  * run_outer.py).  ds_store: [capacity][ncoef] complex128 (packed), 16-byte aligned; mask_store:

@@ -72,6 +72,8 @@ struct SlotStep {
   const unsigned char* warm_mask;  // converged ocean function of this step, previous pass
   double2* rec_ds;                 // where this pass's converged increment goes
   unsigned char* rec_mask;         // where this pass's converged ocean function goes
+  int rates;                       // read the analytic rate spectra before the commit
+  double rate_h;                   // the step's length (years)
 };
 
 enum GridId {
@@ -866,6 +868,63 @@ __global__ void k_rr(Dev D) {
 // commit (solver.py:1080-1096): cur = rhoi dice + rhow load (l = 0 zeroed); p_load += cur;
 // p_ice = dI ; p_ocean = dS_cur ; prev_ice = I*_lm ; extrap history (the older buffer) = load;
 // thread 0 also commits the rotational increments and records I*_00.
+// Analytic rate spectra (per year) at the end of the step, read before the commit
+// (solver.py:464-474, 766-785): with cur = the step's load increment (formed as k_commit forms
+// it), P = the load committed before the step and q = sum_k w_k R_k over the degree's modes,
+//   rs = (ws P - q) + wsphi cur,  dsl = (ttlekhl cur) / h + ttl rs   (sea level, w = w_sl)
+//   rr likewise with w_rr,        drr = (ttlhe cur) / h + ttl rr     (radial)
+// and zero at degree 0; each operation rounded as NumPy rounds it.  The degree-2 rotational rates
+// are added on the host.
+__global__ void k_rate_spec(Dev D, double2* rspec, const double* rtab, double* rrec) {
+  SLOT_OR_RETURN();
+  const SlotStep& ss = D.ss[b];
+  if (!ss.rates || sc->status) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ncoef) return;
+  double2* dsl = rspec + ((size_t)b * 2 + 0) * D.ncoef;
+  double2* drr = rspec + ((size_t)b * 2 + 1) * D.ncoef;
+  if (i == 0) {
+    const double2 d0 = D.sp(S_DICE, b)[0];
+    rrec[2 * b] = d0.x;
+    rrec[2 * b + 1] = d0.y;
+  }
+  const int l = D.lidx[i];
+  if (l == 0) {
+    dsl[i] = make_double2(0.0, 0.0);
+    drr[i] = make_double2(0.0, 0.0);
+    return;
+  }
+  const int nl = D.nl, K = D.K;
+  const double2 ld = D.sp(S_LOAD, b)[i], d = D.sp(S_DICE, b)[i];
+  const double2 cur = make_double2(__dadd_rn(__dmul_rn(d.x, D.rhoi), __dmul_rn(ld.x, D.rhow)),
+                                   __dadd_rn(__dmul_rn(d.y, D.rhoi), __dmul_rn(ld.y, D.rhow)));
+  const double2 P = D.sp(S_P_LOAD, b)[i];
+  const double* t = rtab + (size_t)b * (2 * K + 4) * nl;
+  const double *w_sl = t, *w_rr = t + (size_t)K * nl, *ws_sl = t + (size_t)2 * K * nl, *ws_rr = ws_sl + nl,
+               *wp_sl = ws_rr + nl, *wp_rr = wp_sl + nl;
+  double2 qs = make_double2(0.0, 0.0), qr = qs;
+  const double2* R = D.R + (size_t)b * K * D.ncoef;
+  const int nk = D.nmod[(size_t)b * nl + l];
+  for (int k = 0; k < nk; ++k) {
+    const double2 r = R[(size_t)k * D.ncoef + i];
+    const double a = w_sl[(size_t)k * nl + l], c = w_rr[(size_t)k * nl + l];
+    qs = make_double2(__dadd_rn(qs.x, __dmul_rn(a, r.x)), __dadd_rn(qs.y, __dmul_rn(a, r.y)));
+    qr = make_double2(__dadd_rn(qr.x, __dmul_rn(c, r.x)), __dadd_rn(qr.y, __dmul_rn(c, r.y)));
+  }
+  const double h = ss.rate_h;
+  const size_t tl = (size_t)b * nl + l;
+  const double ttl = D.ttl[tl], tek = D.ttlekhl[tl], the = D.ttlhe[tl];
+  double2 rs, rr;
+  rs.x = __dadd_rn(__dsub_rn(__dmul_rn(ws_sl[l], P.x), qs.x), __dmul_rn(wp_sl[l], cur.x));
+  rs.y = __dadd_rn(__dsub_rn(__dmul_rn(ws_sl[l], P.y), qs.y), __dmul_rn(wp_sl[l], cur.y));
+  rr.x = __dadd_rn(__dsub_rn(__dmul_rn(ws_rr[l], P.x), qr.x), __dmul_rn(wp_rr[l], cur.x));
+  rr.y = __dadd_rn(__dsub_rn(__dmul_rn(ws_rr[l], P.y), qr.y), __dmul_rn(wp_rr[l], cur.y));
+  dsl[i] = make_double2(__dadd_rn(__ddiv_rn(__dmul_rn(tek, cur.x), h), __dmul_rn(ttl, rs.x)),
+                        __dadd_rn(__ddiv_rn(__dmul_rn(tek, cur.y), h), __dmul_rn(ttl, rs.y)));
+  drr[i] = make_double2(__dadd_rn(__ddiv_rn(__dmul_rn(the, cur.x), h), __dmul_rn(ttl, rr.x)),
+                        __dadd_rn(__ddiv_rn(__dmul_rn(the, cur.y), h), __dmul_rn(ttl, rr.y)));
+}
+
 __global__ void k_commit(Dev D, int extrap) {
   SLOT_OR_RETURN();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1064,6 +1123,13 @@ struct sle_batch {
   double* rows;
   unsigned int* badflag;
   int* bstatus;            // batch-wide status raised by a tensor-core timeout
+  // analytic rates read-out (opt-in per slot): rate spectra [nslot][2][ncoef] (sea level, radial),
+  // weight tables [nslot][2 K nl + 4 nl] (w_sl, w_rr, ws_sl, ws_rr, wsphi_sl, wsphi_rr) and a
+  // record [nslot][2] (dI*_00 of the step)
+  double2* rate_spec;
+  double* rate_tab;
+  double* rate_rec;
+  std::vector<char> rates_on;
   // pinned mirrors
   Scal* hsc;
   SlotStep* hss;
@@ -1105,7 +1171,8 @@ void batch_free(sle_batch* s) {
   if (!s) return;
   void* ptrs[] = {s->grid, s->mask, s->spec, s->R, s->nmod, s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr, s->ttl,
                   s->ttlekhl, s->ttlhe, s->a_il, s->a_m, s->a_tsl, s->a_trr, s->rc, s->r_il, s->r_m,
-                  s->r_lam, s->sc, s->ss, s->partials, s->counter, s->rows, s->badflag, s->bstatus};
+                  s->r_lam, s->sc, s->ss, s->partials, s->counter, s->rows, s->badflag, s->bstatus,
+                  s->rate_spec, s->rate_tab, s->rate_rec};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (s->hsc) cudaFreeHost(s->hsc);
@@ -1631,6 +1698,8 @@ int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, cons
     p.active = 1;
     p.first = h.iter == 1;
     p.hsel = h.hsel;
+    p.rates = (b < (int)s->rates_on.size() && s->rates_on[b]) ? 1 : 0;
+    p.rate_h = dt;
     if (s->cfg.inner_extrap && h.nhist >= 2) {
       const double dt0 = dt, dt1 = h.dt_hist[0], dt2 = h.dt_hist[1];
       if (dt0 == dt1 && dt1 == dt2) {
@@ -1712,6 +1781,15 @@ int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, cons
     std::vector<FieldSpec> f;
     for (int b : act) f.push_back(fspec(D.g(G_RR, b), D.sp(S_RRLM, b), &s->sc[b].status));
     SLE_TRY(sht_synthesis_list(s->plan, f.data(), (int)f.size(), st));
+  }
+  // ---- analytic rates of the slots that asked for them, read before the commit
+  {
+    bool any_rates = false;
+    for (int b : act) any_rates |= s->hss[b].rates != 0;
+    if (any_rates) {
+      note_launch();
+      k_rate_spec<<<dim3(nb(nc), UB), 256, 0, st>>>(D, s->rate_spec, s->rate_tab, s->rate_rec);
+    }
   }
   // ---- commit (solver.py:1080-1096); extrap history (solver_opt.py:817-822)
   note_launch();
@@ -2073,6 +2151,62 @@ extern "C" int sle_solver_set_reuse(sle_solver* s, void* ds_store, void* mask_st
     return SLE_ERR_BAD_ARG;
   }
   return sle_batch_set_reuse(s->b, 0, ds_store, mask_store, capacity, valid);
+}
+
+extern "C" int sle_solver_set_rate_tables(sle_solver* s, const double* tab) {
+  if (!s) {
+    set_error("sle_solver_set_rate_tables: NULL solver");
+    return SLE_ERR_BAD_ARG;
+  }
+  sle_batch* b = s->b;
+  b->rates_on.resize(b->nslot, 0);
+  if (!tab) {
+    b->rates_on[0] = 0;
+    return SLE_OK;
+  }
+  const size_t nl = (size_t)b->D.nl, per = (size_t)(2 * b->K + 4) * nl;
+  if (!b->rate_spec) {
+    SLE_TRY(dalloc(&b->rate_spec, (size_t)b->nslot * 2 * b->D.ncoef));
+    SLE_TRY(dalloc(&b->rate_tab, (size_t)b->nslot * per));
+    SLE_TRY(dalloc(&b->rate_rec, (size_t)b->nslot * 2));
+  }
+  SLE_CUDA(cudaMemcpyAsync(b->rate_tab, tab, per * sizeof(double), cudaMemcpyHostToDevice, b->st));
+  SLE_CUDA(cudaStreamSynchronize(b->st));
+  b->rates_on[0] = 1;
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_get_rates(sle_solver* s, void* dsl, void* drr, double* rec, double* rot) {
+  if (!s || !dsl || !drr || !rec || !rot) {
+    set_error("sle_solver_get_rates: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  sle_batch* b = s->b;
+  if (b->rates_on.empty() || !b->rates_on[0] || !b->rate_spec) {
+    set_error("sle_solver_get_rates: no rate tables set (sle_solver_set_rate_tables before the step)");
+    return SLE_ERR_STATE;
+  }
+  const Dev& D = b->D;
+  const size_t dense = sizeof(double2) * (size_t)D.nl * D.nl;
+  double2* stage = b->plan->packbuf;  // staging (nm*nm <= 4*ncoef)
+  for (int q = 0; q < 2; ++q) {
+    SLE_TRY(sht_unpack(b->plan, b->rate_spec + (size_t)q * D.ncoef, stage, b->st));
+    SLE_CUDA(cudaMemcpyAsync(q ? drr : dsl, stage, dense, cudaMemcpyDeviceToHost, b->st));
+    SLE_CUDA(cudaStreamSynchronize(b->st));
+  }
+  double dice[2];
+  SLE_CUDA(cudaMemcpy(dice, b->rate_rec, sizeof(dice), cudaMemcpyDeviceToHost));
+  const Scal& f = b->hsc[0];
+  rec[0] = dice[0];
+  rec[1] = dice[1];
+  for (int q = 0; q < 9; ++q) rec[2 + q] = f.oldil[q];
+  for (int q = 0; q < 3; ++q) rec[11 + q] = f.oldm[q];
+  for (int q = 0; q < 6; ++q) rec[14 + q] = f.dlam_prev2[q];
+  const int K = b->K;
+  SLE_CUDA(cudaMemcpy(rot, b->r_il, sizeof(double) * 9 * K, cudaMemcpyDeviceToHost));
+  SLE_CUDA(cudaMemcpy(rot + 9 * K, b->r_m, sizeof(double) * 3 * K, cudaMemcpyDeviceToHost));
+  SLE_CUDA(cudaMemcpy(rot + 12 * K, b->r_lam, sizeof(double) * 6 * K, cudaMemcpyDeviceToHost));
+  return SLE_OK;
 }
 
 extern "C" int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device) {

@@ -290,9 +290,59 @@ class SeaLevelSolver:
         self.gr_counts["ice_analyses"] += self._info.gr_ice_analyses
         return self._info
 
-    def step(self, icexy_cur, profile=False, dt=None, rates=False):
+    def _rates_setup(self, rates, dt):
+        """Turn the device rate read-out on (with this step's weights) or off."""
         if rates:
-            raise NotImplementedError("analytic rates are not provided by the GPU solver")
+            if self.precision != "fp64":
+                raise NotImplementedError("analytic rates are provided for precision='fp64' solves")
+            from .rates import RateTables
+
+            if getattr(self, "_rate_tabs", None) is None:
+                self._rate_tabs = RateTables(self.love, self.norder)
+            h = float(dt) if dt else float(self.dt)
+            tab = self._rate_tabs.for_dt(h)
+            if getattr(self, "_rates_dt", None) != h:
+                _lib.check(self._L.sle_solver_set_rate_tables(self._h, tab.ctypes.data), "sle_solver_set_rate_tables")
+                self._rates_dt = h
+            return h
+        if getattr(self, "_rates_dt", None) is not None:
+            _lib.check(self._L.sle_solver_set_rate_tables(self._h, None), "sle_solver_set_rate_tables")
+            self._rates_dt = None
+        return None
+
+    def _rates_read(self, info, h):
+        """The reference's rates dict of the step just taken (solver.py:766-806)."""
+        from .rates import rate_grids, rotation_rate
+        from .sht import make_sht
+
+        tabs = self._rate_tabs
+        K = tabs.K
+        dsl = np.empty((self.nl, self.nl), dtype=np.complex128)
+        drr = np.empty_like(dsl)
+        rec = np.empty(20)
+        rot = np.empty(18 * K)
+        _lib.check(self._L.sle_solver_get_rates(self._h, dsl.ctypes.data, drr.ctypes.data, rec.ctypes.data,
+                                                rot.ctypes.data), "sle_solver_get_rates")
+        out_rot = None
+        if self.tpw and self.norder >= 2:
+            lam = np.array(info.lam[:]).reshape(3, 3, 2)
+            rs, rr, out_rot = rotation_rate(
+                tabs, self.love, self.p, h, np.array(info.il[:]).reshape(3, 3), np.array(info.mm[:]),
+                lam[..., 0] + 1j * lam[..., 1], rec[2:11].reshape(3, 3), rec[11:14].copy(),
+                rec[14:20].reshape(3, 2) @ np.array([1.0, 1j]), rot[:9 * K].reshape(K, 3, 3),
+                rot[9 * K:12 * K].reshape(K, 3), rot[12 * K:].reshape(K, 3, 2) @ np.array([1.0, 1j]))
+            dsl[0:3, 0:3] += rs
+            drr[0:3, 0:3] += rr
+        if getattr(self, "_rate_sht", None) is None:
+            self._rate_sht = make_sht("cuda", self.nlat, self.nlon, self.norder)
+        cst = self._fetch("_rate_ocean", _lib.F_OCEAN) * self._fetch("_rate_beta", _lib.F_BETA)
+        out = rate_grids(self._rate_sht, dsl, drr, complex(rec[0], rec[1]), h, cst, self.p)
+        if out_rot is not None:
+            out.update(out_rot)
+        return out
+
+    def step(self, icexy_cur, profile=False, dt=None, rates=False):
+        h_rates = self._rates_setup(rates, dt)
         t0 = time.perf_counter()
         try:
             import torch
@@ -325,7 +375,7 @@ class SeaLevelSolver:
             "il": np.array(info.il[:]).reshape(3, 3),
             "mm": np.array(info.mm[:]),
             "lambda": lam[..., 0] + 1j * lam[..., 1],
-            "rates": None,
+            "rates": self._rates_read(info, h_rates) if rates else None,
             "wall": wall,
             "xi": info.xi,
             "prof": {"total": wall} if profile else None,

@@ -127,3 +127,14 @@ def test_love_reader_roundtrip(tmp_path):
         assert np.allclose(L.r[:K, l], rh, rtol=1e-8)
         assert np.allclose(L.rprime[:K, l], rk / l, rtol=1e-8)
     assert L.max_modes == K
+
+
+def test_ramp_factor_series_and_limits():
+    from slevolve_b200.rates import ramp_factor
+
+    x = np.array([0.0, 1e-9, 5e-5, 9.99e-5, 1.0001e-4, 0.3, 2.0, 50.0])
+    phi, omp = ramp_factor(x)
+    assert phi[0] == 1.0 and omp[0] == 0.0
+    exact = np.where(x > 0, -np.expm1(-np.where(x > 0, x, 1.0)) / np.where(x > 0, x, 1.0), 1.0)
+    assert np.allclose(phi, exact, rtol=1e-13, atol=0)
+    assert np.allclose(phi + omp, 1.0, rtol=0, atol=2e-16)
