@@ -179,6 +179,16 @@ int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device);
  * advance, r_il [K][9], r_m [K][3], r_Lambda [K][3 complex]).  SLE_ERR_STATE without tables. */
 int sle_solver_set_rate_tables(sle_solver* s, const double* tab);
 int sle_solver_get_rates(sle_solver* s, void* dsl, void* drr, double* rec, double* rot);
+/* Horizontal read-out (solver.py:424-448, 687-720; output only).  set_horizontal(tab): host
+ * doubles [a_hl (K x (lmax+1)) = l_k / s_k per mode and degree, then ttl l^E (lmax+1)]; NULL
+ * turns it off.  While on, every step forms before its commit the potential
+ * Psi = ttl l^E (rhoi dI* + rhow dS_prev + rhow load) + ttl sum_k a_hl R_k (degree 0 zero, the
+ * degree-2 rotational term left to the caller).  get_horizontal after a step: psi dense
+ * complex128 [lmax+1][lmax+1] (host), r_lam (6 K doubles: the degree-2 modal Lambda states,
+ * [K][3 complex]) and lam12 (12 doubles: the degree-2 Lambda committed before the step and the
+ * step's increment, 3 complex each).  SLE_ERR_STATE while off. */
+int sle_solver_set_horizontal(sle_solver* s, const double* tab);
+int sle_solver_get_horizontal(sle_solver* s, void* psi, double* r_lam, double* lam12);
 /* Cross-pass warm start, reuse="warm" (solver_opt.py:400-403, 514-528, 932-947): a store in
  * device memory kept by the caller across solves of the same ice history (outer iterations,
  * run_outer.py).  ds_store: [capacity][ncoef] complex128 (packed), 16-byte aligned; mask_store:

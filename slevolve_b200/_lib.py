@@ -87,6 +87,8 @@ _SIGS = {
     "sle_solver_get": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "sle_solver_set_rate_tables": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sle_solver_get_rates": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sle_solver_set_horizontal": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "sle_solver_get_horizontal": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_solver_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "sle_batch_create": (C.c_int, [C.POINTER(SleConfig), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "sle_batch_destroy": (C.c_int, [C.c_void_p]),

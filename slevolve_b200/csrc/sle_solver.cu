@@ -74,6 +74,7 @@ struct SlotStep {
   unsigned char* rec_mask;         // where this pass's converged ocean function goes
   int rates;                       // read the analytic rate spectra before the commit
   double rate_h;                   // the step's length (years)
+  int horiz;                       // read the horizontal-displacement potential before the commit
 };
 
 enum GridId {
@@ -925,6 +926,41 @@ __global__ void k_rate_spec(Dev D, double2* rspec, const double* rtab, double* r
                         __dadd_rn(__ddiv_rn(__dmul_rn(the, cur.y), h), __dmul_rn(ttl, rr.y)));
 }
 
+// Horizontal-displacement potential (solver.py:687-720, horizontal read-out), read before the
+// commit: with A = (rhoi dI* + rhow dS_prev) + rhow load (the load of the radial term, formed as
+// k_rr forms it) and visc_h = sum_k a_hl R_k over the degree's modes,
+//   Psi = (ttl l^E) A + ttl visc_h,  zero at degree 0;
+// the degree-2 rotational term is added on the host.
+__global__ void k_horiz_spec(Dev D, double2* hspec, const double* htab) {
+  SLOT_OR_RETURN();
+  if (!D.ss[b].horiz || sc->status) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D.ncoef) return;
+  double2* out = hspec + (size_t)b * D.ncoef;
+  const int l = D.lidx[i];
+  if (l == 0) {
+    out[i] = make_double2(0.0, 0.0);
+    return;
+  }
+  const int nl = D.nl, K = D.K;
+  const double* a_hl = htab + (size_t)b * (K + 1) * nl;
+  const double ttlle = a_hl[(size_t)K * nl + l];
+  const double2 a = D.sp(S_DI, b)[i], bb = D.sp(S_P_OCEAN, b)[i], c = D.sp(S_LOAD, b)[i];
+  const double re = __dadd_rn(__dadd_rn(__dmul_rn(a.x, D.rhoi), __dmul_rn(bb.x, D.rhow)), __dmul_rn(c.x, D.rhow));
+  const double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(bb.y, D.rhow)), __dmul_rn(c.y, D.rhow));
+  double2 v = make_double2(0.0, 0.0);
+  const double2* R = D.R + (size_t)b * K * D.ncoef;
+  const int nk = D.nmod[(size_t)b * nl + l];
+  for (int k = 0; k < nk; ++k) {
+    const double2 r = R[(size_t)k * D.ncoef + i];
+    const double w = a_hl[(size_t)k * nl + l];
+    v = make_double2(__dadd_rn(v.x, __dmul_rn(w, r.x)), __dadd_rn(v.y, __dmul_rn(w, r.y)));
+  }
+  const double t = D.ttl[(size_t)b * nl + l];
+  out[i] = make_double2(__dadd_rn(__dmul_rn(ttlle, re), __dmul_rn(t, v.x)),
+                        __dadd_rn(__dmul_rn(ttlle, im), __dmul_rn(t, v.y)));
+}
+
 __global__ void k_commit(Dev D, int extrap) {
   SLOT_OR_RETURN();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1130,6 +1166,11 @@ struct sle_batch {
   double* rate_tab;
   double* rate_rec;
   std::vector<char> rates_on;
+  // horizontal read-out (opt-in per slot): potential spectra [nslot][ncoef], weights
+  // [nslot][K nl + nl] (a_hl = l_k / s_k, then ttl l^E)
+  double2* horiz_spec;
+  double* horiz_tab;
+  std::vector<char> horiz_on;
   // pinned mirrors
   Scal* hsc;
   SlotStep* hss;
@@ -1172,7 +1213,7 @@ void batch_free(sle_batch* s) {
   void* ptrs[] = {s->grid, s->mask, s->spec, s->R, s->nmod, s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr, s->ttl,
                   s->ttlekhl, s->ttlhe, s->a_il, s->a_m, s->a_tsl, s->a_trr, s->rc, s->r_il, s->r_m,
                   s->r_lam, s->sc, s->ss, s->partials, s->counter, s->rows, s->badflag, s->bstatus,
-                  s->rate_spec, s->rate_tab, s->rate_rec};
+                  s->rate_spec, s->rate_tab, s->rate_rec, s->horiz_spec, s->horiz_tab};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (s->hsc) cudaFreeHost(s->hsc);
@@ -1700,6 +1741,7 @@ int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, cons
     p.hsel = h.hsel;
     p.rates = (b < (int)s->rates_on.size() && s->rates_on[b]) ? 1 : 0;
     p.rate_h = dt;
+    p.horiz = (b < (int)s->horiz_on.size() && s->horiz_on[b]) ? 1 : 0;
     if (s->cfg.inner_extrap && h.nhist >= 2) {
       const double dt0 = dt, dt1 = h.dt_hist[0], dt2 = h.dt_hist[1];
       if (dt0 == dt1 && dt1 == dt2) {
@@ -1789,6 +1831,12 @@ int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, cons
     if (any_rates) {
       note_launch();
       k_rate_spec<<<dim3(nb(nc), UB), 256, 0, st>>>(D, s->rate_spec, s->rate_tab, s->rate_rec);
+    }
+    bool any_horiz = false;
+    for (int b : act) any_horiz |= s->hss[b].horiz != 0;
+    if (any_horiz) {
+      note_launch();
+      k_horiz_spec<<<dim3(nb(nc), UB), 256, 0, st>>>(D, s->horiz_spec, s->horiz_tab);
     }
   }
   // ---- commit (solver.py:1080-1096); extrap history (solver_opt.py:817-822)
@@ -2206,6 +2254,52 @@ extern "C" int sle_solver_get_rates(sle_solver* s, void* dsl, void* drr, double*
   SLE_CUDA(cudaMemcpy(rot, b->r_il, sizeof(double) * 9 * K, cudaMemcpyDeviceToHost));
   SLE_CUDA(cudaMemcpy(rot + 9 * K, b->r_m, sizeof(double) * 3 * K, cudaMemcpyDeviceToHost));
   SLE_CUDA(cudaMemcpy(rot + 12 * K, b->r_lam, sizeof(double) * 6 * K, cudaMemcpyDeviceToHost));
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_set_horizontal(sle_solver* s, const double* tab) {
+  if (!s) {
+    set_error("sle_solver_set_horizontal: NULL solver");
+    return SLE_ERR_BAD_ARG;
+  }
+  sle_batch* b = s->b;
+  b->horiz_on.resize(b->nslot, 0);
+  if (!tab) {
+    b->horiz_on[0] = 0;
+    return SLE_OK;
+  }
+  const size_t per = (size_t)(b->K + 1) * b->D.nl;
+  if (!b->horiz_spec) {
+    SLE_TRY(dalloc(&b->horiz_spec, (size_t)b->nslot * b->D.ncoef));
+    SLE_TRY(dalloc(&b->horiz_tab, (size_t)b->nslot * per));
+  }
+  SLE_CUDA(cudaMemcpyAsync(b->horiz_tab, tab, per * sizeof(double), cudaMemcpyHostToDevice, b->st));
+  SLE_CUDA(cudaStreamSynchronize(b->st));
+  b->horiz_on[0] = 1;
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_get_horizontal(sle_solver* s, void* psi, double* r_lam, double* lam12) {
+  if (!s || !psi || !r_lam || !lam12) {
+    set_error("sle_solver_get_horizontal: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  sle_batch* b = s->b;
+  if (b->horiz_on.empty() || !b->horiz_on[0] || !b->horiz_spec) {
+    set_error("sle_solver_get_horizontal: the read-out is off (sle_solver_set_horizontal before the step)");
+    return SLE_ERR_STATE;
+  }
+  const Dev& D = b->D;
+  double2* stage = b->plan->packbuf;  // staging (nm*nm <= 4*ncoef)
+  SLE_TRY(sht_unpack(b->plan, b->horiz_spec, stage, b->st));
+  SLE_CUDA(cudaMemcpyAsync(psi, stage, sizeof(double2) * (size_t)D.nl * D.nl, cudaMemcpyDeviceToHost, b->st));
+  SLE_CUDA(cudaStreamSynchronize(b->st));
+  SLE_CUDA(cudaMemcpy(r_lam, b->r_lam, sizeof(double) * 6 * b->K, cudaMemcpyDeviceToHost));
+  const Scal& f = b->hsc[0];
+  for (int q = 0; q < 6; ++q) {
+    lam12[q] = f.dlam_prev2[q];
+    lam12[6 + q] = f.dlam_cur2[q];
+  }
   return SLE_OK;
 }
 

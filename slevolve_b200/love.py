@@ -98,6 +98,13 @@ class LoveNumbers:
         self.rprime = rk
         self.rT = trh
         self.rprimeT = trk
+        # tangential-displacement (l) numbers of the optional horizontal read-out, scaled as k
+        self.le = np.zeros(nl)
+        self.lTE = np.zeros(nl)
+        self.le[1:] = el[1, 1:] / ell
+        self.lTE[1:] = tel[1, 1:] / ell
+        self.rl = rl
+        self.rlT = trl
         self.max_modes = int(nmod.max())
 
 

@@ -310,6 +310,51 @@ class SeaLevelSolver:
             self._rates_dt = None
         return None
 
+    def _horizontal_setup(self):
+        """Weights of the horizontal read-out (a_hl = l_k / s_k, ttl l^E; solver.py:424-434,
+        697-700), uploaded once; off again when ``horizontal`` is cleared."""
+        on = bool(getattr(self, "horizontal", False))
+        if on and not getattr(self, "_horiz_set", False):
+            love, L = self.love, self.norder
+            K = int(love.max_modes)   # the solver's mode capacity (mode_arrays)
+            nl = L + 1
+            a_hl = np.zeros((K, nl))
+            a_thl = np.zeros(K)
+            for l in range(1, nl):
+                nm = int(love.nmod[l])
+                a_hl[:nm, l] = love.rl[:nm, l] / love.s[:nm, l]
+                if l == 2:
+                    a_thl[:nm] = love.rlT[:nm, l] / love.s[:nm, l]
+            le = np.concatenate(([0.0], np.asarray(love.le[1:nl], float)))
+            ttl = np.asarray(self._earth_arrays["ttl"], float)
+            tab = np.ascontiguousarray(np.concatenate([a_hl.ravel(), ttl * le]), dtype=np.float64)
+            _lib.check(self._L.sle_solver_set_horizontal(self._h, tab.ctypes.data), "sle_solver_set_horizontal")
+            self._horiz_set, self._horiz_K, self._a_thl = True, K, a_thl
+        elif not on and getattr(self, "_horiz_set", False):
+            _lib.check(self._L.sle_solver_set_horizontal(self._h, None), "sle_solver_set_horizontal")
+            self._horiz_set = False
+        return on
+
+    def _horizontal_read(self):
+        """Psi_lm of the step in the U convention (solver.py:687-720): the device potential plus
+        the degree-2 rotational term (l^T_E Lambda_tot + sum_k a_thl r_Lambda,k) / g."""
+        K = self._horiz_K
+        hz = np.empty((self.nl, self.nl), dtype=np.complex128)
+        r_lam = np.empty(6 * K)
+        lam12 = np.empty(12)
+        _lib.check(self._L.sle_solver_get_horizontal(self._h, hz.ctypes.data, r_lam.ctypes.data, lam12.ctypes.data),
+                   "sle_solver_get_horizontal")
+        if self.tpw and self.norder >= 2:
+            r_la = r_lam.reshape(K, 3, 2) @ np.array([1.0, 1j])
+            thl = np.zeros(3, dtype=np.complex128)
+            for k in range(int(self.love.nmod[2])):
+                thl += self._a_thl[k] * r_la[k]
+            prev = lam12[:6].reshape(3, 2) @ np.array([1.0, 1j])
+            cur = lam12[6:].reshape(3, 2) @ np.array([1.0, 1j])
+            rot = (self.love.lTE[2] * (prev + cur) + thl) / self.p.gacc
+            hz[2, 0:3] += rot
+        return hz
+
     def _rates_read(self, info, h):
         """The reference's rates dict of the step just taken (solver.py:766-806)."""
         from .rates import rate_grids, rotation_rate
@@ -343,6 +388,7 @@ class SeaLevelSolver:
 
     def step(self, icexy_cur, profile=False, dt=None, rates=False):
         h_rates = self._rates_setup(rates, dt)
+        horiz = self._horizontal_setup()
         t0 = time.perf_counter()
         try:
             import torch
@@ -366,7 +412,7 @@ class SeaLevelSolver:
         scal = {
             "iter": info.iter,
             "numiter": info.numiter,
-            "horiz": None,
+            "horiz": self._horizontal_read() if horiz else None,
             "ocean_area": info.ocean_area,
             "oceanBeta_area": info.oceanBeta_area,
             "gmslc_ocn": info.gmslc_ocn,

@@ -19,7 +19,8 @@ class FixtureLove:
     """Love-number object rebuilt from the arrays stored in a golden fixture."""
 
     def __init__(self, fx, prefix="love_"):
-        for key in ("s", "r", "rprime", "rT", "rprimeT", "he", "ke", "hTE", "kTE", "nmod"):
+        for key in ("s", "r", "rprime", "rT", "rprimeT", "he", "ke", "hTE", "kTE", "nmod", "le", "lTE", "rl",
+                    "rlT"):
             if prefix + key in fx:
                 setattr(self, key, np.asarray(fx[prefix + key]))
         self.max_modes = int(self.s.shape[0])
