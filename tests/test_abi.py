@@ -106,7 +106,7 @@ def test_love_reader_roundtrip(tmp_path):
         el = rng.normal(size=5)
         fl = rng.normal(size=5)
         rh, rl, rk = (rng.normal(size=K) for _ in range(3))
-        vals[l] = (el, rh, rk)
+        vals[l] = (el, rh, rk, rl)
         lines.append(" ".join(f"{x:.8E}" for x in el))
         lines.append(" ".join(f"{x:.8E}" for x in fl))
         for r in (rh, rl, rk):
@@ -120,12 +120,14 @@ def test_love_reader_roundtrip(tmp_path):
     path.write_text("\n".join(lines) + "\n")
     L = LoveNumbers(str(path), lmax)
     for l in range(1, lmax + 1):
-        el, rh, rk = vals[l]
+        el, rh, rk, rl = vals[l]
         assert np.allclose(L.s[:K, l], s[:, l], rtol=1e-8)
         assert np.isclose(L.he[l], el[0], rtol=1e-8)
         assert np.isclose(L.ke[l], el[4] / l, rtol=1e-8)
+        assert np.isclose(L.le[l], el[1] / l, rtol=1e-8)     # tangential numbers, scaled as k
         assert np.allclose(L.r[:K, l], rh, rtol=1e-8)
         assert np.allclose(L.rprime[:K, l], rk / l, rtol=1e-8)
+        assert np.allclose(L.rl[:K, l], rl / l, rtol=1e-8)
     assert L.max_modes == K
 
 
