@@ -153,7 +153,7 @@ class OracleSolver:
             self.state.set_dt(self.dt)
 
     # ------------------------------------------------------------------- step
-    def step(self, icexy_cur, dt=None):
+    def step(self, icexy_cur, dt=None, rates=False):
         self.set_step_dt(dt)
         p, sht, nl = self.p, self.sht, self.nl
         self.iter += 1
@@ -323,6 +323,28 @@ class OracleSolver:
         cur = dice * p.rhoi
         cur += load_inc * p.rhow
         cur[0, :] = 0.0
+        # optional read-outs, before the commit (solver.py:1075-1088)
+        rate_sp = None
+        if rates:
+            from .readouts import RateWeights, rate_spectra, rotation_rate
+
+            if getattr(self, "_rate_w", None) is None:
+                self._rate_w = RateWeights(st)
+            self._rate_w.set_dt(st, self.dt)
+            dsl_r, drr_r = rate_spectra(st, self._rate_w, cur, float(self.dt), self.ttl, self.ttlekhl, self.ttlhe)
+            rot_r = None
+            if self.tpw and nl >= 3:
+                rs_, rr_, rot_r = rotation_rate(st, self._rate_w, self.love, p, float(self.dt), self.il, self.mm,
+                                                self.lam, oldil, oldm, dlam_prev2)
+                dsl_r[0:3, 0:3] += rs_
+                drr_r[0:3, 0:3] += rr_
+            rate_sp = (dsl_r, drr_r, complex(dice[0, 0]), rot_r)
+        hz = None
+        if getattr(self, "horizontal", False):
+            from .readouts import horizontal_psi
+
+            hz = horizontal_psi(st, self.love, p, self.ttl, dI, dS_prev, load_inc,
+                                dlam_prev2 + dlam_cur2 if self.tpw else None, self.tpw)
         if self.tpw:
             st.commit(cur, dil_cur, dm_cur, dlam_cur2)
         else:
@@ -358,7 +380,16 @@ class OracleSolver:
         self.icexy_prev = ice
         self.beta = beta
         self.load_inc_lm = load_inc
+        rate_out = None
+        if rate_sp is not None:
+            from .readouts import rate_grids
+
+            rate_out = rate_grids(sht, rate_sp[0], rate_sp[1], rate_sp[2], self.dt, self.cxy, beta, p)
+            if rate_sp[3] is not None:
+                rate_out.update(rate_sp[3])
         return {
+            "rates": rate_out,
+            "horiz": hz,
             "iter": it,
             "numiter": ninner,
             "tgrid": topo,

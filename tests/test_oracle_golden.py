@@ -160,3 +160,41 @@ def test_variable_step_lengths_against_reference(kind):
             assert np.abs(r["tgrid"] - fx[f"{kind}_tgrid_{k}"]).max() <= TOL_M, k
             assert np.abs(r["R"] - fx[f"{kind}_R_{k}"]).max() <= TOL_M, k
     assert numiter == list(fx[f"{kind}_numiter"])
+
+
+def test_rates_readout_against_reference():
+    """The oracle's analytic rates (step(..., rates=True)) against the reference's own output
+    (golden: make_golden_rates.py): 1e-8 of the largest value of each kind."""
+    from slevolve_b200.synthetic import case_c0
+    fx = load_golden("rates.npz")
+    sht = OracleSHT(64, 128, 63)
+    case = case_c0(sht, nsteps=len(fx["dts"]) + 8)
+    slv = OracleSolver(sht, case.love, case.topo, case.ice(0), norder=63, dt=1.0)
+    for k, dt in enumerate(fx["dts"], start=1):
+        r = slv.step(case.ice(k), dt=float(dt), rates=True)
+        assert r["numiter"] == int(fx[f"numiter_{k}"])
+        for key in ("dSLdt", "dRdt", "dSLdt_lm", "dRdt_lm", "ildot", "mdot", "lambdadot"):
+            name = f"{key}_{k}"
+            if name in fx:
+                ref = fx[name]
+                assert np.abs(np.asarray(r["rates"][key]) - ref).max() <= 1e-8 * np.abs(ref).max(), name
+
+
+def test_horizontal_readout_against_reference():
+    """The oracle's horizontal potential (horizontal = True) against the reference's own output
+    with its PREM Love file (golden: make_golden_horiz.py): 1e-9 of the largest coefficient."""
+    from slevolve_b200.synthetic import case_c0
+    fx = load_golden("horiz.npz")
+    love = FixtureLove(fx)
+    sht = OracleSHT(64, 128, 63)
+    case = case_c0(sht, nsteps=len(fx["dts"]) + 8)
+    slv = OracleSolver(sht, love, case.topo, case.ice(0), norder=63, dt=1.0)
+    slv.horizontal = True
+    numiter = []
+    for k, dt in enumerate(fx["dts"], start=1):
+        r = slv.step(case.ice(k), dt=float(dt))
+        numiter.append(r["numiter"])
+        if f"horiz_{k}" in fx:
+            ref = fx[f"horiz_{k}"]
+            assert np.abs(r["horiz"] - ref).max() <= 1e-9 * np.abs(ref).max(), k
+    assert numiter == list(fx["numiter"])
