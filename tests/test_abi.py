@@ -45,6 +45,17 @@ def test_error_mapping():
         _lib.check(lib.sle_sht_create(16, 32, 17, C.byref(h)), "create")
     with pytest.raises(ValueError, match="power of two"):
         _lib.check(lib.sle_sht_create(16, 48, 15, C.byref(h)), "create")
+    # read-out and driver-helper entry points: NULL arguments are refused before any device call
+    assert lib.sle_solver_set_rate_tables(None, None) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_solver_get_rates(None, None, None, None, None) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_solver_set_horizontal(None, None) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_solver_get_horizontal(None, None, None, None) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_topo_scratch_bytes() >= 16
+    buf = (C.c_double * 2)()
+    assert lib.sle_topo_residual(None, None, 0.0, None, None, None, None, 4, 8, 920.0, 1000.0, None, buf,
+                                 None) == _lib.SLE_ERR_BAD_ARG
+    with pytest.raises(ValueError, match="NULL"):
+        _lib.check(lib.sle_solver_get_rates(None, None, None, None, None), "sle_solver_get_rates")
 
 
 def test_solver_rejects_unprovided_options():
