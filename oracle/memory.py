@@ -52,6 +52,10 @@ class ModalState:
         self.dt_years = None
         self.decay = np.zeros((kmax, nl))
         self.omd = np.ones((kmax, nl))
+        # second-order load placement (solver.py:287-294, 348-368): off unless the solver sets it
+        self.ramp = False
+        self.phi = np.ones((kmax, nl))
+        self.omphi = np.zeros((kmax, nl))
         self.set_dt(dt_years)
 
         self.R = np.zeros((kmax, nl, nl), dtype=np.complex128)
@@ -77,6 +81,25 @@ class ModalState:
         self.decay[...] = d
         self.omd[...] = 1.0 - d
         self.dt_years = dt_years
+        self._ramp_coeffs(dt_years)
+
+    def _ramp_coeffs(self, dt_years):
+        """phi and 1 - phi of every mode for the step length and the same-step viscous weights
+        c = sum_k a_k (1 - phi_k) (solver.py:348-368)."""
+        from .readouts import ramp_factor
+
+        phi, omp = ramp_factor(self.s * (dt_years / 1000.0))
+        exists = self.s > 0
+        self.phi[...] = np.where(exists, phi, 1.0)
+        self.omphi[...] = np.where(exists, omp, 0.0)
+        self.c_sl = (self.a_sl * self.omphi).sum(0)
+        self.c_rr = (self.a_rr * self.omphi).sum(0)
+        n2 = self.nmod2
+        c2 = self.omphi[:n2, 2] if self.lmax >= 2 else np.zeros(0)
+        self.c_il = float(c2 @ self.a_il[:n2])
+        self.c_m = float(c2 @ self.a_m[:n2])
+        self.c_tsl = float(c2 @ self.a_tsl[:n2])
+        self.c_trr = float(c2 @ self.a_trr[:n2])
 
     def advance_and_read(self):
         nl = self.lmax + 1
@@ -107,6 +130,20 @@ class ModalState:
         return visc, rad, s_il, s_m, s_tsl, s_trr
 
     def commit(self, load, dil=None, dm=None, dlam=None):
+        if self.ramp:
+            # the step's increment already carries 1 - phi_k of its response in every mode
+            # (solver.py:450-452, 486-499)
+            for k in range(self.kmax):
+                self.R[k] += self.omphi[k][:, None] * load
+            if self.lmax >= 2:
+                n2 = self.nmod2
+                c = self.omphi[:n2, 2]
+                if dil is not None:
+                    self.r_il[:n2] += c[:, None, None] * dil[None]
+                if dm is not None:
+                    self.r_m[:n2] += c[:, None] * dm[None]
+                if dlam is not None:
+                    self.r_lambda[:n2] += c[:, None] * dlam[None]
         self.p_load += load
         if dil is not None:
             self.p_il += dil

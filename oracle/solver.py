@@ -70,7 +70,7 @@ def extrap_guess(h1, h2, dt0, dt1, dt2):
 class OracleSolver:
     def __init__(self, sht, love, topo0, ice0, *, norder, dt=1.0, tpw=True, checkmarine=True,
                  calcRG=True, epsilon1=1.0e-5, planet=None, opt=(), inner="off",
-                 reuse="off", reuse_store=None):
+                 reuse="off", reuse_store=None, ramp=False):
         if inner not in ("off", "extrap"):
             raise ValueError(f"inner must be off|extrap, got {inner!r}")
         if reuse not in ("off", "warm"):
@@ -113,6 +113,8 @@ class OracleSolver:
         self.ice_volume0 = c[0, 0].real * 4 * PI * p.radius ** 2
 
         self.state = ModalState(love, self.norder, self.dt)
+        self.ramp = bool(ramp)           # second-order load placement (solver.py:584-586)
+        self.state.ramp = self.ramp
         self.il = np.zeros((3, 3))
         self.mm = np.zeros(3)
         self.lam = np.zeros((3, 3), dtype=np.complex128)
@@ -222,11 +224,23 @@ class OracleSolver:
                 self.il[0, 2] = (-8 * PI * p.radius ** 4 / (math.sqrt(30.0))) * z21.real
                 self.il[1, 2] = (8 * PI * p.radius ** 4 / (math.sqrt(30.0))) * (-1.0 * II * z21).real
                 dil_cur = self.il - oldil
-                for i in (0, 1):
-                    self.mm[i] = (1 / (1 - kTE2 / p.kf)) * (
-                        (1 / (p.moiC - p.moiA)) * ((1 + kE2) * self.il[i, 2] + sum_il[i, 2])
-                        + (1 / p.kf) * sum_m[i])
-                self.mm[2] = -(1.0 / p.moiC) * ((1 + kE2) * self.il[2, 2] + sum_il[2, 2])
+                if self.ramp:
+                    # the current increments carry 1 - phi of their viscous response, implicit in m
+                    # (solver.py:922-935)
+                    sil_r = sum_il + st.c_il * dil_cur
+                    al_ = 1 / (1 - kTE2 / p.kf)
+                    for i in (0, 1):
+                        self.mm[i] = al_ * (
+                            (1 / (p.moiC - p.moiA)) * ((1 + kE2) * self.il[i, 2] + sil_r[i, 2])
+                            + (1 / p.kf) * (sum_m[i] - st.c_m * oldm[i])
+                        ) / (1 - al_ * st.c_m / p.kf)
+                    self.mm[2] = -(1.0 / p.moiC) * ((1 + kE2) * self.il[2, 2] + sil_r[2, 2])
+                else:
+                    for i in (0, 1):
+                        self.mm[i] = (1 / (1 - kTE2 / p.kf)) * (
+                            (1 / (p.moiC - p.moiA)) * ((1 + kE2) * self.il[i, 2] + sum_il[i, 2])
+                            + (1 / p.kf) * sum_m[i])
+                    self.mm[2] = -(1.0 / p.moiC) * ((1 + kE2) * self.il[2, 2] + sum_il[2, 2])
                 dm_cur = self.mm - oldm
                 m1, m2, m3 = self.mm[0], self.mm[1], self.mm[2]
                 self.lam[0, 0] = (r2w2 / 3.0) * ((m1 ** 2 + m2 ** 2 + m3 ** 2) + 2.0 * m3)
@@ -236,11 +250,15 @@ class OracleSolver:
                 dlam_cur2 = self.lam[2, 0:3] - dlam_prev2
                 ekhTE = 1 + kTE2 - hTE2
                 tot = dlam_prev2 + dlam_cur2
+                tsl_v, trr_v = exact_tsl, exact_trr
+                if self.ramp:
+                    tsl_v = exact_tsl + st.c_tsl * dlam_cur2
+                    trr_v = exact_trr + st.c_trr * dlam_cur2
                 dsl_rot[:] = 0.0
-                dsl_rot[2, 0:3] = (ekhTE * tot + exact_tsl) / p.gacc
+                dsl_rot[2, 0:3] = (ekhTE * tot + tsl_v) / p.gacc
                 if self.calcRG:
                     rr_rot[:] = 0.0
-                    rr_rot[2, 0:3] = (hTE2 * tot + exact_trr) / p.gacc
+                    rr_rot[2, 0:3] = (hTE2 * tot + trr_v) / p.gacc
 
             # eq. B18 in the reference's statement order (solver.py:977-991)
             A = dI * p.rhoi
@@ -248,6 +266,8 @@ class OracleSolver:
             A += load_inc * p.rhow
             sl_inc = A * self.ttlekhl
             sl_inc += visc * self.ttl
+            if self.ramp:   # same-step viscous weight of the current increment (solver.py:988-989)
+                sl_inc += (self.ttl[:, 0] * st.c_sl)[:, None] * (p.rhoi * dice + p.rhow * load_inc)
             sl_inc[0:3, 0:3] += dsl_rot
 
             dslxy = sht.synthesis(sl_inc)
@@ -317,6 +337,8 @@ class OracleSolver:
             A += load_inc * p.rhow
             rrlm = A * self.ttlhe
             rrlm += radial * self.ttl
+            if self.ramp:   # solver.py:1065-1067
+                rrlm += (self.ttl[:, 0] * st.c_rr)[:, None] * (p.rhoi * dice + p.rhow * load_inc)
             rrlm[0:3, 0:3] += rr_rot
             rrxy = sht.synthesis(rrlm)
 

@@ -198,3 +198,29 @@ def test_horizontal_readout_against_reference():
             ref = fx[f"horiz_{k}"]
             assert np.abs(r["horiz"] - ref).max() <= 1e-9 * np.abs(ref).max(), k
     assert numiter == list(fx["numiter"])
+
+
+def test_ramp_placement_against_reference():
+    """The oracle with the second-order load placement (ramp=True) against the reference's own
+    run (golden: make_golden_ramp.py): 1e-9 m, identical iteration counts, rotational totals and,
+    for the last step, the rates read-out under the ramp-consistent state."""
+    from slevolve_b200.synthetic import case_c0
+    fx = load_golden("ramp.npz")
+    sht = OracleSHT(64, 128, 63)
+    case = case_c0(sht, nsteps=len(fx["dts"]) + 8)
+    slv = OracleSolver(sht, case.love, case.topo, case.ice(0), norder=63, dt=1.0, ramp=True)
+    numiter = []
+    for k, dt in enumerate(fx["dts"], start=1):
+        r = slv.step(case.ice(k), dt=float(dt), rates=k >= int(fx["rates_from"]))
+        numiter.append(r["numiter"])
+        for key in ("mm", "il", "lambda"):
+            ref = fx[key]
+            assert np.abs(np.asarray(r[key]) - ref[k - 1]).max() <= 1e-9 * float(np.abs(ref).max()), (k, key)
+        if f"tgrid_{k}" in fx:
+            assert np.abs(r["tgrid"] - fx[f"tgrid_{k}"]).max() <= TOL_M, k
+            assert np.abs(r["R"] - fx[f"R_{k}"]).max() <= TOL_M, k
+        if k == len(fx["dts"]):
+            for key in ("dSLdt", "dRdt", "ildot", "mdot", "lambdadot"):
+                ref = fx[f"rates_{key}"]
+                assert np.abs(np.asarray(r["rates"][key]) - ref).max() <= 1e-8 * np.abs(ref).max(), key
+    assert numiter == list(fx["numiter"])
