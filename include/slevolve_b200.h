@@ -176,7 +176,8 @@ int sle_solver_get(sle_solver* s, int field, void* dst, int dst_on_device);
  * get_rates after a step: dsl, drr dense complex128 [lmax+1][lmax+1] (host); rec (20 doubles:
  * dI*_00 of the step (re, im), then the rotational totals committed before it: il (9), m (3),
  * Lambda degree 2 (3 complex)); rot (18 K doubles: the degree-2 modal states after the step's
- * advance, r_il [K][9], r_m [K][3], r_Lambda [K][3 complex]).  SLE_ERR_STATE without tables. */
+ * advance and before its commit, r_il [K][9], r_m [K][3], r_Lambda [K][3 complex]).
+ * SLE_ERR_STATE without tables. */
 int sle_solver_set_rate_tables(sle_solver* s, const double* tab);
 int sle_solver_get_rates(sle_solver* s, void* dsl, void* drr, double* rec, double* rot);
 /* Horizontal read-out (solver.py:424-448, 687-720; output only).  set_horizontal(tab): host
@@ -187,6 +188,12 @@ int sle_solver_get_rates(sle_solver* s, void* dsl, void* drr, double* rec, doubl
  * complex128 [lmax+1][lmax+1] (host), r_lam (6 K doubles: the degree-2 modal Lambda states,
  * [K][3 complex]) and lam12 (12 doubles: the degree-2 Lambda committed before the step and the
  * step's increment, 3 complex each).  SLE_ERR_STATE while off. */
+/* Second-order load placement ("ramp", solver.py:229-240, 348-368, 450-499, 904-991, 1065-1067):
+ * the step's load increment accrues linearly over the step, so each mode already holds 1 - phi_k
+ * of its response at the step's end.  tab: host doubles for the coming steps' length,
+ * [omphi = 1 - phi (K x (lmax+1)), ttl c_sl (lmax+1), ttl c_rr (lmax+1), c_il, c_m, c_tsl, c_trr]
+ * (the reference's ExactMemory coefficients); NULL turns the placement off. */
+int sle_solver_set_ramp(sle_solver* s, const double* tab);
 int sle_solver_set_horizontal(sle_solver* s, const double* tab);
 int sle_solver_get_horizontal(sle_solver* s, void* psi, double* r_lam, double* lam12);
 /* Cross-pass warm start, reuse="warm" (solver_opt.py:400-403, 514-528, 932-947): a store in

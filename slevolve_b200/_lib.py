@@ -87,6 +87,7 @@ _SIGS = {
     "sle_solver_get": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "sle_solver_set_rate_tables": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sle_solver_get_rates": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sle_solver_set_ramp": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sle_solver_set_horizontal": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sle_solver_get_horizontal": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_solver_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),

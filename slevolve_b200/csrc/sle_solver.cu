@@ -36,6 +36,7 @@ struct RotConst {
   double c_il22, c_il02, c_il12;   // -8 PI a^4/(3 sqrt5), -8 PI a^4/sqrt30, 8 PI a^4/sqrt30
   double alpha;                    // 1 / (1 - kTE2/kf)
   double inv_CmA, inv_kf, inv_C;   // 1/(C-A), 1/kf, 1.0/C
+  double kf;                       // the ramp's implicit m divides by kf itself
   double onepk;                    // 1 + kE2
   double r2w2_3, r2w2_6s5, r2w2_s30, r2w2_s120;
   double ekhTE, hTE2, gacc;
@@ -75,6 +76,11 @@ struct SlotStep {
   int rates;                       // read the analytic rate spectra before the commit
   double rate_h;                   // the step's length (years)
   int horiz;                       // read the horizontal-displacement potential before the commit
+  // second-order load placement (ramp, solver.py:348-368): the slot's table for this step length,
+  // [omphi (K nl), ttl c_sl (nl), ttl c_rr (nl)], and the degree-2 weights c_il, c_m, c_tsl, c_trr
+  int ramp;
+  const double* ramp_tab;
+  double c_il, c_m, c_tsl, c_trr;
 };
 
 enum GridId {
@@ -452,11 +458,26 @@ __device__ void rotation_block(const Dev& D, int b, Scal* sc) {
   il[2] = __dmul_rn(C.c_il02, z21r);
   il[5] = __dmul_rn(C.c_il12, z21i);
   double mm[3];
-  for (int i = 0; i < 2; ++i) {
-    const double a = __dadd_rn(__dmul_rn(C.onepk, il[i * 3 + 2]), sum_il[i * 3 + 2]);
-    mm[i] = __dmul_rn(C.alpha, __dadd_rn(__dmul_rn(C.inv_CmA, a), __dmul_rn(C.inv_kf, sum_m[i])));
+  const SlotStep& ss = D.ss[b];
+  if (ss.ramp) {
+    // the current increments carry 1 - phi of their viscous response, implicit in m
+    // (solver.py:922-935): sil = sum_il + c_il dil, m_i = alpha (...) / (1 - alpha c_m / kf)
+    double sil[9];
+    for (int q = 0; q < 9; ++q) sil[q] = __dadd_rn(sum_il[q], __dmul_rn(ss.c_il, __dsub_rn(il[q], oldil[q])));
+    const double den = __dsub_rn(1.0, __ddiv_rn(__dmul_rn(C.alpha, ss.c_m), C.kf));
+    for (int i = 0; i < 2; ++i) {
+      const double a = __dadd_rn(__dmul_rn(C.onepk, il[i * 3 + 2]), sil[i * 3 + 2]);
+      const double sm = __dsub_rn(sum_m[i], __dmul_rn(ss.c_m, oldm[i]));
+      mm[i] = __ddiv_rn(__dmul_rn(C.alpha, __dadd_rn(__dmul_rn(C.inv_CmA, a), __dmul_rn(C.inv_kf, sm))), den);
+    }
+    mm[2] = __dmul_rn(-C.inv_C, __dadd_rn(__dmul_rn(C.onepk, il[8]), sil[8]));
+  } else {
+    for (int i = 0; i < 2; ++i) {
+      const double a = __dadd_rn(__dmul_rn(C.onepk, il[i * 3 + 2]), sum_il[i * 3 + 2]);
+      mm[i] = __dmul_rn(C.alpha, __dadd_rn(__dmul_rn(C.inv_CmA, a), __dmul_rn(C.inv_kf, sum_m[i])));
+    }
+    mm[2] = __dmul_rn(-C.inv_C, __dadd_rn(__dmul_rn(C.onepk, il[8]), sum_il[8]));
   }
-  mm[2] = __dmul_rn(-C.inv_C, __dadd_rn(__dmul_rn(C.onepk, il[8]), sum_il[8]));
   const double m1 = mm[0], m2 = mm[1], m3 = mm[2];
   const double m1s = __dmul_rn(m1, m1), m2s = __dmul_rn(m2, m2), m3s = __dmul_rn(m3, m3);
   double lam[18];
@@ -474,10 +495,17 @@ __device__ void rotation_block(const Dev& D, int b, Scal* sc) {
     const double di = __dsub_rn(lam[13 + 2 * q], dprev[2 * q + 1]);
     const double tr = __dadd_rn(dprev[2 * q], dr);
     const double ti = __dadd_rn(dprev[2 * q + 1], di);
-    dsl_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, tr), sum_tsl[2 * q]), C.gacc);
-    dsl_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, ti), sum_tsl[2 * q + 1]), C.gacc);
-    rr_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, tr), sum_trr[2 * q]), C.gacc);
-    rr_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, ti), sum_trr[2 * q + 1]), C.gacc);
+    double tsr = sum_tsl[2 * q], tsi = sum_tsl[2 * q + 1], trr = sum_trr[2 * q], tri = sum_trr[2 * q + 1];
+    if (ss.ramp) {   // solver.py:964-966
+      tsr = __dadd_rn(tsr, __dmul_rn(ss.c_tsl, dr));
+      tsi = __dadd_rn(tsi, __dmul_rn(ss.c_tsl, di));
+      trr = __dadd_rn(trr, __dmul_rn(ss.c_trr, dr));
+      tri = __dadd_rn(tri, __dmul_rn(ss.c_trr, di));
+    }
+    dsl_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, tr), tsr), C.gacc);
+    dsl_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.ekhTE, ti), tsi), C.gacc);
+    rr_rot[2 * q] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, tr), trr), C.gacc);
+    rr_rot[2 * q + 1] = __ddiv_rn(__dadd_rn(__dmul_rn(C.hTE2, ti), tri), C.gacc);
     dcur[2 * q] = dr;
     dcur[2 * q + 1] = di;
   }
@@ -570,6 +598,13 @@ __global__ void k_b18(Dev D) {
   double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(bb.y, D.rhow)), __dmul_rn(c.y, D.rhow));
   re = __dadd_rn(__dmul_rn(re, te), __dmul_rn(v.x, t));
   im = __dadd_rn(__dmul_rn(im, te), __dmul_rn(v.y, t));
+  const SlotStep& ss = D.ss[b];
+  if (ss.ramp) {   // same-step viscous weight of the current increment (solver.py:988-989)
+    const double tc = ss.ramp_tab[(size_t)D.K * D.nl + l];
+    const double2 d = D.sp(S_DICE, b)[i];
+    re = __dadd_rn(re, __dmul_rn(tc, __dadd_rn(__dmul_rn(D.rhoi, d.x), __dmul_rn(D.rhow, c.x))));
+    im = __dadd_rn(im, __dmul_rn(tc, __dadd_rn(__dmul_rn(D.rhoi, d.y), __dmul_rn(D.rhow, c.y))));
+  }
   if (D.tpw) {
     const int q = (i == D.i20) ? 0 : (i == D.i21) ? 1 : (i == D.i22) ? 2 : -1;
     if (q >= 0) {
@@ -856,6 +891,13 @@ __global__ void k_rr(Dev D) {
   double im = __dadd_rn(__dadd_rn(__dmul_rn(a.y, D.rhoi), __dmul_rn(bb.y, D.rhow)), __dmul_rn(c.y, D.rhow));
   re = __dadd_rn(__dmul_rn(re, th), __dmul_rn(v.x, t));
   im = __dadd_rn(__dmul_rn(im, th), __dmul_rn(v.y, t));
+  const SlotStep& ss = D.ss[b];
+  if (ss.ramp) {   // solver.py:1065-1067
+    const double tc = ss.ramp_tab[(size_t)(D.K + 1) * D.nl + l];
+    const double2 d = D.sp(S_DICE, b)[i];
+    re = __dadd_rn(re, __dmul_rn(tc, __dadd_rn(__dmul_rn(D.rhoi, d.x), __dmul_rn(D.rhow, c.x))));
+    im = __dadd_rn(im, __dmul_rn(tc, __dadd_rn(__dmul_rn(D.rhoi, d.y), __dmul_rn(D.rhow, c.y))));
+  }
   if (D.tpw) {
     const int q = (i == D.i20) ? 0 : (i == D.i21) ? 1 : (i == D.i22) ? 2 : -1;
     if (q >= 0) {
@@ -876,7 +918,7 @@ __global__ void k_rr(Dev D) {
 //   rr likewise with w_rr,        drr = (ttlhe cur) / h + ttl rr     (radial)
 // and zero at degree 0; each operation rounded as NumPy rounds it.  The degree-2 rotational rates
 // are added on the host.
-__global__ void k_rate_spec(Dev D, double2* rspec, const double* rtab, double* rrec) {
+__global__ void k_rate_spec(Dev D, double2* rspec, const double* rtab, double* rrec, double* rrot) {
   SLOT_OR_RETURN();
   const SlotStep& ss = D.ss[b];
   if (!ss.rates || sc->status) return;
@@ -888,6 +930,12 @@ __global__ void k_rate_spec(Dev D, double2* rspec, const double* rtab, double* r
     const double2 d0 = D.sp(S_DICE, b)[0];
     rrec[2 * b] = d0.x;
     rrec[2 * b + 1] = d0.y;
+    // the degree-2 modal states as the commit finds them (with ramp placement it changes them)
+    const int K = D.K;
+    double* o = rrot + (size_t)b * 18 * K;
+    for (int q = 0; q < 9 * K; ++q) o[q] = D.r_il[(size_t)b * K * 9 + q];
+    for (int q = 0; q < 3 * K; ++q) o[9 * K + q] = D.r_m[(size_t)b * K * 3 + q];
+    for (int q = 0; q < 6 * K; ++q) o[12 * K + q] = D.r_lam[(size_t)b * K * 6 + q];
   }
   const int l = D.lidx[i];
   if (l == 0) {
@@ -980,6 +1028,31 @@ __global__ void k_commit(Dev D, int extrap) {
     const double2 d = D.sp(S_DICE, b)[i];
     cur = make_double2(__dadd_rn(__dmul_rn(d.x, D.rhoi), __dmul_rn(ld.x, D.rhow)),
                        __dadd_rn(__dmul_rn(d.y, D.rhoi), __dmul_rn(ld.y, D.rhow)));
+  }
+  const SlotStep& ss = D.ss[b];
+  if (ss.ramp) {
+    // second-order placement: the step's increment already carries 1 - phi_k of its response in
+    // every mode (solver.py:450-452, 486-499); at degree 2 the rotational states likewise
+    const double* omphi = ss.ramp_tab;
+    double2* R = D.R + (size_t)b * D.K * D.ncoef;
+    const int nk = D.nmod[(size_t)b * D.nl + l];
+    for (int k = 0; k < nk; ++k) {
+      const double w = omphi[(size_t)k * D.nl + l];
+      const double2 r = R[(size_t)k * D.ncoef + i];
+      R[(size_t)k * D.ncoef + i] = make_double2(__dadd_rn(r.x, __dmul_rn(w, cur.x)), __dadd_rn(r.y, __dmul_rn(w, cur.y)));
+    }
+    if (i == 0 && D.tpw && D.nl > 2) {
+      const int n2 = D.nmod[(size_t)b * D.nl + 2];
+      double* r_il = D.r_il + (size_t)b * D.K * 9;
+      double* r_m = D.r_m + (size_t)b * D.K * 3;
+      double* r_lam = D.r_lam + (size_t)b * D.K * 6;
+      for (int k = 0; k < n2; ++k) {
+        const double c = omphi[(size_t)k * D.nl + 2];
+        for (int q = 0; q < 9; ++q) r_il[k * 9 + q] = __dadd_rn(r_il[k * 9 + q], __dmul_rn(c, sc->dil[q]));
+        for (int q = 0; q < 3; ++q) r_m[k * 3 + q] = __dadd_rn(r_m[k * 3 + q], __dmul_rn(c, sc->dm[q]));
+        for (int q = 0; q < 6; ++q) r_lam[k * 6 + q] = __dadd_rn(r_lam[k * 6 + q], __dmul_rn(c, sc->dlam_cur2[q]));
+      }
+    }
   }
   double2* p_load = D.sp(S_P_LOAD, b);
   const double2 p = p_load[i];
@@ -1165,12 +1238,17 @@ struct sle_batch {
   double2* rate_spec;
   double* rate_tab;
   double* rate_rec;
+  double* rate_rot;   // [nslot][18 K]: the degree-2 modal states before the commit
   std::vector<char> rates_on;
   // horizontal read-out (opt-in per slot): potential spectra [nslot][ncoef], weights
   // [nslot][K nl + nl] (a_hl = l_k / s_k, then ttl l^E)
   double2* horiz_spec;
   double* horiz_tab;
   std::vector<char> horiz_on;
+  // ramp placement (opt-in per slot): tables [nslot][(K + 2) nl] and the degree-2 weights
+  double* ramp_tab;
+  std::vector<char> ramp_on;
+  std::vector<double> ramp_c;   // [nslot][4]
   // pinned mirrors
   Scal* hsc;
   SlotStep* hss;
@@ -1213,7 +1291,7 @@ void batch_free(sle_batch* s) {
   void* ptrs[] = {s->grid, s->mask, s->spec, s->R, s->nmod, s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr, s->ttl,
                   s->ttlekhl, s->ttlhe, s->a_il, s->a_m, s->a_tsl, s->a_trr, s->rc, s->r_il, s->r_m,
                   s->r_lam, s->sc, s->ss, s->partials, s->counter, s->rows, s->badflag, s->bstatus,
-                  s->rate_spec, s->rate_tab, s->rate_rec, s->horiz_spec, s->horiz_tab};
+                  s->rate_spec, s->rate_tab, s->rate_rec, s->rate_rot, s->horiz_spec, s->horiz_tab, s->ramp_tab};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (s->hsc) cudaFreeHost(s->hsc);
@@ -1444,6 +1522,7 @@ int set_earth(sle_batch* s, int b, const sle_earth* earth, double dt) {
   C.alpha = 1 / (1 - earth->kTE2 / cfg->kf);
   C.inv_CmA = 1 / (cfg->moiC - cfg->moiA);
   C.inv_kf = 1 / cfg->kf;
+  C.kf = cfg->kf;
   C.inv_C = 1.0 / cfg->moiC;
   C.onepk = 1 + earth->kE2;
   const double r2w2 = std::pow(cfg->radius, 2) * std::pow(cfg->omega, 2);
@@ -1742,6 +1821,14 @@ int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, cons
     p.rates = (b < (int)s->rates_on.size() && s->rates_on[b]) ? 1 : 0;
     p.rate_h = dt;
     p.horiz = (b < (int)s->horiz_on.size() && s->horiz_on[b]) ? 1 : 0;
+    p.ramp = (b < (int)s->ramp_on.size() && s->ramp_on[b]) ? 1 : 0;
+    if (p.ramp) {
+      p.ramp_tab = s->ramp_tab + (size_t)b * (s->K + 2) * s->D.nl;
+      p.c_il = s->ramp_c[4 * b];
+      p.c_m = s->ramp_c[4 * b + 1];
+      p.c_tsl = s->ramp_c[4 * b + 2];
+      p.c_trr = s->ramp_c[4 * b + 3];
+    }
     if (s->cfg.inner_extrap && h.nhist >= 2) {
       const double dt0 = dt, dt1 = h.dt_hist[0], dt2 = h.dt_hist[1];
       if (dt0 == dt1 && dt1 == dt2) {
@@ -1830,7 +1917,7 @@ int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, cons
     for (int b : act) any_rates |= s->hss[b].rates != 0;
     if (any_rates) {
       note_launch();
-      k_rate_spec<<<dim3(nb(nc), UB), 256, 0, st>>>(D, s->rate_spec, s->rate_tab, s->rate_rec);
+      k_rate_spec<<<dim3(nb(nc), UB), 256, 0, st>>>(D, s->rate_spec, s->rate_tab, s->rate_rec, s->rate_rot);
     }
     bool any_horiz = false;
     for (int b : act) any_horiz |= s->hss[b].horiz != 0;
@@ -2217,6 +2304,7 @@ extern "C" int sle_solver_set_rate_tables(sle_solver* s, const double* tab) {
     SLE_TRY(dalloc(&b->rate_spec, (size_t)b->nslot * 2 * b->D.ncoef));
     SLE_TRY(dalloc(&b->rate_tab, (size_t)b->nslot * per));
     SLE_TRY(dalloc(&b->rate_rec, (size_t)b->nslot * 2));
+    SLE_TRY(dalloc(&b->rate_rot, (size_t)b->nslot * 18 * b->K));
   }
   SLE_CUDA(cudaMemcpyAsync(b->rate_tab, tab, per * sizeof(double), cudaMemcpyHostToDevice, b->st));
   SLE_CUDA(cudaStreamSynchronize(b->st));
@@ -2250,10 +2338,28 @@ extern "C" int sle_solver_get_rates(sle_solver* s, void* dsl, void* drr, double*
   for (int q = 0; q < 9; ++q) rec[2 + q] = f.oldil[q];
   for (int q = 0; q < 3; ++q) rec[11 + q] = f.oldm[q];
   for (int q = 0; q < 6; ++q) rec[14 + q] = f.dlam_prev2[q];
-  const int K = b->K;
-  SLE_CUDA(cudaMemcpy(rot, b->r_il, sizeof(double) * 9 * K, cudaMemcpyDeviceToHost));
-  SLE_CUDA(cudaMemcpy(rot + 9 * K, b->r_m, sizeof(double) * 3 * K, cudaMemcpyDeviceToHost));
-  SLE_CUDA(cudaMemcpy(rot + 12 * K, b->r_lam, sizeof(double) * 6 * K, cudaMemcpyDeviceToHost));
+  SLE_CUDA(cudaMemcpy(rot, b->rate_rot, sizeof(double) * 18 * b->K, cudaMemcpyDeviceToHost));
+  return SLE_OK;
+}
+
+extern "C" int sle_solver_set_ramp(sle_solver* s, const double* tab) {
+  if (!s) {
+    set_error("sle_solver_set_ramp: NULL solver");
+    return SLE_ERR_BAD_ARG;
+  }
+  sle_batch* b = s->b;
+  b->ramp_on.resize(b->nslot, 0);
+  b->ramp_c.resize((size_t)4 * b->nslot, 0.0);
+  if (!tab) {
+    b->ramp_on[0] = 0;
+    return SLE_OK;
+  }
+  const size_t per = (size_t)(b->K + 2) * b->D.nl;
+  if (!b->ramp_tab) SLE_TRY(dalloc(&b->ramp_tab, (size_t)b->nslot * per));
+  SLE_CUDA(cudaMemcpyAsync(b->ramp_tab, tab, per * sizeof(double), cudaMemcpyHostToDevice, b->st));
+  SLE_CUDA(cudaStreamSynchronize(b->st));
+  for (int q = 0; q < 4; ++q) b->ramp_c[q] = tab[per + q];
+  b->ramp_on[0] = 1;
   return SLE_OK;
 }
 

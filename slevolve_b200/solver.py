@@ -10,8 +10,10 @@ buffers that the next step overwrites, as the reference's do (tests/test_small_c
 reference copies them for that reason).
 
 Branches of the reference that this build does not provide raise ``NotImplementedError``: the
-second-order ramp placement, the axial-rotation options, Anderson mixing, analytic rates, the
-horizontal read-out and the reuse variants other than ``"warm"``.  The ``raw`` option needs a raw-mode backend and raises
+axial-rotation options, Anderson mixing, the reuse variants other than ``"warm"``, analytic rates
+of a mixed-precision solve and the horizontal read-out together with ramp placement.  Provided:
+``ramp=True`` (second-order load placement), ``step(..., rates=True)`` and
+``solver.horizontal = True``.  The ``raw`` option needs a raw-mode backend and raises
 ``ValueError`` as in the reference (solver_opt.py:299-301).
 """
 
@@ -134,8 +136,6 @@ class SeaLevelSolver:
         opt = set(self._opt_default if opt is None else opt)
         prec = _lib.precision_code(precision)
         inner = self._inner_default if inner is None else inner
-        if ramp:
-            raise NotImplementedError("ramp placement is not provided by the GPU solver")
         if axial_rotation != "off":
             raise NotImplementedError("axial_rotation options are not provided by the GPU solver")
         if inner not in ("off", "extrap", "anderson"):
@@ -168,6 +168,7 @@ class SeaLevelSolver:
         self.checkmarine = bool(checkmarine)
         self.calcRG = bool(calcRG)
         self.horizontal = False
+        self.ramp = bool(ramp)   # second-order load placement (solver.py:584-586)
         self.epsilon1 = float(epsilon1)
         self.p = planet or Planet()
         self.nlat, self.nlon = nlat, nlon
@@ -310,6 +311,35 @@ class SeaLevelSolver:
             self._rates_dt = None
         return None
 
+    def _ramp_setup(self, dt):
+        """Coefficients of the ramp placement for this step's length, uploaded when the length
+        changes (solver.py:348-368: omphi = 1 - phi, c_sl, c_rr per degree scaled by ttl, and the
+        degree-2 c_il, c_m, c_tsl, c_trr)."""
+        if not self.ramp:
+            return
+        h = float(dt) if dt else float(self.dt)
+        if getattr(self, "_ramp_dt", None) == h:
+            return
+        from .love import mode_arrays
+        from .rates import ramp_factor
+
+        if getattr(self, "_ramp_ma", None) is None:
+            self._ramp_ma = mode_arrays(self.love, self.norder)
+        ma = self._ramp_ma
+        s = ma["s"]
+        phi, omp = ramp_factor(s * (h / 1000.0))
+        omphi = np.where(s > 0, omp, 0.0)
+        c_sl = (ma["a_sl"] * omphi).sum(0)
+        c_rr = (ma["a_rr"] * omphi).sum(0)
+        n2 = int(self.love.nmod[2]) if self.norder >= 2 else 0
+        c2 = omphi[:n2, 2] if self.norder >= 2 else np.zeros(0)
+        c4 = [float(c2 @ ma["a_il"][:n2]), float(c2 @ ma["a_m"][:n2]), float(c2 @ ma["a_tsl"][:n2]),
+              float(c2 @ ma["a_trr"][:n2])]
+        ttl = np.asarray(self._earth_arrays["ttl"], float)
+        tab = np.ascontiguousarray(np.concatenate([omphi.ravel(), ttl * c_sl, ttl * c_rr, c4]), dtype=np.float64)
+        _lib.check(self._L.sle_solver_set_ramp(self._h, tab.ctypes.data), "sle_solver_set_ramp")
+        self._ramp_dt = h
+
     def _horizontal_setup(self):
         """Weights of the horizontal read-out (a_hl = l_k / s_k, ttl l^E; solver.py:424-434,
         697-700), uploaded once; off again when ``horizontal`` is cleared."""
@@ -389,6 +419,9 @@ class SeaLevelSolver:
     def step(self, icexy_cur, profile=False, dt=None, rates=False):
         h_rates = self._rates_setup(rates, dt)
         horiz = self._horizontal_setup()
+        if horiz and self.ramp:
+            raise NotImplementedError("the horizontal read-out is not provided together with ramp placement")
+        self._ramp_setup(dt)
         t0 = time.perf_counter()
         try:
             import torch

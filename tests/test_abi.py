@@ -50,6 +50,7 @@ def test_error_mapping():
     assert lib.sle_solver_get_rates(None, None, None, None, None) == _lib.SLE_ERR_BAD_ARG
     assert lib.sle_solver_set_horizontal(None, None) == _lib.SLE_ERR_BAD_ARG
     assert lib.sle_solver_get_horizontal(None, None, None, None) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_solver_set_ramp(None, None) == _lib.SLE_ERR_BAD_ARG
     assert lib.sle_topo_scratch_bytes() >= 16
     buf = (C.c_double * 2)()
     assert lib.sle_topo_residual(None, None, 0.0, None, None, None, None, 4, 8, 920.0, 1000.0, None, buf,
@@ -64,8 +65,6 @@ def test_solver_rejects_unprovided_options():
     love = SyntheticEarth(15, 2, 1)
     topo = np.full((16, 32), -1000.0)
     ice = np.zeros((16, 32))
-    with pytest.raises(NotImplementedError):
-        SeaLevelSolver(None, love, topo, ice, norder=15, ramp=True)
     with pytest.raises(NotImplementedError):
         SeaLevelSolver(None, love, topo, ice, norder=15, axial_rotation="deg2")
     with pytest.raises(NotImplementedError):
