@@ -31,6 +31,24 @@ def ramp_factor(x):
     return phi, omp
 
 
+def ramp_table(ma, love, lmax, ttl, dt):
+    """Host table of the ramp placement for steps of length ``dt`` years, in the layout
+    ``sle_solver_set_ramp`` takes: omphi = 1 - phi per mode and degree (K x (lmax+1), zero where a
+    degree has fewer modes), ttl c_sl and ttl c_rr per degree with c = sum_k a_k omphi_k, then the
+    degree-2 c_il, c_m, c_tsl, c_trr (solver.py:348-368).  ``ma`` is ``mode_arrays(love, lmax)``."""
+    s = ma["s"]
+    phi, omp = ramp_factor(s * (float(dt) / 1000.0))
+    omphi = np.where(s > 0, omp, 0.0)
+    c_sl = (ma["a_sl"] * omphi).sum(0)
+    c_rr = (ma["a_rr"] * omphi).sum(0)
+    n2 = int(love.nmod[2]) if lmax >= 2 else 0
+    c2 = omphi[:n2, 2] if lmax >= 2 else np.zeros(0)
+    c4 = [float(c2 @ ma["a_il"][:n2]), float(c2 @ ma["a_m"][:n2]), float(c2 @ ma["a_tsl"][:n2]),
+          float(c2 @ ma["a_trr"][:n2])]
+    ttl = np.asarray(ttl, dtype=np.float64)
+    return np.ascontiguousarray(np.concatenate([omphi.ravel(), ttl * c_sl, ttl * c_rr, c4]), dtype=np.float64)
+
+
 class RateTables:
     """Per-step-length weights of the read-out: w = a s / 1000 per mode and degree (per year),
     ws = sum_k w, wsphi = sum_k w phi_k (solver.py:293-294, 347-362), and 1 - phi at degree 2."""

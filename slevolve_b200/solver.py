@@ -321,22 +321,11 @@ class SeaLevelSolver:
         if getattr(self, "_ramp_dt", None) == h:
             return
         from .love import mode_arrays
-        from .rates import ramp_factor
+        from .rates import ramp_table
 
         if getattr(self, "_ramp_ma", None) is None:
             self._ramp_ma = mode_arrays(self.love, self.norder)
-        ma = self._ramp_ma
-        s = ma["s"]
-        phi, omp = ramp_factor(s * (h / 1000.0))
-        omphi = np.where(s > 0, omp, 0.0)
-        c_sl = (ma["a_sl"] * omphi).sum(0)
-        c_rr = (ma["a_rr"] * omphi).sum(0)
-        n2 = int(self.love.nmod[2]) if self.norder >= 2 else 0
-        c2 = omphi[:n2, 2] if self.norder >= 2 else np.zeros(0)
-        c4 = [float(c2 @ ma["a_il"][:n2]), float(c2 @ ma["a_m"][:n2]), float(c2 @ ma["a_tsl"][:n2]),
-              float(c2 @ ma["a_trr"][:n2])]
-        ttl = np.asarray(self._earth_arrays["ttl"], float)
-        tab = np.ascontiguousarray(np.concatenate([omphi.ravel(), ttl * c_sl, ttl * c_rr, c4]), dtype=np.float64)
+        tab = ramp_table(self._ramp_ma, self.love, self.norder, self._earth_arrays["ttl"], h)
         _lib.check(self._L.sle_solver_set_ramp(self._h, tab.ctypes.data), "sle_solver_set_ramp")
         self._ramp_dt = h
 

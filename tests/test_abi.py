@@ -150,3 +150,28 @@ def test_ramp_factor_series_and_limits():
     exact = np.where(x > 0, -np.expm1(-np.where(x > 0, x, 1.0)) / np.where(x > 0, x, 1.0), 1.0)
     assert np.allclose(phi, exact, rtol=1e-13, atol=0)
     assert np.allclose(phi + omp, 1.0, rtol=0, atol=2e-16)
+
+
+@pytest.mark.parametrize("dt", [1.0, 0.37, 2.5e-6, 500.0])
+def test_ramp_table_matches_oracle(dt):
+    """The host table of the GPU ramp placement against the oracle's coefficients (pinned to the
+    reference's ramp run): same values bit for bit, in the layout sle_solver_set_ramp reads."""
+    from oracle.memory import ModalState
+    from slevolve_b200 import SyntheticEarth, mode_arrays
+    from slevolve_b200.rates import ramp_table
+    from slevolve_b200.solver import Planet, degree_weights
+
+    lmax = 31
+    love = SyntheticEarth(lmax, 3, 5)
+    ma = mode_arrays(love, lmax)
+    ttl = degree_weights(love, lmax, Planet())[0]
+    tab = ramp_table(ma, love, lmax, ttl, dt)
+    st = ModalState(love, lmax, dt)
+    K, nl = int(ma["K"]), lmax + 1
+    assert tab.shape == (K * nl + 2 * nl + 4,)
+    om = tab[:K * nl].reshape(K, nl)
+    assert np.array_equal(om[:st.kmax], st.omphi) and not om[st.kmax:].any()
+    assert np.array_equal(tab[K * nl:K * nl + nl], ttl * st.c_sl)
+    assert np.array_equal(tab[K * nl + nl:K * nl + 2 * nl], ttl * st.c_rr)
+    assert np.array_equal(tab[-4:], [st.c_il, st.c_m, st.c_tsl, st.c_trr])
+    assert om.max() > 0.0
