@@ -127,6 +127,7 @@ class CudaSHT:
                 raise ValueError(f"grid shape {tuple(g.shape)} != {(self.nlat, self.nlon)}")
             res = out if out is not None else torch.empty((self.nm, self.nm), dtype=torch.complex128,
                                                         device=g.device)
+            self._check_device_out(res, (self.nm, self.nm), torch.complex128, torch)
             self.analysis_device([g], [res])
             return res
         a = np.ascontiguousarray(grid, dtype=np.float64)
@@ -146,8 +147,11 @@ class CudaSHT:
         torch = _torch()
         if isinstance(coeffs, torch.Tensor) and coeffs.is_cuda:
             c = coeffs.to(torch.complex128).contiguous()
+            if tuple(c.shape) != (self.nm, self.nm):
+                raise ValueError(f"coeffs shape {tuple(c.shape)} != {(self.nm, self.nm)}")
             res = out if out is not None else torch.empty((self.nlat, self.nlon), dtype=torch.float64,
                                                         device=c.device)
+            self._check_device_out(res, (self.nlat, self.nlon), torch.float64, torch)
             self.synthesis_device([c], [res])
             return res
         a = np.ascontiguousarray(coeffs, dtype=np.complex128)
@@ -161,6 +165,12 @@ class CudaSHT:
             return self._grid_out
         out[...] = self._grid_out
         return out
+
+    @staticmethod
+    def _check_device_out(t, shape, dtype, torch):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dtype and tuple(t.shape) == shape
+                and t.is_contiguous()):
+            raise ValueError(f"out must be a contiguous CUDA {dtype} tensor of shape {shape}")
 
     def mean00_weights(self):
         """Row weights with ``analysis(g)[0, 0].real == mean00_weights() @ g.sum(axis=1)`` up to

@@ -118,6 +118,13 @@ def test_batched_and_device_paths():
     for g, b in zip(grids, back):
         single = s.synthesis(s.analysis(g)).cpu().numpy()
         assert np.array_equal(b.cpu().numpy(), single)
+    # device tensors of the wrong shape or type are refused on the host, before any launch
+    with pytest.raises(ValueError, match="coeffs shape"):
+        s.synthesis(torch.zeros((L, L), dtype=torch.complex128, device="cuda"))
+    with pytest.raises(ValueError, match="out must be"):
+        s.synthesis(outs[0], out=torch.empty((n, n), dtype=torch.float64, device="cuda"))
+    with pytest.raises(ValueError, match="out must be"):
+        s.analysis(grids[0], out=torch.empty((L + 1, L + 1), dtype=torch.complex64, device="cuda"))
 
 
 def test_work_fraction_reported():
