@@ -230,6 +230,8 @@ class SolverBatch:
             import torch
 
             for slot, x in ices.items():
+                if tuple(x.shape) != (self.nlat, self.nlon):
+                    raise ValueError(f"ice shape {tuple(x.shape)} != {(self.nlat, self.nlon)}")
                 keep[slot] = x.to(torch.float64).contiguous()
             torch.cuda.current_stream().synchronize()
             ptrs = {slot: t.data_ptr() for slot, t in keep.items()}
@@ -250,6 +252,7 @@ class SolverBatch:
         code = FIELDS[field]
         if out is None:
             out = np.empty((self.nlat, self.nlon))
+        _check_grid_out(out, self.nlat, self.nlon)
         if _is_cuda_tensor(out):
             _lib.check(self._L.sle_batch_get(self._h, int(slot), code, C.c_void_p(out.data_ptr()), 1),
                        "sle_batch_get")
@@ -262,6 +265,20 @@ class SolverBatch:
         s = C.c_void_p()
         _lib.check(self._L.sle_batch_stream(self._h, C.byref(s)), "sle_batch_stream")
         return s.value
+
+
+def _check_grid_out(out, nlat, nlon):
+    """``out`` of ``get``: a C-contiguous float64 (nlat, nlon) NumPy array or CUDA tensor (the
+    library writes nlat * nlon doubles through its pointer)."""
+    shape = tuple(out.shape)
+    if _is_cuda_tensor(out):
+        import torch
+
+        ok = out.dtype == torch.float64 and out.is_contiguous()
+    else:
+        ok = isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+    if not ok or shape != (nlat, nlon):
+        raise ValueError(f"out must be a C-contiguous float64 grid of shape {(nlat, nlon)}")
 
 
 def _info_dict(info):

@@ -175,3 +175,15 @@ def test_ramp_table_matches_oracle(dt):
     assert np.array_equal(tab[K * nl + nl:K * nl + 2 * nl], ttl * st.c_rr)
     assert np.array_equal(tab[-4:], [st.c_il, st.c_m, st.c_tsl, st.c_trr])
     assert om.max() > 0.0
+
+
+def test_batch_get_out_checks():
+    """``SolverBatch.get(out=...)``: the library writes nlat * nlon doubles through the pointer, so
+    anything but a C-contiguous float64 grid of that shape is refused on the host."""
+    from slevolve_b200.batch import _check_grid_out
+
+    _check_grid_out(np.empty((16, 32)), 16, 32)
+    for bad in (np.empty((16, 16)), np.empty((16, 32), np.float32), np.empty((32, 16)).T,
+                np.empty((16, 64))[:, ::2]):
+        with pytest.raises(ValueError, match="out must be"):
+            _check_grid_out(bad, 16, 32)
