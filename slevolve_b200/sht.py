@@ -100,9 +100,26 @@ class CudaSHT:
         return int(nseg * self.nh * 16 + self.ncoef * 16)
 
     # ------------------------------------------------------------- device paths
+    def _check_device_args(self, grids, coeffs, layout, torch):
+        """Equal counts, and every tensor a contiguous CUDA tensor holding what the library reads or
+        writes through its pointer: nlat * nlon float64 per grid, (lmax+1)^2 (dense) or the packed
+        count of complex128 per spectrum."""
+        if len(grids) != len(coeffs):
+            raise ValueError(f"{len(grids)} grids but {len(coeffs)} spectra")
+        ncoef = self.nm * self.nm if layout == _lib.LAYOUT_DENSE else self.ncoef
+        for g in grids:
+            if not (isinstance(g, torch.Tensor) and g.is_cuda and g.dtype == torch.float64 and g.is_contiguous()
+                    and g.numel() == self.nlat * self.nlon):
+                raise ValueError(f"grids must be contiguous CUDA float64 tensors of {self.nlat} x {self.nlon}")
+        for c in coeffs:
+            if not (isinstance(c, torch.Tensor) and c.is_cuda and c.dtype == torch.complex128
+                    and c.is_contiguous() and c.numel() == ncoef):
+                raise ValueError(f"spectra must be contiguous CUDA complex128 tensors of {ncoef} values")
+
     def analysis_device(self, grids, coeffs, layout=_lib.LAYOUT_DENSE):
         """Analyse up to four CUDA float64 grids into CUDA complex128 tensors (in place)."""
         torch = _torch()
+        self._check_device_args(grids, coeffs, layout, torch)
         n = len(grids)
         gp = (C.c_void_p * n)(*[g.data_ptr() for g in grids])
         cp = (C.c_void_p * n)(*[c.data_ptr() for c in coeffs])
@@ -110,7 +127,9 @@ class CudaSHT:
                    "sle_sht_analysis")
 
     def synthesis_device(self, coeffs, grids, layout=_lib.LAYOUT_DENSE):
+        """Synthesise up to four CUDA complex128 spectra into CUDA float64 grids (in place)."""
         torch = _torch()
+        self._check_device_args(grids, coeffs, layout, torch)
         n = len(grids)
         cp = (C.c_void_p * n)(*[c.data_ptr() for c in coeffs])
         gp = (C.c_void_p * n)(*[g.data_ptr() for g in grids])
