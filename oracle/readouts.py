@@ -7,7 +7,7 @@ python/slevolve/solver.py), on the oracle's ``ModalState`` and step.
 * ``rate_spectra``       solver.py:454-474, 766-785 (modal read before the commit)
 * ``rotation_rate``      solver.py:476-484, 722-764
 * ``rate_grids``         solver.py:788-806
-* ``horizontal_psi``     solver.py:424-448, 687-720
+* ``horizontal_psi``     solver.py:424-448, 687-720 (ramp terms 706-715)
 """
 
 from __future__ import annotations
@@ -111,8 +111,11 @@ def rate_grids(sht, dsl, drr, dice00, dt, cxy, beta, p):
     return {"dSLdt": g, "dRdt": gr, "dSLdt_lm": dsl, "dRdt_lm": drr}
 
 
-def horizontal_psi(st, love, p, ttl, dI, dS_prev, load_inc, rot_tot, tpw):
-    """Psi_lm of the horizontal displacement, U convention."""
+def horizontal_psi(st, love, p, ttl, dI, dS_prev, load_inc, rot_tot, tpw, ramp_inc=None):
+    """Psi_lm of the horizontal displacement, U convention.  With the ramp placement
+    (``ramp_inc`` = rho_i dI*_step + rho_w load_inc) the same-step viscous weights
+    c_hl = sum_k a_hl (1 - phi_k) and the degree-2 tidal c_thl = sum_k a_thl (1 - phi_k) add
+    their terms (solver.py:706-715)."""
     nl = st.lmax + 1
     a_hl = np.zeros((st.kmax, nl))
     a_thl = np.zeros(st.kmax)
@@ -133,7 +136,14 @@ def horizontal_psi(st, love, p, ttl, dI, dS_prev, load_inc, rot_tot, tpw):
     A = p.rhoi * dI + p.rhow * dS_prev
     A += p.rhow * load_inc
     hz = ttlle * A + ttl * visc_h
+    if ramp_inc is not None:
+        c_hl = (a_hl * st.omphi).sum(0)
+        hz += (ttl[:, 0] * c_hl)[:, None] * ramp_inc
     hz[0, :] = 0.0
     if tpw and rot_tot is not None and st.lmax >= 2:
+        if ramp_inc is not None:
+            n2 = st.nmod2
+            c_thl = float(st.omphi[:n2, 2] @ a_thl[:n2])
+            thl = thl + c_thl * (rot_tot - st.p_lambda)
         hz[2, 0:3] += (love.lTE[2] * rot_tot + thl) / p.gacc
     return hz

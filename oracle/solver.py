@@ -365,8 +365,11 @@ class OracleSolver:
         if getattr(self, "horizontal", False):
             from .readouts import horizontal_psi
 
+            ramp_inc = None
+            if self.ramp:
+                ramp_inc = p.rhoi * dice + p.rhow * load_inc
             hz = horizontal_psi(st, self.love, p, self.ttl, dI, dS_prev, load_inc,
-                                dlam_prev2 + dlam_cur2 if self.tpw else None, self.tpw)
+                                dlam_prev2 + dlam_cur2 if self.tpw else None, self.tpw, ramp_inc=ramp_inc)
         if self.tpw:
             st.commit(cur, dil_cur, dm_cur, dlam_cur2)
         else:

@@ -200,6 +200,35 @@ def test_horizontal_readout_against_reference():
     assert numiter == list(fx["numiter"])
 
 
+def test_horizontal_readout_under_ramp_against_reference():
+    """The oracle's horizontal potential with the ramp placement (its same-step c_hl and tidal
+    c_thl terms) against the reference's own run (golden: make_golden_horiz_ramp.py, the PREM
+    Love arrays of horiz.npz): 1e-9 of the largest coefficient, identical iteration counts.  The
+    run without the ramp terms misses by far more than that."""
+    from slevolve_b200.synthetic import case_c0
+    fx = load_golden("horiz_ramp.npz")
+    love = FixtureLove(load_golden("horiz.npz"))
+    sht = OracleSHT(64, 128, 63)
+    case = case_c0(sht, nsteps=len(fx["dts"]) + 8)
+    runs = {}
+    for ramp in (True, False):
+        slv = OracleSolver(sht, love, case.topo, case.ice(0), norder=63, dt=1.0, ramp=ramp)
+        slv.horizontal = True
+        numiter, psi = [], {}
+        for k, dt in enumerate(fx["dts"], start=1):
+            r = slv.step(case.ice(k), dt=float(dt))
+            numiter.append(r["numiter"])
+            if f"horiz_{k}" in fx:
+                psi[k] = r["horiz"].copy()
+        runs[ramp] = (numiter, psi)
+    numiter, psi = runs[True]
+    assert numiter == list(fx["numiter"])
+    for k, got in psi.items():
+        ref = fx[f"horiz_{k}"]
+        assert np.abs(got - ref).max() <= 1e-9 * np.abs(ref).max(), k
+        assert np.abs(runs[False][1][k] - ref).max() > 1e-6 * np.abs(ref).max(), k
+
+
 def test_ramp_placement_against_reference():
     """The oracle with the second-order load placement (ramp=True) against the reference's own
     run (golden: make_golden_ramp.py): 1e-9 m, identical iteration counts, rotational totals and,
