@@ -11,9 +11,9 @@ reference copies them for that reason).
 
 Branches of the reference that this build does not provide raise ``NotImplementedError``: the
 axial-rotation options, Anderson mixing, the reuse variants other than ``"warm"``, analytic rates
-of a mixed-precision solve and the horizontal read-out together with ramp placement.  Provided:
-``ramp=True`` (second-order load placement), ``step(..., rates=True)`` and
-``solver.horizontal = True``.  The ``raw`` option needs a raw-mode backend and raises
+of a mixed-precision solve, ramp placement of a mixed-precision solve and the horizontal read-out
+together with ramp placement.  Provided: ``ramp=True`` (second-order load placement, FP64),
+``step(..., rates=True)`` and ``solver.horizontal = True``.  The ``raw`` option needs a raw-mode backend and raises
 ``ValueError`` as in the reference (solver_opt.py:299-301).
 """
 
@@ -138,6 +138,8 @@ class SeaLevelSolver:
         inner = self._inner_default if inner is None else inner
         if axial_rotation != "off":
             raise NotImplementedError("axial_rotation options are not provided by the GPU solver")
+        if ramp and prec != _lib.PREC_FP64:
+            raise NotImplementedError("ramp placement is provided for precision='fp64' solves")
         if inner not in ("off", "extrap", "anderson"):
             raise ValueError(f"inner must be one of ('off', 'extrap', 'anderson'), got {inner!r}")
         if inner == "anderson":

@@ -187,3 +187,14 @@ def test_batch_get_out_checks():
                 np.empty((16, 64))[:, ::2]):
         with pytest.raises(ValueError, match="out must be"):
             _check_grid_out(bad, 16, 32)
+
+
+def test_ramp_refused_for_mixed_precision():
+    """Ramp placement is provided for FP64 solves; a mixed-precision one is refused before any
+    device call."""
+    from slevolve_b200 import SeaLevelSolver, SyntheticEarth
+
+    love = SyntheticEarth(15, 2, 1)
+    with pytest.raises(NotImplementedError, match="ramp"):
+        SeaLevelSolver(None, love, np.full((16, 32), -1000.0), np.zeros((16, 32)), norder=15, ramp=True,
+                       precision="mixed")
