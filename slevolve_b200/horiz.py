@@ -20,7 +20,8 @@ so that, with A_lm = l U_lm, B_{l-1,m} = e_lm U_lm and C_lm = i m U_lm,
     u_theta = (cos theta  synth(A) - synth(B)) / sin theta,   u_phi = synth(C) / sin theta.
 
 The coefficient arrays are formed on the host (O(L^2)), the three transforms run on the GPU and
-the row combine runs on the device before the two grids come back.
+the row combine runs on the device before the two grids come back.  One transform plan per
+(nlat, nlon, lmax) is kept for the calls that follow; ``release_plans()`` frees them.
 """
 
 from __future__ import annotations
@@ -67,6 +68,11 @@ def _sht(nlat, nlon, lmax):
     return sh
 
 
+def release_plans():
+    """Drop the cached transform plans (their device tables are freed with them)."""
+    _SHT_CACHE.clear()
+
+
 def gradient(U, nlat: int, nlon: int, nthreads: int = 1):
     """(u_theta, u_phi) as float64 NumPy arrays (nlat, nlon) from Psi coefficients U[l, m]
     (lmax <= nlat - 1 and lmax <= (nlon - 1) // 2, as the reference requires).  ``nthreads`` is
@@ -94,4 +100,4 @@ def _gradient_with(sh, U, dev):
     return ut.cpu().numpy(), up.cpu().numpy()
 
 
-__all__ = ["gradient", "gradient_coeffs", "combine_rows"]
+__all__ = ["gradient", "gradient_coeffs", "combine_rows", "release_plans"]
