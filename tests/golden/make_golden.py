@@ -107,7 +107,8 @@ def synthetic512_ice(gaulats, topo, nlon):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("SLEVOLVE_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", required=True,
+                    help="SLEvolve checkout whose python/slevolve package is imported read-only")
     ap.add_argument("--skip512", action="store_true", help="skip the L=511 oracle run")
     a = ap.parse_args()
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")

@@ -26,7 +26,8 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("SLEVOLVE_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", required=True,
+                    help="SLEvolve checkout whose python/slevolve package is imported read-only")
     a = ap.parse_args()
     sys.dont_write_bytecode = True
     sys.path.insert(0, REPO)

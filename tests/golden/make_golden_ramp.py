@@ -25,7 +25,8 @@ RATES_FROM = 7
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("SLEVOLVE_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", required=True,
+                    help="SLEvolve checkout whose python/slevolve package is imported read-only")
     a = ap.parse_args()
     sys.dont_write_bytecode = True
     sys.path.insert(0, REPO)

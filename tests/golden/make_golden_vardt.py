@@ -43,7 +43,8 @@ def run(cls, sht, case, L, **kw):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("SLEVOLVE_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", required=True,
+                    help="SLEvolve checkout whose python/slevolve package is imported read-only")
     a = ap.parse_args()
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache_golden")
     sys.dont_write_bytecode = True

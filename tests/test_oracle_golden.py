@@ -253,3 +253,31 @@ def test_ramp_placement_against_reference():
                 ref = fx[f"rates_{key}"]
                 assert np.abs(np.asarray(r["rates"][key]) - ref).max() <= 1e-8 * np.abs(ref).max(), key
     assert numiter == list(fx["numiter"])
+
+
+def test_c1_full_size_oracle_first_steps():
+    """The oracle on c1 at its benchmark size (256 x 512, L = 255) against the reference's 550-step
+    run (make_golden_c1.py): its inputs, step-0 areas and the first three steps (iteration counts,
+    degree-0 diagnostics, the full topography and masks of step 1); the GPU test covers all 550."""
+    from slevolve_b200.synthetic import case_c1
+
+    fx = load_golden("step_c1.npz")
+    osht = OracleSHT(256, 512, 255, workers=os.cpu_count() or 1)
+    case = case_c1(osht, nsteps=550)
+    assert np.array_equal(np.round(case.topo * 1000.0).astype(np.int64), fx["topo_mm"])
+    orc = OracleSolver(osht, case.love, case.topo, case.ice(0), norder=255, dt=1.0)
+    a0, b0, v0 = fx["step0_scalars"]
+    assert abs(orc.ocean_area0 - a0) <= 1e-9 * abs(a0)
+    assert abs(orc.ice_volume0 - v0) <= 1e-9 * abs(v0)
+    for k in (1, 2, 3):
+        ice = case.ice(k)
+        assert float(np.abs(ice).sum()) == fx["ice_abs_sum"][k - 1]
+        r = orc.step(ice)
+        assert r["numiter"] == fx["numiter"][k - 1], k
+        for key in ("gmslc_ocn", "ocean_area", "ice_volume"):
+            assert abs(r[key] - fx[key][k - 1]) <= 1e-9 * max(1.0, abs(fx[key][k - 1])), (k, key)
+        if k == 1:
+            assert np.abs(r["tgrid"] - fx["tgrid_1"]).max() <= TOL_M
+            shape = r["ocean"].shape
+            ocean = np.unpackbits(fx["ocean_1"])[: shape[0] * shape[1]].reshape(shape) != 0
+            assert np.array_equal(np.asarray(r["ocean"]) != 0, ocean)
