@@ -86,7 +86,8 @@ int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* coeffs_dev,
  * latitudes and lmax 511, else SLE_ERR_BAD_SHAPE.  The first call on a device looks up the
  * array's device address and should come before any stream capture.  All calls share the one
  * array: calls that overlap on the GPU (other streams, other threads) race and must be ordered
- * by the caller. */
+ * by the caller.  The arithmetic is always FP64, whatever sle_sht_set_precision selected on the
+ * plan (a mixed-precision plan gives the FP64 result here). */
 int sle_sht_analysis_noalloc(sle_sht* plan, const double* grid_dev, void* coeffs_packed_dev,
                              void* stream);
 /* Select the arithmetic of sle_sht_analysis / sle_sht_synthesis on this plan (default FP64).
@@ -205,6 +206,19 @@ int sle_solver_get_horizontal(sle_solver* s, void* psi, double* r_lam, double* l
 int sle_solver_set_reuse(sle_solver* s, void* ds_store, void* mask_store, int capacity, int valid);
 /* the solver's own CUDA stream (as void*) */
 int sle_solver_stream(sle_solver* s, void** stream);
+/* Snapshot / restore of the solve's whole state as a host byte image (checkpoint, preemption,
+ * migration between solvers or batch slots).  Replaces the reference's modal-state checkpoint
+ * (fortran/src/modal_state_mod.f90:445-477: shapes, decay, loads and modal states to a stream
+ * file) and the Python solver's swappable `state` object (tests/test_small_case.py:106); the image
+ * is this library's own format: header (magic "SLES", configuration, step count, step lengths),
+ * then every per-solve device buffer.  A restored solve continues bit for bit as the original
+ * would have.  The image restores into any solver or batch slot of the same grid, lmax, mode
+ * capacity, precision and option flags (else SLE_ERR_BAD_SHAPE); a reuse store and the read-out
+ * tables (rates, horizontal, ramp) are not part of it and are set again by the caller.
+ * _bytes gives the image size; dst / src are host buffers of at least that many bytes. */
+int sle_solver_snapshot_bytes(const sle_solver* s, long long* nbytes);
+int sle_solver_snapshot(sle_solver* s, void* dst, long long nbytes);
+int sle_solver_restore(sle_solver* s, const void* src, long long nbytes);
 
 /* ------------------------------------------------------------- batches
  * A batch holds nslots independent solves ("slots") of one grid size and configuration (the
@@ -241,6 +255,11 @@ int sle_batch_step(sle_batch* b, const double* const* ice, int on_device, const 
  * on this batch is allowed (they return SLE_ERR_STATE).  No counterpart in the reference. */
 int sle_batch_step_begin(sle_batch* b, const double* const* ice, int on_device, const double* dt_years);
 int sle_batch_step_end(sle_batch* b, sle_step_info* info);
+/* snapshot / restore of one slot, as sle_solver_snapshot / sle_solver_restore (an image of one
+ * slot restores into any slot of a batch of the same configuration, or into a solver) */
+int sle_batch_snapshot_bytes(const sle_batch* b, long long* nbytes);
+int sle_batch_snapshot(sle_batch* b, int slot, void* dst, long long nbytes);
+int sle_batch_restore(sle_batch* b, int slot, const void* src, long long nbytes);
 /* copy one output of a slot's last step (as sle_solver_get) */
 int sle_batch_get(sle_batch* b, int slot, int field, void* dst, int dst_on_device);
 int sle_batch_stream(sle_batch* b, void** stream);

@@ -1080,7 +1080,8 @@ extern "C" int sle_sht_unpack(sle_sht* plan, const void* packed_dev, void* dense
 // of memory from cudaMalloc.  The call launches the same two kernels as sle_sht_analysis; the
 // first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
 // device current.  No element of the scratch needs clearing: every element the second kernel
-// reads is written earlier in the same call by the first.
+// reads is written earlier in the same call by the first.  The FP64 kernels run whatever the
+// plan's precision setting is.
 extern "C" int sle_sht_analysis_noalloc(sle_sht* plan, const double* grid_dev, void* coeffs_packed_dev,
                                         void* stream) {
   if (!plan) {

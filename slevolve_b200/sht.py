@@ -5,6 +5,10 @@ transform interface (SLEvolve ``python/slevolve/sht.py:43-46``, ``sht_ducc.py:20
     ``analysis(grid[nlat, nlon] float64, out=None) -> coeffs[lmax+1, lmax+1] complex128``
     ``synthesis(coeffs, out=None) -> grid``
 
+``raw=True`` is the sign-free convention of the reference's ducc backend (sht_ducc.py:101-110):
+``analysis`` returns V[l, m] = (-1)^m U[l, m] and ``synthesis`` reads V.  The ``*_device`` entry
+points always use U.
+
 ``precision="mixed"`` runs the Legendre contractions as split-TF32 tensor-core GEMMs with FP32
 accumulation (FP64 recurrence, row FFTs and degree-0 coefficient); the default ``"fp64"`` matches
 the reference to round-off.
@@ -46,8 +50,6 @@ class CudaSHT:
 
     def __init__(self, nlat: int, nlon: int, lmax: int, workers: int = 1, chunk: int = 16,
                  raw: bool = False, precision: str = "fp64"):
-        if raw:
-            raise ValueError("raw (sign-free) mode is only implemented for the ducc backend")
         if nlat % 2 != 0:
             raise ValueError("nlat must be even")
         if lmax > nlon // 2:
@@ -63,7 +65,7 @@ class CudaSHT:
         self.nlat, self.nlon, self.lmax = int(nlat), int(nlon), int(lmax)
         self.nm = self.lmax + 1
         self.nh = self.nlat // 2
-        self.raw = False
+        self.raw = bool(raw)
         self.workers = int(workers)
         self.nthreads = int(workers)
         nc = C.c_longlong()
@@ -76,7 +78,8 @@ class CudaSHT:
         frac = C.c_double()
         _lib.check(L.sle_sht_work_fraction(h, C.byref(frac)), "sle_sht_work_fraction")
         self.work_fraction = float(frac.value)
-        dev = torch.device("cuda")
+        self.device_index = torch.cuda.current_device()
+        dev = torch.device("cuda", self.device_index)
         self._grid_d = torch.empty((self.nlat, self.nlon), dtype=torch.float64, device=dev)
         self._coef_d = torch.empty((self.nm, self.nm), dtype=torch.complex128, device=dev)
         self._grid_h = torch.empty((self.nlat, self.nlon), dtype=torch.float64).pin_memory()
@@ -101,9 +104,9 @@ class CudaSHT:
 
     # ------------------------------------------------------------- device paths
     def _check_device_args(self, grids, coeffs, layout, torch):
-        """Equal counts, and every tensor a contiguous CUDA tensor holding what the library reads or
-        writes through its pointer: nlat * nlon float64 per grid, (lmax+1)^2 (dense) or the packed
-        count of complex128 per spectrum."""
+        """Equal counts, and every tensor a contiguous CUDA tensor on the plan's device holding what
+        the library reads or writes through its pointer: nlat * nlon float64 per grid, (lmax+1)^2
+        (dense) or the packed count of complex128 per spectrum."""
         if len(grids) != len(coeffs):
             raise ValueError(f"{len(grids)} grids but {len(coeffs)} spectra")
         ncoef = self.nm * self.nm if layout == _lib.LAYOUT_DENSE else self.ncoef
@@ -111,10 +114,19 @@ class CudaSHT:
             if not (isinstance(g, torch.Tensor) and g.is_cuda and g.dtype == torch.float64 and g.is_contiguous()
                     and g.numel() == self.nlat * self.nlon):
                 raise ValueError(f"grids must be contiguous CUDA float64 tensors of {self.nlat} x {self.nlon}")
+            self._check_on_device(g)
         for c in coeffs:
             if not (isinstance(c, torch.Tensor) and c.is_cuda and c.dtype == torch.complex128
                     and c.is_contiguous() and c.numel() == ncoef):
                 raise ValueError(f"spectra must be contiguous CUDA complex128 tensors of {ncoef} values")
+            self._check_on_device(c)
+
+    def _check_on_device(self, t):
+        """The library dereferences the tensor's pointer on the plan's device: a tensor on another
+        GPU is refused rather than read through a foreign address."""
+        if t.device.index != self.device_index:
+            raise ValueError(f"tensor on cuda:{t.device.index}, but this transform plan lives on "
+                             f"cuda:{self.device_index}")
 
     def analysis_device(self, grids, coeffs, layout=_lib.LAYOUT_DENSE):
         """Analyse up to four CUDA float64 grids into CUDA complex128 tensors (in place)."""
@@ -148,6 +160,8 @@ class CudaSHT:
                                                         device=g.device)
             self._check_device_out(res, (self.nm, self.nm), torch.complex128, torch)
             self.analysis_device([g], [res])
+            if self.raw:
+                res[:, 1::2].neg_()
             return res
         a = np.ascontiguousarray(grid, dtype=np.float64)
         if a.shape != (self.nlat, self.nlon):
@@ -155,6 +169,8 @@ class CudaSHT:
         self._grid_h.numpy()[...] = a
         self._grid_d.copy_(self._grid_h, non_blocking=True)
         self.analysis_device([self._grid_d], [self._coef_d])
+        if self.raw:
+            self._coef_d[:, 1::2].neg_()
         self._coef_h.copy_(self._coef_d)
         if out is None:
             return self._coef_out
@@ -168,6 +184,9 @@ class CudaSHT:
             c = coeffs.to(torch.complex128).contiguous()
             if tuple(c.shape) != (self.nm, self.nm):
                 raise ValueError(f"coeffs shape {tuple(c.shape)} != {(self.nm, self.nm)}")
+            if self.raw:
+                c = c.clone()
+                c[:, 1::2].neg_()
             res = out if out is not None else torch.empty((self.nlat, self.nlon), dtype=torch.float64,
                                                         device=c.device)
             self._check_device_out(res, (self.nlat, self.nlon), torch.float64, torch)
@@ -178,6 +197,8 @@ class CudaSHT:
             raise ValueError(f"coeffs shape {a.shape} != {(self.nm, self.nm)}")
         self._coef_h.numpy()[...] = a
         self._coef_d.copy_(self._coef_h, non_blocking=True)
+        if self.raw:
+            self._coef_d[:, 1::2].neg_()
         self.synthesis_device([self._coef_d], [self._grid_d])
         self._grid_h.copy_(self._grid_d)
         if out is None:
@@ -185,11 +206,11 @@ class CudaSHT:
         out[...] = self._grid_out
         return out
 
-    @staticmethod
-    def _check_device_out(t, shape, dtype, torch):
+    def _check_device_out(self, t, shape, dtype, torch):
         if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dtype and tuple(t.shape) == shape
                 and t.is_contiguous()):
             raise ValueError(f"out must be a contiguous CUDA {dtype} tensor of shape {shape}")
+        self._check_on_device(t)
 
     def mean00_weights(self):
         """Row weights with ``analysis(g)[0, 0].real == mean00_weights() @ g.sum(axis=1)`` up to

@@ -13,8 +13,10 @@ Branches of the reference that this build does not provide raise ``NotImplemente
 axial-rotation options, Anderson mixing, the reuse variants other than ``"warm"``, analytic rates
 of a mixed-precision solve, ramp placement of a mixed-precision solve and the horizontal read-out
 together with ramp placement.  Provided: ``ramp=True`` (second-order load placement, FP64),
-``step(..., rates=True)`` and ``solver.horizontal = True``.  The ``raw`` option needs a raw-mode backend and raises
-``ValueError`` as in the reference (solver_opt.py:299-301).
+``step(..., rates=True)`` and ``solver.horizontal = True``.  The ``raw`` option needs a raw-mode
+backend (``make_sht("cuda", ..., raw=True)``) and raises ``ValueError`` otherwise, as in the reference
+(solver_opt.py:299-301); with it, the spectra the step hands out (``dS_converged``, ``load_inc``,
+``horiz``) are in the sign-free convention V[l, m] = (-1)^m U[l, m] of that backend.
 """
 
 from __future__ import annotations
@@ -107,6 +109,8 @@ class _StepResult(dict):
             v = self._solver._fetch(key, self._GRIDS[key])
         elif key in self._SPECS:
             v = self._solver._fetch(key, self._SPECS[key], spectral=True)
+            if self._solver._raw:
+                v[:, 1::2] *= -1.0
         else:
             raise KeyError(key)
         self[key] = v
@@ -151,8 +155,11 @@ class SeaLevelSolver:
         unknown = opt - {"raw", "diag", "dsl", "numba", "sums"}
         if unknown:
             raise ValueError(f"unknown opt {sorted(unknown)}")
-        if "raw" in opt:
+        raw_backend = bool(getattr(sht, "raw", False))
+        if ("raw" in opt) != raw_backend:
             raise ValueError("--opt raw must be used with a raw-mode SHT backend")
+        # spectra handed out are in the backend's convention: V[l, m] = (-1)^m U[l, m] in raw mode
+        self._raw = raw_backend
         topo0 = np.ascontiguousarray(topo0, dtype=np.float64)
         nlat, nlon = topo0.shape
         norder = int(norder)
@@ -255,9 +262,63 @@ class SeaLevelSolver:
         _lib.check(self._L.sle_solver_stream(self._h, C.byref(s)), "sle_solver_stream")
         return s.value
 
+    # ------------------------------------------------------------ snapshots
+    _SNAP_KEYS = ("iter", "dt", "gr_counts", "reuse_stats", "inner_stats")
+
+    def snapshot(self):
+        """The solve's state after its last step, on the host: ``{"image": uint8 array, ...}``
+        with the device image (modal state, load history, topography, masks, rotational state,
+        step lengths; ``sle_solver_snapshot``) and the solver's own counters.  The dict can be
+        saved with ``numpy.savez``.  The counterpart of the reference's modal-state checkpoint
+        (fortran/src/modal_state_mod.f90:445-477) and of swapping the Python solver's ``state``
+        object (tests/test_small_case.py:106)."""
+        n = C.c_longlong()
+        _lib.check(self._L.sle_solver_snapshot_bytes(self._h, C.byref(n)), "sle_solver_snapshot_bytes")
+        img = np.empty(int(n.value), dtype=np.uint8)
+        _lib.check(self._L.sle_solver_snapshot(self._h, C.c_void_p(img.ctypes.data), n.value),
+                   "sle_solver_snapshot")
+        snap = {"image": img, "ramp": self.ramp, "precision": self.precision,
+                "tinit_0": np.array(self.tinit_0, copy=True), "ocean_area0": self.ocean_area0,
+                "oceanBeta_area0": self.oceanBeta_area0, "ice_volume0": self.ice_volume0}
+        for k in self._SNAP_KEYS:
+            v = getattr(self, k)
+            snap[k] = dict(v) if isinstance(v, dict) else v
+        return snap
+
+    def restore(self, snap):
+        """Continue from ``snapshot()`` of this or another solver of the same grid, degree, mode
+        capacity, precision and options: the next ``step`` gives bit for bit what the
+        snapshotted solver's next step would have given."""
+        if bool(snap.get("ramp", False)) != self.ramp or snap.get("precision", self.precision) != self.precision:
+            raise ValueError("snapshot of a solve with other ramp or precision settings")
+        img = np.ascontiguousarray(snap["image"], dtype=np.uint8)
+        _lib.check(self._L.sle_solver_restore(self._h, C.c_void_p(img.ctypes.data), img.size),
+                   "sle_solver_restore")
+        for k in self._SNAP_KEYS:
+            if k in snap:
+                v = snap[k]
+                setattr(self, k, dict(v) if isinstance(v, dict) else v)
+        self.iter = int(self.iter)
+        self.dt = float(self.dt)
+        self._ramp_dt = None      # ramp table uploaded again for the next step's length
+        # step-0 attributes of the restored solve (run_ais.py:360-367 reads them)
+        if "tinit_0" in snap:
+            self.tinit_0 = self.tinit = np.array(snap["tinit_0"], copy=True)
+        for k in ("ocean_area0", "oceanBeta_area0", "ice_volume0"):
+            if k in snap:
+                setattr(self, k, float(snap[k]))
+        self.cxy0 = self._fetch("_ocean0", _lib.F_OCEAN0).copy()
+        self.beta0 = self._fetch("_beta0", _lib.F_BETA0).copy()
+        self.cstar0 = self.cxy0 * self.beta0
+
     def set_step_dt(self, dt):
+        """Length of the next steps (yr), as the reference's ``set_step_dt``; the device keeps the
+        previous length for a non-positive value, so zero and negative lengths are refused."""
         if dt is not None:
-            self.dt = float(dt)
+            dt = float(dt)
+            if not dt > 0.0:
+                raise ValueError(f"step length must be positive (got dt={dt!r})")
+            self.dt = dt
 
     # ------------------------------------------------------------------ step
     def _reuse_register(self, k):
@@ -278,8 +339,11 @@ class SeaLevelSolver:
         return st
 
     def step_device(self, ice_ptr, on_device, dt=None):
-        """One step from a raw pointer (host or device); returns the step info record."""
+        """One step from a raw pointer (host or device); returns the step info record.  The ramp
+        coefficients follow the step length here, so a ramp solve stepped through this call gets
+        the same placement as through ``step``."""
         self.set_step_dt(dt)
+        self._ramp_setup(self.dt)
         st = self._reuse_register(self.iter + 1) if self.reuse == "warm" else None
         rc = self._L.sle_solver_step(self._h, C.c_void_p(ice_ptr), int(on_device),
                                      float(self.dt), C.byref(self._info))
@@ -302,7 +366,7 @@ class SeaLevelSolver:
 
             if getattr(self, "_rate_tabs", None) is None:
                 self._rate_tabs = RateTables(self.love, self.norder)
-            h = float(dt) if dt else float(self.dt)
+            h = float(dt) if dt is not None else float(self.dt)
             tab = self._rate_tabs.for_dt(h)
             if getattr(self, "_rates_dt", None) != h:
                 _lib.check(self._L.sle_solver_set_rate_tables(self._h, tab.ctypes.data), "sle_solver_set_rate_tables")
@@ -319,7 +383,7 @@ class SeaLevelSolver:
         degree-2 c_il, c_m, c_tsl, c_trr)."""
         if not self.ramp:
             return
-        h = float(dt) if dt else float(self.dt)
+        h = float(dt) if dt is not None else float(self.dt)
         if getattr(self, "_ramp_dt", None) == h:
             return
         from .love import mode_arrays
@@ -374,6 +438,8 @@ class SeaLevelSolver:
             cur = lam12[6:].reshape(3, 2) @ np.array([1.0, 1j])
             rot = (self.love.lTE[2] * (prev + cur) + thl) / self.p.gacc
             hz[2, 0:3] += rot
+        if self._raw:
+            hz[:, 1::2] *= -1.0
         return hz
 
     def _rates_read(self, info, h):
@@ -408,11 +474,12 @@ class SeaLevelSolver:
         return out
 
     def step(self, icexy_cur, profile=False, dt=None, rates=False):
+        if dt is not None and not float(dt) > 0.0:
+            raise ValueError(f"step length must be positive (got dt={dt!r})")
         h_rates = self._rates_setup(rates, dt)
         horiz = self._horizontal_setup()
         if horiz and self.ramp:
             raise NotImplementedError("the horizontal read-out is not provided together with ramp placement")
-        self._ramp_setup(dt)
         t0 = time.perf_counter()
         try:
             import torch
