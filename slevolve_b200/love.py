@@ -14,98 +14,95 @@ import numpy as np
 NPAM = 500  # row capacity of the mode arrays (solver.py:39)
 
 
-class _Records:
-    """Fortran list-directed reads: every read starts a new record (line)."""
+# The Love-number text file (the format SLEvolve's Fortran and Python readers share): a header
+# line, then one block per degree l = 1, 2, ...  A block is a sequence of fields; a field starts on
+# a new line and runs over as many lines as its count of numbers needs (numbers past the count on
+# its last line are ignored, as Fortran list-directed input ignores them).  "K" stands for the
+# block's mode count, the second number of its first field.  Lines of five numbers hold
+# (h, l*l, -, -, l*k): the tangential (l) and potential (k) numbers are stored times the degree.
+BLOCK_FIELDS = (("head", 2), ("relax", "K"), ("elastic", 5), ("fluid", 5),
+                ("res_h", "K"), ("res_l", "K"), ("res_k", "K"))
+TIDAL_FIELDS = (("t_elastic", 5), ("t_fluid", 5), ("t_res_h", "K"), ("t_res_l", "K"), ("t_res_k", "K"))
 
-    def __init__(self, path):
-        with open(path, "r") as fh:
-            self.lines = fh.read().split("\n")
-        self.i = 0
 
-    def skip(self):
-        self.i += 1
+class _FieldCursor:
+    """Walks the lines of a Love-number file one field at a time."""
 
-    def take(self, n):
+    def __init__(self, text):
+        self._lines = text.splitlines()
+        self._at = 1   # the header line carries no numbers the solver uses
+
+    def field(self, count, where):
         vals = []
-        while len(vals) < n:
-            if self.i >= len(self.lines):
-                raise ValueError("Love-number file ended early")
-            vals.extend(self.lines[self.i].split())
-            self.i += 1
-        return vals[:n]
+        while len(vals) < count:
+            if self._at >= len(self._lines):
+                raise ValueError(f"Love-number file ends inside {where}")
+            vals += self._lines[self._at].split()
+            self._at += 1
+        return np.array(vals[:count], dtype=np.float64)
 
-    def floats(self, n):
-        return [float(v) for v in self.take(n)]
+
+def read_love_blocks(path, lmax):
+    """{degree: {field name: values}} of the first ``lmax`` degree blocks of a Love-number file."""
+    with open(path, "r") as fh:
+        cur = _FieldCursor(fh.read())
+    blocks = {}
+    for _ in range(int(lmax)):
+        blk = {}
+        for name, count in BLOCK_FIELDS + TIDAL_FIELDS:
+            if name.startswith("t_") and blk["degree"] < 2:
+                break   # degree 1 has no tidal numbers
+            n = blk["K"] if count == "K" else count
+            v = cur.field(n, f"field {name!r} of block {len(blocks) + 1}")
+            if name == "head":
+                blk["degree"], blk["K"] = int(v[0]), int(v[1])
+                if not 1 <= blk["degree"] <= lmax:
+                    raise ValueError(f"degree {blk['degree']} outside 1..{lmax} in the Love-number file")
+            else:
+                blk[name] = v
+        blocks[blk["degree"]] = blk
+    return blocks
 
 
 class LoveNumbers:
-    """Reader for the SLEvolve Love-number text file (format of solver.py:150-186).
+    """Earth model read from a Love-number text file, truncated at degree ``norder``, with the
+    attributes of the reference's reader (SLEvolve python/slevolve/solver.py:114-225): elastic
+    ``he, ke, le`` and tidal ``hTE, kTE, lTE`` per degree (k and l divided by the degree), mode
+    count ``nmod``, inverse relaxation times ``s[k, l]`` (1/kyr) and residues ``r`` (h),
+    ``rprime`` (k), ``rl`` (l) with their tidal counterparts ``rT, rprimeT, rlT`` (k and l
+    residues divided by the degree)."""
 
-    Per degree block: ``l nmodes``; nmodes inverse relaxation times; elastic line
-    (h, l*l, ., ., l*k); fluid line; nmodes h, l*l, l*k residues; for l >= 2 the same five
-    records for the tidal numbers.  k and l values are stored multiplied by the degree.
-    """
+    # attribute <- (field, position in its five-number line); residue attribute <- field
+    _ELASTIC = {"he": ("elastic", 0), "le": ("elastic", 1), "ke": ("elastic", 4),
+                "hTE": ("t_elastic", 0), "lTE": ("t_elastic", 1), "kTE": ("t_elastic", 4)}
+    _RESIDUES = {"r": "res_h", "rl": "res_l", "rprime": "res_k",
+                 "rT": "t_res_h", "rlT": "t_res_l", "rprimeT": "t_res_k"}
+    _PER_DEGREE = ("le", "ke", "lTE", "kTE", "rl", "rprime", "rlT", "rprimeT")   # stored times l
 
     def __init__(self, path, norder):
         self.norder = int(norder)
         nl = self.norder + 1
-        rd = _Records(path)
-        rd.skip()
-        nmod = np.zeros(nl, dtype=np.int64)
-        s = np.zeros((NPAM, nl))
-        el = np.zeros((3, nl))
-        fl = np.zeros((3, nl))
-        tel = np.zeros((3, nl))
-        tfl = np.zeros((3, nl))
-        rh, rl, rk = (np.zeros((NPAM, nl)) for _ in range(3))
-        trh, trl, trk = (np.zeros((NPAM, nl)) for _ in range(3))
-        for _ in range(self.norder):
-            deg, nk = rd.take(2)
-            l = int(deg)
-            nk = int(nk)
-            nmod[l] = nk
-            s[:nk, l] = rd.floats(nk)
-            v = rd.floats(5)
-            el[:, l] = (v[0], v[1], v[4])
-            v = rd.floats(5)
-            fl[:, l] = (v[0], v[1], v[4])
-            rh[:nk, l] = rd.floats(nk)
-            rl[:nk, l] = rd.floats(nk)
-            rk[:nk, l] = rd.floats(nk)
-            if float(deg) < 1.5:
-                continue
-            v = rd.floats(5)
-            tel[:, l] = (v[0], v[1], v[4])
-            v = rd.floats(5)
-            tfl[:, l] = (v[0], v[1], v[4])
-            trh[:nk, l] = rd.floats(nk)
-            trl[:nk, l] = rd.floats(nk)
-            trk[:nk, l] = rd.floats(nk)
-        ell = np.arange(1, nl, dtype=np.float64)
-        for a in (rl, rk, trl, trk):
-            a[:, 1:] /= ell
-        self.nmod = nmod
-        self.s = s
-        self.he = np.zeros(nl)
-        self.ke = np.zeros(nl)
-        self.hTE = np.zeros(nl)
-        self.kTE = np.zeros(nl)
-        self.he[1:] = el[0, 1:]
-        self.ke[1:] = el[2, 1:] / ell
-        self.hTE[1:] = tel[0, 1:]
-        self.kTE[1:] = tel[2, 1:] / ell
-        self.r = rh
-        self.rprime = rk
-        self.rT = trh
-        self.rprimeT = trk
-        # tangential-displacement (l) numbers of the optional horizontal read-out, scaled as k
-        self.le = np.zeros(nl)
-        self.lTE = np.zeros(nl)
-        self.le[1:] = el[1, 1:] / ell
-        self.lTE[1:] = tel[1, 1:] / ell
-        self.rl = rl
-        self.rlT = trl
-        self.max_modes = int(nmod.max())
+        blocks = read_love_blocks(path, self.norder)
+        self.nmod = np.zeros(nl, dtype=np.int64)
+        self.s = np.zeros((NPAM, nl))
+        for name in self._ELASTIC:
+            setattr(self, name, np.zeros(nl))
+        for name in self._RESIDUES:
+            setattr(self, name, np.zeros((NPAM, nl)))
+        for l, blk in blocks.items():
+            K = blk["K"]
+            self.nmod[l] = K
+            self.s[:K, l] = blk["relax"]
+            for name, (fld, pos) in self._ELASTIC.items():
+                if fld in blk:
+                    getattr(self, name)[l] = blk[fld][pos]
+            for name, fld in self._RESIDUES.items():
+                if fld in blk:
+                    getattr(self, name)[:K, l] = blk[fld]
+        for name in self._PER_DEGREE:
+            a = getattr(self, name)
+            a[..., 1:] /= np.arange(1, nl, dtype=np.float64)
+        self.max_modes = int(self.nmod.max())
 
 
 class SyntheticEarth:

@@ -76,45 +76,59 @@ class RateTables:
         return self.table
 
 
+def _lambda_jacobian(m, r2w2):
+    """d Lambda_2j / d m_i (3 x 3 complex, rows j = 0, 1, 2) of the centrifugal potential's degree-2
+    terms as functions of the rotation vector perturbation m (U convention):
+    Lambda_20 = r2w2 / (6 sqrt5) (m1^2 + m2^2 - 2 m3^2 - 4 m3),
+    Lambda_21 = -r2w2 / sqrt30 (m1 - i m2)(1 + m3),
+    Lambda_22 = r2w2 / sqrt120 (m2^2 - m1^2 + 2 i m1 m2)."""
+    m1, m2, m3 = m
+    c20, c21, c22 = r2w2 / (6.0 * math.sqrt(5.0)), -r2w2 / math.sqrt(30.0), r2w2 / math.sqrt(120.0)
+    return np.array([[c20 * 2 * m1, c20 * 2 * m2, c20 * (-4 * m3 - 4)],
+                     [c21 * (1 + m3), c21 * (-1j) * (1 + m3), c21 * (m1 - 1j * m2)],
+                     [c22 * (-2 * m1 + 2j * m2), c22 * (2 * m2 + 2j * m1), 0.0]], dtype=np.complex128)
+
+
 def rotation_rate(tabs, love, planet, h, il, mm, lam, oldil, oldm, dlam_prev2, r_il, r_m, r_la):
-    """Left derivatives (per year) at the end of the step of the degree-2 rotational sea-level and
-    radial terms (solver.py:722-764): the m equation differentiated with the step's converged
-    il, m, Lambda; returns (rate_sl, rate_rr) 3 x 3 complex (U convention) and the rates dict."""
+    """Left derivatives (per year) at the end of the step of the degree-2 rotational terms
+    (the reference's _rotation_rate, solver.py:722-764), from the step's converged inertia
+    perturbation ``il``, rotation vector ``mm`` and centrifugal potential ``lam``.
+
+    Each degree-2 modal state is first advanced by the commit of this step (its share 1 - phi of
+    the step's increment); a state's rate is then s_k (total - state_k) per mode.  The rotation
+    rate dm/dt follows from the time derivative of the linearised Liouville equation, the potential
+    rate from dLambda/dt = (dLambda/dm) dm/dt.  Returns (rate_sl, rate_rr) as 3 x 3 complex spectra
+    (U convention, rows l = 0..2) and the dict of rotational rates."""
     p = planet
     n2 = tabs.nmod2
-    dil = il - oldil
-    dm = mm - oldm
-    tot = lam[2, 0:3].copy()
-    c = tabs.omphi[:n2, 2]
-    r_il = r_il[:n2] + c[:, None, None] * dil[None]
-    r_m = r_m[:n2] + c[:, None] * dm[None]
-    r_la = r_la[:n2] + c[:, None] * (tot - dlam_prev2)[None]
-    sk = tabs.s[:n2, 2] / 1000.0
-    kTE2, hTE2, kE2 = love.kTE[2], love.hTE[2], love.ke[2]
-    ild = dil / h
-    sild = np.einsum("k,kij->ij", tabs.a_il[:n2] * sk, il[None] - r_il)
-    smd = np.einsum("k,ki->i", tabs.a_m[:n2] * sk, mm[None] - r_m)
-    alpha = 1 / (1 - kTE2 / p.kf)
-    md = np.zeros(3)
-    for i in (0, 1):
-        md[i] = alpha * ((1 / (p.moiC - p.moiA)) * ((1 + kE2) * ild[i, 2] + sild[i, 2]) + smd[i] / p.kf)
-    md[2] = -(1.0 / p.moiC) * ((1 + kE2) * ild[2, 2] + sild[2, 2])
-    m1, m2, m3 = mm
-    d1, d2, d3 = md
+    share = tabs.omphi[:n2, 2]
+    rate_k = tabs.s[:n2, 2] / 1000.0                       # 1/yr per mode
+    tot = lam[2, 0:3]
+    # states after this step's commit
+    st_il = r_il[:n2] + share[:, None, None] * (il - oldil)
+    st_m = r_m[:n2] + share[:, None] * (mm - oldm)
+    st_la = r_la[:n2] + share[:, None] * (tot - dlam_prev2)
+    # viscous parts of the rates: sum_k a_k s_k (total - state_k)
+    visc_il = np.tensordot(tabs.a_il[:n2] * rate_k, il - st_il, axes=1)
+    visc_m = (tabs.a_m[:n2] * rate_k) @ (mm - st_m)
+    visc_tsl = (tabs.a_tsl[:n2] * rate_k) @ (tot - st_la)
+    visc_trr = (tabs.a_trr[:n2] * rate_k) @ (tot - st_la)
+    ildot = (il - oldil) / h
+    # inertia forcing of the third column, elastic (1 + k_E) plus viscous
+    forcing = (1 + love.ke[2]) * ildot[:, 2] + visc_il[:, 2]
+    mdot = np.empty(3)
+    mdot[:2] = (forcing[:2] / (p.moiC - p.moiA) + visc_m[:2] / p.kf) / (1 - love.kTE[2] / p.kf)
+    mdot[2] = -forcing[2] / p.moiC
     r2w2 = p.radius ** 2 * p.omega ** 2
-    II = 1j
-    lad = np.zeros((3, 3), dtype=np.complex128)
-    lad[0, 0] = (r2w2 / 3.0) * (2 * m1 * d1 + 2 * m2 * d2 + 2 * m3 * d3 + 2.0 * d3)
-    lad[2, 0] = (r2w2 / (6.0 * math.sqrt(5.0))) * (2 * m1 * d1 + 2 * m2 * d2 - 4 * m3 * d3 - 4 * d3)
-    lad[2, 1] = -(r2w2 / math.sqrt(30.0)) * ((d1 - II * d2) * (1.0 + m3) + (m1 - II * m2) * d3)
-    lad[2, 2] = (r2w2 / math.sqrt(5.0 * 24.0)) * (2 * m2 * d2 - 2 * m1 * d1 + 2.0 * II * (d1 * m2 + m1 * d2))
-    tsld = np.einsum("k,ki->i", tabs.a_tsl[:n2] * sk, tot[None] - r_la)
-    trrd = np.einsum("k,ki->i", tabs.a_trr[:n2] * sk, tot[None] - r_la)
+    lamdot = np.zeros((3, 3), dtype=np.complex128)
+    m1, m2, m3 = mm
+    lamdot[0, 0] = (r2w2 / 3.0) * (2 * (m1 * mdot[0] + m2 * mdot[1] + m3 * mdot[2]) + 2.0 * mdot[2])
+    lamdot[2, 0:3] = _lambda_jacobian(mm, r2w2) @ mdot
     rate_sl = np.zeros((3, 3), dtype=np.complex128)
     rate_rr = np.zeros((3, 3), dtype=np.complex128)
-    rate_sl[2, 0:3] = ((1 + kTE2 - hTE2) * lad[2, 0:3] + tsld) / p.gacc
-    rate_rr[2, 0:3] = (hTE2 * lad[2, 0:3] + trrd) / p.gacc
-    return rate_sl, rate_rr, {"ildot": ild, "mdot": md, "lambdadot": lad}
+    rate_sl[2, 0:3] = ((1 + love.kTE[2] - love.hTE[2]) * lamdot[2, 0:3] + visc_tsl) / p.gacc
+    rate_rr[2, 0:3] = (love.hTE[2] * lamdot[2, 0:3] + visc_trr) / p.gacc
+    return rate_sl, rate_rr, {"ildot": ildot, "mdot": mdot, "lambdadot": lamdot}
 
 
 def rate_grids(sht, dsl, drr, dice00, dt, cst, planet):

@@ -51,6 +51,13 @@ def test_error_mapping():
     assert lib.sle_solver_set_horizontal(None, None) == _lib.SLE_ERR_BAD_ARG
     assert lib.sle_solver_get_horizontal(None, None, None, None) == _lib.SLE_ERR_BAD_ARG
     assert lib.sle_solver_set_ramp(None, None) == _lib.SLE_ERR_BAD_ARG
+    n = C.c_longlong()
+    assert lib.sle_solver_snapshot_bytes(None, C.byref(n)) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_solver_snapshot(None, None, 0) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_solver_restore(None, None, 0) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_batch_snapshot_bytes(None, C.byref(n)) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_batch_snapshot(None, 0, None, 0) == _lib.SLE_ERR_BAD_ARG
+    assert lib.sle_batch_restore(None, 0, None, 0) == _lib.SLE_ERR_BAD_ARG
     assert lib.sle_topo_scratch_bytes() >= 16
     buf = (C.c_double * 2)()
     assert lib.sle_topo_residual(None, None, 0.0, None, None, None, None, 4, 8, 920.0, 1000.0, None, buf,
@@ -198,3 +205,42 @@ def test_ramp_refused_for_mixed_precision():
     with pytest.raises(NotImplementedError, match="ramp"):
         SeaLevelSolver(None, love, np.full((16, 32), -1000.0), np.zeros((16, 32)), norder=15, ramp=True,
                        precision="mixed")
+
+
+def test_rotation_rate_matches_oracle():
+    """The package's rotational-rate read-out (Jacobian form) against the oracle's restatement of
+    the reference's expressions (pinned to its rates golden): 1e-12 of the largest entry."""
+    from oracle.memory import ModalState
+    from oracle.readouts import RateWeights, rotation_rate as oracle_rate
+    from slevolve_b200 import SyntheticEarth
+    from slevolve_b200.rates import RateTables, rotation_rate
+    from slevolve_b200.solver import Planet
+
+    lmax, dt = 15, 3.7
+    love = SyntheticEarth(lmax, 5, 9)
+    p = Planet()
+    rng = np.random.default_rng(4)
+    st = ModalState(love, lmax, dt)
+    n2 = st.nmod2
+    st.r_il = rng.normal(size=(st.kmax, 3, 3)) * 1e30
+    st.r_m = rng.normal(size=(st.kmax, 3)) * 1e-9
+    st.r_lambda = (rng.normal(size=(st.kmax, 3)) + 1j * rng.normal(size=(st.kmax, 3))) * 1e-3
+    wt = RateWeights(st)
+    wt.set_dt(st, dt)
+    tabs = RateTables(love, lmax)
+    tabs.for_dt(dt)
+    il = rng.normal(size=(3, 3)) * 1e30
+    oldil = il + rng.normal(size=(3, 3)) * 1e28
+    mm = rng.normal(size=3) * 1e-8
+    oldm = mm + rng.normal(size=3) * 1e-10
+    lam = np.zeros((3, 3), dtype=np.complex128)
+    lam[2, :] = (rng.normal(size=3) + 1j * rng.normal(size=3)) * 1e-2
+    lam[0, 0] = 0.3
+    dprev = (rng.normal(size=3) + 1j * rng.normal(size=3)) * 1e-3
+    a_sl, a_rr, a_d = oracle_rate(st, wt, love, p, dt, il, mm, lam, oldil, oldm, dprev)
+    b_sl, b_rr, b_d = rotation_rate(tabs, love, p, dt, il, mm, lam, oldil, oldm, dprev,
+                                    st.r_il, st.r_m, st.r_lambda)
+    for a, b in ((a_sl, b_sl), (a_rr, b_rr), (a_d["mdot"], b_d["mdot"]), (a_d["ildot"], b_d["ildot"]),
+                 (a_d["lambdadot"], b_d["lambdadot"])):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+    assert n2 > 0
