@@ -91,6 +91,12 @@ _SIGS = {
     "sle_solver_set_horizontal": (C.c_int, [C.c_void_p, C.c_void_p]),
     "sle_solver_get_horizontal": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_solver_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "sle_solver_snapshot_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "sle_solver_snapshot": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    "sle_solver_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    "sle_batch_snapshot_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_longlong)]),
+    "sle_batch_snapshot": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong]),
+    "sle_batch_restore": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong]),
     "sle_batch_create": (C.c_int, [C.POINTER(SleConfig), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "sle_batch_destroy": (C.c_int, [C.c_void_p]),
     "sle_batch_load": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(SleEarth), C.c_double, C.c_void_p,

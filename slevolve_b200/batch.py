@@ -132,6 +132,33 @@ class SolverBatch:
         _lib.check(self._L.sle_batch_release(self._h, int(slot)), "sle_batch_release")
         self.loaded[slot] = False
 
+    # ------------------------------------------------------------- snapshots
+    def snapshot_bytes(self) -> int:
+        n = C.c_longlong()
+        _lib.check(self._L.sle_batch_snapshot_bytes(self._h, C.byref(n)), "sle_batch_snapshot_bytes")
+        return int(n.value)
+
+    def snapshot(self, slot, out=None):
+        """The slot's whole solve state as a host byte image (NumPy uint8; ``out``: a buffer of
+        ``snapshot_bytes()`` bytes to fill, e.g. a pinned CPU tensor's NumPy view).  It restores
+        into any slot of a batch of the same configuration, or into a solver (``restore``)."""
+        n = self.snapshot_bytes()
+        img = np.empty(n, dtype=np.uint8) if out is None else out
+        if not (isinstance(img, np.ndarray) and img.dtype == np.uint8 and img.flags.c_contiguous
+                and img.size >= n):
+            raise ValueError(f"out must be a contiguous uint8 array of at least {n} bytes")
+        _lib.check(self._L.sle_batch_snapshot(self._h, int(slot), C.c_void_p(img.ctypes.data), n),
+                   "sle_batch_snapshot")
+        return img
+
+    def restore(self, slot, image):
+        """Make `slot` continue the solve a snapshot image holds (its reuse store, if any, is
+        attached again with ``set_reuse``)."""
+        img = np.ascontiguousarray(image, dtype=np.uint8)
+        _lib.check(self._L.sle_batch_restore(self._h, int(slot), C.c_void_p(img.ctypes.data), img.size),
+                   "sle_batch_restore")
+        self.loaded[slot] = True
+
     # ------------------------------------------------------------------- step
     def step_ptrs(self, ptrs, on_device, dts=None):
         """One step from raw grid pointers: {slot: pointer}; returns {slot: SleStepInfo}.

@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 namespace sle {
@@ -2126,6 +2127,191 @@ extern "C" int sle_batch_release(sle_batch* b, int slot) {
   return SLE_OK;
 }
 
+// ----------------------------------------------------------------- snapshots
+// One slot's whole state as a host byte image: a header (configuration it belongs to, the host
+// bookkeeping of the slot), then every per-slot device buffer in a fixed order.  The device
+// sections hold more than the state a step carries forward (all grids, masks and spectra of the
+// slot, not only the modal state, load history, topography and masks of the last step), so a
+// restored slot continues bit for bit as the original would have.  The reference checkpoints the
+// same state (fortran/src/modal_state_mod.f90:445-477: shapes, decay, loads and modal states) in
+// a stream file of its own format; this image is not that format.
+namespace {
+
+constexpr uint32_t SNAP_MAGIC = 0x534C4553u;   // "SLES"
+constexpr uint32_t SNAP_VERSION = 1;
+
+struct SnapHeader {
+  uint32_t magic, version;
+  int32_t nlat, nlon, lmax, K, precision, flags;
+  long long nbytes;
+  // host bookkeeping of the slot (SlotHost without the caller-owned reuse store)
+  int32_t iter, nhist, hsel, pad;
+  double dt, dt_cur, dt_hist[2];
+  double ocean_area0, oceanBeta_area0, ice_volume0;
+  sle_step_info last;
+};
+
+int snap_flags(const sle_config& c) {
+  return (c.tpw ? 1 : 0) | (c.checkmarine ? 2 : 0) | (c.calcRG ? 4 : 0) | (c.opt_dsl ? 8 : 0) |
+         (c.opt_diag ? 16 : 0) | (c.inner_extrap ? 32 : 0);
+}
+
+// The device sections of slot b: (device address, bytes), in image order.
+std::vector<std::pair<void*, size_t>> snap_sections(sle_batch* s, int b) {
+  const Dev& D = s->D;
+  const size_t ng = (size_t)D.ng, nc = (size_t)D.ncoef, nl = (size_t)D.nl, K = (size_t)s->K;
+  std::vector<std::pair<void*, size_t>> v;
+  for (int g = 0; g < NGRID; ++g) v.push_back({D.g(g, b), sizeof(double) * ng});
+  for (int m = 0; m < NMASK; ++m) v.push_back({D.m(m, b), ng});
+  for (int q = 0; q < NSPEC; ++q) v.push_back({D.sp(q, b), sizeof(double2) * nc});
+  if (K) v.push_back({D.R + (size_t)b * K * nc, sizeof(double2) * K * nc});
+  v.push_back({s->nmod + (size_t)b * nl, sizeof(int) * nl});
+  double* kl[] = {s->s_kl, s->decay, s->omd, s->a_sl, s->a_rr};
+  if (K)
+    for (double* p : kl) v.push_back({p + (size_t)b * K * nl, sizeof(double) * K * nl});
+  double* l1[] = {s->ttl, s->ttlekhl, s->ttlhe};
+  for (double* p : l1) v.push_back({p + (size_t)b * nl, sizeof(double) * nl});
+  if (K) {
+    double* k1[] = {s->a_il, s->a_m, s->a_tsl, s->a_trr};
+    for (double* p : k1) v.push_back({p + (size_t)b * K, sizeof(double) * K});
+    v.push_back({s->r_il + (size_t)b * K * 9, sizeof(double) * K * 9});
+    v.push_back({s->r_m + (size_t)b * K * 3, sizeof(double) * K * 3});
+    v.push_back({s->r_lam + (size_t)b * K * 6, sizeof(double) * K * 6});
+  }
+  v.push_back({s->rc + b, sizeof(RotConst)});
+  v.push_back({s->sc + b, sizeof(Scal)});
+  return v;
+}
+
+long long snap_bytes(sle_batch* s) {
+  long long n = (long long)sizeof(SnapHeader);
+  for (const auto& sec : snap_sections(s, 0)) n += (long long)sec.second;
+  return n;
+}
+
+int batch_snapshot(sle_batch* s, int b, void* dst, long long nbytes) {
+  SLE_TRY(check_slot(s, b, "sle_batch_snapshot"));
+  const SlotHost& h = s->slot[b];
+  if (!h.inited) {
+    set_error("sle_batch_snapshot: slot %d holds no solve", b);
+    return SLE_ERR_STATE;
+  }
+  const long long need = snap_bytes(s);
+  if (!dst || nbytes < need) {
+    set_error("sle_batch_snapshot: the image needs %lld bytes (got %lld)", need, nbytes);
+    return SLE_ERR_BAD_ARG;
+  }
+  SnapHeader hd;
+  std::memset(&hd, 0, sizeof(hd));
+  hd.magic = SNAP_MAGIC;
+  hd.version = SNAP_VERSION;
+  hd.nlat = s->cfg.nlat;
+  hd.nlon = s->cfg.nlon;
+  hd.lmax = s->cfg.lmax;
+  hd.K = s->K;
+  hd.precision = s->cfg.precision;
+  hd.flags = snap_flags(s->cfg);
+  hd.nbytes = need;
+  hd.iter = h.iter;
+  hd.nhist = h.nhist;
+  hd.hsel = h.hsel;
+  hd.dt = h.dt;
+  hd.dt_cur = h.dt_cur;
+  hd.dt_hist[0] = h.dt_hist[0];
+  hd.dt_hist[1] = h.dt_hist[1];
+  hd.ocean_area0 = h.ocean_area0;
+  hd.oceanBeta_area0 = h.oceanBeta_area0;
+  hd.ice_volume0 = h.ice_volume0;
+  hd.last = h.last;
+  unsigned char* out = static_cast<unsigned char*>(dst);
+  std::memcpy(out, &hd, sizeof(hd));
+  size_t off = sizeof(hd);
+  for (const auto& sec : snap_sections(s, b)) {
+    SLE_CUDA(cudaMemcpyAsync(out + off, sec.first, sec.second, cudaMemcpyDeviceToHost, s->st));
+    off += sec.second;
+  }
+  SLE_CUDA(cudaStreamSynchronize(s->st));
+  return SLE_OK;
+}
+
+int batch_restore(sle_batch* s, int b, const void* src, long long nbytes) {
+  SLE_TRY(check_slot(s, b, "sle_batch_restore"));
+  const long long need = snap_bytes(s);
+  if (!src || nbytes < (long long)sizeof(SnapHeader)) {
+    set_error("sle_batch_restore: no snapshot image given");
+    return SLE_ERR_BAD_ARG;
+  }
+  SnapHeader hd;
+  std::memcpy(&hd, src, sizeof(hd));
+  if (hd.magic != SNAP_MAGIC || hd.version != SNAP_VERSION) {
+    set_error("sle_batch_restore: not a snapshot image of this library (magic %08x, version %u)", hd.magic,
+              hd.version);
+    return SLE_ERR_BAD_ARG;
+  }
+  if (hd.nlat != s->cfg.nlat || hd.nlon != s->cfg.nlon || hd.lmax != s->cfg.lmax || hd.K != s->K ||
+      hd.precision != s->cfg.precision || hd.flags != snap_flags(s->cfg)) {
+    set_error("sle_batch_restore: the image belongs to a %d x %d, lmax %d, %d-mode solve of precision %d and "
+              "options %d; this batch is %d x %d, lmax %d, %d modes, precision %d, options %d",
+              hd.nlat, hd.nlon, hd.lmax, hd.K, hd.precision, hd.flags, s->cfg.nlat, s->cfg.nlon, s->cfg.lmax,
+              s->K, s->cfg.precision, snap_flags(s->cfg));
+    return SLE_ERR_BAD_SHAPE;
+  }
+  if (hd.nbytes != need || nbytes < need) {
+    set_error("sle_batch_restore: image of %lld bytes, this batch's images have %lld", nbytes, need);
+    return SLE_ERR_BAD_ARG;
+  }
+  const unsigned char* in = static_cast<const unsigned char*>(src);
+  size_t off = sizeof(hd);
+  for (const auto& sec : snap_sections(s, b)) {
+    SLE_CUDA(cudaMemcpyAsync(sec.first, in + off, sec.second, cudaMemcpyHostToDevice, s->st));
+    off += sec.second;
+  }
+  SLE_CUDA(cudaStreamSynchronize(s->st));
+  SlotHost& h = s->slot[b];
+  h = SlotHost{};
+  h.loaded = 1;
+  h.inited = 1;
+  h.iter = hd.iter;
+  h.nhist = hd.nhist;
+  h.hsel = hd.hsel;
+  h.dt = hd.dt;
+  h.dt_cur = hd.dt_cur;
+  h.dt_hist[0] = hd.dt_hist[0];
+  h.dt_hist[1] = hd.dt_hist[1];
+  h.ocean_area0 = hd.ocean_area0;
+  h.oceanBeta_area0 = hd.oceanBeta_area0;
+  h.ice_volume0 = hd.ice_volume0;
+  h.last = hd.last;
+  return SLE_OK;
+}
+
+}  // namespace
+
+extern "C" int sle_batch_snapshot_bytes(const sle_batch* b, long long* nbytes) {
+  if (!b || !nbytes) {
+    set_error("sle_batch_snapshot_bytes: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  *nbytes = snap_bytes(const_cast<sle_batch*>(b));
+  return SLE_OK;
+}
+
+extern "C" int sle_batch_snapshot(sle_batch* b, int slot, void* dst, long long nbytes) {
+  if (!b) {
+    set_error("sle_batch_snapshot: NULL batch");
+    return SLE_ERR_BAD_ARG;
+  }
+  return batch_snapshot(b, slot, dst, nbytes);
+}
+
+extern "C" int sle_batch_restore(sle_batch* b, int slot, const void* src, long long nbytes) {
+  if (!b) {
+    set_error("sle_batch_restore: NULL batch");
+    return SLE_ERR_BAD_ARG;
+  }
+  return batch_restore(b, slot, src, nbytes);
+}
+
 extern "C" int sle_batch_set_reuse(sle_batch* b, int slot, void* ds_store, void* mask_store, int capacity,
                                    int valid) {
   if (!b) {
@@ -2278,6 +2464,30 @@ extern "C" int sle_solver_step(sle_solver* s, const double* ice, int on_device, 
   const int rc = batch_step(s->b, ices, on_device, dts, &o);
   if (info) *info = o;
   return rc;
+}
+
+extern "C" int sle_solver_snapshot_bytes(const sle_solver* s, long long* nbytes) {
+  if (!s) {
+    set_error("sle_solver_snapshot_bytes: NULL solver");
+    return SLE_ERR_BAD_ARG;
+  }
+  return sle_batch_snapshot_bytes(s->b, nbytes);
+}
+
+extern "C" int sle_solver_snapshot(sle_solver* s, void* dst, long long nbytes) {
+  if (!s) {
+    set_error("sle_solver_snapshot: NULL solver");
+    return SLE_ERR_BAD_ARG;
+  }
+  return batch_snapshot(s->b, 0, dst, nbytes);
+}
+
+extern "C" int sle_solver_restore(sle_solver* s, const void* src, long long nbytes) {
+  if (!s) {
+    set_error("sle_solver_restore: NULL solver");
+    return SLE_ERR_BAD_ARG;
+  }
+  return batch_restore(s->b, 0, src, nbytes);
 }
 
 extern "C" int sle_solver_set_reuse(sle_solver* s, void* ds_store, void* mask_store, int capacity, int valid) {

@@ -17,6 +17,12 @@ admission to completion; the ice of each step is generated on the device.
 
 A solve's result does not depend on what else is in its batch (per-slot reductions in a fixed
 order, per-field tensor-core columns), so a request gives the same answer alone and in the mix.
+
+Requests carry a priority.  With ``preempt=True``, a request that has arrived and finds every slot
+of its degree taken by requests of lower priority preempts one of them between two batch steps:
+the victim's whole solve state is copied to host memory (``SolverBatch.snapshot``), its slot goes
+to the newcomer, and the victim waits in the queue until a slot frees, where it is restored
+(``SolverBatch.restore``, possibly into another slot) and continues bit for bit where it stopped.
 """
 
 from __future__ import annotations
@@ -49,12 +55,14 @@ class Request:
     arrival: float = 0.0
     outer_passes: int = 1
     obs: Optional[np.ndarray] = None
+    priority: int = 0
     # filled in by the server
     t_admit: float = math.nan
     t_done: float = math.nan
     numiter: int = 0
     passes_done: int = 0
     warm_steps: int = 0
+    preemptions: int = 0
     result: dict = dataclasses.field(default_factory=dict)
 
     @property
@@ -62,14 +70,20 @@ class Request:
         return self.t_done - self.arrival
 
 
-def footprint(req: Request, max_modes=8) -> int:
-    """Device bytes a request holds while admitted (admission unit)."""
+def store_bytes(req: Request) -> int:
+    """Device bytes of an outer request's reuse store (0 for a forward solve)."""
+    if req.outer_passes <= 1:
+        return 0
     n = req.lmax + 1
-    b = slot_bytes(n, 2 * n, req.lmax, max_modes)
-    if req.outer_passes > 1:
-        nc = n * (n + 1) // 2
-        b += req.nsteps * (16 * nc + n * 2 * n)
-    return b
+    nc = n * (n + 1) // 2
+    return req.nsteps * (16 * nc + n * 2 * n)
+
+
+def footprint(req: Request, max_modes=8) -> int:
+    """Device bytes a request holds while admitted (admission unit): one slot's solver state plus
+    the reuse store of an outer request."""
+    n = req.lmax + 1
+    return slot_bytes(n, 2 * n, req.lmax, max_modes) + store_bytes(req)
 
 
 class _Running:
@@ -80,14 +94,17 @@ class _Running:
         self.store = None   # ReuseStore of an outer request
         self.T0 = None      # current initial topography (device) of an outer request
         self.obs = None
+        self.image = None   # host snapshot while preempted
 
 
 class Server:
     """groups: {lmax: slots}.  budget_bytes: device memory the admitted requests may hold."""
 
     def __init__(self, groups, precision="mixed", budget_bytes=None, max_modes=8, opt=("dsl", "diag"),
-                 inner="extrap", record=("deltasl", "tgrid")):
+                 inner="extrap", record=("deltasl", "tgrid"), preempt=False):
         self.precision = precision
+        self.preempt = bool(preempt)
+        self.preempted = 0
         self.max_modes = max_modes
         self.record = tuple(record)
         self.batches = {int(L): SolverBatch(L + 1, 2 * (L + 1), L, int(n), max_modes=max_modes,
@@ -103,20 +120,67 @@ class Server:
         self.batch_steps = {L: 0 for L in self.batches}  # batched steps per group
 
     # ---------------------------------------------------------------- helpers
+    @staticmethod
+    def _next(q, now):
+        """The arrived queued request to admit next: highest priority, then earliest arrival."""
+        best = None
+        for r in q:
+            if r.arrival <= now and (best is None or (-r.priority, r.arrival, r.rid) <
+                                     (-best.priority, best.arrival, best.rid)):
+                best = r
+        return best
+
+    def _preempt_for(self, L, bt, running, req):
+        """Free a slot for `req` by preempting the lowest-priority running request (the most
+        recently admitted among equals) if its priority is below req's; returns the slot or None."""
+        victims = [r for r in running.values() if r.req.priority < req.priority]
+        if not victims:
+            return None
+        v = min(victims, key=lambda r: (r.req.priority, -r.req.t_admit))
+        v.image = bt.snapshot(v.slot)
+        bt.release(v.slot)
+        del running[v.slot]
+        v.req.preemptions += 1
+        self.preempted += 1
+        with self.lock:
+            self.used -= footprint(v.req, self.max_modes) - store_bytes(v.req)   # the store stays
+        self.queue[L].append(v.req)
+        v.req._run = v
+        return v.slot
+
     def _admit(self, L, running, now):
         bt = self.batches[L]
         free = [s for s in range(bt.nslots) if s not in running]
         q = self.queue[L]
-        while free and q and q[0].arrival <= now:
-            req = q[0]
-            fp = footprint(req, self.max_modes)
+        while q:
+            req = self._next(q, now)
+            if req is None:
+                return
+            resumed = getattr(req, "_run", None)
+            fp = footprint(req, self.max_modes) - (store_bytes(req) if resumed is not None else 0)
+            if not free and self.preempt:
+                slot = self._preempt_for(L, bt, running, req)
+                if slot is not None:
+                    free.append(slot)
+            if not free:
+                return
             with self.lock:
                 if self.used + fp > self.budget:
                     return
                 self.used += fp
                 self.peak_used = max(self.peak_used, self.used)
-            q.pop(0)
+            q.remove(req)
             slot = free.pop(0)
+            if resumed is not None:
+                # a preempted request: its state comes back from the host image
+                run, req._run = resumed, None
+                run.slot = slot
+                bt.restore(slot, run.image)
+                run.image = None
+                if run.store is not None:
+                    bt.set_reuse(slot, run.store, valid=run.store.recorded)   # as at the pass's load
+                running[slot] = run
+                continue
             run = _Running(req, slot)
             req.t_admit = time.perf_counter() - self._t0
             if req.outer_passes > 1:
@@ -214,7 +278,7 @@ class Server:
                 "member_steps_per_s": steps / self.wall,
                 "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
                 "peak_bytes": int(self.peak_used), "budget_bytes": self.budget,
-                "batch_steps": dict(self.batch_steps)}
+                "batch_steps": dict(self.batch_steps), "preemptions": self.preempted}
 
 
 # ------------------------------------------------------------- synthetic members

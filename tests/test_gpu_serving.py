@@ -30,7 +30,7 @@ def _requests():
 
 
 def _fresh(r):
-    return dataclasses.replace(r, arrival=0.0, result={}, passes_done=0, numiter=0, warm_steps=0)
+    return dataclasses.replace(r, arrival=0.0, result={}, passes_done=0, numiter=0, warm_steps=0, preemptions=0)
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
