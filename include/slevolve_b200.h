@@ -290,7 +290,10 @@ long long sle_topo_scratch_bytes(void);
 /* ------------------------------------------------------- measurement */
 /* Kernel classes timed by sle_prof_*: 0 row FFT + fold, 1 Legendre analysis, 2 Legendre
  * synthesis, 3 inverse FFT + unfold, 4 modal-state advance, 5 the Legendre analysis of the inner
- * iteration's rO field (every stepping slot's field active; class 1 has the other analyses).
+ * iteration's rO field (every stepping slot's field active; class 1 has the other analyses),
+ * then the inner loop's elementwise passes, their units being the slots still iterating:
+ * 6 eq. B18, 7 conservation / load update / xi, 8 deltasl + ocean function + grounded test,
+ * 9 C* refresh, 10 dI after a grounded-mask change.
  * Timing is off by default; when on, each launch of these classes is bracketed by CUDA events on
  * its own stream. */
 int sle_prof_enable(int on);

@@ -124,7 +124,8 @@ _SIGS = {
     "sle_probe_fp64_tflops": (C.c_int, [_DP]),
 }
 
-PROF_FFT, PROF_LEG_ANA, PROF_LEG_SYN, PROF_IFFT, PROF_ADVANCE, PROF_ANA_STEP = range(6)
+(PROF_FFT, PROF_LEG_ANA, PROF_LEG_SYN, PROF_IFFT, PROF_ADVANCE, PROF_ANA_STEP, PROF_B18, PROF_UPDATE,
+ PROF_REFRESH1, PROF_REFRESH2, PROF_DICE) = range(11)
 PREC_FP64, PREC_MIXED = 0, 1
 PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
 

@@ -195,8 +195,10 @@ struct sle_sht {
 namespace sle {
 // Launch accounting / per-kernel event timing (sle_prof.cu).
 // PROF_ANA_STEP: the Legendre analysis of the inner iteration's rO (every stepping field active).
+// Classes 6-10: the inner loop's elementwise passes (units = slots not yet converged).
 enum ProfClass { PROF_FFT = 0, PROF_LEG_ANA = 1, PROF_LEG_SYN = 2, PROF_IFFT = 3, PROF_ADVANCE = 4,
-                 PROF_ANA_STEP = 5, PROF_NCLS = 6 };
+                 PROF_ANA_STEP = 5, PROF_B18 = 6, PROF_UPDATE = 7, PROF_REFRESH1 = 8, PROF_REFRESH2 = 9,
+                 PROF_DICE = 10, PROF_NCLS = 11 };
 struct ProfToken {
   int cls;
   double units;

@@ -1264,6 +1264,7 @@ struct sle_batch {
   bool pending_graph = false;
   std::vector<int> pending_act;
   long long body_launches;   // kernels in one iteration of the graph body
+  int iter_active = 0;       // host-driven loop: stepping slots not yet converged (timing units)
   // static field lists of the loop body
   std::vector<FieldSpec> f_syn_sl, f_ana_ro, f_syn_sltot, f_ana_refresh;
 };
@@ -1375,26 +1376,37 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   cudaStream_t st = s->st;
   const long long nc = D.ncoef, ng = D.ng;
   const unsigned B = (unsigned)s->nslot;
+  const double act = (double)s->iter_active;   // per-class timing units: slots still iterating
   note_launch();
+  ProfToken t = prof_begin(PROF_B18, act, st);
   k_b18<<<dim3(nb(nc), B), 256, 0, st>>>(D);
+  prof_end(t, st);
   SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sl.data(), (int)s->f_syn_sl.size(), st));
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_ro.data(), (int)s->f_ana_ro.size(), st, PROF_ANA_STEP));
   note_launch();
+  t = prof_begin(PROF_UPDATE, act, st);
   k_update<<<dim3(nb(nc), B), 256, 0, st>>>(D);
+  prof_end(t, st);
   if (!s->cfg.opt_dsl) {
     note_launch();
     k_sltot<<<dim3(nb(nc), B), 256, 0, st>>>(D);
     SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sltot.data(), (int)s->f_syn_sltot.size(), st));
   }
   note_launch(2);
+  t = prof_begin(PROF_REFRESH1, act, st);
   k_refresh1<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
+  prof_end(t, st);
+  t = prof_begin(PROF_REFRESH2, act, st);
   if (ng % 8 == 0) k_refresh2_x8<<<dim3(nb(ng / 8), B), 256, 0, st>>>(D);
   else k_refresh2<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
+  prof_end(t, st);
   // I* (only when the grounded mask changed), C* and tO for the next iteration; skipped for
   // slots that converged
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_refresh.data(), (int)s->f_ana_refresh.size(), st));
   note_launch(2);
+  t = prof_begin(PROF_DICE, act, st);
   k_dice<<<dim3(nb(nc), B), 256, 0, st>>>(D);
+  prof_end(t, st);
   k_loop_cond<<<1, 128, 0, st>>>(D, s->bstatus, loop);
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
@@ -1889,6 +1901,7 @@ int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, cons
     if (!s->loop_exec) SLE_TRY(build_loop_graph(s));
     SLE_CUDA(cudaGraphLaunch(s->loop_exec, st));
   } else {
+    s->iter_active = (int)act.size();
     for (int host_iter = 0;; ++host_iter) {
       if (host_iter > MAX_INNER + 2) {  // the device flags must have stopped the loop by now
         set_error("inner loop control lost (device iteration counter did not advance)");
@@ -1896,9 +1909,10 @@ int batch_step_begin(sle_batch* s, const double* const* ice, int on_device, cons
       }
       SLE_TRY(enqueue_iteration(s, 0));
       SLE_TRY(sync_scal(s));
-      bool any = false;
-      for (int b : act) any |= !s->hsc[b].done;
-      if (!any) break;
+      int left = 0;
+      for (int b : act) left += !s->hsc[b].done;
+      s->iter_active = left;
+      if (!left) break;
     }
   }
   note_launch();

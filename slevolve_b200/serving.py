@@ -101,10 +101,13 @@ class Server:
     """groups: {lmax: slots}.  budget_bytes: device memory the admitted requests may hold."""
 
     def __init__(self, groups, precision="mixed", budget_bytes=None, max_modes=8, opt=("dsl", "diag"),
-                 inner="extrap", record=("deltasl", "tgrid"), preempt=False):
+                 inner="extrap", record=("deltasl", "tgrid"), preempt=False, device_bytes=None):
         self.precision = precision
         self.preempt = bool(preempt)
         self.preempted = 0
+        # occupancy record: (time, admitted bytes) at every change, against device_bytes
+        self.device_bytes = device_bytes
+        self._occ = []
         self.max_modes = max_modes
         self.record = tuple(record)
         self.batches = {int(L): SolverBatch(L + 1, 2 * (L + 1), L, int(n), max_modes=max_modes,
@@ -120,6 +123,28 @@ class Server:
         self.batch_steps = {L: 0 for L in self.batches}  # batched steps per group
 
     # ---------------------------------------------------------------- helpers
+    def _note_used(self):
+        """Record the admitted footprint after a change (caller holds the lock)."""
+        self._occ.append((time.perf_counter() - getattr(self, "_t0", time.perf_counter()), self.used))
+
+    def occupancy(self):
+        """Time-weighted mean and peak of the admitted footprint over the run, in bytes and as a
+        fraction of ``device_bytes`` (when given)."""
+        ev = sorted(self._occ)
+        wall = getattr(self, "wall", 0.0)
+        if not ev or wall <= 0:
+            return {"mean_bytes": 0.0, "peak_bytes": int(self.peak_used)}
+        area, t_prev, u_prev = 0.0, 0.0, 0
+        for t, u in ev:
+            area += u_prev * max(0.0, t - t_prev)
+            t_prev, u_prev = t, u
+        area += u_prev * max(0.0, wall - t_prev)
+        out = {"mean_bytes": area / wall, "peak_bytes": int(self.peak_used)}
+        if self.device_bytes:
+            out["hbm_occupancy_mean"] = out["mean_bytes"] / self.device_bytes
+            out["hbm_occupancy_peak"] = self.peak_used / self.device_bytes
+        return out
+
     @staticmethod
     def _next(q, now):
         """The arrived queued request to admit next: highest priority, then earliest arrival."""
@@ -144,6 +169,7 @@ class Server:
         self.preempted += 1
         with self.lock:
             self.used -= footprint(v.req, self.max_modes) - store_bytes(v.req)   # the store stays
+            self._note_used()
         self.queue[L].append(v.req)
         v.req._run = v
         return v.slot
@@ -169,6 +195,7 @@ class Server:
                     return
                 self.used += fp
                 self.peak_used = max(self.peak_used, self.used)
+                self._note_used()
             q.remove(req)
             slot = free.pop(0)
             if resumed is not None:
@@ -225,6 +252,7 @@ class Server:
         del running[run.slot]
         with self.lock:
             self.used -= footprint(req, self.max_modes)
+            self._note_used()
             self.done.append(req)
 
     def _group_loop(self, L):
@@ -273,12 +301,17 @@ class Server:
 
     def stats(self, requests):
         lat = np.array([r.latency for r in requests])
+        wait = np.array([r.t_admit - r.arrival for r in requests])
         steps = sum(self.steps.values())
-        return {"requests": len(requests), "wall_s": self.wall, "member_steps": steps,
-                "member_steps_per_s": steps / self.wall,
-                "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-                "peak_bytes": int(self.peak_used), "budget_bytes": self.budget,
-                "batch_steps": dict(self.batch_steps), "preemptions": self.preempted}
+        out = {"requests": len(requests), "wall_s": self.wall, "member_steps": steps,
+               "member_steps_per_s": steps / self.wall,
+               "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+               "admission_wait_p50_s": float(np.percentile(wait, 50)),
+               "admission_wait_p99_s": float(np.percentile(wait, 99)),
+               "peak_bytes": int(self.peak_used), "budget_bytes": self.budget,
+               "batch_steps": dict(self.batch_steps), "preemptions": self.preempted}
+        out.update({k: v for k, v in self.occupancy().items() if k != "peak_bytes"})
+        return out
 
 
 # ------------------------------------------------------------- synthetic members

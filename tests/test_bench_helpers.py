@@ -1,5 +1,6 @@
 """Host-side arithmetic of bench.py's roofline split (no GPU): the transform share, the modal
-advance share and their time-weighted combination from a per-class device-time profile."""
+advance share, the elementwise passes and their time-weighted combination from a per-class
+device-time profile; the serving loop's occupancy record."""
 
 import importlib.util
 import math
@@ -21,7 +22,7 @@ def _prof(nprof=3):
     per_step = {"k_fold_mx": (1.39, 32.3, 1034.7), "k_leg_tc<analysis of rO>": (0.69, 7.3, 234.7),
                 "k_leg_tc<other analyses>": (1.65, 25.0, 800.0),
                 "k_bsyn_mx + k_leg_tc<synthesis>": (0.97, 8.3, 266.7), "k_unfold_mx": (0.51, 8.3, 266.7),
-                "k_advance": (0.32, 1.0, 32.0)}
+                "k_advance": (0.32, 1.0, 32.0), "k_update": (0.5, 7.0, 150.0)}
     return {k: {"ms": v[0] * nprof, "launches": v[1] * nprof, "fields": v[2] * nprof} for k, v in per_step.items()}
 
 
@@ -34,11 +35,14 @@ def test_step_shares_arithmetic():
     fields = 234.7 + 800.0 + 266.7
     t = (1.39 + 0.69 + 1.65 + 0.97 + 0.51) / 1000.0
     assert sh["transforms"]["achieved"] == pytest.approx(fields * per / t / 1e12, rel=1e-12)
-    assert sh["transforms"]["frac"] == pytest.approx(sh["transforms"]["achieved"] / 795.0, rel=1e-12)
+    assert sh["transforms"]["frac"] == pytest.approx(sh["transforms"]["achieved"] / (1590.0 * b.TENSOR_RATE),
+                                                     rel=1e-12)
     adv = 19 * 16.0 * ncoef * 32.0 / 0.32e-3 / 1e9
     assert sh["modal_advance"]["achieved"] == pytest.approx(adv, rel=1e-12)
-    lo = min(sh["transforms"]["frac"], sh["modal_advance"]["frac"])
-    hi = max(sh["transforms"]["frac"], sh["modal_advance"]["frac"])
+    upd = sh["elementwise"]["k_update"]
+    assert upd["achieved"] == pytest.approx(96.0 * ncoef * 150.0 / 0.5e-3 / 1e9, rel=1e-12)
+    fr = [sh["transforms"]["frac"], sh["modal_advance"]["frac"], upd["frac"]]
+    lo, hi = min(fr), max(fr)
     assert lo <= sh["combined_frac"] <= hi
     assert sh["transforms"]["ms_per_step"] == pytest.approx(5.21, rel=1e-12)
 
@@ -48,3 +52,18 @@ def test_step_shares_empty_profile():
     prof = {k: {"ms": 0.0, "launches": 0, "fields": 0.0} for k in _prof()}
     sh = b.step_shares(prof, 1, {"hbm_gbs": 1.0, "bf16_tflops": 2.0})
     assert sh["combined_frac"] == 0.0 and not math.isnan(sh["transforms"]["frac"])
+
+
+def test_serving_occupancy_record():
+    """Time-weighted mean of the admitted footprint from the server's (time, bytes) record."""
+    from slevolve_b200.serving import Server
+
+    srv = object.__new__(Server)
+    srv._occ = [(0.0, 100), (1.0, 300), (3.0, 0)]
+    srv.wall = 4.0
+    srv.peak_used = 300
+    srv.device_bytes = 1000
+    occ = srv.occupancy()
+    assert occ["mean_bytes"] == pytest.approx((100 * 1.0 + 300 * 2.0) / 4.0)
+    assert occ["hbm_occupancy_mean"] == pytest.approx(occ["mean_bytes"] / 1000)
+    assert occ["hbm_occupancy_peak"] == pytest.approx(0.3)
