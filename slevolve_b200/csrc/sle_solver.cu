@@ -645,7 +645,9 @@ __global__ void k_update(Dev D) {
     nr = __dsub_rn(nr, t.x);
     ni = __dsub_rn(ni, t.y);
     D.sp(S_LOAD, b)[i] = make_double2(nr, ni);
-    D.sp(S_DSCUR, b)[i] = make_double2(__dadd_rn(p.x, nr), __dadd_rn(p.y, ni));
+    // dS_cur = dS_prev + new: the rotation block of the next iteration reads its degree-2 entries;
+    // the commit forms the whole of it from the converged increment (the same sum)
+    if (i == D.i20 || i == D.i21) D.sp(S_DSCUR, b)[i] = make_double2(__dadd_rn(p.x, nr), __dadd_rn(p.y, ni));
     acc = hypot(nr, ni);
   }
   const double part = block_sum(acc, sh);
@@ -710,7 +712,8 @@ __global__ void k_refresh1(Dev D) {
     if (D.opt_dsl) {
       ds[0] = __dadd_rn(a.x, cadd);
       ds[1] = __dadd_rn(a.y, cadd);
-      st2(deltasl, h, ds[0], ds[1]);
+      // only the converged iteration's deltasl is an output; the others only feed the masks below
+      if (conv) st2(deltasl, h, ds[0], ds[1]);
     }
     if (!conv) {
       const double t0 = __dsub_rn(ti.x, ds[0]), t1 = __dsub_rn(ti.y, ds[1]);
@@ -1059,7 +1062,11 @@ __global__ void k_commit(Dev D, int extrap) {
   const double2 p = p_load[i];
   p_load[i] = make_double2(__dadd_rn(p.x, cur.x), __dadd_rn(p.y, cur.y));
   D.sp(S_P_ICE, b)[i] = D.sp(S_DI, b)[i];
-  D.sp(S_P_OCEAN, b)[i] = D.sp(S_DSCUR, b)[i];
+  {
+    // dS_cur of the converged iteration: dS_prev + its load increment, as the update forms it
+    const double2 po = D.sp(S_P_OCEAN, b)[i];
+    D.sp(S_P_OCEAN, b)[i] = make_double2(__dadd_rn(po.x, ld.x), __dadd_rn(po.y, ld.y));
+  }
   D.sp(S_PREV_ICE, b)[i] = D.sp(S_ICELM, b)[i];
   if (extrap) D.sp(D.ss[b].hsel ? S_HA : S_HB, b)[i] = ld;
   if (D.ss[b].rec_ds) D.ss[b].rec_ds[i] = ld;
@@ -1266,7 +1273,7 @@ struct sle_batch {
   long long body_launches;   // kernels in one iteration of the graph body
   int iter_active = 0;       // host-driven loop: stepping slots not yet converged (timing units)
   // static field lists of the loop body
-  std::vector<FieldSpec> f_syn_sl, f_ana_ro, f_syn_sltot, f_ana_refresh;
+  std::vector<FieldSpec> f_syn_sl, f_ana_ro, f_syn_sltot, f_ana_refresh, f_ana_regr;
 };
 
 struct sle_solver {
@@ -1400,9 +1407,10 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   if (ng % 8 == 0) k_refresh2_x8<<<dim3(nb(ng / 8), B), 256, 0, st>>>(D);
   else k_refresh2<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
   prof_end(t, st);
-  // I* (only when the grounded mask changed), C* and tO for the next iteration; skipped for
-  // slots that converged
+  // C* and tO (when a cell of C* flipped), I* (when the grounded mask changed) for the next
+  // iteration; skipped for slots that converged
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_refresh.data(), (int)s->f_ana_refresh.size(), st));
+  SLE_TRY(sht_analysis_list(s->plan, s->f_ana_regr.data(), (int)s->f_ana_regr.size(), st));
   note_launch(2);
   t = prof_begin(PROF_DICE, act, st);
   k_dice<<<dim3(nb(nc), B), 256, 0, st>>>(D);
@@ -1757,10 +1765,15 @@ int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
     s->f_ana_ro.push_back(fprod(D.g(G_DSL, b), D.m(M_CSTAR, b), D.sp(S_ROLM, b), &sb->done));
     s->f_syn_sltot.push_back(fspec(D.g(G_DELTASL, b), D.sp(S_SLTOT, b), &sb->done));
   }
+  // Mixed precision: two lists by gate, C* and tO (open when a cell of C* flipped) and I* (open on
+  // a grounded-mask change, rare after the first iterations), so that the I* tensor-core launches
+  // end at once instead of running for C* / tO fields mixed in with them.  FP64 (four fields per
+  // launch, gates checked per block): one list.
+  const bool split_gates = cfg->precision == SLE_PREC_MIXED;
   for (int b = 0; b < nslot; ++b) {
     Scal* sb = s->sc + b;
-    s->f_ana_refresh.push_back(
-        fice(D.g(G_ICE, b), D.m(M_GR, b), D.sp(S_ICELM, b), &sb->converged, &sb->gr_changed));
+    (split_gates ? s->f_ana_regr : s->f_ana_refresh)
+        .push_back(fice(D.g(G_ICE, b), D.m(M_GR, b), D.sp(S_ICELM, b), &sb->converged, &sb->gr_changed));
     s->f_ana_refresh.push_back(fmask(D.m(M_CSTAR, b), D.sp(S_CSTARLM, b), &sb->converged, &sb->cs_changed));
     s->f_ana_refresh.push_back(fto(D.g(G_TINIT, b), D.m(M_CSTAR, b), D.m(M_CSTAR0, b), D.sp(S_TOLM, b),
                                    &sb->converged, &sb->cs_changed));
