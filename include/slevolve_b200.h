@@ -47,10 +47,11 @@ enum sle_status {
 };
 
 /* Arithmetic of the transforms.  FP64: FP64 end to end (matches the reference to 1e-9 m).
- * MIXED: Legendre contractions as split-TF32 (3xTF32) tensor-core GEMMs with FP32
- * accumulation (operands rounded to FP32 before the split) and FP32 row FFTs; the Legendre
- * recurrence (tables computed in FP64), Gauss nodes and weights, the degree-0 coefficient of
- * every analysis and synthesis and everything outside the transforms stay FP64. */
+ * MIXED: Legendre contractions as split-FP16 tensor-core GEMMs with FP32 accumulation (operands
+ * rounded to FP32, scaled by powers of two and split into FP16 hi + lo: 22 significant bits) and
+ * FP32 row FFTs; the Legendre recurrence (tables computed in FP64), Gauss nodes and weights, the
+ * degree-0 coefficient of every analysis and synthesis and everything outside the transforms stay
+ * FP64. */
 enum sle_precision { SLE_PREC_FP64 = 0, SLE_PREC_MIXED = 1 };
 
 enum sle_layout { SLE_LAYOUT_DENSE = 0, SLE_LAYOUT_PACKED = 1 };
@@ -71,11 +72,13 @@ int sle_sht_info(const sle_sht* plan, int* nlat, int* nlon, int* lmax, long long
 int sle_sht_work_fraction(const sle_sht* plan, double* frac);
 /* Gauss-Legendre nodes mu_j (north -> south) and weights, computed on the device (sht.py:65-101). */
 int sle_sht_gauss(const sle_sht* plan, double* mu_host, double* w_host);
-/* sht.py:274-302.  nfields grids -> nfields coefficient arrays (device pointers;
- * the pointer arrays themselves are host arrays of length nfields, 1 <= nfields <= 4). */
+/* sht.py:274-302.  nfields grids -> nfields coefficient arrays (device pointers; the pointer
+ * arrays themselves are host arrays of length nfields): 1 <= nfields <= 4 with the dense layout,
+ * <= 256 with the packed one. */
 int sle_sht_analysis(sle_sht* plan, int nfields, const double* const* grids_dev,
                      void* const* coeffs_dev, int layout, void* stream);
-/* sht.py:305-343.  Im of the m = 0 coefficients is ignored (irfft semantics). */
+/* sht.py:305-343.  Im of the m = 0 coefficients is ignored (irfft semantics).  Field counts as
+ * for sle_sht_analysis. */
 int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* coeffs_dev, int layout,
                       double* const* grids_dev, void* stream);
 /* Analysis of one grid into packed coefficients without any device allocation.  No counterpart
@@ -93,6 +96,18 @@ int sle_sht_analysis_noalloc(sle_sht* plan, const double* grid_dev, void* coeffs
 /* Select the arithmetic of sle_sht_analysis / sle_sht_synthesis on this plan (default FP64).
  * MIXED needs nlat a multiple of 64 and lmax <= 511; no counterpart in the reference. */
 int sle_sht_set_precision(sle_sht* plan, int precision);
+/* Launch shape of the mixed-precision transforms; no counterpart in the reference (its precedent
+ * is the Fortran OTF/GEMM hybrid switch chosen by field count, otf_kernels.inc:463-516).
+ * fields_per_launch 1..32 (a transform list is cut into launches of at most this many fields),
+ * stages 4 or 6 (pipeline depth of the tensor-core kernel), fold_rows 4 or 8 (rows per block of
+ * the row-FFT fold).  The results do not depend on it; slevolve_b200.tuning picks it by timing. */
+typedef struct {
+  int fields_per_launch;
+  int stages;
+  int fold_rows;
+} sle_mx_tuning;
+int sle_sht_set_tuning(sle_sht* plan, const sle_mx_tuning* t);
+int sle_sht_get_tuning(const sle_sht* plan, sle_mx_tuning* t);
 /* dense <-> packed conversion of one complex128 spectrum (device buffers) */
 int sle_sht_pack(sle_sht* plan, const void* dense_dev, void* packed_dev, void* stream);
 int sle_sht_unpack(sle_sht* plan, const void* packed_dev, void* dense_dev, void* stream);
@@ -263,6 +278,8 @@ int sle_batch_restore(sle_batch* b, int slot, const void* src, long long nbytes)
 /* copy one output of a slot's last step (as sle_solver_get) */
 int sle_batch_get(sle_batch* b, int slot, int field, void* dst, int dst_on_device);
 int sle_batch_stream(sle_batch* b, void** stream);
+/* launch shape of the batch's mixed-precision transforms (as sle_sht_set_tuning) */
+int sle_batch_set_tuning(sle_batch* b, const sle_mx_tuning* t);
 /* slots, mode capacity and the device bytes the batch's solver state occupies */
 int sle_batch_info(const sle_batch* b, int* nslots, int* max_modes, long long* device_bytes);
 

@@ -51,6 +51,10 @@ class SleEarth(C.Structure):
                 ("kTE2", C.c_double), ("hTE2", C.c_double), ("kE2", C.c_double)]
 
 
+class SleMxTuning(C.Structure):
+    _fields_ = [("fields_per_launch", C.c_int), ("stages", C.c_int), ("fold_rows", C.c_int)]
+
+
 class SleStepInfo(C.Structure):
     _fields_ = [("iter", C.c_int), ("numiter", C.c_int), ("status", C.c_int),
                 ("gr_reguess", C.c_int), ("gr_ice_analyses", C.c_int), ("xi", C.c_double),
@@ -77,6 +81,9 @@ _SIGS = {
     "sle_sht_analysis_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_sht_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "sle_sht_pack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sle_sht_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(SleMxTuning)]),
+    "sle_sht_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(SleMxTuning)]),
+    "sle_batch_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(SleMxTuning)]),
     "sle_sht_unpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sle_solver_create": (C.c_int, [C.POINTER(SleConfig), C.POINTER(SleEarth),
                                     C.POINTER(C.c_void_p)]),

@@ -132,6 +132,19 @@ class SolverBatch:
         _lib.check(self._L.sle_batch_release(self._h, int(slot)), "sle_batch_release")
         self.loaded[slot] = False
 
+    def autotune(self, nfields=None):
+        """Time the launch shapes of the mixed-precision transforms for lists of ``nfields`` fields
+        (default: one per slot, the width of the inner loop's synthesis and rO analysis) and use
+        the fastest (``slevolve_b200.tuning``).  Returns (shape, timings); FP64 batches: no-op."""
+        if self.precision != "mixed":
+            return None, []
+        from .tuning import apply, autotune
+
+        best, timings = autotune(self.lmax, nfields or self.nslots)
+        apply(self, best)
+        self.tuning = best
+        return best, timings
+
     # ------------------------------------------------------------- snapshots
     def snapshot_bytes(self) -> int:
         n = C.c_longlong()

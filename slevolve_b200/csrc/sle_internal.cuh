@@ -37,7 +37,8 @@ constexpr int SEG = 64;
 constexpr double SIG_THRESHOLD = 1.0e-35;
 // The legacy literal of spat2spec / spec2spat (SLEvolve sht.py:60-61), not sqrt(2).
 constexpr double SQRT2_LEGACY = 1.41421356;
-constexpr int MAXF = 4;   // fields per batched transform call (FP64 path)
+constexpr int MAXF = 4;   // fields per batched transform launch (FP64 path); per call with the dense layout
+constexpr int MAX_CALL_FIELDS = 256;   // fields per transform call with the packed layout
 constexpr int MX_MAXF = 32;          // fields per mixed-precision transform launch
 constexpr int MX_NMAX = 2 * MX_MAXF; // B-operand rows (Re, Im per field)
 
@@ -70,14 +71,19 @@ struct ShtDev {
   const float2* twf;          // [n2] FP32 twiddles of the mixed-precision row FFTs
   float* mx_xf;               // [MX_MAXF][nm][2][nh][2] folded FP32 rFFT: S, D (complex) per order
   float2* mx_gns;             // [MX_MAXF][nh][nm][2] north / south Legendre sums (synthesis)
-  float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (tile order)
+  float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (FP32, row-major)
   double* mx_s0;              // [MX_MAXF][nh] FP64 fold of the row sums (degree 0)
   int* mx_abort;              // raised by a tensor-core kernel whose wait timed out
   const int4* mx_ana_units;   // (m, span, first chunk, table slot) analysis units, most work first
   const int4* mx_syn_units;   // (m, latitude tile, chunks, table slot) synthesis units
   const int* mx_syn_seg;      // segment of each synthesis table slot
-  const uint32_t* mx_tab_ana; // Legendre tables: [slot][par][128][32] FP32, tile order
-  const uint32_t* mx_tab_syn;
+  // Legendre tables: [slot][par][hi, lo][128 rows][32] FP16 in the tensor cores' 64-byte-swizzled
+  // K-major tile order, each row scaled by 2^e (e per unit, parity and row: etab)
+  const uint16_t* mx_tab_ana;
+  const uint16_t* mx_tab_syn;
+  const short* mx_etab_ana;   // [unit][par][128]
+  const short* mx_etab_syn;
+  unsigned int* mx_bmax;      // [2][MX_MAXF] max |B| per field of the launch (float bits): analysis, synthesis
 };
 
 __device__ __forceinline__ bool field_gated_off(const ShtDev& P, int f) {
@@ -148,7 +154,6 @@ __device__ __forceinline__ void with_src_kind(int kind, const Body& body) {
 // Synthesis epilogue: epi_out[f] = grid[f] * epi_mul[f] when epi_out[f] is set.
 struct MxFieldArgs {
   int nf;
-  int ncols;                       // MMA N: 0 = smallest multiple of 16 >= 2 nf
   double* grid[MX_MAXF];           // analysis input / synthesis output
   double2* spec[MX_MAXF];          // analysis output / synthesis input (packed)
   const int* skip_set[MX_MAXF];
@@ -185,11 +190,18 @@ struct sle_sht {
   int* mx_abort;
   int4 *mx_ana_units, *mx_syn_units;
   int* mx_syn_seg;
-  uint32_t *mx_tab_ana, *mx_tab_syn;
+  uint16_t *mx_tab_ana, *mx_tab_syn;
+  short *mx_etab_ana, *mx_etab_syn;
+  unsigned int* mx_bmax;
   alignas(64) unsigned char mx_tmap[3][128];   // TMA maps of mx_xf (boxes of 8, 16, 32 fields)
   double mx_table_bytes;
   int n_ana_units, n_syn_units;
   int n_sm;                      // SMs of the device (persistent transform grid)
+  // launch shape of the mixed-precision transforms (sle_sht_set_tuning): fields per tensor-core
+  // launch, pipeline stages of the tensor-core kernel, rows per row-FFT block of the fold
+  int tune_fpl = sle::MX_MAXF;
+  int tune_stages = 6;
+  int tune_fold_rows = 8;
 };
 
 namespace sle {
@@ -221,6 +233,5 @@ int sht_mx_analysis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream
                     int prof_cls = PROF_LEG_ANA);
 int sht_mx_synthesis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st);
 int sht_mx_abort_flag(sle_sht* plan, int* flag);
-int mx_cols(int nf);
 int sht_unpack(sle_sht* plan, const double2* packed, double2* dense, cudaStream_t st);
 }  // namespace sle

@@ -640,7 +640,7 @@ static MxFieldArgs mx_args(const FieldSpec* fs, int nf) {
 int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st, int prof_cls) {
   if (n < 1) return SLE_OK;
   const bool mx = plan->precision == SLE_PREC_MIXED;
-  const int group = mx ? MX_MAXF : MAXF;
+  const int group = mx ? plan->tune_fpl : MAXF;
   // equal groups (the tensor-core kernels' cost depends on the launch, not on its width)
   const int ngroups = (n + group - 1) / group;
   for (int g = 0; g < ngroups; ++g) {
@@ -657,7 +657,7 @@ int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st,
 int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st) {
   if (n < 1) return SLE_OK;
   const bool mx = plan->precision == SLE_PREC_MIXED;
-  const int group = mx ? MX_MAXF : MAXF;
+  const int group = mx ? plan->tune_fpl : MAXF;
   const int ngroups = (n + group - 1) / group;
   for (int g = 0; g < ngroups; ++g) {
     const int lo = (int)((long long)n * g / ngroups), hi = (int)((long long)n * (g + 1) / ngroups);
@@ -703,7 +703,8 @@ static void plan_free(sle_sht* p) {
   void* ptrs[] = {p->mu, p->w, p->wn, p->ws, p->be, p->cf, p->moff, p->lidx, p->segoff,
                   p->seg_m, p->seg_l0, p->ana_order, p->seeds, p->tw, p->X, p->EO, p->istart,
                   p->packbuf, p->mx_xf, p->mx_twf, p->mx_gns, p->mx_bsyn, p->mx_s0, p->mx_abort,
-                  p->mx_ana_units, p->mx_syn_units, p->mx_syn_seg, p->mx_tab_ana, p->mx_tab_syn};
+                  p->mx_ana_units, p->mx_syn_units, p->mx_syn_seg, p->mx_tab_ana, p->mx_tab_syn,
+                  p->mx_etab_ana, p->mx_etab_syn, p->mx_bmax};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -982,26 +983,27 @@ extern "C" int sle_sht_analysis(sle_sht* plan, int nfields, const double* const*
     set_error("sle_sht_analysis: NULL argument");
     return SLE_ERR_BAD_ARG;
   }
-  for (int f = 0; f < nfields && f < MAXF; ++f)
+  const int maxf = (layout == SLE_LAYOUT_PACKED) ? MAX_CALL_FIELDS : MAXF;
+  if (nfields < 1 || nfields > maxf) {
+    set_error("sle_sht_analysis: nfields must be 1..%d for this layout", maxf);
+    return SLE_ERR_BAD_ARG;
+  }
+  for (int f = 0; f < nfields; ++f)
     if (!aligned16(grids_dev[f]) || !aligned16(coeffs_dev[f])) {
       set_error("sle_sht_analysis: device buffers must be non-NULL and 16-byte aligned");
       return SLE_ERR_BAD_ARG;
     }
-  if (nfields < 1 || nfields > MAXF) {
-    set_error("sle_sht_analysis: nfields must be 1..%d", MAXF);
-    return SLE_ERR_BAD_ARG;
-  }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  double2* outp[MAXF];
+  std::vector<double2*> outp(nfields);
   for (int f = 0; f < nfields; ++f)
     outp[f] = (layout == SLE_LAYOUT_PACKED) ? reinterpret_cast<double2*>(coeffs_dev[f])
                                             : plan->packbuf + (size_t)f * plan->d.ncoef;
-  FieldSpec fs[MAXF] = {};
+  std::vector<FieldSpec> fs(nfields, FieldSpec{});
   for (int f = 0; f < nfields; ++f) {
     fs[f].grid = const_cast<double*>(grids_dev[f]);
     fs[f].spec = outp[f];
   }
-  SLE_TRY(sht_analysis_list(plan, fs, nfields, st));
+  SLE_TRY(sht_analysis_list(plan, fs.data(), nfields, st));
   SLE_TRY(check_abort(plan));
   if (layout != SLE_LAYOUT_PACKED)
     for (int f = 0; f < nfields; ++f)
@@ -1015,17 +1017,18 @@ extern "C" int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* 
     set_error("sle_sht_synthesis: NULL argument");
     return SLE_ERR_BAD_ARG;
   }
-  for (int f = 0; f < nfields && f < MAXF; ++f)
+  const int maxf = (layout == SLE_LAYOUT_PACKED) ? MAX_CALL_FIELDS : MAXF;
+  if (nfields < 1 || nfields > maxf) {
+    set_error("sle_sht_synthesis: nfields must be 1..%d for this layout", maxf);
+    return SLE_ERR_BAD_ARG;
+  }
+  for (int f = 0; f < nfields; ++f)
     if (!aligned16(grids_dev[f]) || !aligned16(coeffs_dev[f])) {
       set_error("sle_sht_synthesis: device buffers must be non-NULL and 16-byte aligned");
       return SLE_ERR_BAD_ARG;
     }
-  if (nfields < 1 || nfields > MAXF) {
-    set_error("sle_sht_synthesis: nfields must be 1..%d", MAXF);
-    return SLE_ERR_BAD_ARG;
-  }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  const double2* inp[MAXF];
+  std::vector<const double2*> inp(nfields);
   for (int f = 0; f < nfields; ++f) {
     if (layout == SLE_LAYOUT_PACKED) {
       inp[f] = reinterpret_cast<const double2*>(coeffs_dev[f]);
@@ -1035,12 +1038,12 @@ extern "C" int sle_sht_synthesis(sle_sht* plan, int nfields, const void* const* 
       inp[f] = pb;
     }
   }
-  FieldSpec fs[MAXF] = {};
+  std::vector<FieldSpec> fs(nfields, FieldSpec{});
   for (int f = 0; f < nfields; ++f) {
     fs[f].grid = grids_dev[f];
     fs[f].spec = const_cast<double2*>(inp[f]);
   }
-  SLE_TRY(sht_synthesis_list(plan, fs, nfields, st));
+  SLE_TRY(sht_synthesis_list(plan, fs.data(), nfields, st));
   return check_abort(plan);
 }
 
@@ -1055,6 +1058,34 @@ extern "C" int sle_sht_set_precision(sle_sht* plan, int precision) {
   }
   if (precision == SLE_PREC_MIXED) SLE_TRY(sht_mx_prepare(plan));
   plan->precision = precision;
+  return SLE_OK;
+}
+
+extern "C" int sle_sht_set_tuning(sle_sht* plan, const sle_mx_tuning* t) {
+  if (!plan || !t) {
+    set_error("sle_sht_set_tuning: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (t->fields_per_launch < 1 || t->fields_per_launch > MX_MAXF || (t->stages != 4 && t->stages != 6) ||
+      (t->fold_rows != 4 && t->fold_rows != 8)) {
+    set_error("sle_sht_set_tuning: fields_per_launch 1..%d, stages 4 or 6, fold_rows 4 or 8 (got %d, %d, %d)",
+              MX_MAXF, t->fields_per_launch, t->stages, t->fold_rows);
+    return SLE_ERR_BAD_ARG;
+  }
+  plan->tune_fpl = t->fields_per_launch;
+  plan->tune_stages = t->stages;
+  plan->tune_fold_rows = t->fold_rows;
+  return SLE_OK;
+}
+
+extern "C" int sle_sht_get_tuning(const sle_sht* plan, sle_mx_tuning* t) {
+  if (!plan || !t) {
+    set_error("sle_sht_get_tuning: NULL argument");
+    return SLE_ERR_BAD_ARG;
+  }
+  t->fields_per_launch = plan->tune_fpl;
+  t->stages = plan->tune_stages;
+  t->fold_rows = plan->tune_fold_rows;
   return SLE_OK;
 }
 

@@ -2339,6 +2339,24 @@ extern "C" int sle_batch_restore(sle_batch* b, int slot, const void* src, long l
   return batch_restore(b, slot, src, nbytes);
 }
 
+extern "C" int sle_batch_set_tuning(sle_batch* b, const sle_mx_tuning* t) {
+  if (!b) {
+    set_error("sle_batch_set_tuning: NULL batch");
+    return SLE_ERR_BAD_ARG;
+  }
+  if (b->pending) {
+    set_error("sle_batch_set_tuning: a step is in flight");
+    return SLE_ERR_STATE;
+  }
+  SLE_TRY(sle_sht_set_tuning(b->plan, t));
+  // the captured inner-loop graph holds the old launch shape: capture it again at the next step
+  if (b->loop_exec) cudaGraphExecDestroy(b->loop_exec);
+  if (b->loop_graph) cudaGraphDestroy(b->loop_graph);
+  b->loop_exec = nullptr;
+  b->loop_graph = nullptr;
+  return SLE_OK;
+}
+
 extern "C" int sle_batch_set_reuse(sle_batch* b, int slot, void* ds_store, void* mask_store, int capacity,
                                    int valid) {
   if (!b) {

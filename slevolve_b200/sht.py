@@ -9,7 +9,7 @@ transform interface (SLEvolve ``python/slevolve/sht.py:43-46``, ``sht_ducc.py:20
 ``analysis`` returns V[l, m] = (-1)^m U[l, m] and ``synthesis`` reads V.  The ``*_device`` entry
 points always use U.
 
-``precision="mixed"`` runs the Legendre contractions as split-TF32 tensor-core GEMMs with FP32
+``precision="mixed"`` runs the Legendre contractions as split-FP16 tensor-core GEMMs with FP32
 accumulation (FP64 recurrence, row FFTs and degree-0 coefficient); the default ``"fp64"`` matches
 the reference to round-off.
 
@@ -129,7 +129,8 @@ class CudaSHT:
                              f"cuda:{self.device_index}")
 
     def analysis_device(self, grids, coeffs, layout=_lib.LAYOUT_DENSE):
-        """Analyse up to four CUDA float64 grids into CUDA complex128 tensors (in place)."""
+        """Analyse CUDA float64 grids into CUDA complex128 tensors (in place): up to four with the
+        dense layout, up to 256 with the packed one."""
         torch = _torch()
         self._check_device_args(grids, coeffs, layout, torch)
         n = len(grids)
@@ -139,7 +140,8 @@ class CudaSHT:
                    "sle_sht_analysis")
 
     def synthesis_device(self, coeffs, grids, layout=_lib.LAYOUT_DENSE):
-        """Synthesise up to four CUDA complex128 spectra into CUDA float64 grids (in place)."""
+        """Synthesise CUDA complex128 spectra into CUDA float64 grids (in place): up to four with
+        the dense layout, up to 256 with the packed one."""
         torch = _torch()
         self._check_device_args(grids, coeffs, layout, torch)
         n = len(grids)

@@ -1,8 +1,11 @@
-"""Mixed-precision transforms (split-TF32 tensor-core Legendre contraction) against the FP64 ones.
+"""Mixed-precision transforms (split-FP16 tensor-core Legendre contraction) against the FP64 ones.
 
-Bar: 1e-6 of the largest coefficient / grid value for the contraction (3xTF32 with FP32
-accumulation: about 1e-7 in practice), and the FP64 degree-0 coefficient of the analysis and the
-degree-0 term of the synthesis within 1e-13 relative (they bypass the tensor cores).
+Bar: 1e-6 of the largest coefficient / grid value for the contraction (power-of-two scaled FP16
+hi + lo operands, three products, FP32 accumulation: about 1e-7 in practice), and the FP64
+degree-0 coefficient of the analysis and the degree-0 term of the synthesis within 1e-13 relative
+(they bypass the tensor cores).  The operand scales make the relative error independent of the
+field's magnitude: fields scaled by 1e-20 and 1e+20 meet the same bar (the FP32 row FFTs bound the
+range).
 """
 
 import numpy as np
@@ -48,3 +51,39 @@ def test_mixed_degree0_only_is_fp64():
     amx = mx.analysis(g).copy()
     assert abs(amx[0, 0].real - a64[0, 0].real) <= 1e-13 * abs(a64[0, 0].real)
     assert np.abs(amx[1:, :]).max() <= 1e-6 * abs(a64[0, 0].real)
+
+
+@pytest.mark.parametrize("scale", [1e-20, 1e-8, 1e8, 1e20])
+def test_mixed_accuracy_independent_of_magnitude(scale):
+    """FP16's exponent range is narrow; the per-field and per-row power-of-two scales keep the
+    relative error of the contraction at the 1e-7 level for any field magnitude."""
+    from slevolve_b200.synthetic import band_limited_field
+
+    f64, mx = _pair(128, 127)
+    g = (band_limited_field(f64, 11, 1, 127, 2.0) + 0.5) * scale
+    a64 = f64.analysis(g).copy()
+    amx = mx.analysis(g).copy()
+    assert np.abs(amx - a64).max() <= REL_TC * np.abs(a64).max()
+    s64 = f64.synthesis(a64).copy()
+    smx = mx.synthesis(a64).copy()
+    assert np.abs(smx - s64).max() <= REL_TC * np.abs(s64).max()
+
+
+def test_mixed_fields_of_different_magnitudes_in_one_launch():
+    """Fields of one launch with magnitudes 1e-6 .. 1e6 (each field has its own scale)."""
+    import torch
+
+    from slevolve_b200 import _lib
+    from slevolve_b200.synthetic import band_limited_field
+
+    f64, mx = _pair(64, 63)
+    grids = [torch.tensor(band_limited_field(f64, 20 + i, 1, 63, 2.0) * 10.0 ** (3 * i - 6), device="cuda")
+             for i in range(5)]
+    out = {}
+    for sh in (f64, mx):
+        co = [torch.empty(sh.ncoef, dtype=torch.complex128, device="cuda") for _ in grids]
+        for i in range(0, len(grids), 4):
+            sh.analysis_device(grids[i:i + 4], co[i:i + 4], layout=_lib.LAYOUT_PACKED)
+        out[sh.precision] = [c.cpu().numpy() for c in co]
+    for a, b in zip(out["fp64"], out["mixed"]):
+        assert np.abs(a - b).max() <= REL_TC * np.abs(a).max()
