@@ -199,9 +199,7 @@ struct sle_sht {
   int n_sm;                      // SMs of the device (persistent transform grid)
   // launch shape of the mixed-precision transforms (sle_sht_set_tuning): fields per tensor-core
   // launch, pipeline stages of the tensor-core kernel, rows per row-FFT block of the fold
-  int tune_fpl = sle::MX_MAXF;
-  int tune_stages = 6;
-  int tune_fold_rows = 8;
+  int tune_fpl, tune_stages, tune_fold_rows;
 };
 
 namespace sle {

@@ -917,6 +917,10 @@ extern "C" int sle_sht_create(int nlat, int nlon, int lmax, sle_sht** out) {
   }
   sle_sht* p = new sle_sht();
   std::memset(p, 0, sizeof(sle_sht));
+  // launch shape of the mixed-precision transforms (sle_sht_set_tuning changes it)
+  p->tune_fpl = MX_MAXF;
+  p->tune_stages = 6;
+  p->tune_fold_rows = 8;
   int rc = plan_build(p, nlat, nlon, lmax);
   if (rc != SLE_OK) {
     plan_free(p);
