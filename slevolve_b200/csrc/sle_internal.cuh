@@ -83,7 +83,8 @@ struct ShtDev {
   const uint16_t* mx_tab_syn;
   const short* mx_etab_ana;   // [unit][par][128]
   const short* mx_etab_syn;
-  unsigned int* mx_bmax;      // [2][MX_MAXF] max |B| per field of the launch (float bits): analysis, synthesis
+  unsigned int* mx_bmax;      // [2][MX_MAXF][nm] max |B| (float bits): analysis per (field, band of 8 orders),
+                              // synthesis per (field, order)
 };
 
 __device__ __forceinline__ bool field_gated_off(const ShtDev& P, int f) {

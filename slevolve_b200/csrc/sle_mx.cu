@@ -15,8 +15,9 @@
 // (Q_l = mu Q_{l-1} + be_l Q_{l-2}, P~ = cf Q), rounded once to FP32 when the plan is prepared,
 // scaled per table row (a degree in the analysis, a latitude in the synthesis, per work unit) so
 // that the row's largest entry is just below 2^15, and stored split into FP16 hi + lo in the tensor
-// cores' shared-memory tile order.  The B operand of a launch is scaled per field the same way
-// (the producer kernel raises the field's max |B|) and split in shared memory.  An FP16 hi/lo pair
+// cores' shared-memory tile order.  The B operand is scaled the same way per field and order
+// (analysis: per band of 8 orders; the producer kernel raises each maximum) and split in shared
+// memory by the work unit (one order) that reads it.  An FP16 hi/lo pair
 // carries 22 significant bits, as a TF32 pair does; FP16's narrow exponent range is what the
 // power-of-two scales (undone exactly in FP64 by the epilogue) make up for.  The row FFTs of this
 // form run in FP32; the degree-0 terms are FP64: analysis computes U_00 from FP64 row sums of the
@@ -72,6 +73,7 @@ constexpr uint32_t SET_COLS = 256;            // two accumulator sets (units alt
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block ([row][32])
 constexpr int MAX_CTA_UNITS = 16;             // work units per CTA staged in shared memory
 constexpr int B_HEADROOM = 15;                // |x| * 2^e < 2^15: the FP16 hi of the largest entry stays finite
+constexpr int MBAND = 8;                      // orders sharing one analysis B scale (per field)
 static_assert(NSTAGE_MAX % 2 == 0, "a stage must always hold halves of one parity");
 static_assert(mx_smem(NSTAGE_MAX) <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
 static_assert(TILE_B == MX_NMAX * 64, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
@@ -208,19 +210,26 @@ __device__ __forceinline__ void split_h(float xs, uint16_t& hi, uint16_t& lo) {
   lo = __half_as_ushort(__float2half_rn(xs - __half2float(h)));
 }
 
-// 2^e as two factors that stay inside FP32's range for |e| <= 250.
-__device__ __forceinline__ float2 pow2_pair(int e) {
-  const int e1 = e / 2, e2 = e - e1;
-  return make_float2(__int_as_float((127 + e1) << 23), __int_as_float((127 + e2) << 23));
-}
+// 2^e as an FP32 number (-126 <= e <= 127) and 2^e as an FP64 number (|e| <= 1022): exact.
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }
+__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
 
-// Exponent e with max * 2^e < 2^15 (0 for a zero or non-finite maximum), clamped to +-250.
+// Exponent e of a B operand's scale: max * 2^e < 2^15 (0 for a zero or non-finite maximum).  The
+// B data are FP32 numbers (max < 2^128, so e >= -113); e is capped at 127 so that 2^e is an FP32
+// number, which leaves maxima below 2^-112 short of the full scale (their products are FP32
+// subnormals before any scaling).
 __device__ __forceinline__ int scale_exp(unsigned int maxbits) {
   const float m = __uint_as_float(maxbits);
   if (!(m > 0.0f) || !isfinite(m)) return 0;
   int E;
   frexpf(m, &E);   // m < 2^E
-  return max(-250, min(250, B_HEADROOM - E));
+  return min(127, B_HEADROOM - E);
+}
+
+// Index of a field's B maximum in the plan's table: analysis per (field, band of MBAND orders),
+// synthesis per (field, order), after the analysis part.
+__device__ __forceinline__ int bmax_index(bool syn, int f, int m, int nm) {
+  return syn ? (MX_MAXF + f) * nm + m : f * nm + m / MBAND;
 }
 
 // ------------------------------------------------------------------ bounded waits
@@ -327,7 +336,6 @@ struct Misc {
   uint32_t* tmem_holder;
   int* active;          // [MX_MAXF]
   int* any;
-  int* escale;          // [MX_MAXF] power-of-two exponent of each field's B operand
   int4* units;          // [MAX_CTA_UNITS]: this CTA's work units, staged by the prologue
   __device__ uint32_t b(int i) const { return smem_u32(bar + i); }
 };
@@ -338,12 +346,10 @@ __device__ __forceinline__ Misc misc_layout(const Smem& S) {
   m.tmem_holder = reinterpret_cast<uint32_t*>(p + 256);
   m.active = reinterpret_cast<int*>(p + 272);
   m.any = reinterpret_cast<int*>(p + 272 + 4 * MX_MAXF);
-  m.escale = reinterpret_cast<int*>(p + 416);
   m.units = reinterpret_cast<int4*>(p + 640);
   return m;
 }
-static_assert(416 >= 276 + 4 * MX_MAXF && 416 + 4 * MX_MAXF <= 640 && 640 + 16 * MAX_CTA_UNITS <= MISC_BYTES,
-              "misc shared memory layout");
+static_assert(276 + 4 * MX_MAXF <= 640 && 640 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory layout");
 
 // TMEM use (512 columns): two sets of 256, consecutive units alternate between them so that
 // the epilogue of one unit overlaps the MMAs of the next.  Every launch computes N = MX_NMAX
@@ -393,10 +399,8 @@ __device__ __forceinline__ void acc_read(uint32_t lanebase, int cb, double (&ev)
   }
 }
 
-// Common prologue: barriers, gates, the fields' B scales, TMEM.  Returns the TMEM base (all
-// threads).  bmax: the launch's per-field maxima of |B| (float bits) written by the producer kernel.
-__device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a, const int4* units, int nunits,
-                             const unsigned int* bmax) {
+// Common prologue: barriers, gates, TMEM.  Returns the TMEM base (all threads).
+__device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a, const int4* units, int nunits) {
   const int warp = threadIdx.x >> 5;
   if (threadIdx.x < MAX_CTA_UNITS) {
     const int u = blockIdx.x + threadIdx.x * gridDim.x;
@@ -415,10 +419,7 @@ __device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a,
     mbar_init(M.b(BAR_DRAIN), 1);
     fence_mbar_init();
   }
-  if (threadIdx.x < MX_MAXF) {
-    M.active[threadIdx.x] = (threadIdx.x < a.nf) && !field_off(a, threadIdx.x);
-    M.escale[threadIdx.x] = (threadIdx.x < a.nf) ? scale_exp(bmax[threadIdx.x]) : 0;
-  }
+  if (threadIdx.x < MX_MAXF) M.active[threadIdx.x] = (threadIdx.x < a.nf) && !field_off(a, threadIdx.x);
   if (warp == W_MMA) {
     tc_alloc(smem_u32(M.tmem_holder), TMEM_COLS);
     tc_relinquish();
@@ -561,8 +562,9 @@ __global__ void __launch_bounds__(128) k_tab_half(ShtDev P, const float* tmp, ui
 // ============================================================ Legendre contraction
 // Analysis B data of one parity: the TMA box of the folded FFT is [field][32 latitudes][re, im]
 // (8 bytes per entry) in the stage's raw area; rows 2f (re) / 2f+1 (im) of the B hi / lo tiles
-// get its FP16 split, scaled by the field's power of two.
-__device__ __forceinline__ void split_b_ana(const Smem& S, const Misc& M, int st, int nf, int tid) {
+// get its FP16 split.  Thread tid splits the entries of the fields f = tid / 32 + 4 u (u < 8),
+// scaled by sc[u] = 2^e of (field, order band).
+__device__ __forceinline__ void split_b_ana(const Smem& S, int st, int nf, int tid, const float (&sc)[8]) {
   const float2* box = reinterpret_cast<const float2*>(S.raw_ptr(st));
   uint16_t* hp = S.b_ptr(st, 0);
   uint16_t* lp = S.b_ptr(st, 1);
@@ -572,24 +574,37 @@ __device__ __forceinline__ void split_b_ana(const Smem& S, const Misc& M, int st
     const int f = e >> 5, k = e & 31;
     if (f >= nf) continue;
     const float2 v = box[e];
-    const float2 sc = pow2_pair(M.escale[f]);
     const int o0 = sw_off(2 * f, k), o1 = sw_off(2 * f + 1, k);
-    split_h(v.x * sc.x * sc.y, hp[o0], lp[o0]);
-    split_h(v.y * sc.x * sc.y, hp[o1], lp[o1]);
+    split_h(v.x * sc[u], hp[o0], lp[o0]);
+    split_h(v.y * sc[u], hp[o1], lp[o1]);
   }
 }
 
 // Synthesis B data of one parity: the raw block is [row][32] FP32 (row 2f / 2f+1 = Re / Im of
-// field f); the same split into the swizzled tiles.
-__device__ __forceinline__ void split_b_syn(const Smem& S, const Misc& M, int st, int nrow, int tid) {
+// field f); the same split into the swizzled tiles.  Thread tid splits the entries of the fields
+// f = tid / 64 + 2 i (i < 16), scaled by sc[i] = 2^e of (field, order).
+__device__ __forceinline__ void split_b_syn(const Smem& S, int st, int nrow, int tid, const float (&sc)[16]) {
   const float* raw = S.raw_ptr(st);
   uint16_t* hp = S.b_ptr(st, 0);
   uint16_t* lp = S.b_ptr(st, 1);
-  for (int e = tid; e < nrow * KC; e += 128) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int e = tid + 128 * i;
+    if (e >= nrow * KC) break;
     const int row = e >> 5, k = e & 31;
-    const float2 sc = pow2_pair(M.escale[row >> 1]);
     const int o = sw_off(row, k);
-    split_h(raw[e] * sc.x * sc.y, hp[o], lp[o]);
+    split_h(raw[e] * sc[i], hp[o], lp[o]);
+  }
+}
+
+// The B scales a splitter thread applies to the fields of unit order m (field slots beyond the
+// launch get 1).
+template <bool SYN, int NS>
+__device__ __forceinline__ void splitter_scales(const ShtDev& P, int nf, int m, int tid, float (&sc)[NS]) {
+#pragma unroll
+  for (int i = 0; i < NS; ++i) {
+    const int f = SYN ? (tid >> 6) + 2 * i : (tid >> 5) + 4 * i;
+    sc[i] = (f < nf) ? pow2f(scale_exp(__ldg(P.mx_bmax + bmax_index(SYN, f, m, P.nm)))) : 1.0f;
   }
 }
 
@@ -619,8 +634,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int L = P.lmax;
   const uint16_t* tab = SYN ? P.mx_tab_syn : P.mx_tab_ana;
   const short* etab = SYN ? P.mx_etab_syn : P.mx_etab_ana;
-  const uint32_t tmem = prologue(S, M, a, SYN ? P.mx_syn_units : P.mx_ana_units, nunits,
-                                 P.mx_bmax + (SYN ? MX_MAXF : 0));
+  const uint32_t tmem = prologue(S, M, a, SYN ? P.mx_syn_units : P.mx_ana_units, nunits);
   if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
     const int nrow = 2 * a.nf;
     if (warp == W_LOAD) {
@@ -701,6 +715,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int4 unit;
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
+        float sc[SYN ? 16 : 8];
+        splitter_scales<SYN>(P, a.nf, unit.x, tid, sc);
         for (int h = 0; h < 2 * nch; ++h, ++q) {
           if ((h & 1) != g) continue;
           const int st = q % NST;
@@ -711,8 +727,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             ok = false;
             break;
           }
-          if (SYN) split_b_syn(S, M, st, nrow, tid);
-          else split_b_ana(S, M, st, a.nf, tid);
+          if constexpr (SYN) split_b_syn(S, st, nrow, tid, sc);
+          else split_b_ana(S, st, a.nf, tid, sc);
           fence_proxy_async();
           __syncwarp();
           if (lane == 0) mbar_arrive(M.b(BAR_FULL + st));
@@ -747,12 +763,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           for (int q = 0; q < 8; ++q) {
             const int f = 8 * cb + q;
             if (f >= a.nf || !M.active[f]) continue;
-            // undo the scales: row (per parity) and field
-            const int eb = M.escale[f];
-            ve[2 * q] = ldexp(ve[2 * q], -(ea0 + eb));
-            ve[2 * q + 1] = ldexp(ve[2 * q + 1], -(ea0 + eb));
-            vo[2 * q] = ldexp(vo[2 * q], -(ea1 + eb));
-            vo[2 * q + 1] = ldexp(vo[2 * q + 1], -(ea1 + eb));
+            // undo the scales of the row (per parity) and of the field's B: exact powers of two
+            const int eb = scale_exp(__ldg(P.mx_bmax + bmax_index(SYN, f, m, P.nm)));
+            const double se = pow2d(-(ea0 + eb)), so = pow2d(-(ea1 + eb));
+            ve[2 * q] *= se;
+            ve[2 * q + 1] *= se;
+            vo[2 * q] *= so;
+            vo[2 * q + 1] *= so;
             if (SYN) {
               if (j < P.nh) {
                 float4* gq = reinterpret_cast<float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm + m;
@@ -863,45 +880,53 @@ __global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k
   }
   const SmemRows<N, float2> Z{A};
   float2* X = reinterpret_cast<float2*>(P.mx_xf) + (size_t)f * P.nm * P.nh * 2;
-  float bm = 0.0f;   // largest |component| this thread writes: the field's B scale
-  for (int e = threadIdx.x; e < NLAT * P.nm; e += NT) {
-    // consecutive threads: the latitudes of one order (one 32-byte sector of each X plane)
-    const int m = e / NLAT, q = e % NLAT, j = j0 + q;
-    float2 xr[2];
-    const float2 twm = (m > 0 && m < N) ? __ldg(P.twf + m) : make_float2(1.f, 0.f);
+  // consecutive threads: the latitudes of one order (one 32-byte sector of each X plane); the G
+  // lanes of an aligned lane group cover the MBAND orders of one scale band
+  constexpr int G = NLAT * MBAND;
+  static_assert(NT % 32 == 0 && G <= 32 && 32 % G == 0, "fold lane groups");
+  const int ne = NLAT * P.nm;
+  for (int e0 = 0; e0 < ne; e0 += NT) {
+    const int e = e0 + (int)threadIdx.x;
+    float bm = 0.0f;   // largest |component| this thread writes
+    if (e < ne) {
+      const int m = e / NLAT, q = e % NLAT, j = j0 + q;
+      float2 xr[2];
+      const float2 twm = (m > 0 && m < N) ? __ldg(P.twf + m) : make_float2(1.f, 0.f);
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = 2 * q + h;
-      const float2 z0 = Z(r, 0);
-      if (m == 0) {
-        xr[h] = make_float2(z0.x + z0.y, 0.f);
-      } else if (m == N) {
-        xr[h] = make_float2(z0.x - z0.y, 0.f);
-      } else {
-        const float2 zm = Z(r, m);
-        const float2 zn = Z(r, N - m);
-        const float2 zc = make_float2(zn.x, -zn.y);
-        const float2 ev = cscale(cadd(zm, zc), 0.5f);
-        const float2 dz = csub(zm, zc);
-        const float2 o = make_float2(0.5f * dz.y, -0.5f * dz.x);  // (zm - zc) / (2i)
-        xr[h] = cadd(ev, cmul(twm, o));
+      for (int h = 0; h < 2; ++h) {
+        const int r = 2 * q + h;
+        const float2 z0 = Z(r, 0);
+        if (m == 0) {
+          xr[h] = make_float2(z0.x + z0.y, 0.f);
+        } else if (m == N) {
+          xr[h] = make_float2(z0.x - z0.y, 0.f);
+        } else {
+          const float2 zm = Z(r, m);
+          const float2 zn = Z(r, N - m);
+          const float2 zc = make_float2(zn.x, -zn.y);
+          const float2 ev = cscale(cadd(zm, zc), 0.5f);
+          const float2 dz = csub(zm, zc);
+          const float2 o = make_float2(0.5f * dz.y, -0.5f * dz.x);  // (zm - zc) / (2i)
+          xr[h] = cadd(ev, cmul(twm, o));
+        }
       }
+      const double wn = P.wn[j], ws = P.ws[j];
+      const float2 an = cscale(xr[0], (float)wn), bs = cscale(xr[1], (float)ws);
+      if (m == 0) {
+        // S_0(j) in FP64: the weighted sums of the north and south rows of latitude j
+        P.mx_s0[(size_t)f * P.nh + j] = wn * rowtot[2 * q] + ws * rowtot[2 * q + 1];
+      }
+      const float2 sv = make_float2(an.x + bs.x, an.y + bs.y), dv = make_float2(an.x - bs.x, an.y - bs.y);
+      X[((size_t)m * 2 + 0) * P.nh + j] = sv;   // S (even l - m)
+      X[((size_t)m * 2 + 1) * P.nh + j] = dv;   // D (odd l - m)
+      bm = fmaxf(fmaxf(fabsf(sv.x), fabsf(sv.y)), fmaxf(fabsf(dv.x), fabsf(dv.y)));
     }
-    const double wn = P.wn[j], ws = P.ws[j];
-    const float2 an = cscale(xr[0], (float)wn), bs = cscale(xr[1], (float)ws);
-    if (m == 0) {
-      // S_0(j) in FP64: the weighted sums of the north and south rows of latitude j
-      P.mx_s0[(size_t)f * P.nh + j] = wn * rowtot[2 * q] + ws * rowtot[2 * q + 1];
-    }
-    const float2 sv = make_float2(an.x + bs.x, an.y + bs.y), dv = make_float2(an.x - bs.x, an.y - bs.y);
-    X[((size_t)m * 2 + 0) * P.nh + j] = sv;   // S (even l - m)
-    X[((size_t)m * 2 + 1) * P.nh + j] = dv;   // D (odd l - m)
-    bm = fmaxf(bm, fmaxf(fmaxf(fabsf(sv.x), fabsf(sv.y)), fmaxf(fabsf(dv.x), fabsf(dv.y))));
-  }
-  // the field's max |X| (non-negative floats order like their bit patterns)
+    // the band's max |X| over its lane group (non-negative floats order like their bit patterns)
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) bm = fmaxf(bm, __shfl_xor_sync(0xffffffffu, bm, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(P.mx_bmax + f, __float_as_uint(bm));
+    for (int o = G / 2; o > 0; o >>= 1) bm = fmaxf(bm, __shfl_xor_sync(0xffffffffu, bm, o));
+    if (threadIdx.x % G == 0 && e < ne && bm > 0.0f)
+      atomicMax(P.mx_bmax + bmax_index(false, f, e / NLAT, P.nm), __float_as_uint(bm));
+  }
 }
 
 // Inverse: north and south Legendre sums of field blockIdx.y (FP32, m <= lmax, 0 above; one
@@ -970,7 +995,7 @@ __global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArg
 // Re / Im of 1.41421356 U_f[l, m] rounded to FP32, k = the degree's index in its parity, row-major
 // (MX_NMAX x 32 per block); the tensor-core kernel splits it.  l = 0 is left out (the inverse
 // FFT adds it in FP64); degrees beyond lmax are zero.  Block (segment, group of 4 fields), 64
-// threads per field; each warp raises the field's max |B| (the split's scale).
+// threads per field; each warp raises the max |B| of (field, order) (the split's scale).
 __global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
   const int s = blockIdx.x;
   const int f = 4 * blockIdx.y + (threadIdx.x >> 6);
@@ -988,7 +1013,7 @@ __global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
   float bm = fmaxf(fabsf(re), fabsf(im));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) bm = fmaxf(bm, __shfl_xor_sync(0xffffffffu, bm, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(P.mx_bmax + MX_MAXF + f, __float_as_uint(bm));
+  if ((threadIdx.x & 31) == 0 && bm > 0.0f) atomicMax(P.mx_bmax + bmax_index(true, f, m, P.nm), __float_as_uint(bm));
 }
 
 size_t mx_fold_smem(const ShtDev& d, int nr) { return fft_smem_bytes(nr, d.n2, sizeof(float2)); }
@@ -1133,8 +1158,8 @@ int sht_mx_prepare(sle_sht* p) {
   SLE_TRY(mx_alloc(&p->mx_tab_syn, tab_s + 8));
   SLE_TRY(mx_alloc(&p->mx_etab_ana, (size_t)p->n_ana_units * 256 + 1));
   SLE_TRY(mx_alloc(&p->mx_etab_syn, (size_t)p->n_syn_units * 256 + 1));
-  SLE_TRY(mx_alloc(&p->mx_bmax, (size_t)2 * MX_MAXF));
-  SLE_CUDA(cudaMemset(p->mx_bmax, 0, 2 * MX_MAXF * sizeof(unsigned int)));
+  SLE_TRY(mx_alloc(&p->mx_bmax, (size_t)2 * MX_MAXF * d.nm));
+  SLE_CUDA(cudaMemset(p->mx_bmax, 0, (size_t)2 * MX_MAXF * d.nm * sizeof(unsigned int)));
   p->mx_table_bytes = (double)(tab_a + tab_s) * sizeof(uint16_t);
   d.twf = p->mx_twf;
   d.mx_xf = p->mx_xf;
@@ -1231,8 +1256,8 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t
   const MxFieldArgs& a = a0;
   SLE_TRY(mx_check_args(a, "mixed analysis"));
   const ShtDev& d = p->d;
-  // the fold raises each field's max |B| from zero
-  SLE_CUDA(cudaMemsetAsync(p->mx_bmax, 0, MX_MAXF * sizeof(unsigned int), st));
+  // the fold raises the max |B| of each (field, order band) from zero
+  SLE_CUDA(cudaMemsetAsync(p->mx_bmax, 0, (size_t)MX_MAXF * d.nm * sizeof(unsigned int), st));
   ProfToken t0 = prof_begin(PROF_FFT, a.nf, st);
 #define SLE_LAUNCH_MXF4(NN) \
   k_fold_mx<NN, 4><<<dim3(d.nh / 2, a.nf), fft_threads(4, NN), mx_fold_smem(d, 4), st>>>(d, a)
@@ -1266,7 +1291,7 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_
   SLE_TRY(mx_check_args(a, "mixed synthesis"));
   const ShtDev& d = p->d;
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[0]);
-  SLE_CUDA(cudaMemsetAsync(p->mx_bmax + MX_MAXF, 0, MX_MAXF * sizeof(unsigned int), st));
+  SLE_CUDA(cudaMemsetAsync(p->mx_bmax + (size_t)MX_MAXF * d.nm, 0, (size_t)MX_MAXF * d.nm * sizeof(unsigned int), st));
   ProfToken t0 = prof_begin(PROF_LEG_SYN, a.nf, st);
   k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
   const int gs = std::min(p->n_syn_units, p->n_sm);
