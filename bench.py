@@ -245,13 +245,17 @@ def load_peaks():
 # Algorithmic bytes per iterating slot of the inner loop's elementwise passes (one read of each
 # input, one write of each output; ng cells, nc packed coefficients): eq. B18 reads dI, the
 # previous load increment, the current increment and the viscous term and writes the sea-level
-# spectrum; the update reads dS_prev, rO, C* and tO and writes the increment and dS_cur; the
-# refresh reads dsl, T0 and ice plus the beta mask and writes deltasl, the ocean function and the
-# candidate grounded mask (an iteration that does not converge, marine test on); the C* refresh
-# reads the ocean, beta and C* masks and writes C*; dI reads I*_lm, the old I*_lm and p_ice and
-# writes dice and dI (only after a grounded-mask change; otherwise it returns at once).
-ELEMENTWISE = {"k_b18": ("nc", 80.0), "k_update": ("nc", 96.0), "k_refresh1": ("ng", 35.0),
-               "k_refresh2_x8": ("ng", 4.0), "k_dice": ("nc", 80.0)}
+# spectrum; the update reads dS_prev, rO, C*, tO and writes the increment (dS_cur only at its two
+# degree-2 entries); the refresh of an iteration that does not converge reads dsl, T0 and ice plus
+# the beta mask and writes the ocean function and the candidate grounded mask (marine test on;
+# deltasl is written by the converged iteration only); the C* refresh reads the ocean, beta and
+# C* masks and writes C*.
+ELEMENTWISE = {"k_b18": ("nc", 80.0), "k_update": ("nc", 80.0), "k_refresh1": ("ng", 27.0),
+               "k_refresh2_x8": ("ng", 4.0)}
+# Passes whose work depends on the iteration's outcome: dI (k_dice) reads I*_lm, the old I*_lm
+# and p_ice and writes dice and dI only after a grounded-mask change, and returns at once
+# otherwise, so no byte count per launch applies; its time is reported without a fraction.
+GATED_PASSES = ("k_dice",)
 # MMAs per product of the split contraction and the dense tensor rate they run at, as a fraction of
 # the measured BF16 GEMM rate
 TENSOR_RATE = 1.0
@@ -308,6 +312,12 @@ def step_shares(prof, nprof, peaks, nlat=512, lmax=511, modes=8):
                       "achieved": ach, "unit": "GB/s", "peak": peaks["hbm_gbs"], "frac": ach / peaks["hbm_gbs"]}
         weighted += ach / peaks["hbm_gbs"] * t
         tot += t
+    for name in GATED_PASSES:
+        c = prof.get(name)
+        if c and c["ms"] > 0:
+            elem[name] = {"ms_per_step": c["ms"] / nprof, "launches_per_step": c["launches"] / nprof,
+                          "slot_passes_per_step": c["fields"] / nprof, "frac": None,
+                          "note": "works only after a grounded-mask change; no byte count per launch"}
     out["elementwise"] = elem
     out["combined_frac"] = weighted / tot if tot > 0 else 0.0
     return out

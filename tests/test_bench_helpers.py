@@ -22,7 +22,7 @@ def _prof(nprof=3):
     per_step = {"k_fold_mx": (1.39, 32.3, 1034.7), "k_leg_tc<analysis of rO>": (0.69, 7.3, 234.7),
                 "k_leg_tc<other analyses>": (1.65, 25.0, 800.0),
                 "k_bsyn_mx + k_leg_tc<synthesis>": (0.97, 8.3, 266.7), "k_unfold_mx": (0.51, 8.3, 266.7),
-                "k_advance": (0.32, 1.0, 32.0), "k_update": (0.5, 7.0, 150.0)}
+                "k_advance": (0.32, 1.0, 32.0), "k_update": (0.5, 7.0, 150.0), "k_dice": (0.2, 7.0, 150.0)}
     return {k: {"ms": v[0] * nprof, "launches": v[1] * nprof, "fields": v[2] * nprof} for k, v in per_step.items()}
 
 
@@ -40,7 +40,10 @@ def test_step_shares_arithmetic():
     adv = 19 * 16.0 * ncoef * 32.0 / 0.32e-3 / 1e9
     assert sh["modal_advance"]["achieved"] == pytest.approx(adv, rel=1e-12)
     upd = sh["elementwise"]["k_update"]
-    assert upd["achieved"] == pytest.approx(96.0 * ncoef * 150.0 / 0.5e-3 / 1e9, rel=1e-12)
+    assert upd["achieved"] == pytest.approx(80.0 * ncoef * 150.0 / 0.5e-3 / 1e9, rel=1e-12)
+    # dI works only after a grounded-mask change: time reported, no fraction, not in the combination
+    assert sh["elementwise"]["k_dice"]["frac"] is None
+    assert sh["elementwise"]["k_dice"]["ms_per_step"] == pytest.approx(0.2)
     fr = [sh["transforms"]["frac"], sh["modal_advance"]["frac"], upd["frac"]]
     lo, hi = min(fr), max(fr)
     assert lo <= sh["combined_frac"] <= hi
