@@ -10,7 +10,7 @@ grounded-ice test and rotational feedback on), options ``opt={"dsl", "diag"}``,
 ``inner="extrap"``.  A step is one full time step of a member, inner fixed-point loop included.
 
 * ``value``  member-steps/s of a batch of B = 32 members stepped together in mixed precision
-  (split-FP16 tensor-core Legendre contractions, FP32 accumulation; everything else FP64).  The members differ in
+  (split-TF32 tensor-core Legendre contractions, FP32 accumulation; everything else FP64).  The members differ in
   Earth model (relaxation times scaled by a seeded factor log-uniform in [0.3, 3]) and ice
   amplitude (seeded, U[0.5, 1.5]) as in the uneven ensembles.  Ice resident in HBM, CUDA events
   on the batch's stream, L2 flushed (256 MiB write) between steps outside the timed intervals,
@@ -258,9 +258,9 @@ ELEMENTWISE = {"k_b18": ("nc", 80.0), "k_update": ("nc", 80.0), "k_refresh1": ("
 GATED_PASSES = ("k_dice",)
 # MMAs per product of the split contraction and the dense tensor rate they run at, as a fraction of
 # the measured BF16 GEMM rate
-TENSOR_RATE = 1.0
-TENSOR_NAME = "split-FP16 (FP16 hi + lo, three products)"
-TENSOR_PEAK = "the BF16 GEMM rate (dense FP16 runs at the same rate)"
+TENSOR_RATE = 0.5
+TENSOR_NAME = "split-TF32 (TF32 hi + lo, three products)"
+TENSOR_PEAK = "half the BF16 GEMM rate (the dense TF32 rate)"
 
 
 def step_shares(prof, nprof, peaks, nlat=512, lmax=511, modes=8):
@@ -765,9 +765,9 @@ def run_ours(a):
 
     line = {"metric": METRIC, "value": value, "unit": "member-steps/s", "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": t_max / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp16x3+f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "tf32x3+f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": [512, 1024], "lmax": 511, "modes": 8,
-                       "dt_years": 200.0, "precision": "mixed (split-FP16 Legendre contractions with FP32 accumulation, FP64 elsewhere)",
+                       "dt_years": 200.0, "precision": "mixed (split-TF32 Legendre contractions with FP32 accumulation, FP64 elsewhere)",
                        "batch_members": B, "first_step": k0, "opt": list(OPTS), "inner": INNER,
                        "max_numiter_per_batch_step": float(np.mean(numiter)),
                        "l2": ("value: flushed between steps (256 MiB write, outside the timed intervals); "

@@ -47,9 +47,8 @@ enum sle_status {
 };
 
 /* Arithmetic of the transforms.  FP64: FP64 end to end (matches the reference to 1e-9 m).
- * MIXED: Legendre contractions as split-FP16 tensor-core GEMMs with FP32 accumulation (operands
- * rounded to FP32, scaled by powers of two and split into FP16 hi + lo: 22 significant bits) and
- * FP32 row FFTs; the Legendre recurrence (tables computed in FP64), Gauss nodes and weights, the
+ * MIXED: Legendre contractions as split-TF32 (3xTF32) tensor-core GEMMs with FP32 accumulation
+ * (operands rounded to FP32, then split into TF32 hi + lo: 22 significant bits) and FP32 row FFTs; the Legendre recurrence (tables computed in FP64), Gauss nodes and weights, the
  * degree-0 coefficient of every analysis and synthesis and everything outside the transforms stay
  * FP64. */
 enum sle_precision { SLE_PREC_FP64 = 0, SLE_PREC_MIXED = 1 };
@@ -99,7 +98,7 @@ int sle_sht_set_precision(sle_sht* plan, int precision);
 /* Launch shape of the mixed-precision transforms; no counterpart in the reference (its precedent
  * is the Fortran OTF/GEMM hybrid switch chosen by field count, otf_kernels.inc:463-516).
  * fields_per_launch 1..32 (a transform list is cut into launches of at most this many fields),
- * stages 4 or 6 (pipeline depth of the tensor-core kernel), fold_rows 4 or 8 (rows per block of
+ * stages 2 or 4 (pipeline depth of the tensor-core kernel), fold_rows 4 or 8 (rows per block of
  * the row-FFT fold).  The results do not depend on it; slevolve_b200.tuning picks it by timing. */
 typedef struct {
   int fields_per_launch;

@@ -71,20 +71,14 @@ struct ShtDev {
   const float2* twf;          // [n2] FP32 twiddles of the mixed-precision row FFTs
   float* mx_xf;               // [MX_MAXF][nm][2][nh][2] folded FP32 rFFT: S, D (complex) per order
   float2* mx_gns;             // [MX_MAXF][nh][nm][2] north / south Legendre sums (synthesis)
-  float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (FP32, row-major)
+  float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (FP32, tile order)
   double* mx_s0;              // [MX_MAXF][nh] FP64 fold of the row sums (degree 0)
   int* mx_abort;              // raised by a tensor-core kernel whose wait timed out
   const int4* mx_ana_units;   // (m, span, first chunk, table slot) analysis units, most work first
   const int4* mx_syn_units;   // (m, latitude tile, chunks, table slot) synthesis units
   const int* mx_syn_seg;      // segment of each synthesis table slot
-  // Legendre tables: [slot][par][hi, lo][128 rows][32] FP16 in the tensor cores' 64-byte-swizzled
-  // K-major tile order, each row scaled by 2^e (e per unit, parity and row: etab)
-  const uint16_t* mx_tab_ana;
-  const uint16_t* mx_tab_syn;
-  const short* mx_etab_ana;   // [unit][par][128]
-  const short* mx_etab_syn;
-  unsigned int* mx_bmax;      // [2][MX_MAXF][nm] max |B| (float bits): analysis per (field, band of 8 orders),
-                              // synthesis per (field, order)
+  const uint32_t* mx_tab_ana; // Legendre tables: [slot][par][128][32] FP32, 128-byte-swizzled tile order
+  const uint32_t* mx_tab_syn;
 };
 
 __device__ __forceinline__ bool field_gated_off(const ShtDev& P, int f) {
@@ -191,9 +185,7 @@ struct sle_sht {
   int* mx_abort;
   int4 *mx_ana_units, *mx_syn_units;
   int* mx_syn_seg;
-  uint16_t *mx_tab_ana, *mx_tab_syn;
-  short *mx_etab_ana, *mx_etab_syn;
-  unsigned int* mx_bmax;
+  uint32_t *mx_tab_ana, *mx_tab_syn;
   alignas(64) unsigned char mx_tmap[3][128];   // TMA maps of mx_xf (boxes of 8, 16, 32 fields)
   double mx_table_bytes;
   int n_ana_units, n_syn_units;

@@ -1,5 +1,5 @@
-// Mixed-precision Gauss-Legendre transforms for sm_100a: split-FP16 Legendre contractions on the
-// 5th-generation tensor cores (tcgen05.mma kind::f16 with FP32 accumulators in TMEM), FP64
+// Mixed-precision Gauss-Legendre transforms for sm_100a: split-TF32 ("3xTF32") Legendre
+// contractions on the 5th-generation tensor cores (tcgen05.mma, accumulators in TMEM), FP64
 // everywhere else the precision of the step depends on.
 //
 // Same transform as the FP64 path and the reference (SLEvolve python/slevolve/sht.py:274-343):
@@ -8,29 +8,25 @@
 // Per order m both are real GEMMs over the complex fields of a launch (2 columns per field):
 //   analysis   D[l][n] = sum_j  P[l][j]  B[n][j],   B = folded FFT (S for even, D for odd l-m)
 //   synthesis  D[j][n] = sum_l  P[l][j]  B[n][l],   B = coefficients of one parity
-// with each operand scaled by a power of two and split into FP16 hi + lo, and
-// D += Ahi Bhi + Ahi Blo + Alo Bhi in FP32.
+// with each operand split into TF32 hi + lo and D += Ahi Bhi + Ahi Blo + Alo Bhi in FP32.
 //
 // Precision: the Legendre values come from the FP64 recurrence of the plan
-// (Q_l = mu Q_{l-1} + be_l Q_{l-2}, P~ = cf Q), rounded once to FP32 when the plan is prepared,
-// scaled per table row (a degree in the analysis, a latitude in the synthesis, per work unit) so
-// that the row's largest entry is just below 2^15, and stored split into FP16 hi + lo in the tensor
-// cores' shared-memory tile order.  The B operand is scaled the same way per field and order
-// (analysis: per band of 8 orders; the producer kernel raises each maximum) and split in shared
-// memory by the work unit (one order) that reads it.  An FP16 hi/lo pair
-// carries 22 significant bits, as a TF32 pair does; FP16's narrow exponent range is what the
-// power-of-two scales (undone exactly in FP64 by the epilogue) make up for.  The row FFTs of this
-// form run in FP32; the degree-0 terms are FP64: analysis computes U_00 from FP64 row sums of the
-// input grid, synthesis leaves l = 0 out of the tensor-core sum and adds its uniform contribution
-// to the output grid in FP64.  Every launch computes all MX_NMAX columns with the same
-// accumulation structure, so a field's result does not depend on the other fields of its launch.
+// (Q_l = mu Q_{l-1} + be_l Q_{l-2}, P~ = cf Q), rounded once to FP32 when the plan is prepared
+// and stored in the tensor cores' shared-memory tile order; the kernel splits them, and the B
+// operands, into TF32 hi + lo in shared memory.  The row FFTs of this form run in FP32; the
+// degree-0 terms are FP64: analysis computes U_00 from FP64 row sums of the input grid,
+// synthesis leaves l = 0 out of the tensor-core sum and adds its uniform contribution to the
+// output grid in FP64.  The tensor core's FP32 accumulation truncates, so the large products
+// (Ahi Bhi) and the small ones go to separate TMEM accumulators that the epilogue adds in FP64.
+// Every launch computes all MX_NMAX columns with the same accumulation structure, so a field's
+// result does not depend on the other fields of its launch or on the launch shape.
 //
-// Kernel structure (persistent: one CTA per SM over the work units, 14 warps, 4 or 6 stages of
-// one half each, a half being one parity of one 32-wide K chunk):
-//   warp 13     loader: per half, one bulk copy of the FP16 A tiles (hi and lo, 16 KB) and the
-//               raw B data (analysis: one 4-D TMA tensor load of the folded FFT; synthesis: one
-//               bulk copy) into stage q % stages
-//   warps 4-11  splitters, group g = parity g: B -> scaled FP16 hi / lo tiles
+// Kernel structure (persistent: one CTA per SM over the work units, 14 warps, 2 or 4 stages of
+// one half each (a launch-shape choice), a half being one parity of one 32-wide K chunk):
+//   warp 13     loader: per half, one bulk copy of the FP32 A tile (16 KB) and the B data
+//               (analysis: one 4-D TMA tensor load of the folded FFT; synthesis: one bulk copy)
+//               into stage q % stages
+//   warps 4-11  splitters, group g = parity g: A and B -> TF32 hi / lo tiles
 //   warp 12     allocates TMEM and issues the MMAs from one thread, unit i into TMEM set i & 1
 //   warps 0-3   epilogue: read set i & 1 out of TMEM while the MMAs of unit i + 1 run
 // Stages hand over through mbarriers; tcgen05.commit releases a stage when its MMAs are done.
@@ -42,7 +38,6 @@
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
-#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -51,15 +46,13 @@
 namespace sle {
 namespace {
 
-constexpr int KC = 32;                        // K elements per chunk: one 64-byte row of FP16
-constexpr int TILE_H = 128 * KC;              // halfs of one A tile (128 rows x 32)
-constexpr int TILE_A = TILE_H * 2;            // 8 KB
-constexpr int SLOT_HALFS = 4 * TILE_H;        // Legendre table slot: [parity][hi, lo] A tiles
-constexpr int TILE_F = 128 * KC;              // floats of one FP32 A tile of the set-up table
-constexpr int TILE_B = MX_NMAX * 2 * KC;      // 4 KB: MX_NMAX rows of one B tile (hi or lo)
-constexpr int RAW_BYTES = MX_NMAX * KC * 4;   // 8 KB: landing area of one half's FP32 B data
-constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B + RAW_BYTES;   // A hi / lo, B hi / lo, raw B
-constexpr int NSTAGE_MAX = 6;                 // pipeline stages: 4 or 6 (a launch-time choice)
+constexpr int KC = 32;                        // K elements per chunk: one 128-byte row of TF32
+constexpr int TILE_F = 128 * KC;              // words of one A tile (128 rows x 32)
+constexpr int TILE_A = TILE_F * 4;            // 16 KB
+constexpr int SLOT_WORDS = 2 * TILE_F;        // Legendre table slot: FP32 A tiles of both parities
+constexpr int TILE_B = MX_NMAX * 128;         // MX_NMAX rows x 128 bytes = 8 KB
+constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;   // one parity of a chunk: A hi / lo, B hi / lo
+constexpr int NSTAGE_MAX = 4;                 // pipeline stages: 2 or 4 (a launch-time choice)
 constexpr int MISC_BYTES = 1024;              // barriers + bookkeeping
 constexpr int mx_smem(int nst) { return 1024 + nst * STAGE_BYTES + MISC_BYTES; }
 constexpr int W_SPL = 4;                      // warps 4..11: splitters (two groups of four)
@@ -70,14 +63,15 @@ constexpr int ANA_SPAN = 256;                 // degrees per analysis unit (128 
 constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wait gives up
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t SET_COLS = 256;            // two accumulator sets (units alternate)
-constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block ([row][32])
-constexpr int MAX_CTA_UNITS = 16;             // work units per CTA staged in shared memory
-constexpr int B_HEADROOM = 15;                // |x| * 2^e < 2^15: the FP16 hi of the largest entry stays finite
-constexpr int MBAND = 8;                      // orders sharing one analysis B scale (per field)
+constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
+constexpr int MAX_CTA_UNITS = 16;            // work units per CTA staged in shared memory
+constexpr int NCOLS = MX_NMAX;                // accumulator columns of every launch (2 per field slot)
+static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
+
 static_assert(NSTAGE_MAX % 2 == 0, "a stage must always hold halves of one parity");
 static_assert(mx_smem(NSTAGE_MAX) <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
-static_assert(TILE_B == MX_NMAX * 64, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
-static_assert(4 * MX_NMAX <= (int)SET_COLS, "full-width accumulators exceed a TMEM set");
+static_assert(TILE_B == MX_NMAX * 128, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
+static_assert(4 * MX_NMAX <= (int)SET_COLS && 2 * MX_NMAX <= 256, "full-width accumulators exceed a TMEM set");
 
 // ------------------------------------------------------------------ PTX wrappers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -133,6 +127,10 @@ __device__ __forceinline__ void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 // AND of `v` over the `n` threads that reach named barrier `id` (all of them must).
 __device__ __forceinline__ bool bar_and(int id, int n, bool v) {
   uint32_t r;
@@ -161,12 +159,12 @@ __device__ __forceinline__ void tc_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                : "memory");
 }
-// D[tmem] (+)= A[smem desc] * B[smem desc]; M = 128, N from the instruction descriptor, K = 16.
-__device__ __forceinline__ void tc_mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+// D[tmem] (+)= A[smem desc] * B[smem desc]; M = 128, N from the instruction descriptor, K = 8.
+__device__ __forceinline__ void tc_mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   const uint32_t z = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
       "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
       : "memory");
 }
@@ -180,56 +178,31 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
 }
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// Shared-memory matrix descriptor of a K-major tile in the 64-byte swizzle layout: rows of
-// 64 bytes (32 FP16), 8-row groups 512 bytes apart, tile base 512-byte aligned.  The K sub-block
-// kk (16 FP16 = 32 bytes) of one MMA starts 32*kk bytes into the row.
-__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
-  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+// Shared-memory matrix descriptor of a K-major tile in the 128-byte swizzle layout: rows of
+// 128 bytes (32 TF32), 8-row groups 1024 bytes apart, tile base 1024-byte aligned.  The K
+// sub-block kk (8 TF32 = 32 bytes) of one MMA starts 32*kk bytes into the row.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
-// Instruction descriptor: D F32, A and B FP16, both K-major, M x N.
-__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
-  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// Instruction descriptor: D F32, A and B TF32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// Offset (in halfs) of (row, k), k < 32, in a 64-byte-swizzled K-major tile: the 16-byte chunk
-// k / 8 of the row is stored at chunk (k / 8) ^ ((row / 2) % 4).
+// Offset (in 4-byte elements) of (row, k), k < 32, in a 128-byte-swizzled K-major tile.
 __host__ __device__ __forceinline__ int sw_off(int row, int k) {
-  return row * KC + ((((k >> 3) ^ ((row >> 1) & 3)) << 3) | (k & 7));
+  return row * KC + ((((k >> 2) ^ (row & 7)) << 2) | (k & 3));
 }
 
 // ------------------------------------------------------------- precision splits
-// xs = hi + lo + r with hi the nearest FP16 of xs and lo the nearest FP16 of the exact remainder
-// xs - hi: |r| <= 2^-22 |xs| while xs and the remainder stay in FP16's normal range; below it the
-// split keeps an absolute accuracy of 2^-25 (FP16's subnormal spacing is 2^-24).  The operands
-// are scaled by powers of two so that their largest entry is just below 2^15.
-__device__ __forceinline__ void split_h(float xs, uint16_t& hi, uint16_t& lo) {
-  const __half h = __float2half_rn(xs);
-  hi = __half_as_ushort(h);
-  lo = __half_as_ushort(__float2half_rn(xs - __half2float(h)));
-}
-
-// 2^e as an FP32 number (-126 <= e <= 127) and 2^e as an FP64 number (|e| <= 1022): exact.
-__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }
-__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
-
-// Exponent e of a B operand's scale: max * 2^e < 2^15 (0 for a zero or non-finite maximum).  The
-// B data are FP32 numbers (max < 2^128, so e >= -113); e is capped at 127 so that 2^e is an FP32
-// number, which leaves maxima below 2^-112 short of the full scale (their products are FP32
-// subnormals before any scaling).
-__device__ __forceinline__ int scale_exp(unsigned int maxbits) {
-  const float m = __uint_as_float(maxbits);
-  if (!(m > 0.0f) || !isfinite(m)) return 0;
-  int E;
-  frexpf(m, &E);   // m < 2^E
-  return min(127, B_HEADROOM - E);
-}
-
-// Index of a field's B maximum in the plan's table: analysis per (field, band of MBAND orders),
-// synthesis per (field, order), after the analysis part.
-__device__ __forceinline__ int bmax_index(bool syn, int f, int m, int nm) {
-  return syn ? (MX_MAXF + f) * nm + m : f * nm + m / MBAND;
+// x = hi + lo with hi the nearest TF32 of x (ties away from zero) and lo the nearest TF32 of
+// the exact remainder: |x - hi - lo| <= 2^-22 |x| for normal x.
+__device__ __forceinline__ void split_f32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
+  const float r = x - __uint_as_float(hi);
+  lo = (__float_as_uint(r) + 0x1000u) & 0xFFFFE000u;
 }
 
 // ------------------------------------------------------------------ bounded waits
@@ -297,24 +270,19 @@ __device__ __forceinline__ bool field_off(const MxFieldArgs& a, int f) {
   return false;
 }
 
-// Shared memory of a stage (one parity of one chunk): A tiles [hi][lo] (copied from the table,
-// already split), B tiles [hi][lo] (written by the splitters), then the raw FP32 B data the
-// loader lands for them.
+// Shared memory of a stage (one parity of one chunk): A tiles [hi][lo] (the parity's FP32
+// Legendre tile lands in hi and is split in place), then B tiles [hi][lo] (the raw B data lands
+// in lo).
 struct Smem {
   uint8_t* base;        // generic pointer, 1024-aligned
   uint32_t sbase;       // shared-window address of base
   int nst;              // stages of this launch
   __device__ uint32_t a_tile(int stage, int lo) const { return sbase + stage * STAGE_BYTES + lo * TILE_A; }
+  __device__ uint8_t* a_ptr(int stage, int lo) const { return base + stage * STAGE_BYTES + lo * TILE_A; }
   __device__ uint32_t b_tile(int stage, int lo) const {
     return sbase + stage * STAGE_BYTES + 2 * TILE_A + lo * TILE_B;
   }
-  __device__ uint16_t* b_ptr(int stage, int lo) const {
-    return reinterpret_cast<uint16_t*>(base + stage * STAGE_BYTES + 2 * TILE_A + lo * TILE_B);
-  }
-  __device__ uint32_t raw(int stage) const { return sbase + stage * STAGE_BYTES + 2 * TILE_A + 2 * TILE_B; }
-  __device__ const float* raw_ptr(int stage) const {
-    return reinterpret_cast<const float*>(base + stage * STAGE_BYTES + 2 * TILE_A + 2 * TILE_B);
-  }
+  __device__ uint8_t* b_ptr(int stage, int lo) const { return base + stage * STAGE_BYTES + 2 * TILE_A + lo * TILE_B; }
   __device__ uint8_t* misc() const { return base + nst * STAGE_BYTES; }
 };
 
@@ -330,7 +298,7 @@ __device__ __forceinline__ Smem smem_layout(uint8_t* raw, int nst) {
 // room for the largest stage count.
 enum { BAR_FULL = 0, BAR_EMPTY = NSTAGE_MAX, BAR_RAW = 2 * NSTAGE_MAX, BAR_ACCUM = 3 * NSTAGE_MAX,
        BAR_TFREE = 3 * NSTAGE_MAX + 2, BAR_DRAIN = 3 * NSTAGE_MAX + 4, NBAR = 3 * NSTAGE_MAX + 5 };
-static_assert(NBAR <= 32, "barrier area too small");
+static_assert(NBAR * 8 <= 192, "barrier area too small");
 struct Misc {
   uint64_t* bar;
   uint32_t* tmem_holder;
@@ -342,14 +310,13 @@ struct Misc {
 __device__ __forceinline__ Misc misc_layout(const Smem& S) {
   uint8_t* p = S.misc();
   Misc m;
-  m.bar = reinterpret_cast<uint64_t*>(p);                      // NBAR barriers (256 bytes)
-  m.tmem_holder = reinterpret_cast<uint32_t*>(p + 256);
-  m.active = reinterpret_cast<int*>(p + 272);
-  m.any = reinterpret_cast<int*>(p + 272 + 4 * MX_MAXF);
-  m.units = reinterpret_cast<int4*>(p + 640);
+  m.bar = reinterpret_cast<uint64_t*>(p);                      // 17 barriers
+  m.tmem_holder = reinterpret_cast<uint32_t*>(p + 192);
+  m.active = reinterpret_cast<int*>(p + 256);
+  m.any = reinterpret_cast<int*>(p + 256 + 4 * MX_MAXF);
+  m.units = reinterpret_cast<int4*>(p + 512);
   return m;
 }
-static_assert(276 + 4 * MX_MAXF <= 640 && 640 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory layout");
 
 // TMEM use (512 columns): two sets of 256, consecutive units alternate between them so that
 // the epilogue of one unit overlaps the MMAs of the next.  Every launch computes N = MX_NMAX
@@ -358,22 +325,22 @@ static_assert(276 + 4 * MX_MAXF <= 640 && 640 + 16 * MAX_CTA_UNITS <= MISC_BYTES
 // main accumulator (Ahi*Bhi of every chunk) at 2Np and the correction accumulator (Ahi*Blo +
 // Alo*Bhi) right after it at 2Np + N, so that Ahi*Bhi and Ahi*Blo are one MMA of 2N columns over
 // the adjacent B hi and B lo tiles (A hi read from shared memory once per K step).
-constexpr int NCOLS = MX_NMAX;
+static_assert(4 * NCOLS <= (int)SET_COLS, "full-width accumulators exceed a TMEM set");
 
-// MMAs of one parity `par` of chunk k of a unit (stage st) into the set at `set_base`: two K
-// steps of 16.  The K sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the
+// MMAs of one parity `par` of chunk k of a unit (stage st) into the set at `set_base`: four K
+// steps of 8.  The K sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the
 // descriptor's start-address field.
 __device__ __forceinline__ void mma_half(const Smem& S, uint32_t set_base, int st, int par, int k) {
-  const uint64_t ah = sdesc_sw64(S.a_tile(st, 0)), al = sdesc_sw64(S.a_tile(st, 1));
-  const uint64_t bh = sdesc_sw64(S.b_tile(st, 0));
-  const uint32_t idesc = idesc_f16(128, NCOLS), idesc2 = idesc_f16(128, 2 * NCOLS);
+  const uint64_t ah = sdesc_sw128(S.a_tile(st, 0)), al = sdesc_sw128(S.a_tile(st, 1));
+  const uint64_t bh = sdesc_sw128(S.b_tile(st, 0));
+  const uint32_t idesc = idesc_tf32(128, NCOLS), idesc2 = idesc_tf32(128, 2 * NCOLS);
   // B hi rows [0, N) and B lo rows [0, N) are 2N consecutive rows (TILE_B = N rows)
   const uint32_t dm = set_base + (uint32_t)(2 * NCOLS * par), dc = dm + (uint32_t)NCOLS;
 #pragma unroll
-  for (int kk = 0; kk < KC / 16; ++kk) {
+  for (int kk = 0; kk < KC / 8; ++kk) {
     const uint64_t d = (uint64_t)(2 * kk);
-    tc_mma_f16(dm, ah + d, bh + d, idesc2, (k == 0 && kk == 0) ? 0u : 1u);   // [main | corr]
-    tc_mma_f16(dc, al + d, bh + d, idesc, 1u);
+    tc_mma_tf32(dm, ah + d, bh + d, idesc2, (k == 0 && kk == 0) ? 0u : 1u);   // [main | corr]
+    tc_mma_tf32(dc, al + d, bh + d, idesc, 1u);
   }
 }
 
@@ -456,17 +423,15 @@ __device__ __noinline__ void mbar_wait_drain(uint32_t a, uint32_t parity) {
 }
 
 // ===================================================== Legendre tables (once per plan)
-// The A operand of every chunk is precomputed from the FP64 recurrence: first rounded to FP32 in
-// a set-up table of plain row-major tiles (slot = [par0][par1], each 128 rows x 32), then
-// (k_tab_half) scaled per row by a power of two so that the row's largest entry is just below
-// 2^15, split into FP16 hi + lo and stored in the tile order of the shared-memory stage; the
-// exponents go to a side table read by the epilogue.  Entries below the significance threshold
-// of their (segment, latitude group) and rows or columns outside the unit stay zero (the set-up
-// table is zeroed first).
+// The A operand of every chunk is precomputed from the FP64 recurrence, rounded to FP32 and
+// stored in the tile order of the shared-memory stage: slot = [par0][par1], each 128 rows x 32
+// (2 TILE_F words); the transform kernel splits it into TF32 hi / lo.  Entries below the
+// significance threshold of their (segment, latitude group) and rows or columns outside the
+// unit stay zero (the table is zeroed first).
 
 // Analysis unit (m, span s): rows r of parity p = degree lbase + 2r + p, K = latitudes
 // 32c .. 32c + 31 for the chunks c = kstart .. ngrp - 1.  Warp (segment q, chunk parity g).
-__global__ void __launch_bounds__(256) k_tab_ana(ShtDev P, float* tab) {
+__global__ void __launch_bounds__(256) k_tab_ana(ShtDev P, uint32_t* tab) {
   const int4 unit = P.mx_ana_units[blockIdx.x];
   const int m = unit.x, s = unit.y, kstart = unit.z;
   const long long off = unit.w;
@@ -481,7 +446,7 @@ __global__ void __launch_bounds__(256) k_tab_ana(ShtDev P, float* tab) {
   const long long cbase = P.moff[m] + (lbase - m) + SEG * q;
   for (int c = kstart + g; c < P.ngrp; c += 2) {
     if (c < (int)P.istart[seg]) continue;
-    float* slot = tab + (off + (c - kstart)) * (2 * TILE_F);
+    uint32_t* slot = tab + (off + (c - kstart)) * SLOT_WORDS;
     const int j = KC * c + lane;
     const double mu = P.mu[j];
     const double2 sd = P.seeds[(size_t)seg * P.nh + j];
@@ -490,15 +455,15 @@ __global__ void __launch_bounds__(256) k_tab_ana(ShtDev P, float* tab) {
       const double qn = fma(mu, qb, P.be[cbase + t] * qa);
       qa = qb;
       qb = qn;
-      const int row = SEG / 2 * q + (t >> 1);
-      slot[(t & 1) * TILE_F + row * KC + lane] = __double2float_rn(P.cf[cbase + t] * qn);
+      const int o = sw_off(SEG / 2 * q + (t >> 1), lane);
+      slot[(t & 1) * TILE_F + o] = __float_as_uint(__double2float_rn(P.cf[cbase + t] * qn));
     }
   }
 }
 
 // Synthesis unit (m, latitude tile t): rows = latitudes 128 t + row, chunk i = segment
 // seg_list[off + i] of m (K = the degree's index in its parity).  Thread per latitude row.
-__global__ void __launch_bounds__(128) k_tab_syn(ShtDev P, float* tab) {
+__global__ void __launch_bounds__(128) k_tab_syn(ShtDev P, uint32_t* tab) {
   const int4 unit = P.mx_syn_units[blockIdx.x];
   const int m = unit.x, t = unit.y, nch = unit.z;
   const long long off = unit.w;
@@ -513,98 +478,80 @@ __global__ void __launch_bounds__(128) k_tab_syn(ShtDev P, float* tab) {
     const int l0 = P.seg_l0[seg];
     const int len = min(SEG, P.lmax + 1 - l0);
     const long long cbase = P.moff[m] + (l0 - m);
-    float* slot = tab + (off + i) * (2 * TILE_F);
+    uint32_t* slot = tab + (off + i) * SLOT_WORDS;
     const double2 sd = P.seeds[(size_t)seg * P.nh + j];
     double qa = sd.x, qb = sd.y;
     for (int tt = 0; tt < len; ++tt) {
       const double qn = fma(mu, qb, P.be[cbase + tt] * qa);
       qa = qb;
       qb = qn;
-      slot[(tt & 1) * TILE_F + row * KC + (tt >> 1)] = __double2float_rn(P.cf[cbase + tt] * qn);
-    }
-  }
-}
-
-// Block (unit, parity), thread per row: the row's exponent e (largest |entry| * 2^e < 2^15, 0
-// for an all-zero row) into etab[unit][par][row], and the row's entries of every chunk of the
-// unit as FP16 hi / lo of x 2^e (the product and the remainder in FP64) into the swizzled tiles.
-template <bool SYN>
-__global__ void __launch_bounds__(128) k_tab_half(ShtDev P, const float* tmp, uint16_t* tab, short* etab) {
-  const int u = blockIdx.x >> 1, par = blockIdx.x & 1, row = threadIdx.x;
-  const int4 unit = SYN ? P.mx_syn_units[u] : P.mx_ana_units[u];
-  const int nch = SYN ? unit.z : P.ngrp - unit.z;
-  const long long off = unit.w;
-  float mx = 0.0f;
-  for (int c = 0; c < nch; ++c) {
-    const float* t = tmp + (off + c) * (2 * TILE_F) + par * TILE_F + row * KC;
-    for (int k = 0; k < KC; ++k) mx = fmaxf(mx, fabsf(t[k]));
-  }
-  int e = 0;
-  if (mx > 0.0f) {
-    int E;
-    frexpf(mx, &E);
-    e = B_HEADROOM - E;
-  }
-  etab[(size_t)blockIdx.x * 128 + row] = (short)e;
-  for (int c = 0; c < nch; ++c) {
-    const float* t = tmp + (off + c) * (2 * TILE_F) + par * TILE_F + row * KC;
-    uint16_t* hi = tab + (off + c) * SLOT_HALFS + par * 2 * TILE_H;
-    uint16_t* lo = hi + TILE_H;
-    for (int k = 0; k < KC; ++k) {
-      const double xs = ldexp((double)t[k], e);
-      const __half h = __double2half(xs);
-      hi[sw_off(row, k)] = __half_as_ushort(h);
-      lo[sw_off(row, k)] = __half_as_ushort(__double2half(xs - (double)__half2float(h)));
+      const int o = sw_off(row, tt >> 1);
+      slot[(tt & 1) * TILE_F + o] = __float_as_uint(__double2float_rn(P.cf[cbase + tt] * qn));
     }
   }
 }
 
 // ============================================================ Legendre contraction
+// A split: the FP32 Legendre values landed in the hi tiles of the stage; hi <- TF32(x) in
+// place, lo tile <- TF32(x - hi).  Elementwise, so the tile order does not matter.
+__device__ __forceinline__ void split_a(const Smem& S, int st, int tid) {
+  constexpr int NV = TILE_F / 4 / 128;   // 16-byte vectors per thread
+  uint4* hp = reinterpret_cast<uint4*>(S.a_ptr(st, 0));
+  uint4* lp = reinterpret_cast<uint4*>(S.a_ptr(st, 1));
+  uint4 v[NV];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) v[q] = hp[tid + 128 * q];
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    uint4 h, l;
+    split_f32(__uint_as_float(v[q].x), h.x, l.x);
+    split_f32(__uint_as_float(v[q].y), h.y, l.y);
+    split_f32(__uint_as_float(v[q].z), h.z, l.z);
+    split_f32(__uint_as_float(v[q].w), h.w, l.w);
+    hp[tid + 128 * q] = h;
+    lp[tid + 128 * q] = l;
+  }
+}
+
 // Analysis B data of one parity: the TMA box of the folded FFT is [field][32 latitudes][re, im]
-// (8 bytes per entry) in the stage's raw area; rows 2f (re) / 2f+1 (im) of the B hi / lo tiles
-// get its FP16 split.  Thread tid splits the entries of the fields f = tid / 32 + 4 u (u < 8),
-// scaled by sc[u] = 2^e of (field, order band).
-__device__ __forceinline__ void split_b_ana(const Smem& S, int st, int nf, int tid, const float (&sc)[8]) {
-  const float2* box = reinterpret_cast<const float2*>(S.raw_ptr(st));
-  uint16_t* hp = S.b_ptr(st, 0);
-  uint16_t* lp = S.b_ptr(st, 1);
+// (8 bytes per entry) in the stage's B lo tile; the 4 splitter warps read it, synchronise, and
+// write rows 2f (re) / 2f+1 (im) of the B hi / lo tiles.
+__device__ __forceinline__ void split_b_ana(const Smem& S, int st, int nf, int tid, int bar_id) {
+  const float2* box = reinterpret_cast<const float2*>(S.b_ptr(st, 1));
+  float2 v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int e = tid + 128 * u;
+    v[u] = ((e >> 5) < nf) ? box[e] : make_float2(0.f, 0.f);
+  }
+  named_bar(bar_id, 128);
+  uint32_t* hp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0));
+  uint32_t* lp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1));
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int e = tid + 128 * u;
     const int f = e >> 5, k = e & 31;
     if (f >= nf) continue;
-    const float2 v = box[e];
     const int o0 = sw_off(2 * f, k), o1 = sw_off(2 * f + 1, k);
-    split_h(v.x * sc[u], hp[o0], lp[o0]);
-    split_h(v.y * sc[u], hp[o1], lp[o1]);
+    uint32_t h, l;
+    split_f32(v[u].x, h, l);
+    hp[o0] = h;
+    lp[o0] = l;
+    split_f32(v[u].y, h, l);
+    hp[o1] = h;
+    lp[o1] = l;
   }
 }
 
-// Synthesis B data of one parity: the raw block is [row][32] FP32 (row 2f / 2f+1 = Re / Im of
-// field f); the same split into the swizzled tiles.  Thread tid splits the entries of the fields
-// f = tid / 64 + 2 i (i < 16), scaled by sc[i] = 2^e of (field, order).
-__device__ __forceinline__ void split_b_syn(const Smem& S, int st, int nrow, int tid, const float (&sc)[16]) {
-  const float* raw = S.raw_ptr(st);
-  uint16_t* hp = S.b_ptr(st, 0);
-  uint16_t* lp = S.b_ptr(st, 1);
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const int e = tid + 128 * i;
-    if (e >= nrow * KC) break;
-    const int row = e >> 5, k = e & 31;
-    const int o = sw_off(row, k);
-    split_h(raw[e] * sc[i], hp[o], lp[o]);
-  }
-}
-
-// The B scales a splitter thread applies to the fields of unit order m (field slots beyond the
-// launch get 1).
-template <bool SYN, int NS>
-__device__ __forceinline__ void splitter_scales(const ShtDev& P, int nf, int m, int tid, float (&sc)[NS]) {
-#pragma unroll
-  for (int i = 0; i < NS; ++i) {
-    const int f = SYN ? (tid >> 6) + 2 * i : (tid >> 5) + 4 * i;
-    sc[i] = (f < nf) ? pow2f(scale_exp(__ldg(P.mx_bmax + bmax_index(SYN, f, m, P.nm)))) : 1.0f;
+// Synthesis B data of one parity: the raw block is already in the tile order; split in place.
+__device__ __forceinline__ void split_b_syn(const Smem& S, int st, int nrow, int tid) {
+  uint32_t* hp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0));
+  uint32_t* lp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1));
+  for (int e = tid; e < nrow * KC; e += 128) {
+    uint32_t h, l;
+    split_f32(__uint_as_float(lp[e]), h, l);
+    hp[e] = h;
+    lp[e] = l;
   }
 }
 
@@ -618,10 +565,9 @@ __device__ __forceinline__ void unit_info(const ShtDev& P, const Misc& M, int u,
 // Persistent CTAs (one per SM) over the work units u = blockIdx.x + i gridDim.x.  Analysis
 // units: rows of D = degrees, columns = (Re, Im) of the fields; synthesis: rows = latitudes.
 // The CTA's work is a sequence of halves q = 2 (chunk) + parity: warp 13 streams each half's
-// Legendre tiles (FP16 hi and lo, one 16 KB bulk copy) and raw B data into stage q % NST;
-// splitter group g = (warp - 4) / 4 splits the B data of the halves of parity g; warp 12 issues
-// the MMAs of unit i into TMEM set i & 1; warps 0-3 drain set i & 1 for unit i while the MMAs of
-// unit i + 1 run, and undo the row and field scales in FP64.
+// Legendre tile and B data into stage q % NST; splitter group g = (warp - 4) / 4 splits the
+// halves of parity g (the stages of that parity); warp 12 issues the MMAs of unit i into TMEM set
+// i & 1; warps 0-3 drain set i & 1 for unit i while the MMAs of unit i + 1 run.
 template <bool SYN, int NST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox, int nunits) {
@@ -632,8 +578,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const Abort ab{P.mx_abort, status};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int L = P.lmax;
-  const uint16_t* tab = SYN ? P.mx_tab_syn : P.mx_tab_ana;
-  const short* etab = SYN ? P.mx_etab_syn : P.mx_etab_ana;
+  const uint32_t* tab = SYN ? P.mx_tab_syn : P.mx_tab_ana;
   const uint32_t tmem = prologue(S, M, a, SYN ? P.mx_syn_units : P.mx_ana_units, nunits);
   if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
     const int nrow = 2 * a.nf;
@@ -654,14 +599,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
               break;
             }
             const uint32_t raw = M.b(BAR_RAW + st);
-            mbar_arrive_expect_tx(raw, (uint32_t)(2 * TILE_A) + bbytes);
-            bulk_g2s(S.a_tile(st, 0), tab + ((long long)unit.w + k) * SLOT_HALFS + par * 2 * TILE_H,
-                     (uint32_t)(2 * TILE_A), raw);
+            mbar_arrive_expect_tx(raw, (uint32_t)TILE_A + bbytes);
+            bulk_g2s(S.a_tile(st, 0), tab + ((long long)unit.w + k) * SLOT_WORDS + par * TILE_F, (uint32_t)TILE_A,
+                     raw);
             if (SYN) {
               const int seg = P.mx_syn_seg[unit.w + k];
-              bulk_g2s(S.raw(st), P.mx_bsyn + ((size_t)seg * 2 + par) * BBLOCK, (uint32_t)nrow * 128u, raw);
+              bulk_g2s(S.b_tile(st, 1), P.mx_bsyn + ((size_t)seg * 2 + par) * BBLOCK, (uint32_t)nrow * 128u, raw);
             } else {
-              tma_load_4d(S.raw(st), &tmx, 2 * KC * (unit.z + k), par, unit.x, 0, raw);
+              tma_load_4d(S.b_tile(st, 1), &tmx, 2 * KC * (unit.z + k), par, unit.x, 0, raw);
             }
           }
         }
@@ -715,20 +660,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int4 unit;
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
-        float sc[SYN ? 16 : 8];
-        splitter_scales<SYN>(P, a.nf, unit.x, tid, sc);
         for (int h = 0; h < 2 * nch; ++h, ++q) {
           if ((h & 1) != g) continue;
           const int st = q % NST;
           // every wait is bounded, so all four warps of the group reach the vote; they go on
-          // only together
+          // (and meet at the named barrier of the B split) only together
           const bool w = mbar_wait(M.b(BAR_RAW + st), (uint32_t)((q / NST) & 1), ab);
           if (!bar_and(1 + g, 128, w)) {
             ok = false;
             break;
           }
-          if constexpr (SYN) split_b_syn(S, st, nrow, tid, sc);
-          else split_b_ana(S, st, a.nf, tid, sc);
+          split_a(S, st, tid);
+          if (SYN) split_b_syn(S, st, nrow, tid);
+          else split_b_ana(S, st, a.nf, tid, 1 + g);
           fence_proxy_async();
           __syncwarp();
           if (lane == 0) mbar_arrive(M.b(BAR_FULL + st));
@@ -750,7 +694,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const uint32_t lanebase = tmem + SET_COLS * (uint32_t)set + ((uint32_t)(32 * warp) << 16);
         const int le = m + ANA_SPAN * unit.y + 2 * r;   // analysis: even degree of row r
         const int j = 128 * unit.y + r;                 // synthesis: latitude of row r
-        const int ea0 = etab[((size_t)u * 2 + 0) * 128 + r], ea1 = etab[((size_t)u * 2 + 1) * 128 + r];
         for (int cb = 0; cb < (2 * a.nf + 15) / 16; ++cb) {
           double ve[16], vo[16];
           if (nch > 0) {
@@ -763,13 +706,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           for (int q = 0; q < 8; ++q) {
             const int f = 8 * cb + q;
             if (f >= a.nf || !M.active[f]) continue;
-            // undo the scales of the row (per parity) and of the field's B: exact powers of two
-            const int eb = scale_exp(__ldg(P.mx_bmax + bmax_index(SYN, f, m, P.nm)));
-            const double se = pow2d(-(ea0 + eb)), so = pow2d(-(ea1 + eb));
-            ve[2 * q] *= se;
-            ve[2 * q + 1] *= se;
-            vo[2 * q] *= so;
-            vo[2 * q + 1] *= so;
             if (SYN) {
               if (j < P.nh) {
                 float4* gq = reinterpret_cast<float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm + m;
@@ -808,10 +744,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 // ============================================================== row FFT kernels
-// Row rFFT in FP32 of the north and south rows of latitudes j0 = 4 blockIdx.x .. j0 + 3 of
-// field blockIdx.y and the fold with the weights, output FP32: X[f][m][0][j] = S, X[f][m][1][j]
-// = D (complex, 8 bytes per entry), latitude fastest (the four latitudes of a block fill one
-// 32-byte sector of each), the layout whose 32-latitude rows of one parity the analysis
+// Row rFFT in FP32 of the north and south rows of the NR / 2 latitudes j0 = (NR / 2) blockIdx.x
+// .. of field blockIdx.y (NR = 4 or 8 rows per block, a launch-shape choice) and the fold with
+// the weights, output FP32: X[f][m][0][j] = S, X[f][m][1][j] = D (complex, 8 bytes per entry),
+// latitude fastest (four latitudes fill one 32-byte sector of each plane), the layout whose 32-latitude rows of one parity the analysis
 // kernel's TMA box reads.  The m = 0
 // fold (the weighted row sums) is formed in FP64 from the FP64 grid values, in s0[f][j], for the
 // FP64 degree-0 coefficient.
@@ -880,52 +816,37 @@ __global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k
   }
   const SmemRows<N, float2> Z{A};
   float2* X = reinterpret_cast<float2*>(P.mx_xf) + (size_t)f * P.nm * P.nh * 2;
-  // consecutive threads: the latitudes of one order (one 32-byte sector of each X plane); the G
-  // lanes of an aligned lane group cover the MBAND orders of one scale band
-  constexpr int G = NLAT * MBAND;
-  static_assert(NT % 32 == 0 && G <= 32 && 32 % G == 0, "fold lane groups");
-  const int ne = NLAT * P.nm;
-  for (int e0 = 0; e0 < ne; e0 += NT) {
-    const int e = e0 + (int)threadIdx.x;
-    float bm = 0.0f;   // largest |component| this thread writes
-    if (e < ne) {
-      const int m = e / NLAT, q = e % NLAT, j = j0 + q;
-      float2 xr[2];
-      const float2 twm = (m > 0 && m < N) ? __ldg(P.twf + m) : make_float2(1.f, 0.f);
+  for (int e = threadIdx.x; e < NLAT * P.nm; e += NT) {
+    // consecutive threads: the latitudes of one order (one 32-byte sector of each X plane)
+    const int m = e / NLAT, q = e % NLAT, j = j0 + q;
+    float2 xr[2];
+    const float2 twm = (m > 0 && m < N) ? __ldg(P.twf + m) : make_float2(1.f, 0.f);
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = 2 * q + h;
-        const float2 z0 = Z(r, 0);
-        if (m == 0) {
-          xr[h] = make_float2(z0.x + z0.y, 0.f);
-        } else if (m == N) {
-          xr[h] = make_float2(z0.x - z0.y, 0.f);
-        } else {
-          const float2 zm = Z(r, m);
-          const float2 zn = Z(r, N - m);
-          const float2 zc = make_float2(zn.x, -zn.y);
-          const float2 ev = cscale(cadd(zm, zc), 0.5f);
-          const float2 dz = csub(zm, zc);
-          const float2 o = make_float2(0.5f * dz.y, -0.5f * dz.x);  // (zm - zc) / (2i)
-          xr[h] = cadd(ev, cmul(twm, o));
-        }
-      }
-      const double wn = P.wn[j], ws = P.ws[j];
-      const float2 an = cscale(xr[0], (float)wn), bs = cscale(xr[1], (float)ws);
+    for (int h = 0; h < 2; ++h) {
+      const int r = 2 * q + h;
+      const float2 z0 = Z(r, 0);
       if (m == 0) {
-        // S_0(j) in FP64: the weighted sums of the north and south rows of latitude j
-        P.mx_s0[(size_t)f * P.nh + j] = wn * rowtot[2 * q] + ws * rowtot[2 * q + 1];
+        xr[h] = make_float2(z0.x + z0.y, 0.f);
+      } else if (m == N) {
+        xr[h] = make_float2(z0.x - z0.y, 0.f);
+      } else {
+        const float2 zm = Z(r, m);
+        const float2 zn = Z(r, N - m);
+        const float2 zc = make_float2(zn.x, -zn.y);
+        const float2 ev = cscale(cadd(zm, zc), 0.5f);
+        const float2 dz = csub(zm, zc);
+        const float2 o = make_float2(0.5f * dz.y, -0.5f * dz.x);  // (zm - zc) / (2i)
+        xr[h] = cadd(ev, cmul(twm, o));
       }
-      const float2 sv = make_float2(an.x + bs.x, an.y + bs.y), dv = make_float2(an.x - bs.x, an.y - bs.y);
-      X[((size_t)m * 2 + 0) * P.nh + j] = sv;   // S (even l - m)
-      X[((size_t)m * 2 + 1) * P.nh + j] = dv;   // D (odd l - m)
-      bm = fmaxf(fmaxf(fabsf(sv.x), fabsf(sv.y)), fmaxf(fabsf(dv.x), fabsf(dv.y)));
     }
-    // the band's max |X| over its lane group (non-negative floats order like their bit patterns)
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) bm = fmaxf(bm, __shfl_xor_sync(0xffffffffu, bm, o));
-    if (threadIdx.x % G == 0 && e < ne && bm > 0.0f)
-      atomicMax(P.mx_bmax + bmax_index(false, f, e / NLAT, P.nm), __float_as_uint(bm));
+    const double wn = P.wn[j], ws = P.ws[j];
+    const float2 an = cscale(xr[0], (float)wn), bs = cscale(xr[1], (float)ws);
+    if (m == 0) {
+      // S_0(j) in FP64: the weighted sums of the north and south rows of latitude j
+      P.mx_s0[(size_t)f * P.nh + j] = wn * rowtot[2 * q] + ws * rowtot[2 * q + 1];
+    }
+    X[((size_t)m * 2 + 0) * P.nh + j] = make_float2(an.x + bs.x, an.y + bs.y);   // S (even l - m)
+    X[((size_t)m * 2 + 1) * P.nh + j] = make_float2(an.x - bs.x, an.y - bs.y);   // D (odd l - m)
   }
 }
 
@@ -992,10 +913,9 @@ __global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArg
 }
 
 // Synthesis B operand: per segment s (order m, degrees l0..l0+63) and parity, rows 2f / 2f+1 =
-// Re / Im of 1.41421356 U_f[l, m] rounded to FP32, k = the degree's index in its parity, row-major
-// (MX_NMAX x 32 per block); the tensor-core kernel splits it.  l = 0 is left out (the inverse
-// FFT adds it in FP64); degrees beyond lmax are zero.  Block (segment, group of 4 fields), 64
-// threads per field; each warp raises the max |B| of (field, order) (the split's scale).
+// Re / Im of 1.41421356 U_f[l, m] rounded to FP32, k = the degree's index in its parity, in the
+// tile order (MX_NMAX x 32 per block).  l = 0 is left out (the inverse FFT adds it in FP64);
+// degrees beyond lmax are zero.  Block (segment, group of 4 fields), 64 threads per field.
 __global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
   const int s = blockIdx.x;
   const int f = 4 * blockIdx.y + (threadIdx.x >> 6);
@@ -1007,13 +927,8 @@ __global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
   if (t < len && !(m == 0 && l0 + t == 0)) u = a.spec[f][P.moff[m] + (l0 - m) + t];
   float* blk = P.mx_bsyn + ((size_t)s * 2 + (t & 1)) * BBLOCK;
   const int k = t >> 1;
-  const float re = (float)(u.x * SQRT2_LEGACY), im = (float)(u.y * SQRT2_LEGACY);
-  blk[(2 * f) * KC + k] = re;
-  blk[(2 * f + 1) * KC + k] = im;
-  float bm = fmaxf(fabsf(re), fabsf(im));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) bm = fmaxf(bm, __shfl_xor_sync(0xffffffffu, bm, o));
-  if ((threadIdx.x & 31) == 0 && bm > 0.0f) atomicMax(P.mx_bmax + bmax_index(true, f, m, P.nm), __float_as_uint(bm));
+  blk[sw_off(2 * f, k)] = (float)(u.x * SQRT2_LEGACY);
+  blk[sw_off(2 * f + 1, k)] = (float)(u.y * SQRT2_LEGACY);
 }
 
 size_t mx_fold_smem(const ShtDev& d, int nr) { return fft_smem_bytes(nr, d.n2, sizeof(float2)); }
@@ -1151,16 +1066,13 @@ int sht_mx_prepare(sle_sht* p) {
     SLE_CUDA(cudaMemcpy(p->mx_syn_seg, segs.data(), segs.size() * sizeof(int), cudaMemcpyHostToDevice));
   p->n_ana_units = (int)av.size();
   p->n_syn_units = (int)sv.size();
-  // Legendre tables: FP64 recurrence rounded to FP32 in a set-up table (zero where negligible),
-  // then scaled per row and split into FP16 hi / lo in the tensor cores' tile order
-  const size_t tab_a = (size_t)na * SLOT_HALFS, tab_s = (size_t)ns * SLOT_HALFS;
-  SLE_TRY(mx_alloc(&p->mx_tab_ana, tab_a + 8));
-  SLE_TRY(mx_alloc(&p->mx_tab_syn, tab_s + 8));
-  SLE_TRY(mx_alloc(&p->mx_etab_ana, (size_t)p->n_ana_units * 256 + 1));
-  SLE_TRY(mx_alloc(&p->mx_etab_syn, (size_t)p->n_syn_units * 256 + 1));
-  SLE_TRY(mx_alloc(&p->mx_bmax, (size_t)2 * MX_MAXF * d.nm));
-  SLE_CUDA(cudaMemset(p->mx_bmax, 0, (size_t)2 * MX_MAXF * d.nm * sizeof(unsigned int)));
-  p->mx_table_bytes = (double)(tab_a + tab_s) * sizeof(uint16_t);
+  // Legendre tables: FP64 recurrence, split into TF32 hi / lo, zero where negligible
+  const size_t tab_a = (size_t)na * SLOT_WORDS, tab_s = (size_t)ns * SLOT_WORDS;
+  SLE_TRY(mx_alloc(&p->mx_tab_ana, tab_a + 1));
+  SLE_TRY(mx_alloc(&p->mx_tab_syn, tab_s + 1));
+  SLE_CUDA(cudaMemset(p->mx_tab_ana, 0, tab_a * sizeof(uint32_t)));
+  SLE_CUDA(cudaMemset(p->mx_tab_syn, 0, tab_s * sizeof(uint32_t)));
+  p->mx_table_bytes = (double)(tab_a + tab_s) * sizeof(uint32_t);
   d.twf = p->mx_twf;
   d.mx_xf = p->mx_xf;
   d.mx_gns = p->mx_gns;
@@ -1172,34 +1084,8 @@ int sht_mx_prepare(sle_sht* p) {
   d.mx_syn_seg = p->mx_syn_seg;
   d.mx_tab_ana = p->mx_tab_ana;
   d.mx_tab_syn = p->mx_tab_syn;
-  d.mx_etab_ana = p->mx_etab_ana;
-  d.mx_etab_syn = p->mx_etab_syn;
-  d.mx_bmax = p->mx_bmax;
-  {
-    // the FP32 set-up table of the larger of the two, reused for the other
-    const size_t nf32 = (size_t)std::max(na, ns) * 2 * TILE_F;
-    float* tmp = nullptr;
-    SLE_TRY(mx_alloc(&tmp, nf32 + 1));
-    int rc = SLE_OK;
-    cudaError_t e = cudaMemset(tmp, 0, (size_t)na * 2 * TILE_F * sizeof(float));
-    if (e == cudaSuccess) {
-      k_tab_ana<<<p->n_ana_units, 256>>>(d, tmp);
-      k_tab_half<false><<<2 * p->n_ana_units, 128>>>(d, tmp, p->mx_tab_ana, p->mx_etab_ana);
-      e = cudaMemset(tmp, 0, (size_t)ns * 2 * TILE_F * sizeof(float));
-    }
-    if (e == cudaSuccess) {
-      k_tab_syn<<<p->n_syn_units, 128>>>(d, tmp);
-      k_tab_half<true><<<2 * p->n_syn_units, 128>>>(d, tmp, p->mx_tab_syn, p->mx_etab_syn);
-      e = cudaDeviceSynchronize();
-    }
-    if (e == cudaSuccess) e = cudaGetLastError();
-    if (e != cudaSuccess) {
-      set_error("building the mixed-precision Legendre tables failed: %s", cudaGetErrorString(e));
-      rc = SLE_ERR_CUDA;
-    }
-    cudaFree(tmp);
-    if (rc != SLE_OK) return rc;
-  }
+  k_tab_ana<<<p->n_ana_units, 256>>>(d, p->mx_tab_ana);
+  k_tab_syn<<<p->n_syn_units, 128>>>(d, p->mx_tab_syn);
   SLE_CUDA(cudaGetLastError());
   SLE_CUDA(cudaDeviceSynchronize());
   // TMA maps of X[f][m][par][j][2]: dims (2 nh floats, 2 parities, nm orders, MX_MAXF fields),
@@ -1223,10 +1109,10 @@ int sht_mx_prepare(sle_sht* p) {
       return SLE_ERR_CUDA;
     }
   }
+  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(2)));
+  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(2)));
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(4)));
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(4)));
-  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<false, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(6)));
-  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(6)));
 #define SLE_ATTR_MX(NN)                                                                                        \
   do {                                                                                                         \
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_fold_smem(d, 4)));    \
@@ -1250,14 +1136,10 @@ static int mx_check_args(const MxFieldArgs& a, const char* what) {
   return SLE_OK;
 }
 
-
-int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t st, int prof_cls) {
+int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t st, int prof_cls) {
   SLE_TRY(sht_mx_prepare(p));
-  const MxFieldArgs& a = a0;
   SLE_TRY(mx_check_args(a, "mixed analysis"));
   const ShtDev& d = p->d;
-  // the fold raises the max |B| of each (field, order band) from zero
-  SLE_CUDA(cudaMemsetAsync(p->mx_bmax, 0, (size_t)MX_MAXF * d.nm * sizeof(unsigned int), st));
   ProfToken t0 = prof_begin(PROF_FFT, a.nf, st);
 #define SLE_LAUNCH_MXF4(NN) \
   k_fold_mx<NN, 4><<<dim3(d.nh / 2, a.nf), fft_threads(4, NN), mx_fold_smem(d, 4), st>>>(d, a)
@@ -1275,30 +1157,28 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[zi]);
   ProfToken t1 = prof_begin(prof_cls, a.nf, st);
   const int ga = std::min(p->n_ana_units, p->n_sm);
-  if (p->tune_stages == 4)
-    k_leg_tc<false, 4><<<ga, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, ZBOX[zi], p->n_ana_units);
+  if (p->tune_stages == 2)
+    k_leg_tc<false, 2><<<ga, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, ZBOX[zi], p->n_ana_units);
   else
-    k_leg_tc<false, 6><<<ga, TC_THREADS, mx_smem(6), st>>>(d, a, status, *map, ZBOX[zi], p->n_ana_units);
+    k_leg_tc<false, 4><<<ga, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, ZBOX[zi], p->n_ana_units);
   prof_end(t1, st);
   note_launch(2);
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
 }
 
-int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a0, int* status, cudaStream_t st) {
+int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t st) {
   SLE_TRY(sht_mx_prepare(p));
-  const MxFieldArgs& a = a0;
   SLE_TRY(mx_check_args(a, "mixed synthesis"));
   const ShtDev& d = p->d;
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[0]);
-  SLE_CUDA(cudaMemsetAsync(p->mx_bmax + (size_t)MX_MAXF * d.nm, 0, (size_t)MX_MAXF * d.nm * sizeof(unsigned int), st));
   ProfToken t0 = prof_begin(PROF_LEG_SYN, a.nf, st);
   k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
   const int gs = std::min(p->n_syn_units, p->n_sm);
-  if (p->tune_stages == 4)
-    k_leg_tc<true, 4><<<gs, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, 0, p->n_syn_units);
+  if (p->tune_stages == 2)
+    k_leg_tc<true, 2><<<gs, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, 0, p->n_syn_units);
   else
-    k_leg_tc<true, 6><<<gs, TC_THREADS, mx_smem(6), st>>>(d, a, status, *map, 0, p->n_syn_units);
+    k_leg_tc<true, 4><<<gs, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, 0, p->n_syn_units);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
 #define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a)

@@ -703,8 +703,7 @@ static void plan_free(sle_sht* p) {
   void* ptrs[] = {p->mu, p->w, p->wn, p->ws, p->be, p->cf, p->moff, p->lidx, p->segoff,
                   p->seg_m, p->seg_l0, p->ana_order, p->seeds, p->tw, p->X, p->EO, p->istart,
                   p->packbuf, p->mx_xf, p->mx_twf, p->mx_gns, p->mx_bsyn, p->mx_s0, p->mx_abort,
-                  p->mx_ana_units, p->mx_syn_units, p->mx_syn_seg, p->mx_tab_ana, p->mx_tab_syn,
-                  p->mx_etab_ana, p->mx_etab_syn, p->mx_bmax};
+                  p->mx_ana_units, p->mx_syn_units, p->mx_syn_seg, p->mx_tab_ana, p->mx_tab_syn};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -919,7 +918,7 @@ extern "C" int sle_sht_create(int nlat, int nlon, int lmax, sle_sht** out) {
   std::memset(p, 0, sizeof(sle_sht));
   // launch shape of the mixed-precision transforms (sle_sht_set_tuning changes it)
   p->tune_fpl = MX_MAXF;
-  p->tune_stages = 6;
+  p->tune_stages = 4;
   p->tune_fold_rows = 8;
   int rc = plan_build(p, nlat, nlon, lmax);
   if (rc != SLE_OK) {
@@ -1070,9 +1069,9 @@ extern "C" int sle_sht_set_tuning(sle_sht* plan, const sle_mx_tuning* t) {
     set_error("sle_sht_set_tuning: NULL argument");
     return SLE_ERR_BAD_ARG;
   }
-  if (t->fields_per_launch < 1 || t->fields_per_launch > MX_MAXF || (t->stages != 4 && t->stages != 6) ||
+  if (t->fields_per_launch < 1 || t->fields_per_launch > MX_MAXF || (t->stages != 2 && t->stages != 4) ||
       (t->fold_rows != 4 && t->fold_rows != 8)) {
-    set_error("sle_sht_set_tuning: fields_per_launch 1..%d, stages 4 or 6, fold_rows 4 or 8 (got %d, %d, %d)",
+    set_error("sle_sht_set_tuning: fields_per_launch 1..%d, stages 2 or 4, fold_rows 4 or 8 (got %d, %d, %d)",
               MX_MAXF, t->fields_per_launch, t->stages, t->fold_rows);
     return SLE_ERR_BAD_ARG;
   }

@@ -9,7 +9,7 @@ transform interface (SLEvolve ``python/slevolve/sht.py:43-46``, ``sht_ducc.py:20
 ``analysis`` returns V[l, m] = (-1)^m U[l, m] and ``synthesis`` reads V.  The ``*_device`` entry
 points always use U.
 
-``precision="mixed"`` runs the Legendre contractions as split-FP16 tensor-core GEMMs with FP32
+``precision="mixed"`` runs the Legendre contractions as split-TF32 tensor-core GEMMs with FP32
 accumulation (FP64 recurrence, row FFTs and degree-0 coefficient); the default ``"fp64"`` matches
 the reference to round-off.
 

@@ -1,9 +1,9 @@
 """Launch-shape autotuner of the mixed-precision transforms.
 
-The split-FP16 transforms have three launch-time choices that change their speed and not their
+The split-TF32 transforms have three launch-time choices that change their speed and not their
 results: how many fields one tensor-core launch carries (a transform list is cut into launches
 of at most ``fields_per_launch`` fields, each launch streaming the whole Legendre table once), the
-pipeline depth of the tensor-core kernel (``stages``: 4 or 6 shared-memory stages of 32 KB) and the
+pipeline depth of the tensor-core kernel (``stages``: 2 or 4 shared-memory stages of 48 KB) and the
 rows per block of the row-FFT fold (``fold_rows``: 4 or 8).  The best choice depends on the degree,
 on the number of fields a step transforms at once and on the device, so it is measured: for each
 candidate the tuner times, with CUDA events on the device, the analysis and the synthesis of
@@ -24,9 +24,9 @@ import itertools
 from . import _lib
 
 FIELDS_PER_LAUNCH = (16, 32)
-STAGES = (4, 6)
+STAGES = (2, 4)
 FOLD_ROWS = (4, 8)
-DEFAULT = {"fields_per_launch": 32, "stages": 6, "fold_rows": 8}
+DEFAULT = {"fields_per_launch": 32, "stages": 4, "fold_rows": 8}
 
 _cache = {}
 

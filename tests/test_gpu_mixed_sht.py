@@ -1,11 +1,10 @@
-"""Mixed-precision transforms (split-FP16 tensor-core Legendre contraction) against the FP64 ones.
+"""Mixed-precision transforms (split-TF32 tensor-core Legendre contraction) against the FP64 ones.
 
-Bar: 1e-6 of the largest coefficient / grid value for the contraction (power-of-two scaled FP16
-hi + lo operands, three products, FP32 accumulation: about 1e-7 in practice), and the FP64
-degree-0 coefficient of the analysis and the degree-0 term of the synthesis within 1e-13 relative
-(they bypass the tensor cores).  The operand scales make the relative error independent of the
-field's magnitude: fields scaled by 1e-20 and 1e+20 meet the same bar (the FP32 row FFTs bound the
-range).
+Bar: 1e-6 of the largest coefficient / grid value for the contraction (TF32 hi + lo operands,
+three products, FP32 accumulation), and the FP64 degree-0 coefficient of the analysis and the
+degree-0 term of the synthesis within 1e-13 relative (they bypass the tensor cores).  TF32 has
+FP32's exponent range, so the relative error does not depend on the field's magnitude: fields
+scaled by 1e-20 and 1e+20 meet the same bar (the FP32 row FFTs bound the range).
 """
 
 import numpy as np
@@ -55,8 +54,8 @@ def test_mixed_degree0_only_is_fp64():
 
 @pytest.mark.parametrize("scale", [1e-20, 1e-8, 1e8, 1e20])
 def test_mixed_accuracy_independent_of_magnitude(scale):
-    """FP16's exponent range is narrow; the per-field and per-row power-of-two scales keep the
-    relative error of the contraction at the 1e-7 level for any field magnitude."""
+    """The relative error of the contraction does not depend on the field's magnitude (TF32
+    operands keep FP32's exponent range)."""
     from slevolve_b200.synthetic import band_limited_field
 
     f64, mx = _pair(128, 127)
@@ -70,7 +69,8 @@ def test_mixed_accuracy_independent_of_magnitude(scale):
 
 
 def test_mixed_fields_of_different_magnitudes_in_one_launch():
-    """Fields of one launch with magnitudes 1e-6 .. 1e6 (each field has its own scale)."""
+    """Fields of one launch with magnitudes 1e-6 .. 1e6, each within the bar of its own largest
+    coefficient."""
     import torch
 
     from slevolve_b200 import _lib
