@@ -16,8 +16,11 @@
 // operands, into TF32 hi + lo in shared memory.  The row FFTs of this form run in FP32; the
 // degree-0 terms are FP64: analysis computes U_00 from FP64 row sums of the input grid,
 // synthesis leaves l = 0 out of the tensor-core sum and adds its uniform contribution to the
-// output grid in FP64.  The tensor core's FP32 accumulation truncates, so the large products
-// (Ahi Bhi) and the small ones go to separate TMEM accumulators that the epilogue adds in FP64.
+// output grid in FP64.  The tensor core's FP32 accumulation truncates on every MMA, which for
+// a sum whose terms share a sign loses about one unit in the last place per MMA: the large
+// products (Ahi Bhi) go to three main accumulators in turn (chunk k to accumulator k mod 3, so no
+// accumulator takes more than 12 of the 32 MMAs of a full unit) and the small ones to a fourth;
+// the epilogue adds the four in FP64.
 // Every launch computes all MX_NMAX columns with the same accumulation structure, so a field's
 // result does not depend on the other fields of its launch or on the launch shape.
 //
@@ -27,8 +30,9 @@
 //               (analysis: one 4-D TMA tensor load of the folded FFT; synthesis: one bulk copy)
 //               into stage q % stages
 //   warps 4-11  splitters, group g = parity g: A and B -> TF32 hi / lo tiles
-//   warp 12     allocates TMEM and issues the MMAs from one thread, unit i into TMEM set i & 1
-//   warps 0-3   epilogue: read set i & 1 out of TMEM while the MMAs of unit i + 1 run
+//   warp 12     allocates TMEM and issues the MMAs from one thread
+//   warps 0-3   epilogue: read a unit's accumulators out of TMEM, release them to the MMAs of the
+//               next unit, then add them up in FP64 and write the results
 // Stages hand over through mbarriers; tcgen05.commit releases a stage when its MMAs are done.
 // Every wait is bounded: on timeout the CTA raises the plan's abort flag (and the caller's status
 // word), stops waiting, lets issued MMAs and copies land and releases its TMEM.  No load uses
@@ -62,7 +66,8 @@ constexpr int TC_THREADS = 14 * 32;           // warps 0..3: epilogue
 constexpr int ANA_SPAN = 256;                 // degrees per analysis unit (128 per parity)
 constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wait gives up
 constexpr uint32_t TMEM_COLS = 512;
-constexpr uint32_t SET_COLS = 256;            // two accumulator sets (units alternate)
+constexpr uint32_t PAR_COLS = 256;            // TMEM columns per parity: correction + NMAIN main accumulators
+constexpr int NMAIN = 3;                      // main accumulators (chunk k into k mod NMAIN)
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
 constexpr int MAX_CTA_UNITS = 16;            // work units per CTA staged in shared memory
 constexpr int NCOLS = MX_NMAX;                // accumulator columns of every launch (2 per field slot)
@@ -71,7 +76,8 @@ static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too sm
 static_assert(NSTAGE_MAX % 2 == 0, "a stage must always hold halves of one parity");
 static_assert(mx_smem(NSTAGE_MAX) <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
 static_assert(TILE_B == MX_NMAX * 128, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
-static_assert(4 * MX_NMAX <= (int)SET_COLS && 2 * MX_NMAX <= 256, "full-width accumulators exceed a TMEM set");
+static_assert(2 * (NMAIN + 1) * MX_NMAX <= (int)TMEM_COLS && (NMAIN + 1) * MX_NMAX == (int)PAR_COLS,
+              "accumulators exceed TMEM");
 
 // ------------------------------------------------------------------ PTX wrappers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -293,11 +299,11 @@ __device__ __forceinline__ Smem smem_layout(uint8_t* raw, int nst) {
 }
 
 // Barriers: full[nst] (splitters -> MMA), empty[nst] (MMA commit -> loader), raw[nst] (copies
-// landed -> splitters), accum[2] (a unit's MMAs done -> epilogue, per TMEM set), tfree[2]
-// (epilogue done with a TMEM set -> MMA), drain (MMAs issued before an abort); each group has
-// room for the largest stage count.
+// landed -> splitters), accum (a unit's MMAs done -> epilogue), tfree (epilogue done reading the
+// accumulators -> MMA), drain (MMAs issued before an abort); each stage group has room for the
+// largest stage count.
 enum { BAR_FULL = 0, BAR_EMPTY = NSTAGE_MAX, BAR_RAW = 2 * NSTAGE_MAX, BAR_ACCUM = 3 * NSTAGE_MAX,
-       BAR_TFREE = 3 * NSTAGE_MAX + 2, BAR_DRAIN = 3 * NSTAGE_MAX + 4, NBAR = 3 * NSTAGE_MAX + 5 };
+       BAR_TFREE = 3 * NSTAGE_MAX + 1, BAR_DRAIN = 3 * NSTAGE_MAX + 2, NBAR = 3 * NSTAGE_MAX + 3 };
 static_assert(NBAR * 8 <= 192, "barrier area too small");
 struct Misc {
   uint64_t* bar;
@@ -318,51 +324,55 @@ __device__ __forceinline__ Misc misc_layout(const Smem& S) {
   return m;
 }
 
-// TMEM use (512 columns): two sets of 256, consecutive units alternate between them so that
-// the epilogue of one unit overlaps the MMAs of the next.  Every launch computes N = MX_NMAX
-// columns (2 per field slot; slots beyond the launch's fields are not read), so that a field's
-// accumulation does not depend on how many fields share its launch: in a set, per parity p the
-// main accumulator (Ahi*Bhi of every chunk) at 2Np and the correction accumulator (Ahi*Blo +
-// Alo*Bhi) right after it at 2Np + N, so that Ahi*Bhi and Ahi*Blo are one MMA of 2N columns over
-// the adjacent B hi and B lo tiles (A hi read from shared memory once per K step).
-static_assert(4 * NCOLS <= (int)SET_COLS, "full-width accumulators exceed a TMEM set");
+// TMEM use (512 columns): per parity p, at 256 p, the correction accumulator (Ahi*Blo + Alo*Bhi
+// of every chunk) and then NMAIN main accumulators (Ahi*Bhi, chunk k into main k mod NMAIN), N =
+// MX_NMAX columns each.  Every launch computes all N columns (2 per field slot; slots beyond the
+// launch's fields are not read), so that a field's accumulation does not depend on how many
+// fields share its launch.  One unit holds TMEM at a time: the epilogue releases it as soon as
+// it has read the accumulators, while the stages of the next unit keep loading and splitting.
 
-// MMAs of one parity `par` of chunk k of a unit (stage st) into the set at `set_base`: four K
-// steps of 8.  The K sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the
+// MMAs of one parity `par` of chunk k of a unit (stage st): four K steps of 8, three M128 x N64
+// products each.  The K sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the
 // descriptor's start-address field.
-__device__ __forceinline__ void mma_half(const Smem& S, uint32_t set_base, int st, int par, int k) {
+__device__ __forceinline__ void mma_half(const Smem& S, uint32_t tmem, int st, int par, int k) {
   const uint64_t ah = sdesc_sw128(S.a_tile(st, 0)), al = sdesc_sw128(S.a_tile(st, 1));
-  const uint64_t bh = sdesc_sw128(S.b_tile(st, 0));
-  const uint32_t idesc = idesc_tf32(128, NCOLS), idesc2 = idesc_tf32(128, 2 * NCOLS);
-  // B hi rows [0, N) and B lo rows [0, N) are 2N consecutive rows (TILE_B = N rows)
-  const uint32_t dm = set_base + (uint32_t)(2 * NCOLS * par), dc = dm + (uint32_t)NCOLS;
+  const uint64_t bh = sdesc_sw128(S.b_tile(st, 0)), bl = sdesc_sw128(S.b_tile(st, 1));
+  const uint32_t idesc = idesc_tf32(128, NCOLS);
+  const uint32_t dc = tmem + PAR_COLS * (uint32_t)par;
+  const uint32_t dm = dc + (uint32_t)(NCOLS * (1 + k % NMAIN));
+  const bool fresh = k < NMAIN;
 #pragma unroll
   for (int kk = 0; kk < KC / 8; ++kk) {
     const uint64_t d = (uint64_t)(2 * kk);
-    tc_mma_tf32(dm, ah + d, bh + d, idesc2, (k == 0 && kk == 0) ? 0u : 1u);   // [main | corr]
+    tc_mma_tf32(dm, ah + d, bh + d, idesc, (fresh && kk == 0) ? 0u : 1u);
+    tc_mma_tf32(dc, ah + d, bl + d, idesc, (k == 0 && kk == 0) ? 0u : 1u);
     tc_mma_tf32(dc, al + d, bh + d, idesc, 1u);
   }
 }
 
-// Accumulator columns [16 cb, 16 cb + 16) of both parities for this thread's TMEM lane, the
-// correction and the main accumulator summed in FP64 (in that order).
-__device__ __forceinline__ void acc_read(uint32_t lanebase, int cb, double (&ev)[16], double (&od)[16]) {
+// Accumulator columns [16 cb, 16 cb + 16) of both parities for this thread's TMEM lane: the
+// correction and the main accumulators in use (min(nch, NMAIN)) summed in FP64, in that order.
+__device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int cb, double (&ev)[16], double (&od)[16]) {
   uint32_t re[16], ro[16];
-  tc_ld16(lanebase + (uint32_t)(NCOLS + 16 * cb), re);
-  tc_ld16(lanebase + (uint32_t)(3 * NCOLS + 16 * cb), ro);
+  tc_ld16(lanebase + (uint32_t)(16 * cb), re);
+  tc_ld16(lanebase + PAR_COLS + (uint32_t)(16 * cb), ro);
   tc_wait_ld();
 #pragma unroll
   for (int u = 0; u < 16; ++u) {
     ev[u] = (double)__uint_as_float(re[u]);
     od[u] = (double)__uint_as_float(ro[u]);
   }
-  tc_ld16(lanebase + (uint32_t)(16 * cb), re);
-  tc_ld16(lanebase + (uint32_t)(2 * NCOLS + 16 * cb), ro);
-  tc_wait_ld();
+  const int nb = min(nch, NMAIN);
+  for (int b = 0; b < nb; ++b) {
+    const uint32_t off = (uint32_t)(NCOLS * (1 + b) + 16 * cb);
+    tc_ld16(lanebase + off, re);
+    tc_ld16(lanebase + PAR_COLS + off, ro);
+    tc_wait_ld();
 #pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    ev[u] += (double)__uint_as_float(re[u]);
-    od[u] += (double)__uint_as_float(ro[u]);
+    for (int u = 0; u < 16; ++u) {
+      ev[u] += (double)__uint_as_float(re[u]);
+      od[u] += (double)__uint_as_float(ro[u]);
+    }
   }
 }
 
@@ -379,10 +389,8 @@ __device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a,
       mbar_init(M.b(BAR_EMPTY + i), 1);   // one tcgen05.commit
       mbar_init(M.b(BAR_RAW + i), 1);     // loader's expect_tx
     }
-    for (int i = 0; i < 2; ++i) {
-      mbar_init(M.b(BAR_ACCUM + i), 1);   // one tcgen05.commit (or arrive for an empty unit)
-      mbar_init(M.b(BAR_TFREE + i), 4);   // the 4 epilogue warps
-    }
+    mbar_init(M.b(BAR_ACCUM), 1);   // one tcgen05.commit (or arrive for an empty unit)
+    mbar_init(M.b(BAR_TFREE), 4);   // the 4 epilogue warps
     mbar_init(M.b(BAR_DRAIN), 1);
     fence_mbar_init();
   }
@@ -566,8 +574,8 @@ __device__ __forceinline__ void unit_info(const ShtDev& P, const Misc& M, int u,
 // units: rows of D = degrees, columns = (Re, Im) of the fields; synthesis: rows = latitudes.
 // The CTA's work is a sequence of halves q = 2 (chunk) + parity: warp 13 streams each half's
 // Legendre tile and B data into stage q % NST; splitter group g = (warp - 4) / 4 splits the
-// halves of parity g (the stages of that parity); warp 12 issues the MMAs of unit i into TMEM set
-// i & 1; warps 0-3 drain set i & 1 for unit i while the MMAs of unit i + 1 run.
+// halves of parity g (the stages of that parity); warp 12 issues the MMAs of unit i once the
+// epilogue has read unit i - 1 out of TMEM; warps 0-3 drain unit i.
 template <bool SYN, int NST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox, int nunits) {
@@ -625,10 +633,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           int4 unit;
           int nch;
           unit_info<SYN>(P, M, u, i, unit, nch);
-          const int set = i & 1;
-          if (!mbar_spin(M.b(BAR_TFREE + set), (uint32_t)(((i >> 1) & 1) ^ 1), ab)) break;
+          if (!mbar_spin(M.b(BAR_TFREE), (uint32_t)((i & 1) ^ 1), ab)) break;
           tc_fence_after();
-          const uint32_t base = tmem + SET_COLS * (uint32_t)set;
           for (int h = 0; h < 2 * nch; ++h, ++q) {
             const int st = q % NST;
             if (!mbar_spin(M.b(BAR_FULL + st), (uint32_t)((q / NST) & 1), ab)) {
@@ -636,13 +642,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
               break;
             }
             tc_fence_after();
-            mma_half(S, base, st, h & 1, h >> 1);
+            mma_half(S, tmem, st, h & 1, h >> 1);
             issued = true;
             tc_commit(M.b(BAR_EMPTY + st));
           }
           if (!ok) break;
-          if (nch > 0) tc_commit(M.b(BAR_ACCUM + set));
-          else mbar_arrive(M.b(BAR_ACCUM + set));
+          if (nch > 0) tc_commit(M.b(BAR_ACCUM));
+          else mbar_arrive(M.b(BAR_ACCUM));
         }
         if (!ok && issued) {
           // aborted: let the MMAs already issued finish (bounded) before TMEM is released
@@ -687,20 +693,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int4 unit;
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
-        const int set = i & 1, m = unit.x;
-        const bool w = mbar_wait(M.b(BAR_ACCUM + set), (uint32_t)((i >> 1) & 1), ab);
+        const int m = unit.x;
+        const bool w = mbar_wait(M.b(BAR_ACCUM), (uint32_t)(i & 1), ab);
         if (!__all_sync(0xffffffffu, w)) break;
         tc_fence_after();
-        const uint32_t lanebase = tmem + SET_COLS * (uint32_t)set + ((uint32_t)(32 * warp) << 16);
+        const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
         const int le = m + ANA_SPAN * unit.y + 2 * r;   // analysis: even degree of row r
         const int j = 128 * unit.y + r;                 // synthesis: latitude of row r
-        for (int cb = 0; cb < (2 * a.nf + 15) / 16; ++cb) {
+        const int ncb = (2 * a.nf + 15) / 16;
+        for (int cb = 0; cb < ncb; ++cb) {
           double ve[16], vo[16];
           if (nch > 0) {
-            acc_read(lanebase, cb, ve, vo);
+            acc_read(lanebase, nch, cb, ve, vo);
           } else {
 #pragma unroll
             for (int q = 0; q < 16; ++q) ve[q] = vo[q] = 0.0;
+          }
+          if (cb == ncb - 1) {
+            // every accumulator of the unit is in registers: TMEM goes to the next unit's MMAs
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(M.b(BAR_TFREE));
           }
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
@@ -734,9 +747,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (lane == 0) a.spec[f][0] = make_double2(__dmul_rn(__dsqrt_rn(0.5), acc) / SQRT2_LEGACY, 0.0);
           }
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(M.b(BAR_TFREE + set));
       }
     }
   }
