@@ -30,9 +30,11 @@
 //               (analysis: one 4-D TMA tensor load of the folded FFT; synthesis: one bulk copy)
 //               into stage q % stages
 //   warps 4-11  splitters, group g = parity g: A and B -> TF32 hi / lo tiles
-//   warp 12     allocates TMEM and issues the MMAs from one thread
-//   warps 0-3   epilogue: read a unit's accumulators out of TMEM, release them to the MMAs of the
-//               next unit, then add them up in FP64 and write the results
+//   warp 12     allocates TMEM and issues the MMAs from one thread: a unit's halves of parity 0
+//               (all its chunks), then those of parity 1, each parity into its own TMEM half
+//   warps 0-3   epilogue: per parity, read the accumulators out of TMEM (the MMAs of that parity
+//               of the next unit wait for it, those of the other parity run meanwhile), add them
+//               up in FP64 and write the results
 // Stages hand over through mbarriers; tcgen05.commit releases a stage when its MMAs are done.
 // Every wait is bounded: on timeout the CTA raises the plan's abort flag (and the caller's status
 // word), stops waiting, lets issued MMAs and copies land and releases its TMEM.  No load uses
@@ -299,11 +301,11 @@ __device__ __forceinline__ Smem smem_layout(uint8_t* raw, int nst) {
 }
 
 // Barriers: full[nst] (splitters -> MMA), empty[nst] (MMA commit -> loader), raw[nst] (copies
-// landed -> splitters), accum (a unit's MMAs done -> epilogue), tfree (epilogue done reading the
-// accumulators -> MMA), drain (MMAs issued before an abort); each stage group has room for the
-// largest stage count.
+// landed -> splitters), accum[2] (a unit's MMAs of one parity done -> epilogue), tfree[2]
+// (epilogue done reading that parity's accumulators -> MMA), drain (MMAs issued before an
+// abort); each stage group has room for the largest stage count.
 enum { BAR_FULL = 0, BAR_EMPTY = NSTAGE_MAX, BAR_RAW = 2 * NSTAGE_MAX, BAR_ACCUM = 3 * NSTAGE_MAX,
-       BAR_TFREE = 3 * NSTAGE_MAX + 1, BAR_DRAIN = 3 * NSTAGE_MAX + 2, NBAR = 3 * NSTAGE_MAX + 3 };
+       BAR_TFREE = 3 * NSTAGE_MAX + 2, BAR_DRAIN = 3 * NSTAGE_MAX + 4, NBAR = 3 * NSTAGE_MAX + 5 };
 static_assert(NBAR * 8 <= 192, "barrier area too small");
 struct Misc {
   uint64_t* bar;
@@ -328,8 +330,8 @@ __device__ __forceinline__ Misc misc_layout(const Smem& S) {
 // of every chunk) and then NMAIN main accumulators (Ahi*Bhi, chunk k into main k mod NMAIN), N =
 // MX_NMAX columns each.  Every launch computes all N columns (2 per field slot; slots beyond the
 // launch's fields are not read), so that a field's accumulation does not depend on how many
-// fields share its launch.  One unit holds TMEM at a time: the epilogue releases it as soon as
-// it has read the accumulators, while the stages of the next unit keep loading and splitting.
+// fields share its launch.  A unit runs its parity-0 halves first, then its parity-1 halves:
+// while the epilogue drains one parity's half of TMEM, the MMAs of the other parity run.
 
 // MMAs of one parity `par` of chunk k of a unit (stage st): four K steps of 8, three M128 x N64
 // products each.  The K sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the
@@ -350,28 +352,30 @@ __device__ __forceinline__ void mma_half(const Smem& S, uint32_t tmem, int st, i
   }
 }
 
-// Accumulator columns [16 cb, 16 cb + 16) of both parities for this thread's TMEM lane: the
-// correction and the main accumulators in use (min(nch, NMAIN)) summed in FP64, in that order.
-__device__ __forceinline__ void acc_read(uint32_t lanebase, int nch, int cb, double (&ev)[16], double (&od)[16]) {
-  uint32_t re[16], ro[16];
-  tc_ld16(lanebase + (uint32_t)(16 * cb), re);
-  tc_ld16(lanebase + PAR_COLS + (uint32_t)(16 * cb), ro);
+// Accumulator columns [16 cb, 16 cb + 16) of one parity (TMEM address `base` of this thread's
+// lane and that parity): the correction and the main accumulators in use (min(nch, NMAIN))
+// summed in FP64, in that order.
+__device__ __forceinline__ void acc_read(uint32_t base, int nch, int cb, double (&v)[16]) {
+  uint32_t x[16], y[16];
+  tc_ld16(base + (uint32_t)(16 * cb), x);
+  if (nch > 0) tc_ld16(base + (uint32_t)(NCOLS + 16 * cb), y);
   tc_wait_ld();
 #pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    ev[u] = (double)__uint_as_float(re[u]);
-    od[u] = (double)__uint_as_float(ro[u]);
+  for (int u = 0; u < 16; ++u) v[u] = (double)__uint_as_float(x[u]);
+  if (nch > 0) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(y[u]);
   }
   const int nb = min(nch, NMAIN);
-  for (int b = 0; b < nb; ++b) {
-    const uint32_t off = (uint32_t)(NCOLS * (1 + b) + 16 * cb);
-    tc_ld16(lanebase + off, re);
-    tc_ld16(lanebase + PAR_COLS + off, ro);
+  for (int b = 1; b < nb; b += 2) {
+    tc_ld16(base + (uint32_t)(NCOLS * (1 + b) + 16 * cb), x);
+    if (b + 1 < nb) tc_ld16(base + (uint32_t)(NCOLS * (2 + b) + 16 * cb), y);
     tc_wait_ld();
 #pragma unroll
-    for (int u = 0; u < 16; ++u) {
-      ev[u] += (double)__uint_as_float(re[u]);
-      od[u] += (double)__uint_as_float(ro[u]);
+    for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(x[u]);
+    if (b + 1 < nb) {
+#pragma unroll
+      for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(y[u]);
     }
   }
 }
@@ -389,8 +393,10 @@ __device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a,
       mbar_init(M.b(BAR_EMPTY + i), 1);   // one tcgen05.commit
       mbar_init(M.b(BAR_RAW + i), 1);     // loader's expect_tx
     }
-    mbar_init(M.b(BAR_ACCUM), 1);   // one tcgen05.commit (or arrive for an empty unit)
-    mbar_init(M.b(BAR_TFREE), 4);   // the 4 epilogue warps
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(M.b(BAR_ACCUM + i), 1);   // one tcgen05.commit (or arrive for an empty unit)
+      mbar_init(M.b(BAR_TFREE + i), 4);   // the 4 epilogue warps
+    }
     mbar_init(M.b(BAR_DRAIN), 1);
     fence_mbar_init();
   }
@@ -572,10 +578,11 @@ __device__ __forceinline__ void unit_info(const ShtDev& P, const Misc& M, int u,
 
 // Persistent CTAs (one per SM) over the work units u = blockIdx.x + i gridDim.x.  Analysis
 // units: rows of D = degrees, columns = (Re, Im) of the fields; synthesis: rows = latitudes.
-// The CTA's work is a sequence of halves q = 2 (chunk) + parity: warp 13 streams each half's
-// Legendre tile and B data into stage q % NST; splitter group g = (warp - 4) / 4 splits the
-// halves of parity g (the stages of that parity); warp 12 issues the MMAs of unit i once the
-// epilogue has read unit i - 1 out of TMEM; warps 0-3 drain unit i.
+// The CTA's work is a sequence of halves q (per unit: parity 0 of its chunks 0 .. nch - 1, then
+// parity 1 of the same chunks): warp 13 streams each half's Legendre tile and B data into stage
+// q % NST; splitter group g = (warp - 4) / 4 splits the halves q = g mod 2 (the stages of that
+// parity); warp 12 issues the MMAs of a unit's parity p once the epilogue has read parity p of
+// the unit before out of TMEM; warps 0-3 drain the unit parity by parity.
 template <bool SYN, int NST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox, int nunits) {
@@ -601,7 +608,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           int nch;
           unit_info<SYN>(P, M, u, i, unit, nch);
           for (int h = 0; h < 2 * nch; ++h, ++q) {
-            const int st = q % NST, k = h >> 1, par = h & 1;
+            const int par = h >= nch ? 1 : 0, k = h - par * nch, st = q % NST;
             if (!mbar_spin(M.b(BAR_EMPTY + st), (uint32_t)(((q / NST) & 1) ^ 1), ab)) {
               ok = false;
               break;
@@ -633,22 +640,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           int4 unit;
           int nch;
           unit_info<SYN>(P, M, u, i, unit, nch);
-          if (!mbar_spin(M.b(BAR_TFREE), (uint32_t)((i & 1) ^ 1), ab)) break;
-          tc_fence_after();
-          for (int h = 0; h < 2 * nch; ++h, ++q) {
-            const int st = q % NST;
-            if (!mbar_spin(M.b(BAR_FULL + st), (uint32_t)((q / NST) & 1), ab)) {
+          for (int par = 0; par < 2 && ok; ++par) {
+            if (!mbar_spin(M.b(BAR_TFREE + par), (uint32_t)((i & 1) ^ 1), ab)) {
               ok = false;
               break;
             }
             tc_fence_after();
-            mma_half(S, tmem, st, h & 1, h >> 1);
-            issued = true;
-            tc_commit(M.b(BAR_EMPTY + st));
+            for (int k = 0; k < nch; ++k, ++q) {
+              const int st = q % NST;
+              if (!mbar_spin(M.b(BAR_FULL + st), (uint32_t)((q / NST) & 1), ab)) {
+                ok = false;
+                break;
+              }
+              tc_fence_after();
+              mma_half(S, tmem, st, par, k);
+              issued = true;
+              tc_commit(M.b(BAR_EMPTY + st));
+            }
+            if (!ok) break;
+            if (nch > 0) tc_commit(M.b(BAR_ACCUM + par));
+            else mbar_arrive(M.b(BAR_ACCUM + par));
           }
-          if (!ok) break;
-          if (nch > 0) tc_commit(M.b(BAR_ACCUM));
-          else mbar_arrive(M.b(BAR_ACCUM));
         }
         if (!ok && issued) {
           // aborted: let the MMAs already issued finish (bounded) before TMEM is released
@@ -658,7 +670,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
       __syncwarp();
     } else if (warp >= W_SPL) {
-      // ---- splitters: group g takes the halves of parity g (the stages of that parity)
+      // ---- splitters: group g takes the halves q = g mod 2 (the stages of that parity)
       const int g = (warp - W_SPL) >> 2, tid = threadIdx.x - 32 * W_SPL - 128 * g;
       int q = 0, i = 0;
       bool ok = true;
@@ -667,7 +679,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
         for (int h = 0; h < 2 * nch; ++h, ++q) {
-          if ((h & 1) != g) continue;
+          if ((q & 1) != g) continue;
           const int st = q % NST;
           // every wait is bounded, so all four warps of the group reach the vote; they go on
           // (and meet at the named barrier of the B split) only together
@@ -694,44 +706,48 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
         const int m = unit.x;
-        const bool w = mbar_wait(M.b(BAR_ACCUM), (uint32_t)(i & 1), ab);
-        if (!__all_sync(0xffffffffu, w)) break;
-        tc_fence_after();
         const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
         const int le = m + ANA_SPAN * unit.y + 2 * r;   // analysis: even degree of row r
         const int j = 128 * unit.y + r;                 // synthesis: latitude of row r
         const int ncb = (2 * a.nf + 15) / 16;
-        for (int cb = 0; cb < ncb; ++cb) {
-          double ve[16], vo[16];
-          if (nch > 0) {
-            acc_read(lanebase, nch, cb, ve, vo);
-          } else {
-#pragma unroll
-            for (int q = 0; q < 16; ++q) ve[q] = vo[q] = 0.0;
+        bool okp = true;
+        for (int par = 0; par < 2; ++par) {
+          const bool w = mbar_wait(M.b(BAR_ACCUM + par), (uint32_t)(i & 1), ab);
+          if (!__all_sync(0xffffffffu, w)) {
+            okp = false;
+            break;
           }
-          if (cb == ncb - 1) {
-            // every accumulator of the unit is in registers: TMEM goes to the next unit's MMAs
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(M.b(BAR_TFREE));
-          }
+          tc_fence_after();
+          for (int cb = 0; cb < ncb; ++cb) {
+            double v[16];
+            if (nch > 0) {
+              acc_read(lanebase + PAR_COLS * (uint32_t)par, nch, cb, v);
+            } else {
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int f = 8 * cb + q;
-            if (f >= a.nf || !M.active[f]) continue;
-            if (SYN) {
-              if (j < P.nh) {
-                float4* gq = reinterpret_cast<float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm + m;
-                *gq = make_float4((float)(ve[2 * q] + vo[2 * q]), (float)(ve[2 * q + 1] + vo[2 * q + 1]),
-                                  (float)(ve[2 * q] - vo[2 * q]), (float)(ve[2 * q + 1] - vo[2 * q + 1]));
+              for (int q = 0; q < 16; ++q) v[q] = 0.0;
+            }
+            if (cb == ncb - 1) {
+              // this parity's accumulators are in registers: its TMEM half goes to the next unit
+              tc_fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(M.b(BAR_TFREE + par));
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const int f = 8 * cb + q;
+              if (f >= a.nf || !M.active[f]) continue;
+              if (SYN) {
+                // the even- and odd-degree sums E, O of latitude j (the unfold forms E +- O)
+                if (j < P.nh)
+                  reinterpret_cast<float2*>(P.mx_gns)[(((size_t)f * P.nh + j) * P.nm + m) * 2 + par] =
+                      make_float2((float)v[2 * q], (float)v[2 * q + 1]);
+              } else if (le + par <= L) {
+                a.spec[f][P.moff[m] + (le + par - m)] = make_double2(v[2 * q] * inv, v[2 * q + 1] * inv);
               }
-            } else if (le <= L) {
-              double2* dst = a.spec[f] + P.moff[m] + (le - m);
-              dst[0] = make_double2(ve[2 * q] * inv, ve[2 * q + 1] * inv);
-              if (le + 1 <= L) dst[1] = make_double2(vo[2 * q] * inv, vo[2 * q + 1] * inv);
             }
           }
         }
+        if (!okp) break;
         if (!SYN && m == 0 && unit.y == 0) {
           // degree 0 in FP64 from the row sums of the fold: U_00 = sqrt(0.5) sum_j S_0(j) / 1.41421356;
           // warp w sums the fields w, w + 4, ... (lane-strided partial sums, then a fixed
@@ -860,8 +876,9 @@ __global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k
   }
 }
 
-// Inverse: north and south Legendre sums of field blockIdx.y (FP32, m <= lmax, 0 above; one
-// 16-byte entry per order), unnormalised inverse real FFT in FP32; the output rows get the FP64
+// Inverse: even- and odd-degree Legendre sums E, O of field blockIdx.y (FP32, m <= lmax, 0
+// above; one 16-byte entry per order, north = E + O and south = E - O formed in FP32 as they are
+// read), unnormalised inverse real FFT in FP32; the output rows get the FP64
 // degree-0 term 1.41421356 sqrt(0.5) Re U_00 added in FP64; optional epilogue out2 = grid * mul2.
 // The half-length complex packing of the real inverse transform is formed while the first FFT
 // pass reads its inputs; the last pass writes the output rows.
@@ -872,8 +889,8 @@ struct UnfoldSrcMx {
   int nm;
   __device__ __forceinline__ float2 g(int r, int m) const {
     if (m >= nm) return make_float2(0.f, 0.f);
-    const float4 v = __ldg(G + m);
-    return r ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+    const float4 v = __ldg(G + m);   // (E, O): north = E + O, south = E - O
+    return r ? make_float2(v.x - v.z, v.y - v.w) : make_float2(v.x + v.z, v.y + v.w);
   }
   __device__ __forceinline__ float2 operator()(int r, int m) const {
     float2 x, y;
