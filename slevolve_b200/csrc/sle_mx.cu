@@ -17,10 +17,11 @@
 // degree-0 terms are FP64: analysis computes U_00 from FP64 row sums of the input grid,
 // synthesis leaves l = 0 out of the tensor-core sum and adds its uniform contribution to the
 // output grid in FP64.  The tensor core's FP32 accumulation truncates on every MMA, which for
-// a sum whose terms share a sign loses about one unit in the last place per MMA: the large
-// products (Ahi Bhi) go to three main accumulators in turn (chunk k to accumulator k mod 3, so no
-// accumulator takes more than 12 of the 32 MMAs of a full unit) and the small ones to a fourth;
-// the epilogue adds the four in FP64.
+// a sum whose terms share a sign loses about one unit in the last place per MMA: a unit's chunks
+// go to two accumulator pairs in turn (chunk k to pair k mod 2, so no accumulator takes more than
+// 16 of the 32 MMAs of a full unit), each pair a main accumulator for the large products
+// (Ahi Bhi) beside a correction accumulator for the small ones; the epilogue adds the four in
+// FP64.
 // Every launch computes all MX_NMAX columns with the same accumulation structure, so a field's
 // result does not depend on the other fields of its launch or on the launch shape.
 //
@@ -68,8 +69,8 @@ constexpr int TC_THREADS = 14 * 32;           // warps 0..3: epilogue
 constexpr int ANA_SPAN = 256;                 // degrees per analysis unit (128 per parity)
 constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wait gives up
 constexpr uint32_t TMEM_COLS = 512;
-constexpr uint32_t PAR_COLS = 256;            // TMEM columns per parity: correction + NMAIN main accumulators
-constexpr int NMAIN = 3;                      // main accumulators (chunk k into k mod NMAIN)
+constexpr uint32_t PAR_COLS = 256;            // TMEM columns per parity: NPAIR [main | correction] pairs
+constexpr int NPAIR = 2;                      // accumulator pairs (chunk k into pair k mod NPAIR)
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
 constexpr int MAX_CTA_UNITS = 16;            // work units per CTA staged in shared memory
 constexpr int NCOLS = MX_NMAX;                // accumulator columns of every launch (2 per field slot)
@@ -78,7 +79,7 @@ static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too sm
 static_assert(NSTAGE_MAX % 2 == 0, "a stage must always hold halves of one parity");
 static_assert(mx_smem(NSTAGE_MAX) <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
 static_assert(TILE_B == MX_NMAX * 128, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
-static_assert(2 * (NMAIN + 1) * MX_NMAX <= (int)TMEM_COLS && (NMAIN + 1) * MX_NMAX == (int)PAR_COLS,
+static_assert(2 * NPAIR * 2 * MX_NMAX <= (int)TMEM_COLS && NPAIR * 2 * MX_NMAX == (int)PAR_COLS,
               "accumulators exceed TMEM");
 
 // ------------------------------------------------------------------ PTX wrappers
@@ -326,57 +327,58 @@ __device__ __forceinline__ Misc misc_layout(const Smem& S) {
   return m;
 }
 
-// TMEM use (512 columns): per parity p, at 256 p, the correction accumulator (Ahi*Blo + Alo*Bhi
-// of every chunk) and then NMAIN main accumulators (Ahi*Bhi, chunk k into main k mod NMAIN), N =
-// MX_NMAX columns each.  Every launch computes all N columns (2 per field slot; slots beyond the
-// launch's fields are not read), so that a field's accumulation does not depend on how many
-// fields share its launch.  A unit runs its parity-0 halves first, then its parity-1 halves:
-// while the epilogue drains one parity's half of TMEM, the MMAs of the other parity run.
+// TMEM use (512 columns): per parity p, at 256 p, NPAIR accumulator pairs of 2N columns (N =
+// MX_NMAX): pair b holds the main accumulator (Ahi*Bhi of the chunks k = b mod NPAIR) and right
+// after it the correction accumulator (Ahi*Blo + Alo*Bhi of the same chunks), so that Ahi*Bhi and
+// Ahi*Blo are one MMA of 2N columns over the adjacent B hi and B lo tiles.  Every launch computes
+// all N columns (2 per field slot; slots beyond the launch's fields are not read), so that a
+// field's accumulation does not depend on how many fields share its launch.  A unit runs its
+// parity-0 halves first, then its parity-1 halves: while the epilogue drains one parity's half of
+// TMEM, the MMAs of the other parity run.
 
-// MMAs of one parity `par` of chunk k of a unit (stage st): four K steps of 8, three M128 x N64
-// products each.  The K sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the
+// MMAs of one parity `par` of chunk k of a unit (stage st): four K steps of 8, each one
+// M128 x N128 MMA (Ahi [Bhi | Blo] into [main | correction]) and one M128 x N64 (Alo Bhi into the
+// correction).  The K sub-block kk starts 32 kk bytes into the tile rows: +2 kk in the
 // descriptor's start-address field.
 __device__ __forceinline__ void mma_half(const Smem& S, uint32_t tmem, int st, int par, int k) {
   const uint64_t ah = sdesc_sw128(S.a_tile(st, 0)), al = sdesc_sw128(S.a_tile(st, 1));
-  const uint64_t bh = sdesc_sw128(S.b_tile(st, 0)), bl = sdesc_sw128(S.b_tile(st, 1));
-  const uint32_t idesc = idesc_tf32(128, NCOLS);
-  const uint32_t dc = tmem + PAR_COLS * (uint32_t)par;
-  const uint32_t dm = dc + (uint32_t)(NCOLS * (1 + k % NMAIN));
-  const bool fresh = k < NMAIN;
+  const uint64_t bh = sdesc_sw128(S.b_tile(st, 0));
+  const uint32_t idesc = idesc_tf32(128, NCOLS), idesc2 = idesc_tf32(128, 2 * NCOLS);
+  // B hi rows [0, N) and B lo rows [0, N) are 2N consecutive rows (TILE_B = N rows)
+  const uint32_t dm = tmem + PAR_COLS * (uint32_t)par + (uint32_t)(2 * NCOLS * (k % NPAIR));
+  const uint32_t dc = dm + (uint32_t)NCOLS;
+  const bool fresh = k < NPAIR;
 #pragma unroll
   for (int kk = 0; kk < KC / 8; ++kk) {
     const uint64_t d = (uint64_t)(2 * kk);
-    tc_mma_tf32(dm, ah + d, bh + d, idesc, (fresh && kk == 0) ? 0u : 1u);
-    tc_mma_tf32(dc, ah + d, bl + d, idesc, (k == 0 && kk == 0) ? 0u : 1u);
+    tc_mma_tf32(dm, ah + d, bh + d, idesc2, (fresh && kk == 0) ? 0u : 1u);   // [main | corr]
     tc_mma_tf32(dc, al + d, bh + d, idesc, 1u);
   }
 }
 
 // Accumulator columns [16 cb, 16 cb + 16) of one parity (TMEM address `base` of this thread's
-// lane and that parity): the correction and the main accumulators in use (min(nch, NMAIN))
-// summed in FP64, in that order.
+// lane and that parity), summed in FP64 over the pairs in use (min(nch, NPAIR)): the corrections
+// first, then the main accumulators.
 __device__ __forceinline__ void acc_read(uint32_t base, int nch, int cb, double (&v)[16]) {
   uint32_t x[16], y[16];
-  tc_ld16(base + (uint32_t)(16 * cb), x);
-  if (nch > 0) tc_ld16(base + (uint32_t)(NCOLS + 16 * cb), y);
+  const bool two = nch > 1;
+  tc_ld16(base + (uint32_t)(NCOLS + 16 * cb), x);
+  if (two) tc_ld16(base + (uint32_t)(3 * NCOLS + 16 * cb), y);
   tc_wait_ld();
 #pragma unroll
   for (int u = 0; u < 16; ++u) v[u] = (double)__uint_as_float(x[u]);
-  if (nch > 0) {
+  if (two) {
 #pragma unroll
     for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(y[u]);
   }
-  const int nb = min(nch, NMAIN);
-  for (int b = 1; b < nb; b += 2) {
-    tc_ld16(base + (uint32_t)(NCOLS * (1 + b) + 16 * cb), x);
-    if (b + 1 < nb) tc_ld16(base + (uint32_t)(NCOLS * (2 + b) + 16 * cb), y);
-    tc_wait_ld();
+  tc_ld16(base + (uint32_t)(16 * cb), x);
+  if (two) tc_ld16(base + (uint32_t)(2 * NCOLS + 16 * cb), y);
+  tc_wait_ld();
 #pragma unroll
-    for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(x[u]);
-    if (b + 1 < nb) {
+  for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(x[u]);
+  if (two) {
 #pragma unroll
-      for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(y[u]);
-    }
+    for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(y[u]);
   }
 }
 
