@@ -74,8 +74,10 @@ struct ShtDev {
   float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (FP32, tile order)
   double* mx_s0;              // [MX_MAXF][nh] FP64 fold of the row sums (degree 0)
   int* mx_abort;              // raised by a tensor-core kernel whose wait timed out
-  const int4* mx_ana_units;   // (m, span, first chunk, table slot) analysis units, most work first
+  const int4* mx_ana_units;   // (m, span, first chunk, table slot) analysis units, in runs per CTA
   const int4* mx_syn_units;   // (m, latitude tile, chunks, table slot) synthesis units
+  const int2* mx_ana_cta;     // (first unit, units) of each CTA of an analysis launch
+  const int2* mx_syn_cta;     // the same for a synthesis launch
   const int* mx_syn_seg;      // segment of each synthesis table slot
   const uint32_t* mx_tab_ana; // Legendre tables: [slot][par][128][32] FP32, 128-byte-swizzled tile order
   const uint32_t* mx_tab_syn;
@@ -184,11 +186,13 @@ struct sle_sht {
   double* mx_s0;
   int* mx_abort;
   int4 *mx_ana_units, *mx_syn_units;
+  int2 *mx_ana_cta, *mx_syn_cta;
   int* mx_syn_seg;
   uint32_t *mx_tab_ana, *mx_tab_syn;
   alignas(64) unsigned char mx_tmap[3][128];   // TMA maps of mx_xf (boxes of 8, 16, 32 fields)
   double mx_table_bytes;
   int n_ana_units, n_syn_units;
+  int n_ana_cta, n_syn_cta;       // CTAs of an analysis / synthesis launch
   int n_sm;                      // SMs of the device (persistent transform grid)
   // launch shape of the mixed-precision transforms (sle_sht_set_tuning): fields per tensor-core
   // launch, pipeline stages of the tensor-core kernel, rows per row-FFT block of the fold

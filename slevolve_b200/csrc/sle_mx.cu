@@ -73,6 +73,7 @@ constexpr uint32_t PAR_COLS = 256;            // TMEM columns per parity: NPAIR 
 constexpr int NPAIR = 2;                      // accumulator pairs (chunk k into pair k mod NPAIR)
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
 constexpr int MAX_CTA_UNITS = 16;            // work units per CTA staged in shared memory
+constexpr double UNIT_COST_HALVES = 32.0;     // fixed cost of a work unit (epilogue), in half-chunk times
 constexpr int NCOLS = MX_NMAX;                // accumulator columns of every launch (2 per field slot)
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
 
@@ -358,37 +359,32 @@ __device__ __forceinline__ void mma_half(const Smem& S, uint32_t tmem, int st, i
 
 // Accumulator columns [16 cb, 16 cb + 16) of one parity (TMEM address `base` of this thread's
 // lane and that parity), summed in FP64 over the pairs in use (min(nch, NPAIR)): the corrections
-// first, then the main accumulators.
+// first, then the main accumulators.  All loads of a block are issued before one wait.
 __device__ __forceinline__ void acc_read(uint32_t base, int nch, int cb, double (&v)[16]) {
-  uint32_t x[16], y[16];
-  const bool two = nch > 1;
-  tc_ld16(base + (uint32_t)(NCOLS + 16 * cb), x);
-  if (two) tc_ld16(base + (uint32_t)(3 * NCOLS + 16 * cb), y);
-  tc_wait_ld();
-#pragma unroll
-  for (int u = 0; u < 16; ++u) v[u] = (double)__uint_as_float(x[u]);
-  if (two) {
-#pragma unroll
-    for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(y[u]);
+  uint32_t c0[16], c1[16], m0[16], m1[16];
+  const uint32_t off = (uint32_t)(16 * cb);
+  tc_ld16(base + (uint32_t)NCOLS + off, c0);
+  tc_ld16(base + off, m0);
+  if (nch > 1) {
+    tc_ld16(base + (uint32_t)(3 * NCOLS) + off, c1);
+    tc_ld16(base + (uint32_t)(2 * NCOLS) + off, m1);
   }
-  tc_ld16(base + (uint32_t)(16 * cb), x);
-  if (two) tc_ld16(base + (uint32_t)(2 * NCOLS + 16 * cb), y);
   tc_wait_ld();
+  if (nch > 1) {
 #pragma unroll
-  for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(x[u]);
-  if (two) {
+    for (int u = 0; u < 16; ++u)
+      v[u] = (((double)__uint_as_float(c0[u]) + (double)__uint_as_float(c1[u])) + (double)__uint_as_float(m0[u])) +
+             (double)__uint_as_float(m1[u]);
+  } else {
 #pragma unroll
-    for (int u = 0; u < 16; ++u) v[u] += (double)__uint_as_float(y[u]);
+    for (int u = 0; u < 16; ++u) v[u] = (double)__uint_as_float(c0[u]) + (double)__uint_as_float(m0[u]);
   }
 }
 
 // Common prologue: barriers, gates, TMEM.  Returns the TMEM base (all threads).
-__device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a, const int4* units, int nunits) {
+__device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a, const int4* units, int2 rg) {
   const int warp = threadIdx.x >> 5;
-  if (threadIdx.x < MAX_CTA_UNITS) {
-    const int u = blockIdx.x + threadIdx.x * gridDim.x;
-    if (u < nunits) M.units[threadIdx.x] = units[u];
-  }
+  if (threadIdx.x < MAX_CTA_UNITS && (int)threadIdx.x < rg.y) M.units[threadIdx.x] = units[rg.x + threadIdx.x];
   if (threadIdx.x == 0) {
     for (int i = 0; i < S.nst; ++i) {
       mbar_init(M.b(BAR_FULL + i), 4);    // the 4 splitter warps of the stage
@@ -578,7 +574,7 @@ __device__ __forceinline__ void unit_info(const ShtDev& P, const Misc& M, int u,
   nch = SYN ? unit.z : P.ngrp - unit.z;
 }
 
-// Persistent CTAs (one per SM) over the work units u = blockIdx.x + i gridDim.x.  Analysis
+// Persistent CTAs (one per SM), each over its own run of work units (P.mx_*_cta).  Analysis
 // units: rows of D = degrees, columns = (Re, Im) of the fields; synthesis: rows = latitudes.
 // The CTA's work is a sequence of halves q (per unit: parity 0 of its chunks 0 .. nch - 1, then
 // parity 1 of the same chunks): warp 13 streams each half's Legendre tile and B data into stage
@@ -587,7 +583,7 @@ __device__ __forceinline__ void unit_info(const ShtDev& P, const Misc& M, int u,
 // the unit before out of TMEM; warps 0-3 drain the unit parity by parity.
 template <bool SYN, int NST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox, int nunits) {
+    k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox) {
   static_assert(NST % 2 == 0 && NST <= NSTAGE_MAX, "stage count");
   extern __shared__ uint8_t smraw[];
   const Smem S = smem_layout(smraw, NST);
@@ -596,7 +592,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int L = P.lmax;
   const uint32_t* tab = SYN ? P.mx_tab_syn : P.mx_tab_ana;
-  const uint32_t tmem = prologue(S, M, a, SYN ? P.mx_syn_units : P.mx_ana_units, nunits);
+  // this CTA's work units: rg.y units from rg.x on (the plan balances the CTAs' totals)
+  const int2 rg = (SYN ? P.mx_syn_cta : P.mx_ana_cta)[blockIdx.x];
+  const uint32_t tmem = prologue(S, M, a, SYN ? P.mx_syn_units : P.mx_ana_units, rg);
   if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
     const int nrow = 2 * a.nf;
     if (warp == W_LOAD) {
@@ -605,7 +603,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const uint32_t bbytes = SYN ? (uint32_t)nrow * 128u : (uint32_t)zbox * 32u * 8u;
         int q = 0, i = 0;
         bool ok = true;
-        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
+        for (int u = rg.x; i < rg.y && ok; ++u, ++i) {
           int4 unit;
           int nch;
           unit_info<SYN>(P, M, u, i, unit, nch);
@@ -638,7 +636,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       if (lane == 0) {
         int q = 0, i = 0;
         bool ok = true, issued = false;
-        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
+        for (int u = rg.x; i < rg.y && ok; ++u, ++i) {
           int4 unit;
           int nch;
           unit_info<SYN>(P, M, u, i, unit, nch);
@@ -676,7 +674,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       const int g = (warp - W_SPL) >> 2, tid = threadIdx.x - 32 * W_SPL - 128 * g;
       int q = 0, i = 0;
       bool ok = true;
-      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++i) {
+      for (int u = rg.x; i < rg.y && ok; ++u, ++i) {
         int4 unit;
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
@@ -703,7 +701,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       const int r = 32 * warp + lane;
       const double inv = 1.0 / SQRT2_LEGACY;
       int i = 0;
-      for (int u = blockIdx.x; u < nunits; u += gridDim.x, ++i) {
+      for (int u = rg.x; i < rg.y; ++u, ++i) {
         int4 unit;
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
@@ -713,6 +711,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int j = 128 * unit.y + r;                 // synthesis: latitude of row r
         const int ncb = (2 * a.nf + 15) / 16;
         bool okp = true;
+        // this thread's output element: analysis, coefficient (le + par, m) of every field (when
+        // le + par <= L); synthesis, latitude j (when j < nh), order m, component par
+        const long long abase = (long long)P.moff[m] + (le - m);
+        const size_t sbase = ((size_t)j * P.nm + m) * 2, sfield = (size_t)P.nh * P.nm * 2;
         for (int par = 0; par < 2; ++par) {
           const bool w = mbar_wait(M.b(BAR_ACCUM + par), (uint32_t)(i & 1), ab);
           if (!__all_sync(0xffffffffu, w)) {
@@ -720,6 +722,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             break;
           }
           tc_fence_after();
+          const bool live = SYN ? (j < P.nh) : (le + par <= L);
           for (int cb = 0; cb < ncb; ++cb) {
             double v[16];
             if (nch > 0) {
@@ -734,17 +737,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
               __syncwarp();
               if (lane == 0) mbar_arrive(M.b(BAR_TFREE + par));
             }
+            if (!live) continue;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
               const int f = 8 * cb + q;
               if (f >= a.nf || !M.active[f]) continue;
               if (SYN) {
                 // the even- and odd-degree sums E, O of latitude j (the unfold forms E +- O)
-                if (j < P.nh)
-                  reinterpret_cast<float2*>(P.mx_gns)[(((size_t)f * P.nh + j) * P.nm + m) * 2 + par] =
-                      make_float2((float)v[2 * q], (float)v[2 * q + 1]);
-              } else if (le + par <= L) {
-                a.spec[f][P.moff[m] + (le + par - m)] = make_double2(v[2 * q] * inv, v[2 * q + 1] * inv);
+                reinterpret_cast<float2*>(P.mx_gns)[f * sfield + sbase + par] =
+                    make_float2((float)v[2 * q], (float)v[2 * q + 1]);
+              } else {
+                a.spec[f][abase + par] = make_double2(v[2 * q] * inv, v[2 * q + 1] * inv);
               }
             }
           }
@@ -1024,14 +1027,16 @@ int sht_mx_prepare(sle_sht* p) {
     SLE_TRY(mx_alloc(&p->mx_twf, (size_t)ntw));
     SLE_CUDA(cudaMemcpy(p->mx_twf, tw32.data(), ntw * sizeof(float2), cudaMemcpyHostToDevice));
   }
-  // work units, most work first; each unit's chunks are contiguous slots of its Legendre table
+  // work units; each unit's chunks are contiguous slots of its Legendre table
   std::vector<unsigned char> ist(d.nseg);
   std::vector<int> segoff(d.nm + 1);
   SLE_CUDA(cudaMemcpy(ist.data(), p->istart, d.nseg, cudaMemcpyDeviceToHost));
   SLE_CUDA(cudaMemcpy(segoff.data(), p->segoff, (d.nm + 1) * sizeof(int), cudaMemcpyDeviceToHost));
   const int L = d.lmax;
-  struct AU { long long w; int m, s, kstart; };
-  struct SU { long long w; int m, t; std::vector<int> segs; };
+  // a unit's estimated cost in half-chunk times: its halves plus a fixed per-unit cost (pipeline
+  // turn-around and epilogue)
+  struct AU { double w; int m, s, kstart; };
+  struct SU { double w; int m, t; std::vector<int> segs; };
   std::vector<AU> au;
   std::vector<SU> su;
   for (int m = 0; m <= L; ++m) {
@@ -1040,7 +1045,7 @@ int sht_mx_prepare(sle_sht* p) {
       const int nd = std::min(ANA_SPAN, nl - ANA_SPAN * s);
       int kstart = d.ngrp;
       for (int q = 0; q * SEG < nd; ++q) kstart = std::min(kstart, (int)ist[segoff[m] + (ANA_SPAN / SEG) * s + q]);
-      au.push_back({(long long)(d.ngrp - kstart) * 64 + nd, m, s, kstart});
+      au.push_back({2.0 * (d.ngrp - kstart) + UNIT_COST_HALVES, m, s, kstart});
     }
     const int ntile = (d.nh + 127) / 128;
     for (int t = 0; t < ntile; ++t) {
@@ -1048,7 +1053,7 @@ int sht_mx_prepare(sle_sht* p) {
       const int glast = std::min(d.ngrp, 4 * t + 4) - 1;
       for (int seg = segoff[m]; seg < segoff[m + 1]; ++seg)
         if ((int)ist[seg] <= glast) u.segs.push_back(seg);
-      u.w = (long long)u.segs.size() * 64 + 1;
+      u.w = 2.0 * u.segs.size() + UNIT_COST_HALVES;
       su.push_back(u);
     }
   }
@@ -1060,20 +1065,32 @@ int sht_mx_prepare(sle_sht* p) {
     SLE_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     p->n_sm = std::max(1, nsm);
   }
-  // CTA b of a launch of G = min(n, SMs) CTAs takes the units at positions b, b + G, ...; lay the
-  // units sorted by work out in snake order (round r of G positions in rank order when r is even,
-  // reversed when odd) so that every CTA's total is close to the mean
-  auto snake = [&](auto& v) {
-    const int n = (int)v.size(), G = std::min(n, p->n_sm);
+  // CTA b of a launch of G = min(n, SMs) CTAs takes a run of consecutive units: longest first,
+  // each unit goes to the CTA with the least estimated work so far (ties: the lowest index);
+  // within a CTA the units keep that order
+  auto balance = [&](auto& v, std::vector<int2>& cta) {
+    const int n = (int)v.size(), G = std::max(1, std::min(n, p->n_sm));
+    std::vector<double> load(G, 0.0);
+    std::vector<std::vector<int>> of(G);
+    for (int i = 0; i < n; ++i) {
+      int b = 0;
+      for (int c = 1; c < G; ++c)
+        if (load[c] < load[b]) b = c;
+      load[b] += v[i].w;
+      of[b].push_back(i);
+    }
     auto out = v;
-    for (int pos = 0; pos < n; ++pos) {
-      const int r = pos / G, b = pos % G, cnt = std::min(G, n - r * G);
-      out[pos] = v[r * G + ((r & 1) ? cnt - 1 - b : b)];
+    cta.assign(G, make_int2(0, 0));
+    int pos = 0;
+    for (int b = 0; b < G; ++b) {
+      cta[b] = make_int2(pos, (int)of[b].size());
+      for (int i : of[b]) out[pos++] = v[i];
     }
     v.swap(out);
   };
-  snake(au);
-  snake(su);
+  std::vector<int2> acta, scta;
+  balance(au, acta);
+  balance(su, scta);
   std::vector<int4> av, sv;
   std::vector<int> segs;
   long long na = 0, ns = 0;
@@ -1088,6 +1105,12 @@ int sht_mx_prepare(sle_sht* p) {
   }
   SLE_TRY(mx_alloc(&p->mx_ana_units, av.size()));
   SLE_TRY(mx_alloc(&p->mx_syn_units, sv.size()));
+  SLE_TRY(mx_alloc(&p->mx_ana_cta, acta.size()));
+  SLE_TRY(mx_alloc(&p->mx_syn_cta, scta.size()));
+  SLE_CUDA(cudaMemcpy(p->mx_ana_cta, acta.data(), acta.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  SLE_CUDA(cudaMemcpy(p->mx_syn_cta, scta.data(), scta.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  p->n_ana_cta = (int)acta.size();
+  p->n_syn_cta = (int)scta.size();
   SLE_TRY(mx_alloc(&p->mx_syn_seg, segs.size() + 1));
   SLE_CUDA(cudaMemcpy(p->mx_ana_units, av.data(), av.size() * sizeof(int4), cudaMemcpyHostToDevice));
   SLE_CUDA(cudaMemcpy(p->mx_syn_units, sv.data(), sv.size() * sizeof(int4), cudaMemcpyHostToDevice));
@@ -1110,6 +1133,8 @@ int sht_mx_prepare(sle_sht* p) {
   d.mx_abort = p->mx_abort;
   d.mx_ana_units = p->mx_ana_units;
   d.mx_syn_units = p->mx_syn_units;
+  d.mx_ana_cta = p->mx_ana_cta;
+  d.mx_syn_cta = p->mx_syn_cta;
   d.mx_syn_seg = p->mx_syn_seg;
   d.mx_tab_ana = p->mx_tab_ana;
   d.mx_tab_syn = p->mx_tab_syn;
@@ -1185,11 +1210,10 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t 
   const int zi = (a.nf <= ZBOX[0]) ? 0 : (a.nf <= ZBOX[1]) ? 1 : 2;
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[zi]);
   ProfToken t1 = prof_begin(prof_cls, a.nf, st);
-  const int ga = std::min(p->n_ana_units, p->n_sm);
   if (p->tune_stages == 2)
-    k_leg_tc<false, 2><<<ga, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, ZBOX[zi], p->n_ana_units);
+    k_leg_tc<false, 2><<<p->n_ana_cta, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, ZBOX[zi]);
   else
-    k_leg_tc<false, 4><<<ga, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, ZBOX[zi], p->n_ana_units);
+    k_leg_tc<false, 4><<<p->n_ana_cta, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, ZBOX[zi]);
   prof_end(t1, st);
   note_launch(2);
   SLE_CUDA(cudaGetLastError());
@@ -1203,11 +1227,10 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[0]);
   ProfToken t0 = prof_begin(PROF_LEG_SYN, a.nf, st);
   k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
-  const int gs = std::min(p->n_syn_units, p->n_sm);
   if (p->tune_stages == 2)
-    k_leg_tc<true, 2><<<gs, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, 0, p->n_syn_units);
+    k_leg_tc<true, 2><<<p->n_syn_cta, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, 0);
   else
-    k_leg_tc<true, 4><<<gs, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, 0, p->n_syn_units);
+    k_leg_tc<true, 4><<<p->n_syn_cta, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, 0);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
 #define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a)

@@ -703,7 +703,8 @@ static void plan_free(sle_sht* p) {
   void* ptrs[] = {p->mu, p->w, p->wn, p->ws, p->be, p->cf, p->moff, p->lidx, p->segoff,
                   p->seg_m, p->seg_l0, p->ana_order, p->seeds, p->tw, p->X, p->EO, p->istart,
                   p->packbuf, p->mx_xf, p->mx_twf, p->mx_gns, p->mx_bsyn, p->mx_s0, p->mx_abort,
-                  p->mx_ana_units, p->mx_syn_units, p->mx_syn_seg, p->mx_tab_ana, p->mx_tab_syn};
+                  p->mx_ana_units, p->mx_syn_units, p->mx_syn_seg, p->mx_tab_ana, p->mx_tab_syn,
+                  p->mx_ana_cta, p->mx_syn_cta};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;

@@ -98,14 +98,21 @@ class _Running:
 
 
 class Server:
-    """groups: {lmax: slots}.  budget_bytes: device memory the admitted requests may hold."""
+    """groups: {lmax: slots}.  budget_bytes: device memory the admitted requests may hold (their
+    slots' solver state plus the reuse stores of outer requests).  The slot batches are allocated
+    when the server starts, so the device also holds the state of idle slots: a reuse store is
+    allocated only while the device has room for it with ``store_margin`` bytes to spare, and a
+    request that does not fit waits in the queue."""
 
     def __init__(self, groups, precision="mixed", budget_bytes=None, max_modes=8, opt=("dsl", "diag"),
-                 inner="extrap", record=("deltasl", "tgrid"), preempt=False, device_bytes=None):
+                 inner="extrap", record=("deltasl", "tgrid"), preempt=False, device_bytes=None,
+                 store_margin=1 << 30):
         self.precision = precision
+        self.store_margin = int(store_margin)
         self.preempt = bool(preempt)
         self.preempted = 0
-        # occupancy record: (time, admitted bytes) at every change, against device_bytes
+        # occupancy record: (time, admitted bytes, device bytes in use) at every change, against
+        # device_bytes
         self.device_bytes = device_bytes
         self._occ = []
         self.max_modes = max_modes
@@ -124,25 +131,36 @@ class Server:
 
     # ---------------------------------------------------------------- helpers
     def _note_used(self):
-        """Record the admitted footprint after a change (caller holds the lock)."""
-        self._occ.append((time.perf_counter() - getattr(self, "_t0", time.perf_counter()), self.used))
+        """Record the admitted footprint and the device memory in use after a change (caller
+        holds the lock)."""
+        held = 0
+        if self.device_bytes:
+            import torch
+
+            free, total = torch.cuda.mem_get_info()
+            held = total - free
+        self._occ.append((time.perf_counter() - getattr(self, "_t0", time.perf_counter()), self.used, held))
 
     def occupancy(self):
         """Time-weighted mean and peak of the admitted footprint over the run, in bytes and as a
         fraction of ``device_bytes`` (when given)."""
-        ev = sorted(self._occ)
+        ev = sorted(e if len(e) == 3 else (e[0], e[1], 0) for e in self._occ)
         wall = getattr(self, "wall", 0.0)
         if not ev or wall <= 0:
             return {"mean_bytes": 0.0, "peak_bytes": int(self.peak_used)}
-        area, t_prev, u_prev = 0.0, 0.0, 0
-        for t, u in ev:
+        area, held_area, t_prev, u_prev, h_prev = 0.0, 0.0, 0.0, 0, 0
+        for t, u, h in ev:
             area += u_prev * max(0.0, t - t_prev)
-            t_prev, u_prev = t, u
+            held_area += h_prev * max(0.0, t - t_prev)
+            t_prev, u_prev, h_prev = t, u, h
         area += u_prev * max(0.0, wall - t_prev)
+        held_area += h_prev * max(0.0, wall - t_prev)
         out = {"mean_bytes": area / wall, "peak_bytes": int(self.peak_used)}
         if self.device_bytes:
             out["hbm_occupancy_mean"] = out["mean_bytes"] / self.device_bytes
             out["hbm_occupancy_peak"] = self.peak_used / self.device_bytes
+            out["hbm_held_mean"] = held_area / wall / self.device_bytes
+            out["hbm_held_peak"] = max(h for _, _, h in ev) / self.device_bytes
         return out
 
     @staticmethod
@@ -190,9 +208,18 @@ class Server:
                     free.append(slot)
             if not free:
                 return
+            store = None
             with self.lock:
                 if self.used + fp > self.budget:
                     return
+                if resumed is None and req.outer_passes > 1:
+                    # the store is allocated under the lock, once the device has room for it
+                    import torch
+
+                    if torch.cuda.mem_get_info()[0] < store_bytes(req) + self.store_margin:
+                        return
+                    n = req.lmax + 1
+                    store = ReuseStore(n * (n + 1) // 2, n * 2 * n, capacity=req.nsteps)
                 self.used += fp
                 self.peak_used = max(self.peak_used, self.used)
                 self._note_used()
@@ -213,8 +240,7 @@ class Server:
             if req.outer_passes > 1:
                 import torch
 
-                n = req.lmax + 1
-                run.store = ReuseStore(n * (n + 1) // 2, n * 2 * n, capacity=req.nsteps)
+                run.store = store
                 run.T0 = torch.as_tensor(np.ascontiguousarray(req.topo), dtype=torch.float64, device="cuda")
                 obs = req.obs if req.obs is not None else req.topo
                 run.obs = torch.as_tensor(np.ascontiguousarray(obs), dtype=torch.float64, device="cuda")

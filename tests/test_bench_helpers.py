@@ -70,3 +70,8 @@ def test_serving_occupancy_record():
     assert occ["mean_bytes"] == pytest.approx((100 * 1.0 + 300 * 2.0) / 4.0)
     assert occ["hbm_occupancy_mean"] == pytest.approx(occ["mean_bytes"] / 1000)
     assert occ["hbm_occupancy_peak"] == pytest.approx(0.3)
+    # with the device memory in use recorded beside the admitted footprint
+    srv._occ = [(0.0, 100, 500), (1.0, 300, 900), (3.0, 0, 400)]
+    occ = srv.occupancy()
+    assert occ["hbm_held_mean"] == pytest.approx((500 * 1.0 + 900 * 2.0 + 400 * 1.0) / 4.0 / 1000)
+    assert occ["hbm_held_peak"] == pytest.approx(0.9)
