@@ -33,9 +33,10 @@
 //   warps 4-11  splitters, group g = parity g: A and B -> TF32 hi / lo tiles
 //   warp 12     allocates TMEM and issues the MMAs from one thread: a unit's halves of parity 0
 //               (all its chunks), then those of parity 1, each parity into its own TMEM half
-//   warps 0-3   epilogue: per parity, read the accumulators out of TMEM (the MMAs of that parity
-//               of the next unit wait for it, those of the other parity run meanwhile), add them
-//               up in FP64 and write the results
+//   warps 0-3   epilogue of parity 0, warps 14-17 of parity 1 (warp w reads TMEM lanes
+//               32 (w mod 4) ..): read the parity's accumulators out of TMEM (the MMAs of that
+//               parity of the next unit wait for it, those of the other parity run meanwhile),
+//               add them up in FP64 and write the results
 // Stages hand over through mbarriers; tcgen05.commit releases a stage when its MMAs are done.
 // Every wait is bounded: on timeout the CTA raises the plan's abort flag (and the caller's status
 // word), stops waiting, lets issued MMAs and copies land and releases its TMEM.  No load uses
@@ -65,7 +66,8 @@ constexpr int mx_smem(int nst) { return 1024 + nst * STAGE_BYTES + MISC_BYTES; }
 constexpr int W_SPL = 4;                      // warps 4..11: splitters (two groups of four)
 constexpr int W_MMA = 12;                     // TMEM owner, MMA issue
 constexpr int W_LOAD = 13;                    // bulk / TMA loads
-constexpr int TC_THREADS = 14 * 32;           // warps 0..3: epilogue
+constexpr int W_EPI1 = 14;                    // warps 14..17: epilogue of parity 1 (warps 0..3: parity 0)
+constexpr int TC_THREADS = 18 * 32;
 constexpr int ANA_SPAN = 256;                 // degrees per analysis unit (128 per parity)
 constexpr long long WAIT_LIMIT = 1ll << 31;   // clock cycles (~1 s) before a wait gives up
 constexpr uint32_t TMEM_COLS = 512;
@@ -669,7 +671,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
       }
       __syncwarp();
-    } else if (warp >= W_SPL) {
+    } else if (warp >= W_SPL && warp < W_MMA) {
       // ---- splitters: group g takes the halves q = g mod 2 (the stages of that parity)
       const int g = (warp - W_SPL) >> 2, tid = threadIdx.x - 32 * W_SPL - 128 * g;
       int q = 0, i = 0;
@@ -697,8 +699,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
       }
     } else {
-      // ---- epilogue: warps 0-3 own TMEM lanes 0-127
-      const int r = 32 * warp + lane;
+      // ---- epilogue: warps 0-3 (parity 0) and 14-17 (parity 1); warp w owns TMEM lanes
+      // 32 (w mod 4) .. 32 (w mod 4) + 31
+      const int par = warp >= W_EPI1 ? 1 : 0;
+      const int r = 32 * (warp & 3) + lane;
       const double inv = 1.0 / SQRT2_LEGACY;
       int i = 0;
       for (int u = rg.x; i < rg.y; ++u, ++i) {
@@ -706,54 +710,47 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int nch;
         unit_info<SYN>(P, M, u, i, unit, nch);
         const int m = unit.x;
-        const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
+        const uint32_t lanebase = tmem + PAR_COLS * (uint32_t)par + ((uint32_t)(32 * (warp & 3)) << 16);
         const int le = m + ANA_SPAN * unit.y + 2 * r;   // analysis: even degree of row r
         const int j = 128 * unit.y + r;                 // synthesis: latitude of row r
         const int ncb = (2 * a.nf + 15) / 16;
-        bool okp = true;
         // this thread's output element: analysis, coefficient (le + par, m) of every field (when
         // le + par <= L); synthesis, latitude j (when j < nh), order m, component par
         const long long abase = (long long)P.moff[m] + (le - m);
         const size_t sbase = ((size_t)j * P.nm + m) * 2, sfield = (size_t)P.nh * P.nm * 2;
-        for (int par = 0; par < 2; ++par) {
-          const bool w = mbar_wait(M.b(BAR_ACCUM + par), (uint32_t)(i & 1), ab);
-          if (!__all_sync(0xffffffffu, w)) {
-            okp = false;
-            break;
+        const bool w = mbar_wait(M.b(BAR_ACCUM + par), (uint32_t)(i & 1), ab);
+        if (!__all_sync(0xffffffffu, w)) break;
+        tc_fence_after();
+        const bool live = SYN ? (j < P.nh) : (le + par <= L);
+        for (int cb = 0; cb < ncb; ++cb) {
+          double v[16];
+          if (nch > 0) {
+            acc_read(lanebase, nch, cb, v);
+          } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = 0.0;
           }
-          tc_fence_after();
-          const bool live = SYN ? (j < P.nh) : (le + par <= L);
-          for (int cb = 0; cb < ncb; ++cb) {
-            double v[16];
-            if (nch > 0) {
-              acc_read(lanebase + PAR_COLS * (uint32_t)par, nch, cb, v);
+          if (cb == ncb - 1) {
+            // this parity's accumulators are in registers: its TMEM half goes to the next unit
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(M.b(BAR_TFREE + par));
+          }
+          if (!live) continue;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int f = 8 * cb + q;
+            if (f >= a.nf || !M.active[f]) continue;
+            if (SYN) {
+              // the even- and odd-degree sums E, O of latitude j (the unfold forms E +- O)
+              reinterpret_cast<float2*>(P.mx_gns)[f * sfield + sbase + par] =
+                  make_float2((float)v[2 * q], (float)v[2 * q + 1]);
             } else {
-#pragma unroll
-              for (int q = 0; q < 16; ++q) v[q] = 0.0;
-            }
-            if (cb == ncb - 1) {
-              // this parity's accumulators are in registers: its TMEM half goes to the next unit
-              tc_fence_before();
-              __syncwarp();
-              if (lane == 0) mbar_arrive(M.b(BAR_TFREE + par));
-            }
-            if (!live) continue;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-              const int f = 8 * cb + q;
-              if (f >= a.nf || !M.active[f]) continue;
-              if (SYN) {
-                // the even- and odd-degree sums E, O of latitude j (the unfold forms E +- O)
-                reinterpret_cast<float2*>(P.mx_gns)[f * sfield + sbase + par] =
-                    make_float2((float)v[2 * q], (float)v[2 * q + 1]);
-              } else {
-                a.spec[f][abase + par] = make_double2(v[2 * q] * inv, v[2 * q + 1] * inv);
-              }
+              a.spec[f][abase + par] = make_double2(v[2 * q] * inv, v[2 * q + 1] * inv);
             }
           }
         }
-        if (!okp) break;
-        if (!SYN && m == 0 && unit.y == 0) {
+        if (!SYN && par == 0 && m == 0 && unit.y == 0) {
           // degree 0 in FP64 from the row sums of the fold: U_00 = sqrt(0.5) sum_j S_0(j) / 1.41421356;
           // warp w sums the fields w, w + 4, ... (lane-strided partial sums, then a fixed
           // butterfly: the same order in every launch)
