@@ -81,10 +81,11 @@ static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too sm
 
 static_assert(NSTAGE_MAX % 2 == 0, "a stage must always hold halves of one parity");
 
-// Synthesis sums: per field [m][nh / 4][E, O][4] FP32 complex: entry (m, latitude j, parity par),
-// four consecutive latitudes of one (order, parity) in one 32-byte sector.
+// Synthesis sums: per field [nh / 4][m][E, O][4] FP32 complex: entry (m, latitude j, parity par),
+// four consecutive latitudes of one (order, parity) in one 32-byte sector, and the sums of one
+// group of four latitudes contiguous (nm x 64 bytes).
 __host__ __device__ __forceinline__ size_t gns_index(int f, int m, int j, int par, int nm, int nh) {
-  return (((size_t)f * nm + m) * (size_t)(nh >> 2) + (size_t)(j >> 2)) * 8 + (size_t)(par * 4 + (j & 3));
+  return (((size_t)f * (size_t)(nh >> 2) + (size_t)(j >> 2)) * nm + m) * 8 + (size_t)(par * 4 + (j & 3));
 }
 static_assert(mx_smem(NSTAGE_MAX) <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
 static_assert(TILE_B == MX_NMAX * 128, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
@@ -888,20 +889,31 @@ __global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k
 // above; north = E + O and south = E - O formed in FP32 as they are read) for the NP latitude
 // pairs j0 = NP blockIdx.x .. j0 + NP - 1, unnormalised inverse real FFT in FP32; the output rows
 // get the FP64 degree-0 term 1.41421356 sqrt(0.5) Re U_00 added in FP64; optional epilogue
-// out2 = grid * mul2.  Row r of the block is latitude pair r / 2, north (r even) or south.  The
-// half-length complex packing of the real inverse transform is formed while the first FFT pass
-// reads its inputs; the last pass writes the output rows.  With NP = 4 the block's latitudes of
-// one (order, parity) are one 32-byte sector of the sums.
+// out2 = grid * mul2.  Row r of the block is latitude pair r / 2, north (r even) or south.  With
+// NP = 4 the block's sums are one contiguous run of nm x 64 bytes, staged in shared memory with
+// 16-byte loads before the transform; with NP = 1 (row FFTs too long for four pairs per block)
+// they are read where they lie.  The half-length complex packing of the real inverse transform
+// is formed while the first FFT pass reads its inputs; the last pass writes the output rows.
+// Offset (float2 entries, even) of the staged sums after the FFT rows of an unfold block.
+__host__ __device__ constexpr int unfold_stage_offset(int np, int n2) { return (fpad(2 * np * n2) + 8 * np + 2) & ~1; }
+
 template <int N, int NP>
 struct UnfoldSrcMx {
-  const float2* G;   // the sums of field f: [m][nh / 4][E, O][4] (gns_index)
+  const float2* G;   // NP = 4: the staged run [m][E, O][4]; NP = 1: the field's sums (gns_index)
   const float2* tw;
   int nm, nh, j0;
   __device__ __forceinline__ float2 g(int r, int m) const {
     if (m >= nm) return make_float2(0.f, 0.f);
-    const int j = j0 + (r >> 1);
-    const float2* e = G + gns_index(0, m, j, 0, nm, nh);
-    const float2 E = __ldg(e), O = __ldg(e + 4);
+    float2 E, O;
+    if constexpr (NP == 4) {
+      const float2* e = G + m * 8 + (r >> 1);
+      E = e[0];
+      O = e[4];
+    } else {
+      const float2* e = G + gns_index(0, m, j0, 0, nm, nh);
+      E = __ldg(e);
+      O = __ldg(e + 4);
+    }
     return (r & 1) ? make_float2(E.x - O.x, E.y - O.y) : make_float2(E.x + O.x, E.y + O.y);
   }
   __device__ __forceinline__ float2 operator()(int r, int m) const {
@@ -945,10 +957,19 @@ struct GridRowsOutMx {
 template <int N, int NP>
 __global__ void __launch_bounds__(fft_nt(2 * NP, N)) k_unfold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ float2 smf2[];
+  constexpr int NT = fft_nt(2 * NP, N);
   float2* A = smf2;
   const int j0 = NP * blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
-  const float2* G = reinterpret_cast<const float2*>(P.mx_gns) + gns_index(f, 0, 0, 0, P.nm, P.nh);
+  const float2* G = reinterpret_cast<const float2*>(P.mx_gns) + gns_index(f, 0, NP == 4 ? j0 : 0, 0, P.nm, P.nh);
+  if constexpr (NP == 4) {
+    // the block's run of sums -> shared memory, after the FFT rows
+    float4* st = reinterpret_cast<float4*>(smf2 + unfold_stage_offset(NP, N));
+    const float4* src = reinterpret_cast<const float4*>(G);
+    for (int e = threadIdx.x; e < P.nm * 4; e += NT) st[e] = __ldg(src + e);
+    __syncthreads();
+    G = reinterpret_cast<const float2*>(st);
+  }
   const double c00 = __dmul_rn(__dmul_rn(SQRT2_LEGACY, a.spec[f][0].x), __dsqrt_rn(0.5));
   double* out2 = a.epi_out[f];
   const GridRowsOutMx rows{reinterpret_cast<double2*>(a.grid[f]), reinterpret_cast<double2*>(out2),
@@ -979,7 +1000,11 @@ size_t mx_fold_smem(const ShtDev& d, int nr) { return fft_smem_bytes(nr, d.n2, s
 // latitude pairs per block of the unfold: four (32-byte sectors of the sums) while the block's
 // row FFTs fit in 1024 threads
 constexpr int unfold_pairs(int n2) { return fft_nt(8, n2) <= 1024 ? 4 : 1; }
-size_t mx_unfold_smem(const ShtDev& d) { return fft_smem_bytes(2 * unfold_pairs(d.n2), d.n2, sizeof(float2)); }
+size_t mx_unfold_smem(const ShtDev& d) {
+  const int np = unfold_pairs(d.n2);
+  return np == 4 ? (size_t)unfold_stage_offset(np, d.n2) * sizeof(float2) + (size_t)d.nm * 64
+                 : fft_smem_bytes(2 * np, d.n2, sizeof(float2));
+}
 
 template <typename T>
 int mx_alloc(T** p, size_t n) {
