@@ -70,7 +70,7 @@ struct ShtDev {
   // mixed-precision transforms (set once the plan prepared them)
   const float2* twf;          // [n2] FP32 twiddles of the mixed-precision row FFTs
   float* mx_xf;               // [MX_MAXF][nm][2][nh][2] folded FP32 rFFT: S, D (complex) per order
-  float2* mx_gns;             // [MX_MAXF][nm][nh / 4][2][4] even / odd-degree Legendre sums (synthesis)
+  float2* mx_gns;             // [MX_MAXF][nh][nm][2] even / odd-degree Legendre sums (synthesis)
   float* mx_bsyn;             // [nseg][2][MX_NMAX][32] synthesis B operand (FP32, tile order)
   double* mx_s0;              // [MX_MAXF][nh] FP64 fold of the row sums (degree 0)
   int* mx_abort;              // raised by a tensor-core kernel whose wait timed out

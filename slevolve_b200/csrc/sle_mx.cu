@@ -80,13 +80,6 @@ constexpr int NCOLS = MX_NMAX;                // accumulator columns of every la
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
 
 static_assert(NSTAGE_MAX % 2 == 0, "a stage must always hold halves of one parity");
-
-// Synthesis sums: per field [nh / 4][m][E, O][4] FP32 complex: entry (m, latitude j, parity par),
-// four consecutive latitudes of one (order, parity) in one 32-byte sector, and the sums of one
-// group of four latitudes contiguous (nm x 64 bytes).
-__host__ __device__ __forceinline__ size_t gns_index(int f, int m, int j, int par, int nm, int nh) {
-  return (((size_t)f * (size_t)(nh >> 2) + (size_t)(j >> 2)) * nm + m) * 8 + (size_t)(par * 4 + (j & 3));
-}
 static_assert(mx_smem(NSTAGE_MAX) <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
 static_assert(TILE_B == MX_NMAX * 128, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
 static_assert(2 * NPAIR * 2 * MX_NMAX <= (int)TMEM_COLS && NPAIR * 2 * MX_NMAX == (int)PAR_COLS,
@@ -724,7 +717,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // this thread's output element: analysis, coefficient (le + par, m) of every field (when
         // le + par <= L); synthesis, latitude j (when j < nh), order m, component par
         const long long abase = (long long)P.moff[m] + (le - m);
-        const size_t sbase = gns_index(0, m, j, par, P.nm, P.nh), sfield = gns_index(1, 0, 0, 0, P.nm, P.nh);
+        const size_t sbase = ((size_t)j * P.nm + m) * 2, sfield = (size_t)P.nh * P.nm * 2;
         const bool w = mbar_wait(M.b(BAR_ACCUM + par), (uint32_t)(i & 1), ab);
         if (!__all_sync(0xffffffffu, w)) break;
         tc_fence_after();
@@ -750,7 +743,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (f >= a.nf || !M.active[f]) continue;
             if (SYN) {
               // the even- and odd-degree sums E, O of latitude j (the unfold forms E +- O)
-              reinterpret_cast<float2*>(P.mx_gns)[f * sfield + sbase] =
+              reinterpret_cast<float2*>(P.mx_gns)[f * sfield + sbase + par] =
                   make_float2((float)v[2 * q], (float)v[2 * q + 1]);
             } else {
               a.spec[f][abase + par] = make_double2(v[2 * q] * inv, v[2 * q + 1] * inv);
@@ -886,35 +879,20 @@ __global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k
 }
 
 // Inverse: even- and odd-degree Legendre sums E, O of field blockIdx.y (FP32, m <= lmax, 0
-// above; north = E + O and south = E - O formed in FP32 as they are read) for the NP latitude
-// pairs j0 = NP blockIdx.x .. j0 + NP - 1, unnormalised inverse real FFT in FP32; the output rows
-// get the FP64 degree-0 term 1.41421356 sqrt(0.5) Re U_00 added in FP64; optional epilogue
-// out2 = grid * mul2.  Row r of the block is latitude pair r / 2, north (r even) or south.  With
-// NP = 4 the block's sums are one contiguous run of nm x 64 bytes, staged in shared memory with
-// 16-byte loads before the transform; with NP = 1 (row FFTs too long for four pairs per block)
-// they are read where they lie.  The half-length complex packing of the real inverse transform
-// is formed while the first FFT pass reads its inputs; the last pass writes the output rows.
-// Offset (float2 entries, even) of the staged sums after the FFT rows of an unfold block.
-__host__ __device__ constexpr int unfold_stage_offset(int np, int n2) { return (fpad(2 * np * n2) + 8 * np + 2) & ~1; }
-
-template <int N, int NP>
+// above; one 16-byte entry per order, north = E + O and south = E - O formed in FP32 as they are
+// read), unnormalised inverse real FFT in FP32; the output rows get the FP64
+// degree-0 term 1.41421356 sqrt(0.5) Re U_00 added in FP64; optional epilogue out2 = grid * mul2.
+// The half-length complex packing of the real inverse transform is formed while the first FFT
+// pass reads its inputs; the last pass writes the output rows.
+template <int N>
 struct UnfoldSrcMx {
-  const float2* G;   // NP = 4: the staged run [m][E, O][4]; NP = 1: the field's sums (gns_index)
+  const float4* G;   // [m] of this latitude pair
   const float2* tw;
-  int nm, nh, j0;
+  int nm;
   __device__ __forceinline__ float2 g(int r, int m) const {
     if (m >= nm) return make_float2(0.f, 0.f);
-    float2 E, O;
-    if constexpr (NP == 4) {
-      const float2* e = G + m * 8 + (r >> 1);
-      E = e[0];
-      O = e[4];
-    } else {
-      const float2* e = G + gns_index(0, m, j0, 0, nm, nh);
-      E = __ldg(e);
-      O = __ldg(e + 4);
-    }
-    return (r & 1) ? make_float2(E.x - O.x, E.y - O.y) : make_float2(E.x + O.x, E.y + O.y);
+    const float4 v = __ldg(G + m);   // (E, O): north = E + O, south = E - O
+    return r ? make_float2(v.x - v.z, v.y - v.w) : make_float2(v.x + v.z, v.y + v.w);
   }
   __device__ __forceinline__ float2 operator()(int r, int m) const {
     float2 x, y;
@@ -934,47 +912,33 @@ struct UnfoldSrcMx {
   }
 };
 
-// FP32 values of the inverse FFT -> FP64 grid rows plus the degree-0 term; row r of the block is
-// latitude j0 + r / 2 (r even) or its southern mirror (r odd).
+// FP32 values of the inverse FFT -> FP64 grid rows plus the degree-0 term.
 struct GridRowsOutMx {
-  double2* grid;          // [nlat][N] complex pairs of the output grid
-  double2* out2;          // optional grid * mul2
-  const double2* mul2;
-  int j0, nlat, n;
+  GridRowsOut out;
   double c00;
   __device__ __forceinline__ void put(int r, int i, float2 v) const {
-    const int jr = (r & 1) ? nlat - 1 - (j0 + (r >> 1)) : j0 + (r >> 1);
-    const size_t o = (size_t)jr * n + i;
-    const double2 x = make_double2((double)v.x + c00, (double)v.y + c00);
-    grid[o] = x;
-    if (out2) {
-      const double2 w = __ldg(mul2 + o);
-      out2[o] = make_double2(x.x * w.x, x.y * w.y);
-    }
+    out.put(r, i, make_double2((double)v.x + c00, (double)v.y + c00));
   }
 };
 
-template <int N, int NP>
-__global__ void __launch_bounds__(fft_nt(2 * NP, N)) k_unfold_mx(ShtDev P, MxFieldArgs a) {
+template <int N>
+__global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ float2 smf2[];
-  constexpr int NT = fft_nt(2 * NP, N);
   float2* A = smf2;
-  const int j0 = NP * blockIdx.x, f = blockIdx.y;
+  const int j = blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
-  const float2* G = reinterpret_cast<const float2*>(P.mx_gns) + gns_index(f, 0, NP == 4 ? j0 : 0, 0, P.nm, P.nh);
-  if constexpr (NP == 4) {
-    // the block's run of sums -> shared memory, after the FFT rows
-    float4* st = reinterpret_cast<float4*>(smf2 + unfold_stage_offset(NP, N));
-    const float4* src = reinterpret_cast<const float4*>(G);
-    for (int e = threadIdx.x; e < P.nm * 4; e += NT) st[e] = __ldg(src + e);
-    __syncthreads();
-    G = reinterpret_cast<const float2*>(st);
-  }
+  const int js = P.nlat - 1 - j;
+  const float4* G = reinterpret_cast<const float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm;
   const double c00 = __dmul_rn(__dmul_rn(SQRT2_LEGACY, a.spec[f][0].x), __dsqrt_rn(0.5));
+  const size_t ro = (size_t)j * (2 * N), rso = (size_t)js * (2 * N);
   double* out2 = a.epi_out[f];
-  const GridRowsOutMx rows{reinterpret_cast<double2*>(a.grid[f]), reinterpret_cast<double2*>(out2),
-                           out2 ? reinterpret_cast<const double2*>(a.epi_mul[f]) : nullptr, j0, P.nlat, N, c00};
-  fft_rows<2 * NP, N, true>(UnfoldSrcMx<N, NP>{G, P.twf, P.nm, P.nh, j0}, A, P.twf, rows);
+  const double* mul2 = a.epi_mul[f];
+  const GridRowsOut rows{reinterpret_cast<double2*>(a.grid[f] + ro), reinterpret_cast<double2*>(a.grid[f] + rso),
+                         out2 ? reinterpret_cast<double2*>(out2 + ro) : nullptr,
+                         out2 ? reinterpret_cast<double2*>(out2 + rso) : nullptr,
+                         out2 ? reinterpret_cast<const double2*>(mul2 + ro) : nullptr,
+                         out2 ? reinterpret_cast<const double2*>(mul2 + rso) : nullptr};
+  fft_rows<2, N, true>(UnfoldSrcMx<N>{G, P.twf, P.nm}, A, P.twf, GridRowsOutMx{rows, c00});
 }
 
 // Synthesis B operand: per segment s (order m, degrees l0..l0+63) and parity, rows 2f / 2f+1 =
@@ -997,14 +961,7 @@ __global__ void __launch_bounds__(256) k_bsyn_mx(ShtDev P, MxFieldArgs a) {
 }
 
 size_t mx_fold_smem(const ShtDev& d, int nr) { return fft_smem_bytes(nr, d.n2, sizeof(float2)); }
-// latitude pairs per block of the unfold: four (32-byte sectors of the sums) while the block's
-// row FFTs fit in 1024 threads
-constexpr int unfold_pairs(int n2) { return fft_nt(8, n2) <= 1024 ? 4 : 1; }
-size_t mx_unfold_smem(const ShtDev& d) {
-  const int np = unfold_pairs(d.n2);
-  return np == 4 ? (size_t)unfold_stage_offset(np, d.n2) * sizeof(float2) + (size_t)d.nm * 64
-                 : fft_smem_bytes(2 * np, d.n2, sizeof(float2));
-}
+size_t mx_unfold_smem(const ShtDev& d) { return fft_smem_bytes(2, d.n2, sizeof(float2)); }
 
 template <typename T>
 int mx_alloc(T** p, size_t n) {
@@ -1213,9 +1170,8 @@ int sht_mx_prepare(sle_sht* p) {
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_fold_smem(d, 8)));    \
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
-    SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN, unfold_pairs(NN)>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                  (int)mx_unfold_smem(d)));                                                    \
-    SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN, unfold_pairs(NN)>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
+    SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_unfold_smem(d)));      \
+    SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
   } while (0)
   SLE_FFT_SWITCH(d.n2, SLE_ATTR_MX)
 #undef SLE_ATTR_MX
@@ -1274,9 +1230,7 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t
     k_leg_tc<true, 4><<<p->n_syn_cta, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, 0);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
-#define SLE_LAUNCH_MXU(NN)                                                                                   \
-  k_unfold_mx<NN, unfold_pairs(NN)><<<dim3(d.nh / unfold_pairs(NN), a.nf), fft_threads(2 * unfold_pairs(NN), NN), \
-                                     mx_unfold_smem(d), st>>>(d, a)
+#define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXU)
 #undef SLE_LAUNCH_MXU
   prof_end(t1, st);
