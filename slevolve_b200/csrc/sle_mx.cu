@@ -75,7 +75,12 @@ constexpr uint32_t PAR_COLS = 256;            // TMEM columns per parity: NPAIR 
 constexpr int NPAIR = 2;                      // accumulator pairs (chunk k into pair k mod NPAIR)
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
 constexpr int MAX_CTA_UNITS = 16;            // work units per CTA staged in shared memory
-constexpr double UNIT_COST_HALVES = 32.0;     // fixed cost of a work unit (epilogue), in half-chunk times
+// fixed cost of a work unit (its epilogue), in half-chunk times, from per-CTA timings at L = 511
+// with 32 fields: analysis ~1400 cycles per half + ~4500 per unit (coefficients written two
+// 16-byte entries per lane), synthesis ~570 per half + ~13800 per unit (sums written one line
+// per lane)
+constexpr double ANA_UNIT_COST = 3.0;
+constexpr double SYN_UNIT_COST = 24.0;
 constexpr int NCOLS = MX_NMAX;                // accumulator columns of every launch (2 per field slot)
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
 
@@ -1042,7 +1047,7 @@ int sht_mx_prepare(sle_sht* p) {
       const int nd = std::min(ANA_SPAN, nl - ANA_SPAN * s);
       int kstart = d.ngrp;
       for (int q = 0; q * SEG < nd; ++q) kstart = std::min(kstart, (int)ist[segoff[m] + (ANA_SPAN / SEG) * s + q]);
-      au.push_back({2.0 * (d.ngrp - kstart) + UNIT_COST_HALVES, m, s, kstart});
+      au.push_back({2.0 * (d.ngrp - kstart) + ANA_UNIT_COST, m, s, kstart});
     }
     const int ntile = (d.nh + 127) / 128;
     for (int t = 0; t < ntile; ++t) {
@@ -1050,7 +1055,7 @@ int sht_mx_prepare(sle_sht* p) {
       const int glast = std::min(d.ngrp, 4 * t + 4) - 1;
       for (int seg = segoff[m]; seg < segoff[m + 1]; ++seg)
         if ((int)ist[seg] <= glast) u.segs.push_back(seg);
-      u.w = 2.0 * u.segs.size() + UNIT_COST_HALVES;
+      u.w = 2.0 * u.segs.size() + SYN_UNIT_COST;
       su.push_back(u);
     }
   }
