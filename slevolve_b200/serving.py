@@ -97,6 +97,15 @@ class _Running:
         self.image = None   # host snapshot while preempted
 
 
+def _room():
+    """Device bytes an allocation can still get: free device memory plus the blocks torch's
+    caching allocator holds without using."""
+    import torch
+
+    free = torch.cuda.mem_get_info()[0]
+    return free + max(0, torch.cuda.memory_reserved() - torch.cuda.memory_allocated())
+
+
 class Server:
     """groups: {lmax: slots}.  budget_bytes: device memory the admitted requests may hold (their
     slots' solver state plus the reuse stores of outer requests).  The slot batches are allocated
@@ -214,10 +223,14 @@ class Server:
                     return
                 if resumed is None and req.outer_passes > 1:
                     # the store is allocated under the lock, once the device has room for it
-                    import torch
+                    # (free device memory plus what torch's allocator holds unused)
+                    need = store_bytes(req) + self.store_margin
+                    if _room() < need:
+                        import torch
 
-                    if torch.cuda.mem_get_info()[0] < store_bytes(req) + self.store_margin:
-                        return
+                        torch.cuda.empty_cache()
+                        if _room() < need:
+                            return
                     n = req.lmax + 1
                     store = ReuseStore(n * (n + 1) // 2, n * 2 * n, capacity=req.nsteps)
                 self.used += fp
