@@ -826,20 +826,18 @@ __global__ void k_refresh2_x8(Dev D) {
 }
 
 // dice, dI after a grounded-mask change.  Such a change is rare after the first iterations, so
-// the launch is a fixed grid that goes over the slots in turn: a slot whose mask did not change
-// costs each thread one flag read, one that changed is spread over the whole grid.
-__global__ void __launch_bounds__(256) k_dice(Dev D, int nslots) {
+// each slot gets a fixed row of blocks that stride over its coefficients: a slot whose mask did
+// not change costs DICE_BLOCKS early exits instead of one per 256 coefficients.
+constexpr int DICE_BLOCKS = 64;
+__global__ void __launch_bounds__(256) k_dice(Dev D) {
+  SLOT_OR_RETURN();
+  if (sc->converged || !sc->gr_changed) return;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (int s = 0; s < nslots; ++s) {
-    const int b = D.slot0 + s;
-    const Scal* sc = D.sc + b;
-    if (sc->done || sc->converged || !sc->gr_changed) continue;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < D.ncoef; i += stride) {
-      const double2 a = D.sp(S_ICELM, b)[i], o = D.sp(S_OLDICE, b)[i], p = D.sp(S_P_ICE, b)[i];
-      const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
-      D.sp(S_DICE, b)[i] = d;
-      D.sp(S_DI, b)[i] = make_double2(__dadd_rn(p.x, d.x), __dadd_rn(p.y, d.y));
-    }
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < D.ncoef; i += stride) {
+    const double2 a = D.sp(S_ICELM, b)[i], o = D.sp(S_OLDICE, b)[i], p = D.sp(S_P_ICE, b)[i];
+    const double2 d = make_double2(__dsub_rn(a.x, o.x), __dsub_rn(a.y, o.y));
+    D.sp(S_DICE, b)[i] = d;
+    D.sp(S_DI, b)[i] = make_double2(__dadd_rn(p.x, d.x), __dadd_rn(p.y, d.y));
   }
 }
 
@@ -1227,7 +1225,6 @@ struct SlotHost {
 struct sle_batch {
   sle_config cfg;
   int nslot, K;
-  int nsm;                       // SMs of the device (grids of the rarely-open passes)
   sle_sht* plan;
   cudaStream_t st;
   Dev D;
@@ -1419,7 +1416,7 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_regr.data(), (int)s->f_ana_regr.size(), st));
   note_launch(2);
   t = prof_begin(PROF_DICE, act, st);
-  k_dice<<<std::min(nb(nc), (unsigned)(2 * s->nsm)), 256, 0, st>>>(D, (int)B);
+  k_dice<<<dim3(std::min(nb(nc), (unsigned)DICE_BLOCKS), B), 256, 0, st>>>(D);
   prof_end(t, st);
   k_loop_cond<<<1, 128, 0, st>>>(D, s->bstatus, loop);
   SLE_CUDA(cudaGetLastError());
@@ -1649,12 +1646,6 @@ int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
   s->cfg = *cfg;
   s->nslot = nslot;
   s->K = kmax;
-  {
-    int dev = 0, nsm = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-      nsm = 148;
-    s->nsm = nsm > 0 ? nsm : 148;
-  }
   int rc = sle_sht_create(cfg->nlat, cfg->nlon, cfg->lmax, &s->plan);
   if (rc != SLE_OK) {
     delete s;
