@@ -62,7 +62,8 @@ constexpr int TILE_B = MX_NMAX * 128;         // MX_NMAX rows x 128 bytes = 8 KB
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;   // one parity of a chunk: A hi / lo, B hi / lo
 constexpr int NSTAGE_MAX = 4;                 // pipeline stages: 2 or 4 (a launch-time choice)
 constexpr int MISC_BYTES = 1024;              // barriers + bookkeeping
-constexpr int mx_smem(int nst) { return 1024 + nst * STAGE_BYTES + MISC_BYTES; }
+constexpr int EVEN_BYTES = 128 * MX_NMAX * 4;   // synthesis: the even-degree sums of a unit (FP32, 128 rows)
+constexpr int mx_smem(int nst, bool syn = false) { return 1024 + nst * STAGE_BYTES + MISC_BYTES + (syn ? EVEN_BYTES : 0); }
 constexpr int W_SPL = 4;                      // warps 4..11: splitters (two groups of four)
 constexpr int W_MMA = 12;                     // TMEM owner, MMA issue
 constexpr int W_LOAD = 13;                    // bulk / TMA loads
@@ -85,7 +86,7 @@ constexpr int NCOLS = MX_NMAX;                // accumulator columns of every la
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
 
 static_assert(NSTAGE_MAX % 2 == 0, "a stage must always hold halves of one parity");
-static_assert(mx_smem(NSTAGE_MAX) <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
+static_assert(mx_smem(NSTAGE_MAX, true) <= 232448, "mixed transform shared memory exceeds the sm_100a limit");
 static_assert(TILE_B == MX_NMAX * 128, "full-width MMAs read B hi and B lo as one tile of 2 MX_NMAX rows");
 static_assert(2 * NPAIR * 2 * MX_NMAX <= (int)TMEM_COLS && NPAIR * 2 * MX_NMAX == (int)PAR_COLS,
               "accumulators exceed TMEM");
@@ -301,6 +302,7 @@ struct Smem {
   }
   __device__ uint8_t* b_ptr(int stage, int lo) const { return base + stage * STAGE_BYTES + 2 * TILE_A + lo * TILE_B; }
   __device__ uint8_t* misc() const { return base + nst * STAGE_BYTES; }
+  __device__ float* even() const { return reinterpret_cast<float*>(base + nst * STAGE_BYTES + MISC_BYTES); }
 };
 
 __device__ __forceinline__ Smem smem_layout(uint8_t* raw, int nst) {
@@ -389,7 +391,8 @@ __device__ __forceinline__ void acc_read(uint32_t base, int nch, int cb, double 
 }
 
 // Common prologue: barriers, gates, TMEM.  Returns the TMEM base (all threads).
-__device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a, const int4* units, int2 rg) {
+__device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a, const int4* units, int2 rg,
+                             int tfree_warps) {
   const int warp = threadIdx.x >> 5;
   if (threadIdx.x < MAX_CTA_UNITS && (int)threadIdx.x < rg.y) M.units[threadIdx.x] = units[rg.x + threadIdx.x];
   if (threadIdx.x == 0) {
@@ -400,7 +403,7 @@ __device__ uint32_t prologue(const Smem& S, const Misc& M, const MxFieldArgs& a,
     }
     for (int i = 0; i < 2; ++i) {
       mbar_init(M.b(BAR_ACCUM + i), 1);   // one tcgen05.commit (or arrive for an empty unit)
-      mbar_init(M.b(BAR_TFREE + i), 4);   // the 4 epilogue warps
+      mbar_init(M.b(BAR_TFREE + i), tfree_warps);   // the epilogue warps that read the parity
     }
     mbar_init(M.b(BAR_DRAIN), 1);
     fence_mbar_init();
@@ -601,7 +604,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const uint32_t* tab = SYN ? P.mx_tab_syn : P.mx_tab_ana;
   // this CTA's work units: rg.y units from rg.x on (the plan balances the CTAs' totals)
   const int2 rg = (SYN ? P.mx_syn_cta : P.mx_ana_cta)[blockIdx.x];
-  const uint32_t tmem = prologue(S, M, a, SYN ? P.mx_syn_units : P.mx_ana_units, rg);
+  const uint32_t tmem = prologue(S, M, a, SYN ? P.mx_syn_units : P.mx_ana_units, rg, SYN ? 8 : 4);
   if (*M.any && *reinterpret_cast<volatile int*>(P.mx_abort) == 0) {
     const int nrow = 2 * a.nf;
     if (warp == W_LOAD) {
@@ -703,8 +706,68 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           if (lane == 0) mbar_arrive(M.b(BAR_FULL + st));
         }
       }
+    } else if (SYN) {
+      // ---- synthesis epilogue: warps 0-3 take the fields 0-15, warps 14-17 the fields 16-31
+      // (column blocks 2h, 2h + 1 for group h), of both parities; warp w owns TMEM lanes
+      // 32 (w mod 4) .. 32 (w mod 4) + 31.  The even-degree sums wait in shared memory (FP32, each
+      // thread its own row: [column][row]) until the odd-degree ones are read, so that each
+      // (field, latitude, order) gets one 16-byte store.
+      const int h = warp >= W_EPI1 ? 1 : 0;
+      const int r = 32 * (warp & 3) + lane;
+      int i = 0;
+      for (int u = rg.x; i < rg.y; ++u, ++i) {
+        int4 unit;
+        int nch;
+        unit_info<SYN>(P, M, u, i, unit, nch);
+        const int m = unit.x;
+        const int j = 128 * unit.y + r;                 // latitude of row r
+        const uint32_t rowbase = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+        const int ncb = (2 * a.nf + 15) / 16;
+        const int cb0 = 2 * h, cb1 = min(ncb, 2 * h + 2);
+        float4* gq = reinterpret_cast<float4*>(P.mx_gns) + (size_t)j * P.nm + m;
+        const size_t gfield = (size_t)P.nh * P.nm;
+        float* ev = S.even() + r;
+        bool okp = true;
+        for (int par = 0; par < 2; ++par) {
+          const bool w = mbar_wait(M.b(BAR_ACCUM + par), (uint32_t)(i & 1), ab);
+          if (!__all_sync(0xffffffffu, w)) {
+            okp = false;
+            break;
+          }
+          tc_fence_after();
+#pragma unroll 1
+          for (int cb = cb0; cb < cb1; ++cb) {
+            double v[16];
+            if (nch > 0) {
+              acc_read(rowbase + PAR_COLS * (uint32_t)par, nch, cb, v);
+            } else {
+#pragma unroll
+              for (int q = 0; q < 16; ++q) v[q] = 0.0;
+            }
+            if (par == 0) {
+#pragma unroll
+              for (int q = 0; q < 16; ++q) ev[(16 * cb + q) * 128] = (float)v[q];
+            } else if (j < P.nh) {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                const int f = 8 * cb + q;
+                if (f >= a.nf || !M.active[f]) continue;
+                // the even- and odd-degree sums E, O of latitude j (the unfold forms E +- O)
+                gq[f * gfield] = make_float4(ev[(16 * cb + 2 * q) * 128], ev[(16 * cb + 2 * q + 1) * 128], (float)v[2 * q],
+                                             (float)v[2 * q + 1]);
+              }
+            }
+          }
+          // this group's columns of the parity are in registers: its TMEM half goes to the next
+          // unit once both groups have read it
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(M.b(BAR_TFREE + par));
+        }
+        if (!okp) break;
+      }
     } else {
-      // ---- epilogue: warps 0-3 (parity 0) and 14-17 (parity 1); warp w owns TMEM lanes
+      // ---- analysis epilogue: warps 0-3 (parity 0) and 14-17 (parity 1); warp w owns TMEM lanes
       // 32 (w mod 4) .. 32 (w mod 4) + 31
       const int par = warp >= W_EPI1 ? 1 : 0;
       const int r = 32 * (warp & 3) + lane;
@@ -716,17 +779,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         unit_info<SYN>(P, M, u, i, unit, nch);
         const int m = unit.x;
         const uint32_t lanebase = tmem + PAR_COLS * (uint32_t)par + ((uint32_t)(32 * (warp & 3)) << 16);
-        const int le = m + ANA_SPAN * unit.y + 2 * r;   // analysis: even degree of row r
-        const int j = 128 * unit.y + r;                 // synthesis: latitude of row r
+        const int le = m + ANA_SPAN * unit.y + 2 * r;   // even degree of row r
         const int ncb = (2 * a.nf + 15) / 16;
-        // this thread's output element: analysis, coefficient (le + par, m) of every field (when
-        // le + par <= L); synthesis, latitude j (when j < nh), order m, component par
+        // this thread's output element: coefficient (le + par, m) of every field (when le + par <= L)
         const long long abase = (long long)P.moff[m] + (le - m);
-        const size_t sbase = ((size_t)j * P.nm + m) * 2, sfield = (size_t)P.nh * P.nm * 2;
         const bool w = mbar_wait(M.b(BAR_ACCUM + par), (uint32_t)(i & 1), ab);
         if (!__all_sync(0xffffffffu, w)) break;
         tc_fence_after();
-        const bool live = SYN ? (j < P.nh) : (le + par <= L);
+        const bool live = le + par <= L;
         for (int cb = 0; cb < ncb; ++cb) {
           double v[16];
           if (nch > 0) {
@@ -746,16 +806,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           for (int q = 0; q < 8; ++q) {
             const int f = 8 * cb + q;
             if (f >= a.nf || !M.active[f]) continue;
-            if (SYN) {
-              // the even- and odd-degree sums E, O of latitude j (the unfold forms E +- O)
-              reinterpret_cast<float2*>(P.mx_gns)[f * sfield + sbase + par] =
-                  make_float2((float)v[2 * q], (float)v[2 * q + 1]);
-            } else {
-              a.spec[f][abase + par] = make_double2(v[2 * q] * inv, v[2 * q + 1] * inv);
-            }
+            a.spec[f][abase + par] = make_double2(v[2 * q] * inv, v[2 * q + 1] * inv);
           }
         }
-        if (!SYN && par == 0 && m == 0 && unit.y == 0) {
+        if (par == 0 && m == 0 && unit.y == 0) {
           // degree 0 in FP64 from the row sums of the fold: U_00 = sqrt(0.5) sum_j S_0(j) / 1.41421356;
           // warp w sums the fields w, w + 4, ... (lane-strided partial sums, then a fixed
           // butterfly: the same order in every launch)
@@ -1166,9 +1220,9 @@ int sht_mx_prepare(sle_sht* p) {
     }
   }
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(2)));
-  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(2)));
+  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(2, true)));
   SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(4)));
-  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(4)));
+  SLE_CUDA(cudaFuncSetAttribute(k_leg_tc<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx_smem(4, true)));
 #define SLE_ATTR_MX(NN)                                                                                        \
   do {                                                                                                         \
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_fold_smem(d, 4)));    \
@@ -1230,9 +1284,9 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t
   ProfToken t0 = prof_begin(PROF_LEG_SYN, a.nf, st);
   k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
   if (p->tune_stages == 2)
-    k_leg_tc<true, 2><<<p->n_syn_cta, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, 0);
+    k_leg_tc<true, 2><<<p->n_syn_cta, TC_THREADS, mx_smem(2, true), st>>>(d, a, status, *map, 0);
   else
-    k_leg_tc<true, 4><<<p->n_syn_cta, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, 0);
+    k_leg_tc<true, 4><<<p->n_syn_cta, TC_THREADS, mx_smem(4, true), st>>>(d, a, status, *map, 0);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
 #define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a)

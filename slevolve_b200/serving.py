@@ -98,12 +98,11 @@ class _Running:
 
 
 def _room():
-    """Device bytes an allocation can still get: free device memory plus the blocks torch's
-    caching allocator holds without using."""
+    """Free device memory.  Blocks that torch's caching allocator holds unused are not counted:
+    they may be too fragmented for a store (the caller empties the cache before giving up)."""
     import torch
 
-    free = torch.cuda.mem_get_info()[0]
-    return free + max(0, torch.cuda.memory_reserved() - torch.cuda.memory_allocated())
+    return torch.cuda.mem_get_info()[0]
 
 
 class Server:
@@ -115,7 +114,7 @@ class Server:
 
     def __init__(self, groups, precision="mixed", budget_bytes=None, max_modes=8, opt=("dsl", "diag"),
                  inner="extrap", record=("deltasl", "tgrid"), preempt=False, device_bytes=None,
-                 store_margin=1 << 30):
+                 store_margin=4 << 30):
         self.precision = precision
         self.store_margin = int(store_margin)
         self.preempt = bool(preempt)
@@ -223,16 +222,22 @@ class Server:
                     return
                 if resumed is None and req.outer_passes > 1:
                     # the store is allocated under the lock, once the device has room for it
-                    # (free device memory plus what torch's allocator holds unused)
+                    # with store_margin to spare (the other groups' steps allocate their ice grids
+                    # meanwhile)
+                    import torch
+
                     need = store_bytes(req) + self.store_margin
                     if _room() < need:
-                        import torch
-
                         torch.cuda.empty_cache()
                         if _room() < need:
                             return
                     n = req.lmax + 1
-                    store = ReuseStore(n * (n + 1) // 2, n * 2 * n, capacity=req.nsteps)
+                    try:
+                        store = ReuseStore(n * (n + 1) // 2, n * 2 * n, capacity=req.nsteps)
+                    except torch.OutOfMemoryError:
+                        # another group's step took the room meanwhile: try again later
+                        torch.cuda.empty_cache()
+                        return
                 self.used += fp
                 self.peak_used = max(self.peak_used, self.used)
                 self._note_used()
