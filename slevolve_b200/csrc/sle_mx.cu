@@ -8,7 +8,8 @@
 // Per order m both are real GEMMs over the complex fields of a launch (2 columns per field):
 //   analysis   D[l][n] = sum_j  P[l][j]  B[n][j],   B = folded FFT (S for even, D for odd l-m)
 //   synthesis  D[j][n] = sum_l  P[l][j]  B[n][l],   B = coefficients of one parity
-// with each operand split into TF32 hi + lo and D += Ahi Bhi + Ahi Blo + Alo Bhi in FP32.
+// with each FP32 operand split as x = hi + lo, hi = x read as TF32 by the MMA (its 13 low
+// mantissa bits ignored) and lo = TF32(x - hi), and D += Ahi Bhi + Ahi Blo + Alo Bhi in FP32.
 //
 // Precision: the Legendre values come from the FP64 recurrence of the plan
 // (Q_l = mu Q_{l-1} + be_l Q_{l-2}, P~ = cf Q), rounded once to FP32 when the plan is prepared
@@ -215,12 +216,12 @@ __host__ __device__ __forceinline__ int sw_off(int row, int k) {
 }
 
 // ------------------------------------------------------------- precision splits
-// x = hi + lo with hi the nearest TF32 of x (ties away from zero) and lo the nearest TF32 of
-// the exact remainder: |x - hi - lo| <= 2^-22 |x| for normal x.
-__device__ __forceinline__ void split_f32(float x, uint32_t& hi, uint32_t& lo) {
-  hi = (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
-  const float r = x - __uint_as_float(hi);
-  lo = (__float_as_uint(r) + 0x1000u) & 0xFFFFE000u;
+// The lo part for a hi part that is x itself read as TF32: a kind::tf32 MMA ignores the 13 low
+// mantissa bits of an FP32 operand, so x serves as hi = trunc(x) unchanged and only
+// lo = TF32(x - trunc(x)) is written (|x - trunc(x) - lo| <= 2^-21 |x|).
+__device__ __forceinline__ uint32_t lo_of_trunc(float x) {
+  const float r = x - __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
+  return (__float_as_uint(r) + 0x1000u) & 0xFFFFE000u;
 }
 
 // ------------------------------------------------------------------ bounded waits
@@ -514,30 +515,26 @@ __global__ void __launch_bounds__(128) k_tab_syn(ShtDev P, uint32_t* tab) {
 }
 
 // ============================================================ Legendre contraction
-// A split: the FP32 Legendre values landed in the hi tiles of the stage; hi <- TF32(x) in
-// place, lo tile <- TF32(x - hi).  Elementwise, so the tile order does not matter.
+// A split: the FP32 Legendre values landed in the hi tile of the stage and serve as hi as they
+// are (the MMA reads them as TF32, trunc(x)); the lo tile gets TF32(x - trunc(x)).  Elementwise,
+// so the tile order does not matter.
 __device__ __forceinline__ void split_a(const Smem& S, int st, int tid) {
   constexpr int NV = TILE_F / 4 / 128;   // 16-byte vectors per thread
-  uint4* hp = reinterpret_cast<uint4*>(S.a_ptr(st, 0));
+  const uint4* hp = reinterpret_cast<const uint4*>(S.a_ptr(st, 0));
   uint4* lp = reinterpret_cast<uint4*>(S.a_ptr(st, 1));
   uint4 v[NV];
 #pragma unroll
   for (int q = 0; q < NV; ++q) v[q] = hp[tid + 128 * q];
 #pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    uint4 h, l;
-    split_f32(__uint_as_float(v[q].x), h.x, l.x);
-    split_f32(__uint_as_float(v[q].y), h.y, l.y);
-    split_f32(__uint_as_float(v[q].z), h.z, l.z);
-    split_f32(__uint_as_float(v[q].w), h.w, l.w);
-    hp[tid + 128 * q] = h;
-    lp[tid + 128 * q] = l;
-  }
+  for (int q = 0; q < NV; ++q)
+    lp[tid + 128 * q] = make_uint4(lo_of_trunc(__uint_as_float(v[q].x)), lo_of_trunc(__uint_as_float(v[q].y)),
+                                   lo_of_trunc(__uint_as_float(v[q].z)), lo_of_trunc(__uint_as_float(v[q].w)));
 }
 
 // Analysis B data of one parity: the TMA box of the folded FFT is [field][32 latitudes][re, im]
 // (8 bytes per entry) in the stage's B lo tile; the 4 splitter warps read it, synchronise, and
-// write rows 2f (re) / 2f+1 (im) of the B hi / lo tiles.
+// write rows 2f (re) / 2f+1 (im) of the B hi tile (the FP32 values, read as TF32 by the MMA)
+// and of the B lo tile (TF32 of x - trunc(x)).
 __device__ __forceinline__ void split_b_ana(const Smem& S, int st, int nf, int tid, int bar_id) {
   const float2* box = reinterpret_cast<const float2*>(S.b_ptr(st, 1));
   float2 v[8];
@@ -555,26 +552,19 @@ __device__ __forceinline__ void split_b_ana(const Smem& S, int st, int nf, int t
     const int f = e >> 5, k = e & 31;
     if (f >= nf) continue;
     const int o0 = sw_off(2 * f, k), o1 = sw_off(2 * f + 1, k);
-    uint32_t h, l;
-    split_f32(v[u].x, h, l);
-    hp[o0] = h;
-    lp[o0] = l;
-    split_f32(v[u].y, h, l);
-    hp[o1] = h;
-    lp[o1] = l;
+    hp[o0] = __float_as_uint(v[u].x);
+    lp[o0] = lo_of_trunc(v[u].x);
+    hp[o1] = __float_as_uint(v[u].y);
+    lp[o1] = lo_of_trunc(v[u].y);
   }
 }
 
-// Synthesis B data of one parity: the raw block is already in the tile order; split in place.
+// Synthesis B data of one parity: the raw block lands in the hi tile, already in the tile order,
+// and serves as hi as it is; the lo tile gets TF32(x - trunc(x)).
 __device__ __forceinline__ void split_b_syn(const Smem& S, int st, int nrow, int tid) {
-  uint32_t* hp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 0));
+  const uint32_t* hp = reinterpret_cast<const uint32_t*>(S.b_ptr(st, 0));
   uint32_t* lp = reinterpret_cast<uint32_t*>(S.b_ptr(st, 1));
-  for (int e = tid; e < nrow * KC; e += 128) {
-    uint32_t h, l;
-    split_f32(__uint_as_float(lp[e]), h, l);
-    hp[e] = h;
-    lp[e] = l;
-  }
+  for (int e = tid; e < nrow * KC; e += 128) lp[e] = lo_of_trunc(__uint_as_float(hp[e]));
 }
 
 // Work unit u (the CTA's i-th): (m, span | latitude tile, chunk count, first table slot).
@@ -629,7 +619,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                      raw);
             if (SYN) {
               const int seg = P.mx_syn_seg[unit.w + k];
-              bulk_g2s(S.b_tile(st, 1), P.mx_bsyn + ((size_t)seg * 2 + par) * BBLOCK, (uint32_t)nrow * 128u, raw);
+              bulk_g2s(S.b_tile(st, 0), P.mx_bsyn + ((size_t)seg * 2 + par) * BBLOCK, (uint32_t)nrow * 128u, raw);
             } else {
               tma_load_4d(S.b_tile(st, 1), &tmx, 2 * KC * (unit.z + k), par, unit.x, 0, raw);
             }
@@ -1174,7 +1164,7 @@ int sht_mx_prepare(sle_sht* p) {
     SLE_CUDA(cudaMemcpy(p->mx_syn_seg, segs.data(), segs.size() * sizeof(int), cudaMemcpyHostToDevice));
   p->n_ana_units = (int)av.size();
   p->n_syn_units = (int)sv.size();
-  // Legendre tables: FP64 recurrence, split into TF32 hi / lo, zero where negligible
+  // Legendre tables: FP64 recurrence rounded to FP32 (the kernel splits them), zero where negligible
   const size_t tab_a = (size_t)na * SLOT_WORDS, tab_s = (size_t)ns * SLOT_WORDS;
   SLE_TRY(mx_alloc(&p->mx_tab_ana, tab_a + 1));
   SLE_TRY(mx_alloc(&p->mx_tab_syn, tab_s + 1));
