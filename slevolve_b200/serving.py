@@ -453,11 +453,14 @@ def uneven_ensemble(n=64, degrees=(127, 255, 511), steps=(50, 1200), seed=202612
     return [mf.make(i, int(L), int(k)) for i, (L, k) in enumerate(zip(Ls, ks))]
 
 
-def run_ensemble(requests, precision="mixed", slots=None, autotune=True, candidates=(8, 16, 32)):
+def run_ensemble(requests, precision="mixed", slots=None, autotune=True, candidates=(8, 16, 32),
+                 tune_shapes=True):
     """Run a set of requests to completion with one slot batch per degree (continuous batching:
     a member that finishes frees its slot for the next one of its degree).  ``slots``: {lmax:
-    slot count}; missing degrees are autotuned (or get min(32, members)).  Returns the server
-    statistics plus the slot choice and the autotune measurements."""
+    slot count}; missing degrees are autotuned (or get min(32, members)).  With ``tune_shapes``,
+    each mixed-precision batch also times the transforms' launch shapes for its slot count and
+    uses the fastest (``SolverBatch.autotune``) before the run.  Returns the server statistics
+    plus the slot choice, the launch shapes and the autotune measurements."""
     degrees = sorted({r.lmax for r in requests})
     slots = dict(slots or {})
     tuned = {}
@@ -473,9 +476,14 @@ def run_ensemble(requests, precision="mixed", slots=None, autotune=True, candida
         else:
             slots[L] = min(32, count)
     srv = Server(slots, precision=precision)
+    shapes = {}
+    if tune_shapes and precision == "mixed":
+        for L, bt in srv.batches.items():
+            shapes[str(L)] = bt.autotune()[0]
     srv.run(requests)
     st = srv.stats(requests)
-    st.update({"slots": {str(k): v for k, v in slots.items()}, "autotune_member_steps_per_s": tuned,
+    st.update({"slots": {str(k): v for k, v in slots.items()}, "launch_shapes": shapes,
+               "autotune_member_steps_per_s": tuned,
                "members": {str(L): sum(1 for r in requests if r.lmax == L) for L in degrees}})
     return st
 
