@@ -26,18 +26,20 @@
 // Every launch computes all MX_NMAX columns with the same accumulation structure, so a field's
 // result does not depend on the other fields of its launch or on the launch shape.
 //
-// Kernel structure (persistent: one CTA per SM over the work units, 14 warps, 2 or 4 stages of
+// Kernel structure (persistent: one CTA per SM over the work units, 18 warps, 2 or 4 stages of
 // one half each (a launch-shape choice), a half being one parity of one 32-wide K chunk):
 //   warp 13     loader: per half, one bulk copy of the FP32 A tile (16 KB) and the B data
 //               (analysis: one 4-D TMA tensor load of the folded FFT; synthesis: one bulk copy)
 //               into stage q % stages
-//   warps 4-11  splitters, group g = parity g: A and B -> TF32 hi / lo tiles
+//   warps 4-11  splitters, group g takes the halves q = g mod 2: the TF32 lo tiles of A and B
+//               (the FP32 tiles serve as hi; the analysis B box is first moved to the hi tile)
 //   warp 12     allocates TMEM and issues the MMAs from one thread: a unit's halves of parity 0
 //               (all its chunks), then those of parity 1, each parity into its own TMEM half
-//   warps 0-3   epilogue of parity 0, warps 14-17 of parity 1 (warp w reads TMEM lanes
-//               32 (w mod 4) ..): read the parity's accumulators out of TMEM (the MMAs of that
-//               parity of the next unit wait for it, those of the other parity run meanwhile),
-//               add them up in FP64 and write the results
+//   warps 0-3   epilogue, two groups (warp w reads TMEM lanes 32 (w mod 4) ..): analysis,
+//   14-17       warps 0-3 parity 0 and warps 14-17 parity 1; synthesis, warps 0-3 fields 0-15 and
+//               warps 14-17 fields 16-31 of both parities.  A parity's TMEM half goes to the next
+//               unit's MMAs of that parity once read (the other parity's MMAs run meanwhile); the
+//               accumulators are added up in FP64 and the results written
 // Stages hand over through mbarriers; tcgen05.commit releases a stage when its MMAs are done.
 // Every wait is bounded: on timeout the CTA raises the plan's abort flag (and the caller's status
 // word), stops waiting, lets issued MMAs and copies land and releases its TMEM.  No load uses
@@ -580,7 +582,8 @@ __device__ __forceinline__ void unit_info(const ShtDev& P, const Misc& M, int u,
 // parity 1 of the same chunks): warp 13 streams each half's Legendre tile and B data into stage
 // q % NST; splitter group g = (warp - 4) / 4 splits the halves q = g mod 2 (the stages of that
 // parity); warp 12 issues the MMAs of a unit's parity p once the epilogue has read parity p of
-// the unit before out of TMEM; warps 0-3 drain the unit parity by parity.
+// the unit before out of TMEM; warps 0-3 and 14-17 drain the unit (analysis: one parity per
+// group; synthesis: one half of the fields per group, both parities).
 template <bool SYN, int NST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox) {
