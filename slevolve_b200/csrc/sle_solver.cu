@@ -635,25 +635,20 @@ __global__ void k_update(Dev D) {
   const double2 x = make_double2(__dadd_rn(__dsub_rn(__dmul_rn(fr, d00.x), r00.x), t00.x),
                                  __dadd_rn(__dsub_rn(__dmul_rn(fr, d00.y), r00.y), t00.y));
   const double conserv = __dsub_rn(__dmul_rn(rinv.x, x.x), __dmul_rn(rinv.y, x.y));
-  // two coefficients per thread (half the blocks, so half the partial sums and fences)
   double acc = 0.0;
-  const long long i0 = 2 * ((long long)blockIdx.x * blockDim.x + threadIdx.x);
-#pragma unroll
-  for (int u = 0; u < 2; ++u) {
-    const long long i = i0 + u;
-    if (i < D.ncoef) {
-      const double2 p = dSprev[i], r = rOlm[i], c = cstarlm[i], t = tOlm[i];
-      double nr = __dadd_rn(-p.x, r.x), ni = __dadd_rn(-p.y, r.y);
-      nr = __dadd_rn(nr, __dmul_rn(c.x, conserv));
-      ni = __dadd_rn(ni, __dmul_rn(c.y, conserv));
-      nr = __dsub_rn(nr, t.x);
-      ni = __dsub_rn(ni, t.y);
-      D.sp(S_LOAD, b)[i] = make_double2(nr, ni);
-      // dS_cur = dS_prev + new: the rotation block of the next iteration reads its degree-2
-      // entries; the commit forms the whole of it from the converged increment (the same sum)
-      if (i == D.i20 || i == D.i21) D.sp(S_DSCUR, b)[i] = make_double2(__dadd_rn(p.x, nr), __dadd_rn(p.y, ni));
-      acc = __dadd_rn(acc, hypot(nr, ni));
-    }
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < D.ncoef) {
+    const double2 p = dSprev[i], r = rOlm[i], c = cstarlm[i], t = tOlm[i];
+    double nr = __dadd_rn(-p.x, r.x), ni = __dadd_rn(-p.y, r.y);
+    nr = __dadd_rn(nr, __dmul_rn(c.x, conserv));
+    ni = __dadd_rn(ni, __dmul_rn(c.y, conserv));
+    nr = __dsub_rn(nr, t.x);
+    ni = __dsub_rn(ni, t.y);
+    D.sp(S_LOAD, b)[i] = make_double2(nr, ni);
+    // dS_cur = dS_prev + new: the rotation block of the next iteration reads its degree-2 entries;
+    // the commit forms the whole of it from the converged increment (the same sum)
+    if (i == D.i20 || i == D.i21) D.sp(S_DSCUR, b)[i] = make_double2(__dadd_rn(p.x, nr), __dadd_rn(p.y, ni));
+    acc = hypot(nr, ni);
   }
   const double part = block_sum(acc, sh);
   double sa;
@@ -1400,7 +1395,7 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_ro.data(), (int)s->f_ana_ro.size(), st, PROF_ANA_STEP));
   note_launch();
   t = prof_begin(PROF_UPDATE, act, st);
-  k_update<<<dim3(nb((nc + 1) / 2), B), 256, 0, st>>>(D);
+  k_update<<<dim3(nb(nc), B), 256, 0, st>>>(D);
   prof_end(t, st);
   if (!s->cfg.opt_dsl) {
     note_launch();
