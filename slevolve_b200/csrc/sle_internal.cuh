@@ -42,6 +42,18 @@ constexpr int MAX_CALL_FIELDS = 256;   // fields per transform call with the pac
 constexpr int MX_MAXF = 32;          // fields per mixed-precision transform launch
 constexpr int MX_NMAX = 2 * MX_MAXF; // B-operand rows (Re, Im per field)
 
+// Synthesis B operand entry of one packed coefficient for field slot f of a mixed-precision
+// launch: 1.41421356 U rounded to FP32 in rows 2f (Re) and 2f + 1 (Im) of its (segment, parity)
+// block, at K index k, in the tensor cores' 128-byte-swizzled tile order of 32 entries per row.
+// bpos = (block's first entry) * 32 + k, from the plan's mx_bpos table.
+__device__ __forceinline__ void mx_bsyn_put(float* bsyn, int bpos, int f, double2 u) {
+  float* blk = bsyn + (bpos >> 5);
+  const int k = bpos & 31, r0 = 2 * f, r1 = 2 * f + 1;
+  blk[r0 * 32 + ((((k >> 2) ^ (r0 & 7)) << 2) | (k & 3))] = (float)(u.x * SQRT2_LEGACY);
+  blk[r1 * 32 + ((((k >> 2) ^ (r1 & 7)) << 2) | (k & 3))] = (float)(u.y * SQRT2_LEGACY);
+}
+
+
 // Device view of a transform plan, passed to kernels by value.
 struct ShtDev {
   int nlat, nlon, lmax, nh, nm, n2, log2n2, ngrp, nseg;
@@ -183,6 +195,7 @@ struct sle_sht {
   float2* mx_twf;
   float2* mx_gns;
   float* mx_bsyn;
+  int* mx_bpos;                  // [ncoef] synthesis B position of each packed coefficient (mx_bsyn_put)
   double* mx_s0;
   int* mx_abort;
   int4 *mx_ana_units, *mx_syn_units;
@@ -219,14 +232,17 @@ void prof_end(const ProfToken& t, cudaStream_t st);
 // Transforms of a list of fields (packed spectra), launched in groups of MAXF (FP64) or
 // MX_MAXF (mixed) fields with the precision of the plan (sle_sht.cu).
 int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st, int prof_cls = PROF_LEG_ANA);
-int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st);
+// b_ready (mixed precision, n <= the plan's fields per launch): field f's B operand was written by
+// mx_bsyn_put with slot f, so the launch skips forming it
+int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st, bool b_ready = false);
 int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t st);
 // Mixed-precision transforms (sle_mx.cu).  `status` (device int, may be null) receives
 // SLE_ERR_TIMEOUT if a tensor-core kernel gave up waiting.
 int sht_mx_prepare(sle_sht* plan);
 int sht_mx_analysis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st,
                     int prof_cls = PROF_LEG_ANA);
-int sht_mx_synthesis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st);
+// b_ready: the synthesis B operand of the launch's fields is already in place (mx_bsyn_put)
+int sht_mx_synthesis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st, bool b_ready = false);
 int sht_mx_abort_flag(sle_sht* plan, int* flag);
 int sht_unpack(sle_sht* plan, const double2* packed, double2* dense, cudaStream_t st);
 }  // namespace sle

@@ -1152,6 +1152,21 @@ int sht_mx_prepare(sle_sht* p) {
     for (int sg : u.segs) segs.push_back(sg);
     ns += (long long)u.segs.size();
   }
+  {
+    // synthesis B position of every packed coefficient (mx_bsyn_put): segment seg of order m
+    // holds degrees l0 = m + 64 q .. l0 + 63; degree l sits at t = l - l0 in the block of parity
+    // t & 1, K index t / 2
+    std::vector<int> bpos((size_t)d.ncoef);
+    for (int m = 0; m <= L; ++m) {
+      const long long mo = (long long)m * (L + 1) - (long long)m * (m - 1) / 2;
+      for (int l = m; l <= L; ++l) {
+        const int seg = segoff[m] + (l - m) / SEG, t = (l - m) % SEG;
+        bpos[(size_t)(mo + l - m)] = ((seg * 2 + (t & 1)) * BBLOCK) * 32 + (t >> 1);
+      }
+    }
+    SLE_TRY(mx_alloc(&p->mx_bpos, bpos.size()));
+    SLE_CUDA(cudaMemcpy(p->mx_bpos, bpos.data(), bpos.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
   SLE_TRY(mx_alloc(&p->mx_ana_units, av.size()));
   SLE_TRY(mx_alloc(&p->mx_syn_units, sv.size()));
   SLE_TRY(mx_alloc(&p->mx_ana_cta, acta.size()));
@@ -1269,13 +1284,13 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t 
   return SLE_OK;
 }
 
-int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t st) {
+int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t st, bool b_ready) {
   SLE_TRY(sht_mx_prepare(p));
   SLE_TRY(mx_check_args(a, "mixed synthesis"));
   const ShtDev& d = p->d;
   const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[0]);
   ProfToken t0 = prof_begin(PROF_LEG_SYN, a.nf, st);
-  k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
+  if (!b_ready) k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
   if (p->tune_stages == 2)
     k_leg_tc<true, 2><<<p->n_syn_cta, TC_THREADS, mx_smem(2, true), st>>>(d, a, status, *map, 0);
   else

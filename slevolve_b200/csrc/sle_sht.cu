@@ -654,7 +654,7 @@ int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st,
   return SLE_OK;
 }
 
-int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st) {
+int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st, bool b_ready) {
   if (n < 1) return SLE_OK;
   const bool mx = plan->precision == SLE_PREC_MIXED;
   const int group = mx ? plan->tune_fpl : MAXF;
@@ -662,7 +662,7 @@ int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st
   for (int g = 0; g < ngroups; ++g) {
     const int lo = (int)((long long)n * g / ngroups), hi = (int)((long long)n * (g + 1) / ngroups);
     if (mx) {
-      SLE_TRY(sht_mx_synthesis(plan, mx_args(f + lo, hi - lo), plan->mx_status, st));
+      SLE_TRY(sht_mx_synthesis(plan, mx_args(f + lo, hi - lo), plan->mx_status, st, b_ready && ngroups == 1));
     } else {
       SLE_TRY(fp64_synthesis(plan, f + lo, hi - lo, st));
     }
@@ -704,7 +704,7 @@ static void plan_free(sle_sht* p) {
                   p->seg_m, p->seg_l0, p->ana_order, p->seeds, p->tw, p->X, p->EO, p->istart,
                   p->packbuf, p->mx_xf, p->mx_twf, p->mx_gns, p->mx_bsyn, p->mx_s0, p->mx_abort,
                   p->mx_ana_units, p->mx_syn_units, p->mx_syn_seg, p->mx_tab_ana, p->mx_tab_syn,
-                  p->mx_ana_cta, p->mx_syn_cta};
+                  p->mx_ana_cta, p->mx_syn_cta, p->mx_bpos};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;

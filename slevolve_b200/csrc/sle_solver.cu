@@ -582,8 +582,11 @@ __global__ void k_pre_spec(Dev D) {
   }
 }
 
-// Eq. B18 (solver.py:977-991) plus the degree-2 rotational term of the current iteration.
-__global__ void k_b18(Dev D) {
+// Eq. B18 (solver.py:977-991) plus the degree-2 rotational term of the current iteration.  With
+// bsyn (mixed precision, the iteration's synthesis one launch), the result goes straight into
+// that launch's B operand as field b instead of the FP64 spectrum, of which only (0, 0) is kept
+// (the degree-0 term the unfold adds in FP64).
+__global__ void k_b18(Dev D, float* bsyn, const int* bpos) {
   SLOT_OR_RETURN();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= D.ncoef) return;
@@ -613,7 +616,12 @@ __global__ void k_b18(Dev D) {
       im = __dadd_rn(im, sc->dsl_rot[2 * q + 1]);
     }
   }
-  D.sp(S_SL, b)[i] = make_double2(re, im);
+  if (bsyn) {
+    mx_bsyn_put(bsyn, __ldg(bpos + i), b, i == 0 ? make_double2(0.0, 0.0) : make_double2(re, im));
+    if (i == 0) D.sp(S_SL, b)[0] = make_double2(re, im);
+  } else {
+    D.sp(S_SL, b)[i] = make_double2(re, im);
+  }
 }
 
 // conserv, the load update and xi (solver.py:1002-1030):
@@ -1389,9 +1397,14 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   const double act = (double)s->iter_active;   // per-class timing units: slots still iterating
   note_launch();
   ProfToken t = prof_begin(PROF_B18, act, st);
-  k_b18<<<dim3(nb(nc), B), 256, 0, st>>>(D);
+  // mixed precision with the dsl identity (the spectrum has no other reader) and the synthesis
+  // one launch (field b = slot b): B18 writes the synthesis B operand itself
+  const int nsyn = (int)s->f_syn_sl.size();
+  const bool fuse = s->cfg.precision == SLE_PREC_MIXED && s->cfg.opt_dsl && s->plan->mx_ready &&
+                    nsyn <= std::min(MX_MAXF, s->plan->tune_fpl);
+  k_b18<<<dim3(nb(nc), B), 256, 0, st>>>(D, fuse ? s->plan->mx_bsyn : nullptr, fuse ? s->plan->mx_bpos : nullptr);
   prof_end(t, st);
-  SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sl.data(), (int)s->f_syn_sl.size(), st));
+  SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sl.data(), nsyn, st, fuse));
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_ro.data(), (int)s->f_ana_ro.size(), st, PROF_ANA_STEP));
   note_launch();
   t = prof_begin(PROF_UPDATE, act, st);
