@@ -235,11 +235,6 @@ int sht_analysis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st,
 // b_ready (mixed precision, n <= the plan's fields per launch): field f's B operand was written by
 // mx_bsyn_put with slot f, so the launch skips forming it
 int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st, bool b_ready = false);
-// Synthesis of fs[0..n) then analysis of fa[0..n), fa[i] reading the grid fs[i] produces; one
-// interleaved mixed-precision pass (sht_mx_syn_ana) when both lists are one launch, else the two
-// lists in turn.
-int sht_syn_ana_list(sle_sht* plan, const FieldSpec* fs, const FieldSpec* fa, int n, cudaStream_t st, bool b_ready,
-                     int prof_cls);
 int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t st);
 // Mixed-precision transforms (sle_mx.cu).  `status` (device int, may be null) receives
 // SLE_ERR_TIMEOUT if a tensor-core kernel gave up waiting.
@@ -248,11 +243,6 @@ int sht_mx_analysis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream
                     int prof_cls = PROF_LEG_ANA);
 // b_ready: the synthesis B operand of the launch's fields is already in place (mx_bsyn_put)
 int sht_mx_synthesis(sle_sht* plan, const MxFieldArgs& a, int* status, cudaStream_t st, bool b_ready = false);
-// Synthesis of the fields of `as`, then analysis of the fields of `aa`, field f of `aa` reading the
-// grid that field f of `as` produces (same field count): the unfolds and folds run in groups of
-// fields, so that each group's grids are read back from L2.
-int sht_mx_syn_ana(sle_sht* plan, const MxFieldArgs& as, const MxFieldArgs& aa, int* status, cudaStream_t st,
-                   bool b_ready, int prof_cls);
 int sht_mx_abort_flag(sle_sht* plan, int* flag);
 int sht_unpack(sle_sht* plan, const double2* packed, double2* dense, cudaStream_t st);
 }  // namespace sle

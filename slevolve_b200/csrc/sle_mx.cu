@@ -84,9 +84,6 @@ constexpr int MAX_CTA_UNITS = 16;            // work units per CTA staged in sha
 // 16-byte entries per lane), synthesis ~570 per half + ~13800 per unit (sums written one line
 // per lane)
 constexpr double ANA_UNIT_COST = 3.0;
-// fields per unfold / fold group of sht_mx_syn_ana: 16 grids of 4 MB at L = 511 (64 MB) stay in
-// the 126 MB L2 between the unfold that writes them and the fold that reads them
-constexpr int MX_L2_GROUP = 16;
 constexpr double SYN_UNIT_COST = 24.0;
 constexpr int NCOLS = MX_NMAX;                // accumulator columns of every launch (2 per field slot)
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
@@ -863,11 +860,11 @@ struct FoldRowsMx {
 };
 
 template <int N, int NR>
-__global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k_fold_mx(ShtDev P, MxFieldArgs a, int f0) {
+__global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k_fold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ float2 smf2[];
   float2* A = smf2;
   constexpr int NLAT = NR / 2;               // latitudes of the block
-  const int j0 = NLAT * blockIdx.x, f = f0 + (int)blockIdx.y;
+  const int j0 = NLAT * blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
   constexpr int NT = fft_nt(NR, N);
   constexpr int Q = N / FftRadix<N, 1>::R;   // first-pass items per row: one per thread
@@ -977,10 +974,10 @@ struct GridRowsOutMx {
 };
 
 template <int N>
-__global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArgs a, int f0) {
+__global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ float2 smf2[];
   float2* A = smf2;
-  const int j = blockIdx.x, f = f0 + (int)blockIdx.y;
+  const int j = blockIdx.x, f = blockIdx.y;
   if (field_off(a, f)) return;
   const int js = P.nlat - 1 - j;
   const float4* G = reinterpret_cast<const float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm;
@@ -1257,13 +1254,15 @@ static int mx_check_args(const MxFieldArgs& a, const char* what) {
   return SLE_OK;
 }
 
-// Row FFT + fold of the fields f0 .. f0 + nfl - 1 of an analysis launch.
-static void mx_fold(const sle_sht* p, const MxFieldArgs& a, int f0, int nfl, cudaStream_t st) {
+int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t st, int prof_cls) {
+  SLE_TRY(sht_mx_prepare(p));
+  SLE_TRY(mx_check_args(a, "mixed analysis"));
   const ShtDev& d = p->d;
+  ProfToken t0 = prof_begin(PROF_FFT, a.nf, st);
 #define SLE_LAUNCH_MXF4(NN) \
-  k_fold_mx<NN, 4><<<dim3(d.nh / 2, nfl), fft_threads(4, NN), mx_fold_smem(d, 4), st>>>(d, a, f0)
+  k_fold_mx<NN, 4><<<dim3(d.nh / 2, a.nf), fft_threads(4, NN), mx_fold_smem(d, 4), st>>>(d, a)
 #define SLE_LAUNCH_MXF8(NN) \
-  k_fold_mx<NN, 8><<<dim3(d.nh / 4, nfl), fft_threads(8, NN), mx_fold_smem(d, 8), st>>>(d, a, f0)
+  k_fold_mx<NN, 8><<<dim3(d.nh / 4, a.nf), fft_threads(8, NN), mx_fold_smem(d, 8), st>>>(d, a)
   if (p->tune_fold_rows == 4) {
     SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXF4)
   } else {
@@ -1271,43 +1270,14 @@ static void mx_fold(const sle_sht* p, const MxFieldArgs& a, int f0, int nfl, cud
   }
 #undef SLE_LAUNCH_MXF4
 #undef SLE_LAUNCH_MXF8
-}
-
-// Unfold + inverse row FFT of the fields f0 .. f0 + nfl - 1 of a synthesis launch.
-static void mx_unfold(const sle_sht* p, const MxFieldArgs& a, int f0, int nfl, cudaStream_t st) {
-  const ShtDev& d = p->d;
-#define SLE_LAUNCH_MXU(NN) \
-  k_unfold_mx<NN><<<dim3(d.nh, nfl), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a, f0)
-  SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXU)
-#undef SLE_LAUNCH_MXU
-}
-
-static void mx_contract(const sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t st, bool syn) {
-  const ShtDev& d = p->d;
-  if (syn) {
-    const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[0]);
-    if (p->tune_stages == 2)
-      k_leg_tc<true, 2><<<p->n_syn_cta, TC_THREADS, mx_smem(2, true), st>>>(d, a, status, *map, 0);
-    else
-      k_leg_tc<true, 4><<<p->n_syn_cta, TC_THREADS, mx_smem(4, true), st>>>(d, a, status, *map, 0);
-  } else {
-    const int zi = (a.nf <= ZBOX[0]) ? 0 : (a.nf <= ZBOX[1]) ? 1 : 2;
-    const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[zi]);
-    if (p->tune_stages == 2)
-      k_leg_tc<false, 2><<<p->n_ana_cta, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, ZBOX[zi]);
-    else
-      k_leg_tc<false, 4><<<p->n_ana_cta, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, ZBOX[zi]);
-  }
-}
-
-int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t st, int prof_cls) {
-  SLE_TRY(sht_mx_prepare(p));
-  SLE_TRY(mx_check_args(a, "mixed analysis"));
-  ProfToken t0 = prof_begin(PROF_FFT, a.nf, st);
-  mx_fold(p, a, 0, a.nf, st);
   prof_end(t0, st);
+  const int zi = (a.nf <= ZBOX[0]) ? 0 : (a.nf <= ZBOX[1]) ? 1 : 2;
+  const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[zi]);
   ProfToken t1 = prof_begin(prof_cls, a.nf, st);
-  mx_contract(p, a, status, st, false);
+  if (p->tune_stages == 2)
+    k_leg_tc<false, 2><<<p->n_ana_cta, TC_THREADS, mx_smem(2), st>>>(d, a, status, *map, ZBOX[zi]);
+  else
+    k_leg_tc<false, 4><<<p->n_ana_cta, TC_THREADS, mx_smem(4), st>>>(d, a, status, *map, ZBOX[zi]);
   prof_end(t1, st);
   note_launch(2);
   SLE_CUDA(cudaGetLastError());
@@ -1318,47 +1288,20 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t
   SLE_TRY(sht_mx_prepare(p));
   SLE_TRY(mx_check_args(a, "mixed synthesis"));
   const ShtDev& d = p->d;
+  const CUtensorMap* map = reinterpret_cast<const CUtensorMap*>(p->mx_tmap[0]);
   ProfToken t0 = prof_begin(PROF_LEG_SYN, a.nf, st);
   if (!b_ready) k_bsyn_mx<<<dim3(d.nseg, (a.nf + 3) / 4), 256, 0, st>>>(d, a);
-  mx_contract(p, a, status, st, true);
+  if (p->tune_stages == 2)
+    k_leg_tc<true, 2><<<p->n_syn_cta, TC_THREADS, mx_smem(2, true), st>>>(d, a, status, *map, 0);
+  else
+    k_leg_tc<true, 4><<<p->n_syn_cta, TC_THREADS, mx_smem(4, true), st>>>(d, a, status, *map, 0);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
-  mx_unfold(p, a, 0, a.nf, st);
+#define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a)
+  SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXU)
+#undef SLE_LAUNCH_MXU
   prof_end(t1, st);
-  note_launch(b_ready ? 2 : 3);
-  SLE_CUDA(cudaGetLastError());
-  return SLE_OK;
-}
-
-int sht_mx_syn_ana(sle_sht* p, const MxFieldArgs& as, const MxFieldArgs& aa, int* status, cudaStream_t st,
-                   bool b_ready, int prof_cls) {
-  SLE_TRY(sht_mx_prepare(p));
-  SLE_TRY(mx_check_args(as, "mixed synthesis"));
-  SLE_TRY(mx_check_args(aa, "mixed analysis"));
-  if (as.nf != aa.nf) {
-    set_error("mixed synthesis + analysis: %d synthesised against %d analysed fields", as.nf, aa.nf);
-    return SLE_ERR_BAD_ARG;
-  }
-  const ShtDev& d = p->d;
-  ProfToken t0 = prof_begin(PROF_LEG_SYN, as.nf, st);
-  if (!b_ready) k_bsyn_mx<<<dim3(d.nseg, (as.nf + 3) / 4), 256, 0, st>>>(d, as);
-  mx_contract(p, as, status, st, true);
-  prof_end(t0, st);
-  // groups of MX_L2_GROUP fields: each group's synthesised grids are read back by its folds
-  // while they are still in L2
-  for (int f0 = 0; f0 < as.nf; f0 += MX_L2_GROUP) {
-    const int nfl = std::min(MX_L2_GROUP, as.nf - f0);
-    ProfToken t1 = prof_begin(PROF_IFFT, nfl, st);
-    mx_unfold(p, as, f0, nfl, st);
-    prof_end(t1, st);
-    ProfToken t2 = prof_begin(PROF_FFT, nfl, st);
-    mx_fold(p, aa, f0, nfl, st);
-    prof_end(t2, st);
-  }
-  ProfToken t3 = prof_begin(prof_cls, aa.nf, st);
-  mx_contract(p, aa, status, st, false);
-  prof_end(t3, st);
-  note_launch((b_ready ? 2 : 3) + 2 * ((as.nf + MX_L2_GROUP - 1) / MX_L2_GROUP));
+  note_launch(3);
   SLE_CUDA(cudaGetLastError());
   return SLE_OK;
 }

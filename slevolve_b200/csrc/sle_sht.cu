@@ -670,15 +670,6 @@ int sht_synthesis_list(sle_sht* plan, const FieldSpec* f, int n, cudaStream_t st
   return SLE_OK;
 }
 
-int sht_syn_ana_list(sle_sht* plan, const FieldSpec* fs, const FieldSpec* fa, int n, cudaStream_t st, bool b_ready,
-                     int prof_cls) {
-  if (n < 1) return SLE_OK;
-  if (plan->precision == SLE_PREC_MIXED && n <= plan->tune_fpl && n <= MX_MAXF)
-    return sht_mx_syn_ana(plan, mx_args(fs, n), mx_args(fa, n), plan->mx_status, st, b_ready, prof_cls);
-  SLE_TRY(sht_synthesis_list(plan, fs, n, st, b_ready));
-  return sht_analysis_list(plan, fa, n, st, prof_cls);
-}
-
 int sht_pack(sle_sht* plan, const double2* dense, double2* packed, cudaStream_t st) {
   const long long n = (long long)plan->d.nm * plan->d.nm;
   k_pack<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(plan->d, dense, packed);

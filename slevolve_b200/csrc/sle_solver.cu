@@ -1404,8 +1404,8 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
                     nsyn <= std::min(MX_MAXF, s->plan->tune_fpl);
   k_b18<<<dim3(nb(nc), B), 256, 0, st>>>(D, fuse ? s->plan->mx_bsyn : nullptr, fuse ? s->plan->mx_bpos : nullptr);
   prof_end(t, st);
-  // synthesis of the sea level, then the analysis of rO = dsl C* (field b reads slot b's dsl)
-  SLE_TRY(sht_syn_ana_list(s->plan, s->f_syn_sl.data(), s->f_ana_ro.data(), nsyn, st, fuse, PROF_ANA_STEP));
+  SLE_TRY(sht_synthesis_list(s->plan, s->f_syn_sl.data(), nsyn, st, fuse));
+  SLE_TRY(sht_analysis_list(s->plan, s->f_ana_ro.data(), (int)s->f_ana_ro.size(), st, PROF_ANA_STEP));
   note_launch();
   t = prof_begin(PROF_UPDATE, act, st);
   k_update<<<dim3(nb(nc), B), 256, 0, st>>>(D);
