@@ -80,10 +80,10 @@ constexpr int NPAIR = 2;                      // accumulator pairs (chunk k into
 constexpr int BBLOCK = MX_NMAX * KC;          // floats of one synthesis B block
 constexpr int MAX_CTA_UNITS = 16;            // work units per CTA staged in shared memory
 // fixed cost of a work unit (its epilogue), in half-chunk times, from per-CTA timings at L = 511
-// with 32 fields: analysis ~1400 cycles per half + ~4500 per unit (coefficients written two
-// 16-byte entries per lane), synthesis ~570 per half + ~13800 per unit (sums written one line
-// per lane)
-constexpr double ANA_UNIT_COST = 3.0;
+// with 32 fields: analysis ~1180 cycles per half + ~5800 per unit, synthesis ~570 per half +
+// ~13800 per unit (measured before its epilogue wrote one 16-byte store per sum pair; its CTAs
+// stay within 3 % of each other)
+constexpr double ANA_UNIT_COST = 5.0;
 constexpr double SYN_UNIT_COST = 24.0;
 constexpr int NCOLS = MX_NMAX;                // accumulator columns of every launch (2 per field slot)
 static_assert(512 + 16 * MAX_CTA_UNITS <= MISC_BYTES, "misc shared memory too small");
