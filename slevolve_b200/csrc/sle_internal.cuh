@@ -206,7 +206,6 @@ struct sle_sht {
   double mx_table_bytes;
   int n_ana_units, n_syn_units;
   int n_ana_cta, n_syn_cta;       // CTAs of an analysis / synthesis launch
-  int fold_bpsm[2];              // resident blocks per SM of the fold kernel (4 / 8 rows per block)
   int n_sm;                      // SMs of the device (persistent transform grid)
   // launch shape of the mixed-precision transforms (sle_sht_set_tuning): fields per tensor-core
   // launch, pipeline stages of the tensor-core kernel, rows per row-FFT block of the fold

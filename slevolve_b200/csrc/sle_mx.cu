@@ -863,75 +863,70 @@ template <int N, int NR>
 __global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k_fold_mx(ShtDev P, MxFieldArgs a) {
   extern __shared__ float2 smf2[];
   float2* A = smf2;
-  constexpr int NLAT = NR / 2;               // latitudes of an item
+  constexpr int NLAT = NR / 2;               // latitudes of the block
+  const int j0 = NLAT * blockIdx.x, f = blockIdx.y;
+  if (field_off(a, f)) return;
   constexpr int NT = fft_nt(NR, N);
   constexpr int Q = N / FftRadix<N, 1>::R;   // first-pass items per row: one per thread
-  // persistent: item = (field f, latitude group) with the groups of a field consecutive
-  const int ngl = P.nh / NLAT, nitems = ngl * a.nf;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int f = item / ngl, j0 = NLAT * (item - f * ngl);
-    if (field_off(a, f)) continue;
-    double acc = 0.0;
-    with_src_kind(a.kind[f], FoldRowsMx<N, NR>{a.grid[f], a.m0[f], a.m1[f], j0, P.nlat, P.twf, A, &acc});
-    // FP64 row sums: the Q threads r Q .. r Q + Q - 1 hold the partial sums of row r (Q a power
-    // of two): a butterfly within aligned groups of min(Q, 32) lanes, then the warps of a row in
-    // order
-    __shared__ double rowtot[NR];
-    {
-      const int t = threadIdx.x;
-      double v = (t < NR * Q) ? acc : 0.0;
-      constexpr int W = Q < 32 ? Q : 32;
-  #pragma unroll
-      for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if constexpr (Q <= 32) {
-        if (t < NR * Q && t % Q == 0) rowtot[t / Q] = v;
-      } else {
-        __shared__ double wsum[NT / 32];
-        if ((t & 31) == 0) wsum[t >> 5] = v;
-        __syncthreads();
-        if (t < NR) {
-          double sum = 0.0;
-          for (int w = t * (Q / 32); w < (t + 1) * (Q / 32); ++w) sum += wsum[w];
-          rowtot[t] = sum;
-        }
-      }
+  double acc = 0.0;
+  with_src_kind(a.kind[f], FoldRowsMx<N, NR>{a.grid[f], a.m0[f], a.m1[f], j0, P.nlat, P.twf, A, &acc});
+  // FP64 row sums: the Q threads r Q .. r Q + Q - 1 hold the partial sums of row r (Q a power
+  // of two): a butterfly within aligned groups of min(Q, 32) lanes, then the warps of a row in
+  // order
+  __shared__ double rowtot[NR];
+  {
+    const int t = threadIdx.x;
+    double v = (t < NR * Q) ? acc : 0.0;
+    constexpr int W = Q < 32 ? Q : 32;
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if constexpr (Q <= 32) {
+      if (t < NR * Q && t % Q == 0) rowtot[t / Q] = v;
+    } else {
+      __shared__ double wsum[NT / 32];
+      if ((t & 31) == 0) wsum[t >> 5] = v;
       __syncthreads();
-    }
-    const SmemRows<N, float2> Z{A};
-    float2* X = reinterpret_cast<float2*>(P.mx_xf) + (size_t)f * P.nm * P.nh * 2;
-    for (int e = threadIdx.x; e < NLAT * P.nm; e += NT) {
-      // consecutive threads: the latitudes of one order (one 32-byte sector of each X plane)
-      const int m = e / NLAT, q = e % NLAT, j = j0 + q;
-      float2 xr[2];
-      const float2 twm = (m > 0 && m < N) ? __ldg(P.twf + m) : make_float2(1.f, 0.f);
-  #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = 2 * q + h;
-        const float2 z0 = Z(r, 0);
-        if (m == 0) {
-          xr[h] = make_float2(z0.x + z0.y, 0.f);
-        } else if (m == N) {
-          xr[h] = make_float2(z0.x - z0.y, 0.f);
-        } else {
-          const float2 zm = Z(r, m);
-          const float2 zn = Z(r, N - m);
-          const float2 zc = make_float2(zn.x, -zn.y);
-          const float2 ev = cscale(cadd(zm, zc), 0.5f);
-          const float2 dz = csub(zm, zc);
-          const float2 o = make_float2(0.5f * dz.y, -0.5f * dz.x);  // (zm - zc) / (2i)
-          xr[h] = cadd(ev, cmul(twm, o));
-        }
+      if (t < NR) {
+        double sum = 0.0;
+        for (int w = t * (Q / 32); w < (t + 1) * (Q / 32); ++w) sum += wsum[w];
+        rowtot[t] = sum;
       }
-      const double wn = P.wn[j], ws = P.ws[j];
-      const float2 an = cscale(xr[0], (float)wn), bs = cscale(xr[1], (float)ws);
+    }
+    __syncthreads();
+  }
+  const SmemRows<N, float2> Z{A};
+  float2* X = reinterpret_cast<float2*>(P.mx_xf) + (size_t)f * P.nm * P.nh * 2;
+  for (int e = threadIdx.x; e < NLAT * P.nm; e += NT) {
+    // consecutive threads: the latitudes of one order (one 32-byte sector of each X plane)
+    const int m = e / NLAT, q = e % NLAT, j = j0 + q;
+    float2 xr[2];
+    const float2 twm = (m > 0 && m < N) ? __ldg(P.twf + m) : make_float2(1.f, 0.f);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = 2 * q + h;
+      const float2 z0 = Z(r, 0);
       if (m == 0) {
-        // S_0(j) in FP64: the weighted sums of the north and south rows of latitude j
-        P.mx_s0[(size_t)f * P.nh + j] = wn * rowtot[2 * q] + ws * rowtot[2 * q + 1];
+        xr[h] = make_float2(z0.x + z0.y, 0.f);
+      } else if (m == N) {
+        xr[h] = make_float2(z0.x - z0.y, 0.f);
+      } else {
+        const float2 zm = Z(r, m);
+        const float2 zn = Z(r, N - m);
+        const float2 zc = make_float2(zn.x, -zn.y);
+        const float2 ev = cscale(cadd(zm, zc), 0.5f);
+        const float2 dz = csub(zm, zc);
+        const float2 o = make_float2(0.5f * dz.y, -0.5f * dz.x);  // (zm - zc) / (2i)
+        xr[h] = cadd(ev, cmul(twm, o));
       }
-      X[((size_t)m * 2 + 0) * P.nh + j] = make_float2(an.x + bs.x, an.y + bs.y);   // S (even l - m)
-      X[((size_t)m * 2 + 1) * P.nh + j] = make_float2(an.x - bs.x, an.y - bs.y);   // D (odd l - m)
     }
-  __syncthreads();   // the rows and row sums are reused by the block's next item
+    const double wn = P.wn[j], ws = P.ws[j];
+    const float2 an = cscale(xr[0], (float)wn), bs = cscale(xr[1], (float)ws);
+    if (m == 0) {
+      // S_0(j) in FP64: the weighted sums of the north and south rows of latitude j
+      P.mx_s0[(size_t)f * P.nh + j] = wn * rowtot[2 * q] + ws * rowtot[2 * q + 1];
+    }
+    X[((size_t)m * 2 + 0) * P.nh + j] = make_float2(an.x + bs.x, an.y + bs.y);   // S (even l - m)
+    X[((size_t)m * 2 + 1) * P.nh + j] = make_float2(an.x - bs.x, an.y - bs.y);   // D (odd l - m)
   }
 }
 
@@ -1242,10 +1237,6 @@ int sht_mx_prepare(sle_sht* p) {
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_fold_smem(d, 8)));    \
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
-    SLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p->fold_bpsm[0], k_fold_mx<NN, 4>,        \
-                                                           fft_threads(4, NN), mx_fold_smem(d, 4)));     \
-    SLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p->fold_bpsm[1], k_fold_mx<NN, 8>,        \
-                                                           fft_threads(8, NN), mx_fold_smem(d, 8)));     \
     SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_unfold_smem(d)));      \
     SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
   } while (0)
@@ -1268,12 +1259,10 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t 
   SLE_TRY(mx_check_args(a, "mixed analysis"));
   const ShtDev& d = p->d;
   ProfToken t0 = prof_begin(PROF_FFT, a.nf, st);
-  // persistent fold: as many blocks as fit on the device at once, at most one per item
-  const int nitems4 = (d.nh / 2) * a.nf, nitems8 = (d.nh / 4) * a.nf;
-  const int g4 = std::max(1, std::min(nitems4, std::max(1, p->fold_bpsm[0]) * p->n_sm));
-  const int g8 = std::max(1, std::min(nitems8, std::max(1, p->fold_bpsm[1]) * p->n_sm));
-#define SLE_LAUNCH_MXF4(NN) k_fold_mx<NN, 4><<<g4, fft_threads(4, NN), mx_fold_smem(d, 4), st>>>(d, a)
-#define SLE_LAUNCH_MXF8(NN) k_fold_mx<NN, 8><<<g8, fft_threads(8, NN), mx_fold_smem(d, 8), st>>>(d, a)
+#define SLE_LAUNCH_MXF4(NN) \
+  k_fold_mx<NN, 4><<<dim3(d.nh / 2, a.nf), fft_threads(4, NN), mx_fold_smem(d, 4), st>>>(d, a)
+#define SLE_LAUNCH_MXF8(NN) \
+  k_fold_mx<NN, 8><<<dim3(d.nh / 4, a.nf), fft_threads(8, NN), mx_fold_smem(d, 8), st>>>(d, a)
   if (p->tune_fold_rows == 4) {
     SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXF4)
   } else {
