@@ -207,6 +207,9 @@ struct sle_sht {
   int n_ana_units, n_syn_units;
   int n_ana_cta, n_syn_cta;       // CTAs of an analysis / synthesis launch
   int n_sm;                      // SMs of the device (persistent transform grid)
+  // blocks of the unfold resident on the device at once (occupancy x SMs): each block prefetches
+  // into L2 the input of the block that many places further on in launch order
+  int unfold_ahead;
   // launch shape of the mixed-precision transforms (sle_sht_set_tuning): fields per tensor-core
   // launch, pipeline stages of the tensor-core kernel, rows per row-FFT block of the fold
   int tune_fpl, tune_stages, tune_fold_rows;

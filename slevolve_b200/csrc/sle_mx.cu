@@ -140,6 +140,13 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
+// Prefetch of `bytes` of global memory into L2 (a hint; nothing waits for it).  The bulk prefetch
+// wants a 16-byte aligned start and a multiple of 16 bytes; anything else is left out.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  if (((reinterpret_cast<uintptr_t>(p) | bytes) & 15u) != 0 || bytes == 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -973,11 +980,33 @@ struct GridRowsOutMx {
   }
 };
 
+// The block `ahead` places on from this one in launch order (x fastest), whose inputs this one
+// prefetches into L2: false past the grid's end.
+__device__ __forceinline__ bool block_ahead(int ahead, int& bx, int& by) {
+  const long long lin = (long long)blockIdx.y * gridDim.x + blockIdx.x + ahead;
+  if (ahead <= 0 || lin >= (long long)gridDim.x * gridDim.y) return false;
+  by = (int)(lin / gridDim.x);
+  bx = (int)(lin - (long long)by * gridDim.x);
+  return true;
+}
+
+// `ahead`: the blocks resident on the device at once; the sums of the block that many places
+// further on (and the multiplier rows of its epilogue) are prefetched into L2.
 template <int N>
-__global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArgs a) {
+__global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArgs a, int ahead) {
   extern __shared__ float2 smf2[];
   float2* A = smf2;
   const int j = blockIdx.x, f = blockIdx.y;
+  int bx, by;
+  if (threadIdx.x < 3 && block_ahead(ahead, bx, by) && !field_off(a, by)) {
+    if (threadIdx.x == 0) {
+      prefetch_l2(reinterpret_cast<const float4*>(P.mx_gns) + ((size_t)by * P.nh + bx) * P.nm,
+                  (uint32_t)(P.nm * sizeof(float4)));
+    } else if (a.epi_out[by]) {
+      const int row = (threadIdx.x == 1) ? bx : P.nlat - 1 - bx;
+      prefetch_l2(a.epi_mul[by] + (size_t)row * (2 * N), (uint32_t)(2 * N * sizeof(double)));
+    }
+  }
   if (field_off(a, f)) return;
   const int js = P.nlat - 1 - j;
   const float4* G = reinterpret_cast<const float4*>(P.mx_gns) + ((size_t)f * P.nh + j) * P.nm;
@@ -1239,9 +1268,12 @@ int sht_mx_prepare(sle_sht* p) {
     SLE_CUDA(cudaFuncSetAttribute(k_fold_mx<NN, 8>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
     SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx_unfold_smem(d)));      \
     SLE_CUDA(cudaFuncSetAttribute(k_unfold_mx<NN>, cudaFuncAttributePreferredSharedMemoryCarveout, 100)); \
+    SLE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p->unfold_ahead, k_unfold_mx<NN>,                    \
+                                                           fft_threads(2, NN), mx_unfold_smem(d)));              \
   } while (0)
   SLE_FFT_SWITCH(d.n2, SLE_ATTR_MX)
 #undef SLE_ATTR_MX
+  p->unfold_ahead *= p->n_sm;
   p->mx_ready = 1;
   return SLE_OK;
 }
@@ -1297,7 +1329,7 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t
     k_leg_tc<true, 4><<<p->n_syn_cta, TC_THREADS, mx_smem(4, true), st>>>(d, a, status, *map, 0);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
-#define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a)
+#define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a, p->unfold_ahead)
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXU)
 #undef SLE_LAUNCH_MXU
   prof_end(t1, st);
