@@ -53,6 +53,23 @@ __device__ __forceinline__ void mx_bsyn_put(float* bsyn, int bpos, int f, double
   blk[r1 * 32 + ((((k >> 2) ^ (r1 & 7)) << 2) | (k & 3))] = (float)(u.y * SQRT2_LEGACY);
 }
 
+// Prefetch of `bytes` of global memory into L2 (a hint; nothing waits for it).  The bulk prefetch
+// wants a 16-byte aligned start and a multiple of 16 bytes; anything else is left out.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  if (((reinterpret_cast<uintptr_t>(p) | bytes) & 15u) != 0 || bytes == 0) return;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// The block `ahead` places on from this one in launch order (x fastest), whose inputs this one
+// prefetches into L2: false past the grid's end.
+__device__ __forceinline__ bool block_ahead(int ahead, int& bx, int& by) {
+  const long long lin = (long long)blockIdx.y * gridDim.x + blockIdx.x + ahead;
+  if (ahead <= 0 || lin >= (long long)gridDim.x * gridDim.y) return false;
+  by = (int)(lin / gridDim.x);
+  bx = (int)(lin - (long long)by * gridDim.x);
+  return true;
+}
+
 
 // Device view of a transform plan, passed to kernels by value.
 struct ShtDev {

@@ -140,13 +140,6 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
       : "memory");
 }
 
-// Prefetch of `bytes` of global memory into L2 (a hint; nothing waits for it).  The bulk prefetch
-// wants a 16-byte aligned start and a multiple of 16 bytes; anything else is left out.
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-  if (((reinterpret_cast<uintptr_t>(p) | bytes) & 15u) != 0 || bytes == 0) return;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -979,16 +972,6 @@ struct GridRowsOutMx {
     out.put(r, i, make_double2((double)v.x + c00, (double)v.y + c00));
   }
 };
-
-// The block `ahead` places on from this one in launch order (x fastest), whose inputs this one
-// prefetches into L2: false past the grid's end.
-__device__ __forceinline__ bool block_ahead(int ahead, int& bx, int& by) {
-  const long long lin = (long long)blockIdx.y * gridDim.x + blockIdx.x + ahead;
-  if (ahead <= 0 || lin >= (long long)gridDim.x * gridDim.y) return false;
-  by = (int)(lin / gridDim.x);
-  bx = (int)(lin - (long long)by * gridDim.x);
-  return true;
-}
 
 // `ahead`: the blocks resident on the device at once; the sums of the block that many places
 // further on (and the multiplier rows of its epilogue) are prefetched into L2.

@@ -121,6 +121,9 @@ struct Dev {
   const double* w;              // Gauss weights
   double rhoi, rhow, epsilon1;
   int checkmarine, tpw, calcRG, opt_dsl;
+  // blocks resident at once of the modal advance and of the load update (each block prefetches
+  // into L2 the inputs of the block that many places on)
+  int adv_ahead, upd_ahead;
   long long i20, i21, i22;      // packed indices of (l=2, m=0..2)
   int slot0;                    // slot of blockIdx.y == 0
   __host__ __device__ double* g(int id, int b) const { return grid + ((size_t)id * nslot + b) * ng; }
@@ -345,8 +348,19 @@ __device__ void rot_advance_block(const Dev& D, int b, Scal* sc) {
 }
 
 // R_k <- d R_k + (1-d) P ; visc = sum_k a_sl R_k ; rad = sum_k a_rr R_k   (solver.py:386-407)
-// The first block of each slot advances the degree-2 rotational state instead.
+// The first block of each slot advances the degree-2 rotational state instead.  Each block first
+// prefetches into L2 the state rows and the load of the block one resident wave further on in
+// launch order, so that the DRAM keeps reading while the blocks before it compute and store.
 __global__ void __launch_bounds__(256) k_advance(Dev D) {
+  int bx, by;
+  if (threadIdx.x <= D.K && block_ahead(D.adv_ahead, bx, by) && bx > 0 && !D.sc[D.slot0 + by].done) {
+    const int b2 = D.slot0 + by;
+    const long long i0 = (long long)(bx - 1) * blockDim.x;
+    const uint32_t bytes = (uint32_t)min((long long)blockDim.x, D.ncoef - i0) * (uint32_t)sizeof(double2);
+    prefetch_l2((int)threadIdx.x < D.K ? D.R + ((size_t)b2 * D.K + threadIdx.x) * D.ncoef + i0
+                                       : D.sp(S_P_LOAD, b2) + i0,
+                bytes);
+  }
   SLOT_OR_RETURN();
   if (blockIdx.x == 0) {   // scheduled first: its serial work overlaps the grid
     rot_advance_block(D, b, sc);
@@ -626,8 +640,19 @@ __global__ void k_b18(Dev D, float* bsyn, const int* bpos) {
 
 // conserv, the load update and xi (solver.py:1002-1030):
 //   new = ((-dSprev + rO) + C*_lm conserv) - tO ;  dS_cur = dSprev + new ;  sa = sum|new|
-// The slot's last block decides its convergence.
+// The slot's last block decides its convergence.  Each block first prefetches into L2 the four
+// input spectra of the block one resident wave further on in launch order.
 __global__ void k_update(Dev D) {
+  {
+    int bx, by;
+    if (threadIdx.x < 4 && block_ahead(D.upd_ahead, bx, by) && !D.sc[D.slot0 + by].done) {
+      const int b2 = D.slot0 + by;
+      const long long i0 = (long long)bx * blockDim.x;
+      const int id = threadIdx.x == 0 ? S_P_OCEAN : threadIdx.x == 1 ? S_ROLM : threadIdx.x == 2 ? S_CSTARLM : S_TOLM;
+      prefetch_l2(D.sp(id, b2) + i0,
+                  (uint32_t)min((long long)blockDim.x, D.ncoef - i0) * (uint32_t)sizeof(double2));
+    }
+  }
   SLOT_OR_RETURN();
   __shared__ double sh[32];
   const double2* dSprev = D.sp(S_P_OCEAN, b);
@@ -1737,6 +1762,15 @@ int batch_create(const sle_config* cfg, int nslot, int kmax, sle_batch** out) {
   D.mask = s->mask;
   D.spec = s->spec;
   D.R = s->R;
+  {
+    int dev = 0, nsm = 0, per_sm = 0;
+    TRYC(cudaGetDevice(&dev));
+    TRYC(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    TRYC(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance, 256, 0));
+    D.adv_ahead = per_sm * nsm;
+    TRYC(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update, 256, 0));
+    D.upd_ahead = per_sm * nsm;
+  }
   D.nmod = s->nmod;
   D.s_kl = s->s_kl;
   D.decay = s->decay;
