@@ -70,6 +70,35 @@ __device__ __forceinline__ bool block_ahead(int ahead, int& bx, int& by) {
   return true;
 }
 
+// Programmatic dependent launch.  A kernel launched by launch_pdl may be scheduled while the
+// kernel before it in the stream is finishing; it calls pdl_wait() before its first access to
+// global memory, which returns once that kernel has completed and its writes are visible (at once
+// for a plain launch).  Every kernel launched this way waits unconditionally, so the ordering
+// stays transitive along the stream.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the next kernel of the stream, if launched by launch_pdl, be scheduled once every block of
+// this one has passed here (its blocks then wait in pdl_wait for this kernel to complete).
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Programmatic launches are on unless SLEVOLVE_B200_NO_PDL is set (to a non-empty value other
+// than "0") when the library first launches one.
+bool pdl_enabled();
+
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+  cudaLaunchConfig_t c = {};
+  c.gridDim = grid;
+  c.blockDim = block;
+  c.dynamicSmemBytes = smem;
+  c.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  c.attrs = at;
+  c.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&c, k, static_cast<A&&>(args)...);
+}
+
 
 // Device view of a transform plan, passed to kernels by value.
 struct ShtDev {

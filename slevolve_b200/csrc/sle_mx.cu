@@ -589,6 +589,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     k_leg_tc(ShtDev P, MxFieldArgs a, int* status, const __grid_constant__ CUtensorMap tmx, int zbox) {
   static_assert(NST % 2 == 0 && NST <= NSTAGE_MAX, "stage count");
   extern __shared__ uint8_t smraw[];
+  pdl_trigger();   // one CTA per SM, all resident: the next kernel may queue behind them
   const Smem S = smem_layout(smraw, NST);
   const Misc M = misc_layout(S);
   const Abort ab{P.mx_abort, status};
@@ -865,6 +866,8 @@ __global__ void __launch_bounds__(fft_nt(NR, N), fft_nt(NR, N) <= 512 ? 3 : 1) k
   float2* A = smf2;
   constexpr int NLAT = NR / 2;               // latitudes of the block
   const int j0 = NLAT * blockIdx.x, f = blockIdx.y;
+  pdl_wait();
+  pdl_trigger();
   if (field_off(a, f)) return;
   constexpr int NT = fft_nt(NR, N);
   constexpr int Q = N / FftRadix<N, 1>::R;   // first-pass items per row: one per thread
@@ -980,6 +983,8 @@ __global__ void __launch_bounds__(fft_nt(2, N)) k_unfold_mx(ShtDev P, MxFieldArg
   extern __shared__ float2 smf2[];
   float2* A = smf2;
   const int j = blockIdx.x, f = blockIdx.y;
+  pdl_wait();
+  pdl_trigger();
   int bx, by;
   if (threadIdx.x < 3 && block_ahead(ahead, bx, by) && !field_off(a, by)) {
     if (threadIdx.x == 0) {
@@ -1275,9 +1280,9 @@ int sht_mx_analysis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t 
   const ShtDev& d = p->d;
   ProfToken t0 = prof_begin(PROF_FFT, a.nf, st);
 #define SLE_LAUNCH_MXF4(NN) \
-  k_fold_mx<NN, 4><<<dim3(d.nh / 2, a.nf), fft_threads(4, NN), mx_fold_smem(d, 4), st>>>(d, a)
+  SLE_CUDA(launch_pdl(k_fold_mx<NN, 4>, dim3(d.nh / 2, a.nf), dim3(fft_threads(4, NN)), mx_fold_smem(d, 4), st, d, a))
 #define SLE_LAUNCH_MXF8(NN) \
-  k_fold_mx<NN, 8><<<dim3(d.nh / 4, a.nf), fft_threads(8, NN), mx_fold_smem(d, 8), st>>>(d, a)
+  SLE_CUDA(launch_pdl(k_fold_mx<NN, 8>, dim3(d.nh / 4, a.nf), dim3(fft_threads(8, NN)), mx_fold_smem(d, 8), st, d, a))
   if (p->tune_fold_rows == 4) {
     SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXF4)
   } else {
@@ -1312,7 +1317,8 @@ int sht_mx_synthesis(sle_sht* p, const MxFieldArgs& a, int* status, cudaStream_t
     k_leg_tc<true, 4><<<p->n_syn_cta, TC_THREADS, mx_smem(4, true), st>>>(d, a, status, *map, 0);
   prof_end(t0, st);
   ProfToken t1 = prof_begin(PROF_IFFT, a.nf, st);
-#define SLE_LAUNCH_MXU(NN) k_unfold_mx<NN><<<dim3(d.nh, a.nf), fft_threads(2, NN), mx_unfold_smem(d), st>>>(d, a, p->unfold_ahead)
+#define SLE_LAUNCH_MXU(NN) \
+  SLE_CUDA(launch_pdl(k_unfold_mx<NN>, dim3(d.nh, a.nf), dim3(fft_threads(2, NN)), mx_unfold_smem(d), st, d, a, p->unfold_ahead))
   SLE_FFT_SWITCH(d.n2, SLE_LAUNCH_MXU)
 #undef SLE_LAUNCH_MXU
   prof_end(t1, st);

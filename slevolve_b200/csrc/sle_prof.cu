@@ -7,6 +7,9 @@
 // the run that uses them.
 #include "sle_internal.cuh"
 
+#include <cstdlib>
+#include <cstring>
+
 #include <mutex>
 #include <vector>
 
@@ -43,6 +46,14 @@ cudaEvent_t take_event() {
 }  // namespace
 
 bool prof_enabled() { return g_prof.enabled; }
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("SLEVOLVE_B200_NO_PDL");
+    return !(e && e[0] != '\0' && std::strcmp(e, "0") != 0);
+  }();
+  return on;
+}
 
 void note_launch(int n) {
   __atomic_fetch_add(&g_launches, (unsigned long long)(long long)n, __ATOMIC_RELAXED);

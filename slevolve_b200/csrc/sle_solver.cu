@@ -643,6 +643,8 @@ __global__ void k_b18(Dev D, float* bsyn, const int* bpos) {
 // The slot's last block decides its convergence.  Each block first prefetches into L2 the four
 // input spectra of the block one resident wave further on in launch order.
 __global__ void k_update(Dev D) {
+  pdl_wait();
+  pdl_trigger();
   {
     int bx, by;
     if (threadIdx.x < 4 && block_ahead(D.upd_ahead, bx, by) && !D.sc[D.slot0 + by].done) {
@@ -723,6 +725,8 @@ __global__ void k_sltot(Dev D) {
 // deltasl (dsl identity) and, when not converged, the ocean function of the refreshed
 // topography and the grounded-ice test on it (solver.py:1032-1037, 661-684).
 __global__ void k_refresh1(Dev D) {
+  pdl_wait();
+  pdl_trigger();
   SLOT_OR_RETURN();
   __shared__ double sh[32];
   const bool conv = sc->converged != 0;
@@ -781,6 +785,8 @@ __global__ void k_refresh1(Dev D) {
 // C* on the refreshed ocean function; accepted grounded-ice mask (solver.py:664-684).  tO =
 // T0 (C* - C*0) is formed by its analysis.
 __global__ void k_refresh2(Dev D) {
+  pdl_wait();
+  pdl_trigger();
   SLOT_OR_RETURN();
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (2 * h >= D.ng || sc->converged) return;
@@ -816,6 +822,8 @@ __device__ __forceinline__ unsigned char byte_of(uint2 v, int i) {
   return (unsigned char)(((i < 4 ? v.x : v.y) >> (8 * (i & 3))) & 0xffu);
 }
 __global__ void k_refresh2_x8(Dev D) {
+  pdl_wait();
+  pdl_trigger();
   SLOT_OR_RETURN();
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (8 * q >= D.ng || sc->converged) return;
@@ -863,6 +871,7 @@ __global__ void k_refresh2_x8(Dev D) {
 // not change costs DICE_BLOCKS early exits instead of one per 256 coefficients.
 constexpr int DICE_BLOCKS = 64;
 __global__ void __launch_bounds__(256) k_dice(Dev D) {
+  pdl_wait();
   SLOT_OR_RETURN();
   if (sc->converged || !sc->gr_changed) return;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -1433,7 +1442,7 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_ro.data(), (int)s->f_ana_ro.size(), st, PROF_ANA_STEP));
   note_launch();
   t = prof_begin(PROF_UPDATE, act, st);
-  k_update<<<dim3(nb(nc), B), 256, 0, st>>>(D);
+  SLE_CUDA(launch_pdl(k_update, dim3(nb(nc), B), dim3(256), 0, st, D));
   prof_end(t, st);
   if (!s->cfg.opt_dsl) {
     note_launch();
@@ -1442,11 +1451,11 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   }
   note_launch(2);
   t = prof_begin(PROF_REFRESH1, act, st);
-  k_refresh1<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
+  SLE_CUDA(launch_pdl(k_refresh1, dim3(nb(ng / 2), B), dim3(256), 0, st, D));
   prof_end(t, st);
   t = prof_begin(PROF_REFRESH2, act, st);
-  if (ng % 8 == 0) k_refresh2_x8<<<dim3(nb(ng / 8), B), 256, 0, st>>>(D);
-  else k_refresh2<<<dim3(nb(ng / 2), B), 256, 0, st>>>(D);
+  if (ng % 8 == 0) SLE_CUDA(launch_pdl(k_refresh2_x8, dim3(nb(ng / 8), B), dim3(256), 0, st, D));
+  else SLE_CUDA(launch_pdl(k_refresh2, dim3(nb(ng / 2), B), dim3(256), 0, st, D));
   prof_end(t, st);
   // C* and tO (when a cell of C* flipped), I* (when the grounded mask changed) for the next
   // iteration; skipped for slots that converged
@@ -1454,7 +1463,7 @@ int enqueue_iteration(sle_batch* s, cudaGraphConditionalHandle loop) {
   SLE_TRY(sht_analysis_list(s->plan, s->f_ana_regr.data(), (int)s->f_ana_regr.size(), st));
   note_launch(2);
   t = prof_begin(PROF_DICE, act, st);
-  k_dice<<<dim3(std::min(nb(nc), (unsigned)DICE_BLOCKS), B), 256, 0, st>>>(D);
+  SLE_CUDA(launch_pdl(k_dice, dim3(std::min(nb(nc), (unsigned)DICE_BLOCKS), B), dim3(256), 0, st, D));
   prof_end(t, st);
   k_loop_cond<<<1, 128, 0, st>>>(D, s->bstatus, loop);
   SLE_CUDA(cudaGetLastError());
