@@ -319,6 +319,14 @@ int sle_prof_reset(void);          /* also resets the launch counter */
 int sle_prof_read(int cls, double* ms, long long* count, double* units);
 /* kernels launched by this library since the last sle_prof_reset() */
 long long sle_launch_count(void);
+/* Launch mode of the inner loop's elementwise kernels, the row-FFT fold and the unfold: 1 launches
+ * each as a programmatic dependent of the kernel before it in its stream (scheduled while that
+ * kernel drains; it waits for that kernel's completion before touching memory, so results do not
+ * change), 0 as plain launches.  The initial mode is 1 unless the environment variable
+ * SLEVOLVE_B200_NO_PDL is set to a non-empty value other than "0".  Applies to work enqueued or
+ * captured afterwards: a batch keeps the mode its loop graph was captured with.  Returns the
+ * previous mode. */
+int sle_set_programmatic_launch(int on);
 /* FP64 FMA throughput of the current device (TFLOP/s), from a timed dependent-free FMA kernel */
 int sle_probe_fp64_tflops(double* tflops);
 

@@ -128,6 +128,7 @@ _SIGS = {
     "sle_prof_reset": (C.c_int, []),
     "sle_prof_read": (C.c_int, [C.c_int, _DP, C.POINTER(C.c_longlong), _DP]),
     "sle_launch_count": (C.c_longlong, []),
+    "sle_set_programmatic_launch": (C.c_int, [C.c_int]),
     "sle_probe_fp64_tflops": (C.c_int, [_DP]),
 }
 

@@ -81,7 +81,7 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // Programmatic launches are on unless SLEVOLVE_B200_NO_PDL is set (to a non-empty value other
-// than "0") when the library first launches one.
+// than "0") when the library first launches one, or sle_set_programmatic_launch turned them off.
 bool pdl_enabled();
 
 template <typename... P, typename... A>

@@ -7,6 +7,7 @@
 // the run that uses them.
 #include "sle_internal.cuh"
 
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 
@@ -47,12 +48,18 @@ cudaEvent_t take_event() {
 
 bool prof_enabled() { return g_prof.enabled; }
 
+// programmatic launch mode: -1 until first read (then from SLEVOLVE_B200_NO_PDL), 0 or 1
+static std::atomic<int> g_pdl{-1};
+
 bool pdl_enabled() {
-  static const bool on = [] {
+  int v = g_pdl.load(std::memory_order_relaxed);
+  if (v < 0) {
     const char* e = std::getenv("SLEVOLVE_B200_NO_PDL");
-    return !(e && e[0] != '\0' && std::strcmp(e, "0") != 0);
-  }();
-  return on;
+    int unset = -1;
+    g_pdl.compare_exchange_strong(unset, (e && e[0] != '\0' && std::strcmp(e, "0") != 0) ? 0 : 1);
+    v = g_pdl.load();
+  }
+  return v != 0;
 }
 
 void note_launch(int n) {
@@ -97,6 +104,12 @@ __global__ void k_fp64_probe(int iters, double seed, double* out) {
 }  // namespace sle
 
 using namespace sle;
+
+extern "C" int sle_set_programmatic_launch(int on) {
+  const int prev = pdl_enabled() ? 1 : 0;
+  g_pdl.store(on ? 1 : 0);
+  return prev;
+}
 
 extern "C" int sle_prof_enable(int on) {
   std::lock_guard<std::mutex> lk(g_prof.mu);

@@ -31,6 +31,31 @@ def test_library_exports_every_declared_symbol():
     assert set(_lib.exported_symbols()) <= set(declared_symbols())
 
 
+def test_programmatic_launch_switch():
+    """sle_set_programmatic_launch returns the previous mode; the initial mode follows
+    SLEVOLVE_B200_NO_PDL (host state only, no device call)."""
+    import sys
+
+    from slevolve_b200 import _lib
+
+    lib = _lib.lib()
+    prev = lib.sle_set_programmatic_launch(0)
+    try:
+        assert prev in (0, 1)
+        assert lib.sle_set_programmatic_launch(1) == 0
+        assert lib.sle_set_programmatic_launch(1) == 1
+    finally:
+        lib.sle_set_programmatic_launch(prev)
+    code = "from slevolve_b200 import _lib; print(_lib.lib().sle_set_programmatic_launch(1))"
+    for value, mode in (("1", 0), ("yes", 0), ("0", 1), ("", 1), (None, 1)):
+        env = {k: v for k, v in os.environ.items() if k != "SLEVOLVE_B200_NO_PDL"}
+        if value is not None:
+            env["SLEVOLVE_B200_NO_PDL"] = value
+        out = subprocess.run([sys.executable, "-c", code], cwd=REPO, env=env, capture_output=True,
+                             text=True, check=True, timeout=300).stdout
+        assert int(out.strip().splitlines()[-1]) == mode, (value, out)
+
+
 def test_error_mapping():
     from slevolve_b200 import _lib
 

@@ -72,6 +72,36 @@ def test_fp64_batch_slots_match_single_solves():
             _same(_snap(bt, s, infos[s]), alone[i][k - 1], (i, k))
 
 
+def test_programmatic_launches_do_not_change_results():
+    """A mixed batch of four uneven members stepped with the inner loop's kernels launched as
+    programmatic dependents and as plain launches (each mode in its own batch, whose loop graph is
+    captured with it): bit-identical results."""
+    from slevolve_b200 import _lib
+
+    lib = _lib.lib()
+    ms = _members()
+    nsteps = 4
+    runs = []
+    prev = lib.sle_set_programmatic_launch(1)
+    try:
+        for mode in (1, 0):
+            lib.sle_set_programmatic_launch(mode)
+            bt = _batch("mixed", len(ms))
+            for s, m in enumerate(ms):
+                bt.load(s, m["love"], m["topo"], m["ice"](0), m["dt"])
+            res = []
+            for k in range(1, nsteps + 1):
+                infos = bt.step({s: m["ice"](k) for s, m in enumerate(ms)})
+                res.append([_snap(bt, s, infos[s]) for s in range(len(ms))])
+            runs.append(res)
+            del bt
+    finally:
+        lib.sle_set_programmatic_launch(prev)
+    for k in range(nsteps):
+        for s in range(len(ms)):
+            _same(runs[0][k][s], runs[1][k][s], (k + 1, s))
+
+
 def test_continuous_batching_join_leave():
     """Slots join and leave between steps; each member still gets its solo result."""
     ms = _members()
