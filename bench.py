@@ -274,8 +274,16 @@ def step_shares(prof, nprof, peaks, nlat=512, lmax=511, modes=8):
     * modal advance: (2K + 3) 16 ncoef bytes per member over its time, against the copy bandwidth;
     * elementwise: each inner-loop pass with its algorithmic bytes per iterating slot
       (ELEMENTWISE) over its time, against the copy bandwidth;
-    * combined: the fractions weighted by their times."""
+    * combined: the fractions weighted by their times.
+
+    `transforms["classes"]` gives each transform kernel class its own figure: the Legendre
+    contractions 12 nh ncoef FLOPs per field against the dense tensor rate, the fold and the unfold
+    8 ng + 16 nm nh bytes per field (the FP64 grid one way, the FP32 S / D planes or E / O sums,
+    16 bytes per latitude and order, the other) against the copy bandwidth.  The classes count
+    every field of a launch; for the fold and the gated analyses that includes fields gated off
+    (and mask sources, one byte per cell), so their figures are upper bounds."""
     nh, nlon = nlat // 2, 2 * nlat
+    nm = lmax + 1
     ncoef = (lmax + 1) * (lmax + 2) // 2
     ng = nlat * nlon
     tpk = peaks["bf16_tflops"] * TENSOR_RATE
@@ -298,6 +306,25 @@ def step_shares(prof, nprof, peaks, nlat=512, lmax=511, modes=8):
                           "ms_per_step": 1000.0 * t_m / nprof, "achieved": m_ach, "unit": "GB/s",
                           "peak": peaks["hbm_gbs"], "frac": m_frac},
     }
+    classes = {}
+    for name in tr_names:
+        c = prof[name]
+        t = c["ms"] / 1000.0
+        if t <= 0:
+            continue
+        if name in ("k_fold_mx", "k_unfold_mx"):
+            per = 8.0 * ng + 16.0 * nm * nh
+            ach = per * c["fields"] / t / 1e9
+            classes[name] = {"bound": "hbm", "bytes_per_field": per, "achieved": ach, "unit": "GB/s",
+                             "peak": peaks["hbm_gbs"], "frac": ach / peaks["hbm_gbs"]}
+        else:
+            per = 12.0 * nh * ncoef
+            ach = per * c["fields"] / t / 1e12
+            classes[name] = {"bound": "tensor", "flops_per_field": per, "achieved": ach, "unit": "TFLOP/s",
+                             "peak": tpk, "frac": ach / tpk}
+        classes[name]["ms_per_step"] = 1000.0 * t / nprof
+        classes[name]["fields_per_step"] = c["fields"] / nprof
+    out["transforms"]["classes"] = classes
     weighted, tot = tr_frac * t_tr + m_frac * t_m, t_tr + t_m
     elem = {}
     for name, (kind, per) in ELEMENTWISE.items():

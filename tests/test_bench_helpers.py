@@ -48,6 +48,19 @@ def test_step_shares_arithmetic():
     lo, hi = min(fr), max(fr)
     assert lo <= sh["combined_frac"] <= hi
     assert sh["transforms"]["ms_per_step"] == pytest.approx(5.21, rel=1e-12)
+    # per transform class: the contractions in TFLOP/s, the row FFTs in GB/s
+    cl = sh["transforms"]["classes"]
+    assert set(cl) == {"k_fold_mx", "k_leg_tc<analysis of rO>", "k_leg_tc<other analyses>",
+                       "k_bsyn_mx + k_leg_tc<synthesis>", "k_unfold_mx"}
+    ro = cl["k_leg_tc<analysis of rO>"]
+    assert ro["achieved"] == pytest.approx(12.0 * nh * ncoef * 234.7 / 0.69e-3 / 1e12, rel=1e-12)
+    assert ro["frac"] == pytest.approx(ro["achieved"] / (1590.0 * b.TENSOR_RATE), rel=1e-12)
+    fold = cl["k_fold_mx"]
+    assert fold["bytes_per_field"] == 8.0 * 512 * 1024 + 16.0 * 512 * 256
+    assert fold["achieved"] == pytest.approx(fold["bytes_per_field"] * 1034.7 / 1.39e-3 / 1e9, rel=1e-12)
+    assert fold["frac"] == pytest.approx(fold["achieved"] / 6650.0, rel=1e-12)
+    assert cl["k_unfold_mx"]["unit"] == "GB/s" and cl["k_bsyn_mx + k_leg_tc<synthesis>"]["unit"] == "TFLOP/s"
+    assert cl["k_unfold_mx"]["ms_per_step"] == pytest.approx(0.51, rel=1e-12)
 
 
 def test_step_shares_empty_profile():
@@ -55,6 +68,7 @@ def test_step_shares_empty_profile():
     prof = {k: {"ms": 0.0, "launches": 0, "fields": 0.0} for k in _prof()}
     sh = b.step_shares(prof, 1, {"hbm_gbs": 1.0, "bf16_tflops": 2.0})
     assert sh["combined_frac"] == 0.0 and not math.isnan(sh["transforms"]["frac"])
+    assert sh["transforms"]["classes"] == {}
 
 
 def test_serving_occupancy_record():
