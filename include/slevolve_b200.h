@@ -324,9 +324,9 @@ long long sle_launch_count(void);
  * kernel drains; it waits for that kernel's completion before touching memory, so results do not
  * change), 0 as plain launches.  The initial mode is 1 unless the environment variable
  * SLEVOLVE_B200_NO_PDL is set to a non-empty value other than "0".  Applies to work enqueued or
- * captured afterwards: a batch keeps the mode its loop graph was captured with.  Returns the
- * previous mode. */
-int sle_set_programmatic_launch(int on);
+ * captured afterwards: a batch keeps the mode its loop graph was captured with.  *previous (may
+ * be NULL) receives the mode before the call.  No counterpart in the reference. */
+int sle_set_programmatic_launch(int on, int* previous);
 /* FP64 FMA throughput of the current device (TFLOP/s), from a timed dependent-free FMA kernel */
 int sle_probe_fp64_tflops(double* tflops);
 

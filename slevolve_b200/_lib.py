@@ -128,7 +128,7 @@ _SIGS = {
     "sle_prof_reset": (C.c_int, []),
     "sle_prof_read": (C.c_int, [C.c_int, _DP, C.POINTER(C.c_longlong), _DP]),
     "sle_launch_count": (C.c_longlong, []),
-    "sle_set_programmatic_launch": (C.c_int, [C.c_int]),
+    "sle_set_programmatic_launch": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     "sle_probe_fp64_tflops": (C.c_int, [_DP]),
 }
 
@@ -166,6 +166,14 @@ def lib():
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def set_programmatic_launch(on: bool) -> bool:
+    """Programmatic dependent launches of the inner loop on / off (sle_set_programmatic_launch)
+    for batches and transforms created afterwards; returns the previous setting."""
+    prev = C.c_int(0)
+    check(lib().sle_set_programmatic_launch(1 if on else 0, C.byref(prev)), "sle_set_programmatic_launch")
+    return bool(prev.value)
 
 
 def check(rc: int, what: str = ""):

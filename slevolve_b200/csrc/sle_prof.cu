@@ -105,10 +105,11 @@ __global__ void k_fp64_probe(int iters, double seed, double* out) {
 
 using namespace sle;
 
-extern "C" int sle_set_programmatic_launch(int on) {
+extern "C" int sle_set_programmatic_launch(int on, int* previous) {
   const int prev = pdl_enabled() ? 1 : 0;
   g_pdl.store(on ? 1 : 0);
-  return prev;
+  if (previous) *previous = prev;
+  return SLE_OK;
 }
 
 extern "C" int sle_prof_enable(int on) {

@@ -32,21 +32,21 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_programmatic_launch_switch():
-    """sle_set_programmatic_launch returns the previous mode; the initial mode follows
+    """sle_set_programmatic_launch reports the previous mode; the initial mode follows
     SLEVOLVE_B200_NO_PDL (host state only, no device call)."""
     import sys
 
     from slevolve_b200 import _lib
 
-    lib = _lib.lib()
-    prev = lib.sle_set_programmatic_launch(0)
+    prev = _lib.set_programmatic_launch(False)
     try:
-        assert prev in (0, 1)
-        assert lib.sle_set_programmatic_launch(1) == 0
-        assert lib.sle_set_programmatic_launch(1) == 1
+        assert _lib.set_programmatic_launch(True) is False
+        assert _lib.set_programmatic_launch(True) is True
+        assert _lib.lib().sle_set_programmatic_launch(0, None) == 0   # status; previous may be NULL
+        assert _lib.set_programmatic_launch(True) is False
     finally:
-        lib.sle_set_programmatic_launch(prev)
-    code = "from slevolve_b200 import _lib; print(_lib.lib().sle_set_programmatic_launch(1))"
+        _lib.set_programmatic_launch(prev)
+    code = "from slevolve_b200 import _lib; print(int(_lib.set_programmatic_launch(True)))"
     for value, mode in (("1", 0), ("yes", 0), ("0", 1), ("", 1), (None, 1)):
         env = {k: v for k, v in os.environ.items() if k != "SLEVOLVE_B200_NO_PDL"}
         if value is not None:

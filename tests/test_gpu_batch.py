@@ -78,14 +78,13 @@ def test_programmatic_launches_do_not_change_results():
     captured with it): bit-identical results."""
     from slevolve_b200 import _lib
 
-    lib = _lib.lib()
     ms = _members()
     nsteps = 4
     runs = []
-    prev = lib.sle_set_programmatic_launch(1)
+    prev = _lib.set_programmatic_launch(True)
     try:
-        for mode in (1, 0):
-            lib.sle_set_programmatic_launch(mode)
+        for mode in (True, False):
+            _lib.set_programmatic_launch(mode)
             bt = _batch("mixed", len(ms))
             for s, m in enumerate(ms):
                 bt.load(s, m["love"], m["topo"], m["ice"](0), m["dt"])
@@ -96,7 +95,7 @@ def test_programmatic_launches_do_not_change_results():
             runs.append(res)
             del bt
     finally:
-        lib.sle_set_programmatic_launch(prev)
+        _lib.set_programmatic_launch(prev)
     for k in range(nsteps):
         for s in range(len(ms)):
             _same(runs[0][k][s], runs[1][k][s], (k + 1, s))
