@@ -1,7 +1,7 @@
 """The serving loop's host logic without a GPU: the queue order, admission against the HBM budget
 and the free slots, preemption (snapshot, release, re-admission from the host image) and the
 admitted-footprint accounting, with a stand-in for the slot batch that records what the server
-asks of it."""
+asks of it; the launch-shape candidates the tuner times."""
 
 import threading
 
@@ -144,3 +144,17 @@ def test_preemption_and_resume():
     assert running[0].req is low and bt.log[-1] == ("restore", 0, 0)
     assert low._run is None and running[0].image is None
     assert srv.used == footprint(low)
+
+
+def test_tuning_candidates():
+    from slevolve_b200 import tuning
+
+    c32 = tuning.candidates(32)
+    assert len(c32) == 8 and tuning.DEFAULT in c32
+    assert {c["fields_per_launch"] for c in c32} == {16, 32}
+    assert all(c["stages"] in tuning.STAGES and c["fold_rows"] in tuning.FOLD_ROWS for c in c32)
+    # launches wider than the list are the list's own width
+    assert {c["fields_per_launch"] for c in tuning.candidates(20)} == {16, 20}
+    c8 = tuning.candidates(8)
+    assert {c["fields_per_launch"] for c in c8} == {8} and len(c8) == 4
+    assert {c["fields_per_launch"] for c in tuning.candidates(0)} == {1}
